@@ -1,0 +1,337 @@
+"""FP64 NumPy restatement of CuboPtycho's single-slice gradient descent — TEST INFRASTRUCTURE ONLY.
+
+This module is an oracle: only ``tests/``, ``__graft_entry__.smoke()`` and ``bench.py``'s CPU-baseline leg may import it,
+and only to check or time against the CUDA path.  Nothing in ``cubokit_b200`` imports it; the product has no CPU fallback.
+
+It restates, in vectorised NumPy (``np.fft`` is pocketfft in double, NumPy's fft/ifft convention, as CuboKit's
+``FFT2D``), the arithmetic of (paths inside the CuboKit project):
+  * ``Sources/CuboPtycho/Ptychography.swift:142-172``  ``PtychographyProbe.build``
+  * ``Sources/CuboPtycho/Ptychography.swift:218-406``  ``SingleslicePtychography.reconstruct`` (Double path)
+  * ``Sources/CuboPtycho/Ptychography.swift:474``      ``frequency``
+  * ``Sources/CuboPtycho/PtychographyConstraints.swift:9-83``  probe constraints
+  * ``Sources/CuboPtycho/PtychographyPreparation.swift:244-259``  ``initialProbe`` energy scaling
+Position correction (``Ptychography.swift:371-377,411-472``) is not part of the GPU path and is not restated here.
+
+Pinned against the py4DSTEM fixtures of CuboKit's own tests (``tests/golden/*.npz``) by ``tests/test_oracle.py``.
+"""
+from __future__ import annotations
+
+import math
+from dataclasses import dataclass
+
+import numpy as np
+
+try:  # scipy's erf is vectorised; math.erf is the fallback
+    from scipy.special import erf as _erf
+except Exception:  # pragma: no cover
+    _erf = np.vectorize(math.erf)
+
+
+class PtychographyError(ValueError):
+    """``PtychographyError.invalidInput`` (``Ptychography.swift:24-27``)."""
+
+
+def frequency(k, n):
+    """``fftfreq`` sample ``k`` of ``n`` (``Ptychography.swift:474``)."""
+    k = np.asarray(k)
+    return np.where(k < (n + 1) // 2, k, k - n) / n
+
+
+def fftfreq_grid(rows, columns):
+    return frequency(np.arange(rows), rows), frequency(np.arange(columns), columns)
+
+
+@dataclass
+class AberrationTerm:
+    """``PtychographyAberrationTerm`` (``Ptychography.swift:101-133``)."""
+    radial_order: int
+    angular_order: int
+    sine: bool
+    coefficient: float
+
+    @staticmethod
+    def polar(radial_order, angular_order, magnitude, azimuth):
+        if angular_order == 0:
+            return [AberrationTerm(radial_order, 0, False, magnitude)]
+        m = float(angular_order)
+        return [AberrationTerm(radial_order, angular_order, False, magnitude * math.cos(m * azimuth)),
+                AberrationTerm(radial_order, angular_order, True, magnitude * math.sin(m * azimuth))]
+
+    def valid(self):
+        return (math.isfinite(self.coefficient) and 1 <= self.radial_order <= 64 and self.angular_order >= 0
+                and (not self.sine or self.angular_order > 0))
+
+    def phase(self, alpha, azimuth):
+        radial = alpha ** (self.radial_order + 1) / (self.radial_order + 1)
+        if self.angular_order == 0:
+            return self.coefficient * radial
+        angle = self.angular_order * azimuth
+        return self.coefficient * radial * (np.sin(angle) if self.sine else np.cos(angle))
+
+
+def probe_build(rows, columns, row_sampling, column_sampling, wavelength, cutoff, rolloff=0.002, defocus=0.0,
+                astigmatism=0.0, astigmatism_angle=0.0, spherical_aberration=0.0, higher_order=()):
+    """Corner-centred unit-norm probe (``Ptychography.swift:142-172``)."""
+    vals = [row_sampling, column_sampling, wavelength, cutoff]
+    if not (rows > 1 and columns > 1 and all(math.isfinite(v) and v > 0 for v in vals)
+            and math.isfinite(rolloff) and rolloff >= 0
+            and all(math.isfinite(v) for v in (defocus, astigmatism, astigmatism_angle, spherical_aberration))
+            and all(t.valid() for t in higher_order)):
+        raise PtychographyError("invalid probe parameters")
+    fr, fc = fftfreq_grid(rows, columns)
+    qr = (fr / row_sampling)[:, None] * np.ones((1, columns))
+    qc = np.ones((rows, 1)) * (fc / column_sampling)[None, :]
+    alpha = np.hypot(qr, qc) * wavelength
+    angle = np.arctan2(qc, qr)
+    if rolloff > 0:
+        soft = np.where(alpha > cutoff, 0.0, 0.5 * (1 + np.cos(np.pi * (alpha - cutoff + rolloff) / rolloff)))
+        aperture = np.where(alpha > cutoff - rolloff, soft, 1.0)
+    else:
+        aperture = np.where(alpha < cutoff, 1.0, 0.0)
+    a2 = alpha * alpha
+    phase = a2 / 2 * (-defocus + astigmatism * np.cos(2 * (angle - astigmatism_angle))) + a2 * a2 / 4 * spherical_aberration
+    for t in higher_order:
+        phase = phase + t.phase(alpha, angle)
+    chi = 2 * np.pi / wavelength * phase
+    spec = aperture * np.cos(chi) - 1j * aperture * np.sin(chi)
+    p = np.fft.ifft2(spec)
+    norm = math.sqrt(float(np.sum(p.real ** 2 + p.imag ** 2)))
+    if not (norm > 0 and math.isfinite(norm)):
+        raise PtychographyError("probe without intensity")
+    return p / norm
+
+
+def initial_probe(rows, columns, sampling_row, sampling_column, wavelength, semiangle, rolloff=2.0, defocus=0.0,
+                  astigmatism=0.0, astigmatism_angle=0.0, spherical_aberration=0.0, higher_order=(), mean_intensity=1.0):
+    """Probe scaled so ``sum |fft2(probe)|^2 == mean_intensity`` (``PtychographyPreparation.swift:244-259``)."""
+    if not (math.isfinite(mean_intensity) and mean_intensity > 0):
+        raise PtychographyError("mean intensity")
+    p = probe_build(rows, columns, sampling_row, sampling_column, wavelength, semiangle / 1e3, rolloff / 1e3, defocus,
+                    astigmatism, astigmatism_angle, spherical_aberration, higher_order)
+    energy = float(np.sum(np.abs(np.fft.fft2(p)) ** 2))
+    return p * math.sqrt(mean_intensity / energy)
+
+
+# ---------------------------------------------------------------- probe constraints (PtychographyConstraints.swift)
+
+def probe_center_of_mass(p):
+    """``PtychographyConstraints.swift:9-18``."""
+    rows, columns = p.shape
+    w = p.real ** 2 + p.imag ** 2
+    total = float(w.sum())
+    if not (total > 0 and math.isfinite(total)):
+        return None
+    fr, fc = fftfreq_grid(rows, columns)
+    return float((fr * rows) @ w.sum(axis=1)) / total, float(w.sum(axis=0) @ (fc * columns)) / total
+
+
+def fourier_shift(p, row, column):
+    """``PtychographyConstraints.swift:21-31``: ``out[x] = in[x - shift]``."""
+    rows, columns = p.shape
+    fr, fc = fftfreq_grid(rows, columns)
+    phase = -2 * np.pi * (fr[:, None] * row + fc[None, :] * column)
+    return np.fft.ifft2(np.fft.fft2(p) * (np.cos(phase) + 1j * np.sin(phase)))
+
+
+def center_of_mass_constraint(p):
+    com = probe_center_of_mass(p)
+    return p if com is None else fourier_shift(p, -com[0], -com[1])
+
+
+def amplitude_constraint(p, radius, width):
+    """``PtychographyConstraints.swift:40-55``."""
+    rows, columns = p.shape
+    before = float(np.sum(p.real ** 2 + p.imag ** 2))
+    sigma = math.sqrt(math.pi) / width
+    fr, fc = fftfreq_grid(rows, columns)
+    d = np.hypot(fr[:, None], fc[None, :]) - radius
+    mask = 0.5 * (1 - _erf(sigma * d / (1 - d * d)))
+    q = p * mask
+    after = float(np.sum(q.real ** 2 + q.imag ** 2))
+    if not (before > 0 and after > 0):
+        return q
+    return q * math.sqrt(before / after)
+
+
+def aperture_constraint(p, aperture):
+    """``PtychographyConstraints.swift:59-71``."""
+    before = float(np.sum(p.real ** 2 + p.imag ** 2))
+    f = np.fft.fft2(p)
+    ph = np.arctan2(f.imag, f.real)
+    q = np.fft.ifft2(aperture * np.cos(ph) + 1j * aperture * np.sin(ph))
+    after = float(np.sum(q.real ** 2 + q.imag ** 2))
+    if not (before > 0 and after > 0):
+        return q
+    return q * math.sqrt(before / after)
+
+
+# ---------------------------------------------------------------- the engine
+
+def round_half_even(x):
+    return np.round(x)  # numpy rounds half to even
+
+
+def patch_indices(rows, columns, object_rows, object_columns, rr, cc):
+    """Periodic corner-centred patch indices ``Ptychography.swift:321-336`` for integer centres ``rr, cc`` (P,)."""
+    ro = np.arange(rows)
+    ro = np.where(ro < (rows + 1) // 2, ro, ro - rows)
+    co = np.arange(columns)
+    co = np.where(co < (columns + 1) // 2, co, co - columns)
+    r = np.mod(rr[:, None] + ro[None, :], object_rows)
+    c = np.mod(cc[:, None] + co[None, :], object_columns)
+    return (r[:, :, None] * object_columns + c[:, None, :]).reshape(len(rr), rows * columns)
+
+
+def shifted_probes(probe_spectrum, dr, dc):
+    """``Ptychography.swift:303-320``: ``ifft2(spectrum * ramp(dr, dc))`` for each position, grouped by its fraction."""
+    rows, columns = probe_spectrum.shape
+    fr, fc = fftfreq_grid(rows, columns)
+    out = np.empty((len(dr), rows, columns), np.complex128)
+    keys = {}
+    for i, key in enumerate(zip(dr.tolist(), dc.tolist())):
+        keys.setdefault(key, []).append(i)
+    for (a, b), idx in keys.items():
+        ar = -2 * np.pi * fr * a
+        ac = -2 * np.pi * fc * b
+        ramp = (np.cos(ar) + 1j * np.sin(ar))[:, None] * (np.cos(ac) + 1j * np.sin(ac))[None, :]
+        out[idx] = np.fft.ifft2(probe_spectrum * ramp)
+    return out
+
+
+def error_divisor(amplitudes, count, error_normalization, mean_intensity):
+    """``Ptychography.swift:40-47``."""
+    if error_normalization == "meanIntensity":
+        d = mean_intensity * count
+    else:
+        d = float(np.sum(np.asarray(amplitudes, np.float64) ** 2))
+    if not (math.isfinite(d) and d > 0):
+        raise PtychographyError("error normalisation")
+    return d
+
+
+def validate(amplitudes, positions, object_shape, probe_shape, iterations, step_size, normalization_minimum,
+             radius, width, probe_support_mask):
+    """The refusals of ``Ptychography.swift:247-259``."""
+    n = probe_shape[0] * probe_shape[1]
+    count = len(positions)
+    a = np.asarray(amplitudes, np.float64)
+    pos = np.asarray(positions, np.float64).reshape(-1, 2) if count else np.zeros((0, 2))
+    ok = (count > 0 and a.size == count * n and np.all(np.isfinite(a)) and np.all(a >= 0)
+          and iterations >= 0 and math.isfinite(step_size) and step_size > 0
+          and math.isfinite(normalization_minimum) and 0 <= normalization_minimum <= 1
+          and np.all(np.isfinite(pos)) and np.all(np.abs(pos) < float((2 ** 63 - 1) // 4))
+          and math.isfinite(radius) and 0 <= radius <= 0.5 and math.isfinite(width) and 0 < width <= 0.5
+          and object_shape[0] >= probe_shape[0] and object_shape[1] >= probe_shape[1]
+          and (probe_support_mask is None or np.asarray(probe_support_mask).size == n))
+    if not ok:
+        raise PtychographyError("invalid input")
+
+
+def reconstruct(amplitudes, positions, obj, probe, iterations=8, step_size=0.5, normalization_minimum=1.0,
+                fix_probe=False, pure_phase_object=False, constrain_object_amplitude=True,
+                fix_probe_center_of_mass=False, constrain_probe_amplitude=False,
+                probe_amplitude_relative_radius=0.5, probe_amplitude_relative_width=0.05,
+                fix_probe_aperture=False, probe_support_mask=None, error_normalization="suppliedAmplitudeEnergy",
+                mean_intensity=None, progress=None):
+    """``SingleslicePtychography.reconstruct`` Double path (``Ptychography.swift:218-406``), positions fixed.
+
+    ``amplitudes`` (P, R, C) or flat; ``positions`` (P, 2) rows/columns in object pixels; ``obj`` (OR, OC) and
+    ``probe`` (R, C) complex.  Returns ``(object, probe, errors)``.
+    """
+    obj = np.array(obj, np.complex128)
+    probe = np.array(probe, np.complex128)
+    rows, columns = probe.shape
+    n = rows * columns
+    positions = np.asarray(positions, np.float64).reshape(-1, 2)
+    count = len(positions)
+    validate(amplitudes, positions, obj.shape, probe.shape, iterations, step_size, normalization_minimum,
+             probe_amplitude_relative_radius, probe_amplitude_relative_width, probe_support_mask)
+    amp = np.asarray(amplitudes, np.float64).reshape(count, n)
+    divisor = error_divisor(amp, count, error_normalization, mean_intensity)
+    initial_aperture = np.abs(np.fft.fft2(probe)) if fix_probe_aperture else None
+    object_rows, object_columns = obj.shape
+    rr = round_half_even(positions[:, 0])
+    cc = round_half_even(positions[:, 1])
+    dr = positions[:, 0] - rr
+    dc = positions[:, 1] - cc
+    idx = patch_indices(rows, columns, object_rows, object_columns, rr.astype(np.int64), cc.astype(np.int64))
+    mask = None if probe_support_mask is None else np.asarray(probe_support_mask, bool).reshape(rows, columns)
+    m = normalization_minimum
+    errors = []
+    o = obj.reshape(-1).copy()
+    p = probe.copy()
+    for it in range(iterations):
+        spectrum = np.fft.fft2(p)
+        s = shifted_probes(spectrum, dr, dc).reshape(count, n)
+        op = o[idx]
+        psi = (s * op).reshape(count, rows, columns)
+        f = np.fft.fft2(psi).reshape(count, n)
+        mag = np.abs(f)
+        error = float(np.sum((amp - mag) ** 2))
+        with np.errstate(divide="ignore", invalid="ignore"):
+            scale = np.where(mag > 0, amp / np.where(mag > 0, mag, 1.0), 0.0)
+        proj = np.where(mag > 0, scale * f - f, amp + 0j)
+        d = np.fft.ifft2(proj.reshape(count, rows, columns)).reshape(count, n)
+        grad_o = np.zeros(o.size, np.complex128)
+        pn = np.zeros(o.size)
+        np.add.at(grad_o, idx.ravel(), (np.conj(s) * d).ravel())
+        np.add.at(pn, idx.ravel(), (s.real ** 2 + s.imag ** 2).ravel())
+        grad_p = np.sum(np.conj(op) * d, axis=0).reshape(rows, columns)
+        on = np.sum(op.real ** 2 + op.imag ** 2, axis=0).reshape(rows, columns)
+        max_pn, max_on = pn.max(), on.max()
+
+        def inverse(local, maximum):
+            return 1 / np.sqrt(1e-16 + ((1 - m) * local) ** 2 + (m * maximum) ** 2)
+
+        o = o + step_size * inverse(pn, max_pn) * grad_o
+        if constrain_object_amplitude or pure_phase_object:
+            a = np.abs(o)
+            target = np.ones_like(a) if pure_phase_object else np.minimum(a, 1.0)
+            with np.errstate(divide="ignore", invalid="ignore"):
+                o = np.where(a > 0, o * (target / np.where(a > 0, a, 1.0)), target + 0j)
+        if not fix_probe:
+            p = p + step_size * inverse(on, max_on) * grad_p
+            if fix_probe_center_of_mass:
+                p = center_of_mass_constraint(p)
+            if fix_probe_aperture:
+                p = aperture_constraint(p, initial_aperture)
+            if constrain_probe_amplitude:
+                p = amplitude_constraint(p, probe_amplitude_relative_radius, probe_amplitude_relative_width)
+        if mask is not None:
+            p = np.where(mask, p, 0)
+        errors.append(error / divisor)
+        if progress is not None:
+            progress(it + 1, iterations)
+    return o.reshape(object_rows, object_columns), p, np.asarray(errors)
+
+
+def loss_and_gradients(amplitudes, positions, obj, probe):
+    """The real loss ``L = sum_p sum_k (|F_k| - A_k)^2`` and its gradients, for INTEGER positions.
+
+    With the unnormalised forward FFT, ``dL/dRe O + i dL/dIm O = -2 n * sum_p conj(S) dpsi`` and likewise for the probe
+    with ``conj(O) dpsi`` (the accumulations of ``Ptychography.swift:351-358``).  Returns ``(L, gO, gP)``.
+    """
+    obj = np.asarray(obj, np.complex128)
+    probe = np.asarray(probe, np.complex128)
+    rows, columns = probe.shape
+    n = rows * columns
+    positions = np.asarray(positions, np.float64).reshape(-1, 2)
+    count = len(positions)
+    amp = np.asarray(amplitudes, np.float64).reshape(count, n)
+    rr = round_half_even(positions[:, 0]).astype(np.int64)
+    cc = round_half_even(positions[:, 1]).astype(np.int64)
+    idx = patch_indices(rows, columns, obj.shape[0], obj.shape[1], rr, cc)
+    o = obj.reshape(-1)
+    s = np.broadcast_to(probe.reshape(1, n), (count, n))
+    op = o[idx]
+    f = np.fft.fft2((s * op).reshape(count, rows, columns)).reshape(count, n)
+    mag = np.abs(f)
+    loss = float(np.sum((mag - amp) ** 2))
+    with np.errstate(divide="ignore", invalid="ignore"):
+        scale = np.where(mag > 0, amp / np.where(mag > 0, mag, 1.0), 0.0)
+    proj = np.where(mag > 0, scale * f - f, amp + 0j)
+    d = np.fft.ifft2(proj.reshape(count, rows, columns)).reshape(count, n)
+    go = np.zeros(o.size, np.complex128)
+    np.add.at(go, idx.ravel(), (np.conj(s) * d).ravel())
+    gp = np.sum(np.conj(op) * d, axis=0)
+    return loss, (-2 * n * go).reshape(obj.shape), (-2 * n * gp).reshape(rows, columns)

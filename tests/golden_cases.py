@@ -1,0 +1,187 @@
+"""The golden cases of CuboKit's single-slice pins (``tests/golden/*.npz``) as engine calls.
+
+Each case carries the inputs of one ``SingleslicePtychography.reconstruct`` call of CuboKit's tests (file:line in the
+case's ``source``) and the py4DSTEM outputs it is pinned to.  The metric and bound are the reference's:
+``max|a - b| / max(1, max|b|) < 2e-6`` for the Double engine (``PtychographyTests.swift:28-31``).
+"""
+from __future__ import annotations
+
+from dataclasses import dataclass, field
+from pathlib import Path
+
+import numpy as np
+
+GOLDEN = Path(__file__).resolve().parent / "golden"
+
+
+def gap(a, b):
+    """``PtychographyTests.swift:28-31``: max abs difference over max(1, max |b|); a NaN fails."""
+    a = np.asarray(a, np.float64).ravel()
+    b = np.asarray(b, np.float64).ravel()
+    if a.shape != b.shape or not np.all(np.isfinite(a)):
+        return np.inf
+    return float(np.max(np.abs(a - b)) / max(1.0, float(np.max(np.abs(b)))))
+
+
+def complex_gap(a, b):
+    return max(gap(np.real(a), np.real(b)), gap(np.imag(a), np.imag(b)))
+
+
+def load(name):
+    return dict(np.load(GOLDEN / f"{name}.npz"))
+
+
+def _cx(z, key, shape):
+    return (z[key + "_re"] + 1j * z[key + "_im"]).reshape(shape)
+
+
+@dataclass
+class Case:
+    name: str
+    source: str
+    amplitudes: np.ndarray
+    positions: np.ndarray
+    object: np.ndarray
+    probe: np.ndarray
+    kwargs: dict
+    expect_object: np.ndarray
+    expect_probe: np.ndarray
+    expect_errors: np.ndarray
+    extra: dict = field(default_factory=dict)
+
+    def result_gap(self, obj, probe, errors):
+        return max(complex_gap(obj, self.expect_object), complex_gap(probe, self.expect_probe),
+                   gap(errors, self.expect_errors))
+
+
+def engine_cases():
+    """Every single-slice engine pin of CuboKit's tests."""
+    cases = []
+    z = load("ptycho")
+    R, C, OR, OC = (int(z[k]) for k in ("rows", "columns", "objectRows", "objectColumns"))
+    probe = _cx(z, "initialProbe", (R, C))
+    obj = _cx(z, "initialObject", (OR, OC))
+    off = _cx(z, "offcentreProbe", (R, C))
+    mean = dict(error_normalization="meanIntensity", mean_intensity=float(z["meanIntensity"]))
+    amps = z["amplitudes"].reshape(-1, R, C)
+    pos = z["positions"]
+    cases.append(Case("ptycho.main", "PtychographyTests.swift:48-60", amps, pos, obj, probe,
+                      dict(iterations=3, step_size=0.35, normalization_minimum=0.7, **mean),
+                      _cx(z, "object", (OR, OC)), _cx(z, "probe", (R, C)), z["errors"]))
+    for i in range(int(z["variants"])):
+        v = lambda k: z[f"variant{i}_" + k]
+        cases.append(Case(f"ptycho.variant{i}", "PtychographyTests.swift:61-70", amps, pos, obj, probe,
+                          dict(iterations=3, step_size=float(v("step")), normalization_minimum=float(v("minimum")),
+                               fix_probe=bool(v("fixProbe")), pure_phase_object=bool(v("purePhase")), **mean),
+                          _cx(z, f"variant{i}_object", (OR, OC)), _cx(z, f"variant{i}_probe", (R, C)), v("errors")))
+    for i in range(int(z["constraintCases"])):
+        v = lambda k: z[f"constraint{i}_" + k]
+        cases.append(Case(f"ptycho.constraint.{v('name')}", "PtychographyTests.swift:104-118", amps, pos, obj, off,
+                          dict(iterations=3, step_size=0.35, normalization_minimum=0.7,
+                               fix_probe_center_of_mass=bool(v("fixProbeCenterOfMass")),
+                               constrain_probe_amplitude=bool(v("constrainProbeAmplitude")),
+                               probe_amplitude_relative_radius=float(v("radius")),
+                               probe_amplitude_relative_width=float(v("width")), **mean),
+                          _cx(z, f"constraint{i}_object", (OR, OC)), _cx(z, f"constraint{i}_probe", (R, C)),
+                          v("errors")))
+    z = load("odd")
+    R, C, OR, OC = (int(z[k]) for k in ("rows", "columns", "objectRows", "objectColumns"))
+    probe = _cx(z, "startProbe", (R, C))
+    obj = _cx(z, "initialObject", (OR, OC))
+    mean = dict(error_normalization="meanIntensity", mean_intensity=float(z["meanIntensity"]))
+    for i in range(int(z["cases"])):
+        v = lambda k: z[f"case{i}_" + k]
+        cases.append(Case(f"odd.{v('name')}", "OddSizeTests.swift:132-146", z["amplitudes"].reshape(-1, R, C),
+                          z["positions"], obj, probe,
+                          dict(iterations=3, step_size=0.35, normalization_minimum=0.7,
+                               fix_probe_center_of_mass=bool(v("fixProbeCenterOfMass")),
+                               constrain_probe_amplitude=bool(v("constrainProbeAmplitude")),
+                               probe_amplitude_relative_radius=float(v("radius")),
+                               probe_amplitude_relative_width=float(v("width")),
+                               fix_probe_aperture=bool(v("aperture")),
+                               probe_support_mask=z["support"].reshape(R, C) if bool(v("support")) else None, **mean),
+                          _cx(z, f"case{i}_object", (OR, OC)), _cx(z, f"case{i}_probe", (R, C)), v("errors")))
+    z = load("engines")
+    R, C, OR, OC = (int(z[k]) for k in ("rows", "columns", "objectRows", "objectColumns"))
+    probe = _cx(z, "startProbe", (R, C))
+    obj = _cx(z, "initialObject", (OR, OC))
+    mean = dict(error_normalization="meanIntensity", mean_intensity=float(z["meanIntensity"]))
+    for i in range(int(z["cases"])):
+        v = lambda k: z[f"case{i}_" + k]
+        cases.append(Case(f"engines.{v('name')}", "EngineTests.swift:262-305", z["amplitudes"].reshape(-1, R, C),
+                          z["positions"], obj, probe,
+                          dict(iterations=3, step_size=0.35, normalization_minimum=0.7, fix_probe=bool(v("fixProbe")),
+                               fix_probe_center_of_mass=bool(v("fixProbeCenterOfMass")),
+                               constrain_probe_amplitude=bool(v("constrainProbeAmplitude")),
+                               probe_amplitude_relative_radius=float(v("radius")),
+                               probe_amplitude_relative_width=float(v("width")),
+                               fix_probe_aperture=bool(v("fixProbeAperture")),
+                               probe_support_mask=z["support"].reshape(R, C), **mean),
+                          _cx(z, f"case{i}_object", (OR, OC)), _cx(z, f"case{i}_probe", (R, C)), v("errors")))
+    p = load("ptycho")
+    o = load("options")
+    R, C, OR, OC = (int(p[k]) for k in ("rows", "columns", "objectRows", "objectColumns"))
+    probe = _cx(p, "initialProbe", (R, C))
+    start = _cx(o, "startObject", (OR, OC))
+    mean = dict(error_normalization="meanIntensity", mean_intensity=float(p["meanIntensity"]))
+    for i in range(int(o["amplitudeCases"])):
+        v = lambda k: o[f"amp{i}_" + k]
+        cases.append(Case(f"options.{v('name')}", "OptionsTests.swift:63-80", p["amplitudes"].reshape(-1, R, C),
+                          p["positions"], start, probe,
+                          dict(iterations=int(v("iterations")), step_size=float(v("step")), normalization_minimum=0.7,
+                               fix_probe=bool(v("fixProbe")), pure_phase_object=bool(v("purePhase")),
+                               constrain_object_amplitude=False, **mean),
+                          _cx(o, f"amp{i}_object", (OR, OC)), _cx(o, f"amp{i}_probe", (R, C)), v("errors"),
+                          extra=dict(maxAmplitude=float(v("maxAmplitude")))))
+    return cases
+
+
+def probe_cases():
+    """Probe-builder pins: (name, kwargs of PtychographyProbe.build, expected probe)."""
+    out = []
+    z = load("ptycho")
+    R, C = int(z["rows"]), int(z["columns"])
+    wl = float(z["wavelength"])
+    base = dict(row_sampling=0.8, column_sampling=1.1, wavelength=wl, cutoff=0.018, defocus=70, astigmatism=25,
+                astigmatism_angle=0.31, spherical_aberration=2e4)
+    out.append(("ptycho.builtProbe", dict(rows=R, columns=C, rolloff=0.002, **base), _cx(z, "builtProbe", (R, C))))
+    out.append(("ptycho.rectangularProbe", dict(rows=7, columns=10, rolloff=0.0, **base),
+                _cx(z, "rectangularProbe", (7, 10))))
+    z = load("odd")
+    R, C = int(z["rows"]), int(z["columns"])
+    out.append(("odd.builtProbe", dict(rows=R, columns=C, row_sampling=float(z["rowSampling"]),
+                                       column_sampling=float(z["columnSampling"]), wavelength=float(z["wavelength"]),
+                                       cutoff=0.018, rolloff=0.002, defocus=70, astigmatism=25, astigmatism_angle=0.31,
+                                       spherical_aberration=2e4), _cx(z, "builtProbe", (R, C))))
+    o = load("options")
+    g = lambda k: o["probes_" + k]
+    R, C = int(g("rows")), int(g("columns"))
+    for i in range(int(o["probeCases"])):
+        v = lambda k: o[f"probe{i}_" + k]
+        terms = []
+        for n, m, mag, az in v("terms"):
+            if int(m) == 0:
+                terms.append((n, 0, 0.0, mag))
+            else:
+                terms.append((n, m, 0.0, mag * np.cos(m * az)))
+                terms.append((n, m, 1.0, mag * np.sin(m * az)))
+        out.append((f"options.{v('name')}", dict(rows=R, columns=C, row_sampling=float(g("rowSampling")),
+                                                 column_sampling=float(g("columnSampling")),
+                                                 wavelength=float(g("wavelength")), cutoff=float(g("cutoff")),
+                                                 rolloff=float(g("rolloff")), defocus=float(v("defocus")),
+                                                 astigmatism=float(v("astigmatism")),
+                                                 astigmatism_angle=float(v("astigmatismAngle")),
+                                                 spherical_aberration=float(v("sphericalAberration")),
+                                                 terms=np.asarray(terms, np.float64).reshape(-1, 4)),
+                    _cx(o, f"probe{i}_probe", (R, C))))
+    for i in range(int(o["appCases"])):
+        v = lambda k: o[f"app{i}_" + k]
+        c12a, c12b = float(v("c12a")), float(v("c12b"))
+        out.append((f"options.app.{v('name')}", dict(rows=R, columns=C, row_sampling=float(g("rowSampling")),
+                                                     column_sampling=float(g("columnSampling")),
+                                                     wavelength=float(g("wavelength")), cutoff=float(g("cutoff")),
+                                                     rolloff=float(g("rolloff")), defocus=float(v("defocus")),
+                                                     astigmatism=float(np.hypot(c12a, c12b)),
+                                                     astigmatism_angle=float(0.5 * np.arctan2(c12b, c12a)),
+                                                     terms=v("terms")), _cx(o, f"app{i}_probe", (R, C))))
+    return out

@@ -1,0 +1,157 @@
+"""The oracles (C and NumPy FP64 restatements of CuboPtycho's Double path) against CuboKit's own py4DSTEM pins.
+
+Bound and metric are the reference's: ``max|a - b| / max(1, max|b|) < 2e-6`` (``PtychographyTests.swift:28-31,60``).
+"""
+import numpy as np
+import pytest
+
+from oracle import c_oracle, numpy_oracle
+from tests import golden_cases as gc
+from tests import scenes
+
+ENGINE_CASES = gc.engine_cases()
+PROBE_CASES = gc.probe_cases()
+
+
+def _numpy_call(case):
+    kw = dict(case.kwargs)
+    return numpy_oracle.reconstruct(case.amplitudes, case.positions, case.object, case.probe, **kw)
+
+
+def _c_call(case, **extra):
+    kw = dict(case.kwargs)
+    kw.update(extra)
+    return c_oracle.reconstruct(case.amplitudes, case.positions, case.object, case.probe, **kw)
+
+
+@pytest.mark.parametrize("case", ENGINE_CASES, ids=[c.name for c in ENGINE_CASES])
+def test_c_oracle_against_pins(case):
+    o, p, e = _c_call(case)
+    g = case.result_gap(o, p, e)
+    assert g < 2e-6, (case.name, case.source, g)
+
+
+@pytest.mark.parametrize("case", ENGINE_CASES, ids=[c.name for c in ENGINE_CASES])
+def test_numpy_oracle_against_pins(case):
+    o, p, e = _numpy_call(case)
+    g = case.result_gap(o, p, e)
+    assert g < 2e-6, (case.name, case.source, g)
+
+
+def test_c_and_numpy_oracles_agree_to_roundoff():
+    for case in ENGINE_CASES[:4]:
+        a = _c_call(case)
+        b = _numpy_call(case)
+        for x, y in zip(a, b):
+            assert gc.complex_gap(x, y) < 1e-11, case.name
+
+
+def test_uncapped_object_really_exceeds_one():
+    """``OptionsTests.swift:71-78``: the pinned uncapped runs leave |object| > 1, and the cap changes the result."""
+    for case in [c for c in ENGINE_CASES if c.name.startswith("options.") and not c.kwargs["pure_phase_object"]]:
+        o, _, _ = _c_call(case)
+        amp = np.abs(o).max()
+        assert amp > 1.002 and abs(amp - case.extra["maxAmplitude"]) < 1e-5
+        capped, _, _ = _c_call(case, constrain_object_amplitude=True)
+        assert np.abs(capped).max() <= 1 + 1e-12
+        assert gc.gap(capped.real, o.real) > 1e-3
+
+
+@pytest.mark.parametrize("name,kw,expect", PROBE_CASES, ids=[c[0] for c in PROBE_CASES])
+def test_probe_build_against_pins(name, kw, expect):
+    kw = dict(kw)
+    terms = kw.pop("terms", None)
+    got = c_oracle.probe_build(**kw, terms=terms)
+    bound = 1e-8 if name.startswith("options.app.") else 2e-6  # OptionsTests.swift:143 vs :107
+    assert gc.complex_gap(got, expect) < bound, name
+    ho = [] if terms is None else [numpy_oracle.AberrationTerm(int(t[0]), int(t[1]), bool(t[2]), float(t[3])) for t in terms]
+    got_np = numpy_oracle.probe_build(kw["rows"], kw["columns"], kw["row_sampling"], kw["column_sampling"],
+                                      kw["wavelength"], kw["cutoff"], kw.get("rolloff", 0.002), kw.get("defocus", 0.0),
+                                      kw.get("astigmatism", 0.0), kw.get("astigmatism_angle", 0.0),
+                                      kw.get("spherical_aberration", 0.0), ho)
+    assert gc.complex_gap(got_np, expect) < bound, name
+
+
+def test_initial_probe_energy_scaling():
+    """``OptionsTests.swift:115-123``: ``PtychographyPreparation.initialProbe`` (probe build + energy scaling)."""
+    o = gc.load("options")
+    g = lambda k: o["initial_" + k]
+    terms = []
+    for n, m, mag, az in g("terms"):
+        terms += numpy_oracle.AberrationTerm.polar(int(n), int(m), float(mag), float(az))
+    p = numpy_oracle.initial_probe(int(g("rows")), int(g("columns")), float(g("samplingRow")),
+                                   float(g("samplingColumn")), float(g("wavelength")), float(g("semiangle")),
+                                   float(g("rolloff")), float(g("defocus")), float(g("astigmatism")),
+                                   float(g("astigmatismAngle")), float(g("sphericalAberration")), terms,
+                                   float(g("meanIntensity")))
+    expect = (o["initial_probe_re"] + 1j * o["initial_probe_im"]).reshape(p.shape)
+    assert gc.complex_gap(p, expect) < 2e-6
+
+
+def test_invalid_inputs_are_refused():
+    """``PtychographyTests.swift:73-85,172-180``, ``SinglePrecisionTests.swift:111-116``."""
+    case = ENGINE_CASES[0]
+    with pytest.raises(ValueError):
+        c_oracle.reconstruct(np.zeros(0), np.zeros((0, 2)), case.object, case.probe)
+    for radius, width in [(-0.1, 0.05), (0.51, 0.05), (np.nan, 0.05), (0.5, 0.0), (0.5, 0.51), (0.5, np.inf)]:
+        with pytest.raises(ValueError):
+            _c_call(case, iterations=1, constrain_probe_amplitude=True, probe_amplitude_relative_radius=radius,
+                    probe_amplitude_relative_width=width)
+    with pytest.raises(ValueError):
+        c_oracle.probe_build(2, 2, 0, 1, 0.02, 0.01)
+    wide = np.full((16, 96), 0.1 + 0j)
+    with pytest.raises(ValueError):
+        c_oracle.reconstruct(np.ones(16 * 96), [[4, 4]], np.ones((80, 80), complex), wide, iterations=1)
+
+
+def test_threaded_oracle_is_deterministic_and_agrees():
+    case = ENGINE_CASES[0]
+    a = _c_call(case, threads=3)
+    b = _c_call(case, threads=3)
+    for x, y in zip(a, b):
+        assert np.array_equal(x, y)
+    c = _c_call(case)
+    for x, y in zip(a, c):
+        assert gc.complex_gap(x, y) < 1e-12
+
+
+def test_float_path_agrees_with_double_on_the_gaussian_scene():
+    """``SinglePrecisionTests.swift:58-72``: object 1e-4, probe 1e-5 absolute, errors 1e-5 relative, convergence."""
+    s = scenes.gaussian_scene()
+    ref = c_oracle.reconstruct(s["amplitudes"], s["positions"], s["object"], s["probe"], iterations=3)
+    sgl = c_oracle.reconstruct(s["amplitudes"], s["positions"], s["object"], s["probe"], iterations=3, single=True)
+    assert np.max(np.abs(ref[0].real - sgl[0].real)) <= 1e-4 and np.max(np.abs(ref[0].imag - sgl[0].imag)) <= 1e-4
+    assert np.max(np.abs(ref[1].real - sgl[1].real)) <= 1e-5 and np.max(np.abs(ref[1].imag - sgl[1].imag)) <= 1e-5
+    assert np.all(np.abs(ref[2] - sgl[2]) <= 1e-5 * np.abs(ref[2]))
+    assert sgl[2][2] < sgl[2][0]
+
+
+@pytest.mark.parametrize("shape", [(32, 48), (22, 21), (13, 26)])
+def test_float_path_agrees_with_double_on_fractional_nonsquare_scenes(shape):
+    """``SinglePrecisionTests.swift:148-210`` (a subset of its sizes)."""
+    s = scenes.nonsquare_scene(shape[0], shape[1], 96 if shape == (32, 48) else 2 * max(shape) + 40)
+    ref = c_oracle.reconstruct(s["amplitudes"], s["positions"], s["object"], s["probe"], iterations=3)
+    sgl = c_oracle.reconstruct(s["amplitudes"], s["positions"], s["object"], s["probe"], iterations=3, single=True)
+    assert np.max(np.abs(ref[0] - sgl[0])) <= 1.5e-4
+    assert np.max(np.abs(ref[1] - sgl[1])) <= 1.5e-5
+    assert np.all(np.abs(ref[2] - sgl[2]) <= 1e-4 * np.abs(ref[2]))
+    assert ref[2][2] < ref[2][0]
+
+
+def test_adjoint_matches_central_differences_in_fp64():
+    """The loss gradient ``-2 n sum conj(S) dpsi`` (object) and ``-2 n sum conj(O) dpsi`` (probe) of the reference's
+    accumulations, against central differences, integer positions."""
+    s = scenes.raster_scene(scan=4, det=16, step=4, seed=3)
+    amps = s["amplitudes"] * 1.05  # off the solution, so the gradient is not ~0
+    loss, go, gp = numpy_oracle.loss_and_gradients(amps, s["positions"], s["object"], s["probe"])
+    rng = np.random.default_rng(5)
+    h = 1e-6
+    for _ in range(8):
+        j = tuple(rng.integers(0, n) for n in s["object"].shape)
+        for unit, part in ((1.0, "re"), (1j, "im")):
+            o1 = s["object"].copy(); o1[j] += unit * h
+            o2 = s["object"].copy(); o2[j] -= unit * h
+            fd = (numpy_oracle.loss_and_gradients(amps, s["positions"], o1, s["probe"])[0] -
+                  numpy_oracle.loss_and_gradients(amps, s["positions"], o2, s["probe"])[0]) / (2 * h)
+            an = go[j].real if part == "re" else go[j].imag
+            assert abs(fd - an) <= 1e-6 * max(1.0, abs(an)) + 1e-5 * abs(loss) * h, (j, part, fd, an)
