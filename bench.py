@@ -1,0 +1,328 @@
+"""Benchmark of the single-slice ptychography GD engine on B200.
+
+Workload (the precision-form configuration): 256 x 256 raster scan, step 4 px, 128 x 128 detector, object 1152 x 1152,
+Float32 amplitudes at 1e5 e/pattern, seeded synthetic data (cubokit_b200.synthetic).  One step = one full-batch GD
+iteration over all 65,536 positions.  Metric: positions * iterations / s.
+
+  python bench.py [--gpus N] [--steps K] [--warmup W] [--form fp32|split_bf16] [--impl ours|reference]
+
+`value` is device-timed (CUDA events on the engine's stream) with amplitudes resident in HBM; the 4.3 GB amplitude
+stack and the 8.6 GB residual buffer are far larger than L2, so no flush is needed.  `e2e` is one
+SingleslicePtychography.reconstruct call (the public API) of K iterations from pinned host buffers, host<->device
+copies, validation and plan set-up included, timed by the wall clock around the blocking call.  With --gpus N > 1
+(torchrun), every rank runs an independent replica on its own GPU (the path has no cross-GPU exchange: "replicas
+only"); value = sum over ranks, time = max over ranks.  --impl reference times the FP64 C restatement of CuboPtycho's
+Double CPU path (oracle/, OpenMP over all host cores) on a bounded sample of the same workload.
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import math
+import os
+import statistics
+import subprocess
+import sys
+import tempfile
+import threading
+import time
+from pathlib import Path
+
+import numpy as np
+
+ROOT = Path(__file__).resolve().parent
+sys.path.insert(0, str(ROOT))
+
+METRIC = "positions*iter/s, 128^2 det GD: split-BF16 vs FP32 at <=1e-4 object err"
+UNIT = "positions*iter/s"
+SCAN, DET, STEP, DOSE = 256, 128, 4, 1e5
+
+
+def algorithmic(P, n, objects):
+    """Per-iteration algorithmic bytes and flops of the path (amplitudes read once; object and probe complex64 read
+    and written once; two n-point 2-D FFTs and 40 flops per pixel per position)."""
+    bytes_iter = P * 4 * n + 16 * objects + 16 * n
+    flops_iter = P * (10 * n * math.log2(n) + 40 * n)
+    return bytes_iter, flops_iter
+
+
+class ClockSampler:
+    """nvidia-smi clocks and throttle reasons sampled every 200 ms while running."""
+
+    FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+              "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, gpu_index):
+        self.gpu = gpu_index
+        self.proc = None
+        self.path = None
+
+    def __enter__(self):
+        fd, self.path = tempfile.mkstemp(suffix=".csv")
+        os.close(fd)
+        try:
+            self.proc = subprocess.Popen(["nvidia-smi", "-i", str(self.gpu), f"--query-gpu={self.FIELDS}",
+                                          "--format=csv,noheader,nounits", "-lms", "200"],
+                                         stdout=open(self.path, "w"), stderr=subprocess.DEVNULL)
+        except FileNotFoundError:
+            self.proc = None
+        time.sleep(0.3)
+        return self
+
+    def __exit__(self, *exc):
+        if self.proc is not None:
+            self.proc.terminate()
+            try:
+                self.proc.wait(timeout=5)
+            except subprocess.TimeoutExpired:
+                self.proc.kill()
+
+    def summary(self):
+        if not self.path or not os.path.exists(self.path):
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["unsampled"]}
+        rows = [l.split(",") for l in open(self.path).read().strip().splitlines() if l.strip()]
+        os.unlink(self.path)
+        sm, mx, reasons, power = [], [], set(), []
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for r in rows:
+            try:
+                sm.append(float(r[1])); mx.append(float(r[2])); power.append(float(r[3]))
+            except (ValueError, IndexError):
+                continue
+            for name, v in zip(names, r[5:9]):
+                if v.strip() == "Active":
+                    reasons.add(name)
+        if not sm:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["unsampled"]}
+        return {"sm_mhz": statistics.median(sm), "sm_max_mhz": max(mx), "power_w_max": max(power),
+                "samples": len(sm), "reasons": sorted(reasons)}
+
+
+def measured_peaks():
+    p = ROOT / "MEASURED_PEAKS.json"
+    if p.exists():
+        d = json.loads(p.read_text())
+        return d["hbm_gbs"], d.get("bf16_tflops"), "measured"
+    return 6650.0, 1590.0, "fallback"
+
+
+def dist_setup(args):
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    if world > 1:
+        import torch.distributed as dist
+        from datetime import timedelta
+        backend = "gloo" if args.impl == "reference" else "nccl"
+        dist.init_process_group(backend, timeout=timedelta(seconds=600))
+    return world, rank, local
+
+
+def max_over_ranks(v, world):
+    if world == 1:
+        return v
+    import torch
+    import torch.distributed as dist
+    t = torch.tensor([v], dtype=torch.float64, device="cuda" if dist.get_backend() == "nccl" else "cpu")
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return float(t.item())
+
+
+def barrier(world):
+    if world > 1:
+        import torch.distributed as dist
+        dist.barrier()
+
+
+def cpu_oracle_sample(ds, threads, target_s=12.0):
+    """The FP64 C restatement of the Double path on a contiguous subset of the positions (whole detector, whole
+    object), one iteration, sized to about `target_s` seconds; returns positions*iter/s and the sample."""
+    from oracle import c_oracle
+    P = len(ds.positions)
+    amps = ds.amplitudes.reshape(P, -1)
+
+    def run(count):
+        t0 = time.perf_counter()
+        c_oracle.reconstruct(amps[:count].astype(np.float64), ds.positions[:count], ds.object_start, ds.probe,
+                             iterations=1, step_size=0.5, threads=threads)
+        return time.perf_counter() - t0
+
+    count = max(threads, 16)
+    t = run(count)
+    count = int(min(P, max(count, count * target_s / max(t, 1e-3))))
+    t = run(count)
+    return count / t, f"{count} of {P} positions, 1 iteration, full 128x128 detector and 1152x1152 object"
+
+
+def run_reference(args, world, rank):
+    if rank != 0:
+        return
+    from cubokit_b200 import synthetic
+    from oracle import c_oracle
+    threads = c_oracle.host_cores()
+    ds = synthetic_dataset_cpu()
+    P = len(ds.positions)
+    amps = ds.amplitudes.reshape(P, -1)
+    # one step = a bounded sample of the iteration: a fixed subset of positions, scaled to positions*iter/s
+    sample = min(2048, max(threads * 8, 256))
+    times = []
+    for i in range(args.warmup + args.steps):
+        t0 = time.perf_counter()
+        c_oracle.reconstruct(amps[:sample].astype(np.float64), ds.positions[:sample], ds.object_start, ds.probe,
+                             iterations=1, step_size=0.5, threads=threads)
+        dt = time.perf_counter() - t0
+        if i >= args.warmup:
+            times.append(dt)
+    mean = sum(times) / len(times)
+    value = sample / mean
+    line = {"impl": "reference", "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": args.gpus,
+            "steps": args.steps, "warmup": args.warmup, "ms_per_step": mean * 1e3, "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+            "config": {"workload": f"{SCAN}x{SCAN} scan, {DET}x{DET} detector, object 1152x1152, dose 1e5, GD",
+                       "form": "CuboPtycho Double CPU path (FP64 C restatement, OpenMP)",
+                       "sample_positions_per_step": sample, "l2": "n/a (CPU)"},
+            "cpu_baseline": {"value": value, "unit": UNIT, "cores": threads, "kind": "port",
+                             "sample": f"{sample} of {P} positions per step, 1 iteration each"},
+            "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+    print(json.dumps(line), flush=True)
+
+
+def synthetic_dataset_cpu():
+    """The same workload's inputs without a GPU: probe and amplitudes from the NumPy oracle (for the CPU arm only)."""
+    from cubokit_b200 import synthetic
+    from oracle import numpy_oracle
+    import cubokit_b200.ptycho as cp
+    n = DET
+    wavelength = cp.electron_wavelength(300e3)
+    dk = 64.0 / n * 1e-3
+    sampling = wavelength / (dk * n)
+    p = numpy_oracle.probe_build(n, n, sampling, sampling, wavelength, 0.020, 0.002, 100.0)
+    p = p * np.sqrt(DOSE / (n * n * np.sum(np.abs(p) ** 2)))
+    size = SCAN * STEP + n
+    truth = np.exp(1j * synthetic.phase_field(size, size, 1))
+    positions = synthetic.raster(SCAN, n, STEP)
+    # a sample of rows of the raster is enough for the CPU arm; synthesise only what it reads
+    count = 2048
+    idx = numpy_oracle.patch_indices(n, n, size, size, positions[:count, 0].astype(np.int64),
+                                     positions[:count, 1].astype(np.int64))
+    f = np.fft.fft2((p.reshape(1, -1) * truth.reshape(-1)[idx]).reshape(count, n, n))
+    rng = np.random.default_rng(2)
+    amps = np.sqrt(rng.poisson(np.abs(f) ** 2)).astype(np.float32)
+    full = np.zeros((len(positions), n, n), np.float32)
+    full[:count] = amps
+    start = np.exp(1j * np.random.default_rng(3).normal(0, 0.02, (size, size)))
+    return synthetic.Dataset(full, positions, start, p, truth, {})
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=20)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--form", default="fp32", choices=["fp32", "split_bf16"])
+    ap.add_argument("--no-e2e", action="store_true")
+    ap.add_argument("--no-cpu", action="store_true")
+    args = ap.parse_args()
+    world, rank, local = dist_setup(args)
+    if args.impl == "reference":
+        run_reference(args, world, rank)
+        barrier(world)
+        return
+
+    import torch
+    torch.cuda.set_device(local)
+    import cubokit_b200 as cb
+    from cubokit_b200 import synthetic
+
+    ds = synthetic.dataset(SCAN, DET, dose=DOSE, step=STEP, pinned=True, device=local)
+    P, n = len(ds.positions), DET * DET
+    objects = ds.object_start.size
+    ctx = cb.Context(local)
+    plan = cb.Plan(ds.amplitudes, ds.positions, ds.object_start.shape, ds.probe.shape, ctx=ctx, step_size=0.5,
+                   precision=args.form)
+    plan.set_state(ds.object_start, ds.probe)
+    stream = torch.cuda.ExternalStream(ctx.stream, device=torch.device("cuda", local))
+    plan.enqueue(args.warmup)
+    ctx.synchronize()
+    barrier(world)
+    start, stop = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    launches0 = plan.launch_count
+    with ClockSampler(local) as clocks:
+        torch.cuda.synchronize()
+        start.record(stream)
+        plan.enqueue(args.steps)
+        stop.record(stream)
+        stop.synchronize()
+    ms = start.elapsed_time(stop)
+    launches = plan.launch_count - launches0
+    ms = max_over_ranks(ms, world)
+    errors = plan.errors(args.warmup + args.steps)
+    # per-kernel device time over separate timed iterations (events around every launch)
+    plan.set_timing(True)
+    plan.enqueue(max(3, min(args.steps, 10)))
+    stats = plan.kernel_stats()
+    plan.set_timing(False)
+    plan.close()
+
+    bytes_iter, flops_iter = algorithmic(P, n, objects)
+    hbm_peak, _, peak_kind = measured_peaks()
+    pass_ms, pass_launches = stats["position_pass"]
+    pass_avg_s = pass_ms / max(pass_launches, 1) * 1e-3
+    pass_bytes = P * 4 * n  # algorithmic bytes of one position-pass launch: the amplitudes it reads
+    pass_flops = P * (10 * n * math.log2(n) + 40 * n)
+    total_stat_ms = sum(v[0] for v in stats.values())
+    value = P * args.steps / (ms * 1e-3) * world
+
+    e2e = None
+    if not args.no_e2e:
+        t0 = time.perf_counter()
+        r = cb.SingleslicePtychography.reconstruct(ds.amplitudes, ds.positions, ds.object_start, ds.probe,
+                                                   iterations=args.steps, step_size=0.5, precision=args.form,
+                                                   device=local)
+        e2e_s = time.perf_counter() - t0
+        e2e_s = max_over_ranks(e2e_s, world)
+        h2d = ds.amplitudes.nbytes + ds.positions.nbytes + objects * 16 + n * 16
+        d2h = objects * 16 + n * 16 + args.steps * 8
+        e2e = {"value": P * args.steps / e2e_s * world, "unit": UNIT, "seconds": e2e_s,
+               "h2d_bytes_per_step": h2d / args.steps, "d2h_bytes_per_step": d2h / args.steps,
+               "final_error": float(r.errors[-1])}
+
+    cpu = None
+    if rank == 0 and not args.no_cpu:
+        from oracle import c_oracle
+        threads = c_oracle.host_cores()
+        v, sample = cpu_oracle_sample(ds, threads)
+        cpu = {"value": v, "unit": UNIT, "cores": threads, "kind": "port", "sample": sample}
+
+    if rank == 0:
+        line = {
+            "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
+            "warmup": args.warmup, "ms_per_step": ms / args.steps, "higher_is_better": True, "scaling": "weak",
+            "vs_baseline": None, "dtype": "f32" if args.form == "fp32" else "bf16x2/f32", "data": "synthetic",
+            "config": {"workload": f"{SCAN}x{SCAN} scan, step {STEP} px, {DET}x{DET} detector, object "
+                                   f"{ds.object_start.shape[0]}x{ds.object_start.shape[1]}, dose 1e5, GD step 0.5",
+                       "form": args.form, "positions": P, "parallelism": f"replicas x{world}" if world > 1 else "1 GPU",
+                       "l2": "inputs larger than L2 (4.3 GB amplitudes, 8.6 GB residuals)"},
+            "roofline": {"kernel": "position_pass", "bound": "hbm", "achieved": pass_bytes / pass_avg_s / 1e9,
+                         "peak": hbm_peak, "unit": "GB/s", "frac": pass_bytes / pass_avg_s / 1e9 / hbm_peak,
+                         "peak_kind": peak_kind, "traffic": None,
+                         "note": "algorithmic bytes = amplitudes read; the FP32 form is FP32-pipe bound",
+                         "fp32_tflops": pass_flops / pass_avg_s / 1e12,
+                         "iteration_hbm_gbs": bytes_iter / (ms / args.steps * 1e-3) / 1e9,
+                         "iteration_tflops": flops_iter / (ms / args.steps * 1e-3) / 1e12},
+            "kernels": {k: {"ms_per_launch": v[0] / max(v[1], 1), "launches": v[1],
+                            "share": v[0] / total_stat_ms if total_stat_ms else None} for k, v in stats.items() if v[1]},
+            "cpu_baseline": cpu, "e2e": e2e, "gpu_launches": launches, "clocks": clocks.summary(),
+            "errors_first_last": [float(errors[0]), float(errors[-1])],
+        }
+        print(json.dumps(line), flush=True)
+    barrier(world)
+    if world > 1:
+        import torch.distributed as dist
+        dist.destroy_process_group()
+
+
+if __name__ == "__main__":
+    main()

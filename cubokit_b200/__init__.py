@@ -1,0 +1,10 @@
+"""cubokit_b200: CuboPtycho's single-slice gradient-descent ptychography on NVIDIA B200 (sm_100a).
+
+The engine is ``libcuboptycho.so`` (CUDA kernels behind the C ABI of ``include/cubo_ptycho.h``); this package is its
+Python binding and the host-side mirror of CuboPtycho's API.
+"""
+from .ptycho import (CancellationError, Context, DeviceError, Plan, PtychographyError, PtychographyProbe, Result,
+                     SingleslicePtychography, UnsupportedError, context, electron_wavelength)
+
+__all__ = ["CancellationError", "Context", "DeviceError", "Plan", "PtychographyError", "PtychographyProbe", "Result",
+           "SingleslicePtychography", "UnsupportedError", "context", "electron_wavelength"]

@@ -1,0 +1,111 @@
+// Internal interface between the host orchestration (plan.cu) and the kernels (engine_kernels.cu, probe_kernels.cu).
+#pragma once
+
+#include <cuda_runtime.h>
+
+#include "common.cuh"
+#include "fft_smem.cuh"
+
+namespace cubo {
+
+// Per-position data of the scan, on the device.
+struct ScanTables {
+    const int *rr;    // ties-to-even rounded row centre, wrapped into [0, object_rows)
+    const int *cc;    // same for columns
+    const int *cls;   // shift class (index into the shifted-probe table)
+};
+
+template <typename T>
+struct PositionPassArgs {
+    int rows, columns, object_rows, object_columns, n;
+    int first, count;          // positions [first, first + count)
+    ScanTables scan;
+    const C2<T> *shifted;      // [classes][n] shifted probes
+    const C2<T> *object;       // [object_rows * object_columns]
+    const float *amplitudes;   // [positions][n]
+    C2<T> *dpsi;               // [positions][n] the inverse transform of the projection residual
+    double *error;             // [positions] squared amplitude residual
+    const C2<T> *tw_rows, *tw_columns;  // W_rows^t, W_columns^t
+    Radices rad_rows, rad_columns;
+    T inv_n;
+};
+
+template <typename T>
+struct ObjectGatherArgs {
+    int rows, columns, object_rows, object_columns, n;
+    int tiles_x;               // tiles per object row
+    const int *tile_start;     // CSR offsets, [tiles + 1]
+    const int *tile_list;      // position indices, ascending within each tile
+    ScanTables scan;
+    const C2<T> *shifted;
+    const C2<T> *dpsi;
+    C2<T> *grad;               // object gradient sum conj(S) dpsi
+    T *weight;                 // sum |S|^2
+    double *tile_max;          // per-tile max of weight
+};
+
+template <typename T>
+struct ProbeGatherArgs {
+    int rows, columns, object_rows, object_columns, n;
+    int count, groups;         // positions, position groups (one partial sum each)
+    ScanTables scan;
+    const C2<T> *object;
+    const C2<T> *dpsi;
+    C2<T> *partial_grad;       // [groups][n]
+    T *partial_weight;         // [groups][n]
+};
+
+constexpr int kTileW = 32, kTileH = 8;   // object-gather tile (one pixel per thread)
+constexpr int kGatherThreads = kTileW * kTileH;
+
+// engine_kernels.cu
+template <typename T> cudaError_t launch_position_pass(const PositionPassArgs<T> &a, cudaStream_t s);
+template <typename T> cudaError_t launch_object_gather(const ObjectGatherArgs<T> &a, int tiles, cudaStream_t s);
+template <typename T> cudaError_t launch_probe_gather(const ProbeGatherArgs<T> &a, cudaStream_t s);
+template <typename T>
+cudaError_t launch_probe_reduce(const C2<T> *partial_grad, const T *partial_weight, int groups, int n,
+                                double2 *grad, double *weight, double *block_max, cudaStream_t s);
+cudaError_t launch_max_reduce(const double *values, int count, double *out, cudaStream_t s);
+template <typename T>
+cudaError_t launch_object_update(C2<T> *object, const C2<T> *grad, const T *weight, int count, const double *max_weight,
+                                 double step, double minimum, int cap, int pure_phase, cudaStream_t s);
+cudaError_t launch_error_reduce(const double *error, int count, double divisor, double *errors, int *iteration,
+                                cudaStream_t s);
+bool position_pass_supported(int n, bool fp64);
+size_t position_pass_smem(int n, int rows, int columns, bool fp64);
+
+// probe_kernels.cu — FP64, probe-sized work
+struct Fft2Plan64 {
+    int rows, columns;
+    Radices rad_rows, rad_columns;
+    const double2 *tw_rows, *tw_columns;
+};
+cudaError_t launch_fft2_f64(const Fft2Plan64 &p, double2 *data, int batch, bool inverse, cudaStream_t s);
+cudaError_t launch_scale_f64(double2 *data, int count, double scale, cudaStream_t s);
+cudaError_t launch_probe_update(double2 *probe, const double2 *grad, const double *weight, int n, const double *max_weight,
+                                double step, double minimum, cudaStream_t s);
+// sums[0] = sum |p|^2, sums[1] = sum fr*R*w, sums[2] = sum fc*C*w (fixed order, one CTA)
+cudaError_t launch_probe_moments(const double2 *probe, int rows, int columns, double *sums, cudaStream_t s);
+cudaError_t launch_energy(const double2 *data, int n, double *sum, cudaStream_t s);
+cudaError_t launch_com_ramp(double2 *spectrum, int rows, int columns, const double *sums, cudaStream_t s);
+cudaError_t launch_commit_if_valid(double2 *probe, const double2 *candidate, int n, const double *sums,
+                                   cudaStream_t s);
+cudaError_t launch_aperture_phase(double2 *spectrum, const double *aperture, int n, cudaStream_t s);
+cudaError_t launch_amplitude_mask(double2 *probe, int rows, int columns, double radius, double width,
+                                  cudaStream_t s);
+// dst = src * sqrt(before / after) when both are positive, else dst = src
+cudaError_t launch_renormalise(double2 *dst, const double2 *src, int n, const double *before, const double *after,
+                               cudaStream_t s);
+cudaError_t launch_support_mask(double2 *probe, const unsigned char *mask, int n, cudaStream_t s);
+cudaError_t launch_magnitude(const double2 *data, double *out, int n, cudaStream_t s);
+cudaError_t launch_shift_ramps(const double2 *spectrum, const double2 *ramps_rows, const double2 *ramps_columns,
+                               int rows, int columns, int classes, double2 *out, cudaStream_t s);
+template <typename T>
+cudaError_t launch_convert(const double2 *in, C2<T> *out, long long count, cudaStream_t s);
+cudaError_t configure_kernels();
+cudaError_t launch_probe_spectrum(double2 *out, int rows, int columns, double row_sampling, double column_sampling,
+                                  double wavelength, double cutoff, double rolloff, double defocus, double astigmatism,
+                                  double astigmatism_angle, double spherical, int term_count, const double *terms,
+                                  cudaStream_t s);
+
+}  // namespace cubo

@@ -1,0 +1,355 @@
+// Generic per-iteration kernels of the single-slice gradient descent, for any detector size (FP32 and FP64 forms).
+//
+// One iteration of SingleslicePtychography.reconstruct (Sources/CuboPtycho/Ptychography.swift:280-402) becomes:
+//   position pass   one CTA per scan position: exit wave S * O[patch] (:321-336), forward FFT (:337), Fourier-modulus
+//                   projection and squared residual (:338-349), inverse FFT with its 1/n folded into the projection
+//                   (:350); writes dpsi and the position's residual.
+//   object gather   one thread per object pixel: the sum over the positions whose window covers the pixel, in ascending
+//                   position order, of conj(S) dpsi and |S|^2 (the scatter-add of :351-355 turned into a gather, so
+//                   no atomics and a fixed summation order: bitwise reproducible).
+//   probe gather    per detector pixel and position group: sum of conj(O[patch]) dpsi and |O|^2 (:356-357); the groups
+//                   are summed in a fixed order by probe reduce (FP64).
+//   max / update    the global maxima (:362) and the normalised object update with the amplitude cap (:363-382).
+//   error reduce    FP64 fixed-order sum of the per-position residuals divided by the normalisation (:400).
+#include <cfloat>
+
+#include "engine.h"
+
+namespace cubo {
+
+namespace {
+
+constexpr int kPassThreads = 512;
+constexpr int kMaxNFloat = 16384;   // 128 x 128 complex64 = 128 KB of shared memory
+constexpr int kMaxNDouble = 12288;  // 12288 complex128 = 192 KB
+
+template <typename T> struct PassConfig;
+template <> struct PassConfig<float> { static constexpr int maxn = kMaxNFloat; };
+template <> struct PassConfig<double> { static constexpr int maxn = kMaxNDouble; };
+
+__device__ __forceinline__ double warp_sum(double v) {
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) v += __shfl_down_sync(0xffffffffu, v, o);
+    return v;
+}
+__device__ __forceinline__ double warp_max(double v) {
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) v = fmax(v, __shfl_down_sync(0xffffffffu, v, o));
+    return v;
+}
+
+// Fixed-order CTA sum: warps reduce by shuffles, then thread 0 adds the warp sums in warp order.
+template <int NT>
+__device__ double block_sum(double v, double *scratch) {
+    v = warp_sum(v);
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    if (lane == 0) scratch[warp] = v;
+    __syncthreads();
+    double total = 0;
+    if (threadIdx.x == 0)
+        for (int w = 0; w < NT / 32; w++) total += scratch[w];
+    __syncthreads();
+    return total;  // valid in thread 0
+}
+
+template <int NT>
+__device__ double block_max(double v, double *scratch) {
+    v = warp_max(v);
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    if (lane == 0) scratch[warp] = v;
+    __syncthreads();
+    double m = -DBL_MAX;
+    if (threadIdx.x == 0)
+        for (int w = 0; w < NT / 32; w++) m = fmax(m, scratch[w]);
+    __syncthreads();
+    return m;
+}
+
+__device__ __forceinline__ int wrap_once(int v, int size) { return v < 0 ? v + size : (v >= size ? v - size : v); }
+
+// ------------------------------------------------------------------------------------------------ position pass
+
+template <typename T, int NT, int MAXN>
+__global__ void __launch_bounds__(NT, 1) position_pass_kernel(PositionPassArgs<T> a) {
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    C2<T> *D = reinterpret_cast<C2<T> *>(smem_raw);
+    C2<T> *twr = D + a.n;
+    C2<T> *twc = twr + a.rows;
+    double *scratch = reinterpret_cast<double *>(twc + a.columns);
+    const int tid = threadIdx.x;
+    const int p = a.first + blockIdx.x;
+    for (int i = tid; i < a.rows; i += NT) twr[i] = a.tw_rows[i];
+    for (int i = tid; i < a.columns; i += NT) twc[i] = a.tw_columns[i];
+    const int rr = a.scan.rr[p], cc = a.scan.cc[p], cls = a.scan.cls[p];
+    const C2<T> *S = a.shifted + (size_t)cls * a.n;
+    // exit wave psi = S * O[patch] (Ptychography.swift:321-336)
+    for (int k = tid; k < a.n; k += NT) {
+        const int kr = k / a.columns, kc = k - kr * a.columns;
+        const int y = wrap_once(rr + corner_offset(kr, a.rows), a.object_rows);
+        const int x = wrap_once(cc + corner_offset(kc, a.columns), a.object_columns);
+        D[k] = cmul(S[k], a.object[(size_t)y * a.object_columns + x]);
+    }
+    __syncthreads();
+    fft2_smem<T, NT, MAXN>(D, a.rows, a.columns, a.rad_rows, a.rad_columns, twr, twc, false);
+    // Fourier-modulus projection (Ptychography.swift:338-349), the inverse's 1/n folded in
+    const float *A = a.amplitudes + (size_t)p * a.n;
+    double err = 0;
+    for (int k = tid; k < a.n; k += NT) {
+        const C2<T> f = D[k];
+        const T mag = sqrt(f.x * f.x + f.y * f.y);
+        const T measured = (T)A[k];
+        const T miss = measured - mag;
+        err += (double)(miss * miss);
+        if (mag > (T)0) {
+            const T s = (measured / mag - (T)1) * a.inv_n;
+            D[k] = mk<T>(f.x * s, f.y * s);
+        } else {
+            D[k] = mk<T>(measured * a.inv_n, (T)0);
+        }
+    }
+    const double total = block_sum<NT>(err, scratch);
+    if (tid == 0) a.error[p] = total;
+    __syncthreads();
+    fft2_smem<T, NT, MAXN>(D, a.rows, a.columns, a.rad_rows, a.rad_columns, twr, twc, true);
+    C2<T> *out = a.dpsi + (size_t)p * a.n;
+    for (int k = tid; k < a.n; k += NT) out[k] = D[k];
+}
+
+// ------------------------------------------------------------------------------------------------ object gather
+
+constexpr int kChunk = 256;
+
+template <typename T>
+__global__ void __launch_bounds__(kGatherThreads) object_gather_kernel(ObjectGatherArgs<T> a) {
+    __shared__ int s_p[kChunk], s_rr[kChunk], s_cc[kChunk], s_cls[kChunk];
+    __shared__ double scratch[32];
+    const int tile = blockIdx.x;
+    const int tx = tile % a.tiles_x, ty = tile / a.tiles_x;
+    const int x = tx * kTileW + (threadIdx.x % kTileW), y = ty * kTileH + threadIdx.x / kTileW;
+    const bool inside = x < a.object_columns && y < a.object_rows;
+    C2<T> g = mk<T>(0, 0);
+    T w = 0;
+    const int begin = a.tile_start[tile], end = a.tile_start[tile + 1];
+    for (int base = begin; base < end; base += kChunk) {
+        const int cnt = min(kChunk, end - base);
+        __syncthreads();
+        for (int i = threadIdx.x; i < cnt; i += kGatherThreads) {
+            const int p = a.tile_list[base + i];
+            s_p[i] = p; s_rr[i] = a.scan.rr[p]; s_cc[i] = a.scan.cc[p]; s_cls[i] = a.scan.cls[p];
+        }
+        __syncthreads();
+        if (inside) {
+            for (int i = 0; i < cnt; i++) {
+                int dy = y - s_rr[i];
+                if (dy < 0) dy += a.object_rows;
+                const int kr = window_index(dy, a.rows, a.object_rows);
+                if (kr < 0) continue;
+                int dx = x - s_cc[i];
+                if (dx < 0) dx += a.object_columns;
+                const int kc = window_index(dx, a.columns, a.object_columns);
+                if (kc < 0) continue;
+                const int k = kr * a.columns + kc;
+                const C2<T> d = a.dpsi[(size_t)s_p[i] * a.n + k];
+                const C2<T> s = a.shifted[(size_t)s_cls[i] * a.n + k];
+                g = cadd(g, cmulc(s, d));
+                w += s.x * s.x + s.y * s.y;
+            }
+        }
+    }
+    if (inside) {
+        const size_t j = (size_t)y * a.object_columns + x;
+        a.grad[j] = g;
+        a.weight[j] = w;
+    }
+    const double m = block_max<kGatherThreads>(inside ? (double)w : -DBL_MAX, scratch);
+    if (threadIdx.x == 0) a.tile_max[tile] = m;
+}
+
+// ------------------------------------------------------------------------------------------------ probe gather
+
+constexpr int kProbeThreads = 256;
+
+template <typename T>
+__global__ void __launch_bounds__(kProbeThreads) probe_gather_kernel(ProbeGatherArgs<T> a) {
+    __shared__ int s_rr[kChunk], s_cc[kChunk];
+    const int k = blockIdx.x * kProbeThreads + threadIdx.x;
+    const int group = blockIdx.y;
+    const int p0 = (int)((long long)a.count * group / a.groups), p1 = (int)((long long)a.count * (group + 1) / a.groups);
+    const bool valid = k < a.n;
+    const int kr = valid ? k / a.columns : 0, kc = valid ? k - kr * a.columns : 0;
+    const int offr = corner_offset(kr, a.rows), offc = corner_offset(kc, a.columns);
+    C2<T> g = mk<T>(0, 0);
+    T w = 0;
+    for (int base = p0; base < p1; base += kChunk) {
+        const int cnt = min(kChunk, p1 - base);
+        __syncthreads();
+        for (int i = threadIdx.x; i < cnt; i += kProbeThreads) { s_rr[i] = a.scan.rr[base + i]; s_cc[i] = a.scan.cc[base + i]; }
+        __syncthreads();
+        if (valid) {
+            for (int i = 0; i < cnt; i++) {
+                const int y = wrap_once(s_rr[i] + offr, a.object_rows);
+                const int x = wrap_once(s_cc[i] + offc, a.object_columns);
+                const C2<T> o = a.object[(size_t)y * a.object_columns + x];
+                const C2<T> d = a.dpsi[(size_t)(base + i) * a.n + k];
+                g = cadd(g, cmulc(o, d));
+                w += o.x * o.x + o.y * o.y;
+            }
+        }
+    }
+    if (valid) {
+        a.partial_grad[(size_t)group * a.n + k] = g;
+        a.partial_weight[(size_t)group * a.n + k] = w;
+    }
+}
+
+template <typename T>
+__global__ void __launch_bounds__(256) probe_reduce_kernel(const C2<T> *pg, const T *pw, int groups, int n,
+                                                           double2 *grad, double *weight, double *block_max_out) {
+    __shared__ double scratch[32];
+    const int k = blockIdx.x * 256 + threadIdx.x;
+    double gx = 0, gy = 0, w = 0;
+    if (k < n) {
+        for (int g = 0; g < groups; g++) {
+            const C2<T> v = pg[(size_t)g * n + k];
+            gx += (double)v.x; gy += (double)v.y; w += (double)pw[(size_t)g * n + k];
+        }
+        grad[k] = make_double2(gx, gy);
+        weight[k] = w;
+    }
+    const double m = block_max<256>(k < n ? w : -DBL_MAX, scratch);
+    if (threadIdx.x == 0) block_max_out[blockIdx.x] = m;
+}
+
+__global__ void __launch_bounds__(1024) max_reduce_kernel(const double *v, int count, double *out) {
+    __shared__ double scratch[32];
+    double m = -DBL_MAX;
+    for (int i = threadIdx.x; i < count; i += 1024) m = fmax(m, v[i]);
+    m = block_max<1024>(m, scratch);
+    if (threadIdx.x == 0) *out = m;
+}
+
+// Ptychography.swift:362-370,378-382: O += step / sqrt(1e-16 + ((1 - m) w)^2 + (m max w)^2) * grad, then the cap.
+template <typename T>
+__global__ void __launch_bounds__(256) object_update_kernel(C2<T> *object, const C2<T> *grad, const T *weight,
+                                                            int count, const double *max_weight, double step,
+                                                            double minimum, int cap, int pure_phase) {
+    const int j = blockIdx.x * 256 + threadIdx.x;
+    if (j >= count) return;
+    const double l = (1 - minimum) * (double)weight[j], x = minimum * *max_weight;
+    const T s = (T)(step * (1 / sqrt(1e-16 + l * l + x * x)));
+    C2<T> o = object[j];
+    const C2<T> g = grad[j];
+    o.x += s * g.x; o.y += s * g.y;
+    if (cap || pure_phase) {
+        const T amp = sqrt(o.x * o.x + o.y * o.y);
+        const T target = pure_phase ? (T)1 : (amp < (T)1 ? amp : (T)1);
+        if (amp > (T)0) { const T r = target / amp; o.x *= r; o.y *= r; }
+        else { o.x = target; o.y = 0; }
+    }
+    object[j] = o;
+}
+
+__global__ void __launch_bounds__(1024) error_reduce_kernel(const double *error, int count, double divisor,
+                                                            double *errors, int *iteration) {
+    __shared__ double scratch[32];
+    // thread t sums the contiguous slice [t*count/1024, (t+1)*count/1024) in order, then a fixed tree
+    const long long b = (long long)count * threadIdx.x / 1024, e = (long long)count * (threadIdx.x + 1) / 1024;
+    double s = 0;
+    for (long long i = b; i < e; i++) s += error[i];
+    s = block_sum<1024>(s, scratch);
+    if (threadIdx.x == 0) {
+        const int it = *iteration;
+        errors[it] = s / divisor;
+        *iteration = it + 1;
+    }
+}
+
+template <typename T>
+size_t pass_smem(int n, int rows, int columns) {
+    return (size_t)(n + rows + columns) * sizeof(C2<T>) + 32 * sizeof(double);
+}
+
+}  // namespace
+
+bool position_pass_supported(int n, bool fp64) {
+    return fp64 ? n <= kMaxNDouble : n <= kMaxNFloat;
+}
+
+// Raises the dynamic shared-memory limit of the position-pass kernels to the device's opt-in maximum.  Per device: the
+// plan calls it with its device current.
+cudaError_t configure_kernels() {
+    int device = 0, optin = 0;
+    cudaError_t e = cudaGetDevice(&device);
+    if (e != cudaSuccess) return e;
+    e = cudaDeviceGetAttribute(&optin, cudaDevAttrMaxSharedMemoryPerBlockOptin, device);
+    if (e != cudaSuccess) return e;
+    e = cudaFuncSetAttribute(position_pass_kernel<float, kPassThreads, kMaxNFloat>,
+                             cudaFuncAttributeMaxDynamicSharedMemorySize, optin);
+    if (e != cudaSuccess) return e;
+    return cudaFuncSetAttribute(position_pass_kernel<double, kPassThreads, kMaxNDouble>,
+                                cudaFuncAttributeMaxDynamicSharedMemorySize, optin);
+}
+
+size_t position_pass_smem(int n, int rows, int columns, bool fp64) {
+    return fp64 ? pass_smem<double>(n, rows, columns) : pass_smem<float>(n, rows, columns);
+}
+
+template <typename T>
+cudaError_t launch_position_pass(const PositionPassArgs<T> &a, cudaStream_t s) {
+    constexpr int maxn = PassConfig<T>::maxn;
+    if (a.count <= 0) return cudaSuccess;
+    position_pass_kernel<T, kPassThreads, maxn><<<a.count, kPassThreads, pass_smem<T>(a.n, a.rows, a.columns), s>>>(a);
+    return cudaGetLastError();
+}
+
+template <typename T>
+cudaError_t launch_object_gather(const ObjectGatherArgs<T> &a, int tiles, cudaStream_t s) {
+    object_gather_kernel<T><<<tiles, kGatherThreads, 0, s>>>(a);
+    return cudaGetLastError();
+}
+
+template <typename T>
+cudaError_t launch_probe_gather(const ProbeGatherArgs<T> &a, cudaStream_t s) {
+    dim3 grid((a.n + kProbeThreads - 1) / kProbeThreads, a.groups);
+    probe_gather_kernel<T><<<grid, kProbeThreads, 0, s>>>(a);
+    return cudaGetLastError();
+}
+
+template <typename T>
+cudaError_t launch_probe_reduce(const C2<T> *pg, const T *pw, int groups, int n, double2 *grad, double *weight,
+                                double *block_max_out, cudaStream_t s) {
+    probe_reduce_kernel<T><<<(n + 255) / 256, 256, 0, s>>>(pg, pw, groups, n, grad, weight, block_max_out);
+    return cudaGetLastError();
+}
+
+cudaError_t launch_max_reduce(const double *values, int count, double *out, cudaStream_t s) {
+    max_reduce_kernel<<<1, 1024, 0, s>>>(values, count, out);
+    return cudaGetLastError();
+}
+
+template <typename T>
+cudaError_t launch_object_update(C2<T> *object, const C2<T> *grad, const T *weight, int count, const double *max_weight,
+                                 double step, double minimum, int cap, int pure_phase, cudaStream_t s) {
+    object_update_kernel<T><<<(count + 255) / 256, 256, 0, s>>>(object, grad, weight, count, max_weight, step, minimum,
+                                                                 cap, pure_phase);
+    return cudaGetLastError();
+}
+
+cudaError_t launch_error_reduce(const double *error, int count, double divisor, double *errors, int *iteration,
+                                cudaStream_t s) {
+    error_reduce_kernel<<<1, 1024, 0, s>>>(error, count, divisor, errors, iteration);
+    return cudaGetLastError();
+}
+
+#define INSTANTIATE(T)                                                                                                 \
+    template cudaError_t launch_position_pass<T>(const PositionPassArgs<T> &, cudaStream_t);                           \
+    template cudaError_t launch_object_gather<T>(const ObjectGatherArgs<T> &, int, cudaStream_t);                      \
+    template cudaError_t launch_probe_gather<T>(const ProbeGatherArgs<T> &, cudaStream_t);                             \
+    template cudaError_t launch_probe_reduce<T>(const C2<T> *, const T *, int, int, double2 *, double *, double *,     \
+                                                cudaStream_t);                                                         \
+    template cudaError_t launch_object_update<T>(C2<T> *, const C2<T> *, const T *, int, const double *, double,       \
+                                                 double, int, int, cudaStream_t);
+INSTANTIATE(float)
+INSTANTIATE(double)
+
+}  // namespace cubo

@@ -1,0 +1,826 @@
+// Host side of the engine: the C ABI of include/cubo_ptycho.h, input validation, the scan tables, device buffers and
+// the per-iteration launch sequence.  Runs on the caller's thread; all device work goes to the context's stream.
+#include <algorithm>
+#include <cmath>
+#include <functional>
+#include <cstdint>
+#include <cstdio>
+#include <cstring>
+#include <map>
+#include <memory>
+#include <new>
+#include <string>
+#include <vector>
+
+#include "../../include/cubo_ptycho.h"
+#include "engine.h"
+
+using namespace cubo;
+
+struct cubo_ptycho_context {
+    int device = 0;
+    cudaStream_t stream = nullptr;
+    std::string last_error;
+};
+
+namespace {
+
+constexpr double kPi = 3.14159265358979323846;
+
+// --------------------------------------------------------------------------------------------- device buffers
+
+struct DeviceBuffer {
+    void *ptr = nullptr;
+    size_t bytes = 0;
+    DeviceBuffer() = default;
+    DeviceBuffer(const DeviceBuffer &) = delete;
+    DeviceBuffer &operator=(const DeviceBuffer &) = delete;
+    ~DeviceBuffer() { release(); }
+    void release() {
+        if (ptr) cudaFree(ptr);
+        ptr = nullptr;
+        bytes = 0;
+    }
+    cudaError_t alloc(size_t b) {
+        release();
+        if (b == 0) b = 16;
+        cudaError_t e = cudaMalloc(&ptr, b);
+        if (e == cudaSuccess) bytes = b;
+        else ptr = nullptr;
+        return e;
+    }
+    template <typename X> X *as() const { return static_cast<X *>(ptr); }
+};
+
+struct Failure {
+    int status;
+    std::string message;
+};
+
+[[noreturn]] void fail(int status, const std::string &message) { throw Failure{status, message}; }
+
+void check(cudaError_t e, const char *what) {
+    if (e == cudaSuccess) return;
+    cudaGetLastError();  // clear a sticky launch error flag where possible
+    const int status = (e == cudaErrorMemoryAllocation) ? CUBO_PTYCHO_OUT_OF_MEMORY : CUBO_PTYCHO_CUDA_ERROR;
+    fail(status, std::string(what) + ": " + cudaGetErrorString(e));
+}
+
+std::vector<double2> twiddles(int L) {
+    std::vector<double2> t(L);
+    for (int k = 0; k < L; k++) {
+        const double a = -2.0 * kPi * (double)k / (double)L;
+        t[k] = make_double2(std::cos(a), std::sin(a));
+    }
+    return t;
+}
+
+template <typename X>
+void upload(DeviceBuffer &b, const std::vector<X> &v, cudaStream_t s) {
+    check(b.alloc(v.size() * sizeof(X)), "cudaMalloc");
+    if (!v.empty()) check(cudaMemcpyAsync(b.ptr, v.data(), v.size() * sizeof(X), cudaMemcpyHostToDevice, s), "upload");
+}
+
+bool finite_positive(double v) { return std::isfinite(v) && v > 0; }
+
+}  // namespace
+
+// ------------------------------------------------------------------------------------------------ the plan
+
+struct cubo_ptycho_plan {
+    cubo_ptycho_context *ctx = nullptr;
+    int R = 0, C = 0, OR = 0, OC = 0, P = 0, n = 0;
+    long long objects = 0;
+    cubo_ptycho_params params{};
+    std::vector<unsigned char> mask;
+    double divisor = 0;
+    bool fp64 = false;
+    int classes = 1;        // shift classes; class 0 is the zero shift
+    int groups = 1;         // probe-gather position groups
+    int tiles_x = 0, tiles = 0;
+    int probe_blocks = 0;
+    long long iterations_done = 0;
+    long long errors_capacity = 0;
+    long long launches = 0;
+    Radices rad_rows{}, rad_columns{};
+
+    // timing
+    bool timing = false;
+    struct Timed { int kind; cudaEvent_t a, b; };
+    std::vector<Timed> pending;
+    std::vector<cudaEvent_t> event_pool;
+    std::vector<double> kind_ms;
+    std::vector<long long> kind_launches;
+
+    // device memory
+    DeviceBuffer amplitudes, rr, cc, cls, tile_start, tile_list;
+    DeviceBuffer object, grad_o, weight_o, tile_max;
+    DeviceBuffer dpsi, error, errors, iteration;
+    DeviceBuffer probe64, scratch64, spectrum64, shifted, shift_tmp64, ramps_r64, ramps_c64;
+    DeviceBuffer partial_grad, partial_weight, grad_p64, weight_p64, probe_block_max;
+    DeviceBuffer maxes, sums, aperture64, mask_dev;
+    DeviceBuffer tw_r, tw_c, tw_r64, tw_c64;
+
+    ~cubo_ptycho_plan() {
+        for (auto &t : pending) { event_pool.push_back(t.a); event_pool.push_back(t.b); }
+        for (auto e : event_pool) cudaEventDestroy(e);
+    }
+};
+
+namespace {
+
+enum Kind { kPositionPass, kObjectGather, kProbeGather, kProbeReduce, kMaxReduce, kObjectUpdate, kProbeSide,
+            kErrorReduce, kShiftTable, kKinds };
+const char *kKindNames[kKinds] = {"position_pass", "object_gather", "probe_gather", "probe_reduce", "max_reduce",
+                                  "object_update", "probe_update_constraints", "error_reduce", "shift_table"};
+
+cudaEvent_t take_event(cubo_ptycho_plan *p) {
+    if (!p->event_pool.empty()) {
+        cudaEvent_t e = p->event_pool.back();
+        p->event_pool.pop_back();
+        return e;
+    }
+    cudaEvent_t e;
+    check(cudaEventCreate(&e), "cudaEventCreate");
+    return e;
+}
+
+// Runs `launch` (which enqueues `count` kernels) and accounts for it.
+template <typename F>
+void timed(cubo_ptycho_plan *p, Kind kind, int count, F &&launch) {
+    cudaStream_t s = p->ctx->stream;
+    cudaEvent_t a = nullptr, b = nullptr;
+    if (p->timing) {
+        a = take_event(p);
+        b = take_event(p);
+        check(cudaEventRecord(a, s), "cudaEventRecord");
+    }
+    check(launch(), kKindNames[kind]);
+    p->launches += count;
+    if (p->timing) {
+        check(cudaEventRecord(b, s), "cudaEventRecord");
+        p->pending.push_back({kind, a, b});
+        p->kind_launches[kind] += count;
+    }
+}
+
+void collect_timing(cubo_ptycho_plan *p) {
+    if (p->pending.empty()) return;
+    check(cudaStreamSynchronize(p->ctx->stream), "cudaStreamSynchronize");
+    for (auto &t : p->pending) {
+        float ms = 0;
+        check(cudaEventElapsedTime(&ms, t.a, t.b), "cudaEventElapsedTime");
+        p->kind_ms[t.kind] += ms;
+        p->event_pool.push_back(t.a);
+        p->event_pool.push_back(t.b);
+    }
+    p->pending.clear();
+}
+
+// Ptychography.swift:247-259 (+ :236 for position correction, refused as .single refuses it).
+void validate(const cubo_ptycho_problem *pr, const cubo_ptycho_params *pp, double *divisor_out) {
+    if (!pr || !pp) fail(CUBO_PTYCHO_INVALID_INPUT, "null problem or params");
+    if (pp->has_position_correction) fail(CUBO_PTYCHO_INVALID_INPUT, "position correction is not available on the GPU path");
+    if (!(pr->rows > 1 && pr->columns > 1 && pr->object_rows > 1 && pr->object_columns > 1))
+        fail(CUBO_PTYCHO_INVALID_INPUT, "array dimensions must exceed 1");
+    const long long n = (long long)pr->rows * pr->columns;
+    if (!(pr->count > 0)) fail(CUBO_PTYCHO_INVALID_INPUT, "no positions");
+    if ((long long)pr->count * n > (1LL << 40)) fail(CUBO_PTYCHO_INVALID_INPUT, "too many samples");
+    if (!pr->amplitudes || !pr->position_rows || !pr->position_columns) fail(CUBO_PTYCHO_INVALID_INPUT, "null input");
+    if (!(pp->iterations >= 0 && finite_positive(pp->step_size))) fail(CUBO_PTYCHO_INVALID_INPUT, "iterations or step");
+    if (!(std::isfinite(pp->normalization_minimum) && pp->normalization_minimum >= 0 && pp->normalization_minimum <= 1))
+        fail(CUBO_PTYCHO_INVALID_INPUT, "normalization minimum");
+    const double limit = (double)(INT64_MAX / 4);
+    for (int i = 0; i < pr->count; i++) {
+        const double r = pr->position_rows[i], c = pr->position_columns[i];
+        if (!(std::isfinite(r) && std::isfinite(c) && std::fabs(r) < limit && std::fabs(c) < limit))
+            fail(CUBO_PTYCHO_INVALID_INPUT, "position");
+    }
+    const double rad = pp->probe_amplitude_relative_radius, wid = pp->probe_amplitude_relative_width;
+    if (!(std::isfinite(rad) && rad >= 0 && rad <= 0.5 && std::isfinite(wid) && wid > 0 && wid <= 0.5))
+        fail(CUBO_PTYCHO_INVALID_INPUT, "probe amplitude constraint parameters");
+    if (!(pr->object_rows >= pr->rows && pr->object_columns >= pr->columns))
+        fail(CUBO_PTYCHO_INVALID_INPUT, "object smaller than probe");
+    double energy = 0;
+    const long long total = (long long)pr->count * n;
+    for (long long i = 0; i < total; i++) {
+        const double a = (double)pr->amplitudes[i];
+        if (!(std::isfinite(a) && a >= 0)) fail(CUBO_PTYCHO_INVALID_INPUT, "amplitude not finite and non-negative");
+        energy += a * a;
+    }
+    const double d = pp->error_normalization == CUBO_PTYCHO_ERRORS_MEAN_INTENSITY ? pp->mean_intensity * (double)pr->count
+                                                                                  : energy;
+    if (!finite_positive(d)) fail(CUBO_PTYCHO_INVALID_INPUT, "error normalisation divisor");
+    if (pp->form < CUBO_PTYCHO_FORM_FP32 || pp->form > CUBO_PTYCHO_FORM_FP64) fail(CUBO_PTYCHO_INVALID_INPUT, "form");
+    *divisor_out = d;
+}
+
+long long wrap_ll(long long v, long long m) {
+    long long r = v % m;
+    return r < 0 ? r + m : r;
+}
+
+template <typename T>
+void build_plan(cubo_ptycho_plan *p, const cubo_ptycho_problem *pr) {
+    cudaStream_t s = p->ctx->stream;
+    const int R = p->R, C = p->C, n = p->n, P = p->P;
+    // ---- scan tables: ties-to-even centres (Ptychography.swift:301), wrapped; shift classes by exact fraction
+    std::vector<int> rr(P), cc(P), cls(P);
+    std::map<std::pair<uint64_t, uint64_t>, int> class_of;
+    std::vector<std::pair<double, double>> fractions;  // classes 1..
+    for (int i = 0; i < P; i++) {
+        const double r = pr->position_rows[i], c = pr->position_columns[i];
+        const double rn = std::nearbyint(r), cn = std::nearbyint(c);
+        const double dr = r - rn, dc = c - cn;
+        rr[i] = (int)wrap_ll((long long)rn, p->OR);
+        cc[i] = (int)wrap_ll((long long)cn, p->OC);
+        if (dr == 0 && dc == 0) { cls[i] = 0; continue; }
+        uint64_t kr, kc;
+        std::memcpy(&kr, &dr, 8);
+        std::memcpy(&kc, &dc, 8);
+        auto key = std::make_pair(kr, kc);
+        auto it = class_of.find(key);
+        if (it == class_of.end()) {
+            fractions.push_back({dr, dc});
+            it = class_of.emplace(key, (int)fractions.size()).first;
+        }
+        cls[i] = it->second;
+    }
+    p->classes = 1 + (int)fractions.size();
+    upload(p->rr, rr, s);
+    upload(p->cc, cc, s);
+    upload(p->cls, cls, s);
+    // ---- object-gather candidate lists: for each tile, the positions whose window touches it, ascending
+    p->tiles_x = (p->OC + kTileW - 1) / kTileW;
+    const int tiles_y = (p->OR + kTileH - 1) / kTileH;
+    p->tiles = p->tiles_x * tiles_y;
+    std::vector<int> counts(p->tiles + 1, 0);
+    std::vector<int> mark_y(tiles_y, -1), mark_x(p->tiles_x, -1);
+    std::vector<int> ty_list, tx_list;
+    auto tiles_of = [&](int i) {
+        ty_list.clear();
+        tx_list.clear();
+        for (int k = 0; k < R; k++) {
+            const int y = (int)wrap_ll((long long)rr[i] + corner_offset(k, R), p->OR);
+            const int t = y / kTileH;
+            if (mark_y[t] != i) { mark_y[t] = i; ty_list.push_back(t); }
+        }
+        for (int k = 0; k < C; k++) {
+            const int x = (int)wrap_ll((long long)cc[i] + corner_offset(k, C), p->OC);
+            const int t = x / kTileW;
+            if (mark_x[t] != i) { mark_x[t] = i; tx_list.push_back(t); }
+        }
+    };
+    for (int i = 0; i < P; i++) {
+        tiles_of(i);
+        for (int ty : ty_list)
+            for (int tx : tx_list) counts[ty * p->tiles_x + tx + 1]++;
+    }
+    for (int t = 0; t < p->tiles; t++) counts[t + 1] += counts[t];
+    std::vector<int> list((size_t)counts[p->tiles]);
+    std::vector<int> fill(counts.begin(), counts.end() - 1);
+    std::fill(mark_y.begin(), mark_y.end(), -1);
+    std::fill(mark_x.begin(), mark_x.end(), -1);
+    for (int i = 0; i < P; i++) {
+        tiles_of(i);
+        for (int ty : ty_list)
+            for (int tx : tx_list) list[fill[ty * p->tiles_x + tx]++] = i;
+    }
+    upload(p->tile_start, counts, s);
+    upload(p->tile_list, list, s);
+    // ---- amplitudes (Float32, [position][row][column])
+    check(p->amplitudes.alloc((size_t)P * n * sizeof(float)), "cudaMalloc amplitudes");
+    check(cudaMemcpyAsync(p->amplitudes.ptr, pr->amplitudes, (size_t)P * n * sizeof(float), cudaMemcpyHostToDevice, s),
+          "upload amplitudes");
+    // ---- state and work buffers
+    check(p->object.alloc((size_t)p->objects * sizeof(C2<T>)), "cudaMalloc object");
+    check(p->grad_o.alloc((size_t)p->objects * sizeof(C2<T>)), "cudaMalloc");
+    check(p->weight_o.alloc((size_t)p->objects * sizeof(T)), "cudaMalloc");
+    check(p->tile_max.alloc((size_t)p->tiles * sizeof(double)), "cudaMalloc");
+    check(p->dpsi.alloc((size_t)P * n * sizeof(C2<T>)), "cudaMalloc dpsi");
+    check(p->error.alloc((size_t)P * sizeof(double)), "cudaMalloc");
+    check(p->iteration.alloc(sizeof(int)), "cudaMalloc");
+    check(cudaMemsetAsync(p->iteration.ptr, 0, sizeof(int), s), "memset");
+    check(p->probe64.alloc((size_t)n * sizeof(double2)), "cudaMalloc");
+    check(p->scratch64.alloc((size_t)n * sizeof(double2)), "cudaMalloc");
+    check(p->spectrum64.alloc((size_t)n * sizeof(double2)), "cudaMalloc");
+    check(p->shifted.alloc((size_t)p->classes * n * sizeof(C2<T>)), "cudaMalloc");
+    const int frac = p->classes - 1;
+    if (frac > 0) {
+        check(p->shift_tmp64.alloc((size_t)frac * n * sizeof(double2)), "cudaMalloc shift table");
+        std::vector<double2> rrmp((size_t)frac * R), crmp((size_t)frac * C);
+        for (int f = 0; f < frac; f++) {  // Ptychography.swift:304-311
+            for (int r = 0; r < R; r++) {
+                const double a = -2 * kPi * frequency(r, R) * fractions[f].first;
+                rrmp[(size_t)f * R + r] = make_double2(std::cos(a), std::sin(a));
+            }
+            for (int c = 0; c < C; c++) {
+                const double a = -2 * kPi * frequency(c, C) * fractions[f].second;
+                crmp[(size_t)f * C + c] = make_double2(std::cos(a), std::sin(a));
+            }
+        }
+        upload(p->ramps_r64, rrmp, s);
+        upload(p->ramps_c64, crmp, s);
+    }
+    // probe-gather groups: about eight CTAs per SM of a 148-SM part; a function of the problem only, so the summation
+    // order (and the result) does not depend on the device
+    const int kblocks = (n + 255) / 256;
+    p->groups = std::max(1, std::min(P, (148 * 8 + kblocks - 1) / kblocks));
+    check(p->partial_grad.alloc((size_t)p->groups * n * sizeof(C2<T>)), "cudaMalloc");
+    check(p->partial_weight.alloc((size_t)p->groups * n * sizeof(T)), "cudaMalloc");
+    check(p->grad_p64.alloc((size_t)n * sizeof(double2)), "cudaMalloc");
+    check(p->weight_p64.alloc((size_t)n * sizeof(double)), "cudaMalloc");
+    p->probe_blocks = kblocks;
+    check(p->probe_block_max.alloc((size_t)kblocks * sizeof(double)), "cudaMalloc");
+    check(p->maxes.alloc(4 * sizeof(double)), "cudaMalloc");
+    check(p->sums.alloc(8 * sizeof(double)), "cudaMalloc");
+    check(p->aperture64.alloc((size_t)n * sizeof(double)), "cudaMalloc");
+    if (!p->mask.empty()) upload(p->mask_dev, p->mask, s);
+    // ---- twiddles
+    const std::vector<double2> tr = twiddles(R), tc = twiddles(C);
+    upload(p->tw_r64, tr, s);
+    upload(p->tw_c64, tc, s);
+    std::vector<C2<T>> trt(R), tct(C);
+    for (int i = 0; i < R; i++) trt[i] = mk<T>((T)tr[i].x, (T)tr[i].y);
+    for (int i = 0; i < C; i++) tct[i] = mk<T>((T)tc[i].x, (T)tc[i].y);
+    upload(p->tw_r, trt, s);
+    upload(p->tw_c, tct, s);
+    p->rad_rows = factor_length(R);
+    p->rad_columns = factor_length(C);
+}
+
+Fft2Plan64 fft64(const cubo_ptycho_plan *p) {
+    return Fft2Plan64{p->R, p->C, p->rad_rows, p->rad_columns, p->tw_r64.as<double2>(), p->tw_c64.as<double2>()};
+}
+
+void ensure_errors(cubo_ptycho_plan *p, long long needed) {
+    if (needed <= p->errors_capacity) return;
+    long long cap = std::max<long long>(needed, std::max<long long>(64, 2 * p->errors_capacity));
+    DeviceBuffer fresh;
+    check(fresh.alloc((size_t)cap * sizeof(double)), "cudaMalloc errors");
+    if (p->iterations_done > 0)
+        check(cudaMemcpyAsync(fresh.ptr, p->errors.ptr, (size_t)p->iterations_done * sizeof(double),
+                              cudaMemcpyDeviceToDevice, p->ctx->stream), "copy errors");
+    check(cudaStreamSynchronize(p->ctx->stream), "cudaStreamSynchronize");
+    std::swap(p->errors.ptr, fresh.ptr);
+    std::swap(p->errors.bytes, fresh.bytes);
+    p->errors_capacity = cap;
+}
+
+// The shifted-probe table for the current probe: class 0 is the probe itself, classes 1.. its Fourier shifts.
+template <typename T>
+void enqueue_shift_table(cubo_ptycho_plan *p) {
+    cudaStream_t s = p->ctx->stream;
+    const int n = p->n, frac = p->classes - 1;
+    timed(p, kShiftTable, 1, [&] { return launch_convert<T>(p->probe64.as<double2>(), p->shifted.as<C2<T>>(), n, s); });
+    if (frac == 0) return;
+    timed(p, kShiftTable, 2 + 1 + 2 + 1 + 1, [&] {
+        cudaError_t e = cudaMemcpyAsync(p->spectrum64.ptr, p->probe64.ptr, (size_t)n * sizeof(double2),
+                                        cudaMemcpyDeviceToDevice, s);
+        if (e == cudaSuccess) e = launch_fft2_f64(fft64(p), p->spectrum64.as<double2>(), 1, false, s);
+        if (e == cudaSuccess)
+            e = launch_shift_ramps(p->spectrum64.as<double2>(), p->ramps_r64.as<double2>(), p->ramps_c64.as<double2>(),
+                                   p->R, p->C, frac, p->shift_tmp64.as<double2>(), s);
+        if (e == cudaSuccess) e = launch_fft2_f64(fft64(p), p->shift_tmp64.as<double2>(), frac, true, s);
+        if (e == cudaSuccess) e = launch_scale_f64(p->shift_tmp64.as<double2>(), frac * n, 1.0 / n, s);
+        if (e == cudaSuccess)
+            e = launch_convert<T>(p->shift_tmp64.as<double2>(), p->shifted.as<C2<T>>() + n, (long long)frac * n, s);
+        return e;
+    });
+}
+
+// Probe update and constraints, FP64 (Ptychography.swift:383-395).
+void enqueue_probe_side(cubo_ptycho_plan *p) {
+    cudaStream_t s = p->ctx->stream;
+    const cubo_ptycho_params &pp = p->params;
+    const int n = p->n;
+    double2 *probe = p->probe64.as<double2>(), *x = p->scratch64.as<double2>();
+    double *sums = p->sums.as<double>();
+    if (!pp.fix_probe) {
+        timed(p, kProbeSide, 1, [&] {
+            return launch_probe_update(probe, p->grad_p64.as<double2>(), p->weight_p64.as<double>(), n,
+                                       p->maxes.as<double>() + 1, pp.step_size, pp.normalization_minimum, s);
+        });
+        if (pp.fix_probe_center_of_mass) {  // PtychographyConstraints.swift:34-37
+            timed(p, kProbeSide, 7, [&] {
+                cudaError_t e = launch_probe_moments(probe, p->R, p->C, sums, s);
+                if (e == cudaSuccess) e = cudaMemcpyAsync(x, probe, (size_t)n * sizeof(double2), cudaMemcpyDeviceToDevice, s);
+                if (e == cudaSuccess) e = launch_fft2_f64(fft64(p), x, 1, false, s);
+                if (e == cudaSuccess) e = launch_com_ramp(x, p->R, p->C, sums, s);
+                if (e == cudaSuccess) e = launch_fft2_f64(fft64(p), x, 1, true, s);
+                if (e == cudaSuccess) e = launch_scale_f64(x, n, 1.0 / n, s);
+                if (e == cudaSuccess) e = launch_commit_if_valid(probe, x, n, sums, s);
+                return e;
+            });
+        }
+        if (pp.fix_probe_aperture) {  // PtychographyConstraints.swift:59-71
+            timed(p, kProbeSide, 8, [&] {
+                cudaError_t e = launch_energy(probe, n, sums + 3, s);
+                if (e == cudaSuccess) e = cudaMemcpyAsync(x, probe, (size_t)n * sizeof(double2), cudaMemcpyDeviceToDevice, s);
+                if (e == cudaSuccess) e = launch_fft2_f64(fft64(p), x, 1, false, s);
+                if (e == cudaSuccess) e = launch_aperture_phase(x, p->aperture64.as<double>(), n, s);
+                if (e == cudaSuccess) e = launch_fft2_f64(fft64(p), x, 1, true, s);
+                if (e == cudaSuccess) e = launch_scale_f64(x, n, 1.0 / n, s);
+                if (e == cudaSuccess) e = launch_energy(x, n, sums + 4, s);
+                if (e == cudaSuccess) e = launch_renormalise(probe, x, n, sums + 3, sums + 4, s);
+                return e;
+            });
+        }
+        if (pp.constrain_probe_amplitude) {  // PtychographyConstraints.swift:40-55
+            timed(p, kProbeSide, 4, [&] {
+                cudaError_t e = launch_energy(probe, n, sums + 3, s);
+                if (e == cudaSuccess)
+                    e = launch_amplitude_mask(probe, p->R, p->C, pp.probe_amplitude_relative_radius,
+                                              pp.probe_amplitude_relative_width, s);
+                if (e == cudaSuccess) e = launch_energy(probe, n, sums + 4, s);
+                if (e == cudaSuccess) e = launch_renormalise(probe, probe, n, sums + 3, sums + 4, s);
+                return e;
+            });
+        }
+    }
+    if (!p->mask.empty())  // Ptychography.swift:395, not gated on fixProbe
+        timed(p, kProbeSide, 1, [&] { return launch_support_mask(probe, p->mask_dev.as<unsigned char>(), n, s); });
+}
+
+template <typename T>
+void enqueue_iteration(cubo_ptycho_plan *p) {
+    cudaStream_t s = p->ctx->stream;
+    const int n = p->n;
+    const ScanTables scan{p->rr.as<int>(), p->cc.as<int>(), p->cls.as<int>()};
+    enqueue_shift_table<T>(p);
+    PositionPassArgs<T> pa{};
+    pa.rows = p->R; pa.columns = p->C; pa.object_rows = p->OR; pa.object_columns = p->OC; pa.n = n;
+    pa.first = 0; pa.count = p->P; pa.scan = scan;
+    pa.shifted = p->shifted.as<C2<T>>(); pa.object = p->object.as<C2<T>>();
+    pa.amplitudes = p->amplitudes.as<float>(); pa.dpsi = p->dpsi.as<C2<T>>(); pa.error = p->error.as<double>();
+    pa.tw_rows = p->tw_r.as<C2<T>>(); pa.tw_columns = p->tw_c.as<C2<T>>();
+    pa.rad_rows = p->rad_rows; pa.rad_columns = p->rad_columns; pa.inv_n = (T)(1.0 / n);
+    timed(p, kPositionPass, 1, [&] { return launch_position_pass<T>(pa, s); });
+
+    ObjectGatherArgs<T> ga{};
+    ga.rows = p->R; ga.columns = p->C; ga.object_rows = p->OR; ga.object_columns = p->OC; ga.n = n;
+    ga.tiles_x = p->tiles_x; ga.tile_start = p->tile_start.as<int>(); ga.tile_list = p->tile_list.as<int>();
+    ga.scan = scan; ga.shifted = p->shifted.as<C2<T>>(); ga.dpsi = p->dpsi.as<C2<T>>();
+    ga.grad = p->grad_o.as<C2<T>>(); ga.weight = p->weight_o.as<T>(); ga.tile_max = p->tile_max.as<double>();
+    timed(p, kObjectGather, 1, [&] { return launch_object_gather<T>(ga, p->tiles, s); });
+
+    ProbeGatherArgs<T> pg{};
+    pg.rows = p->R; pg.columns = p->C; pg.object_rows = p->OR; pg.object_columns = p->OC; pg.n = n;
+    pg.count = p->P; pg.groups = p->groups; pg.scan = scan; pg.object = p->object.as<C2<T>>();
+    pg.dpsi = p->dpsi.as<C2<T>>(); pg.partial_grad = p->partial_grad.as<C2<T>>(); pg.partial_weight = p->partial_weight.as<T>();
+    timed(p, kProbeGather, 1, [&] { return launch_probe_gather<T>(pg, s); });
+    timed(p, kProbeReduce, 1, [&] {
+        return launch_probe_reduce<T>(p->partial_grad.as<C2<T>>(), p->partial_weight.as<T>(), p->groups, n,
+                                      p->grad_p64.as<double2>(), p->weight_p64.as<double>(),
+                                      p->probe_block_max.as<double>(), s);
+    });
+    timed(p, kMaxReduce, 2, [&] {
+        cudaError_t e = launch_max_reduce(p->tile_max.as<double>(), p->tiles, p->maxes.as<double>(), s);
+        if (e == cudaSuccess) e = launch_max_reduce(p->probe_block_max.as<double>(), p->probe_blocks, p->maxes.as<double>() + 1, s);
+        return e;
+    });
+    const cubo_ptycho_params &pp = p->params;
+    timed(p, kObjectUpdate, 1, [&] {
+        return launch_object_update<T>(p->object.as<C2<T>>(), p->grad_o.as<C2<T>>(), p->weight_o.as<T>(),
+                                       (int)p->objects, p->maxes.as<double>(), pp.step_size, pp.normalization_minimum,
+                                       pp.constrain_object_amplitude ? 1 : 0, pp.pure_phase_object ? 1 : 0, s);
+    });
+    enqueue_probe_side(p);
+    timed(p, kErrorReduce, 1, [&] {
+        return launch_error_reduce(p->error.as<double>(), p->P, p->divisor, p->errors.as<double>(),
+                                   p->iteration.as<int>(), s);
+    });
+}
+
+void enqueue_iterations(cubo_ptycho_plan *p, int iterations) {
+    ensure_errors(p, p->iterations_done + iterations);
+    for (int i = 0; i < iterations; i++) {
+        if (p->fp64) enqueue_iteration<double>(p);
+        else enqueue_iteration<float>(p);
+        p->iterations_done++;
+    }
+}
+
+}  // namespace
+
+// ------------------------------------------------------------------------------------------------ C ABI
+
+namespace {
+int run_guarded(cubo_ptycho_context *ctx, const std::function<void()> &body) {
+    if (!ctx) return CUBO_PTYCHO_INVALID_INPUT;
+    try {
+        cudaError_t e = cudaSetDevice(ctx->device);
+        if (e != cudaSuccess) fail(CUBO_PTYCHO_CUDA_ERROR, std::string("cudaSetDevice: ") + cudaGetErrorString(e));
+        body();
+        ctx->last_error.clear();
+        return CUBO_PTYCHO_OK;
+    } catch (const Failure &f) {
+        ctx->last_error = f.message;
+        return f.status;
+    } catch (const std::bad_alloc &) {
+        ctx->last_error = "host out of memory";
+        return CUBO_PTYCHO_OUT_OF_MEMORY;
+    }
+}
+}  // namespace
+
+extern "C" {
+
+void cubo_ptycho_params_default(cubo_ptycho_params *p) {
+    if (!p) return;
+    std::memset(p, 0, sizeof(*p));
+    p->iterations = 8;
+    p->step_size = 0.5;
+    p->normalization_minimum = 1;
+    p->constrain_object_amplitude = 1;
+    p->probe_amplitude_relative_radius = 0.5;
+    p->probe_amplitude_relative_width = 0.05;
+    p->error_normalization = CUBO_PTYCHO_ERRORS_SUPPLIED_AMPLITUDE_ENERGY;
+    p->form = CUBO_PTYCHO_FORM_FP32;
+}
+
+int cubo_ptycho_create(int device, cubo_ptycho_context **out) {
+    if (!out) return CUBO_PTYCHO_INVALID_INPUT;
+    *out = nullptr;
+    int count = 0;
+    if (cudaGetDeviceCount(&count) != cudaSuccess || count == 0) {
+        cudaGetLastError();
+        return CUBO_PTYCHO_NO_DEVICE;
+    }
+    if (device < 0 || device >= count) return CUBO_PTYCHO_INVALID_INPUT;
+    auto *ctx = new (std::nothrow) cubo_ptycho_context();
+    if (!ctx) return CUBO_PTYCHO_OUT_OF_MEMORY;
+    ctx->device = device;
+    if (cudaSetDevice(device) != cudaSuccess || cudaStreamCreateWithFlags(&ctx->stream, cudaStreamNonBlocking) != cudaSuccess) {
+        cudaGetLastError();
+        delete ctx;
+        return CUBO_PTYCHO_CUDA_ERROR;
+    }
+    *out = ctx;
+    return CUBO_PTYCHO_OK;
+}
+
+int cubo_ptycho_destroy(cubo_ptycho_context *ctx) {
+    if (!ctx) return CUBO_PTYCHO_OK;
+    cudaSetDevice(ctx->device);
+    if (ctx->stream) {
+        cudaStreamSynchronize(ctx->stream);
+        cudaStreamDestroy(ctx->stream);
+    }
+    delete ctx;
+    return CUBO_PTYCHO_OK;
+}
+
+const char *cubo_ptycho_last_error(const cubo_ptycho_context *ctx) {
+    return ctx ? ctx->last_error.c_str() : "no context";
+}
+
+void *cubo_ptycho_stream(cubo_ptycho_context *ctx) { return ctx ? (void *)ctx->stream : nullptr; }
+
+int cubo_ptycho_synchronize(cubo_ptycho_context *ctx) {
+    return run_guarded(ctx, [&] { check(cudaStreamSynchronize(ctx->stream), "cudaStreamSynchronize"); });
+}
+
+int cubo_ptycho_plan_create(cubo_ptycho_context *ctx, const cubo_ptycho_problem *pr, const cubo_ptycho_params *pp,
+                            cubo_ptycho_plan **out) {
+    if (!out) return CUBO_PTYCHO_INVALID_INPUT;
+    *out = nullptr;
+    std::unique_ptr<cubo_ptycho_plan> plan;
+    const int status = run_guarded(ctx, [&] {
+        double divisor = 0;
+        validate(pr, pp, &divisor);
+        plan.reset(new cubo_ptycho_plan());
+        cubo_ptycho_plan *p = plan.get();
+        p->ctx = ctx;
+        p->R = pr->rows; p->C = pr->columns; p->OR = pr->object_rows; p->OC = pr->object_columns; p->P = pr->count;
+        p->n = p->R * p->C;
+        p->objects = (long long)p->OR * p->OC;
+        p->params = *pp;
+        if (pp->probe_support_mask) p->mask.assign(pp->probe_support_mask, pp->probe_support_mask + p->n);
+        for (auto &m : p->mask) m = m ? 1 : 0;
+        p->params.probe_support_mask = nullptr;
+        p->divisor = divisor;
+        p->fp64 = pp->form == CUBO_PTYCHO_FORM_FP64;
+        if (pp->form == CUBO_PTYCHO_FORM_SPLIT_BF16)
+            fail(CUBO_PTYCHO_UNSUPPORTED, "the split-BF16 form is not available in this build");
+        if (!position_pass_supported(p->n, p->fp64))
+            fail(CUBO_PTYCHO_UNSUPPORTED, "detector of " + std::to_string(p->n) + " pixels exceeds the shared-memory "
+                                              "transform of this form");
+        int optin = 0;
+        check(cudaDeviceGetAttribute(&optin, cudaDevAttrMaxSharedMemoryPerBlockOptin, ctx->device), "attribute");
+        if (position_pass_smem(p->n, p->R, p->C, p->fp64) > (size_t)optin)
+            fail(CUBO_PTYCHO_UNSUPPORTED, "detector too large for shared memory");
+        check(configure_kernels(), "configure kernels");
+        p->kind_ms.assign(kKinds, 0.0);
+        p->kind_launches.assign(kKinds, 0);
+        if (p->fp64) build_plan<double>(p, pr);
+        else build_plan<float>(p, pr);
+        check(cudaStreamSynchronize(ctx->stream), "plan upload");
+    });
+    if (status == CUBO_PTYCHO_OK) *out = plan.release();
+    return status;
+}
+
+int cubo_ptycho_plan_destroy(cubo_ptycho_plan *plan) {
+    if (!plan) return CUBO_PTYCHO_OK;
+    cudaSetDevice(plan->ctx->device);
+    cudaStreamSynchronize(plan->ctx->stream);
+    delete plan;
+    return CUBO_PTYCHO_OK;
+}
+
+int cubo_ptycho_plan_set_state(cubo_ptycho_plan *p, const double *ore, const double *oim, const double *pre,
+                               const double *pim) {
+    if (!p) return CUBO_PTYCHO_INVALID_INPUT;
+    return run_guarded(p->ctx, [&] {
+        if (!ore || !oim || !pre || !pim) fail(CUBO_PTYCHO_INVALID_INPUT, "null state");
+        for (long long j = 0; j < p->objects; j++)
+            if (!std::isfinite(ore[j]) || !std::isfinite(oim[j])) fail(CUBO_PTYCHO_INVALID_INPUT, "object not finite");
+        for (int k = 0; k < p->n; k++)
+            if (!std::isfinite(pre[k]) || !std::isfinite(pim[k])) fail(CUBO_PTYCHO_INVALID_INPUT, "probe not finite");
+        cudaStream_t s = p->ctx->stream;
+        std::vector<double2> probe(p->n);
+        for (int k = 0; k < p->n; k++) probe[k] = make_double2(pre[k], pim[k]);
+        check(cudaMemcpyAsync(p->probe64.ptr, probe.data(), (size_t)p->n * sizeof(double2), cudaMemcpyHostToDevice, s), "upload probe");
+        if (p->fp64) {
+            std::vector<double2> o((size_t)p->objects);
+            for (long long j = 0; j < p->objects; j++) o[j] = make_double2(ore[j], oim[j]);
+            check(cudaMemcpyAsync(p->object.ptr, o.data(), o.size() * sizeof(double2), cudaMemcpyHostToDevice, s), "upload object");
+            check(cudaStreamSynchronize(s), "sync");
+        } else {
+            std::vector<float2> o((size_t)p->objects);
+            for (long long j = 0; j < p->objects; j++) o[j] = make_float2((float)ore[j], (float)oim[j]);
+            check(cudaMemcpyAsync(p->object.ptr, o.data(), o.size() * sizeof(float2), cudaMemcpyHostToDevice, s), "upload object");
+            check(cudaStreamSynchronize(s), "sync");
+        }
+        // the initial Fourier amplitude for fixProbeAperture (PtychographyConstraints.swift:79-83)
+        if (p->params.fix_probe_aperture) {
+            check(cudaMemcpyAsync(p->scratch64.ptr, p->probe64.ptr, (size_t)p->n * sizeof(double2), cudaMemcpyDeviceToDevice, s), "copy");
+            check(launch_fft2_f64(fft64(p), p->scratch64.as<double2>(), 1, false, s), "fft");
+            check(launch_magnitude(p->scratch64.as<double2>(), p->aperture64.as<double>(), p->n, s), "magnitude");
+            check(cudaStreamSynchronize(s), "sync");
+        }
+    });
+}
+
+int cubo_ptycho_plan_get_state(cubo_ptycho_plan *p, double *ore, double *oim, double *pre, double *pim) {
+    if (!p) return CUBO_PTYCHO_INVALID_INPUT;
+    return run_guarded(p->ctx, [&] {
+        cudaStream_t s = p->ctx->stream;
+        std::vector<double2> probe(p->n);
+        check(cudaMemcpyAsync(probe.data(), p->probe64.ptr, (size_t)p->n * sizeof(double2), cudaMemcpyDeviceToHost, s), "download probe");
+        if (p->fp64) {
+            std::vector<double2> o((size_t)p->objects);
+            check(cudaMemcpyAsync(o.data(), p->object.ptr, o.size() * sizeof(double2), cudaMemcpyDeviceToHost, s), "download object");
+            check(cudaStreamSynchronize(s), "sync");
+            for (long long j = 0; j < p->objects; j++) { if (ore) ore[j] = o[j].x; if (oim) oim[j] = o[j].y; }
+        } else {
+            std::vector<float2> o((size_t)p->objects);
+            check(cudaMemcpyAsync(o.data(), p->object.ptr, o.size() * sizeof(float2), cudaMemcpyDeviceToHost, s), "download object");
+            check(cudaStreamSynchronize(s), "sync");
+            for (long long j = 0; j < p->objects; j++) { if (ore) ore[j] = o[j].x; if (oim) oim[j] = o[j].y; }
+        }
+        for (int k = 0; k < p->n; k++) { if (pre) pre[k] = probe[k].x; if (pim) pim[k] = probe[k].y; }
+    });
+}
+
+int cubo_ptycho_plan_enqueue(cubo_ptycho_plan *p, int iterations) {
+    if (!p) return CUBO_PTYCHO_INVALID_INPUT;
+    return run_guarded(p->ctx, [&] {
+        if (iterations < 0) fail(CUBO_PTYCHO_INVALID_INPUT, "iterations");
+        enqueue_iterations(p, iterations);
+    });
+}
+
+int cubo_ptycho_plan_errors(cubo_ptycho_plan *p, int count, double *errors) {
+    if (!p) return CUBO_PTYCHO_INVALID_INPUT;
+    return run_guarded(p->ctx, [&] {
+        if (count < 0 || count > p->iterations_done || (count > 0 && !errors)) fail(CUBO_PTYCHO_INVALID_INPUT, "count");
+        check(cudaStreamSynchronize(p->ctx->stream), "sync");
+        if (count > 0)
+            check(cudaMemcpy(errors, p->errors.as<double>() + (p->iterations_done - count), (size_t)count * sizeof(double),
+                             cudaMemcpyDeviceToHost), "download errors");
+    });
+}
+
+int cubo_ptycho_plan_iterate(cubo_ptycho_plan *p, int iterations, double *errors) {
+    if (!p) return CUBO_PTYCHO_INVALID_INPUT;
+    int cancelled = 0;
+    const int status = run_guarded(p->ctx, [&] {
+        if (iterations < 0) fail(CUBO_PTYCHO_INVALID_INPUT, "iterations");
+        const long long start = p->iterations_done;
+        ensure_errors(p, start + iterations);
+        for (int i = 0; i < iterations; i++) {
+            if (p->params.cancel && *p->params.cancel) { cancelled = 1; break; }  // Ptychography.swift:281
+            enqueue_iterations(p, 1);
+            if (p->params.progress) {
+                check(cudaStreamSynchronize(p->ctx->stream), "sync");
+                p->params.progress(i + 1, iterations, p->params.progress_user);  // Ptychography.swift:401
+            }
+        }
+        check(cudaStreamSynchronize(p->ctx->stream), "sync");
+        if (!cancelled && errors && iterations > 0)
+            check(cudaMemcpy(errors, p->errors.as<double>() + start, (size_t)iterations * sizeof(double),
+                             cudaMemcpyDeviceToHost), "download errors");
+    });
+    if (status == CUBO_PTYCHO_OK && cancelled) {
+        p->ctx->last_error = "cancelled";
+        return CUBO_PTYCHO_CANCELLED;
+    }
+    return status;
+}
+
+int cubo_ptycho_reconstruct(cubo_ptycho_context *ctx, const cubo_ptycho_problem *pr, const cubo_ptycho_params *pp,
+                            double *ore, double *oim, double *pre, double *pim, double *errors) {
+    if (!ctx) return CUBO_PTYCHO_INVALID_INPUT;
+    if (!ore || !oim || !pre || !pim || (pp && pp->iterations > 0 && !errors)) {
+        ctx->last_error = "null output";
+        return CUBO_PTYCHO_INVALID_INPUT;
+    }
+    cubo_ptycho_plan *plan = nullptr;
+    int status = cubo_ptycho_plan_create(ctx, pr, pp, &plan);
+    if (status != CUBO_PTYCHO_OK) return status;
+    status = cubo_ptycho_plan_set_state(plan, ore, oim, pre, pim);
+    if (status == CUBO_PTYCHO_OK) status = cubo_ptycho_plan_iterate(plan, pp->iterations, errors);
+    if (status == CUBO_PTYCHO_OK) status = cubo_ptycho_plan_get_state(plan, ore, oim, pre, pim);
+    const std::string message = ctx->last_error;
+    cubo_ptycho_plan_destroy(plan);
+    ctx->last_error = message;
+    return status;
+}
+
+int cubo_ptycho_plan_set_timing(cubo_ptycho_plan *p, int enabled) {
+    if (!p) return CUBO_PTYCHO_INVALID_INPUT;
+    return run_guarded(p->ctx, [&] {
+        collect_timing(p);
+        p->timing = enabled != 0;
+        std::fill(p->kind_ms.begin(), p->kind_ms.end(), 0.0);
+        std::fill(p->kind_launches.begin(), p->kind_launches.end(), 0);
+    });
+}
+
+int cubo_ptycho_plan_kernel_stats(cubo_ptycho_plan *p, int capacity, const char **names, double *ms,
+                                  long long *launches, int *count) {
+    if (!p || !count) return CUBO_PTYCHO_INVALID_INPUT;
+    return run_guarded(p->ctx, [&] {
+        collect_timing(p);
+        int filled = 0;
+        for (int k = 0; k < kKinds && filled < capacity; k++) {
+            if (names) names[filled] = kKindNames[k];
+            if (ms) ms[filled] = p->kind_ms[k];
+            if (launches) launches[filled] = p->kind_launches[k];
+            filled++;
+        }
+        *count = filled;
+    });
+}
+
+long long cubo_ptycho_plan_launch_count(const cubo_ptycho_plan *p) { return p ? p->launches : -1; }
+
+int cubo_ptycho_probe_build(cubo_ptycho_context *ctx, int rows, int columns, double row_sampling, double column_sampling,
+                            double wavelength, double cutoff, double rolloff, double defocus, double astigmatism,
+                            double astigmatism_angle, double spherical_aberration, int term_count, const double *terms,
+                            double *re, double *im) {
+    return run_guarded(ctx, [&] {
+        // Ptychography.swift:147-153
+        if (!(rows > 1 && columns > 1) || !re || !im) fail(CUBO_PTYCHO_INVALID_INPUT, "probe shape");
+        const double pos[4] = {row_sampling, column_sampling, wavelength, cutoff};
+        for (double v : pos) if (!finite_positive(v)) fail(CUBO_PTYCHO_INVALID_INPUT, "probe sampling");
+        if (!(std::isfinite(rolloff) && rolloff >= 0)) fail(CUBO_PTYCHO_INVALID_INPUT, "rolloff");
+        if (!(std::isfinite(defocus) && std::isfinite(astigmatism) && std::isfinite(astigmatism_angle) &&
+              std::isfinite(spherical_aberration)))
+            fail(CUBO_PTYCHO_INVALID_INPUT, "aberrations");
+        if (term_count < 0 || (term_count > 0 && !terms)) fail(CUBO_PTYCHO_INVALID_INPUT, "terms");
+        for (int t = 0; t < term_count; t++) {  // PtychographyAberrationTerm.isValid, Ptychography.swift:123-125
+            const double nr = terms[4 * t], mr = terms[4 * t + 1], sine = terms[4 * t + 2], c = terms[4 * t + 3];
+            if (!(std::isfinite(c) && nr >= 1 && nr <= 64 && mr >= 0 && (sine == 0 || mr > 0)))
+                fail(CUBO_PTYCHO_INVALID_INPUT, "aberration term");
+        }
+        const int n = rows * columns;
+        cudaStream_t s = ctx->stream;
+        DeviceBuffer field, dterms, twr, twc, sum;
+        check(field.alloc((size_t)n * sizeof(double2)), "cudaMalloc");
+        check(sum.alloc(sizeof(double)), "cudaMalloc");
+        std::vector<double> tv(terms ? terms : nullptr, terms ? terms + 4 * term_count : nullptr);
+        upload(dterms, tv, s);
+        upload(twr, twiddles(rows), s);
+        upload(twc, twiddles(columns), s);
+        Fft2Plan64 f{rows, columns, factor_length(rows), factor_length(columns), twr.as<double2>(), twc.as<double2>()};
+        check(launch_probe_spectrum(field.as<double2>(), rows, columns, row_sampling, column_sampling, wavelength, cutoff,
+                                    rolloff, defocus, astigmatism, astigmatism_angle, spherical_aberration, term_count,
+                                    dterms.as<double>(), s), "probe spectrum");
+        check(launch_fft2_f64(f, field.as<double2>(), 1, true, s), "probe transform");
+        check(launch_scale_f64(field.as<double2>(), n, 1.0 / n, s), "scale");
+        check(launch_energy(field.as<double2>(), n, sum.as<double>(), s), "energy");
+        double energy = 0;
+        check(cudaMemcpyAsync(&energy, sum.ptr, sizeof(double), cudaMemcpyDeviceToHost, s), "download");
+        std::vector<double2> out(n);
+        check(cudaMemcpyAsync(out.data(), field.ptr, (size_t)n * sizeof(double2), cudaMemcpyDeviceToHost, s), "download");
+        check(cudaStreamSynchronize(s), "sync");
+        const double norm = std::sqrt(energy);
+        if (!finite_positive(norm)) fail(CUBO_PTYCHO_INVALID_INPUT, "probe without intensity");
+        for (int k = 0; k < n; k++) { re[k] = out[k].x / norm; im[k] = out[k].y / norm; }
+    });
+}
+
+}  // extern "C"

@@ -1,0 +1,324 @@
+"""Python mirror of CuboPtycho's single-slice API over the B200 engine.
+
+``SingleslicePtychography.reconstruct`` here takes the parameters of the Swift call of the same name
+(``Sources/CuboPtycho/Ptychography.swift:218-234``) in snake case, with the same defaults, refusals
+(``PtychographyError`` for ``invalidInput``) and ``CancellationError``; ``precision`` picks the GPU form.  Every
+call goes through the C ABI of ``include/cubo_ptycho.h``; nothing here computes on the CPU.
+"""
+from __future__ import annotations
+
+import ctypes as C
+from dataclasses import dataclass
+from typing import Callable, Optional, Sequence
+
+import numpy as np
+
+from . import _lib as L
+
+
+class PtychographyError(ValueError):
+    """``PtychographyError.invalidInput`` (``Ptychography.swift:24-27``)."""
+
+
+class CancellationError(Exception):
+    """Swift's ``CancellationError`` (``PtychographySingle.swift:222-224``)."""
+
+
+class DeviceError(RuntimeError):
+    """A device failure the CPU path cannot have (CUDA error, out of memory, device wait timed out, no device)."""
+
+    def __init__(self, status: int, message: str):
+        super().__init__(f"status {status}: {message}")
+        self.status = status
+
+
+class UnsupportedError(DeviceError):
+    pass
+
+
+FORMS = {"fp32": L.FORM_FP32, "split_bf16": L.FORM_SPLIT_BF16, "fp64": L.FORM_FP64}
+
+
+def _raise(status: int, message: str):
+    if status == L.INVALID_INPUT:
+        raise PtychographyError(message)
+    if status == L.CANCELLED:
+        raise CancellationError(message)
+    if status == L.UNSUPPORTED:
+        raise UnsupportedError(status, message)
+    raise DeviceError(status, message)
+
+
+class Context:
+    """A device context (``cubo_ptycho_create``): a CUDA stream and the engine's scratch on one GPU."""
+
+    def __init__(self, device: int = 0):
+        self.lib = L.load()
+        h = C.c_void_p()
+        st = self.lib.cubo_ptycho_create(device, C.byref(h))
+        if st != L.OK:
+            _raise(st, "cubo_ptycho_create failed")
+        self.handle = h
+        self.device = device
+
+    def check(self, status: int):
+        if status != L.OK:
+            _raise(status, self.lib.cubo_ptycho_last_error(self.handle).decode())
+
+    @property
+    def stream(self) -> int:
+        return self.lib.cubo_ptycho_stream(self.handle)
+
+    def synchronize(self):
+        self.check(self.lib.cubo_ptycho_synchronize(self.handle))
+
+    def close(self):
+        if getattr(self, "handle", None):
+            self.lib.cubo_ptycho_destroy(self.handle)
+            self.handle = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+
+_default_contexts: dict[int, Context] = {}
+
+
+def context(device: int = 0) -> Context:
+    if device not in _default_contexts:
+        _default_contexts[device] = Context(device)
+    return _default_contexts[device]
+
+
+@dataclass
+class Result:
+    """``SingleslicePtychography.Result`` (``Ptychography.swift:179-188``)."""
+    object: np.ndarray
+    probe: np.ndarray
+    errors: np.ndarray
+    positions: np.ndarray
+
+
+def _split(z, shape=None):
+    z = np.asarray(z)
+    if shape is not None and z.size != int(np.prod(shape)):
+        raise PtychographyError("array size")
+    re = np.ascontiguousarray(np.real(z), dtype=np.float64).ravel()
+    im = np.ascontiguousarray(np.imag(z), dtype=np.float64).ravel()
+    return re, im
+
+
+def _ptr(a, t=C.c_double):
+    return a.ctypes.data_as(C.POINTER(t))
+
+
+class _Inputs:
+    """Keeps the ctypes structures and the arrays they point into alive for one call."""
+
+    def __init__(self, amplitudes, positions, object_shape, probe_shape, iterations, step_size, normalization_minimum,
+                 fix_probe, pure_phase_object, constrain_object_amplitude, fix_probe_center_of_mass,
+                 constrain_probe_amplitude, probe_amplitude_relative_radius, probe_amplitude_relative_width,
+                 fix_probe_aperture, probe_support_mask, error_normalization, position_correction, precision):
+        rows, columns = probe_shape
+        positions = np.asarray(positions, np.float64).reshape(-1, 2) if np.size(positions) else np.zeros((0, 2))
+        count = len(positions)
+        amps = np.asarray(amplitudes)
+        if amps.size != count * rows * columns:
+            raise PtychographyError("amplitudes.count != positions * probe pixels")  # Ptychography.swift:248
+        self.amplitudes = np.ascontiguousarray(amps, dtype=np.float32).ravel()
+        self.rows_ = np.ascontiguousarray(positions[:, 0])
+        self.cols_ = np.ascontiguousarray(positions[:, 1])
+        self.problem = L.Problem(rows, columns, object_shape[0], object_shape[1], count, _ptr(self.amplitudes, C.c_float),
+                                 _ptr(self.rows_), _ptr(self.cols_))
+        self.params = L.Params()
+        p = self.params
+        p.iterations = int(iterations)
+        p.step_size = float(step_size)
+        p.normalization_minimum = float(normalization_minimum)
+        p.fix_probe = int(bool(fix_probe))
+        p.pure_phase_object = int(bool(pure_phase_object))
+        p.constrain_object_amplitude = int(bool(constrain_object_amplitude))
+        p.fix_probe_center_of_mass = int(bool(fix_probe_center_of_mass))
+        p.constrain_probe_amplitude = int(bool(constrain_probe_amplitude))
+        p.probe_amplitude_relative_radius = float(probe_amplitude_relative_radius)
+        p.probe_amplitude_relative_width = float(probe_amplitude_relative_width)
+        p.fix_probe_aperture = int(bool(fix_probe_aperture))
+        self.mask = None
+        if probe_support_mask is not None:
+            m = np.asarray(probe_support_mask, bool).ravel()
+            if m.size != rows * columns:
+                raise PtychographyError("probeSupportMask.count != probe pixels")  # Ptychography.swift:256
+            self.mask = np.ascontiguousarray(m.astype(np.uint8))
+            p.probe_support_mask = _ptr(self.mask, C.c_ubyte)
+        if isinstance(error_normalization, tuple):
+            kind, mean = error_normalization
+            if kind != "meanIntensity":
+                raise PtychographyError("error normalisation")
+            p.error_normalization = L.ERRORS_MEAN_INTENSITY
+            p.mean_intensity = float(mean)
+        elif error_normalization == "suppliedAmplitudeEnergy":
+            p.error_normalization = L.ERRORS_SUPPLIED_AMPLITUDE_ENERGY
+        else:
+            raise PtychographyError("error normalisation")
+        p.has_position_correction = 0 if position_correction is None else 1
+        if precision not in FORMS:
+            raise PtychographyError(f"precision {precision!r}")
+        p.form = FORMS[precision]
+        self.cancel_flag = C.c_int(0)
+        self.count = count
+
+
+class SingleslicePtychography:
+    """``SingleslicePtychography`` (``Ptychography.swift:176-407``) on the GPU."""
+
+    Result = Result
+
+    @staticmethod
+    def reconstruct(amplitudes, positions, object, probe, iterations: int = 8, step_size: float = 0.5,
+                    normalization_minimum: float = 1.0, fix_probe: bool = False, pure_phase_object: bool = False,
+                    constrain_object_amplitude: bool = True, fix_probe_center_of_mass: bool = False,
+                    constrain_probe_amplitude: bool = False, probe_amplitude_relative_radius: float = 0.5,
+                    probe_amplitude_relative_width: float = 0.05, fix_probe_aperture: bool = False,
+                    probe_support_mask=None, error_normalization="suppliedAmplitudeEnergy",
+                    position_correction=None, precision: str = "fp32",
+                    is_cancelled: Optional[Callable[[], bool]] = None,
+                    progress: Optional[Callable[[int, int], None]] = None, device: int = 0) -> Result:
+        """Reconstructs from corner-centred amplitudes ``[position][row][column]``; see ``include/cubo_ptycho.h``.
+
+        ``object`` and ``probe`` are complex 2-D arrays (``PtychographyArray``); ``positions`` is ``(P, 2)`` rows and
+        columns in object pixels.  ``error_normalization`` is ``"suppliedAmplitudeEnergy"`` or
+        ``("meanIntensity", m)``.  ``precision`` is ``"fp32"``, ``"split_bf16"`` or ``"fp64"``.
+        ``is_cancelled`` is polled before every iteration and raises ``CancellationError``; ``progress(completed,
+        total)`` runs after each iteration.
+        """
+        obj = np.asarray(object)
+        prb = np.asarray(probe)
+        if obj.ndim != 2 or prb.ndim != 2:
+            raise PtychographyError("object and probe must be 2-D")
+        ctx = context(device)
+        inp = _Inputs(amplitudes, positions, obj.shape, prb.shape, iterations, step_size, normalization_minimum,
+                      fix_probe, pure_phase_object, constrain_object_amplitude, fix_probe_center_of_mass,
+                      constrain_probe_amplitude, probe_amplitude_relative_radius, probe_amplitude_relative_width,
+                      fix_probe_aperture, probe_support_mask, error_normalization, position_correction, precision)
+        if is_cancelled is not None and is_cancelled():
+            raise CancellationError("cancelled")
+        cb = None
+        if is_cancelled is not None or progress is not None:
+            def _progress(done, total, _user):
+                if progress is not None:
+                    progress(done, total)
+                if is_cancelled is not None and is_cancelled():
+                    inp.cancel_flag.value = 1
+            cb = L.PROGRESS_FN(_progress)
+            inp.params.progress = cb
+            inp.params.cancel = C.pointer(inp.cancel_flag)
+        ore, oim = _split(obj)
+        pre, pim = _split(prb)
+        errors = np.zeros(max(int(iterations), 1))
+        st = ctx.lib.cubo_ptycho_reconstruct(ctx.handle, C.byref(inp.problem), C.byref(inp.params), _ptr(ore),
+                                             _ptr(oim), _ptr(pre), _ptr(pim), _ptr(errors))
+        ctx.check(st)
+        pos = np.column_stack([inp.rows_, inp.cols_]) if inp.count else np.zeros((0, 2))
+        return Result((ore + 1j * oim).reshape(obj.shape), (pre + 1j * pim).reshape(prb.shape),
+                      errors[: int(iterations)].copy(), pos)
+
+
+class Plan:
+    """A device-resident reconstruction (``cubo_ptycho_plan_*``): upload once, iterate, read the state back."""
+
+    def __init__(self, amplitudes, positions, object_shape, probe_shape, ctx: Optional[Context] = None, **kwargs):
+        self.ctx = ctx or context(kwargs.pop("device", 0))
+        defaults = dict(iterations=0, step_size=0.5, normalization_minimum=1.0, fix_probe=False,
+                        pure_phase_object=False, constrain_object_amplitude=True, fix_probe_center_of_mass=False,
+                        constrain_probe_amplitude=False, probe_amplitude_relative_radius=0.5,
+                        probe_amplitude_relative_width=0.05, fix_probe_aperture=False, probe_support_mask=None,
+                        error_normalization="suppliedAmplitudeEnergy", position_correction=None, precision="fp32")
+        defaults.update(kwargs)
+        self.inputs = _Inputs(amplitudes, positions, tuple(object_shape), tuple(probe_shape), **defaults)
+        self.object_shape = tuple(object_shape)
+        self.probe_shape = tuple(probe_shape)
+        h = C.c_void_p()
+        self.ctx.check(self.ctx.lib.cubo_ptycho_plan_create(self.ctx.handle, C.byref(self.inputs.problem),
+                                                            C.byref(self.inputs.params), C.byref(h)))
+        self.handle = h
+
+    def set_state(self, obj, probe):
+        ore, oim = _split(obj, self.object_shape)
+        pre, pim = _split(probe, self.probe_shape)
+        self.ctx.check(self.ctx.lib.cubo_ptycho_plan_set_state(self.handle, _ptr(ore), _ptr(oim), _ptr(pre), _ptr(pim)))
+
+    def get_state(self):
+        no = int(np.prod(self.object_shape))
+        npb = int(np.prod(self.probe_shape))
+        ore, oim, pre, pim = np.zeros(no), np.zeros(no), np.zeros(npb), np.zeros(npb)
+        self.ctx.check(self.ctx.lib.cubo_ptycho_plan_get_state(self.handle, _ptr(ore), _ptr(oim), _ptr(pre), _ptr(pim)))
+        return (ore + 1j * oim).reshape(self.object_shape), (pre + 1j * pim).reshape(self.probe_shape)
+
+    def iterate(self, iterations: int):
+        errors = np.zeros(max(iterations, 1))
+        self.ctx.check(self.ctx.lib.cubo_ptycho_plan_iterate(self.handle, iterations, _ptr(errors)))
+        return errors[:iterations]
+
+    def enqueue(self, iterations: int):
+        self.ctx.check(self.ctx.lib.cubo_ptycho_plan_enqueue(self.handle, iterations))
+
+    def errors(self, count: int):
+        out = np.zeros(max(count, 1))
+        self.ctx.check(self.ctx.lib.cubo_ptycho_plan_errors(self.handle, count, _ptr(out)))
+        return out[:count]
+
+    def set_timing(self, enabled: bool):
+        self.ctx.check(self.ctx.lib.cubo_ptycho_plan_set_timing(self.handle, 1 if enabled else 0))
+
+    def kernel_stats(self):
+        cap = 32
+        names = (C.c_char_p * cap)()
+        ms = (C.c_double * cap)()
+        launches = (C.c_longlong * cap)()
+        count = C.c_int(0)
+        self.ctx.check(self.ctx.lib.cubo_ptycho_plan_kernel_stats(self.handle, cap, names, ms, launches, C.byref(count)))
+        return {names[i].decode(): (ms[i], launches[i]) for i in range(count.value)}
+
+    @property
+    def launch_count(self) -> int:
+        return int(self.ctx.lib.cubo_ptycho_plan_launch_count(self.handle))
+
+    def close(self):
+        if getattr(self, "handle", None):
+            self.ctx.lib.cubo_ptycho_plan_destroy(self.handle)
+            self.handle = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+
+class PtychographyProbe:
+    """``PtychographyProbe.build`` (``Ptychography.swift:142-172``), evaluated on the device in FP64."""
+
+    @staticmethod
+    def build(rows: int, columns: int, row_sampling: float, column_sampling: float, wavelength: float, cutoff: float,
+              rolloff: float = 0.002, defocus: float = 0.0, astigmatism: float = 0.0, astigmatism_angle: float = 0.0,
+              spherical_aberration: float = 0.0, higher_order: Sequence = (), device: int = 0) -> np.ndarray:
+        """``higher_order`` rows are ``(radialOrder, angularOrder, sine, coefficient)``."""
+        ctx = context(device)
+        t = np.ascontiguousarray(np.asarray(higher_order, np.float64).reshape(-1, 4))
+        re = np.zeros(rows * columns)
+        im = np.zeros(rows * columns)
+        st = ctx.lib.cubo_ptycho_probe_build(ctx.handle, rows, columns, row_sampling, column_sampling, wavelength,
+                                             cutoff, rolloff, defocus, astigmatism, astigmatism_angle,
+                                             spherical_aberration, len(t), _ptr(t), _ptr(re), _ptr(im))
+        ctx.check(st)
+        return (re + 1j * im).reshape(rows, columns)
+
+
+def electron_wavelength(energy_ev: float) -> float:
+    """Relativistic electron wavelength in angstrom from CODATA constants."""
+    h, m, e, c = 6.62607015e-34, 9.1093837015e-31, 1.602176634e-19, 299792458.0
+    v = energy_ev * e
+    return h / np.sqrt(2 * m * v * (1 + v / (2 * m * c * c))) * 1e10

@@ -1,0 +1,164 @@
+/*
+ * cubo_ptycho.h — C ABI of the B200 (sm_100a) single-slice ptychography gradient-descent engine.
+ *
+ * This is the drop-in boundary for CuboKit's CuboPtycho hot path.  A SwiftPM system-library target (the way CuboKit
+ * already declares CStrainLAPACK and CEmbeddingLAPACK, Package.swift:48,50, with their headers in include/) exposes these
+ * functions to Swift; the Swift shim converts [Double]/[Float] to pointers and maps the int status to the reference's
+ * throws (INTEGRATION.md shows it).  Conventions follow the reference's C shims
+ * (Sources/CStrainLAPACK/include/CStrainLAPACK.h:1-2, Sources/CStrainLAPACK/LeastSquares.c:4-14): functions named
+ * cubo_<module>_<verb>, an int status (0 = ok), caller-owned buffers, plain pointers and sizes.
+ *
+ * Layouts are the reference's: every complex field is split into a real and an imaginary plane of doubles, row-major
+ * (PtychographyArray, Sources/CuboPtycho/Ptychography.swift:5-21); amplitudes are corner-centred
+ * [position][row][column] (Ptychography.swift:189); positions are in object pixels, row then column
+ * (PtychographyPosition, Ptychography.swift:88-93).
+ *
+ * Threading: every call is synchronous and blocking on the calling thread.  A context belongs to one host thread at a
+ * time; different contexts (also on the same device) are independent.  There is no global mutable state.
+ */
+#ifndef CUBO_PTYCHO_H
+#define CUBO_PTYCHO_H
+
+#include <stddef.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define CUBO_PTYCHO_ABI_VERSION 1
+
+#if defined(__GNUC__)
+#define CUBO_PTYCHO_API __attribute__((visibility("default")))
+#else
+#define CUBO_PTYCHO_API
+#endif
+
+/* Status codes.  Positive values are the reference's own throws; negative ones are device failures the CPU path cannot
+ * have (a Swift shim maps them to a new error case).  The device never traps: a device-side wait that runs out reports
+ * CUBO_PTYCHO_DEVICE_TIMEOUT and leaves the context usable. */
+enum {
+    CUBO_PTYCHO_OK = 0,
+    CUBO_PTYCHO_INVALID_INPUT = 1,   /* PtychographyError.invalidInput (Ptychography.swift:24-27, :247-259) */
+    CUBO_PTYCHO_CANCELLED = 2,       /* CancellationError (PtychographySingle.swift:222-224) */
+    CUBO_PTYCHO_CUDA_ERROR = -1,
+    CUBO_PTYCHO_OUT_OF_MEMORY = -2,
+    CUBO_PTYCHO_DEVICE_TIMEOUT = -3,
+    CUBO_PTYCHO_NO_DEVICE = -4,
+    CUBO_PTYCHO_UNSUPPORTED = -5     /* a size or form this build has no kernel for (the message names it) */
+};
+
+/* Arithmetic of the per-position transforms.  FP32: complex64 state and shared-memory FFTs.  SPLIT_BF16: the 128 x 128
+ * detector transforms as DFT-matrix products on the tensor cores with hi/lo BF16 operands and FP32 accumulation.  FP64:
+ * complex128 everywhere (the adjoint check's form).  In every form the loss, the normalisation maxima and the probe
+ * constraints are FP64. */
+enum { CUBO_PTYCHO_FORM_FP32 = 0, CUBO_PTYCHO_FORM_SPLIT_BF16 = 1, CUBO_PTYCHO_FORM_FP64 = 2 };
+
+/* PtychographyErrorNormalization (Ptychography.swift:30-48). */
+enum { CUBO_PTYCHO_ERRORS_SUPPLIED_AMPLITUDE_ENERGY = 0, CUBO_PTYCHO_ERRORS_MEAN_INTENSITY = 1 };
+
+typedef struct cubo_ptycho_context cubo_ptycho_context;
+typedef struct cubo_ptycho_plan cubo_ptycho_plan;
+
+/* The measured data and the geometry: SingleslicePtychography.reconstruct's amplitudes, positions and the shapes of its
+ * object and probe (Ptychography.swift:218-219).  Amplitudes are Float32 on the host, as reconstructSingle takes them
+ * (PtychographySingle.swift:40-41); the Swift shim converts the Double path's [Double] exactly as the reference's
+ * .single branch does (Ptychography.swift:237-239). */
+typedef struct {
+    int rows, columns;                 /* detector = probe shape */
+    int object_rows, object_columns;
+    int count;                         /* number of scan positions */
+    const float *amplitudes;           /* count * rows * columns */
+    const double *position_rows;       /* count */
+    const double *position_columns;    /* count */
+} cubo_ptycho_problem;
+
+typedef void (*cubo_ptycho_progress_fn)(int completed, int total, void *user);
+
+/* Every parameter of SingleslicePtychography.reconstruct (Ptychography.swift:218-234) except positionCorrection, which
+ * the GPU path refuses as the reference's .single path does (Ptychography.swift:236).  Booleans are ints (0 / nonzero).
+ * cubo_ptycho_params_default fills in the reference's defaults. */
+typedef struct {
+    int iterations;                    /* 8 */
+    double step_size;                  /* 0.5 */
+    double normalization_minimum;      /* 1 */
+    int fix_probe;                     /* false */
+    int pure_phase_object;             /* false */
+    int constrain_object_amplitude;    /* true */
+    int fix_probe_center_of_mass;      /* false */
+    int constrain_probe_amplitude;     /* false */
+    double probe_amplitude_relative_radius;  /* 0.5 */
+    double probe_amplitude_relative_width;   /* 0.05 */
+    int fix_probe_aperture;            /* false */
+    const unsigned char *probe_support_mask; /* NULL, or rows * columns bytes, nonzero = kept */
+    int error_normalization;           /* CUBO_PTYCHO_ERRORS_SUPPLIED_AMPLITUDE_ENERGY */
+    double mean_intensity;             /* for CUBO_PTYCHO_ERRORS_MEAN_INTENSITY */
+    int has_position_correction;       /* nonzero: refused with CUBO_PTYCHO_INVALID_INPUT */
+    int form;                          /* CUBO_PTYCHO_FORM_FP32 */
+    /* isCancelled: read before every iteration; nonzero stops the call with CUBO_PTYCHO_CANCELLED and leaves the
+     * caller's object and probe untouched.  NULL: never cancelled. */
+    const volatile int *cancel;
+    /* progress(completed, total) after each iteration, on the calling thread.  NULL: none. */
+    cubo_ptycho_progress_fn progress;
+    void *progress_user;
+} cubo_ptycho_params;
+
+/* Replaces the default arguments of SingleslicePtychography.reconstruct (Ptychography.swift:220-232). */
+CUBO_PTYCHO_API void cubo_ptycho_params_default(cubo_ptycho_params *params);
+
+/* A context owns a CUDA stream and device scratch on one device.  Replaces nothing in the reference (its CPU path has no
+ * device state); it is the handle the Swift shim keeps. */
+CUBO_PTYCHO_API int cubo_ptycho_create(int device, cubo_ptycho_context **out);
+CUBO_PTYCHO_API int cubo_ptycho_destroy(cubo_ptycho_context *context);
+/* Human-readable reason of the last non-zero status returned on this context (never NULL). */
+CUBO_PTYCHO_API const char *cubo_ptycho_last_error(const cubo_ptycho_context *context);
+
+/* SingleslicePtychography.reconstruct (Ptychography.swift:218-406) with positions fixed.
+ * object_re/object_im (object_rows * object_columns) and probe_re/probe_im (rows * columns) hold the start on entry and
+ * the result on return (Result.object, Result.probe, Ptychography.swift:179-188); errors receives params->iterations
+ * values (Result.errors).  Result.positions are the positions given.  Validation is the reference's
+ * (Ptychography.swift:247-259): CUBO_PTYCHO_INVALID_INPUT and nothing written on a refusal. */
+CUBO_PTYCHO_API int cubo_ptycho_reconstruct(cubo_ptycho_context *context, const cubo_ptycho_problem *problem,
+                            const cubo_ptycho_params *params, double *object_re, double *object_im, double *probe_re,
+                            double *probe_im, double *errors);
+
+/* ---- Device-resident plans: the same reconstruction split into its upload, iterations and download, so data stays in
+ * HBM across calls (resume = more iterations on the same plan).  No counterpart in the reference, whose arrays are
+ * Swift values; reconstruct() is create + set_state + iterate + get_state + destroy. */
+CUBO_PTYCHO_API int cubo_ptycho_plan_create(cubo_ptycho_context *context, const cubo_ptycho_problem *problem,
+                            const cubo_ptycho_params *params, cubo_ptycho_plan **out);
+CUBO_PTYCHO_API int cubo_ptycho_plan_destroy(cubo_ptycho_plan *plan);
+CUBO_PTYCHO_API int cubo_ptycho_plan_set_state(cubo_ptycho_plan *plan, const double *object_re, const double *object_im,
+                               const double *probe_re, const double *probe_im);
+CUBO_PTYCHO_API int cubo_ptycho_plan_get_state(cubo_ptycho_plan *plan, double *object_re, double *object_im, double *probe_re,
+                               double *probe_im);
+/* Runs `iterations` GD iterations on the resident state; errors (may be NULL) receives one value per iteration.
+ * Honours params->cancel and params->progress. */
+CUBO_PTYCHO_API int cubo_ptycho_plan_iterate(cubo_ptycho_plan *plan, int iterations, double *errors);
+/* Enqueues `iterations` iterations on the context's stream and returns without waiting (no cancel, no progress; the
+ * errors stay on the device, read them with cubo_ptycho_plan_errors after a synchronize).  For timing. */
+CUBO_PTYCHO_API int cubo_ptycho_plan_enqueue(cubo_ptycho_plan *plan, int iterations);
+CUBO_PTYCHO_API int cubo_ptycho_plan_errors(cubo_ptycho_plan *plan, int count, double *errors);
+/* The context's cudaStream_t, as an opaque pointer. */
+CUBO_PTYCHO_API void *cubo_ptycho_stream(cubo_ptycho_context *context);
+CUBO_PTYCHO_API int cubo_ptycho_synchronize(cubo_ptycho_context *context);
+
+/* Launch accounting of a plan: kernels launched since the plan was created, and, when timing is on, the device time of
+ * each kernel kind summed over its launches (CUDA events on the context stream).  kinds/ms/launches have room for
+ * `capacity` entries; *count receives the number of kinds filled in.  names are static strings. */
+CUBO_PTYCHO_API int cubo_ptycho_plan_set_timing(cubo_ptycho_plan *plan, int enabled);
+CUBO_PTYCHO_API int cubo_ptycho_plan_kernel_stats(cubo_ptycho_plan *plan, int capacity, const char **names, double *ms,
+                                  long long *launches, int *count);
+CUBO_PTYCHO_API long long cubo_ptycho_plan_launch_count(const cubo_ptycho_plan *plan);
+
+/* PtychographyProbe.build (Ptychography.swift:142-172) evaluated on the device in FP64 (the inverse transform is this
+ * library's FP64 FFT).  terms: term_count rows of {radialOrder, angularOrder, sine (0/1), coefficient}
+ * (PtychographyAberrationTerm, Ptychography.swift:101-133).  Writes rows * columns samples to re and im. */
+CUBO_PTYCHO_API int cubo_ptycho_probe_build(cubo_ptycho_context *context, int rows, int columns, double row_sampling,
+                            double column_sampling, double wavelength, double cutoff, double rolloff, double defocus,
+                            double astigmatism, double astigmatism_angle, double spherical_aberration, int term_count,
+                            const double *terms, double *re, double *im);
+
+#ifdef __cplusplus
+}
+#endif
+#endif
