@@ -224,6 +224,7 @@ def main():
     ap.add_argument("--form", default="fp32", choices=["fp32", "split_bf16"])
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--no-cpu", action="store_true")
+    ap.add_argument("--scan", type=int, default=SCAN, help="scan side (the benchmark workload is 256)")
     args = ap.parse_args()
     world, rank, local = dist_setup(args)
     if args.impl == "reference":
@@ -236,7 +237,7 @@ def main():
     import cubokit_b200 as cb
     from cubokit_b200 import synthetic
 
-    ds = synthetic.dataset(SCAN, DET, dose=DOSE, step=STEP, pinned=True, device=local)
+    ds = synthetic.dataset(args.scan, DET, dose=DOSE, step=STEP, pinned=True, device=local)
     P, n = len(ds.positions), DET * DET
     objects = ds.object_start.size
     ctx = cb.Context(local)
@@ -301,7 +302,7 @@ def main():
             "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
             "warmup": args.warmup, "ms_per_step": ms / args.steps, "higher_is_better": True, "scaling": "weak",
             "vs_baseline": None, "dtype": "f32" if args.form == "fp32" else "bf16x2/f32", "data": "synthetic",
-            "config": {"workload": f"{SCAN}x{SCAN} scan, step {STEP} px, {DET}x{DET} detector, object "
+            "config": {"workload": f"{args.scan}x{args.scan} scan, step {STEP} px, {DET}x{DET} detector, object "
                                    f"{ds.object_start.shape[0]}x{ds.object_start.shape[1]}, dose 1e5, GD step 0.5",
                        "form": args.form, "positions": P, "parallelism": f"replicas x{world}" if world > 1 else "1 GPU",
                        "l2": "inputs larger than L2 (4.3 GB amplitudes, 8.6 GB residuals)"},

@@ -14,6 +14,7 @@ OK, INVALID_INPUT, CANCELLED = 0, 1, 2
 CUDA_ERROR, OUT_OF_MEMORY, DEVICE_TIMEOUT, NO_DEVICE, UNSUPPORTED = -1, -2, -3, -4, -5
 FORM_FP32, FORM_SPLIT_BF16, FORM_FP64 = 0, 1, 2
 ERRORS_SUPPLIED_AMPLITUDE_ENERGY, ERRORS_MEAN_INTENSITY = 0, 1
+VARIANT_AUTO, VARIANT_GENERIC = 0, 1
 
 PROGRESS_FN = C.CFUNCTYPE(None, C.c_int, C.c_int, C.c_void_p)
 
@@ -35,6 +36,7 @@ class Params(C.Structure):
         ("fix_probe_aperture", C.c_int), ("probe_support_mask", C.POINTER(C.c_ubyte)),
         ("error_normalization", C.c_int), ("mean_intensity", C.c_double), ("has_position_correction", C.c_int),
         ("form", C.c_int), ("cancel", C.POINTER(C.c_int)), ("progress", PROGRESS_FN), ("progress_user", C.c_void_p),
+        ("variant", C.c_int),
     ]
 
 

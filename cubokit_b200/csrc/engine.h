@@ -55,6 +55,24 @@ struct ProbeGatherArgs {
     T *partial_weight;         // [groups][n]
 };
 
+// The 128 x 128 FP32 position pass (fast128.cu); amplitudes in its register order, 32 residual partials per position.
+struct Fast128Args {
+    int object_rows, object_columns;
+    int first, count;
+    ScanTables scan;
+    const float2 *shifted;
+    const float2 *object;
+    const float *amplitudes;   // [positions][column][t][parity][s]
+    float2 *dpsi;              // [positions][row][column]
+    double *error;             // [positions][32]
+    const float2 *tw128;       // W_128^t
+};
+bool fast128_applicable(int rows, int columns);
+size_t fast128_smem();
+cudaError_t configure_fast128();
+cudaError_t launch_fast128(const Fast128Args &a, int ctas, cudaStream_t s);
+cudaError_t launch_permute_amplitudes(const float *in, float *out, long long positions, cudaStream_t s);
+
 constexpr int kTileW = 32, kTileH = 8;   // object-gather tile (one pixel per thread)
 constexpr int kGatherThreads = kTileW * kTileH;
 

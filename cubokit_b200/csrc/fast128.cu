@@ -1,0 +1,271 @@
+// The FP32 position pass for a 128 x 128 detector: register-resident 2-D FFT pair (sm_100a).
+//
+// Same arithmetic as the generic position pass (exit wave, forward 2-D FFT, Fourier-modulus projection with the 1/n of
+// ifft2 folded in, inverse 2-D FFT; Ptychography.swift:321-350), laid out for the hardware:
+//
+//  * Persistent CTAs of 1024 threads (one per SM) walk the positions in a fixed stride; 8-thread groups own one line
+//    (a row in the row pass, a column in the column pass); each thread holds 16 complex samples in registers.
+//  * A 128-point line transform is 128 = 16 x 8 (four-step): with c = t + 8m and k = q + 16s,
+//      X[q + 16s] = sum_t W8^{ts} W128^{tq} sum_m W16^{mq} x[t + 8m],
+//    i.e. a 16-point DFT in registers, a twiddle, one exchange inside the 8-thread group (shared memory, __syncwarp
+//    only) and two 8-point DFTs in registers.  The inverse runs the same steps mirrored with conjugate twiddles.
+//  * The spectrum is never put back in natural order: the projection is pointwise, so each thread projects the 16
+//    frequencies it holds and the inverse starts from the same registers.  The amplitudes are stored once per plan
+//    in that register order ([position][column][t][parity][s]), so each thread reads 64 contiguous bytes.
+//  * Shared memory holds one 128 x 132 complex64 tile (pitch 132: row-major float4 writes and 8-row column reads
+//    are free of bank conflicts); the group exchanges use a rotated slot order for the same reason.
+//  * The squared residual is summed per warp and written as 32 FP64 partials per position (reduced in a fixed order
+//    by the error kernel): no atomics, bitwise reproducible.
+#include "engine.h"
+
+namespace cubo {
+
+namespace {
+
+constexpr int kN = 128;          // detector side
+constexpr int kPitch = 132;      // shared-memory row pitch (complex64)
+constexpr int kThreads = 1024;
+
+__device__ __forceinline__ float2 fm(float2 a, float2 b) { return make_float2(a.x * b.x - a.y * b.y, a.x * b.y + a.y * b.x); }
+__device__ __forceinline__ float2 fmc(float2 a, float2 b) {  // a * conj(b)
+    return make_float2(a.x * b.x + a.y * b.y, a.y * b.x - a.x * b.y);
+}
+__device__ __forceinline__ float2 fadd(float2 a, float2 b) { return make_float2(a.x + b.x, a.y + b.y); }
+__device__ __forceinline__ float2 fsub(float2 a, float2 b) { return make_float2(a.x - b.x, a.y - b.y); }
+
+template <bool INV>
+__device__ __forceinline__ float2 mul_mi(float2 a) {  // * (-i) forward, * (+i) inverse
+    return INV ? make_float2(-a.y, a.x) : make_float2(a.y, -a.x);
+}
+
+template <bool INV>
+__device__ __forceinline__ void f4(float2 &x0, float2 &x1, float2 &x2, float2 &x3) {
+    const float2 t0 = fadd(x0, x2), t1 = fsub(x0, x2), t2 = fadd(x1, x3), t3 = mul_mi<INV>(fsub(x1, x3));
+    x0 = fadd(t0, t2); x2 = fsub(t0, t2); x1 = fadd(t1, t3); x3 = fsub(t1, t3);
+}
+
+// W16^k (forward e^{-2 pi i k / 16}); cos(pi/8), sin(pi/8), cos(pi/4) written out.
+template <bool INV, int K>
+__device__ __forceinline__ float2 tw16(float2 a) {
+    constexpr float c1 = 0.92387953251128675613f, s1 = 0.38268343236508977173f, h = 0.70710678118654752440f;
+    constexpr float sg = INV ? 1.f : -1.f;  // sign of the imaginary part of the twiddle
+    if (K == 0) return a;
+    if (K == 1) return fm(a, make_float2(c1, sg * s1));
+    if (K == 2) return make_float2(h * (a.x - sg * a.y), h * (a.y + sg * a.x));
+    if (K == 3) return fm(a, make_float2(s1, sg * c1));
+    if (K == 4) return mul_mi<INV>(a);
+    if (K == 6) return make_float2(h * (-a.x - sg * a.y), h * (-a.y + sg * a.x));
+    if (K == 9) return fm(a, make_float2(-c1, -sg * s1));
+    return a;
+}
+
+// 16-point DFT in registers, natural order in and out (4 x 4 with W16 twiddles).
+template <bool INV>
+__device__ __forceinline__ void dft16(float2 (&x)[16]) {
+#pragma unroll
+    for (int b = 0; b < 4; b++) f4<INV>(x[b], x[4 + b], x[8 + b], x[12 + b]);  // x[4c + b] = y_b[c]
+    x[5] = tw16<INV, 1>(x[5]); x[9] = tw16<INV, 2>(x[9]); x[13] = tw16<INV, 3>(x[13]);
+    x[6] = tw16<INV, 2>(x[6]); x[10] = tw16<INV, 4>(x[10]); x[14] = tw16<INV, 6>(x[14]);
+    x[7] = tw16<INV, 3>(x[7]); x[11] = tw16<INV, 6>(x[11]); x[15] = tw16<INV, 9>(x[15]);
+#pragma unroll
+    for (int c = 0; c < 4; c++) f4<INV>(x[4 * c], x[4 * c + 1], x[4 * c + 2], x[4 * c + 3]);  // x[4c + d] = X[c + 4d]
+    float2 y[16];
+#pragma unroll
+    for (int q = 0; q < 16; q++) y[q] = x[4 * (q & 3) + (q >> 2)];
+#pragma unroll
+    for (int q = 0; q < 16; q++) x[q] = y[q];
+}
+
+// 8-point DFT in registers, natural order in and out.
+template <bool INV>
+__device__ __forceinline__ void dft8(float2 (&v)[8]) {
+    float2 e0 = v[0], e1 = v[2], e2 = v[4], e3 = v[6], o0 = v[1], o1 = v[3], o2 = v[5], o3 = v[7];
+    f4<INV>(e0, e1, e2, e3);
+    f4<INV>(o0, o1, o2, o3);
+    o1 = tw16<INV, 2>(o1);
+    o2 = mul_mi<INV>(o2);
+    o3 = tw16<INV, 6>(o3);
+    v[0] = fadd(e0, o0); v[4] = fsub(e0, o0);
+    v[1] = fadd(e1, o1); v[5] = fsub(e1, o1);
+    v[2] = fadd(e2, o2); v[6] = fsub(e2, o2);
+    v[3] = fadd(e3, o3); v[7] = fsub(e3, o3);
+}
+
+// Group exchange, forward direction: thread t holds x[q] = Y[t][q] (q = 0..15); afterwards u0[t'] = Y[t'][2t],
+// u1[t'] = Y[t'][2t + 1].  Slot of Y[t][q]: t * 16 + ((q + 2t) & 15), so both the float4 writes and reads of the 8
+// threads cover all 32 banks.
+__device__ __forceinline__ void exchange_fwd(float2 *base, const float2 (&x)[16], int t, float2 (&u0)[8], float2 (&u1)[8]) {
+#pragma unroll
+    for (int j = 0; j < 8; j++)
+        *reinterpret_cast<float4 *>(base + t * 16 + ((2 * j + 2 * t) & 15)) = make_float4(x[2 * j].x, x[2 * j].y, x[2 * j + 1].x, x[2 * j + 1].y);
+    __syncwarp();
+#pragma unroll
+    for (int s = 0; s < 8; s++) {
+        const float4 v = *reinterpret_cast<const float4 *>(base + s * 16 + ((2 * t + 2 * s) & 15));
+        u0[s] = make_float2(v.x, v.y);
+        u1[s] = make_float2(v.z, v.w);
+    }
+    __syncwarp();
+}
+
+// Inverse direction: thread t holds u0[t'] = Z[t'][2t], u1[t'] = Z[t'][2t + 1]; afterwards x[q] = Z[t][q].
+__device__ __forceinline__ void exchange_inv(float2 *base, const float2 (&u0)[8], const float2 (&u1)[8], int t, float2 (&x)[16]) {
+#pragma unroll
+    for (int s = 0; s < 8; s++)
+        *reinterpret_cast<float4 *>(base + s * 16 + ((2 * t + 2 * s) & 15)) = make_float4(u0[s].x, u0[s].y, u1[s].x, u1[s].y);
+    __syncwarp();
+#pragma unroll
+    for (int j = 0; j < 8; j++) {
+        const float4 v = *reinterpret_cast<const float4 *>(base + t * 16 + ((2 * j + 2 * t) & 15));
+        x[2 * j] = make_float2(v.x, v.y);
+        x[2 * j + 1] = make_float2(v.z, v.w);
+    }
+    __syncwarp();
+}
+
+// Forward line transform of the 16 samples x[m] = line[t + 8m]: on return u0[s] = X[2t + 16s], u1[s] = X[2t+1+16s].
+__device__ __forceinline__ void line_forward(float2 (&x)[16], int t, const float2 *tw, float2 *scratch, float2 (&u0)[8], float2 (&u1)[8]) {
+    dft16<false>(x);
+#pragma unroll
+    for (int q = 1; q < 16; q++) x[q] = fm(x[q], tw[(t * q) & 127]);
+    exchange_fwd(scratch, x, t, u0, u1);
+    dft8<false>(u0);
+    dft8<false>(u1);
+}
+
+// Inverse of line_forward (unnormalised): from u0/u1 as line_forward leaves them, x[m] = line[t + 8m].
+__device__ __forceinline__ void line_inverse(float2 (&u0)[8], float2 (&u1)[8], int t, const float2 *tw, float2 *scratch, float2 (&x)[16]) {
+    dft8<true>(u0);
+    dft8<true>(u1);
+    // u0[t'] = G[t'][2t], u1[t'] = G[t'][2t+1]; twiddle by conj(W128^{t' q})
+#pragma unroll
+    for (int s = 1; s < 8; s++) {
+        u0[s] = fmc(u0[s], tw[(s * 2 * t) & 127]);
+        u1[s] = fmc(u1[s], tw[(s * (2 * t + 1)) & 127]);
+    }
+    exchange_inv(scratch, u0, u1, t, x);
+    dft16<true>(x);
+}
+
+__device__ __forceinline__ int wrap_once(int v, int size) { return v < 0 ? v + size : (v >= size ? v - size : v); }
+
+__global__ void __launch_bounds__(kThreads, 1) fast128_kernel(Fast128Args a) {
+    extern __shared__ __align__(16) float2 sm[];
+    float2 *tw = sm + kN * kPitch;
+    const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+    const int g = warp * 4 + (lane >> 3);  // the line this 8-thread group owns
+    const int t = lane & 7;
+    for (int i = tid; i < kN; i += kThreads) tw[i] = a.tw128[i];
+    __syncthreads();
+    float2 *line = sm + g * kPitch;  // row g: the group's own region
+    const float inv_n = 1.0f / (float)(kN * kN);
+    for (int p = a.first + blockIdx.x; p < a.first + a.count; p += gridDim.x) {
+        const int rr = a.scan.rr[p], cc = a.scan.cc[p], cls = a.scan.cls[p];
+        const float2 *S = a.shifted + (size_t)cls * (kN * kN) + g * kN;
+        const float2 *orow = a.object + (size_t)wrap_once(rr + (g < kN / 2 ? g : g - kN), a.object_rows) * a.object_columns;
+        float2 x[16], u0[8], u1[8];
+        // exit wave, row g, columns t + 8m (Ptychography.swift:321-336)
+#pragma unroll
+        for (int m = 0; m < 16; m++) {
+            const int c = t + 8 * m;
+            const int xc = wrap_once(cc + (c < kN / 2 ? c : c - kN), a.object_columns);
+            x[m] = fm(S[c], orow[xc]);
+        }
+        // row pass
+        line_forward(x, t, tw, line, u0, u1);
+#pragma unroll
+        for (int s = 0; s < 8; s++)
+            *reinterpret_cast<float4 *>(line + 2 * t + 16 * s) = make_float4(u0[s].x, u0[s].y, u1[s].x, u1[s].y);
+        __syncthreads();
+        // column pass: column g, rows t + 8m
+#pragma unroll
+        for (int m = 0; m < 16; m++) x[m] = sm[(t + 8 * m) * kPitch + g];
+        __syncthreads();
+        line_forward(x, t, tw, line, u0, u1);
+        // projection (Ptychography.swift:338-349); this thread holds F[2t + parity + 16s][g]
+        const float4 *A = reinterpret_cast<const float4 *>(a.amplitudes + ((size_t)p * kN + g) * kN + t * 16);
+        double err = 0;
+#pragma unroll
+        for (int h = 0; h < 4; h++) {
+            const float4 av = A[h];
+            const float am[4] = {av.x, av.y, av.z, av.w};
+#pragma unroll
+            for (int e = 0; e < 4; e++) {
+                const int j = h * 4 + e;       // j = parity * 8 + s
+                float2 &f = (j < 8) ? u0[j] : u1[j - 8];
+                const float mag = sqrtf(f.x * f.x + f.y * f.y);
+                const float miss = am[e] - mag;
+                err += (double)(miss * miss);
+                if (mag > 0.f) {
+                    const float sc = (am[e] / mag - 1.0f) * inv_n;
+                    f = make_float2(f.x * sc, f.y * sc);
+                } else {
+                    f = make_float2(am[e] * inv_n, 0.f);
+                }
+            }
+        }
+#pragma unroll
+        for (int o = 16; o > 0; o >>= 1) err += __shfl_down_sync(0xffffffffu, err, o);
+        if (lane == 0) a.error[(size_t)p * 32 + warp] = err;
+        // inverse column pass
+        line_inverse(u0, u1, t, tw, line, x);
+        __syncthreads();  // every group is done with its scratch row before the columns are written back
+#pragma unroll
+        for (int m = 0; m < 16; m++) sm[(t + 8 * m) * kPitch + g] = x[m];
+        __syncthreads();
+        // inverse row pass from the row-pass layout
+#pragma unroll
+        for (int s = 0; s < 8; s++) {
+            const float4 v = *reinterpret_cast<const float4 *>(line + 2 * t + 16 * s);
+            u0[s] = make_float2(v.x, v.y);
+            u1[s] = make_float2(v.z, v.w);
+        }
+        __syncwarp();
+        line_inverse(u0, u1, t, tw, line, x);
+        float2 *out = a.dpsi + (size_t)p * (kN * kN) + g * kN;
+#pragma unroll
+        for (int m = 0; m < 16; m++) out[t + 8 * m] = x[m];
+    }
+}
+
+// [position][row][column] -> [position][column][t][parity][s] with row = 2t + parity + 16s.
+__global__ void permute_amplitudes_kernel(const float *in, float *out, long long positions) {
+    const long long i = (long long)blockIdx.x * 256 + threadIdx.x;
+    if (i >= positions * kN * kN) return;
+    const long long p = i / (kN * kN);
+    const int rem = (int)(i - p * kN * kN);
+    const int column = rem >> 7, t = (rem >> 4) & 7, j = rem & 15;
+    const int row = 2 * t + (j >> 3) + 16 * (j & 7);
+    out[i] = in[p * kN * kN + row * kN + column];
+}
+
+}  // namespace
+
+bool fast128_applicable(int rows, int columns) { return rows == kN && columns == kN; }
+
+size_t fast128_smem() { return (size_t)(kN * kPitch + kN) * sizeof(float2); }
+
+cudaError_t configure_fast128() {
+    int device = 0, optin = 0;
+    cudaError_t e = cudaGetDevice(&device);
+    if (e != cudaSuccess) return e;
+    e = cudaDeviceGetAttribute(&optin, cudaDevAttrMaxSharedMemoryPerBlockOptin, device);
+    if (e != cudaSuccess) return e;
+    if ((size_t)optin < fast128_smem()) return cudaErrorInvalidValue;
+    return cudaFuncSetAttribute(fast128_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)fast128_smem());
+}
+
+cudaError_t launch_fast128(const Fast128Args &a, int ctas, cudaStream_t s) {
+    if (a.count <= 0) return cudaSuccess;
+    const int grid = a.count < ctas ? a.count : ctas;
+    fast128_kernel<<<grid, kThreads, fast128_smem(), s>>>(a);
+    return cudaGetLastError();
+}
+
+cudaError_t launch_permute_amplitudes(const float *in, float *out, long long positions, cudaStream_t s) {
+    const long long total = positions * kN * kN;
+    permute_amplitudes_kernel<<<(unsigned)((total + 255) / 256), 256, 0, s>>>(in, out, positions);
+    return cudaGetLastError();
+}
+
+}  // namespace cubo

@@ -99,6 +99,9 @@ struct cubo_ptycho_plan {
     int groups = 1;         // probe-gather position groups
     int tiles_x = 0, tiles = 0;
     int probe_blocks = 0;
+    bool fast = false;      // 128 x 128 FP32 register-resident position pass
+    int sms = 148;
+    long long error_count = 0;  // residual partials summed by the error kernel
     long long iterations_done = 0;
     long long errors_capacity = 0;
     long long launches = 0;
@@ -288,17 +291,26 @@ void build_plan(cubo_ptycho_plan *p, const cubo_ptycho_problem *pr) {
     }
     upload(p->tile_start, counts, s);
     upload(p->tile_list, list, s);
-    // ---- amplitudes (Float32, [position][row][column])
+    // ---- amplitudes (Float32, [position][row][column]; the 128 x 128 kernel's register order when it runs)
     check(p->amplitudes.alloc((size_t)P * n * sizeof(float)), "cudaMalloc amplitudes");
     check(cudaMemcpyAsync(p->amplitudes.ptr, pr->amplitudes, (size_t)P * n * sizeof(float), cudaMemcpyHostToDevice, s),
           "upload amplitudes");
+    if (p->fast) {
+        DeviceBuffer permuted;
+        check(permuted.alloc((size_t)P * n * sizeof(float)), "cudaMalloc amplitudes");
+        check(launch_permute_amplitudes(p->amplitudes.as<float>(), permuted.as<float>(), P, s), "permute amplitudes");
+        check(cudaStreamSynchronize(s), "permute amplitudes");
+        std::swap(p->amplitudes.ptr, permuted.ptr);
+        std::swap(p->amplitudes.bytes, permuted.bytes);
+    }
     // ---- state and work buffers
     check(p->object.alloc((size_t)p->objects * sizeof(C2<T>)), "cudaMalloc object");
     check(p->grad_o.alloc((size_t)p->objects * sizeof(C2<T>)), "cudaMalloc");
     check(p->weight_o.alloc((size_t)p->objects * sizeof(T)), "cudaMalloc");
     check(p->tile_max.alloc((size_t)p->tiles * sizeof(double)), "cudaMalloc");
     check(p->dpsi.alloc((size_t)P * n * sizeof(C2<T>)), "cudaMalloc dpsi");
-    check(p->error.alloc((size_t)P * sizeof(double)), "cudaMalloc");
+    p->error_count = p->fast ? (long long)P * 32 : P;
+    check(p->error.alloc((size_t)p->error_count * sizeof(double)), "cudaMalloc");
     check(p->iteration.alloc(sizeof(int)), "cudaMalloc");
     check(cudaMemsetAsync(p->iteration.ptr, 0, sizeof(int), s), "memset");
     check(p->probe64.alloc((size_t)n * sizeof(double2)), "cudaMalloc");
@@ -455,7 +467,16 @@ void enqueue_iteration(cubo_ptycho_plan *p) {
     pa.amplitudes = p->amplitudes.as<float>(); pa.dpsi = p->dpsi.as<C2<T>>(); pa.error = p->error.as<double>();
     pa.tw_rows = p->tw_r.as<C2<T>>(); pa.tw_columns = p->tw_c.as<C2<T>>();
     pa.rad_rows = p->rad_rows; pa.rad_columns = p->rad_columns; pa.inv_n = (T)(1.0 / n);
-    timed(p, kPositionPass, 1, [&] { return launch_position_pass<T>(pa, s); });
+    if (p->fast) {
+        Fast128Args fa{};
+        fa.object_rows = p->OR; fa.object_columns = p->OC; fa.first = 0; fa.count = p->P; fa.scan = scan;
+        fa.shifted = p->shifted.as<float2>(); fa.object = p->object.as<float2>();
+        fa.amplitudes = p->amplitudes.as<float>(); fa.dpsi = p->dpsi.as<float2>(); fa.error = p->error.as<double>();
+        fa.tw128 = p->tw_r.as<float2>();
+        timed(p, kPositionPass, 1, [&] { return launch_fast128(fa, p->sms, s); });
+    } else {
+        timed(p, kPositionPass, 1, [&] { return launch_position_pass<T>(pa, s); });
+    }
 
     ObjectGatherArgs<T> ga{};
     ga.rows = p->R; ga.columns = p->C; ga.object_rows = p->OR; ga.object_columns = p->OC; ga.n = n;
@@ -487,7 +508,7 @@ void enqueue_iteration(cubo_ptycho_plan *p) {
     });
     enqueue_probe_side(p);
     timed(p, kErrorReduce, 1, [&] {
-        return launch_error_reduce(p->error.as<double>(), p->P, p->divisor, p->errors.as<double>(),
+        return launch_error_reduce(p->error.as<double>(), (int)p->error_count, p->divisor, p->errors.as<double>(),
                                    p->iteration.as<int>(), s);
     });
 }
@@ -611,6 +632,9 @@ int cubo_ptycho_plan_create(cubo_ptycho_context *ctx, const cubo_ptycho_problem 
         if (position_pass_smem(p->n, p->R, p->C, p->fp64) > (size_t)optin)
             fail(CUBO_PTYCHO_UNSUPPORTED, "detector too large for shared memory");
         check(configure_kernels(), "configure kernels");
+        p->fast = !p->fp64 && pp->variant != CUBO_PTYCHO_VARIANT_GENERIC && fast128_applicable(p->R, p->C);
+        if (p->fast) check(configure_fast128(), "configure 128 x 128 kernel");
+        check(cudaDeviceGetAttribute(&p->sms, cudaDevAttrMultiProcessorCount, ctx->device), "attribute");
         p->kind_ms.assign(kKinds, 0.0);
         p->kind_launches.assign(kKinds, 0);
         if (p->fp64) build_plan<double>(p, pr);

@@ -121,7 +121,8 @@ class _Inputs:
     def __init__(self, amplitudes, positions, object_shape, probe_shape, iterations, step_size, normalization_minimum,
                  fix_probe, pure_phase_object, constrain_object_amplitude, fix_probe_center_of_mass,
                  constrain_probe_amplitude, probe_amplitude_relative_radius, probe_amplitude_relative_width,
-                 fix_probe_aperture, probe_support_mask, error_normalization, position_correction, precision):
+                 fix_probe_aperture, probe_support_mask, error_normalization, position_correction, precision,
+                 variant="auto"):
         rows, columns = probe_shape
         positions = np.asarray(positions, np.float64).reshape(-1, 2) if np.size(positions) else np.zeros((0, 2))
         count = len(positions)
@@ -167,6 +168,9 @@ class _Inputs:
         if precision not in FORMS:
             raise PtychographyError(f"precision {precision!r}")
         p.form = FORMS[precision]
+        if variant not in ("auto", "generic"):
+            raise PtychographyError(f"variant {variant!r}")
+        p.variant = L.VARIANT_GENERIC if variant == "generic" else L.VARIANT_AUTO
         self.cancel_flag = C.c_int(0)
         self.count = count
 
@@ -185,7 +189,8 @@ class SingleslicePtychography:
                     probe_support_mask=None, error_normalization="suppliedAmplitudeEnergy",
                     position_correction=None, precision: str = "fp32",
                     is_cancelled: Optional[Callable[[], bool]] = None,
-                    progress: Optional[Callable[[int, int], None]] = None, device: int = 0) -> Result:
+                    progress: Optional[Callable[[int, int], None]] = None, device: int = 0,
+                    variant: str = "auto") -> Result:
         """Reconstructs from corner-centred amplitudes ``[position][row][column]``; see ``include/cubo_ptycho.h``.
 
         ``object`` and ``probe`` are complex 2-D arrays (``PtychographyArray``); ``positions`` is ``(P, 2)`` rows and
@@ -202,7 +207,8 @@ class SingleslicePtychography:
         inp = _Inputs(amplitudes, positions, obj.shape, prb.shape, iterations, step_size, normalization_minimum,
                       fix_probe, pure_phase_object, constrain_object_amplitude, fix_probe_center_of_mass,
                       constrain_probe_amplitude, probe_amplitude_relative_radius, probe_amplitude_relative_width,
-                      fix_probe_aperture, probe_support_mask, error_normalization, position_correction, precision)
+                      fix_probe_aperture, probe_support_mask, error_normalization, position_correction, precision,
+                      variant)
         if is_cancelled is not None and is_cancelled():
             raise CancellationError("cancelled")
         cb = None
@@ -235,7 +241,8 @@ class Plan:
                         pure_phase_object=False, constrain_object_amplitude=True, fix_probe_center_of_mass=False,
                         constrain_probe_amplitude=False, probe_amplitude_relative_radius=0.5,
                         probe_amplitude_relative_width=0.05, fix_probe_aperture=False, probe_support_mask=None,
-                        error_normalization="suppliedAmplitudeEnergy", position_correction=None, precision="fp32")
+                        error_normalization="suppliedAmplitudeEnergy", position_correction=None, precision="fp32",
+                        variant="auto")
         defaults.update(kwargs)
         self.inputs = _Inputs(amplitudes, positions, tuple(object_shape), tuple(probe_shape), **defaults)
         self.object_shape = tuple(object_shape)

@@ -100,7 +100,12 @@ typedef struct {
     /* progress(completed, total) after each iteration, on the calling thread.  NULL: none. */
     cubo_ptycho_progress_fn progress;
     void *progress_user;
+    /* Kernel choice: CUBO_PTYCHO_VARIANT_AUTO picks the specialised kernel for the detector size when there is one;
+     * CUBO_PTYCHO_VARIANT_GENERIC forces the any-size shared-memory transform (for cross-checks). */
+    int variant;
 } cubo_ptycho_params;
+
+enum { CUBO_PTYCHO_VARIANT_AUTO = 0, CUBO_PTYCHO_VARIANT_GENERIC = 1 };
 
 /* Replaces the default arguments of SingleslicePtychography.reconstruct (Ptychography.swift:220-232). */
 CUBO_PTYCHO_API void cubo_ptycho_params_default(cubo_ptycho_params *params);

@@ -187,3 +187,23 @@ def test_fixed_probe_is_returned_unchanged(cb):
     r = _gpu(cb, case, "fp32", fix_probe=True, fix_probe_center_of_mass=True, constrain_probe_amplitude=True,
              probe_amplitude_relative_radius=0.3, probe_amplitude_relative_width=0.1)
     assert np.array_equal(r.probe, case.probe)
+
+
+@pytest.mark.parametrize("fractional", [False, True])
+def test_fast128_against_generic_and_oracle(cb, fractional):
+    """The 128 x 128 register-resident kernel against the any-size kernel and the FP64 oracle."""
+    if fractional:
+        s = scenes.nonsquare_scene(128, 128, 300)
+    else:
+        s = scenes.raster_scene(scan=3, det=128, step=4, seed=9)
+    ref = c_oracle.reconstruct(s["amplitudes"].astype(np.float32), s["positions"], s["object"], s["probe"],
+                               iterations=3)
+    fast = cb.SingleslicePtychography.reconstruct(s["amplitudes"], s["positions"], s["object"], s["probe"],
+                                                  iterations=3)
+    gen = cb.SingleslicePtychography.reconstruct(s["amplitudes"], s["positions"], s["object"], s["probe"],
+                                                 iterations=3, variant="generic")
+    for r in (fast, gen):
+        assert np.max(np.abs(r.object - ref[0])) <= 1e-4
+        assert np.max(np.abs(r.probe - ref[1])) <= 1e-5 * max(1.0, np.max(np.abs(ref[1])))
+        assert np.all(np.abs(r.errors - ref[2]) <= 1e-5 * ref[2])
+    assert np.max(np.abs(fast.object - gen.object)) <= 2e-5
