@@ -163,6 +163,26 @@ CUBO_PTYCHO_API int cubo_ptycho_probe_build(cubo_ptycho_context *context, int ro
                             double astigmatism, double astigmatism_angle, double spherical_aberration, int term_count,
                             const double *terms, double *re, double *im);
 
+/* ---- Loss without allocating.  No counterpart in the reference: CuboPtycho computes on the CPU and never allocates
+ * device memory.  For callers that cannot call cudaMalloc: a host application whose device memory belongs to its own
+ * pool allocator, or a latency-critical loop that must not allocate (cudaMalloc can synchronise the device).
+ * Computes loss[0] = sum over positions and detector pixels of (A - |fft2(P * O[patch])|)^2 in FP32 with FP64 sums
+ * (the squared amplitude residual of Ptychography.swift:338-342, before any normalisation) for integer scan centres.
+ * All pointers are the caller's device memory: amplitudes (count * rows * columns floats, [position][row][column]),
+ * centre_rows / centre_columns (count ints, the rounded scan centres; wrapped periodically), object and probe as
+ * interleaved complex64 (2 floats per sample, row-major), loss (one double).  Enqueued on `stream` (a cudaStream_t,
+ * NULL = the default stream); returns without waiting.  Allocates nothing: the per-position scratch is a fixed device
+ * array of CUBO_PTYCHO_NOALLOC_MAX_POSITIONS doubles inside the library, held on every GPU that loads it until the
+ * process exits; count above that maximum is refused with CUBO_PTYCHO_INVALID_INPUT, detectors above 128 x 128 pixels
+ * with CUBO_PTYCHO_UNSUPPORTED.  The first call on a device resolves that array's device address (set-up done once per
+ * device, with the device current); make that first call before any stream capture.  Every call shares the array, so
+ * calls that overlap on the GPU race: order them on one stream. */
+#define CUBO_PTYCHO_NOALLOC_MAX_POSITIONS (1 << 20)
+CUBO_PTYCHO_API int cubo_ptycho_loss_fp32_noalloc(int rows, int columns, int object_rows, int object_columns, int count,
+                                                  const float *amplitudes, const int *centre_rows,
+                                                  const int *centre_columns, const float *object, const float *probe,
+                                                  double *loss, void *stream);
+
 #ifdef __cplusplus
 }
 #endif
