@@ -64,10 +64,11 @@ struct Fast128Args {
     const float2 *object;
     const float *amplitudes;   // [positions][column][t][parity][s]
     float2 *dpsi;              // [positions][row][column]
-    double *error;             // [positions][32]
+    double *error;             // [positions][fast128_partials_per_position()]
     const float2 *tw128;       // W_128^t
 };
 bool fast128_applicable(int rows, int columns);
+int fast128_partials_per_position();
 size_t fast128_smem();
 cudaError_t configure_fast128();
 cudaError_t launch_fast128(const Fast128Args &a, int ctas, cudaStream_t s);
@@ -87,8 +88,10 @@ cudaError_t launch_max_reduce(const double *values, int count, double *out, cuda
 template <typename T>
 cudaError_t launch_object_update(C2<T> *object, const C2<T> *grad, const T *weight, int count, const double *max_weight,
                                  double step, double minimum, int cap, int pure_phase, cudaStream_t s);
-cudaError_t launch_error_reduce(const double *error, int count, double divisor, double *errors, int *iteration,
-                                cudaStream_t s);
+// Fixed-order FP64 sum of error[0, count) divided by `divisor` into errors[*iteration], then ++*iteration.
+cudaError_t launch_error_reduce(const double *error, long long count, double divisor, double *errors, int *iteration,
+                                double *scratch, cudaStream_t s);
+int error_reduce_scratch();  // doubles of scratch launch_error_reduce needs
 bool position_pass_supported(int n, bool fp64);
 size_t position_pass_smem(int n, int rows, int columns, bool fp64);
 

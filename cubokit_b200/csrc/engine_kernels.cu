@@ -139,20 +139,37 @@ __global__ void __launch_bounds__(kGatherThreads) object_gather_kernel(ObjectGat
         }
         __syncthreads();
         if (inside) {
-            for (int i = 0; i < cnt; i++) {
-                int dy = y - s_rr[i];
-                if (dy < 0) dy += a.object_rows;
-                const int kr = window_index(dy, a.rows, a.object_rows);
-                if (kr < 0) continue;
-                int dx = x - s_cc[i];
-                if (dx < 0) dx += a.object_columns;
-                const int kc = window_index(dx, a.columns, a.object_columns);
-                if (kc < 0) continue;
-                const int k = kr * a.columns + kc;
-                const C2<T> d = a.dpsi[(size_t)s_p[i] * a.n + k];
-                const C2<T> s = a.shifted[(size_t)s_cls[i] * a.n + k];
-                g = cadd(g, cmulc(s, d));
-                w += s.x * s.x + s.y * s.y;
+            // four candidates at a time: their loads are independent, the sums stay in candidate order
+            for (int i = 0; i < cnt; i += 4) {
+                int k[4];
+#pragma unroll
+                for (int u = 0; u < 4; u++) {
+                    k[u] = -1;
+                    if (i + u < cnt) {
+                        int dy = y - s_rr[i + u];
+                        if (dy < 0) dy += a.object_rows;
+                        const int kr = window_index(dy, a.rows, a.object_rows);
+                        int dx = x - s_cc[i + u];
+                        if (dx < 0) dx += a.object_columns;
+                        const int kc = window_index(dx, a.columns, a.object_columns);
+                        if (kr >= 0 && kc >= 0) k[u] = kr * a.columns + kc;
+                    }
+                }
+                C2<T> d[4], sv[4];
+#pragma unroll
+                for (int u = 0; u < 4; u++) {
+                    if (k[u] >= 0) {
+                        d[u] = a.dpsi[(size_t)s_p[i + u] * a.n + k[u]];
+                        sv[u] = a.shifted[(size_t)s_cls[i + u] * a.n + k[u]];
+                    }
+                }
+#pragma unroll
+                for (int u = 0; u < 4; u++) {
+                    if (k[u] >= 0) {
+                        g = cadd(g, cmulc(sv[u], d[u]));
+                        w += sv[u].x * sv[u].x + sv[u].y * sv[u].y;
+                    }
+                }
             }
         }
     }
@@ -186,13 +203,25 @@ __global__ void __launch_bounds__(kProbeThreads) probe_gather_kernel(ProbeGather
         for (int i = threadIdx.x; i < cnt; i += kProbeThreads) { s_rr[i] = a.scan.rr[base + i]; s_cc[i] = a.scan.cc[base + i]; }
         __syncthreads();
         if (valid) {
-            for (int i = 0; i < cnt; i++) {
-                const int y = wrap_once(s_rr[i] + offr, a.object_rows);
-                const int x = wrap_once(s_cc[i] + offc, a.object_columns);
-                const C2<T> o = a.object[(size_t)y * a.object_columns + x];
-                const C2<T> d = a.dpsi[(size_t)(base + i) * a.n + k];
-                g = cadd(g, cmulc(o, d));
-                w += o.x * o.x + o.y * o.y;
+            // four positions at a time: independent loads, sums in position order
+            for (int i = 0; i < cnt; i += 4) {
+                C2<T> o[4], d[4];
+#pragma unroll
+                for (int u = 0; u < 4; u++) {
+                    if (i + u < cnt) {
+                        const int y = wrap_once(s_rr[i + u] + offr, a.object_rows);
+                        const int x = wrap_once(s_cc[i + u] + offc, a.object_columns);
+                        o[u] = a.object[(size_t)y * a.object_columns + x];
+                        d[u] = a.dpsi[(size_t)(base + i + u) * a.n + k];
+                    }
+                }
+#pragma unroll
+                for (int u = 0; u < 4; u++) {
+                    if (i + u < cnt) {
+                        g = cadd(g, cmulc(o[u], d[u]));
+                        w += o[u].x * o[u].x + o[u].y * o[u].y;
+                    }
+                }
             }
         }
     }
@@ -249,14 +278,23 @@ __global__ void __launch_bounds__(256) object_update_kernel(C2<T> *object, const
     object[j] = o;
 }
 
-__global__ void __launch_bounds__(1024) error_reduce_kernel(const double *error, int count, double divisor,
-                                                            double *errors, int *iteration) {
+constexpr int kErrorBlocks = 256;
+
+// Stage 1: block b sums the fixed slice [b*count/B, (b+1)*count/B) (thread t takes every 1024th element of it, then a
+// fixed tree); stage 2 sums the B block sums in order.  No atomics: the same inputs give the same bits.
+__global__ void __launch_bounds__(1024) error_partial_kernel(const double *error, long long count, double *block_sums) {
     __shared__ double scratch[32];
-    // thread t sums the contiguous slice [t*count/1024, (t+1)*count/1024) in order, then a fixed tree
-    const long long b = (long long)count * threadIdx.x / 1024, e = (long long)count * (threadIdx.x + 1) / 1024;
+    const long long b = count * blockIdx.x / kErrorBlocks, e = count * (blockIdx.x + 1) / kErrorBlocks;
     double s = 0;
-    for (long long i = b; i < e; i++) s += error[i];
+    for (long long i = b + threadIdx.x; i < e; i += 1024) s += error[i];
     s = block_sum<1024>(s, scratch);
+    if (threadIdx.x == 0) block_sums[blockIdx.x] = s;
+}
+
+__global__ void __launch_bounds__(kErrorBlocks) error_final_kernel(const double *block_sums, double divisor,
+                                                                  double *errors, int *iteration) {
+    __shared__ double scratch[32];
+    const double s = block_sum<kErrorBlocks>(block_sums[threadIdx.x], scratch);
     if (threadIdx.x == 0) {
         const int it = *iteration;
         errors[it] = s / divisor;
@@ -335,9 +373,14 @@ cudaError_t launch_object_update(C2<T> *object, const C2<T> *grad, const T *weig
     return cudaGetLastError();
 }
 
-cudaError_t launch_error_reduce(const double *error, int count, double divisor, double *errors, int *iteration,
-                                cudaStream_t s) {
-    error_reduce_kernel<<<1, 1024, 0, s>>>(error, count, divisor, errors, iteration);
+int error_reduce_scratch() { return kErrorBlocks; }
+
+cudaError_t launch_error_reduce(const double *error, long long count, double divisor, double *errors, int *iteration,
+                                double *scratch, cudaStream_t s) {
+    error_partial_kernel<<<kErrorBlocks, 1024, 0, s>>>(error, count, scratch);
+    cudaError_t e = cudaGetLastError();
+    if (e != cudaSuccess) return e;
+    error_final_kernel<<<1, kErrorBlocks, 0, s>>>(scratch, divisor, errors, iteration);
     return cudaGetLastError();
 }
 

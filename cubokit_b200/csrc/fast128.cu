@@ -3,8 +3,9 @@
 // Same arithmetic as the generic position pass (exit wave, forward 2-D FFT, Fourier-modulus projection with the 1/n of
 // ifft2 folded in, inverse 2-D FFT; Ptychography.swift:321-350), laid out for the hardware:
 //
-//  * Persistent CTAs of 1024 threads (one per SM) walk the positions in a fixed stride; 8-thread groups own one line
-//    (a row in the row pass, a column in the column pass); each thread holds 16 complex samples in registers.
+//  * Persistent CTAs of 512 threads (one per SM) walk the positions in a fixed stride; each 8-thread group owns two
+//    lines (rows g and g + 64 in the row pass, columns in the column pass) and each thread holds 2 x 16 complex
+//    samples in registers, so every phase has two independent instruction streams and nothing spills.
 //  * A 128-point line transform is 128 = 16 x 8 (four-step): with c = t + 8m and k = q + 16s,
 //      X[q + 16s] = sum_t W8^{ts} W128^{tq} sum_m W16^{mq} x[t + 8m],
 //    i.e. a 16-point DFT in registers, a twiddle, one exchange inside the 8-thread group (shared memory, __syncwarp
@@ -14,8 +15,8 @@
 //    in that register order ([position][column][t][parity][s]), so each thread reads 64 contiguous bytes.
 //  * Shared memory holds one 128 x 132 complex64 tile (pitch 132: row-major float4 writes and 8-row column reads
 //    are free of bank conflicts); the group exchanges use a rotated slot order for the same reason.
-//  * The squared residual is summed per warp and written as 32 FP64 partials per position (reduced in a fixed order
-//    by the error kernel): no atomics, bitwise reproducible.
+//  * The squared residual is summed per warp and written as 16 FP64 partials per position (reduced in a fixed order
+//    by the error kernels): no atomics, bitwise reproducible.
 #include "engine.h"
 
 namespace cubo {
@@ -24,7 +25,9 @@ namespace {
 
 constexpr int kN = 128;          // detector side
 constexpr int kPitch = 132;      // shared-memory row pitch (complex64)
-constexpr int kThreads = 1024;
+constexpr int kThreads = 512;
+constexpr int kLines = kThreads / 8;    // lines per pass handled at once; each group owns two (g, g + kLines)
+constexpr int kWarps = kThreads / 32;   // residual partials per position
 
 __device__ __forceinline__ float2 fm(float2 a, float2 b) { return make_float2(a.x * b.x - a.y * b.y, a.x * b.y + a.y * b.x); }
 __device__ __forceinline__ float2 fmc(float2 a, float2 b) {  // a * conj(b)
@@ -91,60 +94,72 @@ __device__ __forceinline__ void dft8(float2 (&v)[8]) {
     v[3] = fadd(e3, o3); v[7] = fsub(e3, o3);
 }
 
-// Group exchange, forward direction: thread t holds x[q] = Y[t][q] (q = 0..15); afterwards u0[t'] = Y[t'][2t],
-// u1[t'] = Y[t'][2t + 1].  Slot of Y[t][q]: t * 16 + ((q + 2t) & 15), so both the float4 writes and reads of the 8
-// threads cover all 32 banks.
-__device__ __forceinline__ void exchange_fwd(float2 *base, const float2 (&x)[16], int t, float2 (&u0)[8], float2 (&u1)[8]) {
+// Group exchange (inside lines_forward / lines_inverse): Y[t][q] of a line sits at slot t * 16 + ((q + 2t) & 15) of
+// that line's scratch row, so the float4 writes and reads of the 8 threads of a group cover all 32 banks.
+
+// Forward transform of two lines at once (independent work for the scheduler): for each line l, the 16 samples
+// x[l][m] = line[t + 8m]; on return u0[l][s] = X[2t + 16s], u1[l][s] = X[2t+1+16s].
+__device__ __forceinline__ void lines_forward(float2 (&x)[2][16], int t, const float2 *tw, float2 *const (&scratch)[2],
+                                              float2 (&u0)[2][8], float2 (&u1)[2][8]) {
+    dft16<false>(x[0]);
+    dft16<false>(x[1]);
 #pragma unroll
-    for (int j = 0; j < 8; j++)
-        *reinterpret_cast<float4 *>(base + t * 16 + ((2 * j + 2 * t) & 15)) = make_float4(x[2 * j].x, x[2 * j].y, x[2 * j + 1].x, x[2 * j + 1].y);
-    __syncwarp();
-#pragma unroll
-    for (int s = 0; s < 8; s++) {
-        const float4 v = *reinterpret_cast<const float4 *>(base + s * 16 + ((2 * t + 2 * s) & 15));
-        u0[s] = make_float2(v.x, v.y);
-        u1[s] = make_float2(v.z, v.w);
+    for (int q = 1; q < 16; q++) {
+        const float2 w = tw[(t * q) & 127];
+        x[0][q] = fm(x[0][q], w);
+        x[1][q] = fm(x[1][q], w);
     }
+    // group exchange for both lines: thread t then holds u0[l][t'] = Y_l[t'][2t], u1[l][t'] = Y_l[t'][2t + 1]
+#pragma unroll
+    for (int l = 0; l < 2; l++)
+#pragma unroll
+        for (int j = 0; j < 8; j++)
+            *reinterpret_cast<float4 *>(scratch[l] + t * 16 + ((2 * j + 2 * t) & 15)) =
+                make_float4(x[l][2 * j].x, x[l][2 * j].y, x[l][2 * j + 1].x, x[l][2 * j + 1].y);
     __syncwarp();
+#pragma unroll
+    for (int l = 0; l < 2; l++)
+#pragma unroll
+        for (int s = 0; s < 8; s++) {
+            const float4 v = *reinterpret_cast<const float4 *>(scratch[l] + s * 16 + ((2 * t + 2 * s) & 15));
+            u0[l][s] = make_float2(v.x, v.y);
+            u1[l][s] = make_float2(v.z, v.w);
+        }
+    __syncwarp();
+#pragma unroll
+    for (int l = 0; l < 2; l++) { dft8<false>(u0[l]); dft8<false>(u1[l]); }
 }
 
-// Inverse direction: thread t holds u0[t'] = Z[t'][2t], u1[t'] = Z[t'][2t + 1]; afterwards x[q] = Z[t][q].
-__device__ __forceinline__ void exchange_inv(float2 *base, const float2 (&u0)[8], const float2 (&u1)[8], int t, float2 (&x)[16]) {
+// Inverse of lines_forward (unnormalised): from u0/u1 as lines_forward leaves them, x[l][m] = line[t + 8m].
+__device__ __forceinline__ void lines_inverse(float2 (&u0)[2][8], float2 (&u1)[2][8], int t, const float2 *tw,
+                                              float2 *const (&scratch)[2], float2 (&x)[2][16]) {
 #pragma unroll
-    for (int s = 0; s < 8; s++)
-        *reinterpret_cast<float4 *>(base + s * 16 + ((2 * t + 2 * s) & 15)) = make_float4(u0[s].x, u0[s].y, u1[s].x, u1[s].y);
-    __syncwarp();
-#pragma unroll
-    for (int j = 0; j < 8; j++) {
-        const float4 v = *reinterpret_cast<const float4 *>(base + t * 16 + ((2 * j + 2 * t) & 15));
-        x[2 * j] = make_float2(v.x, v.y);
-        x[2 * j + 1] = make_float2(v.z, v.w);
-    }
-    __syncwarp();
-}
-
-// Forward line transform of the 16 samples x[m] = line[t + 8m]: on return u0[s] = X[2t + 16s], u1[s] = X[2t+1+16s].
-__device__ __forceinline__ void line_forward(float2 (&x)[16], int t, const float2 *tw, float2 *scratch, float2 (&u0)[8], float2 (&u1)[8]) {
-    dft16<false>(x);
-#pragma unroll
-    for (int q = 1; q < 16; q++) x[q] = fm(x[q], tw[(t * q) & 127]);
-    exchange_fwd(scratch, x, t, u0, u1);
-    dft8<false>(u0);
-    dft8<false>(u1);
-}
-
-// Inverse of line_forward (unnormalised): from u0/u1 as line_forward leaves them, x[m] = line[t + 8m].
-__device__ __forceinline__ void line_inverse(float2 (&u0)[8], float2 (&u1)[8], int t, const float2 *tw, float2 *scratch, float2 (&x)[16]) {
-    dft8<true>(u0);
-    dft8<true>(u1);
+    for (int l = 0; l < 2; l++) { dft8<true>(u0[l]); dft8<true>(u1[l]); }
     // u0[t'] = G[t'][2t], u1[t'] = G[t'][2t+1]; twiddle by conj(W128^{t' q})
 #pragma unroll
     for (int s = 1; s < 8; s++) {
-        u0[s] = fmc(u0[s], tw[(s * 2 * t) & 127]);
-        u1[s] = fmc(u1[s], tw[(s * (2 * t + 1)) & 127]);
+        const float2 w0 = tw[(s * 2 * t) & 127], w1 = tw[(s * (2 * t + 1)) & 127];
+#pragma unroll
+        for (int l = 0; l < 2; l++) { u0[l][s] = fmc(u0[l][s], w0); u1[l][s] = fmc(u1[l][s], w1); }
     }
-    exchange_inv(scratch, u0, u1, t, x);
-    dft16<true>(x);
+#pragma unroll
+    for (int l = 0; l < 2; l++)
+#pragma unroll
+        for (int s = 0; s < 8; s++)
+            *reinterpret_cast<float4 *>(scratch[l] + s * 16 + ((2 * t + 2 * s) & 15)) =
+                make_float4(u0[l][s].x, u0[l][s].y, u1[l][s].x, u1[l][s].y);
+    __syncwarp();
+#pragma unroll
+    for (int l = 0; l < 2; l++)
+#pragma unroll
+        for (int j = 0; j < 8; j++) {
+            const float4 v = *reinterpret_cast<const float4 *>(scratch[l] + t * 16 + ((2 * j + 2 * t) & 15));
+            x[l][2 * j] = make_float2(v.x, v.y);
+            x[l][2 * j + 1] = make_float2(v.z, v.w);
+        }
+    __syncwarp();
+    dft16<true>(x[0]);
+    dft16<true>(x[1]);
 }
 
 __device__ __forceinline__ int wrap_once(int v, int size) { return v < 0 ? v + size : (v >= size ? v - size : v); }
@@ -153,78 +168,96 @@ __global__ void __launch_bounds__(kThreads, 1) fast128_kernel(Fast128Args a) {
     extern __shared__ __align__(16) float2 sm[];
     float2 *tw = sm + kN * kPitch;
     const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
-    const int g = warp * 4 + (lane >> 3);  // the line this 8-thread group owns
+    const int g = warp * 4 + (lane >> 3);  // this 8-thread group owns lines g and g + 64
     const int t = lane & 7;
     for (int i = tid; i < kN; i += kThreads) tw[i] = a.tw128[i];
     __syncthreads();
-    float2 *line = sm + g * kPitch;  // row g: the group's own region
+    float2 *line[2] = {sm + g * kPitch, sm + (g + kLines) * kPitch};  // the group's own rows (scratch)
     const float inv_n = 1.0f / (float)(kN * kN);
     for (int p = a.first + blockIdx.x; p < a.first + a.count; p += gridDim.x) {
         const int rr = a.scan.rr[p], cc = a.scan.cc[p], cls = a.scan.cls[p];
-        const float2 *S = a.shifted + (size_t)cls * (kN * kN) + g * kN;
-        const float2 *orow = a.object + (size_t)wrap_once(rr + (g < kN / 2 ? g : g - kN), a.object_rows) * a.object_columns;
-        float2 x[16], u0[8], u1[8];
-        // exit wave, row g, columns t + 8m (Ptychography.swift:321-336)
+        float2 x[2][16], u0[2][8], u1[2][8];
+        // exit wave, rows g and g + 64, columns t + 8m (Ptychography.swift:321-336)
 #pragma unroll
-        for (int m = 0; m < 16; m++) {
-            const int c = t + 8 * m;
-            const int xc = wrap_once(cc + (c < kN / 2 ? c : c - kN), a.object_columns);
-            x[m] = fm(S[c], orow[xc]);
+        for (int l = 0; l < 2; l++) {
+            const int row = g + l * kLines;
+            const float2 *S = a.shifted + (size_t)cls * (kN * kN) + row * kN;
+            const float2 *orow = a.object + (size_t)wrap_once(rr + (row < kN / 2 ? row : row - kN), a.object_rows) * a.object_columns;
+#pragma unroll
+            for (int m = 0; m < 16; m++) {
+                const int c = t + 8 * m;
+                const int xc = wrap_once(cc + (c < kN / 2 ? c : c - kN), a.object_columns);
+                x[l][m] = fm(S[c], orow[xc]);
+            }
         }
         // row pass
-        line_forward(x, t, tw, line, u0, u1);
+        lines_forward(x, t, tw, line, u0, u1);
 #pragma unroll
-        for (int s = 0; s < 8; s++)
-            *reinterpret_cast<float4 *>(line + 2 * t + 16 * s) = make_float4(u0[s].x, u0[s].y, u1[s].x, u1[s].y);
-        __syncthreads();
-        // column pass: column g, rows t + 8m
+        for (int l = 0; l < 2; l++)
 #pragma unroll
-        for (int m = 0; m < 16; m++) x[m] = sm[(t + 8 * m) * kPitch + g];
+            for (int s = 0; s < 8; s++)
+                *reinterpret_cast<float4 *>(line[l] + 2 * t + 16 * s) = make_float4(u0[l][s].x, u0[l][s].y, u1[l][s].x, u1[l][s].y);
         __syncthreads();
-        line_forward(x, t, tw, line, u0, u1);
-        // projection (Ptychography.swift:338-349); this thread holds F[2t + parity + 16s][g]
-        const float4 *A = reinterpret_cast<const float4 *>(a.amplitudes + ((size_t)p * kN + g) * kN + t * 16);
+        // column pass: columns g and g + 64, rows t + 8m
+#pragma unroll
+        for (int l = 0; l < 2; l++)
+#pragma unroll
+            for (int m = 0; m < 16; m++) x[l][m] = sm[(t + 8 * m) * kPitch + g + l * kLines];
+        __syncthreads();
+        lines_forward(x, t, tw, line, u0, u1);
+        // projection (Ptychography.swift:338-349); line l holds F[2t + parity + 16s][g + 64 l]
         double err = 0;
 #pragma unroll
-        for (int h = 0; h < 4; h++) {
-            const float4 av = A[h];
-            const float am[4] = {av.x, av.y, av.z, av.w};
+        for (int l = 0; l < 2; l++) {
+            const float4 *A = reinterpret_cast<const float4 *>(a.amplitudes + ((size_t)p * kN + g + l * kLines) * kN + t * 16);
 #pragma unroll
-            for (int e = 0; e < 4; e++) {
-                const int j = h * 4 + e;       // j = parity * 8 + s
-                float2 &f = (j < 8) ? u0[j] : u1[j - 8];
-                const float mag = sqrtf(f.x * f.x + f.y * f.y);
-                const float miss = am[e] - mag;
-                err += (double)(miss * miss);
-                if (mag > 0.f) {
-                    const float sc = (am[e] / mag - 1.0f) * inv_n;
-                    f = make_float2(f.x * sc, f.y * sc);
-                } else {
-                    f = make_float2(am[e] * inv_n, 0.f);
+            for (int h = 0; h < 4; h++) {
+                const float4 av = A[h];
+                const float am[4] = {av.x, av.y, av.z, av.w};
+#pragma unroll
+                for (int e = 0; e < 4; e++) {
+                    const int j = h * 4 + e;  // j = parity * 8 + s
+                    float2 &f = (j < 8) ? u0[l][j] : u1[l][j - 8];
+                    const float mag = sqrtf(f.x * f.x + f.y * f.y);
+                    const float miss = am[e] - mag;
+                    err += (double)(miss * miss);
+                    if (mag > 0.f) {
+                        const float sc = (am[e] / mag - 1.0f) * inv_n;
+                        f = make_float2(f.x * sc, f.y * sc);
+                    } else {
+                        f = make_float2(am[e] * inv_n, 0.f);
+                    }
                 }
             }
         }
 #pragma unroll
         for (int o = 16; o > 0; o >>= 1) err += __shfl_down_sync(0xffffffffu, err, o);
-        if (lane == 0) a.error[(size_t)p * 32 + warp] = err;
+        if (lane == 0) a.error[(size_t)p * kWarps + warp] = err;
         // inverse column pass
-        line_inverse(u0, u1, t, tw, line, x);
-        __syncthreads();  // every group is done with its scratch row before the columns are written back
+        lines_inverse(u0, u1, t, tw, line, x);
+        __syncthreads();  // every group is done with its scratch rows before the columns are written back
 #pragma unroll
-        for (int m = 0; m < 16; m++) sm[(t + 8 * m) * kPitch + g] = x[m];
+        for (int l = 0; l < 2; l++)
+#pragma unroll
+            for (int m = 0; m < 16; m++) sm[(t + 8 * m) * kPitch + g + l * kLines] = x[l][m];
         __syncthreads();
         // inverse row pass from the row-pass layout
 #pragma unroll
-        for (int s = 0; s < 8; s++) {
-            const float4 v = *reinterpret_cast<const float4 *>(line + 2 * t + 16 * s);
-            u0[s] = make_float2(v.x, v.y);
-            u1[s] = make_float2(v.z, v.w);
-        }
-        __syncwarp();
-        line_inverse(u0, u1, t, tw, line, x);
-        float2 *out = a.dpsi + (size_t)p * (kN * kN) + g * kN;
+        for (int l = 0; l < 2; l++)
 #pragma unroll
-        for (int m = 0; m < 16; m++) out[t + 8 * m] = x[m];
+            for (int s = 0; s < 8; s++) {
+                const float4 v = *reinterpret_cast<const float4 *>(line[l] + 2 * t + 16 * s);
+                u0[l][s] = make_float2(v.x, v.y);
+                u1[l][s] = make_float2(v.z, v.w);
+            }
+        __syncwarp();
+        lines_inverse(u0, u1, t, tw, line, x);
+#pragma unroll
+        for (int l = 0; l < 2; l++) {
+            float2 *out = a.dpsi + (size_t)p * (kN * kN) + (g + l * kLines) * kN;
+#pragma unroll
+            for (int m = 0; m < 16; m++) out[t + 8 * m] = x[l][m];
+        }
     }
 }
 
@@ -242,6 +275,8 @@ __global__ void permute_amplitudes_kernel(const float *in, float *out, long long
 }  // namespace
 
 bool fast128_applicable(int rows, int columns) { return rows == kN && columns == kN; }
+
+int fast128_partials_per_position() { return kWarps; }
 
 size_t fast128_smem() { return (size_t)(kN * kPitch + kN) * sizeof(float2); }
 

@@ -121,7 +121,7 @@ struct cubo_ptycho_plan {
     DeviceBuffer dpsi, error, errors, iteration;
     DeviceBuffer probe64, scratch64, spectrum64, shifted, shift_tmp64, ramps_r64, ramps_c64;
     DeviceBuffer partial_grad, partial_weight, grad_p64, weight_p64, probe_block_max;
-    DeviceBuffer maxes, sums, aperture64, mask_dev;
+    DeviceBuffer maxes, sums, aperture64, mask_dev, error_scratch;
     DeviceBuffer tw_r, tw_c, tw_r64, tw_c64;
 
     ~cubo_ptycho_plan() {
@@ -309,7 +309,7 @@ void build_plan(cubo_ptycho_plan *p, const cubo_ptycho_problem *pr) {
     check(p->weight_o.alloc((size_t)p->objects * sizeof(T)), "cudaMalloc");
     check(p->tile_max.alloc((size_t)p->tiles * sizeof(double)), "cudaMalloc");
     check(p->dpsi.alloc((size_t)P * n * sizeof(C2<T>)), "cudaMalloc dpsi");
-    p->error_count = p->fast ? (long long)P * 32 : P;
+    p->error_count = p->fast ? (long long)P * fast128_partials_per_position() : P;
     check(p->error.alloc((size_t)p->error_count * sizeof(double)), "cudaMalloc");
     check(p->iteration.alloc(sizeof(int)), "cudaMalloc");
     check(cudaMemsetAsync(p->iteration.ptr, 0, sizeof(int), s), "memset");
@@ -345,6 +345,7 @@ void build_plan(cubo_ptycho_plan *p, const cubo_ptycho_problem *pr) {
     p->probe_blocks = kblocks;
     check(p->probe_block_max.alloc((size_t)kblocks * sizeof(double)), "cudaMalloc");
     check(p->maxes.alloc(4 * sizeof(double)), "cudaMalloc");
+    check(p->error_scratch.alloc((size_t)error_reduce_scratch() * sizeof(double)), "cudaMalloc");
     check(p->sums.alloc(8 * sizeof(double)), "cudaMalloc");
     check(p->aperture64.alloc((size_t)n * sizeof(double)), "cudaMalloc");
     if (!p->mask.empty()) upload(p->mask_dev, p->mask, s);
@@ -507,9 +508,9 @@ void enqueue_iteration(cubo_ptycho_plan *p) {
                                        pp.constrain_object_amplitude ? 1 : 0, pp.pure_phase_object ? 1 : 0, s);
     });
     enqueue_probe_side(p);
-    timed(p, kErrorReduce, 1, [&] {
-        return launch_error_reduce(p->error.as<double>(), (int)p->error_count, p->divisor, p->errors.as<double>(),
-                                   p->iteration.as<int>(), s);
+    timed(p, kErrorReduce, 2, [&] {
+        return launch_error_reduce(p->error.as<double>(), p->error_count, p->divisor, p->errors.as<double>(),
+                                   p->iteration.as<int>(), p->error_scratch.as<double>(), s);
     });
 }
 

@@ -1,0 +1,128 @@
+// Minimal tcgen05 (5th-generation tensor core) helpers for sm_100a, written as inline PTX.
+//
+// Operand layouts are the no-swizzle canonical ones: a "core matrix" is 8 rows x 16 bytes stored contiguously
+// (128 bytes).  For a K-major operand (rows = M or N, K contiguous) the 16-byte chunk j along K of row group i sits at
+// i * SBO + j * LBO; for an MN-major operand (K rows, MN contiguous) the 16-byte chunk of 8 MN elements of MN group i and
+// K group j sits at i * SBO + j * LBO, each core matrix holding 8 K rows of 16 bytes.  Bit layouts of the descriptors
+// follow the PTX ISA's shared-memory matrix descriptor and kind::f16 instruction descriptor.
+//
+// Every wait here is bounded: a wait that runs out returns false, the caller records an error flag and finishes
+// without trapping, so a bad state costs a status code and never a hung GPU.
+#pragma once
+
+#include <stdint.h>
+
+namespace cubo {
+namespace umma {
+
+__device__ __forceinline__ uint32_t smem_u32(const void *p) { return (uint32_t)__cvta_generic_to_shared(p); }
+
+// Shared-memory matrix descriptor, no swizzle: start address >> 4 in bits [0,14), LBO >> 4 in [16,30), SBO >> 4 in
+// [32,46), descriptor version 1 in [46,48), base offset 0, layout type 0 (no swizzle) in [61,64).
+__device__ __forceinline__ uint64_t smem_desc(uint32_t addr, uint32_t lbo, uint32_t sbo) {
+    uint64_t d = 0;
+    d |= (uint64_t)((addr >> 4) & 0x3FFFu);
+    d |= (uint64_t)((lbo >> 4) & 0x3FFFu) << 16;
+    d |= (uint64_t)((sbo >> 4) & 0x3FFFu) << 32;
+    d |= (uint64_t)1 << 46;
+    return d;
+}
+
+// kind::f16 instruction descriptor: F32 accumulator (bits [4,6) = 1), A and B BF16 ([7,10) = [10,13) = 1), optional
+// negation of A / B (bits 13 / 14), A / B MN-major (bits 15 / 16), N >> 3 in [17,23), M >> 4 in [24,29).
+__host__ __device__ constexpr uint32_t idesc_bf16(int M, int N, bool a_mn_major, bool b_mn_major, bool negate_a = false,
+                                                  bool negate_b = false) {
+    return (1u << 4) | (1u << 7) | (1u << 10) | ((negate_a ? 1u : 0u) << 13) | ((negate_b ? 1u : 0u) << 14) |
+           ((a_mn_major ? 1u : 0u) << 15) | ((b_mn_major ? 1u : 0u) << 16) | ((uint32_t)(N >> 3) << 17) |
+           ((uint32_t)(M >> 4) << 24);
+}
+
+// Tensor-memory allocation by one full warp; the allocated base address is written to *dst (shared memory).
+__device__ __forceinline__ void tmem_alloc(uint32_t *dst, uint32_t columns) {
+    asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(smem_u32(dst)), "r"(columns)
+                 : "memory");
+}
+__device__ __forceinline__ void tmem_relinquish() {
+    asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;" ::: "memory");
+}
+__device__ __forceinline__ void tmem_dealloc(uint32_t taddr, uint32_t columns) {
+    asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(taddr), "r"(columns) : "memory");
+}
+
+// D[tmem] = A[smem] * B[smem] (+ D when accumulate); issued by one thread.
+__device__ __forceinline__ void mma_ss(uint32_t d_tmem, uint64_t a_desc, uint64_t b_desc, uint32_t idesc,
+                                       uint32_t accumulate) {
+    asm volatile(
+        "{\n\t.reg .pred p;\n\tsetp.ne.b32 p, %4, 0;\n\t"
+        "tcgen05.mma.cta_group::1.kind::f16 [%0], %1, %2, %3, p;\n\t}\n" ::"r"(d_tmem),
+        "l"(a_desc), "l"(b_desc), "r"(idesc), "r"(accumulate)
+        : "memory");
+}
+
+// Arrive once on *mbar when every MMA this thread issued before has completed.
+__device__ __forceinline__ void mma_commit(uint64_t *mbar) {
+    asm volatile("tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];" ::"r"(smem_u32(mbar))
+                 : "memory");
+}
+
+__device__ __forceinline__ void mbar_init(uint64_t *mbar, uint32_t count) {
+    asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(smem_u32(mbar)), "r"(count) : "memory");
+}
+
+__device__ __forceinline__ bool mbar_try_wait(uint64_t *mbar, uint32_t parity) {
+    uint32_t ok;
+    asm volatile(
+        "{\n\t.reg .pred p;\n\tmbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n\t"
+        "selp.b32 %0, 1, 0, p;\n\t}\n"
+        : "=r"(ok)
+        : "r"(smem_u32(mbar)), "r"(parity)
+        : "memory");
+    return ok != 0;
+}
+
+// Waits for the phase of parity `parity` to complete, at most `limit` polls; false when it ran out.
+__device__ __forceinline__ bool mbar_wait(uint64_t *mbar, uint32_t parity, uint32_t limit) {
+    for (uint32_t i = 0; i < limit; i++)
+        if (mbar_try_wait(mbar, parity)) return true;
+    return false;
+}
+
+__device__ __forceinline__ void fence_before_sync() { asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory"); }
+__device__ __forceinline__ void fence_after_sync() { asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory"); }
+// Makes this thread's generic-proxy shared-memory writes visible to the tensor core (async proxy).
+__device__ __forceinline__ void fence_proxy_async() { asm volatile("fence.proxy.async.shared::cta;" ::: "memory"); }
+
+// 32 lanes x 32 bits x 16 columns: thread i of the warp receives lane (lane field of taddr) + i, columns col..col+15.
+__device__ __forceinline__ void tmem_ld16(uint32_t taddr, float (&v)[16]) {
+    uint32_t r[16];
+    asm volatile(
+        "tcgen05.ld.sync.aligned.32x32b.x16.b32 {%0,%1,%2,%3,%4,%5,%6,%7,%8,%9,%10,%11,%12,%13,%14,%15}, [%16];"
+        : "=r"(r[0]), "=r"(r[1]), "=r"(r[2]), "=r"(r[3]), "=r"(r[4]), "=r"(r[5]), "=r"(r[6]), "=r"(r[7]), "=r"(r[8]),
+          "=r"(r[9]), "=r"(r[10]), "=r"(r[11]), "=r"(r[12]), "=r"(r[13]), "=r"(r[14]), "=r"(r[15])
+        : "r"(taddr));
+#pragma unroll
+    for (int i = 0; i < 16; i++) v[i] = __uint_as_float(r[i]);
+}
+__device__ __forceinline__ void tmem_wait_ld() { asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory"); }
+
+// TMEM address of lane `lane`, column `column` relative to the allocation base.
+__device__ __forceinline__ uint32_t tmem_addr(uint32_t base, uint32_t lane, uint32_t column) {
+    return base + (lane << 16) + column;
+}
+
+// bf16 bit patterns without the cuda_bf16 header: round-to-nearest-even of a finite float.
+__device__ __forceinline__ uint16_t bf16_bits(float x) {
+    const uint32_t u = __float_as_uint(x);
+    const uint32_t rounding = 0x7FFFu + ((u >> 16) & 1u);
+    return (uint16_t)((u + rounding) >> 16);
+}
+__device__ __forceinline__ float bf16_value(uint16_t b) { return __uint_as_float((uint32_t)b << 16); }
+
+// Split x into hi + lo, both bf16: hi = bf16(x), lo = bf16(x - hi) (x - hi is exact in FP32).
+__device__ __forceinline__ void split_bf16(float x, uint16_t &hi, uint16_t &lo) {
+    hi = bf16_bits(x);
+    lo = bf16_bits(x - bf16_value(hi));
+}
+
+}  // namespace umma
+}  // namespace cubo
