@@ -62,6 +62,8 @@ SIGNATURES = {
                                                 C.POINTER(C.c_longlong), C.POINTER(C.c_int)]),
     "cubo_ptycho_plan_launch_count": (C.c_longlong, [C.c_void_p]),
     "cubo_ptycho_probe_build": (C.c_int, [C.c_void_p, C.c_int, C.c_int] + [C.c_double] * 9 + [C.c_int, _dp, _dp, _dp]),
+    "cubo_ptycho_plan_forward": (C.c_int, [C.c_void_p, _dp]),
+    "cubo_ptycho_plan_backward": (C.c_int, [C.c_void_p, C.c_int, _dp, _dp, _dp, _dp, _dp]),
     "cubo_ptycho_loss_fp32_noalloc": (C.c_int, [C.c_int] * 5 + [C.c_void_p] * 7),
 }
 

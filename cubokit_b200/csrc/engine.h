@@ -39,6 +39,7 @@ struct ObjectGatherArgs {
     ScanTables scan;
     const C2<T> *shifted;
     const C2<T> *dpsi;
+    int dpsi_transposed;       // dpsi stored [position][column][row]
     C2<T> *grad;               // object gradient sum conj(S) dpsi
     T *weight;                 // sum |S|^2
     double *tile_max;          // per-tile max of weight
@@ -51,6 +52,7 @@ struct ProbeGatherArgs {
     ScanTables scan;
     const C2<T> *object;
     const C2<T> *dpsi;
+    int dpsi_transposed;       // dpsi stored [position][column][row]
     C2<T> *partial_grad;       // [groups][n]
     T *partial_weight;         // [groups][n]
 };
@@ -73,6 +75,25 @@ size_t fast128_smem();
 cudaError_t configure_fast128();
 cudaError_t launch_fast128(const Fast128Args &a, int ctas, cudaStream_t s);
 cudaError_t launch_permute_amplitudes(const float *in, float *out, long long positions, cudaStream_t s);
+
+// The 128 x 128 split-BF16 position pass (bf16dense.cu): DFT-matrix products on the tensor cores.
+struct Bf16Args {
+    int object_rows, object_columns;
+    int first, count;
+    ScanTables scan;
+    const float2 *shifted;
+    const float2 *object;
+    const float *amplitudes;   // [positions][column / 16][row][column mod 16]
+    float2 *dpsi;              // [positions][column][row] (transposed)
+    double *error;             // [positions][bf16_partials_per_position()]
+    const uint16_t *w_planes;  // [4][128][128] bf16 bits: Re W hi, Re W lo, Im W hi, Im W lo
+    int *fault;                // set when a device wait ran out
+};
+bool bf16_applicable(int rows, int columns);
+int bf16_partials_per_position();
+cudaError_t configure_bf16();
+cudaError_t launch_bf16(const Bf16Args &a, int ctas, cudaStream_t s);
+cudaError_t launch_permute_bf16_amplitudes(const float *in, float *out, long long positions, cudaStream_t s);
 
 constexpr int kTileW = 32, kTileH = 8;   // object-gather tile (one pixel per thread)
 constexpr int kGatherThreads = kTileW * kTileH;

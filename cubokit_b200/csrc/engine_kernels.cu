@@ -159,7 +159,12 @@ __global__ void __launch_bounds__(kGatherThreads) object_gather_kernel(ObjectGat
 #pragma unroll
                 for (int u = 0; u < 4; u++) {
                     if (k[u] >= 0) {
-                        d[u] = a.dpsi[(size_t)s_p[i + u] * a.n + k[u]];
+                        int kd = k[u];
+                        if (a.dpsi_transposed) {
+                            const int kr = kd / a.columns, kc = kd - kr * a.columns;
+                            kd = kc * a.rows + kr;
+                        }
+                        d[u] = a.dpsi[(size_t)s_p[i + u] * a.n + kd];
                         sv[u] = a.shifted[(size_t)s_cls[i + u] * a.n + k[u]];
                     }
                 }
@@ -195,6 +200,7 @@ __global__ void __launch_bounds__(kProbeThreads) probe_gather_kernel(ProbeGather
     const bool valid = k < a.n;
     const int kr = valid ? k / a.columns : 0, kc = valid ? k - kr * a.columns : 0;
     const int offr = corner_offset(kr, a.rows), offc = corner_offset(kc, a.columns);
+    const int kd = a.dpsi_transposed ? kc * a.rows + kr : k;  // where pixel k of a residual is stored
     C2<T> g = mk<T>(0, 0);
     T w = 0;
     for (int base = p0; base < p1; base += kChunk) {
@@ -212,7 +218,7 @@ __global__ void __launch_bounds__(kProbeThreads) probe_gather_kernel(ProbeGather
                         const int y = wrap_once(s_rr[i + u] + offr, a.object_rows);
                         const int x = wrap_once(s_cc[i + u] + offc, a.object_columns);
                         o[u] = a.object[(size_t)y * a.object_columns + x];
-                        d[u] = a.dpsi[(size_t)(base + i + u) * a.n + k];
+                        d[u] = a.dpsi[(size_t)(base + i + u) * a.n + kd];
                     }
                 }
 #pragma unroll

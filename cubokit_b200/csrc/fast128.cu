@@ -33,8 +33,22 @@ __device__ __forceinline__ float2 fm(float2 a, float2 b) { return make_float2(a.
 __device__ __forceinline__ float2 fmc(float2 a, float2 b) {  // a * conj(b)
     return make_float2(a.x * b.x + a.y * b.y, a.y * b.x - a.x * b.y);
 }
-__device__ __forceinline__ float2 fadd(float2 a, float2 b) { return make_float2(a.x + b.x, a.y + b.y); }
-__device__ __forceinline__ float2 fsub(float2 a, float2 b) { return make_float2(a.x - b.x, a.y - b.y); }
+// Complex add / subtract as one packed FP32x2 instruction each (sm_100 add.rn.f32x2 / sub.rn.f32x2), same rounding as
+// two scalar FP32 operations.
+__device__ __forceinline__ float2 fadd(float2 a, float2 b) {
+    float2 d;
+    asm("{\n\t.reg .b64 ra, rb, rd;\n\tmov.b64 ra, {%2, %3};\n\tmov.b64 rb, {%4, %5};\n\t"
+        "add.rn.f32x2 rd, ra, rb;\n\tmov.b64 {%0, %1}, rd;\n\t}"
+        : "=f"(d.x), "=f"(d.y) : "f"(a.x), "f"(a.y), "f"(b.x), "f"(b.y));
+    return d;
+}
+__device__ __forceinline__ float2 fsub(float2 a, float2 b) {
+    float2 d;
+    asm("{\n\t.reg .b64 ra, rb, rd;\n\tmov.b64 ra, {%2, %3};\n\tmov.b64 rb, {%4, %5};\n\t"
+        "sub.rn.f32x2 rd, ra, rb;\n\tmov.b64 {%0, %1}, rd;\n\t}"
+        : "=f"(d.x), "=f"(d.y) : "f"(a.x), "f"(a.y), "f"(b.x), "f"(b.y));
+    return d;
+}
 
 template <bool INV>
 __device__ __forceinline__ float2 mul_mi(float2 a) {  // * (-i) forward, * (+i) inverse
@@ -177,17 +191,24 @@ __global__ void __launch_bounds__(kThreads, 1) fast128_kernel(Fast128Args a) {
     for (int p = a.first + blockIdx.x; p < a.first + a.count; p += gridDim.x) {
         const int rr = a.scan.rr[p], cc = a.scan.cc[p], cls = a.scan.cls[p];
         float2 x[2][16], u0[2][8], u1[2][8];
-        // exit wave, rows g and g + 64, columns t + 8m (Ptychography.swift:321-336)
+        // exit wave, rows g and g + 64, columns t + 8m (Ptychography.swift:321-336).  Column t + 8m lies left of the
+        // centre for m >= 8 (corner offset t + 8m - 128); when the whole window is inside the object no wrap is needed.
+        const bool interior = cc >= kN / 2 && cc + kN / 2 <= a.object_columns;
 #pragma unroll
         for (int l = 0; l < 2; l++) {
             const int row = g + l * kLines;
             const float2 *S = a.shifted + (size_t)cls * (kN * kN) + row * kN;
-            const float2 *orow = a.object + (size_t)wrap_once(rr + (row < kN / 2 ? row : row - kN), a.object_rows) * a.object_columns;
+            const float2 *orow = a.object + (size_t)wrap_once(rr + (l == 0 ? row : row - kN), a.object_rows) * a.object_columns;
+            if (interior) {
+                const float2 *centre = orow + cc + t;
 #pragma unroll
-            for (int m = 0; m < 16; m++) {
-                const int c = t + 8 * m;
-                const int xc = wrap_once(cc + (c < kN / 2 ? c : c - kN), a.object_columns);
-                x[l][m] = fm(S[c], orow[xc]);
+                for (int m = 0; m < 16; m++) x[l][m] = fm(S[t + 8 * m], centre[m < 8 ? 8 * m : 8 * m - kN]);
+            } else {
+#pragma unroll
+                for (int m = 0; m < 16; m++) {
+                    const int xc = wrap_once(cc + t + (m < 8 ? 8 * m : 8 * m - kN), a.object_columns);
+                    x[l][m] = fm(S[t + 8 * m], orow[xc]);
+                }
             }
         }
         // row pass

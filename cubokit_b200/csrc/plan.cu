@@ -83,6 +83,20 @@ void upload(DeviceBuffer &b, const std::vector<X> &v, cudaStream_t s) {
 
 bool finite_positive(double v) { return std::isfinite(v) && v > 0; }
 
+// bf16 bits of a double: rounded to float, then to bf16 (nearest, ties to even) on the float's bits.
+uint16_t bf16_round(double v) {
+    const float f = (float)v;
+    uint32_t u;
+    std::memcpy(&u, &f, 4);
+    return (uint16_t)((u + 0x7FFFu + ((u >> 16) & 1u)) >> 16);
+}
+double bf16_to_double(uint16_t b) {
+    const uint32_t u = (uint32_t)b << 16;
+    float f;
+    std::memcpy(&f, &u, 4);
+    return (double)f;
+}
+
 }  // namespace
 
 // ------------------------------------------------------------------------------------------------ the plan
@@ -100,8 +114,10 @@ struct cubo_ptycho_plan {
     int tiles_x = 0, tiles = 0;
     int probe_blocks = 0;
     bool fast = false;      // 128 x 128 FP32 register-resident position pass
+    bool bf16 = false;      // 128 x 128 split-BF16 tensor-core position pass
     int sms = 148;
     long long error_count = 0;  // residual partials summed by the error kernel
+    bool tape_valid = false;    // dpsi holds the residuals of the current state (forward ran, nothing changed since)
     long long iterations_done = 0;
     long long errors_capacity = 0;
     long long launches = 0;
@@ -121,8 +137,9 @@ struct cubo_ptycho_plan {
     DeviceBuffer dpsi, error, errors, iteration;
     DeviceBuffer probe64, scratch64, spectrum64, shifted, shift_tmp64, ramps_r64, ramps_c64;
     DeviceBuffer partial_grad, partial_weight, grad_p64, weight_p64, probe_block_max;
-    DeviceBuffer maxes, sums, aperture64, mask_dev, error_scratch;
+    DeviceBuffer maxes, sums, aperture64, mask_dev, error_scratch, loss_slot;
     DeviceBuffer tw_r, tw_c, tw_r64, tw_c64;
+    DeviceBuffer w_planes, fault;
 
     ~cubo_ptycho_plan() {
         for (auto &t : pending) { event_pool.push_back(t.a); event_pool.push_back(t.b); }
@@ -295,10 +312,11 @@ void build_plan(cubo_ptycho_plan *p, const cubo_ptycho_problem *pr) {
     check(p->amplitudes.alloc((size_t)P * n * sizeof(float)), "cudaMalloc amplitudes");
     check(cudaMemcpyAsync(p->amplitudes.ptr, pr->amplitudes, (size_t)P * n * sizeof(float), cudaMemcpyHostToDevice, s),
           "upload amplitudes");
-    if (p->fast) {
+    if (p->fast || p->bf16) {
         DeviceBuffer permuted;
         check(permuted.alloc((size_t)P * n * sizeof(float)), "cudaMalloc amplitudes");
-        check(launch_permute_amplitudes(p->amplitudes.as<float>(), permuted.as<float>(), P, s), "permute amplitudes");
+        if (p->fast) check(launch_permute_amplitudes(p->amplitudes.as<float>(), permuted.as<float>(), P, s), "permute amplitudes");
+        else check(launch_permute_bf16_amplitudes(p->amplitudes.as<float>(), permuted.as<float>(), P, s), "permute amplitudes");
         check(cudaStreamSynchronize(s), "permute amplitudes");
         std::swap(p->amplitudes.ptr, permuted.ptr);
         std::swap(p->amplitudes.bytes, permuted.bytes);
@@ -309,7 +327,26 @@ void build_plan(cubo_ptycho_plan *p, const cubo_ptycho_problem *pr) {
     check(p->weight_o.alloc((size_t)p->objects * sizeof(T)), "cudaMalloc");
     check(p->tile_max.alloc((size_t)p->tiles * sizeof(double)), "cudaMalloc");
     check(p->dpsi.alloc((size_t)P * n * sizeof(C2<T>)), "cudaMalloc dpsi");
-    p->error_count = p->fast ? (long long)P * fast128_partials_per_position() : P;
+    p->error_count = p->fast ? (long long)P * fast128_partials_per_position()
+                             : p->bf16 ? (long long)P * bf16_partials_per_position() : P;
+    if (p->bf16) {
+        // the 128-point DFT matrix split into bf16 hi + lo, evaluated in FP64: planes Re hi, Re lo, Im hi, Im lo, [m][k]
+        std::vector<uint16_t> planes(4 * (size_t)n);
+        for (int m = 0; m < R; m++)
+            for (int k = 0; k < C; k++) {
+                const double a = -2.0 * kPi * (double)((m * k) % R) / (double)R;
+                const double v[2] = {std::cos(a), std::sin(a)};
+                for (int part = 0; part < 2; part++) {
+                    const uint16_t hi = bf16_round(v[part]);
+                    const uint16_t lo = bf16_round(v[part] - bf16_to_double(hi));
+                    planes[(size_t)(2 * part) * n + m * C + k] = hi;
+                    planes[(size_t)(2 * part + 1) * n + m * C + k] = lo;
+                }
+            }
+        upload(p->w_planes, planes, s);
+        check(p->fault.alloc(sizeof(int)), "cudaMalloc");
+        check(cudaMemsetAsync(p->fault.ptr, 0, sizeof(int), s), "memset");
+    }
     check(p->error.alloc((size_t)p->error_count * sizeof(double)), "cudaMalloc");
     check(p->iteration.alloc(sizeof(int)), "cudaMalloc");
     check(cudaMemsetAsync(p->iteration.ptr, 0, sizeof(int), s), "memset");
@@ -346,6 +383,7 @@ void build_plan(cubo_ptycho_plan *p, const cubo_ptycho_problem *pr) {
     check(p->probe_block_max.alloc((size_t)kblocks * sizeof(double)), "cudaMalloc");
     check(p->maxes.alloc(4 * sizeof(double)), "cudaMalloc");
     check(p->error_scratch.alloc((size_t)error_reduce_scratch() * sizeof(double)), "cudaMalloc");
+    check(p->loss_slot.alloc(2 * sizeof(double)), "cudaMalloc");  // [0] the loss, [1] an int counter
     check(p->sums.alloc(8 * sizeof(double)), "cudaMalloc");
     check(p->aperture64.alloc((size_t)n * sizeof(double)), "cudaMalloc");
     if (!p->mask.empty()) upload(p->mask_dev, p->mask, s);
@@ -364,6 +402,17 @@ void build_plan(cubo_ptycho_plan *p, const cubo_ptycho_problem *pr) {
 
 Fft2Plan64 fft64(const cubo_ptycho_plan *p) {
     return Fft2Plan64{p->R, p->C, p->rad_rows, p->rad_columns, p->tw_r64.as<double2>(), p->tw_c64.as<double2>()};
+}
+
+// After a synchronize: a device wait that ran out (split-BF16 kernel) turns into CUBO_PTYCHO_DEVICE_TIMEOUT.
+void check_fault(cubo_ptycho_plan *p) {
+    if (!p->bf16) return;
+    int f = 0;
+    check(cudaMemcpy(&f, p->fault.ptr, sizeof(int), cudaMemcpyDeviceToHost), "read fault flag");
+    if (f) {
+        cudaMemset(p->fault.ptr, 0, sizeof(int));
+        fail(CUBO_PTYCHO_DEVICE_TIMEOUT, "a tensor-core completion wait ran out on the device");
+    }
 }
 
 void ensure_errors(cubo_ptycho_plan *p, long long needed) {
@@ -455,8 +504,9 @@ void enqueue_probe_side(cubo_ptycho_plan *p) {
         timed(p, kProbeSide, 1, [&] { return launch_support_mask(probe, p->mask_dev.as<unsigned char>(), n, s); });
 }
 
+// Shifted probes, then the position pass over every position: residuals (dpsi) and per-position squared errors.
 template <typename T>
-void enqueue_iteration(cubo_ptycho_plan *p) {
+void enqueue_position_pass(cubo_ptycho_plan *p) {
     cudaStream_t s = p->ctx->stream;
     const int n = p->n;
     const ScanTables scan{p->rr.as<int>(), p->cc.as<int>(), p->cls.as<int>()};
@@ -468,7 +518,14 @@ void enqueue_iteration(cubo_ptycho_plan *p) {
     pa.amplitudes = p->amplitudes.as<float>(); pa.dpsi = p->dpsi.as<C2<T>>(); pa.error = p->error.as<double>();
     pa.tw_rows = p->tw_r.as<C2<T>>(); pa.tw_columns = p->tw_c.as<C2<T>>();
     pa.rad_rows = p->rad_rows; pa.rad_columns = p->rad_columns; pa.inv_n = (T)(1.0 / n);
-    if (p->fast) {
+    if (p->bf16) {
+        Bf16Args ba{};
+        ba.object_rows = p->OR; ba.object_columns = p->OC; ba.first = 0; ba.count = p->P; ba.scan = scan;
+        ba.shifted = p->shifted.as<float2>(); ba.object = p->object.as<float2>();
+        ba.amplitudes = p->amplitudes.as<float>(); ba.dpsi = p->dpsi.as<float2>(); ba.error = p->error.as<double>();
+        ba.w_planes = p->w_planes.as<uint16_t>(); ba.fault = p->fault.as<int>();
+        timed(p, kPositionPass, 1, [&] { return launch_bf16(ba, p->sms, s); });
+    } else if (p->fast) {
         Fast128Args fa{};
         fa.object_rows = p->OR; fa.object_columns = p->OC; fa.first = 0; fa.count = p->P; fa.scan = scan;
         fa.shifted = p->shifted.as<float2>(); fa.object = p->object.as<float2>();
@@ -478,18 +535,25 @@ void enqueue_iteration(cubo_ptycho_plan *p) {
     } else {
         timed(p, kPositionPass, 1, [&] { return launch_position_pass<T>(pa, s); });
     }
+}
 
+// Object and probe gradient sums from dpsi: grad_o / weight_o (object), grad_p64 / weight_p64 (probe), maxima.
+template <typename T>
+void enqueue_gathers(cubo_ptycho_plan *p) {
+    cudaStream_t s = p->ctx->stream;
+    const int n = p->n;
+    const ScanTables scan{p->rr.as<int>(), p->cc.as<int>(), p->cls.as<int>()};
     ObjectGatherArgs<T> ga{};
     ga.rows = p->R; ga.columns = p->C; ga.object_rows = p->OR; ga.object_columns = p->OC; ga.n = n;
     ga.tiles_x = p->tiles_x; ga.tile_start = p->tile_start.as<int>(); ga.tile_list = p->tile_list.as<int>();
-    ga.scan = scan; ga.shifted = p->shifted.as<C2<T>>(); ga.dpsi = p->dpsi.as<C2<T>>();
+    ga.scan = scan; ga.shifted = p->shifted.as<C2<T>>(); ga.dpsi = p->dpsi.as<C2<T>>(); ga.dpsi_transposed = p->bf16;
     ga.grad = p->grad_o.as<C2<T>>(); ga.weight = p->weight_o.as<T>(); ga.tile_max = p->tile_max.as<double>();
     timed(p, kObjectGather, 1, [&] { return launch_object_gather<T>(ga, p->tiles, s); });
 
     ProbeGatherArgs<T> pg{};
     pg.rows = p->R; pg.columns = p->C; pg.object_rows = p->OR; pg.object_columns = p->OC; pg.n = n;
     pg.count = p->P; pg.groups = p->groups; pg.scan = scan; pg.object = p->object.as<C2<T>>();
-    pg.dpsi = p->dpsi.as<C2<T>>(); pg.partial_grad = p->partial_grad.as<C2<T>>(); pg.partial_weight = p->partial_weight.as<T>();
+    pg.dpsi = p->dpsi.as<C2<T>>(); pg.dpsi_transposed = p->bf16; pg.partial_grad = p->partial_grad.as<C2<T>>(); pg.partial_weight = p->partial_weight.as<T>();
     timed(p, kProbeGather, 1, [&] { return launch_probe_gather<T>(pg, s); });
     timed(p, kProbeReduce, 1, [&] {
         return launch_probe_reduce<T>(p->partial_grad.as<C2<T>>(), p->partial_weight.as<T>(), p->groups, n,
@@ -501,6 +565,13 @@ void enqueue_iteration(cubo_ptycho_plan *p) {
         if (e == cudaSuccess) e = launch_max_reduce(p->probe_block_max.as<double>(), p->probe_blocks, p->maxes.as<double>() + 1, s);
         return e;
     });
+}
+
+template <typename T>
+void enqueue_iteration(cubo_ptycho_plan *p) {
+    cudaStream_t s = p->ctx->stream;
+    enqueue_position_pass<T>(p);
+    enqueue_gathers<T>(p);
     const cubo_ptycho_params &pp = p->params;
     timed(p, kObjectUpdate, 1, [&] {
         return launch_object_update<T>(p->object.as<C2<T>>(), p->grad_o.as<C2<T>>(), p->weight_o.as<T>(),
@@ -516,6 +587,7 @@ void enqueue_iteration(cubo_ptycho_plan *p) {
 
 void enqueue_iterations(cubo_ptycho_plan *p, int iterations) {
     ensure_errors(p, p->iterations_done + iterations);
+    if (iterations > 0) p->tape_valid = false;
     for (int i = 0; i < iterations; i++) {
         if (p->fp64) enqueue_iteration<double>(p);
         else enqueue_iteration<float>(p);
@@ -623,8 +695,8 @@ int cubo_ptycho_plan_create(cubo_ptycho_context *ctx, const cubo_ptycho_problem 
         p->params.probe_support_mask = nullptr;
         p->divisor = divisor;
         p->fp64 = pp->form == CUBO_PTYCHO_FORM_FP64;
-        if (pp->form == CUBO_PTYCHO_FORM_SPLIT_BF16)
-            fail(CUBO_PTYCHO_UNSUPPORTED, "the split-BF16 form is not available in this build");
+        if (pp->form == CUBO_PTYCHO_FORM_SPLIT_BF16 && !bf16_applicable(p->R, p->C))
+            fail(CUBO_PTYCHO_UNSUPPORTED, "the split-BF16 tensor-core form needs a 128 x 128 detector");
         if (!position_pass_supported(p->n, p->fp64))
             fail(CUBO_PTYCHO_UNSUPPORTED, "detector of " + std::to_string(p->n) + " pixels exceeds the shared-memory "
                                               "transform of this form");
@@ -633,7 +705,9 @@ int cubo_ptycho_plan_create(cubo_ptycho_context *ctx, const cubo_ptycho_problem 
         if (position_pass_smem(p->n, p->R, p->C, p->fp64) > (size_t)optin)
             fail(CUBO_PTYCHO_UNSUPPORTED, "detector too large for shared memory");
         check(configure_kernels(), "configure kernels");
-        p->fast = !p->fp64 && pp->variant != CUBO_PTYCHO_VARIANT_GENERIC && fast128_applicable(p->R, p->C);
+        p->bf16 = pp->form == CUBO_PTYCHO_FORM_SPLIT_BF16;
+        if (p->bf16) check(configure_bf16(), "configure split-BF16 kernel");
+        p->fast = !p->fp64 && !p->bf16 && pp->variant != CUBO_PTYCHO_VARIANT_GENERIC && fast128_applicable(p->R, p->C);
         if (p->fast) check(configure_fast128(), "configure 128 x 128 kernel");
         check(cudaDeviceGetAttribute(&p->sms, cudaDevAttrMultiProcessorCount, ctx->device), "attribute");
         p->kind_ms.assign(kKinds, 0.0);
@@ -664,6 +738,7 @@ int cubo_ptycho_plan_set_state(cubo_ptycho_plan *p, const double *ore, const dou
         for (int k = 0; k < p->n; k++)
             if (!std::isfinite(pre[k]) || !std::isfinite(pim[k])) fail(CUBO_PTYCHO_INVALID_INPUT, "probe not finite");
         cudaStream_t s = p->ctx->stream;
+        p->tape_valid = false;
         std::vector<double2> probe(p->n);
         for (int k = 0; k < p->n; k++) probe[k] = make_double2(pre[k], pim[k]);
         check(cudaMemcpyAsync(p->probe64.ptr, probe.data(), (size_t)p->n * sizeof(double2), cudaMemcpyHostToDevice, s), "upload probe");
@@ -722,6 +797,7 @@ int cubo_ptycho_plan_errors(cubo_ptycho_plan *p, int count, double *errors) {
     return run_guarded(p->ctx, [&] {
         if (count < 0 || count > p->iterations_done || (count > 0 && !errors)) fail(CUBO_PTYCHO_INVALID_INPUT, "count");
         check(cudaStreamSynchronize(p->ctx->stream), "sync");
+        check_fault(p);
         if (count > 0)
             check(cudaMemcpy(errors, p->errors.as<double>() + (p->iterations_done - count), (size_t)count * sizeof(double),
                              cudaMemcpyDeviceToHost), "download errors");
@@ -744,6 +820,7 @@ int cubo_ptycho_plan_iterate(cubo_ptycho_plan *p, int iterations, double *errors
             }
         }
         check(cudaStreamSynchronize(p->ctx->stream), "sync");
+        check_fault(p);
         if (!cancelled && errors && iterations > 0)
             check(cudaMemcpy(errors, p->errors.as<double>() + start, (size_t)iterations * sizeof(double),
                              cudaMemcpyDeviceToHost), "download errors");
@@ -772,6 +849,79 @@ int cubo_ptycho_reconstruct(cubo_ptycho_context *ctx, const cubo_ptycho_problem 
     cubo_ptycho_plan_destroy(plan);
     ctx->last_error = message;
     return status;
+}
+
+}  // extern "C"
+
+namespace {
+template <typename T>
+void enqueue_forward(cubo_ptycho_plan *p) {
+    enqueue_position_pass<T>(p);
+    check(cudaMemsetAsync(p->loss_slot.ptr, 0, 2 * sizeof(double), p->ctx->stream), "memset");
+    timed(p, kErrorReduce, 2, [&] {
+        return launch_error_reduce(p->error.as<double>(), p->error_count, 1.0, p->loss_slot.as<double>(),
+                                   reinterpret_cast<int *>(p->loss_slot.as<double>() + 1), p->error_scratch.as<double>(),
+                                   p->ctx->stream);
+    });
+}
+
+template <typename T>
+void download_object_gradient(cubo_ptycho_plan *p, double scale, double *re, double *im) {
+    std::vector<C2<T>> g((size_t)p->objects);
+    check(cudaMemcpyAsync(g.data(), p->grad_o.ptr, g.size() * sizeof(C2<T>), cudaMemcpyDeviceToHost, p->ctx->stream),
+          "download gradient");
+    check(cudaStreamSynchronize(p->ctx->stream), "sync");
+    for (long long j = 0; j < p->objects; j++) {
+        if (re) re[j] = scale * (double)g[j].x;
+        if (im) im[j] = scale * (double)g[j].y;
+    }
+}
+}  // namespace
+
+extern "C" {
+
+int cubo_ptycho_plan_forward(cubo_ptycho_plan *p, double *loss) {
+    if (!p) return CUBO_PTYCHO_INVALID_INPUT;
+    return run_guarded(p->ctx, [&] {
+        if (p->fp64) enqueue_forward<double>(p);
+        else enqueue_forward<float>(p);
+        p->tape_valid = true;
+        double l = 0;
+        check(cudaMemcpyAsync(&l, p->loss_slot.ptr, sizeof(double), cudaMemcpyDeviceToHost, p->ctx->stream), "loss");
+        check(cudaStreamSynchronize(p->ctx->stream), "sync");
+        check_fault(p);
+        if (loss) *loss = l;
+    });
+}
+
+int cubo_ptycho_plan_backward(cubo_ptycho_plan *p, int recompute, double *loss, double *gore, double *goim,
+                              double *gpre, double *gpim) {
+    if (!p) return CUBO_PTYCHO_INVALID_INPUT;
+    return run_guarded(p->ctx, [&] {
+        if (recompute || !p->tape_valid) {
+            if (p->fp64) enqueue_forward<double>(p);
+            else enqueue_forward<float>(p);
+            p->tape_valid = true;
+        }
+        if (p->fp64) enqueue_gathers<double>(p);
+        else enqueue_gathers<float>(p);
+        // dL/dRe + i dL/dIm = -2 n * (sum of conj(.) dpsi): dpsi carries the inverse transform's 1/n
+        const double scale = -2.0 * (double)p->n;
+        if (p->fp64) download_object_gradient<double>(p, scale, gore, goim);
+        else download_object_gradient<float>(p, scale, gore, goim);
+        std::vector<double2> gp(p->n);
+        double l = 0;
+        check(cudaMemcpyAsync(gp.data(), p->grad_p64.ptr, (size_t)p->n * sizeof(double2), cudaMemcpyDeviceToHost,
+                              p->ctx->stream), "download gradient");
+        check(cudaMemcpyAsync(&l, p->loss_slot.ptr, sizeof(double), cudaMemcpyDeviceToHost, p->ctx->stream), "loss");
+        check(cudaStreamSynchronize(p->ctx->stream), "sync");
+        check_fault(p);
+        for (int k = 0; k < p->n; k++) {
+            if (gpre) gpre[k] = scale * gp[k].x;
+            if (gpim) gpim[k] = scale * gp[k].y;
+        }
+        if (loss) *loss = l;
+    });
 }
 
 int cubo_ptycho_plan_set_timing(cubo_ptycho_plan *p, int enabled) {

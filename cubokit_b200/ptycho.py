@@ -277,6 +277,24 @@ class Plan:
         self.ctx.check(self.ctx.lib.cubo_ptycho_plan_errors(self.handle, count, _ptr(out)))
         return out[:count]
 
+    def forward(self) -> float:
+        """The unnormalised loss sum (|F| - A)^2 of the current state (``cubo_ptycho_plan_forward``)."""
+        loss = C.c_double(0)
+        self.ctx.check(self.ctx.lib.cubo_ptycho_plan_forward(self.handle, C.byref(loss)))
+        return loss.value
+
+    def backward(self, recompute_exit_waves: bool = False):
+        """``(loss, grad_object, grad_probe)``: dL/dRe + i dL/dIm of the forward loss (``cubo_ptycho_plan_backward``)."""
+        no = int(np.prod(self.object_shape))
+        npb = int(np.prod(self.probe_shape))
+        gore, goim, gpre, gpim = np.zeros(no), np.zeros(no), np.zeros(npb), np.zeros(npb)
+        loss = C.c_double(0)
+        self.ctx.check(self.ctx.lib.cubo_ptycho_plan_backward(self.handle, 1 if recompute_exit_waves else 0,
+                                                              C.byref(loss), _ptr(gore), _ptr(goim), _ptr(gpre),
+                                                              _ptr(gpim)))
+        return (loss.value, (gore + 1j * goim).reshape(self.object_shape),
+                (gpre + 1j * gpim).reshape(self.probe_shape))
+
     def set_timing(self, enabled: bool):
         self.ctx.check(self.ctx.lib.cubo_ptycho_plan_set_timing(self.handle, 1 if enabled else 0))
 

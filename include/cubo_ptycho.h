@@ -147,6 +147,21 @@ CUBO_PTYCHO_API int cubo_ptycho_plan_errors(cubo_ptycho_plan *plan, int count, d
 CUBO_PTYCHO_API void *cubo_ptycho_stream(cubo_ptycho_context *context);
 CUBO_PTYCHO_API int cubo_ptycho_synchronize(cubo_ptycho_context *context);
 
+/* ---- Adjoint pair on a plan's current state (no update is applied).  No counterpart function in the reference: its
+ * reconstruct() computes these quantities inside the loop (Ptychography.swift:337-358); the pair exposes them.
+ * forward: loss = sum over positions and detector pixels of (|F_k| - A_k)^2, F = fft2(S * O[patch]) unnormalised (the
+ *   unnormalised residual of Ptychography.swift:342).  It keeps the inverse-transformed projection residuals of every
+ *   position on the device (the tape) for backward.
+ * backward: gradients of that loss, dL/dRe + i dL/dIm: object -2n sum_p conj(S_p) dpsi_p scattered to the patches, probe
+ *   -2n sum_p conj(O[patch_p]) dpsi_p (the accumulations of Ptychography.swift:351-358 scaled to the loss; for
+ *   fractional positions the probe term is the reference's, which does not undo each shift).  recompute_exit_waves != 0
+ *   recomputes the exit waves and residuals instead of reading the tape (also done when no valid tape exists).  loss
+ *   may be NULL.  Gradient buffers have the object's and the probe's sizes; any of them may be NULL. */
+CUBO_PTYCHO_API int cubo_ptycho_plan_forward(cubo_ptycho_plan *plan, double *loss);
+CUBO_PTYCHO_API int cubo_ptycho_plan_backward(cubo_ptycho_plan *plan, int recompute_exit_waves, double *loss,
+                                              double *grad_object_re, double *grad_object_im, double *grad_probe_re,
+                                              double *grad_probe_im);
+
 /* Launch accounting of a plan: kernels launched since the plan was created, and, when timing is on, the device time of
  * each kernel kind summed over its launches (CUDA events on the context stream).  kinds/ms/launches have room for
  * `capacity` entries; *count receives the number of kinds filled in.  names are static strings. */

@@ -1,0 +1,67 @@
+"""The split-BF16 tensor-core form (128 x 128 detector) against the FP64 oracle and the FP32 form.
+
+Bound: relative L2 error of the reconstructed object against the FP64 oracle <= 1e-4 (the precision form's target), and
+per-iteration errors within 1e-4 relative.
+"""
+import numpy as np
+import pytest
+
+from oracle import c_oracle
+from tests import scenes
+
+pytestmark = pytest.mark.gpu
+
+
+def rel_l2(a, b):
+    return float(np.linalg.norm(a - b) / np.linalg.norm(b))
+
+
+@pytest.mark.parametrize("fractional", [False, True])
+def test_split_bf16_against_fp64_oracle(fractional):
+    import cubokit_b200 as cb
+    if fractional:
+        s = scenes.nonsquare_scene(128, 128, 300)
+    else:
+        s = scenes.raster_scene(scan=4, det=128, step=4, seed=13)
+    ref = c_oracle.reconstruct(s["amplitudes"].astype(np.float32), s["positions"], s["object"], s["probe"],
+                               iterations=3)
+    r = cb.SingleslicePtychography.reconstruct(s["amplitudes"], s["positions"], s["object"], s["probe"], iterations=3,
+                                               precision="split_bf16")
+    assert rel_l2(r.object, ref[0]) <= 1e-4, rel_l2(r.object, ref[0])
+    assert rel_l2(r.probe, ref[1]) <= 1e-4, rel_l2(r.probe, ref[1])
+    assert np.all(np.abs(r.errors - ref[2]) <= 1e-4 * ref[2]), (r.errors, ref[2])
+
+
+def test_split_bf16_is_deterministic_and_close_to_fp32():
+    import cubokit_b200 as cb
+    s = scenes.raster_scene(scan=4, det=128, step=4, seed=17)
+    a = cb.SingleslicePtychography.reconstruct(s["amplitudes"], s["positions"], s["object"], s["probe"], iterations=2,
+                                               precision="split_bf16")
+    b = cb.SingleslicePtychography.reconstruct(s["amplitudes"], s["positions"], s["object"], s["probe"], iterations=2,
+                                               precision="split_bf16")
+    assert np.array_equal(a.object, b.object) and np.array_equal(a.probe, b.probe)
+    f = cb.SingleslicePtychography.reconstruct(s["amplitudes"], s["positions"], s["object"], s["probe"], iterations=2)
+    assert rel_l2(a.object, f.object) <= 1e-4
+
+
+def test_split_bf16_refuses_other_detector_sizes():
+    import cubokit_b200 as cb
+    s = scenes.raster_scene(scan=3, det=64, step=4, seed=1)
+    with pytest.raises(cb.UnsupportedError):
+        cb.SingleslicePtychography.reconstruct(s["amplitudes"], s["positions"], s["object"], s["probe"], iterations=1,
+                                               precision="split_bf16")
+
+
+def test_split_bf16_adjoint_against_fp64():
+    import cubokit_b200 as cb
+    s = scenes.raster_scene(scan=4, det=128, step=4, seed=19)
+    amps = (s["amplitudes"] * 1.05).astype(np.float32)
+    out = {}
+    for precision in ("split_bf16", "fp32"):
+        plan = cb.Plan(amps, s["positions"], s["object"].shape, s["probe"].shape, precision=precision)
+        plan.set_state(s["object"], s["probe"])
+        out[precision] = plan.backward(recompute_exit_waves=True)
+    (l1, go1, gp1), (l2, go2, gp2) = out["split_bf16"], out["fp32"]
+    assert abs(l1 - l2) <= 1e-4 * l2
+    assert np.max(np.abs(go1 - go2)) <= 1e-3 * np.max(np.abs(go2))
+    assert np.max(np.abs(gp1 - gp2)) <= 1e-3 * np.max(np.abs(gp2))
