@@ -4,7 +4,10 @@ Workload (the precision-form configuration): 256 x 256 raster scan, step 4 px, 1
 Float32 amplitudes at 1e5 e/pattern, seeded synthetic data (cubokit_b200.synthetic).  One step = one full-batch GD
 iteration over all 65,536 positions.  Metric: positions * iterations / s.
 
-  python bench.py [--gpus N] [--steps K] [--warmup W] [--form fp32|split_bf16] [--impl ours|reference]
+  python bench.py [--gpus N] [--steps K] [--warmup W] [--form both|fp32|split_bf16] [--impl ours|reference]
+
+The headline form is split-BF16 (the DFT-matrix products on the tensor cores); the FP32 form runs on the same data in
+the same invocation and the line reports both, their ratio and the relative L2 difference of their objects.
 
 `value` is device-timed (CUDA events on the engine's stream) with amplitudes resident in HBM; the 4.3 GB amplitude
 stack and the 8.6 GB residual buffer are far larger than L2, so no flush is needed.  `e2e` is one
@@ -221,7 +224,8 @@ def main():
     ap.add_argument("--steps", type=int, default=20)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
-    ap.add_argument("--form", default="fp32", choices=["fp32", "split_bf16"])
+    ap.add_argument("--form", default="both", choices=["both", "fp32", "split_bf16"],
+                    help="both: split-BF16 (the headline) and FP32 measured on the same data")
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--no-cpu", action="store_true")
     ap.add_argument("--scan", type=int, default=SCAN, help="scan side (the benchmark workload is 256)")
@@ -241,54 +245,92 @@ def main():
     P, n = len(ds.positions), DET * DET
     objects = ds.object_start.size
     ctx = cb.Context(local)
-    plan = cb.Plan(ds.amplitudes, ds.positions, ds.object_start.shape, ds.probe.shape, ctx=ctx, step_size=0.5,
-                   precision=args.form)
-    plan.set_state(ds.object_start, ds.probe)
     stream = torch.cuda.ExternalStream(ctx.stream, device=torch.device("cuda", local))
-    plan.enqueue(args.warmup)
-    ctx.synchronize()
-    barrier(world)
-    start, stop = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
-    launches0 = plan.launch_count
-    with ClockSampler(local) as clocks:
-        torch.cuda.synchronize()
-        start.record(stream)
-        plan.enqueue(args.steps)
-        stop.record(stream)
-        stop.synchronize()
-    ms = start.elapsed_time(stop)
-    launches = plan.launch_count - launches0
-    ms = max_over_ranks(ms, world)
-    errors = plan.errors(args.warmup + args.steps)
-    # per-kernel device time over separate timed iterations (events around every launch)
-    plan.set_timing(True)
-    plan.enqueue(max(3, min(args.steps, 10)))
-    stats = plan.kernel_stats()
-    plan.set_timing(False)
-    plan.close()
+    forms = ["split_bf16", "fp32"] if args.form == "both" else [args.form]
+    results = {}
+    for form in forms:
+        plan = cb.Plan(ds.amplitudes, ds.positions, ds.object_start.shape, ds.probe.shape, ctx=ctx, step_size=0.5,
+                       precision=form)
+        plan.set_state(ds.object_start, ds.probe)
+        plan.enqueue(args.warmup)
+        ctx.synchronize()
+        barrier(world)
+        start, stop = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        launches0 = plan.launch_count
+        with ClockSampler(local) as clocks:
+            torch.cuda.synchronize()
+            start.record(stream)
+            plan.enqueue(args.steps)
+            stop.record(stream)
+            stop.synchronize()
+        ms = max_over_ranks(start.elapsed_time(stop), world)
+        launches = plan.launch_count - launches0
+        errors = plan.errors(args.warmup + args.steps)
+        obj, _ = plan.get_state()
+        # per-kernel device time over separate iterations (events around every launch)
+        plan.set_timing(True)
+        plan.enqueue(max(3, min(args.steps, 10)))
+        stats = plan.kernel_stats()
+        plan.set_timing(False)
+        plan.close()
+        results[form] = dict(ms=ms, launches=launches, errors=errors, object=obj, stats=stats,
+                             clocks=clocks.summary())
 
+    head = forms[0]
+    r = results[head]
+    ms = r["ms"]
+    stats = r["stats"]
     bytes_iter, flops_iter = algorithmic(P, n, objects)
-    hbm_peak, _, peak_kind = measured_peaks()
+    hbm_peak, bf16_peak, peak_kind = measured_peaks()
+    value = P * args.steps / (ms * 1e-3) * world
     pass_ms, pass_launches = stats["position_pass"]
     pass_avg_s = pass_ms / max(pass_launches, 1) * 1e-3
-    pass_bytes = P * 4 * n  # algorithmic bytes of one position-pass launch: the amplitudes it reads
-    pass_flops = P * (10 * n * math.log2(n) + 40 * n)
+    fft_flops = P * (10 * n * math.log2(n) + 40 * n)  # algorithmic: two 2-D FFTs + 40 flops per pixel per position
+    if head == "split_bf16":
+        # executed tensor work: 4 complex 128^3 DFT-matrix products per position, 4 real products each, 3 bf16 splits
+        tensor_flops = P * 4 * 4 * 3 * 2 * 128 ** 3
+        roofline = {"kernel": "position_pass (bf16_position_kernel)", "bound": "tensor",
+                    "achieved": tensor_flops / pass_avg_s / 1e12, "peak": bf16_peak, "unit": "TFLOP/s",
+                    "frac": tensor_flops / pass_avg_s / 1e12 / bf16_peak, "peak_kind": peak_kind + " (bf16 dense burst)",
+                    "traffic": None, "executed_tflop_per_launch": tensor_flops / 1e12,
+                    "note": "executed split-BF16 DFT-GEMM flops (201 MFLOP per position); the FFT-equivalent "
+                            "algorithmic rate is fft_equivalent_tflops",
+                    "fft_equivalent_tflops": fft_flops / pass_avg_s / 1e12,
+                    "amplitude_hbm_gbs": P * 4 * n / pass_avg_s / 1e9}
+    else:
+        roofline = {"kernel": "position_pass (fast128_kernel)", "bound": "hbm",
+                    "achieved": P * 4 * n / pass_avg_s / 1e9, "peak": hbm_peak, "unit": "GB/s",
+                    "frac": P * 4 * n / pass_avg_s / 1e9 / hbm_peak, "peak_kind": peak_kind, "traffic": None,
+                    "note": "algorithmic bytes = amplitudes read (4n per position); the FP32 form is bound by FP32 "
+                            "issue, reported as fft_equivalent_tflops",
+                    "fft_equivalent_tflops": fft_flops / pass_avg_s / 1e12}
+    roofline["iteration_hbm_gbs"] = bytes_iter / (ms / args.steps * 1e-3) / 1e9
     total_stat_ms = sum(v[0] for v in stats.values())
-    value = P * args.steps / (ms * 1e-3) * world
+
+    forms_out = {}
+    for form, fr in results.items():
+        forms_out[form] = {"value": P * args.steps / (fr["ms"] * 1e-3) * world, "ms_per_step": fr["ms"] / args.steps,
+                           "position_pass_ms": fr["stats"]["position_pass"][0] / max(fr["stats"]["position_pass"][1], 1),
+                           "error_last": float(fr["errors"][-1])}
+    comparison = None
+    if len(results) == 2:
+        a, b = results["split_bf16"]["object"], results["fp32"]["object"]
+        comparison = {"ratio_split_bf16_over_fp32": forms_out["split_bf16"]["value"] / forms_out["fp32"]["value"],
+                      "object_rel_l2_split_bf16_vs_fp32": float(np.linalg.norm(a - b) / np.linalg.norm(b)),
+                      "iterations_compared": args.warmup + args.steps}
 
     e2e = None
     if not args.no_e2e:
         t0 = time.perf_counter()
-        r = cb.SingleslicePtychography.reconstruct(ds.amplitudes, ds.positions, ds.object_start, ds.probe,
-                                                   iterations=args.steps, step_size=0.5, precision=args.form,
-                                                   device=local)
-        e2e_s = time.perf_counter() - t0
-        e2e_s = max_over_ranks(e2e_s, world)
+        rr = cb.SingleslicePtychography.reconstruct(ds.amplitudes, ds.positions, ds.object_start, ds.probe,
+                                                    iterations=args.steps, step_size=0.5, precision=head,
+                                                    device=local)
+        e2e_s = max_over_ranks(time.perf_counter() - t0, world)
         h2d = ds.amplitudes.nbytes + ds.positions.nbytes + objects * 16 + n * 16
         d2h = objects * 16 + n * 16 + args.steps * 8
-        e2e = {"value": P * args.steps / e2e_s * world, "unit": UNIT, "seconds": e2e_s,
+        e2e = {"value": P * args.steps / e2e_s * world, "unit": UNIT, "seconds": e2e_s, "form": head,
                "h2d_bytes_per_step": h2d / args.steps, "d2h_bytes_per_step": d2h / args.steps,
-               "final_error": float(r.errors[-1])}
+               "final_error": float(rr.errors[-1])}
 
     cpu = None
     if rank == 0 and not args.no_cpu:
@@ -301,22 +343,16 @@ def main():
         line = {
             "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
             "warmup": args.warmup, "ms_per_step": ms / args.steps, "higher_is_better": True, "scaling": "weak",
-            "vs_baseline": None, "dtype": "f32" if args.form == "fp32" else "bf16x2/f32", "data": "synthetic",
+            "vs_baseline": None, "dtype": "bf16x3/f32" if head == "split_bf16" else "f32", "data": "synthetic",
             "config": {"workload": f"{args.scan}x{args.scan} scan, step {STEP} px, {DET}x{DET} detector, object "
                                    f"{ds.object_start.shape[0]}x{ds.object_start.shape[1]}, dose 1e5, GD step 0.5",
-                       "form": args.form, "positions": P, "parallelism": f"replicas x{world}" if world > 1 else "1 GPU",
+                       "form": head, "positions": P, "parallelism": f"replicas x{world}" if world > 1 else "1 GPU",
                        "l2": "inputs larger than L2 (4.3 GB amplitudes, 8.6 GB residuals)"},
-            "roofline": {"kernel": "position_pass", "bound": "hbm", "achieved": pass_bytes / pass_avg_s / 1e9,
-                         "peak": hbm_peak, "unit": "GB/s", "frac": pass_bytes / pass_avg_s / 1e9 / hbm_peak,
-                         "peak_kind": peak_kind, "traffic": None,
-                         "note": "algorithmic bytes = amplitudes read; the FP32 form is FP32-pipe bound",
-                         "fp32_tflops": pass_flops / pass_avg_s / 1e12,
-                         "iteration_hbm_gbs": bytes_iter / (ms / args.steps * 1e-3) / 1e9,
-                         "iteration_tflops": flops_iter / (ms / args.steps * 1e-3) / 1e12},
+            "forms": forms_out, "comparison": comparison, "roofline": roofline,
             "kernels": {k: {"ms_per_launch": v[0] / max(v[1], 1), "launches": v[1],
                             "share": v[0] / total_stat_ms if total_stat_ms else None} for k, v in stats.items() if v[1]},
-            "cpu_baseline": cpu, "e2e": e2e, "gpu_launches": launches, "clocks": clocks.summary(),
-            "errors_first_last": [float(errors[0]), float(errors[-1])],
+            "cpu_baseline": cpu, "e2e": e2e, "gpu_launches": r["launches"], "clocks": r["clocks"],
+            "errors_first_last": [float(r["errors"][0]), float(r["errors"][-1])],
         }
         print(json.dumps(line), flush=True)
     barrier(world)

@@ -50,15 +50,8 @@ __device__ __forceinline__ void store_chunk(uint8_t *planes, uint32_t off, const
     uint32_t rh[4], rl[4], ih[4], il[4];
 #pragma unroll
     for (int i = 0; i < 4; i++) {
-        uint16_t h0, l0, h1, l1;
-        split_bf16(re[2 * i], h0, l0);
-        split_bf16(re[2 * i + 1], h1, l1);
-        rh[i] = (uint32_t)h0 | ((uint32_t)h1 << 16);
-        rl[i] = (uint32_t)l0 | ((uint32_t)l1 << 16);
-        split_bf16(im[2 * i], h0, l0);
-        split_bf16(im[2 * i + 1], h1, l1);
-        ih[i] = (uint32_t)h0 | ((uint32_t)h1 << 16);
-        il[i] = (uint32_t)l0 | ((uint32_t)l1 << 16);
+        split_bf16x2(re[2 * i], re[2 * i + 1], rh[i], rl[i]);
+        split_bf16x2(im[2 * i], im[2 * i + 1], ih[i], il[i]);
     }
     *reinterpret_cast<uint4 *>(planes + 0 * kPlaneBytes + off) = make_uint4(rh[0], rh[1], rh[2], rh[3]);
     *reinterpret_cast<uint4 *>(planes + 1 * kPlaneBytes + off) = make_uint4(rl[0], rl[1], rl[2], rl[3]);

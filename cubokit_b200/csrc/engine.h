@@ -34,6 +34,7 @@ template <typename T>
 struct ObjectGatherArgs {
     int rows, columns, object_rows, object_columns, n;
     int tiles_x;               // tiles per object row
+    int tile_w, tile_h;        // tile shape: kTileW x kTileH, or kTileH x kTileW (wide axis = residual's contiguous axis)
     const int *tile_start;     // CSR offsets, [tiles + 1]
     const int *tile_list;      // position indices, ascending within each tile
     ScanTables scan;

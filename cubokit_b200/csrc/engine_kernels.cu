@@ -125,7 +125,16 @@ __global__ void __launch_bounds__(kGatherThreads) object_gather_kernel(ObjectGat
     __shared__ double scratch[32];
     const int tile = blockIdx.x;
     const int tx = tile % a.tiles_x, ty = tile / a.tiles_x;
-    const int x = tx * kTileW + (threadIdx.x % kTileW), y = ty * kTileH + threadIdx.x / kTileW;
+    // consecutive threads take consecutive residual addresses: along x for [row][column] residuals, along y (a
+    // transposed kTileH x kTileW walk of the same tile) for [column][row] ones
+    int x, y;
+    if (a.dpsi_transposed) {
+        x = tx * a.tile_w + threadIdx.x / a.tile_h;
+        y = ty * a.tile_h + threadIdx.x % a.tile_h;
+    } else {
+        x = tx * a.tile_w + (threadIdx.x % a.tile_w);
+        y = ty * a.tile_h + threadIdx.x / a.tile_w;
+    }
     const bool inside = x < a.object_columns && y < a.object_rows;
     C2<T> g = mk<T>(0, 0);
     T w = 0;
@@ -194,13 +203,16 @@ constexpr int kProbeThreads = 256;
 template <typename T>
 __global__ void __launch_bounds__(kProbeThreads) probe_gather_kernel(ProbeGatherArgs<T> a) {
     __shared__ int s_rr[kChunk], s_cc[kChunk];
-    const int k = blockIdx.x * kProbeThreads + threadIdx.x;
+    const int idx = blockIdx.x * kProbeThreads + threadIdx.x;  // index in the residual's storage order
     const int group = blockIdx.y;
     const int p0 = (int)((long long)a.count * group / a.groups), p1 = (int)((long long)a.count * (group + 1) / a.groups);
-    const bool valid = k < a.n;
-    const int kr = valid ? k / a.columns : 0, kc = valid ? k - kr * a.columns : 0;
+    const bool valid = idx < a.n;
+    int kr, kc;
+    if (a.dpsi_transposed) { kc = valid ? idx / a.rows : 0; kr = valid ? idx - kc * a.rows : 0; }
+    else { kr = valid ? idx / a.columns : 0; kc = valid ? idx - kr * a.columns : 0; }
+    const int k = kr * a.columns + kc;  // natural pixel index (where the partial sums go)
+    const int kd = idx;                 // where pixel k of a residual is stored
     const int offr = corner_offset(kr, a.rows), offc = corner_offset(kc, a.columns);
-    const int kd = a.dpsi_transposed ? kc * a.rows + kr : k;  // where pixel k of a residual is stored
     C2<T> g = mk<T>(0, 0);
     T w = 0;
     for (int base = p0; base < p1; base += kChunk) {

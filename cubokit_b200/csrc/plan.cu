@@ -112,6 +112,7 @@ struct cubo_ptycho_plan {
     int classes = 1;        // shift classes; class 0 is the zero shift
     int groups = 1;         // probe-gather position groups
     int tiles_x = 0, tiles = 0;
+    int tile_w = kTileW, tile_h = kTileH;  // object-gather tile
     int probe_blocks = 0;
     bool fast = false;      // 128 x 128 FP32 register-resident position pass
     bool bf16 = false;      // 128 x 128 split-BF16 tensor-core position pass
@@ -271,8 +272,9 @@ void build_plan(cubo_ptycho_plan *p, const cubo_ptycho_problem *pr) {
     upload(p->cc, cc, s);
     upload(p->cls, cls, s);
     // ---- object-gather candidate lists: for each tile, the positions whose window touches it, ascending
-    p->tiles_x = (p->OC + kTileW - 1) / kTileW;
-    const int tiles_y = (p->OR + kTileH - 1) / kTileH;
+    if (p->bf16) { p->tile_w = kTileH; p->tile_h = kTileW; }  // the residual is stored [column][row]
+    p->tiles_x = (p->OC + p->tile_w - 1) / p->tile_w;
+    const int tiles_y = (p->OR + p->tile_h - 1) / p->tile_h;
     p->tiles = p->tiles_x * tiles_y;
     std::vector<int> counts(p->tiles + 1, 0);
     std::vector<int> mark_y(tiles_y, -1), mark_x(p->tiles_x, -1);
@@ -282,12 +284,12 @@ void build_plan(cubo_ptycho_plan *p, const cubo_ptycho_problem *pr) {
         tx_list.clear();
         for (int k = 0; k < R; k++) {
             const int y = (int)wrap_ll((long long)rr[i] + corner_offset(k, R), p->OR);
-            const int t = y / kTileH;
+            const int t = y / p->tile_h;
             if (mark_y[t] != i) { mark_y[t] = i; ty_list.push_back(t); }
         }
         for (int k = 0; k < C; k++) {
             const int x = (int)wrap_ll((long long)cc[i] + corner_offset(k, C), p->OC);
-            const int t = x / kTileW;
+            const int t = x / p->tile_w;
             if (mark_x[t] != i) { mark_x[t] = i; tx_list.push_back(t); }
         }
     };
@@ -545,7 +547,7 @@ void enqueue_gathers(cubo_ptycho_plan *p) {
     const ScanTables scan{p->rr.as<int>(), p->cc.as<int>(), p->cls.as<int>()};
     ObjectGatherArgs<T> ga{};
     ga.rows = p->R; ga.columns = p->C; ga.object_rows = p->OR; ga.object_columns = p->OC; ga.n = n;
-    ga.tiles_x = p->tiles_x; ga.tile_start = p->tile_start.as<int>(); ga.tile_list = p->tile_list.as<int>();
+    ga.tiles_x = p->tiles_x; ga.tile_w = p->tile_w; ga.tile_h = p->tile_h; ga.tile_start = p->tile_start.as<int>(); ga.tile_list = p->tile_list.as<int>();
     ga.scan = scan; ga.shifted = p->shifted.as<C2<T>>(); ga.dpsi = p->dpsi.as<C2<T>>(); ga.dpsi_transposed = p->bf16;
     ga.grad = p->grad_o.as<C2<T>>(); ga.weight = p->weight_o.as<T>(); ga.tile_max = p->tile_max.as<double>();
     timed(p, kObjectGather, 1, [&] { return launch_object_gather<T>(ga, p->tiles, s); });

@@ -138,6 +138,21 @@ __device__ __forceinline__ uint16_t bf16_bits(float x) {
 }
 __device__ __forceinline__ float bf16_value(uint16_t b) { return __uint_as_float((uint32_t)b << 16); }
 
+// Two floats to packed bf16x2 (round to nearest even): low half = lo_elem, high half = hi_elem.
+__device__ __forceinline__ uint32_t pack_bf16x2(float lo_elem, float hi_elem) {
+    uint32_t d;
+    asm("cvt.rn.bf16x2.f32 %0, %1, %2;" : "=r"(d) : "f"(hi_elem), "f"(lo_elem));
+    return d;
+}
+
+// Split (x0, x1) into bf16 hi and lo pairs: hi = bf16(x), lo = bf16(x - hi) (x - hi is exact in FP32); packed with x0 in
+// the low half, the order of K (or MN) elements in a 32-bit word of an operand.
+__device__ __forceinline__ void split_bf16x2(float x0, float x1, uint32_t &hi, uint32_t &lo) {
+    hi = pack_bf16x2(x0, x1);
+    const float h0 = __uint_as_float(hi << 16), h1 = __uint_as_float(hi & 0xFFFF0000u);
+    lo = pack_bf16x2(x0 - h0, x1 - h1);
+}
+
 // Split x into hi + lo, both bf16: hi = bf16(x), lo = bf16(x - hi) (x - hi is exact in FP32).
 __device__ __forceinline__ void split_bf16(float x, uint16_t &hi, uint16_t &lo) {
     hi = bf16_bits(x);
