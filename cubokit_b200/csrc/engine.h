@@ -124,6 +124,7 @@ struct Fft2Plan64 {
     const double2 *tw_rows, *tw_columns;
 };
 cudaError_t launch_fft2_f64(const Fft2Plan64 &p, double2 *data, int batch, bool inverse, cudaStream_t s);
+cudaError_t configure_fft_lines();
 cudaError_t launch_scale_f64(double2 *data, int count, double scale, cudaStream_t s);
 cudaError_t launch_probe_update(double2 *probe, const double2 *grad, const double *weight, int n, const double *max_weight,
                                 double step, double minimum, cudaStream_t s);

@@ -707,6 +707,7 @@ int cubo_ptycho_plan_create(cubo_ptycho_context *ctx, const cubo_ptycho_problem 
         if (position_pass_smem(p->n, p->R, p->C, p->fp64) > (size_t)optin)
             fail(CUBO_PTYCHO_UNSUPPORTED, "detector too large for shared memory");
         check(configure_kernels(), "configure kernels");
+        check(configure_fft_lines(), "configure line transforms");
         p->bf16 = pp->form == CUBO_PTYCHO_FORM_SPLIT_BF16;
         if (p->bf16) check(configure_bf16(), "configure split-BF16 kernel");
         p->fast = !p->fp64 && !p->bf16 && pp->variant != CUBO_PTYCHO_VARIANT_GENERIC && fast128_applicable(p->R, p->C);
@@ -975,6 +976,7 @@ int cubo_ptycho_probe_build(cubo_ptycho_context *ctx, int rows, int columns, dou
         }
         const int n = rows * columns;
         cudaStream_t s = ctx->stream;
+        check(configure_fft_lines(), "configure line transforms");
         DeviceBuffer field, dterms, twr, twc, sum;
         check(field.alloc((size_t)n * sizeof(double2)), "cudaMalloc");
         check(sum.alloc(sizeof(double)), "cudaMalloc");

@@ -231,8 +231,6 @@ cudaError_t launch_fft2_f64(const Fft2Plan64 &p, double2 *data, int batch, bool 
         const int lines = batch * (cols ? p.columns : p.rows);
         const int lpb = kLineMaxN / L;
         const size_t smem = ((size_t)lpb * L + L) * sizeof(double2);
-        cudaError_t e = cudaFuncSetAttribute(fft_lines_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
-        if (e != cudaSuccess) return e;
         fft_lines_kernel<<<(lines + lpb - 1) / lpb, kLineThreads, smem, s>>>(
             data, p.rows, p.columns, batch, cols, lpb, cols ? p.rad_rows : p.rad_columns,
             cols ? p.tw_rows : p.tw_columns, inverse);
@@ -240,6 +238,12 @@ cudaError_t launch_fft2_f64(const Fft2Plan64 &p, double2 *data, int batch, bool 
         if (e != cudaSuccess) return e;
     }
     return cudaSuccess;
+}
+
+// The line-FFT kernel's shared-memory limit, once per device (outside any stream capture).
+cudaError_t configure_fft_lines() {
+    return cudaFuncSetAttribute(fft_lines_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                (int)((kLineMaxN + kLineMaxN) * sizeof(double2)));
 }
 
 cudaError_t launch_scale_f64(double2 *data, int count, double scale, cudaStream_t s) {
