@@ -3,8 +3,8 @@
 The engine is ``libcuboptycho.so`` (CUDA kernels behind the C ABI of ``include/cubo_ptycho.h``); this package is its
 Python binding and the host-side mirror of CuboPtycho's API.
 """
-from .ptycho import (CancellationError, Context, DeviceError, Plan, PtychographyError, PtychographyProbe, Result,
+from .ptycho import (Batch, CancellationError, Context, DeviceError, Plan, PtychographyError, PtychographyProbe, Result,
                      SingleslicePtychography, UnsupportedError, context, electron_wavelength)
 
-__all__ = ["CancellationError", "Context", "DeviceError", "Plan", "PtychographyError", "PtychographyProbe", "Result",
+__all__ = ["Batch", "CancellationError", "Context", "DeviceError", "Plan", "PtychographyError", "PtychographyProbe", "Result",
            "SingleslicePtychography", "UnsupportedError", "context", "electron_wavelength"]

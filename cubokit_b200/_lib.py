@@ -64,6 +64,14 @@ SIGNATURES = {
     "cubo_ptycho_probe_build": (C.c_int, [C.c_void_p, C.c_int, C.c_int] + [C.c_double] * 9 + [C.c_int, _dp, _dp, _dp]),
     "cubo_ptycho_plan_forward": (C.c_int, [C.c_void_p, _dp]),
     "cubo_ptycho_plan_backward": (C.c_int, [C.c_void_p, C.c_int, _dp, _dp, _dp, _dp, _dp]),
+    "cubo_ptycho_batch_create": (C.c_int, [C.c_void_p, C.c_int, C.POINTER(Problem), C.POINTER(Params),
+                                           C.POINTER(C.c_void_p)]),
+    "cubo_ptycho_batch_destroy": (C.c_int, [C.c_void_p]),
+    "cubo_ptycho_batch_set_state": (C.c_int, [C.c_void_p, C.c_int, _dp, _dp, _dp, _dp]),
+    "cubo_ptycho_batch_get_state": (C.c_int, [C.c_void_p, C.c_int, _dp, _dp, _dp, _dp]),
+    "cubo_ptycho_batch_run": (C.c_int, [C.c_void_p, C.c_int, C.c_int]),
+    "cubo_ptycho_batch_errors": (C.c_int, [C.c_void_p, C.c_int, C.c_int, _dp]),
+    "cubo_ptycho_batch_launches_per_iteration": (C.c_longlong, [C.c_void_p]),
     "cubo_ptycho_loss_fp32_noalloc": (C.c_int, [C.c_int] * 5 + [C.c_void_p] * 7),
 }
 

@@ -955,6 +955,129 @@ int cubo_ptycho_plan_kernel_stats(cubo_ptycho_plan *p, int capacity, const char 
 
 long long cubo_ptycho_plan_launch_count(const cubo_ptycho_plan *p) { return p ? p->launches : -1; }
 
+}  // extern "C"
+
+struct cubo_ptycho_batch {
+    cubo_ptycho_context *ctx = nullptr;
+    std::vector<cubo_ptycho_plan *> plans;
+    cudaGraph_t graph = nullptr;
+    cudaGraphExec_t exec = nullptr;
+    std::vector<void *> captured_errors;  // the error buffers the graph was captured with
+    long long launches_per_iteration = 0;
+    ~cubo_ptycho_batch() {
+        if (exec) cudaGraphExecDestroy(exec);
+        if (graph) cudaGraphDestroy(graph);
+        for (auto *p : plans) delete p;
+    }
+};
+
+namespace {
+
+// Captures one iteration of every plan of the batch into a graph (again when an error buffer moved).
+void capture_batch(cubo_ptycho_batch *b) {
+    if (b->exec) { cudaGraphExecDestroy(b->exec); b->exec = nullptr; }
+    if (b->graph) { cudaGraphDestroy(b->graph); b->graph = nullptr; }
+    cudaStream_t s = b->ctx->stream;
+    long long before = 0;
+    for (auto *p : b->plans) before += p->launches;
+    check(cudaStreamBeginCapture(s, cudaStreamCaptureModeThreadLocal), "cudaStreamBeginCapture");
+    try {
+        for (auto *p : b->plans) {
+            if (p->fp64) enqueue_iteration<double>(p);
+            else enqueue_iteration<float>(p);
+        }
+    } catch (...) {
+        cudaGraph_t g = nullptr;
+        cudaStreamEndCapture(s, &g);
+        if (g) cudaGraphDestroy(g);
+        throw;
+    }
+    check(cudaStreamEndCapture(s, &b->graph), "cudaStreamEndCapture");
+    check(cudaGraphInstantiate(&b->exec, b->graph, 0), "cudaGraphInstantiate");
+    long long after = 0;
+    for (auto *p : b->plans) after += p->launches;
+    b->launches_per_iteration = after - before;
+    b->captured_errors.clear();
+    for (auto *p : b->plans) b->captured_errors.push_back(p->errors.ptr);
+}
+
+}  // namespace
+
+extern "C" {
+
+int cubo_ptycho_batch_create(cubo_ptycho_context *ctx, int count, const cubo_ptycho_problem *problems,
+                             const cubo_ptycho_params *params, cubo_ptycho_batch **out) {
+    if (!ctx || !out || count < 1 || !problems || !params) return CUBO_PTYCHO_INVALID_INPUT;
+    *out = nullptr;
+    auto *b = new (std::nothrow) cubo_ptycho_batch();
+    if (!b) return CUBO_PTYCHO_OUT_OF_MEMORY;
+    b->ctx = ctx;
+    for (int i = 0; i < count; i++) {
+        cubo_ptycho_plan *p = nullptr;
+        const int st = cubo_ptycho_plan_create(ctx, &problems[i], &params[i], &p);
+        if (st != CUBO_PTYCHO_OK) {
+            const std::string msg = "reconstruction " + std::to_string(i) + ": " + ctx->last_error;
+            delete b;
+            ctx->last_error = msg;
+            return st;
+        }
+        b->plans.push_back(p);
+    }
+    *out = b;
+    return CUBO_PTYCHO_OK;
+}
+
+int cubo_ptycho_batch_destroy(cubo_ptycho_batch *b) {
+    if (!b) return CUBO_PTYCHO_OK;
+    cudaSetDevice(b->ctx->device);
+    cudaStreamSynchronize(b->ctx->stream);
+    delete b;
+    return CUBO_PTYCHO_OK;
+}
+
+int cubo_ptycho_batch_set_state(cubo_ptycho_batch *b, int index, const double *ore, const double *oim,
+                                const double *pre, const double *pim) {
+    if (!b || index < 0 || index >= (int)b->plans.size()) return CUBO_PTYCHO_INVALID_INPUT;
+    return cubo_ptycho_plan_set_state(b->plans[index], ore, oim, pre, pim);
+}
+
+int cubo_ptycho_batch_get_state(cubo_ptycho_batch *b, int index, double *ore, double *oim, double *pre, double *pim) {
+    if (!b || index < 0 || index >= (int)b->plans.size()) return CUBO_PTYCHO_INVALID_INPUT;
+    return cubo_ptycho_plan_get_state(b->plans[index], ore, oim, pre, pim);
+}
+
+int cubo_ptycho_batch_errors(cubo_ptycho_batch *b, int index, int count, double *errors) {
+    if (!b || index < 0 || index >= (int)b->plans.size()) return CUBO_PTYCHO_INVALID_INPUT;
+    return cubo_ptycho_plan_errors(b->plans[index], count, errors);
+}
+
+long long cubo_ptycho_batch_launches_per_iteration(const cubo_ptycho_batch *b) {
+    return b ? b->launches_per_iteration : -1;
+}
+
+int cubo_ptycho_batch_run(cubo_ptycho_batch *b, int iterations, int synchronize) {
+    if (!b) return CUBO_PTYCHO_INVALID_INPUT;
+    return run_guarded(b->ctx, [&] {
+        if (iterations < 0) fail(CUBO_PTYCHO_INVALID_INPUT, "iterations");
+        for (auto *p : b->plans) {
+            if (p->timing) fail(CUBO_PTYCHO_INVALID_INPUT, "timing is on for a plan of the batch");
+            ensure_errors(p, p->iterations_done + iterations);
+        }
+        bool stale = !b->exec || b->captured_errors.size() != b->plans.size();
+        for (size_t i = 0; !stale && i < b->plans.size(); i++) stale = b->captured_errors[i] != b->plans[i]->errors.ptr;
+        if (stale) capture_batch(b);
+        for (int it = 0; it < iterations; it++) check(cudaGraphLaunch(b->exec, b->ctx->stream), "cudaGraphLaunch");
+        for (auto *p : b->plans) {
+            p->iterations_done += iterations;
+            p->tape_valid = false;
+        }
+        if (synchronize) {
+            check(cudaStreamSynchronize(b->ctx->stream), "sync");
+            for (auto *p : b->plans) check_fault(p);
+        }
+    });
+}
+
 int cubo_ptycho_probe_build(cubo_ptycho_context *ctx, int rows, int columns, double row_sampling, double column_sampling,
                             double wavelength, double cutoff, double rolloff, double defocus, double astigmatism,
                             double astigmatism_angle, double spherical_aberration, int term_count, const double *terms,

@@ -234,7 +234,7 @@ cudaError_t launch_fft2_f64(const Fft2Plan64 &p, double2 *data, int batch, bool 
         fft_lines_kernel<<<(lines + lpb - 1) / lpb, kLineThreads, smem, s>>>(
             data, p.rows, p.columns, batch, cols, lpb, cols ? p.rad_rows : p.rad_columns,
             cols ? p.tw_rows : p.tw_columns, inverse);
-        e = cudaGetLastError();
+        const cudaError_t e = cudaGetLastError();
         if (e != cudaSuccess) return e;
     }
     return cudaSuccess;

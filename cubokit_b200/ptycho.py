@@ -323,6 +323,84 @@ class Plan:
             pass
 
 
+class Batch:
+    """Many independent reconstructions advanced together (``cubo_ptycho_batch_*``): one iteration of all of them is
+    captured once into a CUDA graph and replayed.
+
+    ``items`` is a list of dicts with ``amplitudes``, ``positions``, ``object``, ``probe`` and optional keyword
+    parameters of ``SingleslicePtychography.reconstruct`` (``step_size``, ``precision``, ...).
+    """
+
+    def __init__(self, items, ctx: Optional[Context] = None):
+        self.ctx = ctx or context(0)
+        keys = ("iterations", "step_size", "normalization_minimum", "fix_probe", "pure_phase_object",
+                "constrain_object_amplitude", "fix_probe_center_of_mass", "constrain_probe_amplitude",
+                "probe_amplitude_relative_radius", "probe_amplitude_relative_width", "fix_probe_aperture",
+                "probe_support_mask", "error_normalization", "position_correction", "precision", "variant")
+        defaults = dict(iterations=0, step_size=0.5, normalization_minimum=1.0, fix_probe=False,
+                        pure_phase_object=False, constrain_object_amplitude=True, fix_probe_center_of_mass=False,
+                        constrain_probe_amplitude=False, probe_amplitude_relative_radius=0.5,
+                        probe_amplitude_relative_width=0.05, fix_probe_aperture=False, probe_support_mask=None,
+                        error_normalization="suppliedAmplitudeEnergy", position_correction=None, precision="fp32",
+                        variant="auto")
+        self.inputs, self.shapes = [], []
+        for it in items:
+            kw = dict(defaults)
+            kw.update({k: v for k, v in it.items() if k in keys})
+            obj, prb = np.asarray(it["object"]), np.asarray(it["probe"])
+            self.inputs.append(_Inputs(it["amplitudes"], it["positions"], obj.shape, prb.shape, **kw))
+            self.shapes.append((obj.shape, prb.shape))
+        n = len(self.inputs)
+        problems = (L.Problem * n)(*[i.problem for i in self.inputs])
+        params = (L.Params * n)(*[i.params for i in self.inputs])
+        h = C.c_void_p()
+        self.ctx.check(self.ctx.lib.cubo_ptycho_batch_create(self.ctx.handle, n, problems, params, C.byref(h)))
+        self.handle = h
+        for i, it in enumerate(items):
+            self.set_state(i, it["object"], it["probe"])
+
+    def __len__(self):
+        return len(self.inputs)
+
+    def set_state(self, index, obj, probe):
+        os_, ps = self.shapes[index]
+        ore, oim = _split(obj, os_)
+        pre, pim = _split(probe, ps)
+        self.ctx.check(self.ctx.lib.cubo_ptycho_batch_set_state(self.handle, index, _ptr(ore), _ptr(oim), _ptr(pre),
+                                                                _ptr(pim)))
+
+    def get_state(self, index):
+        os_, ps = self.shapes[index]
+        no, npb = int(np.prod(os_)), int(np.prod(ps))
+        ore, oim, pre, pim = np.zeros(no), np.zeros(no), np.zeros(npb), np.zeros(npb)
+        self.ctx.check(self.ctx.lib.cubo_ptycho_batch_get_state(self.handle, index, _ptr(ore), _ptr(oim), _ptr(pre),
+                                                                _ptr(pim)))
+        return (ore + 1j * oim).reshape(os_), (pre + 1j * pim).reshape(ps)
+
+    def run(self, iterations: int, synchronize: bool = True):
+        self.ctx.check(self.ctx.lib.cubo_ptycho_batch_run(self.handle, iterations, 1 if synchronize else 0))
+
+    def errors(self, index, count):
+        out = np.zeros(max(count, 1))
+        self.ctx.check(self.ctx.lib.cubo_ptycho_batch_errors(self.handle, index, count, _ptr(out)))
+        return out[:count]
+
+    @property
+    def launches_per_iteration(self) -> int:
+        return int(self.ctx.lib.cubo_ptycho_batch_launches_per_iteration(self.handle))
+
+    def close(self):
+        if getattr(self, "handle", None):
+            self.ctx.lib.cubo_ptycho_batch_destroy(self.handle)
+            self.handle = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+
 class PtychographyProbe:
     """``PtychographyProbe.build`` (``Ptychography.swift:142-172``), evaluated on the device in FP64."""
 

@@ -162,6 +162,26 @@ CUBO_PTYCHO_API int cubo_ptycho_plan_backward(cubo_ptycho_plan *plan, int recomp
                                               double *grad_object_re, double *grad_object_im, double *grad_probe_re,
                                               double *grad_probe_im);
 
+/* ---- Batches: many independent reconstructions (each its own problem and parameters: scan, detector and object sizes
+ * may differ) advanced together.  One iteration of every reconstruction of the batch is captured once into a CUDA graph
+ * and replayed, so a run of the whole batch costs one graph launch per iteration.  No counterpart in the reference,
+ * which reconstructs one dataset per call.  Cancellation and progress hooks of the params are not used by batch runs. */
+typedef struct cubo_ptycho_batch cubo_ptycho_batch;
+CUBO_PTYCHO_API int cubo_ptycho_batch_create(cubo_ptycho_context *context, int count,
+                                             const cubo_ptycho_problem *problems, const cubo_ptycho_params *params,
+                                             cubo_ptycho_batch **out);
+CUBO_PTYCHO_API int cubo_ptycho_batch_destroy(cubo_ptycho_batch *batch);
+CUBO_PTYCHO_API int cubo_ptycho_batch_set_state(cubo_ptycho_batch *batch, int index, const double *object_re,
+                                                const double *object_im, const double *probe_re,
+                                                const double *probe_im);
+CUBO_PTYCHO_API int cubo_ptycho_batch_get_state(cubo_ptycho_batch *batch, int index, double *object_re,
+                                                double *object_im, double *probe_re, double *probe_im);
+/* Enqueues `iterations` replays of the captured iteration on the context stream; synchronize = 0 returns at once. */
+CUBO_PTYCHO_API int cubo_ptycho_batch_run(cubo_ptycho_batch *batch, int iterations, int synchronize);
+CUBO_PTYCHO_API int cubo_ptycho_batch_errors(cubo_ptycho_batch *batch, int index, int count, double *errors);
+/* Kernel launches one replay of the captured iteration contains. */
+CUBO_PTYCHO_API long long cubo_ptycho_batch_launches_per_iteration(const cubo_ptycho_batch *batch);
+
 /* Launch accounting of a plan: kernels launched since the plan was created, and, when timing is on, the device time of
  * each kernel kind summed over its launches (CUDA events on the context stream).  kinds/ms/launches have room for
  * `capacity` entries; *count receives the number of kinds filled in.  names are static strings. */

@@ -1,0 +1,38 @@
+"""Batches: independent reconstructions of different scan, detector and object sizes, replayed from one captured CUDA
+graph, give bitwise the results of running each reconstruction alone."""
+import numpy as np
+import pytest
+
+from tests import scenes
+
+pytestmark = pytest.mark.gpu
+
+
+def _items():
+    items = []
+    for scan, det, seed, prec in [(4, 32, 1, "fp32"), (6, 64, 2, "fp32"), (3, 128, 3, "fp32"), (3, 128, 4, "split_bf16"),
+                                  (5, 48, 5, "fp32"), (4, 64, 6, "fp64")]:
+        s = scenes.raster_scene(scan=scan, det=det, step=4, seed=seed)
+        items.append(dict(amplitudes=s["amplitudes"], positions=s["positions"], object=s["object"], probe=s["probe"],
+                          step_size=0.5, precision=prec))
+    s = scenes.nonsquare_scene(22, 21, 84)  # fractional positions, a Bluestein-length detector
+    items.append(dict(amplitudes=s["amplitudes"], positions=s["positions"], object=s["object"], probe=s["probe"],
+                      step_size=0.5, fix_probe_center_of_mass=True))
+    return items
+
+
+def test_batch_matches_individual_reconstructions_bitwise():
+    import cubokit_b200 as cb
+    items = _items()
+    batch = cb.Batch(items)
+    batch.run(2)
+    batch.run(1)  # a second run replays the same graph
+    assert batch.launches_per_iteration > len(items)
+    for i, it in enumerate(items):
+        kw = {k: v for k, v in it.items() if k not in ("amplitudes", "positions", "object", "probe")}
+        r = cb.SingleslicePtychography.reconstruct(it["amplitudes"], it["positions"], it["object"], it["probe"],
+                                                   iterations=3, **kw)
+        o, p = batch.get_state(i)
+        assert np.array_equal(o, r.object) and np.array_equal(p, r.probe), i
+        assert np.array_equal(batch.errors(i, 3), r.errors), i
+    batch.close()
