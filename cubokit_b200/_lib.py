@@ -36,7 +36,7 @@ class Params(C.Structure):
         ("fix_probe_aperture", C.c_int), ("probe_support_mask", C.POINTER(C.c_ubyte)),
         ("error_normalization", C.c_int), ("mean_intensity", C.c_double), ("has_position_correction", C.c_int),
         ("form", C.c_int), ("cancel", C.POINTER(C.c_int)), ("progress", PROGRESS_FN), ("progress_user", C.c_void_p),
-        ("variant", C.c_int),
+        ("variant", C.c_int), ("gather_tile", C.c_int),
     ]
 
 

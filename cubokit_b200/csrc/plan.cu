@@ -233,6 +233,7 @@ void validate(const cubo_ptycho_problem *pr, const cubo_ptycho_params *pp, doubl
                                                                                   : energy;
     if (!finite_positive(d)) fail(CUBO_PTYCHO_INVALID_INPUT, "error normalisation divisor");
     if (pp->form < CUBO_PTYCHO_FORM_FP32 || pp->form > CUBO_PTYCHO_FORM_FP64) fail(CUBO_PTYCHO_INVALID_INPUT, "form");
+    if (pp->gather_tile < 0 || pp->gather_tile > 3) fail(CUBO_PTYCHO_INVALID_INPUT, "gather tile");
     *divisor_out = d;
 }
 
@@ -272,7 +273,12 @@ void build_plan(cubo_ptycho_plan *p, const cubo_ptycho_problem *pr) {
     upload(p->cc, cc, s);
     upload(p->cls, cls, s);
     // ---- object-gather candidate lists: for each tile, the positions whose window touches it, ascending
-    if (p->bf16) { p->tile_w = kTileH; p->tile_h = kTileW; }  // the residual is stored [column][row]
+    // tile along the residual's contiguous axis: x for [row][column] residuals, y for [column][row] ones
+    const int choice = p->params.gather_tile;
+    const int wide = choice == 2 ? 16 : choice == 3 ? 64 : kTileW;
+    const int narrow = kGatherThreads / wide;
+    if (p->bf16) { p->tile_w = narrow; p->tile_h = wide; }
+    else { p->tile_w = wide; p->tile_h = narrow; }
     p->tiles_x = (p->OC + p->tile_w - 1) / p->tile_w;
     const int tiles_y = (p->OR + p->tile_h - 1) / p->tile_h;
     p->tiles = p->tiles_x * tiles_y;

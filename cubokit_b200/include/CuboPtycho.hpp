@@ -147,6 +147,7 @@ struct SingleslicePtychographyOptions {
     PtychographyErrorNormalization errorNormalization = PtychographyErrorNormalization::suppliedAmplitudeEnergy();
     bool positionCorrection = false;  // refused on the GPU path, as .single refuses it (Ptychography.swift:236)
     PtychographyPrecision precision = PtychographyPrecision::fp32;
+    int gatherTile = 0;  // object-gather tile choice (performance only), see cubo_ptycho_params.gather_tile
     std::function<bool()> isCancelled;
     std::function<void(int, int)> progress;
 };
@@ -196,6 +197,7 @@ struct SingleslicePtychography {
                                                           : CUBO_PTYCHO_ERRORS_SUPPLIED_AMPLITUDE_ENERGY;
         p.mean_intensity = o.errorNormalization.meanIntensityValue;
         p.has_position_correction = o.positionCorrection;
+        p.gather_tile = o.gatherTile;
         p.form = o.precision == PtychographyPrecision::fp64        ? CUBO_PTYCHO_FORM_FP64
                  : o.precision == PtychographyPrecision::splitBF16 ? CUBO_PTYCHO_FORM_SPLIT_BF16
                                                                    : CUBO_PTYCHO_FORM_FP32;

@@ -103,6 +103,10 @@ typedef struct {
     /* Kernel choice: CUBO_PTYCHO_VARIANT_AUTO picks the specialised kernel for the detector size when there is one;
      * CUBO_PTYCHO_VARIANT_GENERIC forces the any-size shared-memory transform (for cross-checks). */
     int variant;
+    /* Object-gather tile (pixels per CTA, 256 in all): 0 = default, 1 = 32 x 8, 2 = 16 x 16, 3 = 64 x 4 (width x height
+     * along the residual's contiguous axis).  A performance choice only: every pixel sums the same positions in the same
+     * order whatever the tile, so results are bitwise the same. */
+    int gather_tile;
 } cubo_ptycho_params;
 
 enum { CUBO_PTYCHO_VARIANT_AUTO = 0, CUBO_PTYCHO_VARIANT_GENERIC = 1 };

@@ -36,3 +36,21 @@ def test_batch_matches_individual_reconstructions_bitwise():
         assert np.array_equal(o, r.object) and np.array_equal(p, r.probe), i
         assert np.array_equal(batch.errors(i, 3), r.errors), i
     batch.close()
+
+
+def test_gather_tiles_agree_bitwise_and_autotune_picks_one(tmp_path, monkeypatch):
+    import cubokit_b200 as cb
+    from cubokit_b200 import autotune
+    monkeypatch.setenv("CUBOKIT_B200_CACHE", str(tmp_path))
+    for precision, det in (("fp32", 64), ("split_bf16", 128)):
+        s = scenes.raster_scene(scan=5, det=det, step=4, seed=8)
+        ref = None
+        for tile in (0, 1, 2, 3):
+            r = cb.SingleslicePtychography.reconstruct(s["amplitudes"], s["positions"], s["object"], s["probe"],
+                                                       iterations=2, precision=precision, gather_tile=tile)
+            if ref is None:
+                ref = r
+            assert np.array_equal(r.object, ref.object) and np.array_equal(r.errors, ref.errors), (precision, tile)
+        best, ms = autotune.tune(s["amplitudes"], s["positions"], s["object"], s["probe"], precision=precision)
+        assert best in autotune.CANDIDATES and set(ms) == {"32x8", "16x16", "64x4"}
+        assert autotune.tune(s["amplitudes"], s["positions"], s["object"], s["probe"], precision=precision)[0] == best
