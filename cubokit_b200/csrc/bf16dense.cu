@@ -33,7 +33,7 @@ constexpr int kN = 128;
 constexpr int kThreads = 256;
 constexpr uint32_t kSBO = 2048, kLBO = 128;     // canonical no-swizzle layout of a 128 x 128 bf16 plane
 constexpr int kPlaneBytes = kN * kN * 2;        // 32 KB
-constexpr uint32_t kWaitLimit = 1u << 22;       // mbarrier polls before giving up
+constexpr uint64_t kWaitLimit = 2000000000ull;  // ns of wall time an mbarrier wait may take before giving up
 
 __device__ __forceinline__ uint32_t kmajor_offset(int row, int k) {
     return (row >> 3) * kSBO + (k >> 3) * kLBO + (row & 7) * 16 + (k & 7) * 2;

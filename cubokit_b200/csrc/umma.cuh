@@ -80,10 +80,20 @@ __device__ __forceinline__ bool mbar_try_wait(uint64_t *mbar, uint32_t parity) {
     return ok != 0;
 }
 
-// Waits for the phase of parity `parity` to complete, at most `limit` polls; false when it ran out.
-__device__ __forceinline__ bool mbar_wait(uint64_t *mbar, uint32_t parity, uint32_t limit) {
-    for (uint32_t i = 0; i < limit; i++)
+__device__ __forceinline__ uint64_t globaltimer_ns() {
+    uint64_t t;
+    asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(t));
+    return t;
+}
+
+// Waits for the phase of parity `parity` to complete, for at most `limit_ns` nanoseconds of wall time (and at most
+// 2^30 polls); false when it ran out.
+__device__ __forceinline__ bool mbar_wait(uint64_t *mbar, uint32_t parity, uint64_t limit_ns) {
+    const uint64_t start = globaltimer_ns();
+    for (uint32_t i = 0; i < (1u << 30); i++) {
         if (mbar_try_wait(mbar, parity)) return true;
+        if ((i & 63) == 63 && globaltimer_ns() - start > limit_ns) return false;
+    }
     return false;
 }
 

@@ -193,7 +193,7 @@ class SingleslicePtychography:
                     position_correction=None, precision: str = "fp32",
                     is_cancelled: Optional[Callable[[], bool]] = None,
                     progress: Optional[Callable[[int, int], None]] = None, device: int = 0,
-                    variant: str = "auto") -> Result:
+                    variant: str = "auto", gather_tile: int = 0) -> Result:
         """Reconstructs from corner-centred amplitudes ``[position][row][column]``; see ``include/cubo_ptycho.h``.
 
         ``object`` and ``probe`` are complex 2-D arrays (``PtychographyArray``); ``positions`` is ``(P, 2)`` rows and
@@ -211,7 +211,7 @@ class SingleslicePtychography:
                       fix_probe, pure_phase_object, constrain_object_amplitude, fix_probe_center_of_mass,
                       constrain_probe_amplitude, probe_amplitude_relative_radius, probe_amplitude_relative_width,
                       fix_probe_aperture, probe_support_mask, error_normalization, position_correction, precision,
-                      variant)
+                      variant, gather_tile)
         if is_cancelled is not None and is_cancelled():
             raise CancellationError("cancelled")
         cb = None

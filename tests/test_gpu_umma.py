@@ -25,7 +25,7 @@ def _lib():
         subprocess.run([nvcc(), *ARCH, "-O2", "-std=c++17", "-shared", "-Xcompiler", "-fPIC",
                         "-I", str(ROOT / "cubokit_b200" / "csrc"), str(SRC), "-o", str(LIB)], check=True)
     lib = C.CDLL(str(LIB))
-    lib.umma_probe_complex.argtypes = [C.c_void_p, C.c_void_p, C.c_int, C.c_int, C.c_void_p]
+    lib.umma_probe_complex.argtypes = [C.c_void_p, C.c_void_p, C.c_int, C.c_int, C.c_int, C.c_void_p]
     lib.umma_probe_complex.restype = C.c_int
     return lib
 
@@ -61,7 +61,7 @@ def test_split_bf16_complex_product(mn_major, conj):
     wp, (wrh, wrl, wih, wil) = planes(w)
     bp, (brh, brl, bih, bil) = planes(b)
     out = np.zeros((2, n, n), np.float32)
-    st = lib.umma_probe_complex(wp.ctypes.data, bp.ctypes.data, int(mn_major), int(conj), out.ctypes.data)
+    st = lib.umma_probe_complex(wp.ctypes.data, bp.ctypes.data, int(mn_major), int(conj), 0, out.ctypes.data)
     assert st == 0, st
     mm = lambda p, q: p @ q
     s = -1.0 if conj else 1.0
@@ -78,3 +78,16 @@ def test_split_bf16_complex_product(mn_major, conj):
     exact = (np.conj(w) if conj else w) @ b
     rel = np.max(np.abs(out[0] + 1j * out[1] - exact)) / np.max(np.abs(exact))
     assert rel < 2e-5, rel
+
+
+def test_a_wait_that_nothing_completes_runs_out_with_a_status():
+    """The bounded-wait path: no MMA is issued and nothing arrives on the barrier; the kernel must give up after its
+    time limit (0.2 s here), free its tensor memory and report status 1, leaving the context usable."""
+    lib = _lib()
+    n = 128
+    planes = np.zeros((4, n, n), np.uint16)
+    out = np.zeros((2, n, n), np.float32)
+    assert lib.umma_probe_complex(planes.ctypes.data, planes.ctypes.data, 0, 0, 1, out.ctypes.data) == 1
+    # the context is still usable: a normal product right after
+    w = np.ones((4, n, n), np.uint16)
+    assert lib.umma_probe_complex(w.ctypes.data, w.ctypes.data, 0, 0, 0, out.ctypes.data) == 0
