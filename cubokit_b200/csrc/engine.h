@@ -65,11 +65,15 @@ struct Fast128Args {
     ScanTables scan;
     const float2 *shifted;
     const float2 *object;
-    const float *amplitudes;   // [positions][column][t][parity][s]
+    const float *amplitudes;   // [positions][column][h][t][e] (fast128.cu)
     float2 *dpsi;              // [positions][row][column]
     double *error;             // [positions][fast128_partials_per_position()]
     const float2 *tw128;       // W_128^t
+    float2 *partial_grad;      // [fast128_ctas()][n] probe-gradient partials, one per CTA
+    float *partial_weight;     // [fast128_ctas()][n]
+    int *fault;                // set when the amplitude prefetch wait ran out
 };
+int fast128_ctas();
 bool fast128_applicable(int rows, int columns);
 int fast128_partials_per_position();
 size_t fast128_smem();

@@ -17,7 +17,13 @@
 //    are free of bank conflicts); the group exchanges use a rotated slot order for the same reason.
 //  * The squared residual is summed per warp and written as 16 FP64 partials per position (reduced in a fixed order
 //    by the error kernels): no atomics, bitwise reproducible.
+//  * The next position's amplitudes are prefetched into shared memory by a bulk copy (no multicast) while the current
+//    one is transformed.
+//  * The probe gradient (conj(O[patch]) dpsi and |O|^2, Ptychography.swift:356-357) is accumulated here, in tensor
+//    memory: every thread owns 32 fixed detector pixels, so each CTA sums its positions in order and writes one
+//    partial; a fixed-order FP64 reduction over the 148 partials follows.  This replaces a second pass over dpsi.
 #include "engine.h"
+#include "umma.cuh"
 
 namespace cubo {
 
@@ -178,36 +184,69 @@ __device__ __forceinline__ void lines_inverse(float2 (&u0)[2][8], float2 (&u1)[2
 
 __device__ __forceinline__ int wrap_once(int v, int size) { return v < 0 ? v + size : (v >= size ? v - size : v); }
 
+// Tensor-memory columns of this thread's probe-gradient accumulators: 32 detector pixels (two lines x 16), real,
+// imaginary and weight planes of 32 columns each; the four warps that share a lane quadrant take 96 columns each.
+__device__ __forceinline__ uint32_t acc_base(uint32_t tmem, int warp) {
+    return umma::tmem_addr(tmem, 32 * (warp & 3), 96 * (warp >> 2));
+}
+
 __global__ void __launch_bounds__(kThreads, 1) fast128_kernel(Fast128Args a) {
     extern __shared__ __align__(16) float2 sm[];
     float2 *tw = sm + kN * kPitch;
+    float *amp_smem = reinterpret_cast<float *>(tw + kN);  // the current position's amplitudes, 64 KB
+    __shared__ uint64_t amp_bar;
+    __shared__ uint32_t tmem_base;
+    __shared__ int amp_fault;
     const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
     const int g = warp * 4 + (lane >> 3);  // this 8-thread group owns lines g and g + 64
     const int t = lane & 7;
     for (int i = tid; i < kN; i += kThreads) tw[i] = a.tw128[i];
+    if (warp == 0) {
+        umma::tmem_alloc(&tmem_base, 512);
+        umma::tmem_relinquish();
+    }
+    const int first = a.first + blockIdx.x;
+    if (tid == 0) {
+        umma::mbar_init(&amp_bar, 1);
+        asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+        amp_fault = 0;
+        if (first < a.first + a.count)
+            umma::bulk_load(amp_smem, a.amplitudes + (size_t)first * (kN * kN), kN * kN * sizeof(float), &amp_bar);
+    }
+    umma::fence_before_sync();
     __syncthreads();
+    umma::fence_after_sync();
+    const uint32_t acc = acc_base(tmem_base, warp);
+    {
+        const float zero[8] = {0, 0, 0, 0, 0, 0, 0, 0};
+#pragma unroll
+        for (int c = 0; c < 96; c += 8) umma::tmem_st8(acc + c, zero);
+        umma::tmem_wait_st();
+    }
     float2 *line[2] = {sm + g * kPitch, sm + (g + kLines) * kPitch};  // the group's own rows (scratch)
     const float inv_n = 1.0f / (float)(kN * kN);
-    for (int p = a.first + blockIdx.x; p < a.first + a.count; p += gridDim.x) {
+    uint32_t amp_phase = 0;
+    for (int p = first; p < a.first + a.count; p += gridDim.x) {
         const int rr = a.scan.rr[p], cc = a.scan.cc[p], cls = a.scan.cls[p];
         float2 x[2][16], u0[2][8], u1[2][8];
         // exit wave, rows g and g + 64, columns t + 8m (Ptychography.swift:321-336).  Column t + 8m lies left of the
         // centre for m >= 8 (corner offset t + 8m - 128); when the whole window is inside the object no wrap is needed.
         const bool interior = cc >= kN / 2 && cc + kN / 2 <= a.object_columns;
+        const float2 *orows[2];
 #pragma unroll
         for (int l = 0; l < 2; l++) {
             const int row = g + l * kLines;
             const float2 *S = a.shifted + (size_t)cls * (kN * kN) + row * kN;
-            const float2 *orow = a.object + (size_t)wrap_once(rr + (l == 0 ? row : row - kN), a.object_rows) * a.object_columns;
+            orows[l] = a.object + (size_t)wrap_once(rr + (l == 0 ? row : row - kN), a.object_rows) * a.object_columns;
             if (interior) {
-                const float2 *centre = orow + cc + t;
+                const float2 *centre = orows[l] + cc + t;
 #pragma unroll
                 for (int m = 0; m < 16; m++) x[l][m] = fm(S[t + 8 * m], centre[m < 8 ? 8 * m : 8 * m - kN]);
             } else {
 #pragma unroll
                 for (int m = 0; m < 16; m++) {
                     const int xc = wrap_once(cc + t + (m < 8 ? 8 * m : 8 * m - kN), a.object_columns);
-                    x[l][m] = fm(S[t + 8 * m], orow[xc]);
+                    x[l][m] = fm(S[t + 8 * m], orows[l][xc]);
                 }
             }
         }
@@ -226,14 +265,18 @@ __global__ void __launch_bounds__(kThreads, 1) fast128_kernel(Fast128Args a) {
             for (int m = 0; m < 16; m++) x[l][m] = sm[(t + 8 * m) * kPitch + g + l * kLines];
         __syncthreads();
         lines_forward(x, t, tw, line, u0, u1);
-        // projection (Ptychography.swift:338-349); line l holds F[2t + parity + 16s][g + 64 l]
+        // projection (Ptychography.swift:338-349); line l holds F[2t + parity + 16s][g + 64 l].  This position's
+        // amplitudes were prefetched into shared memory ([column][h][t][4]: float4 h of the 8 threads of a group is
+        // one 128-byte row, free of bank conflicts).
+        if (!umma::mbar_wait(&amp_bar, amp_phase, 2000000000ull)) amp_fault = 1;
+        amp_phase ^= 1u;
         double err = 0;
 #pragma unroll
         for (int l = 0; l < 2; l++) {
-            const float4 *A = reinterpret_cast<const float4 *>(a.amplitudes + ((size_t)p * kN + g + l * kLines) * kN + t * 16);
+            const float4 *A = reinterpret_cast<const float4 *>(amp_smem + (size_t)(g + l * kLines) * kN) + t;
 #pragma unroll
             for (int h = 0; h < 4; h++) {
-                const float4 av = A[h];
+                const float4 av = A[h * 8];
                 const float am[4] = {av.x, av.y, av.z, av.w};
 #pragma unroll
                 for (int e = 0; e < 4; e++) {
@@ -256,7 +299,10 @@ __global__ void __launch_bounds__(kThreads, 1) fast128_kernel(Fast128Args a) {
         if (lane == 0) a.error[(size_t)p * kWarps + warp] = err;
         // inverse column pass
         lines_inverse(u0, u1, t, tw, line, x);
-        __syncthreads();  // every group is done with its scratch rows before the columns are written back
+        __syncthreads();  // every group is done with its scratch rows (and the amplitude buffer) before reuse
+        if (tid == 0 && p + (int)gridDim.x < a.first + a.count)
+            umma::bulk_load(amp_smem, a.amplitudes + (size_t)(p + gridDim.x) * (kN * kN), kN * kN * sizeof(float),
+                            &amp_bar);
 #pragma unroll
         for (int l = 0; l < 2; l++)
 #pragma unroll
@@ -279,16 +325,68 @@ __global__ void __launch_bounds__(kThreads, 1) fast128_kernel(Fast128Args a) {
 #pragma unroll
             for (int m = 0; m < 16; m++) out[t + 8 * m] = x[l][m];
         }
+        // probe gradient (Ptychography.swift:356-357): conj(O[patch]) dpsi and |O|^2 added to this thread's 32 pixels,
+        // in tensor memory, in this CTA's position order
+#pragma unroll
+        for (int l = 0; l < 2; l++)
+#pragma unroll
+            for (int m0 = 0; m0 < 16; m0 += 8) {
+                float gr[8], gi[8], gw[8];
+                const uint32_t col = acc + l * 16 + m0;
+                umma::tmem_ld8(col, gr);
+                umma::tmem_ld8(col + 32, gi);
+                umma::tmem_ld8(col + 64, gw);
+                umma::tmem_wait_ld();
+#pragma unroll
+                for (int i = 0; i < 8; i++) {
+                    const int m = m0 + i;
+                    const int xc = interior ? cc + t + (m < 8 ? 8 * m : 8 * m - kN)
+                                            : wrap_once(cc + t + (m < 8 ? 8 * m : 8 * m - kN), a.object_columns);
+                    const float2 o = orows[l][xc], d = x[l][m];
+                    gr[i] += o.x * d.x + o.y * d.y;
+                    gi[i] += o.x * d.y - o.y * d.x;
+                    gw[i] += o.x * o.x + o.y * o.y;
+                }
+                umma::tmem_st8(col, gr);
+                umma::tmem_st8(col + 32, gi);
+                umma::tmem_st8(col + 64, gw);
+            }
+        umma::tmem_wait_st();
     }
+    // this CTA's probe-gradient partial, natural pixel order
+#pragma unroll
+    for (int l = 0; l < 2; l++)
+#pragma unroll
+        for (int m0 = 0; m0 < 16; m0 += 8) {
+            float gr[8], gi[8], gw[8];
+            const uint32_t col = acc + l * 16 + m0;
+            umma::tmem_ld8(col, gr);
+            umma::tmem_ld8(col + 32, gi);
+            umma::tmem_ld8(col + 64, gw);
+            umma::tmem_wait_ld();
+#pragma unroll
+            for (int i = 0; i < 8; i++) {
+                const int k = (g + l * kLines) * kN + t + 8 * (m0 + i);
+                a.partial_grad[(size_t)blockIdx.x * (kN * kN) + k] = make_float2(gr[i], gi[i]);
+                a.partial_weight[(size_t)blockIdx.x * (kN * kN) + k] = gw[i];
+            }
+        }
+    if (amp_fault && tid == 0) *a.fault = 1;
+    umma::fence_before_sync();
+    __syncthreads();
+    umma::fence_after_sync();
+    if (warp == 0) umma::tmem_dealloc(tmem_base, 512);
 }
 
-// [position][row][column] -> [position][column][t][parity][s] with row = 2t + parity + 16s.
+// [position][row][column] -> [position][column][h][t][e]: element j = 4h + e (j = parity * 8 + s) of thread t of the
+// column's group, row = 2t + parity + 16s.
 __global__ void permute_amplitudes_kernel(const float *in, float *out, long long positions) {
     const long long i = (long long)blockIdx.x * 256 + threadIdx.x;
     if (i >= positions * kN * kN) return;
     const long long p = i / (kN * kN);
     const int rem = (int)(i - p * kN * kN);
-    const int column = rem >> 7, t = (rem >> 4) & 7, j = rem & 15;
+    const int column = rem >> 7, h = (rem >> 5) & 3, t = (rem >> 2) & 7, e = rem & 3;
+    const int j = 4 * h + e;
     const int row = 2 * t + (j >> 3) + 16 * (j & 7);
     out[i] = in[p * kN * kN + row * kN + column];
 }
@@ -299,7 +397,9 @@ bool fast128_applicable(int rows, int columns) { return rows == kN && columns ==
 
 int fast128_partials_per_position() { return kWarps; }
 
-size_t fast128_smem() { return (size_t)(kN * kPitch + kN) * sizeof(float2); }
+size_t fast128_smem() { return (size_t)(kN * kPitch + kN) * sizeof(float2) + (size_t)kN * kN * sizeof(float); }
+
+int fast128_ctas() { return 148; }  // fixed, so the probe-gradient summation order does not depend on the device
 
 cudaError_t configure_fast128() {
     int device = 0, optin = 0;
@@ -313,7 +413,8 @@ cudaError_t configure_fast128() {
 
 cudaError_t launch_fast128(const Fast128Args &a, int ctas, cudaStream_t s) {
     if (a.count <= 0) return cudaSuccess;
-    const int grid = a.count < ctas ? a.count : ctas;
+    (void)ctas;
+    const int grid = a.count < fast128_ctas() ? a.count : fast128_ctas();
     fast128_kernel<<<grid, kThreads, fast128_smem(), s>>>(a);
     return cudaGetLastError();
 }

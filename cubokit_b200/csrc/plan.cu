@@ -337,6 +337,10 @@ void build_plan(cubo_ptycho_plan *p, const cubo_ptycho_problem *pr) {
     check(p->dpsi.alloc((size_t)P * n * sizeof(C2<T>)), "cudaMalloc dpsi");
     p->error_count = p->fast ? (long long)P * fast128_partials_per_position()
                              : p->bf16 ? (long long)P * bf16_partials_per_position() : P;
+    if (p->fast) {
+        check(p->fault.alloc(sizeof(int)), "cudaMalloc");
+        check(cudaMemsetAsync(p->fault.ptr, 0, sizeof(int), s), "memset");
+    }
     if (p->bf16) {
         // the 128-point DFT matrix split into bf16 hi + lo, evaluated in FP64: planes Re hi, Re lo, Im hi, Im lo, [m][k]
         std::vector<uint16_t> planes(4 * (size_t)n);
@@ -383,6 +387,7 @@ void build_plan(cubo_ptycho_plan *p, const cubo_ptycho_problem *pr) {
     // order (and the result) does not depend on the device
     const int kblocks = (n + 255) / 256;
     p->groups = std::max(1, std::min(P, (148 * 8 + kblocks - 1) / kblocks));
+    if (p->fast) p->groups = std::min(P, fast128_ctas());  // the position pass writes one partial per CTA
     check(p->partial_grad.alloc((size_t)p->groups * n * sizeof(C2<T>)), "cudaMalloc");
     check(p->partial_weight.alloc((size_t)p->groups * n * sizeof(T)), "cudaMalloc");
     check(p->grad_p64.alloc((size_t)n * sizeof(double2)), "cudaMalloc");
@@ -414,12 +419,12 @@ Fft2Plan64 fft64(const cubo_ptycho_plan *p) {
 
 // After a synchronize: a device wait that ran out (split-BF16 kernel) turns into CUBO_PTYCHO_DEVICE_TIMEOUT.
 void check_fault(cubo_ptycho_plan *p) {
-    if (!p->bf16) return;
+    if (!p->bf16 && !p->fast) return;
     int f = 0;
     check(cudaMemcpy(&f, p->fault.ptr, sizeof(int), cudaMemcpyDeviceToHost), "read fault flag");
     if (f) {
         cudaMemset(p->fault.ptr, 0, sizeof(int));
-        fail(CUBO_PTYCHO_DEVICE_TIMEOUT, "a tensor-core completion wait ran out on the device");
+        fail(CUBO_PTYCHO_DEVICE_TIMEOUT, "a device-side completion wait ran out");
     }
 }
 
@@ -539,6 +544,8 @@ void enqueue_position_pass(cubo_ptycho_plan *p) {
         fa.shifted = p->shifted.as<float2>(); fa.object = p->object.as<float2>();
         fa.amplitudes = p->amplitudes.as<float>(); fa.dpsi = p->dpsi.as<float2>(); fa.error = p->error.as<double>();
         fa.tw128 = p->tw_r.as<float2>();
+        fa.partial_grad = p->partial_grad.as<float2>(); fa.partial_weight = p->partial_weight.as<float>();
+        fa.fault = p->fault.as<int>();
         timed(p, kPositionPass, 1, [&] { return launch_fast128(fa, p->sms, s); });
     } else {
         timed(p, kPositionPass, 1, [&] { return launch_position_pass<T>(pa, s); });
@@ -562,7 +569,8 @@ void enqueue_gathers(cubo_ptycho_plan *p) {
     pg.rows = p->R; pg.columns = p->C; pg.object_rows = p->OR; pg.object_columns = p->OC; pg.n = n;
     pg.count = p->P; pg.groups = p->groups; pg.scan = scan; pg.object = p->object.as<C2<T>>();
     pg.dpsi = p->dpsi.as<C2<T>>(); pg.dpsi_transposed = p->bf16; pg.partial_grad = p->partial_grad.as<C2<T>>(); pg.partial_weight = p->partial_weight.as<T>();
-    timed(p, kProbeGather, 1, [&] { return launch_probe_gather<T>(pg, s); });
+    if (!p->fast)  // the 128 x 128 FP32 position pass already wrote per-CTA probe partials
+        timed(p, kProbeGather, 1, [&] { return launch_probe_gather<T>(pg, s); });
     timed(p, kProbeReduce, 1, [&] {
         return launch_probe_reduce<T>(p->partial_grad.as<C2<T>>(), p->partial_weight.as<T>(), p->groups, n,
                                       p->grad_p64.as<double2>(), p->weight_p64.as<double>(),
