@@ -1,25 +1,35 @@
-// The split-BF16 position pass for a 128 x 128 detector: the 2-D DFT pair as DFT-matrix products on the tensor cores.
+// The split-BF16 position pass for a 128 x 128 detector: the 2-D DFT pair as products with a real 128 x 128 matrix on
+// the tensor cores.
 //
-// Arithmetic (Ptychography.swift:321-350): exit wave X = S * O[patch], F = W X W (W the symmetric 128-point DFT matrix,
-// unnormalised), the Fourier-modulus projection with the 1/n of ifft2 folded in, then dpsi = conj(W) F' conj(W).
-// Every product is a left multiplication D = W * B with the DFT matrix as the A operand, kept in tensor memory for the
-// whole kernel (re hi, re lo, im hi, im lo: 4 x 64 columns), and the data as the B operand in shared memory:
+// Arithmetic (Ptychography.swift:321-350): exit wave X = S * O[patch], F = fft2(X), the Fourier-modulus projection with
+// the 1/n of ifft2 folded in, then dpsi = ifft2(F').  The 128-point DFT matrix factors as W = T C with C real:
 //
-//   stage 1  D = W X^T      = Y^T    (Y = X W, the row transform)      B = X     K-major, row r of X per lane r
-//   stage 2  D = W Y        = F                                        B = Y     K-major, row k of Y^T per lane k
-//   stage 3  D = conj(W) F' = Y'                                       B = F'    MN-major, row k of F' per lane k
-//   stage 4  D = conj(W) Y'^T = dpsi^T                                 B = Y'^T  K-major, row r of Y' per lane r
+//   C row 0 = 1, row 1 = cos(pi k), rows 2j and 2j + 1 = cos(2 pi j k / 128) and sin(2 pi j k / 128)  (j = 1..63)
 //
-// so no stage needs a transpose: each TMEM lane's row of one stage's result is written, split into bf16 hi and lo, as
-// one contiguous row of the next stage's B operand.  Each real product P Q is P_hi Q_hi + P_hi Q_lo + P_lo Q_hi (the
-// lo * lo term is below FP32 resolution of the sum), accumulated in FP32 in tensor memory: 12 streams x 8 K-steps = 96
-// tcgen05.mma (M = N = 128, K = 16) per stage, issued by one thread and completed through an mbarrier.  Signs of conj(W)
-// and of the - Wi Bi term come from the instruction descriptor's negate bit.
+// and T combining row pairs: for z = C x, (W x)[j] = z[2j] - i z[2j+1] and (W x)[128 - j] = z[2j] + i z[2j+1]
+// ((W x)[0] = z[0], (W x)[64] = z[1]); conj(W) swaps the two.  Every transform is therefore the real product D = C B of
+// the re and the im plane separately, half the multiply-adds of a complex DFT matrix, and T is applied only where a
+// stage's result is needed in the frequency or pixel basis: on a row of D inside one thread, and between the rows of
+// TMEM lanes 2j and 2j + 1 (adjacent lanes of a warp) with one shuffle per value.  With D[m][n] = sum_k A[m][k] B[n][k]
+// (A = C or C_sigma in tensor memory, B = data in shared memory):
 //
-// One persistent CTA of 256 threads per SM: thread (warp w, lane i) owns TMEM lane 32 (w mod 4) + i and column half
-// w / 4.  The residual is written transposed ([position][column][row]); the amplitudes are read in 16-float chunks
-// ([position][column / 16][row][column mod 16]) so a warp reads 2 KB contiguously.  Waits are bounded: a wait that runs
-// out sets *fault and the CTA stops after freeing its tensor memory.
+//   stage 1  B[n = r][k = c]   = X                       K-major   D[raw c][r]
+//   stage 2  B[n = raw c][k = r] = D1                    K-major   D[raw r][raw c]  -> T both ways -> F[kr][kc]
+//   stage 3  B[n = pos][k = kr] = F'[kr][sigma(pos)]     MN-major  D[raw r][pos]
+//   stage 4  B[n = raw r][k = pos] = D3, A = C_sigma     K-major   D[raw c][raw r]  -> T both ways -> dpsi[r][c]
+//
+// sigma orders the frequencies kc the way one thread holds them after T (8 consecutive positions per thread and
+// row), and C_sigma[m][pos] = C[m][sigma(pos)] contracts over them in that order.  Each real product P Q is
+// P_hi Q_hi + P_hi Q_lo + P_lo Q_hi in bf16 with FP32 accumulation in tensor memory: 3 x 8 K-steps = 24 tcgen05.mma
+// (M = N = 128, K = 16) per plane and stage.  The two planes run as a pipeline: the re plane's result is read out and
+// its next stage issued while the tensor core still works on the im plane.
+//
+// One persistent CTA of 512 threads per SM with 192 KB of shared memory: the four B planes and the next position's
+// amplitudes, bulk-copied in behind stages 3 to 2.  Tensor memory: C hi / lo (columns 0-127), C_sigma hi / lo (128-255), the
+// re-plane result (256-383), the im-plane result (384-511).  Thread (warp w, lane i) owns TMEM lane 32 (w mod 4) + i and
+// the 32-column group w / 4 of each result.  Amplitudes are pre-permuted into the order each thread consumes them
+// (a warp reads 512 contiguous bytes per load); dpsi is written [position][row][column].  Waits are bounded: a wait
+// that runs out sets *fault and the CTA stops after freeing its tensor memory.
 #include "engine.h"
 #include "umma.cuh"
 
@@ -30,10 +40,13 @@ namespace {
 using namespace umma;
 
 constexpr int kN = 128;
-constexpr int kThreads = 256;
+constexpr int kThreads = 512;
 constexpr uint32_t kSBO = 2048, kLBO = 128;     // canonical no-swizzle layout of a 128 x 128 bf16 plane
 constexpr int kPlaneBytes = kN * kN * 2;        // 32 KB
 constexpr uint64_t kWaitLimit = 2000000000ull;  // ns of wall time an mbarrier wait may take before giving up
+constexpr uint32_t kCNat = 0, kCSigma = 128, kSlotRe = 256, kSlotIm = 384;  // tensor-memory columns
+constexpr int kReHi = 0, kImHi = 2;             // B planes: re hi, re lo, im hi, im lo
+constexpr uint32_t kIdescK = idesc_bf16(128, 128, false, false), kIdescMN = idesc_bf16(128, 128, false, true);
 
 __device__ __forceinline__ uint32_t kmajor_offset(int row, int k) {
     return (row >> 3) * kSBO + (k >> 3) * kLBO + (row & 7) * 16 + (k & 7) * 2;
@@ -44,238 +57,375 @@ __device__ __forceinline__ uint32_t mnmajor_offset(int k, int col) {
 
 __device__ __forceinline__ int wrap_once(int v, int size) { return v < 0 ? v + size : (v >= size ? v - size : v); }
 
-// Writes 8 consecutive K (or MN) values, split into hi and lo, of one row of the four B planes (16 bytes per plane).
-// re/im hold 8 values; `off` is the byte offset of the chunk inside a plane.
-__device__ __forceinline__ void store_chunk(uint8_t *planes, uint32_t off, const float (&re)[8], const float (&im)[8]) {
-    uint32_t rh[4], rl[4], ih[4], il[4];
+// The frequency paired with j by T: 128 - j, and 64 for j = 0.
+__host__ __device__ __forceinline__ int mirror(int j) { return j == 0 ? 64 : kN - j; }
+
+// Writes 8 consecutive K (or MN) values of one row, split into bf16 hi and lo, into planes hi_plane and hi_plane + 1.
+__device__ __forceinline__ void store_split8(uint8_t *planes, int hi_plane, uint32_t off, const float (&v)[8]) {
+    uint32_t h[4], l[4];
 #pragma unroll
-    for (int i = 0; i < 4; i++) {
-        split_bf16x2(re[2 * i], re[2 * i + 1], rh[i], rl[i]);
-        split_bf16x2(im[2 * i], im[2 * i + 1], ih[i], il[i]);
-    }
-    *reinterpret_cast<uint4 *>(planes + 0 * kPlaneBytes + off) = make_uint4(rh[0], rh[1], rh[2], rh[3]);
-    *reinterpret_cast<uint4 *>(planes + 1 * kPlaneBytes + off) = make_uint4(rl[0], rl[1], rl[2], rl[3]);
-    *reinterpret_cast<uint4 *>(planes + 2 * kPlaneBytes + off) = make_uint4(ih[0], ih[1], ih[2], ih[3]);
-    *reinterpret_cast<uint4 *>(planes + 3 * kPlaneBytes + off) = make_uint4(il[0], il[1], il[2], il[3]);
+    for (int i = 0; i < 4; i++) split_bf16x2(v[2 * i], v[2 * i + 1], h[i], l[i]);
+    *reinterpret_cast<uint4 *>(planes + hi_plane * kPlaneBytes + off) = make_uint4(h[0], h[1], h[2], h[3]);
+    *reinterpret_cast<uint4 *>(planes + (hi_plane + 1) * kPlaneBytes + off) = make_uint4(l[0], l[1], l[2], l[3]);
 }
 
-// The 96 MMAs of one stage, D (re at d, im at d + 128) = (conj?)W * B.
-__device__ __forceinline__ void issue_stage(uint32_t tmem, uint32_t planes_smem, bool conj, bool b_mn_major) {
-    // (destination 0 re / 1 im, W plane, B plane, negative)
-    constexpr int prod[12][4] = {{0, 0, 0, 0}, {0, 0, 1, 0}, {0, 1, 0, 0},   // + Wr Br
-                                 {0, 2, 2, 1}, {0, 2, 3, 1}, {0, 3, 2, 1},   // - Wi Bi
-                                 {1, 0, 2, 0}, {1, 0, 3, 0}, {1, 1, 2, 0},   // + Wr Bi
-                                 {1, 2, 0, 0}, {1, 2, 1, 0}, {1, 3, 0, 0}};  // + Wi Br
-#pragma unroll 1
-    for (int s = 0; s < kN / 16; s++) {
+// The 24 MMAs of one plane: D (columns d_col) = A (hi at a_col, lo at a_col + 64) * B (planes b_hi, b_hi + 32 KB).
+__device__ __forceinline__ void issue_plane(uint32_t tmem, uint32_t a_col, uint32_t d_col, uint32_t b_hi, uint32_t idesc) {
 #pragma unroll
-        for (int i = 0; i < 12; i++) {
-            const bool neg = (prod[i][3] != 0) != (conj && prod[i][1] >= 2);
-            const uint32_t idesc = idesc_bf16(128, 128, false, b_mn_major, false, neg);
-            const uint64_t bdesc = smem_desc(planes_smem + prod[i][2] * kPlaneBytes + s * 2 * kLBO, kLBO, kSBO);
-            mma_ts(tmem + 256 + prod[i][0] * 128, tmem + prod[i][1] * 64 + s * 8, bdesc, idesc,
-                   (s > 0 || (i % 6) != 0) ? 1u : 0u);
-        }
+    for (int s = 0; s < kN / 16; s++) {
+        const uint64_t dh = smem_desc(b_hi + s * 2 * kLBO, kLBO, kSBO);
+        const uint64_t dl = smem_desc(b_hi + kPlaneBytes + s * 2 * kLBO, kLBO, kSBO);
+        mma_ts(tmem + d_col, tmem + a_col + s * 8, dh, idesc, s > 0 ? 1u : 0u);
+        mma_ts(tmem + d_col, tmem + a_col + s * 8, dl, idesc, 1u);
+        mma_ts(tmem + d_col, tmem + a_col + 64 + s * 8, dh, idesc, 1u);
     }
+}
+
+// Lane `row`'s 32 columns of one result (from taddr) -> 32 consecutive K of row `row` of a K-major B plane pair.
+__device__ __forceinline__ void readout_kmajor(uint32_t taddr, uint8_t *planes, int hi_plane, int row, int k0) {
+    float a[16], b[16];
+    tmem_ld16(taddr, a);
+    tmem_ld16(taddr + 16, b);
+    tmem_wait_ld();
+#pragma unroll
+    for (int c = 0; c < 2; c++) {
+        float v0[8], v1[8];
+#pragma unroll
+        for (int i = 0; i < 8; i++) { v0[i] = a[8 * c + i]; v1[i] = b[8 * c + i]; }
+        store_split8(planes, hi_plane, kmajor_offset(row, k0 + 8 * c), v0);
+        store_split8(planes, hi_plane, kmajor_offset(row, k0 + 16 + 8 * c), v1);
+    }
+}
+
+// T on the columns of one lane: raw pairs (zc, zs) = columns (2J, 2J+1) -> the values at J (y0) and mirror(J) (y1).
+// Forward: y0 = zc - i zs, y1 = zc + i zs; inverse the other way round; J = 0 passes (z0, z1) through.
+template <bool kInverse>
+__device__ __forceinline__ void combine(float zr, float zi, float sr, float si, bool passthrough, float &y0r, float &y0i,
+                                        float &y1r, float &y1i) {
+    if (passthrough) {
+        y0r = zr; y0i = zi; y1r = sr; y1i = si;
+    } else if (!kInverse) {
+        y0r = zr + si; y0i = zi - sr; y1r = zr - si; y1i = zi + sr;
+    } else {
+        y0r = zr - si; y0i = zi + sr; y1r = zr + si; y1i = zi - sr;
+    }
+}
+
+// One thread's 16 values of a combined stage result for sub-block u: T on the columns (in the thread), then the
+// exchange with lane L ^ 1, then T on the row pair (2j, 2j + 1).  out[side][s][i] is the value at row
+// (side ? mirror(j) : j) and column (s ? mirror(J) : J), J = 16 g + 8 h + 4 u + i, h = L & 1.
+template <bool kInverse>
+__device__ __forceinline__ void combined_block(uint32_t lane_addr, int g, int u, int j, int h, float (&out_re)[2][8],
+                                               float (&out_im)[2][8]) {
+    float r0[8], r1[8], i0[8], i1[8];  // raw columns of parity sets 0 and 1: 32 g + 16 h' + 8 u .. + 8
+    tmem_ld8(lane_addr + kSlotRe + 32 * g + 8 * u, r0);
+    tmem_ld8(lane_addr + kSlotRe + 32 * g + 16 + 8 * u, r1);
+    tmem_ld8(lane_addr + kSlotIm + 32 * g + 8 * u, i0);
+    tmem_ld8(lane_addr + kSlotIm + 32 * g + 16 + 8 * u, i1);
+    tmem_wait_ld();
+    // T on the columns for both parity sets: ya / yb [s][i] (complex as re, im)
+    float ar[2][4], ai[2][4], br[2][4], bi[2][4];
+    const bool first = g == 0 && u == 0;  // J = 0 sits at i = 0 of parity set 0
+#pragma unroll
+    for (int i = 0; i < 4; i++) {
+        combine<kInverse>(r0[2 * i], i0[2 * i], r0[2 * i + 1], i0[2 * i + 1], first && i == 0, ar[0][i], ai[0][i],
+                          ar[1][i], ai[1][i]);
+        combine<kInverse>(r1[2 * i], i1[2 * i], r1[2 * i + 1], i1[2 * i + 1], false, br[0][i], bi[0][i], br[1][i],
+                          bi[1][i]);
+    }
+    // keep the own parity set, send the other: afterwards `mine` is lane L's row and `theirs` lane L ^ 1's, both for
+    // the columns of set h
+#pragma unroll
+    for (int s = 0; s < 2; s++)
+#pragma unroll
+        for (int i = 0; i < 4; i++) {
+            const float mr = h ? br[s][i] : ar[s][i], mi = h ? bi[s][i] : ai[s][i];
+            const float sr = h ? ar[s][i] : br[s][i], si = h ? ai[s][i] : bi[s][i];
+            const float tr = __shfl_xor_sync(0xffffffffu, sr, 1), ti = __shfl_xor_sync(0xffffffffu, si, 1);
+            // a = row 2j, b = row 2j + 1
+            const float a_r = h ? tr : mr, a_i = h ? ti : mi, b_r = h ? mr : tr, b_i = h ? mi : ti;
+            float y0r, y0i, y1r, y1i;
+            combine<kInverse>(a_r, a_i, b_r, b_i, j == 0, y0r, y0i, y1r, y1i);
+            out_re[0][4 * s + i] = y0r; out_im[0][4 * s + i] = y0i;
+            out_re[1][4 * s + i] = y1r; out_im[1][4 * s + i] = y1i;
+        }
 }
 
 __global__ void __launch_bounds__(kThreads, 1) bf16_position_kernel(Bf16Args a) {
-    extern __shared__ __align__(1024) uint8_t planes[];  // 4 x 32 KB: the B operand
-    __shared__ uint64_t mbar;
+    extern __shared__ __align__(1024) uint8_t planes[];  // 4 x 32 KB: the B operand, then 64 KB of amplitudes
+    __shared__ uint64_t mbar[2];                         // completion of the re / im plane's MMAs
+    __shared__ uint64_t amp_bar;                         // arrival of the next position's amplitudes
     __shared__ uint32_t tmem_base;
-    __shared__ int stop;
     const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
-    const int row = 32 * (warp & 3) + lane;  // this thread's TMEM lane
-    const int half = warp >> 2;              // its half of the columns
+    const int q = warp & 3, g = warp >> 2;
+    const int L = 32 * q + lane;      // this thread's TMEM lane
+    const int j = L >> 1, h = L & 1;  // its row pair and parity
     if (warp == 0) {
         tmem_alloc(&tmem_base, 512);
         tmem_relinquish();
     }
     if (tid == 0) {
-        mbar_init(&mbar, 1);
+        mbar_init(&mbar[0], 1);
+        mbar_init(&mbar[1], 1);
+        mbar_init(&amp_bar, 1);
         asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
-        stop = 0;
     }
     fence_before_sync();
     __syncthreads();
     fence_after_sync();
     const uint32_t tmem = tmem_base;
-    const uint32_t lane_addr = tmem_addr(tmem, 32 * (warp & 3), 0);
-    const uint32_t planes_smem = smem_u32(planes);
-    // W planes into tensor memory: plane q at columns 64 q, lane m = row m, column j = W[m][2j] | W[m][2j+1] << 16
-    for (int q = 0; q < 4; q++)
-        for (int c0 = 0; c0 < 32; c0 += 16) {
-            uint32_t r[16];
-            const uint32_t *src = reinterpret_cast<const uint32_t *>(a.w_planes + ((size_t)q * kN + row) * kN) + 32 * half + c0;
+    const uint32_t lane_addr = tmem_addr(tmem, 32 * q, 0);
+    const uint32_t smem = smem_u32(planes);
+    float4 *amp_smem = reinterpret_cast<float4 *>(planes + 4 * kPlaneBytes);
+    const int last = a.first + a.count;
+    bool amp_pending = a.first + (int)blockIdx.x < last;  // a bulk copy of amplitudes is in flight
+    if (tid == 0 && amp_pending)
+        bulk_load(amp_smem, a.amplitudes + (size_t)(a.first + blockIdx.x) * (kN * kN), kN * kN * 4, &amp_bar);
+    uint32_t amp_phase = 0;
+    // C hi, C lo, C_sigma hi, C_sigma lo into tensor memory: plane v at columns 64 v, lane m, column c = the bf16 pair
+    // (k = 2c, 2c + 1) of row m
+#pragma unroll 1
+    for (int v = 0; v < 4; v++) {
+        uint32_t r[16];
+        const uint32_t *src = reinterpret_cast<const uint32_t *>(a.c_planes + ((size_t)v * kN + L) * kN) + 16 * g;
 #pragma unroll
-            for (int j = 0; j < 16; j++) r[j] = src[j];
-            tmem_st16(lane_addr + q * 64 + 32 * half + c0, r);
-        }
+        for (int i = 0; i < 16; i++) r[i] = src[i];
+        tmem_st16(lane_addr + 64 * v + 16 * g, r);
+    }
     tmem_wait_st();
-    uint32_t phase = 0;
-    const float inv_n = 1.0f / (float)(kN * kN);
-    // one stage's MMAs after the B operand is in shared memory; false when the wait ran out
-    auto run_stage = [&](bool conj, bool mn_major) -> bool {
-        fence_proxy_async();
-        fence_before_sync();
-        __syncthreads();
-        if (tid == 0) {
-            fence_after_sync();
-            issue_stage(tmem, planes_smem, conj, mn_major);
-            mma_commit(&mbar);
-        }
-        const bool ok = mbar_wait(&mbar, phase, kWaitLimit);
-        if (ok) phase ^= 1u;  // on a timeout `phase` keeps the parity still outstanding, for the drain below
-        else {
-            stop = 1;
+    uint32_t phase[2] = {0u, 0u};
+    bool pending[2] = {false, false};
+    bool bad = false;
+    // waits for plane x's MMAs; a wait that runs out marks this thread bad and raises the fault flag
+    auto wait_plane = [&](int x) {
+        if (mbar_wait(&mbar[x], phase[x], kWaitLimit)) {
+            phase[x] ^= 1u;
+            pending[x] = false;
+        } else {
+            bad = true;
             *a.fault = 1;
         }
         fence_after_sync();
-        return ok;
     };
-    for (int p = a.first + blockIdx.x; p < a.first + a.count; p += gridDim.x) {
-        // ---- stage 1: B = X (row `row` of the exit wave, columns of this half), K-major
+    // publishes this thread's B-operand writes and tensor-memory reads; false (for every thread) when any thread is bad
+    auto publish = [&]() -> bool {
+        fence_proxy_async();
+        fence_before_sync();
+        const int any_bad = __syncthreads_or(bad ? 1 : 0);
+        fence_after_sync();
+        return any_bad == 0;
+    };
+    const float inv_n = 1.0f / (float)(kN * kN);
+    for (int p = a.first + blockIdx.x; p < last; p += gridDim.x) {
+        // ---- stage 1: B[n = r][k = c] = X, 4 chunks of 8 columns per thread (a warp: 8 rows x 4 chunks), two at a
+        // time with every load of both issued before the first product
         {
             const int rr = a.scan.rr[p], cc = a.scan.cc[p], cls = a.scan.cls[p];
-            const float2 *S = a.shifted + (size_t)cls * (kN * kN) + row * kN;
-            const float2 *orow = a.object + (size_t)wrap_once(rr + (row < kN / 2 ? row : row - kN), a.object_rows) * a.object_columns;
+            const float2 *S = a.shifted + (size_t)cls * (kN * kN);
 #pragma unroll 1
-            for (int c8 = 64 * half; c8 < 64 * half + 64; c8 += 8) {
-                float re[8], im[8];
+            for (int it = 0; it < 4; it += 2) {
+                float4 sv[2][4];
+                float2 ov[2][8];
+                int rows[2], cols[2];
 #pragma unroll
-                for (int i = 0; i < 8; i++) {
-                    const int c = c8 + i;
-                    const int x = wrap_once(cc + (c < kN / 2 ? c : c - kN), a.object_columns);
-                    const float2 s = S[c], o = orow[x];
-                    re[i] = s.x * o.x - s.y * o.y;
-                    im[i] = s.x * o.y + s.y * o.x;
-                }
-                store_chunk(planes, kmajor_offset(row, c8), re, im);
-            }
-        }
-        run_stage(false, false);
-        __syncthreads();
-        if (stop) break;
-        // ---- stage 2: B = Y, K-major [k][r]: lane k's row of Y^T
-#pragma unroll 1
-        for (int c16 = 64 * half; c16 < 64 * half + 64; c16 += 16) {
-            float re[16], im[16];
-            tmem_ld16(lane_addr + 256 + c16, re);
-            tmem_ld16(lane_addr + 384 + c16, im);
-            tmem_wait_ld();
-            float r0[8], i0[8], r1[8], i1[8];
+                for (int b = 0; b < 2; b++) {
+                    const int ch = kThreads * (it + b) + tid;
+                    const int r = 8 * (ch >> 7) + (ch & 7), c8 = 8 * ((ch >> 3) & 15);
+                    rows[b] = r;
+                    cols[b] = c8;
+                    const float2 *orow =
+                        a.object + (size_t)wrap_once(rr + (r < kN / 2 ? r : r - kN), a.object_rows) * a.object_columns;
+                    const int x0 = cc + (c8 < kN / 2 ? c8 : c8 - kN);
+                    const float4 *s4 = reinterpret_cast<const float4 *>(S + r * kN + c8);
 #pragma unroll
-            for (int i = 0; i < 8; i++) { r0[i] = re[i]; i0[i] = im[i]; r1[i] = re[8 + i]; i1[i] = im[8 + i]; }
-            store_chunk(planes, kmajor_offset(row, c16), r0, i0);
-            store_chunk(planes, kmajor_offset(row, c16 + 8), r1, i1);
-        }
-        run_stage(false, false);
-        __syncthreads();
-        if (stop) break;
-        // ---- projection on F (lane k_r, columns k_c of this half); stage 3: B = F', MN-major [k_r][k_c]
-        {
-            double err = 0;
-            const float *A = a.amplitudes + (size_t)p * (kN * kN);
-#pragma unroll 1
-            for (int c16 = 64 * half; c16 < 64 * half + 64; c16 += 16) {
-                float re[16], im[16];
-                tmem_ld16(lane_addr + 256 + c16, re);
-                tmem_ld16(lane_addr + 384 + c16, im);
-                tmem_wait_ld();
-                const float4 *am4 = reinterpret_cast<const float4 *>(A + ((size_t)(c16 >> 4) * kN + row) * 16);
+                    for (int e = 0; e < 4; e++) sv[b][e] = __ldg(s4 + e);
+                    if (x0 >= 0 && x0 + 8 <= a.object_columns) {
 #pragma unroll
-                for (int h4 = 0; h4 < 4; h4++) {
-                    const float4 av = am4[h4];
-                    const float am[4] = {av.x, av.y, av.z, av.w};
+                        for (int e = 0; e < 8; e++) ov[b][e] = __ldg(orow + x0 + e);
+                    } else {
 #pragma unroll
-                    for (int e = 0; e < 4; e++) {
-                        const int i = 4 * h4 + e;
-                        const float mag = sqrtf(re[i] * re[i] + im[i] * im[i]);
-                        const float miss = am[e] - mag;
-                        err += (double)(miss * miss);
-                        if (mag > 0.f) {
-                            const float sc = (am[e] / mag - 1.0f) * inv_n;
-                            re[i] *= sc;
-                            im[i] *= sc;
-                        } else {
-                            re[i] = am[e] * inv_n;
-                            im[i] = 0.f;
-                        }
+                        for (int e = 0; e < 8; e++) ov[b][e] = __ldg(orow + wrap_once(x0 + e, a.object_columns));
                     }
                 }
-                float r0[8], i0[8], r1[8], i1[8];
 #pragma unroll
-                for (int i = 0; i < 8; i++) { r0[i] = re[i]; i0[i] = im[i]; r1[i] = re[8 + i]; i1[i] = im[8 + i]; }
-                store_chunk(planes, mnmajor_offset(row, c16), r0, i0);
-                store_chunk(planes, mnmajor_offset(row, c16 + 8), r1, i1);
+                for (int b = 0; b < 2; b++) {
+                    float re[8], im[8];
+#pragma unroll
+                    for (int e = 0; e < 4; e++) {
+                        const float4 s = sv[b][e];
+                        const float2 o0 = ov[b][2 * e], o1 = ov[b][2 * e + 1];
+                        re[2 * e] = s.x * o0.x - s.y * o0.y;
+                        im[2 * e] = s.x * o0.y + s.y * o0.x;
+                        re[2 * e + 1] = s.z * o1.x - s.w * o1.y;
+                        im[2 * e + 1] = s.z * o1.y + s.w * o1.x;
+                    }
+                    const uint32_t off = kmajor_offset(rows[b], cols[b]);
+                    store_split8(planes, kReHi, off, re);
+                    store_split8(planes, kImHi, off, im);
+                }
+            }
+        }
+        if (!publish()) break;
+        if (tid == 0) {
+            issue_plane(tmem, kCNat, kSlotRe, smem + kReHi * kPlaneBytes, kIdescK);
+            mma_commit(&mbar[0]);
+            issue_plane(tmem, kCNat, kSlotIm, smem + kImHi * kPlaneBytes, kIdescK);
+            mma_commit(&mbar[1]);
+        }
+        pending[0] = pending[1] = true;
+        // ---- stage 2: B[n = raw c][k = r] = D1, each plane as soon as its stage-1 product is done
+        wait_plane(0);
+        readout_kmajor(lane_addr + kSlotRe + 32 * g, planes, kReHi, L, 32 * g);
+        if (!publish()) break;
+        if (tid == 0) {
+            issue_plane(tmem, kCNat, kSlotRe, smem + kReHi * kPlaneBytes, kIdescK);
+            mma_commit(&mbar[0]);
+        }
+        pending[0] = true;
+        wait_plane(1);
+        readout_kmajor(lane_addr + kSlotIm + 32 * g, planes, kImHi, L, 32 * g);
+        if (!publish()) break;
+        if (tid == 0) {
+            issue_plane(tmem, kCNat, kSlotIm, smem + kImHi * kPlaneBytes, kIdescK);
+            mma_commit(&mbar[1]);
+        }
+        pending[1] = true;
+        // ---- projection on F (rows kr = j, mirror(j); this thread's 16 columns kc); stage 3: B = F', MN-major
+        wait_plane(0);
+        wait_plane(1);
+        if (mbar_wait(&amp_bar, amp_phase, kWaitLimit)) {
+            amp_phase ^= 1u;
+            amp_pending = false;
+        } else {
+            bad = true;
+            *a.fault = 1;
+        }
+        {
+            double err = 0;
+#pragma unroll 1
+            for (int u = 0; u < 2; u++) {
+                float4 am4[4];
+#pragma unroll
+                for (int e = 0; e < 4; e++) am4[e] = amp_smem[(4 * u + e) * kThreads + tid];
+                float fr[2][8], fi[2][8];
+                combined_block<false>(lane_addr, g, u, j, h, fr, fi);
+#pragma unroll
+                for (int side = 0; side < 2; side++) {
+#pragma unroll
+                    for (int e = 0; e < 8; e++) {
+                        const float4 av = am4[2 * side + (e >> 2)];
+                        const float am = (e & 3) == 0 ? av.x : (e & 3) == 1 ? av.y : (e & 3) == 2 ? av.z : av.w;
+                        // |F| and A / |F| through one reciprocal square root; F = 0 takes the amplitude itself
+                        const float m2 = fr[side][e] * fr[side][e] + fi[side][e] * fi[side][e];
+                        const bool nonzero = m2 > 0.f;
+                        const float inv = rsqrtf(m2);
+                        const float miss = am - (nonzero ? m2 * inv : 0.f);
+                        err += (double)(miss * miss);
+                        const float sc = (am * inv - 1.0f) * inv_n;
+                        fr[side][e] = nonzero ? fr[side][e] * sc : am * inv_n;
+                        fi[side][e] = nonzero ? fi[side][e] * sc : 0.f;
+                    }
+                    const uint32_t off = mnmajor_offset(side ? mirror(j) : j, 32 * g + 16 * h + 8 * u);
+                    store_split8(planes, kReHi, off, fr[side]);
+                    store_split8(planes, kImHi, off, fi[side]);
+                }
             }
 #pragma unroll
             for (int o = 16; o > 0; o >>= 1) err += __shfl_down_sync(0xffffffffu, err, o);
             if (lane == 0) a.error[(size_t)p * (kThreads / 32) + warp] = err;
         }
-        run_stage(true, true);
-        __syncthreads();
-        if (stop) break;
-        // ---- stage 4: B = Y'^T, K-major [r][k]: lane r's row of Y'
-#pragma unroll 1
-        for (int c16 = 64 * half; c16 < 64 * half + 64; c16 += 16) {
-            float re[16], im[16];
-            tmem_ld16(lane_addr + 256 + c16, re);
-            tmem_ld16(lane_addr + 384 + c16, im);
-            tmem_wait_ld();
-            float r0[8], i0[8], r1[8], i1[8];
-#pragma unroll
-            for (int i = 0; i < 8; i++) { r0[i] = re[i]; i0[i] = im[i]; r1[i] = re[8 + i]; i1[i] = im[8 + i]; }
-            store_chunk(planes, kmajor_offset(row, c16), r0, i0);
-            store_chunk(planes, kmajor_offset(row, c16 + 8), r1, i1);
+        if (!publish()) break;
+        if (tid == 0) {
+            issue_plane(tmem, kCNat, kSlotRe, smem + kReHi * kPlaneBytes, kIdescMN);
+            mma_commit(&mbar[0]);
+            issue_plane(tmem, kCNat, kSlotIm, smem + kImHi * kPlaneBytes, kIdescMN);
+            mma_commit(&mbar[1]);
+            // every thread has read this position's amplitudes: fetch the next one's behind stages 3 to 2
+            if (p + (int)gridDim.x < last)
+                bulk_load(amp_smem, a.amplitudes + (size_t)(p + gridDim.x) * (kN * kN), kN * kN * 4, &amp_bar);
         }
-        run_stage(true, false);
-        __syncthreads();
-        if (stop) break;
-        // ---- dpsi^T: lane c, columns r of this half -> [position][c][r]
+        amp_pending = p + (int)gridDim.x < last;
+        pending[0] = pending[1] = true;
+        // ---- stage 4: B[n = raw r][k = pos] = D3, contracted with C_sigma
+        wait_plane(0);
+        readout_kmajor(lane_addr + kSlotRe + 32 * g, planes, kReHi, L, 32 * g);
+        if (!publish()) break;
+        if (tid == 0) {
+            issue_plane(tmem, kCSigma, kSlotRe, smem + kReHi * kPlaneBytes, kIdescK);
+            mma_commit(&mbar[0]);
+        }
+        pending[0] = true;
+        wait_plane(1);
+        readout_kmajor(lane_addr + kSlotIm + 32 * g, planes, kImHi, L, 32 * g);
+        if (!publish()) break;
+        if (tid == 0) {
+            issue_plane(tmem, kCSigma, kSlotIm, smem + kImHi * kPlaneBytes, kIdescK);
+            mma_commit(&mbar[1]);
+        }
+        pending[1] = true;
+        // ---- dpsi[r][c]: columns c = j, mirror(j) of this lane pair, rows r = J, mirror(J)
+        wait_plane(0);
+        wait_plane(1);
         {
-            float2 *out = a.dpsi + (size_t)p * (kN * kN) + (size_t)row * kN;
+            float2 *out = a.dpsi + (size_t)p * (kN * kN);
 #pragma unroll 1
-            for (int c16 = 64 * half; c16 < 64 * half + 64; c16 += 16) {
-                float re[16], im[16];
-                tmem_ld16(lane_addr + 256 + c16, re);
-                tmem_ld16(lane_addr + 384 + c16, im);
-                tmem_wait_ld();
+            for (int u = 0; u < 2; u++) {
+                float dr[2][8], di[2][8];
+                combined_block<true>(lane_addr, g, u, j, h, dr, di);
 #pragma unroll
-                for (int i = 0; i < 16; i += 2)
-                    *reinterpret_cast<float4 *>(out + c16 + i) = make_float4(re[i], im[i], re[i + 1], im[i + 1]);
+                for (int side = 0; side < 2; side++) {
+                    const int c = side ? mirror(j) : j;
+#pragma unroll
+                    for (int e = 0; e < 8; e++) {
+                        const int J = 16 * g + 8 * h + 4 * u + (e & 3);
+                        const int r = (e >> 2) ? mirror(J) : J;
+                        out[r * kN + c] = make_float2(dr[side][e], di[side][e]);
+                    }
+                }
             }
         }
-        fence_before_sync();
-        __syncthreads();  // every lane has read D before the next stage's MMAs overwrite it
-        fence_after_sync();
+        // the next position's stage 1 overwrites the B planes (its MMAs are issued after the next publish)
     }
     fence_before_sync();
-    __syncthreads();
-    if (stop) {
+    if (__syncthreads_or(bad ? 1 : 0)) {
         // a wait ran out: give the tensor core a bounded chance to drain before the columns are freed
-        mbar_wait(&mbar, phase, kWaitLimit);
+        for (int x = 0; x < 2; x++)
+            if (pending[x]) mbar_wait(&mbar[x], phase[x], kWaitLimit);
+        if (amp_pending) mbar_wait(&amp_bar, amp_phase, kWaitLimit);  // no copy may land after the CTA has gone
     }
     fence_after_sync();
     if (warp == 0) tmem_dealloc(tmem, 512);
 }
 
-// [position][row][column] -> [position][column / 16][row][column mod 16]
+// [position][row][column] -> [position][e4][thread][4]: thread T's float4 e4 = 4 u + 2 side + s holds the amplitudes of
+// row (side ? mirror(j) : j), columns (s ? mirror(J) : J), J = 16 g + 8 h + 4 u + i, i = 0..3, for T's lane pair j,
+// parity h and column group g.
 __global__ void permute_bf16_amplitudes_kernel(const float *in, float *out, long long positions) {
-    const long long i = (long long)blockIdx.x * 256 + threadIdx.x;
-    if (i >= positions * kN * kN) return;
-    const long long p = i / (kN * kN);
-    const int rem = (int)(i - p * kN * kN);
-    const int chunk = rem >> 11, row = (rem >> 4) & 127, c = rem & 15;
-    out[i] = in[p * kN * kN + row * kN + chunk * 16 + c];
+    const long long idx = (long long)blockIdx.x * 256 + threadIdx.x;
+    if (idx >= positions * kN * kN) return;
+    const long long p = idx / (kN * kN);
+    const int rem = (int)(idx - p * kN * kN);
+    const int i = rem & 3, T = (rem >> 2) & (kThreads - 1), e4 = rem >> 11;
+    const int u = e4 >> 2, side = (e4 >> 1) & 1, s = e4 & 1;
+    const int w = T >> 5, L = 32 * (w & 3) + (T & 31), g = w >> 2;
+    const int jj = L >> 1, h = L & 1;
+    const int J = 16 * g + 8 * h + 4 * u + i;
+    const int kc = s ? mirror(J) : J, kr = side ? mirror(jj) : jj;
+    out[idx] = in[p * kN * kN + kr * kN + kc];
 }
 
-size_t bf16_smem() { return 4 * (size_t)kPlaneBytes; }
+size_t bf16_smem() { return 4 * (size_t)kPlaneBytes + (size_t)kN * kN * sizeof(float); }
 
 }  // namespace
 
 bool bf16_applicable(int rows, int columns) { return rows == kN && columns == kN; }
 int bf16_partials_per_position() { return kThreads / 32; }
+
+int bf16_sigma(int pos) {
+    const int g = pos >> 5, h = (pos >> 4) & 1, u = (pos >> 3) & 1, s = (pos >> 2) & 1, i = pos & 3;
+    const int J = 16 * g + 8 * h + 4 * u + i;
+    return s ? mirror(J) : J;
+}
 
 cudaError_t configure_bf16() {
     int device = 0, optin = 0;

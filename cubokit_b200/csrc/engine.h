@@ -34,13 +34,12 @@ template <typename T>
 struct ObjectGatherArgs {
     int rows, columns, object_rows, object_columns, n;
     int tiles_x;               // tiles per object row
-    int tile_w, tile_h;        // tile shape: kTileW x kTileH, or kTileH x kTileW (wide axis = residual's contiguous axis)
+    int tile_w, tile_h;        // tile shape, tile_w x tile_h = kGatherThreads pixels
     const int *tile_start;     // CSR offsets, [tiles + 1]
     const int *tile_list;      // position indices, ascending within each tile
     ScanTables scan;
     const C2<T> *shifted;
     const C2<T> *dpsi;
-    int dpsi_transposed;       // dpsi stored [position][column][row]
     C2<T> *grad;               // object gradient sum conj(S) dpsi
     T *weight;                 // sum |S|^2
     double *tile_max;          // per-tile max of weight
@@ -53,7 +52,6 @@ struct ProbeGatherArgs {
     ScanTables scan;
     const C2<T> *object;
     const C2<T> *dpsi;
-    int dpsi_transposed;       // dpsi stored [position][column][row]
     C2<T> *partial_grad;       // [groups][n]
     T *partial_weight;         // [groups][n]
 };
@@ -88,14 +86,15 @@ struct Bf16Args {
     ScanTables scan;
     const float2 *shifted;
     const float2 *object;
-    const float *amplitudes;   // [positions][column / 16][row][column mod 16]
-    float2 *dpsi;              // [positions][column][row] (transposed)
+    const float *amplitudes;   // permuted into the order the kernel's threads consume them (permute_bf16_amplitudes)
+    float2 *dpsi;              // [positions][row][column]
     double *error;             // [positions][bf16_partials_per_position()]
-    const uint16_t *w_planes;  // [4][128][128] bf16 bits: Re W hi, Re W lo, Im W hi, Im W lo
+    const uint16_t *c_planes;  // [4][128][128] bf16 bits: C hi, C lo, C_sigma hi, C_sigma lo (rows m, columns k)
     int *fault;                // set when a device wait ran out
 };
 bool bf16_applicable(int rows, int columns);
 int bf16_partials_per_position();
+int bf16_sigma(int pos);  // the frequency at contraction position pos of the kernel's stage 4
 cudaError_t configure_bf16();
 cudaError_t launch_bf16(const Bf16Args &a, int ctas, cudaStream_t s);
 cudaError_t launch_permute_bf16_amplitudes(const float *in, float *out, long long positions, cudaStream_t s);

@@ -125,16 +125,9 @@ __global__ void __launch_bounds__(kGatherThreads) object_gather_kernel(ObjectGat
     __shared__ double scratch[32];
     const int tile = blockIdx.x;
     const int tx = tile % a.tiles_x, ty = tile / a.tiles_x;
-    // consecutive threads take consecutive residual addresses: along x for [row][column] residuals, along y (a
-    // transposed kTileH x kTileW walk of the same tile) for [column][row] ones
-    int x, y;
-    if (a.dpsi_transposed) {
-        x = tx * a.tile_w + threadIdx.x / a.tile_h;
-        y = ty * a.tile_h + threadIdx.x % a.tile_h;
-    } else {
-        x = tx * a.tile_w + (threadIdx.x % a.tile_w);
-        y = ty * a.tile_h + threadIdx.x / a.tile_w;
-    }
+    // consecutive threads take consecutive object columns, hence consecutive addresses of each [row][column] residual
+    const int x = tx * a.tile_w + (threadIdx.x % a.tile_w);
+    const int y = ty * a.tile_h + threadIdx.x / a.tile_w;
     const bool inside = x < a.object_columns && y < a.object_rows;
     C2<T> g = mk<T>(0, 0);
     T w = 0;
@@ -168,12 +161,7 @@ __global__ void __launch_bounds__(kGatherThreads) object_gather_kernel(ObjectGat
 #pragma unroll
                 for (int u = 0; u < 4; u++) {
                     if (k[u] >= 0) {
-                        int kd = k[u];
-                        if (a.dpsi_transposed) {
-                            const int kr = kd / a.columns, kc = kd - kr * a.columns;
-                            kd = kc * a.rows + kr;
-                        }
-                        d[u] = a.dpsi[(size_t)s_p[i + u] * a.n + kd];
+                        d[u] = a.dpsi[(size_t)s_p[i + u] * a.n + k[u]];
                         sv[u] = a.shifted[(size_t)s_cls[i + u] * a.n + k[u]];
                     }
                 }
@@ -203,15 +191,11 @@ constexpr int kProbeThreads = 256;
 template <typename T>
 __global__ void __launch_bounds__(kProbeThreads) probe_gather_kernel(ProbeGatherArgs<T> a) {
     __shared__ int s_rr[kChunk], s_cc[kChunk];
-    const int idx = blockIdx.x * kProbeThreads + threadIdx.x;  // index in the residual's storage order
+    const int k = blockIdx.x * kProbeThreads + threadIdx.x;  // pixel index, [row][column]
     const int group = blockIdx.y;
     const int p0 = (int)((long long)a.count * group / a.groups), p1 = (int)((long long)a.count * (group + 1) / a.groups);
-    const bool valid = idx < a.n;
-    int kr, kc;
-    if (a.dpsi_transposed) { kc = valid ? idx / a.rows : 0; kr = valid ? idx - kc * a.rows : 0; }
-    else { kr = valid ? idx / a.columns : 0; kc = valid ? idx - kr * a.columns : 0; }
-    const int k = kr * a.columns + kc;  // natural pixel index (where the partial sums go)
-    const int kd = idx;                 // where pixel k of a residual is stored
+    const bool valid = k < a.n;
+    const int kr = valid ? k / a.columns : 0, kc = valid ? k - kr * a.columns : 0;
     const int offr = corner_offset(kr, a.rows), offc = corner_offset(kc, a.columns);
     C2<T> g = mk<T>(0, 0);
     T w = 0;
@@ -230,7 +214,7 @@ __global__ void __launch_bounds__(kProbeThreads) probe_gather_kernel(ProbeGather
                         const int y = wrap_once(s_rr[i + u] + offr, a.object_rows);
                         const int x = wrap_once(s_cc[i + u] + offc, a.object_columns);
                         o[u] = a.object[(size_t)y * a.object_columns + x];
-                        d[u] = a.dpsi[(size_t)(base + i + u) * a.n + kd];
+                        d[u] = a.dpsi[(size_t)(base + i + u) * a.n + k];
                     }
                 }
 #pragma unroll

@@ -140,7 +140,7 @@ struct cubo_ptycho_plan {
     DeviceBuffer partial_grad, partial_weight, grad_p64, weight_p64, probe_block_max;
     DeviceBuffer maxes, sums, aperture64, mask_dev, error_scratch, loss_slot;
     DeviceBuffer tw_r, tw_c, tw_r64, tw_c64;
-    DeviceBuffer w_planes, fault;
+    DeviceBuffer c_planes, fault;
 
     ~cubo_ptycho_plan() {
         for (auto &t : pending) { event_pool.push_back(t.a); event_pool.push_back(t.b); }
@@ -273,12 +273,12 @@ void build_plan(cubo_ptycho_plan *p, const cubo_ptycho_problem *pr) {
     upload(p->cc, cc, s);
     upload(p->cls, cls, s);
     // ---- object-gather candidate lists: for each tile, the positions whose window touches it, ascending
-    // tile along the residual's contiguous axis: x for [row][column] residuals, y for [column][row] ones
+    // tiles wide along x, the residual's contiguous axis
     const int choice = p->params.gather_tile;
     const int wide = choice == 2 ? 16 : choice == 3 ? 64 : kTileW;
     const int narrow = kGatherThreads / wide;
-    if (p->bf16) { p->tile_w = narrow; p->tile_h = wide; }
-    else { p->tile_w = wide; p->tile_h = narrow; }
+    p->tile_w = wide;
+    p->tile_h = narrow;
     p->tiles_x = (p->OC + p->tile_w - 1) / p->tile_w;
     const int tiles_y = (p->OR + p->tile_h - 1) / p->tile_h;
     p->tiles = p->tiles_x * tiles_y;
@@ -342,12 +342,19 @@ void build_plan(cubo_ptycho_plan *p, const cubo_ptycho_problem *pr) {
         check(cudaMemsetAsync(p->fault.ptr, 0, sizeof(int), s), "memset");
     }
     if (p->bf16) {
-        // the 128-point DFT matrix split into bf16 hi + lo, evaluated in FP64: planes Re hi, Re lo, Im hi, Im lo, [m][k]
+        // the real factor C of the 128-point DFT matrix (row 0 = 1, row 1 = cos(pi k), rows 2j, 2j + 1 = cos, sin of
+        // 2 pi j k / 128) and C_sigma (its columns in the kernel's stage-4 order), split into bf16 hi + lo in FP64:
+        // planes C hi, C lo, C_sigma hi, C_sigma lo, [m][k]
+        auto c_value = [&](int m, int k) -> double {
+            if (m == 0) return 1.0;
+            if (m == 1) return (k & 1) ? -1.0 : 1.0;
+            const double a = 2.0 * kPi * (double)(((m >> 1) * k) % R) / (double)R;
+            return (m & 1) ? std::sin(a) : std::cos(a);
+        };
         std::vector<uint16_t> planes(4 * (size_t)n);
         for (int m = 0; m < R; m++)
             for (int k = 0; k < C; k++) {
-                const double a = -2.0 * kPi * (double)((m * k) % R) / (double)R;
-                const double v[2] = {std::cos(a), std::sin(a)};
+                const double v[2] = {c_value(m, k), c_value(m, bf16_sigma(k))};
                 for (int part = 0; part < 2; part++) {
                     const uint16_t hi = bf16_round(v[part]);
                     const uint16_t lo = bf16_round(v[part] - bf16_to_double(hi));
@@ -355,7 +362,7 @@ void build_plan(cubo_ptycho_plan *p, const cubo_ptycho_problem *pr) {
                     planes[(size_t)(2 * part + 1) * n + m * C + k] = lo;
                 }
             }
-        upload(p->w_planes, planes, s);
+        upload(p->c_planes, planes, s);
         check(p->fault.alloc(sizeof(int)), "cudaMalloc");
         check(cudaMemsetAsync(p->fault.ptr, 0, sizeof(int), s), "memset");
     }
@@ -536,7 +543,7 @@ void enqueue_position_pass(cubo_ptycho_plan *p) {
         ba.object_rows = p->OR; ba.object_columns = p->OC; ba.first = 0; ba.count = p->P; ba.scan = scan;
         ba.shifted = p->shifted.as<float2>(); ba.object = p->object.as<float2>();
         ba.amplitudes = p->amplitudes.as<float>(); ba.dpsi = p->dpsi.as<float2>(); ba.error = p->error.as<double>();
-        ba.w_planes = p->w_planes.as<uint16_t>(); ba.fault = p->fault.as<int>();
+        ba.c_planes = p->c_planes.as<uint16_t>(); ba.fault = p->fault.as<int>();
         timed(p, kPositionPass, 1, [&] { return launch_bf16(ba, p->sms, s); });
     } else if (p->fast) {
         Fast128Args fa{};
@@ -561,14 +568,14 @@ void enqueue_gathers(cubo_ptycho_plan *p) {
     ObjectGatherArgs<T> ga{};
     ga.rows = p->R; ga.columns = p->C; ga.object_rows = p->OR; ga.object_columns = p->OC; ga.n = n;
     ga.tiles_x = p->tiles_x; ga.tile_w = p->tile_w; ga.tile_h = p->tile_h; ga.tile_start = p->tile_start.as<int>(); ga.tile_list = p->tile_list.as<int>();
-    ga.scan = scan; ga.shifted = p->shifted.as<C2<T>>(); ga.dpsi = p->dpsi.as<C2<T>>(); ga.dpsi_transposed = p->bf16;
+    ga.scan = scan; ga.shifted = p->shifted.as<C2<T>>(); ga.dpsi = p->dpsi.as<C2<T>>();
     ga.grad = p->grad_o.as<C2<T>>(); ga.weight = p->weight_o.as<T>(); ga.tile_max = p->tile_max.as<double>();
     timed(p, kObjectGather, 1, [&] { return launch_object_gather<T>(ga, p->tiles, s); });
 
     ProbeGatherArgs<T> pg{};
     pg.rows = p->R; pg.columns = p->C; pg.object_rows = p->OR; pg.object_columns = p->OC; pg.n = n;
     pg.count = p->P; pg.groups = p->groups; pg.scan = scan; pg.object = p->object.as<C2<T>>();
-    pg.dpsi = p->dpsi.as<C2<T>>(); pg.dpsi_transposed = p->bf16; pg.partial_grad = p->partial_grad.as<C2<T>>(); pg.partial_weight = p->partial_weight.as<T>();
+    pg.dpsi = p->dpsi.as<C2<T>>(); pg.partial_grad = p->partial_grad.as<C2<T>>(); pg.partial_weight = p->partial_weight.as<T>();
     if (!p->fast)  // the 128 x 128 FP32 position pass already wrote per-CTA probe partials
         timed(p, kProbeGather, 1, [&] { return launch_probe_gather<T>(pg, s); });
     timed(p, kProbeReduce, 1, [&] {

@@ -187,7 +187,12 @@ __device__ __forceinline__ uint32_t pack_bf16x2(float lo_elem, float hi_elem) {
 __device__ __forceinline__ void split_bf16x2(float x0, float x1, uint32_t &hi, uint32_t &lo) {
     hi = pack_bf16x2(x0, x1);
     const float h0 = __uint_as_float(hi << 16), h1 = __uint_as_float(hi & 0xFFFF0000u);
-    lo = pack_bf16x2(x0 - h0, x1 - h1);
+    float d0, d1;  // (x0 - h0, x1 - h1) as one packed FP32x2 subtraction, rounded like two scalar ones
+    asm("{\n\t.reg .b64 ra, rb, rd;\n\tmov.b64 ra, {%2, %3};\n\tmov.b64 rb, {%4, %5};\n\t"
+        "sub.rn.f32x2 rd, ra, rb;\n\tmov.b64 {%0, %1}, rd;\n\t}"
+        : "=f"(d0), "=f"(d1)
+        : "f"(x0), "f"(x1), "f"(h0), "f"(h1));
+    lo = pack_bf16x2(d0, d1);
 }
 
 // Split x into hi + lo, both bf16: hi = bf16(x), lo = bf16(x - hi) (x - hi is exact in FP32).
