@@ -24,7 +24,7 @@
 // (M = N = 128, K = 16) per plane and stage.  The two planes run as a pipeline: the re plane's result is read out and
 // its next stage issued while the tensor core still works on the im plane.
 //
-// One persistent CTA of 512 threads per SM with 192 KB of shared memory: the four B planes and the next position's
+// One persistent CTA of 512 threads per SM with 208 KB of shared memory: the four B planes and the next position's
 // amplitudes, bulk-copied in behind stages 3 to 2.  Tensor memory: C hi / lo (columns 0-127), C_sigma hi / lo (128-255), the
 // re-plane result (256-383), the im-plane result (384-511).  Thread (warp w, lane i) owns TMEM lane 32 (w mod 4) + i and
 // the 32-column group w / 4 of each result.  Amplitudes are pre-permuted into the order each thread consumes them
@@ -41,8 +41,11 @@ using namespace umma;
 
 constexpr int kN = 128;
 constexpr int kThreads = 512;
-constexpr uint32_t kSBO = 2048, kLBO = 128;     // canonical no-swizzle layout of a 128 x 128 bf16 plane
-constexpr int kPlaneBytes = kN * kN * 2;        // 32 KB
+// Canonical no-swizzle layout of a 128 x 128 bf16 plane with its core matrices (8 rows x 16 bytes) 144 bytes apart
+// along K: the 16 bytes of padding put the K chunks of one row in different banks, so 4-byte stores of consecutive K
+// by consecutive lanes (the exit wave) and 16-byte stores of consecutive rows (the other stages) are conflict-free.
+constexpr uint32_t kLBO = 144, kSBO = 16 * kLBO;
+constexpr int kPlaneBytes = 16 * kSBO;          // 36 KB
 constexpr uint64_t kWaitLimit = 2000000000ull;  // ns of wall time an mbarrier wait may take before giving up
 constexpr uint32_t kCNat = 0, kCSigma = 128, kSlotRe = 256, kSlotIm = 384;  // tensor-memory columns
 constexpr int kReHi = 0, kImHi = 2;             // B planes: re hi, re lo, im hi, im lo
@@ -69,7 +72,7 @@ __device__ __forceinline__ void store_split8(uint8_t *planes, int hi_plane, uint
     *reinterpret_cast<uint4 *>(planes + (hi_plane + 1) * kPlaneBytes + off) = make_uint4(l[0], l[1], l[2], l[3]);
 }
 
-// The 24 MMAs of one plane: D (columns d_col) = A (hi at a_col, lo at a_col + 64) * B (planes b_hi, b_hi + 32 KB).
+// The 24 MMAs of one plane: D (columns d_col) = A (hi at a_col, lo at a_col + 64) * B (planes at b_hi, b_hi + one plane).
 __device__ __forceinline__ void issue_plane(uint32_t tmem, uint32_t a_col, uint32_t d_col, uint32_t b_hi, uint32_t idesc) {
 #pragma unroll
     for (int s = 0; s < kN / 16; s++) {
@@ -152,7 +155,7 @@ __device__ __forceinline__ void combined_block(uint32_t lane_addr, int g, int u,
 }
 
 __global__ void __launch_bounds__(kThreads, 1) bf16_position_kernel(Bf16Args a) {
-    extern __shared__ __align__(1024) uint8_t planes[];  // 4 x 32 KB: the B operand, then 64 KB of amplitudes
+    extern __shared__ __align__(1024) uint8_t planes[];  // 4 x 36 KB: the B operand, then 64 KB of amplitudes
     __shared__ uint64_t mbar[2];                         // completion of the re / im plane's MMAs
     __shared__ uint64_t amp_bar;                         // arrival of the next position's amplitudes
     __shared__ uint32_t tmem_base;
@@ -217,51 +220,52 @@ __global__ void __launch_bounds__(kThreads, 1) bf16_position_kernel(Bf16Args a) 
     };
     const float inv_n = 1.0f / (float)(kN * kN);
     for (int p = a.first + blockIdx.x; p < last; p += gridDim.x) {
-        // ---- stage 1: B[n = r][k = c] = X, 4 chunks of 8 columns per thread (a warp: 8 rows x 4 chunks), two at a
-        // time with every load of both issued before the first product
+        // ---- stage 1: B[n = r][k = c] = X.  Warp w takes rows 8w .. 8w + 7, each in two halves of 64 columns; lane i
+        // the columns 2i, 2i + 1 of a half: one contiguous 512-byte segment of the object row and of the probe row per
+        // warp and load, one 4-byte bf16 pair per plane and lane per store.  Four halves per batch, loads first.
         {
             const int rr = a.scan.rr[p], cc = a.scan.cc[p], cls = a.scan.cls[p];
             const float2 *S = a.shifted + (size_t)cls * (kN * kN);
+            const int OC = a.object_columns;
+            // the patch row is the object row segment [cc - 64, cc + 64) (its columns 64..127, then 0..63)
+            const bool contiguous = cc >= kN / 2 && cc + kN / 2 <= OC;
 #pragma unroll 1
-            for (int it = 0; it < 4; it += 2) {
-                float4 sv[2][4];
-                float2 ov[2][8];
-                int rows[2], cols[2];
+            for (int b0 = 0; b0 < 16; b0 += 4) {
+                float4 sv[4];
+                float2 o0[4], o1[4];
 #pragma unroll
-                for (int b = 0; b < 2; b++) {
-                    const int ch = kThreads * (it + b) + tid;
-                    const int r = 8 * (ch >> 7) + (ch & 7), c8 = 8 * ((ch >> 3) & 15);
-                    rows[b] = r;
-                    cols[b] = c8;
-                    const float2 *orow =
-                        a.object + (size_t)wrap_once(rr + (r < kN / 2 ? r : r - kN), a.object_rows) * a.object_columns;
-                    const int x0 = cc + (c8 < kN / 2 ? c8 : c8 - kN);
-                    const float4 *s4 = reinterpret_cast<const float4 *>(S + r * kN + c8);
-#pragma unroll
-                    for (int e = 0; e < 4; e++) sv[b][e] = __ldg(s4 + e);
-                    if (x0 >= 0 && x0 + 8 <= a.object_columns) {
-#pragma unroll
-                        for (int e = 0; e < 8; e++) ov[b][e] = __ldg(orow + x0 + e);
+                for (int b = 0; b < 4; b++) {
+                    const int r = 8 * warp + ((b0 + b) >> 1), c = 64 * ((b0 + b) & 1) + 2 * lane;
+                    const int y = wrap_once(rr + (r < kN / 2 ? r : r - kN), a.object_rows);
+                    const float2 *orow = a.object + (size_t)y * OC;
+                    const int x = cc + (c < kN / 2 ? c : c - kN);
+                    sv[b] = __ldg(reinterpret_cast<const float4 *>(S + r * kN + c));
+                    if (contiguous && (((size_t)y * OC + cc) & 1) == 0) {
+                        const float4 v = __ldg(reinterpret_cast<const float4 *>(orow + x));
+                        o0[b] = make_float2(v.x, v.y);
+                        o1[b] = make_float2(v.z, v.w);
+                    } else if (contiguous) {
+                        o0[b] = __ldg(orow + x);
+                        o1[b] = __ldg(orow + x + 1);
                     } else {
-#pragma unroll
-                        for (int e = 0; e < 8; e++) ov[b][e] = __ldg(orow + wrap_once(x0 + e, a.object_columns));
+                        o0[b] = __ldg(orow + wrap_once(x, OC));
+                        o1[b] = __ldg(orow + wrap_once(x + 1, OC));
                     }
                 }
 #pragma unroll
-                for (int b = 0; b < 2; b++) {
-                    float re[8], im[8];
-#pragma unroll
-                    for (int e = 0; e < 4; e++) {
-                        const float4 s = sv[b][e];
-                        const float2 o0 = ov[b][2 * e], o1 = ov[b][2 * e + 1];
-                        re[2 * e] = s.x * o0.x - s.y * o0.y;
-                        im[2 * e] = s.x * o0.y + s.y * o0.x;
-                        re[2 * e + 1] = s.z * o1.x - s.w * o1.y;
-                        im[2 * e + 1] = s.z * o1.y + s.w * o1.x;
-                    }
-                    const uint32_t off = kmajor_offset(rows[b], cols[b]);
-                    store_split8(planes, kReHi, off, re);
-                    store_split8(planes, kImHi, off, im);
+                for (int b = 0; b < 4; b++) {
+                    const int r = 8 * warp + ((b0 + b) >> 1), c = 64 * ((b0 + b) & 1) + 2 * lane;
+                    const float4 sp = sv[b];
+                    const float xr0 = sp.x * o0[b].x - sp.y * o0[b].y, xi0 = sp.x * o0[b].y + sp.y * o0[b].x;
+                    const float xr1 = sp.z * o1[b].x - sp.w * o1[b].y, xi1 = sp.z * o1[b].y + sp.w * o1[b].x;
+                    uint32_t rh, rl, ih, il;
+                    split_bf16x2(xr0, xr1, rh, rl);
+                    split_bf16x2(xi0, xi1, ih, il);
+                    const uint32_t off = kmajor_offset(r, c);
+                    *reinterpret_cast<uint32_t *>(planes + (kReHi + 0) * kPlaneBytes + off) = rh;
+                    *reinterpret_cast<uint32_t *>(planes + (kReHi + 1) * kPlaneBytes + off) = rl;
+                    *reinterpret_cast<uint32_t *>(planes + (kImHi + 0) * kPlaneBytes + off) = ih;
+                    *reinterpret_cast<uint32_t *>(planes + (kImHi + 1) * kPlaneBytes + off) = il;
                 }
             }
         }

@@ -14,18 +14,21 @@ using namespace cubo::umma;
 namespace {
 
 constexpr int N = 128;
-constexpr uint32_t kSBO = 2048, kLBO = 128;  // 16 core matrices of 128 bytes per 8-row group; adjacent K chunks
 
-__device__ __forceinline__ uint32_t kmajor_offset(int row, int k) {  // bytes; row = M/N index, k = K index
-    return (row >> 3) * kSBO + (k >> 3) * kLBO + (row & 7) * 16 + (k & 7) * 2;
+// Canonical no-swizzle layouts with core matrices adjacent in K `lbo` bytes apart and 8-row groups `sbo` bytes apart
+// (lbo = 128, sbo = 2048 packs them; lbo = 144 pads 16 bytes between K chunks).
+__device__ __forceinline__ uint32_t kmajor_offset(int row, int k, uint32_t lbo, uint32_t sbo) {  // row = M/N, k = K
+    return (row >> 3) * sbo + (k >> 3) * lbo + (row & 7) * 16 + (k & 7) * 2;
 }
-__device__ __forceinline__ uint32_t mnmajor_offset(int k, int col) {  // bytes; k = K index, col = M/N index
-    return (col >> 3) * kSBO + (k >> 3) * kLBO + (k & 7) * 16 + (col & 7) * 2;
+__device__ __forceinline__ uint32_t mnmajor_offset(int k, int col, uint32_t lbo, uint32_t sbo) {  // col = M/N
+    return (col >> 3) * sbo + (k >> 3) * lbo + (k & 7) * 16 + (col & 7) * 2;
 }
 
 // withhold_commit: issue nothing and never commit, so the completion wait must run out (the bounded-wait path).
 __global__ void __launch_bounds__(256, 1) probe_kernel(const uint16_t *w, const uint16_t *b, int b_mn_major, int conj_w,
-                                                       int withhold_commit, float *out, int *status) {
+                                                       int withhold_commit, uint32_t lbo, uint32_t sbo, float *out,
+                                                       int *status) {
+    const uint32_t plane = 16 * sbo;  // bytes of one B plane
     extern __shared__ __align__(1024) uint8_t smem[];
     __shared__ uint64_t mbar;
     __shared__ uint32_t tmem_base;
@@ -59,8 +62,8 @@ __global__ void __launch_bounds__(256, 1) probe_kernel(const uint16_t *w, const 
     for (int q = 0; q < 4; q++)
         for (int e = tid; e < N * N; e += 256) {
             const int k = e / N, n = e % N;  // logical B[k][n]
-            const uint32_t off = b_mn_major ? mnmajor_offset(k, n) : kmajor_offset(n, k);
-            *reinterpret_cast<uint16_t *>(smem + q * (N * N * 2) + off) = b[(q * N + k) * N + n];
+            const uint32_t off = b_mn_major ? mnmajor_offset(k, n, lbo, sbo) : kmajor_offset(n, k, lbo, sbo);
+            *reinterpret_cast<uint16_t *>(smem + q * plane + off) = b[(q * N + k) * N + n];
         }
     fence_proxy_async();
     fence_before_sync();
@@ -78,7 +81,7 @@ __global__ void __launch_bounds__(256, 1) probe_kernel(const uint16_t *w, const 
                 bool neg = prod[i][3] != 0;
                 if (conj_w && prod[i][1] >= 2) neg = !neg;  // conj(W): every Wi term changes sign
                 const uint32_t idesc = idesc_bf16(128, 128, false, b_mn_major != 0, false, neg);
-                const uint64_t bdesc = smem_desc(smem_base + prod[i][2] * (N * N * 2) + s * 2 * kLBO, kLBO, kSBO);
+                const uint64_t bdesc = smem_desc(smem_base + prod[i][2] * plane + s * 2 * lbo, lbo, sbo);
                 const uint32_t d = base + 256 + prod[i][0] * 128;
                 const uint32_t a = base + prod[i][1] * 64 + s * 8;
                 const uint32_t acc = (s > 0 || (i % 6) != 0) ? 1u : 0u;
@@ -106,8 +109,9 @@ __global__ void __launch_bounds__(256, 1) probe_kernel(const uint16_t *w, const 
 
 }  // namespace
 
-extern "C" int umma_probe_complex(const uint16_t *w_host, const uint16_t *b_host, int b_mn_major, int conj_w,
-                                  int withhold_commit, float *out_host) {
+extern "C" int umma_probe_complex_strided(const uint16_t *w_host, const uint16_t *b_host, int b_mn_major, int conj_w,
+                                          int withhold_commit, uint32_t lbo, uint32_t sbo, float *out_host) {
+    if (lbo < 128 || lbo % 16 || sbo < 16 * lbo || sbo % 16) return -3;  // layouts that keep core matrices apart
     uint16_t *w = nullptr, *b = nullptr;
     float *out = nullptr;
     int *status = nullptr, st = 0;
@@ -119,9 +123,9 @@ extern "C" int umma_probe_complex(const uint16_t *w_host, const uint16_t *b_host
     cudaMemcpy(b, b_host, planes, cudaMemcpyHostToDevice);
     cudaMemset(status, 0, sizeof(int));
     cudaMemset(out, 0, 2 * N * N * sizeof(float));
-    const int smem = 4 * N * N * 2;
+    const int smem = 4 * 16 * (int)sbo;
     cudaFuncSetAttribute(probe_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, smem);
-    probe_kernel<<<1, 256, smem>>>(w, b, b_mn_major, conj_w, withhold_commit, out, status);
+    probe_kernel<<<1, 256, smem>>>(w, b, b_mn_major, conj_w, withhold_commit, lbo, sbo, out, status);
     cudaError_t e = cudaDeviceSynchronize();
     if (e != cudaSuccess) return -2;
     cudaMemcpy(out_host, out, 2 * N * N * sizeof(float), cudaMemcpyDeviceToHost);
@@ -131,4 +135,9 @@ extern "C" int umma_probe_complex(const uint16_t *w_host, const uint16_t *b_host
     cudaFree(out);
     cudaFree(status);
     return st;
+}
+
+extern "C" int umma_probe_complex(const uint16_t *w_host, const uint16_t *b_host, int b_mn_major, int conj_w,
+                                  int withhold_commit, float *out_host) {
+    return umma_probe_complex_strided(w_host, b_host, b_mn_major, conj_w, withhold_commit, 128, 2048, out_host);
 }

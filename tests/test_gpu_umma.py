@@ -27,6 +27,9 @@ def _lib():
     lib = C.CDLL(str(LIB))
     lib.umma_probe_complex.argtypes = [C.c_void_p, C.c_void_p, C.c_int, C.c_int, C.c_int, C.c_void_p]
     lib.umma_probe_complex.restype = C.c_int
+    lib.umma_probe_complex_strided.argtypes = [C.c_void_p, C.c_void_p, C.c_int, C.c_int, C.c_int, C.c_uint32, C.c_uint32,
+                                               C.c_void_p]
+    lib.umma_probe_complex_strided.restype = C.c_int
     return lib
 
 
@@ -50,8 +53,11 @@ def planes(z):
     return np.ascontiguousarray(np.stack([rh, rl, ih, il])), (rhv, rlv, ihv, ilv)
 
 
+@pytest.mark.parametrize("lbo,sbo", [(128, 2048), (144, 2304)])
 @pytest.mark.parametrize("mn_major,conj", [(False, False), (True, False), (False, True), (True, True)])
-def test_split_bf16_complex_product(mn_major, conj):
+def test_split_bf16_complex_product(mn_major, conj, lbo, sbo):
+    """Packed core matrices (LBO 128) and core matrices 144 bytes apart along K (16 bytes of padding, the layout whose
+    4-byte stores of consecutive K by consecutive lanes hit 32 different banks)."""
     lib = _lib()
     n = 128
     k = np.arange(n)
@@ -61,7 +67,8 @@ def test_split_bf16_complex_product(mn_major, conj):
     wp, (wrh, wrl, wih, wil) = planes(w)
     bp, (brh, brl, bih, bil) = planes(b)
     out = np.zeros((2, n, n), np.float32)
-    st = lib.umma_probe_complex(wp.ctypes.data, bp.ctypes.data, int(mn_major), int(conj), 0, out.ctypes.data)
+    st = lib.umma_probe_complex_strided(wp.ctypes.data, bp.ctypes.data, int(mn_major), int(conj), 0, lbo, sbo,
+                                        out.ctypes.data)
     assert st == 0, st
     mm = lambda p, q: p @ q
     s = -1.0 if conj else 1.0
