@@ -48,7 +48,8 @@ constexpr uint32_t kLBO = 144, kSBO = 16 * kLBO;
 constexpr int kPlaneBytes = 16 * kSBO;          // 36 KB
 constexpr uint64_t kWaitLimit = 2000000000ull;  // ns of wall time an mbarrier wait may take before giving up
 constexpr uint32_t kCNat = 0, kCSigma = 128, kSlotRe = 256, kSlotIm = 384;  // tensor-memory columns
-constexpr int kReHi = 0, kImHi = 2;             // B planes: re hi, re lo, im hi, im lo
+constexpr int kReHi = 0, kImHi = 2;
+constexpr int kBatch = 8;                       // exit-wave row halves whose loads are in flight together             // B planes: re hi, re lo, im hi, im lo
 constexpr uint32_t kIdescK = idesc_bf16(128, 128, false, false), kIdescMN = idesc_bf16(128, 128, false, true);
 
 __device__ __forceinline__ uint32_t kmajor_offset(int row, int k) {
@@ -196,14 +197,13 @@ __global__ void __launch_bounds__(kThreads, 1) bf16_position_kernel(Bf16Args a) 
         tmem_st16(lane_addr + 64 * v + 16 * g, r);
     }
     tmem_wait_st();
-    uint32_t phase[2] = {0u, 0u};
-    bool pending[2] = {false, false};
+    uint32_t phase = 0u, pending = 0u;  // bit x: parity to wait for / commit outstanding, of plane x's barrier
     bool bad = false;
     // waits for plane x's MMAs; a wait that runs out marks this thread bad and raises the fault flag
     auto wait_plane = [&](int x) {
-        if (mbar_wait(&mbar[x], phase[x], kWaitLimit)) {
-            phase[x] ^= 1u;
-            pending[x] = false;
+        if (mbar_wait(&mbar[x], (phase >> x) & 1u, kWaitLimit)) {
+            phase ^= 1u << x;
+            pending &= ~(1u << x);
         } else {
             bad = true;
             *a.fault = 1;
@@ -222,7 +222,7 @@ __global__ void __launch_bounds__(kThreads, 1) bf16_position_kernel(Bf16Args a) 
     for (int p = a.first + blockIdx.x; p < last; p += gridDim.x) {
         // ---- stage 1: B[n = r][k = c] = X.  Warp w takes rows 8w .. 8w + 7, each in two halves of 64 columns; lane i
         // the columns 2i, 2i + 1 of a half: one contiguous 512-byte segment of the object row and of the probe row per
-        // warp and load, one 4-byte bf16 pair per plane and lane per store.  Four halves per batch, loads first.
+        // warp and load, one 4-byte bf16 pair per plane and lane per store.  kBatch halves per batch, loads first.
         {
             const int rr = a.scan.rr[p], cc = a.scan.cc[p], cls = a.scan.cls[p];
             const float2 *S = a.shifted + (size_t)cls * (kN * kN);
@@ -230,11 +230,11 @@ __global__ void __launch_bounds__(kThreads, 1) bf16_position_kernel(Bf16Args a) 
             // the patch row is the object row segment [cc - 64, cc + 64) (its columns 64..127, then 0..63)
             const bool contiguous = cc >= kN / 2 && cc + kN / 2 <= OC;
 #pragma unroll 1
-            for (int b0 = 0; b0 < 16; b0 += 4) {
-                float4 sv[4];
-                float2 o0[4], o1[4];
+            for (int b0 = 0; b0 < 16; b0 += kBatch) {
+                float4 sv[kBatch];
+                float2 o0[kBatch], o1[kBatch];
 #pragma unroll
-                for (int b = 0; b < 4; b++) {
+                for (int b = 0; b < kBatch; b++) {
                     const int r = 8 * warp + ((b0 + b) >> 1), c = 64 * ((b0 + b) & 1) + 2 * lane;
                     const int y = wrap_once(rr + (r < kN / 2 ? r : r - kN), a.object_rows);
                     const float2 *orow = a.object + (size_t)y * OC;
@@ -253,7 +253,7 @@ __global__ void __launch_bounds__(kThreads, 1) bf16_position_kernel(Bf16Args a) 
                     }
                 }
 #pragma unroll
-                for (int b = 0; b < 4; b++) {
+                for (int b = 0; b < kBatch; b++) {
                     const int r = 8 * warp + ((b0 + b) >> 1), c = 64 * ((b0 + b) & 1) + 2 * lane;
                     const float4 sp = sv[b];
                     const float xr0 = sp.x * o0[b].x - sp.y * o0[b].y, xi0 = sp.x * o0[b].y + sp.y * o0[b].x;
@@ -276,7 +276,7 @@ __global__ void __launch_bounds__(kThreads, 1) bf16_position_kernel(Bf16Args a) 
             issue_plane(tmem, kCNat, kSlotIm, smem + kImHi * kPlaneBytes, kIdescK);
             mma_commit(&mbar[1]);
         }
-        pending[0] = pending[1] = true;
+        pending = 3u;
         // ---- stage 2: B[n = raw c][k = r] = D1, each plane as soon as its stage-1 product is done
         wait_plane(0);
         readout_kmajor(lane_addr + kSlotRe + 32 * g, planes, kReHi, L, 32 * g);
@@ -285,7 +285,7 @@ __global__ void __launch_bounds__(kThreads, 1) bf16_position_kernel(Bf16Args a) 
             issue_plane(tmem, kCNat, kSlotRe, smem + kReHi * kPlaneBytes, kIdescK);
             mma_commit(&mbar[0]);
         }
-        pending[0] = true;
+        pending |= 1u;
         wait_plane(1);
         readout_kmajor(lane_addr + kSlotIm + 32 * g, planes, kImHi, L, 32 * g);
         if (!publish()) break;
@@ -293,7 +293,7 @@ __global__ void __launch_bounds__(kThreads, 1) bf16_position_kernel(Bf16Args a) 
             issue_plane(tmem, kCNat, kSlotIm, smem + kImHi * kPlaneBytes, kIdescK);
             mma_commit(&mbar[1]);
         }
-        pending[1] = true;
+        pending |= 2u;
         // ---- projection on F (rows kr = j, mirror(j); this thread's 16 columns kc); stage 3: B = F', MN-major
         wait_plane(0);
         wait_plane(1);
@@ -349,7 +349,7 @@ __global__ void __launch_bounds__(kThreads, 1) bf16_position_kernel(Bf16Args a) 
                 bulk_load(amp_smem, a.amplitudes + (size_t)(p + gridDim.x) * (kN * kN), kN * kN * 4, &amp_bar);
         }
         amp_pending = p + (int)gridDim.x < last;
-        pending[0] = pending[1] = true;
+        pending = 3u;
         // ---- stage 4: B[n = raw r][k = pos] = D3, contracted with C_sigma
         wait_plane(0);
         readout_kmajor(lane_addr + kSlotRe + 32 * g, planes, kReHi, L, 32 * g);
@@ -358,7 +358,7 @@ __global__ void __launch_bounds__(kThreads, 1) bf16_position_kernel(Bf16Args a) 
             issue_plane(tmem, kCSigma, kSlotRe, smem + kReHi * kPlaneBytes, kIdescK);
             mma_commit(&mbar[0]);
         }
-        pending[0] = true;
+        pending |= 1u;
         wait_plane(1);
         readout_kmajor(lane_addr + kSlotIm + 32 * g, planes, kImHi, L, 32 * g);
         if (!publish()) break;
@@ -366,7 +366,7 @@ __global__ void __launch_bounds__(kThreads, 1) bf16_position_kernel(Bf16Args a) 
             issue_plane(tmem, kCSigma, kSlotIm, smem + kImHi * kPlaneBytes, kIdescK);
             mma_commit(&mbar[1]);
         }
-        pending[1] = true;
+        pending |= 2u;
         // ---- dpsi[r][c]: columns c = j, mirror(j) of this lane pair, rows r = J, mirror(J)
         wait_plane(0);
         wait_plane(1);
@@ -394,7 +394,7 @@ __global__ void __launch_bounds__(kThreads, 1) bf16_position_kernel(Bf16Args a) 
     if (__syncthreads_or(bad ? 1 : 0)) {
         // a wait ran out: give the tensor core a bounded chance to drain before the columns are freed
         for (int x = 0; x < 2; x++)
-            if (pending[x]) mbar_wait(&mbar[x], phase[x], kWaitLimit);
+            if ((pending >> x) & 1u) mbar_wait(&mbar[x], (phase >> x) & 1u, kWaitLimit);
         if (amp_pending) mbar_wait(&amp_bar, amp_phase, kWaitLimit);  // no copy may land after the CTA has gone
     }
     fence_after_sync();

@@ -117,6 +117,10 @@ cudaError_t launch_object_update(C2<T> *object, const C2<T> *grad, const T *weig
 cudaError_t launch_error_reduce(const double *error, long long count, double divisor, double *errors, int *iteration,
                                 double *scratch, cudaStream_t s);
 int error_reduce_scratch();  // doubles of scratch launch_error_reduce needs
+// sum A^2 of `count` amplitudes into scratch[amplitude_check_scratch() - 1] (FP64, fixed order); *bad = 1 if any is not
+// finite and non-negative (*bad is not cleared)
+cudaError_t launch_amplitude_check(const float *amplitudes, long long count, double *scratch, int *bad, cudaStream_t s);
+int amplitude_check_scratch();
 bool position_pass_supported(int n, bool fp64);
 size_t position_pass_smem(int n, int rows, int columns, bool fp64);
 

@@ -304,6 +304,43 @@ __global__ void __launch_bounds__(kErrorBlocks) error_final_kernel(const double 
     }
 }
 
+constexpr int kAmplitudeBlocks = 1024;
+
+// The supplied-amplitude checks of Ptychography.swift:247-259 on the device: every amplitude finite and non-negative
+// (*bad = 1 otherwise), and their energy sum A^2 in FP64 (the errors' divisor, :257-259), in the fixed two-level order
+// of the error sums: block b takes the slice [b*count/B, (b+1)*count/B), four consecutive values per thread and step.
+__global__ void __launch_bounds__(1024) amplitude_partial_kernel(const float *a, long long count, double *block_sums,
+                                                                int *bad) {
+    __shared__ double scratch[32];
+    const long long b = count * blockIdx.x / kAmplitudeBlocks, e = count * (blockIdx.x + 1) / kAmplitudeBlocks;
+    double s = 0;
+    int flag = 0;
+    for (long long i = b + 4 * (long long)threadIdx.x; i < e; i += 4 * 1024) {
+        float v[4];
+        if (i + 4 <= e && (((uintptr_t)(a + i)) & 15) == 0) {
+            const float4 q = *reinterpret_cast<const float4 *>(a + i);
+            v[0] = q.x; v[1] = q.y; v[2] = q.z; v[3] = q.w;
+        } else {
+#pragma unroll
+            for (int k = 0; k < 4; k++) v[k] = i + k < e ? a[i + k] : 0.f;
+        }
+#pragma unroll
+        for (int k = 0; k < 4; k++) {
+            if (!(v[k] >= 0.f && v[k] <= FLT_MAX)) flag = 1;
+            s += (double)v[k] * (double)v[k];
+        }
+    }
+    s = block_sum<1024>(s, scratch);
+    if (threadIdx.x == 0) block_sums[blockIdx.x] = s;
+    if (flag) *bad = 1;
+}
+
+__global__ void __launch_bounds__(1024) amplitude_final_kernel(const double *block_sums, double *energy) {
+    __shared__ double scratch[32];
+    const double s = block_sum<1024>(block_sums[threadIdx.x], scratch);
+    if (threadIdx.x == 0) *energy = s;
+}
+
 template <typename T>
 size_t pass_smem(int n, int rows, int columns) {
     return (size_t)(n + rows + columns) * sizeof(C2<T>) + 32 * sizeof(double);
@@ -376,6 +413,16 @@ cudaError_t launch_object_update(C2<T> *object, const C2<T> *grad, const T *weig
 }
 
 int error_reduce_scratch() { return kErrorBlocks; }
+
+int amplitude_check_scratch() { return kAmplitudeBlocks + 1; }
+
+cudaError_t launch_amplitude_check(const float *amplitudes, long long count, double *scratch, int *bad, cudaStream_t s) {
+    amplitude_partial_kernel<<<kAmplitudeBlocks, 1024, 0, s>>>(amplitudes, count, scratch, bad);
+    cudaError_t e = cudaGetLastError();
+    if (e != cudaSuccess) return e;
+    amplitude_final_kernel<<<1, kAmplitudeBlocks, 0, s>>>(scratch, scratch + kAmplitudeBlocks);
+    return cudaGetLastError();
+}
 
 cudaError_t launch_error_reduce(const double *error, long long count, double divisor, double *errors, int *iteration,
                                 double *scratch, cudaStream_t s) {

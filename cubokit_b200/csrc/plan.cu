@@ -222,16 +222,12 @@ void validate(const cubo_ptycho_problem *pr, const cubo_ptycho_params *pp, doubl
         fail(CUBO_PTYCHO_INVALID_INPUT, "probe amplitude constraint parameters");
     if (!(pr->object_rows >= pr->rows && pr->object_columns >= pr->columns))
         fail(CUBO_PTYCHO_INVALID_INPUT, "object smaller than probe");
-    double energy = 0;
-    const long long total = (long long)pr->count * n;
-    for (long long i = 0; i < total; i++) {
-        const double a = (double)pr->amplitudes[i];
-        if (!(std::isfinite(a) && a >= 0)) fail(CUBO_PTYCHO_INVALID_INPUT, "amplitude not finite and non-negative");
-        energy += a * a;
+    // the amplitudes themselves (finite, non-negative) and their energy are checked on the device once uploaded
+    double d = 1.0;
+    if (pp->error_normalization == CUBO_PTYCHO_ERRORS_MEAN_INTENSITY) {
+        d = pp->mean_intensity * (double)pr->count;
+        if (!finite_positive(d)) fail(CUBO_PTYCHO_INVALID_INPUT, "error normalisation divisor");
     }
-    const double d = pp->error_normalization == CUBO_PTYCHO_ERRORS_MEAN_INTENSITY ? pp->mean_intensity * (double)pr->count
-                                                                                  : energy;
-    if (!finite_positive(d)) fail(CUBO_PTYCHO_INVALID_INPUT, "error normalisation divisor");
     if (pp->form < CUBO_PTYCHO_FORM_FP32 || pp->form > CUBO_PTYCHO_FORM_FP64) fail(CUBO_PTYCHO_INVALID_INPUT, "form");
     if (pp->gather_tile < 0 || pp->gather_tile > 3) fail(CUBO_PTYCHO_INVALID_INPUT, "gather tile");
     *divisor_out = d;
@@ -320,6 +316,26 @@ void build_plan(cubo_ptycho_plan *p, const cubo_ptycho_problem *pr) {
     check(p->amplitudes.alloc((size_t)P * n * sizeof(float)), "cudaMalloc amplitudes");
     check(cudaMemcpyAsync(p->amplitudes.ptr, pr->amplitudes, (size_t)P * n * sizeof(float), cudaMemcpyHostToDevice, s),
           "upload amplitudes");
+    {
+        // every amplitude finite and non-negative, and sum A^2 (Ptychography.swift:247-259), in the supplied order
+        DeviceBuffer scratch, bad;
+        check(scratch.alloc((size_t)amplitude_check_scratch() * sizeof(double)), "cudaMalloc");
+        check(bad.alloc(sizeof(int)), "cudaMalloc");
+        check(cudaMemsetAsync(bad.ptr, 0, sizeof(int), s), "memset");
+        check(launch_amplitude_check(p->amplitudes.as<float>(), (long long)P * n, scratch.as<double>(), bad.as<int>(), s),
+              "amplitude check");
+        double energy = 0;
+        int any_bad = 0;
+        check(cudaMemcpyAsync(&energy, scratch.as<double>() + amplitude_check_scratch() - 1, sizeof(double),
+                              cudaMemcpyDeviceToHost, s), "download");
+        check(cudaMemcpyAsync(&any_bad, bad.ptr, sizeof(int), cudaMemcpyDeviceToHost, s), "download");
+        check(cudaStreamSynchronize(s), "amplitude check");
+        if (any_bad) fail(CUBO_PTYCHO_INVALID_INPUT, "amplitude not finite and non-negative");
+        if (p->params.error_normalization != CUBO_PTYCHO_ERRORS_MEAN_INTENSITY) {
+            if (!finite_positive(energy)) fail(CUBO_PTYCHO_INVALID_INPUT, "error normalisation divisor");
+            p->divisor = energy;
+        }
+    }
     if (p->fast || p->bf16) {
         DeviceBuffer permuted;
         check(permuted.alloc((size_t)P * n * sizeof(float)), "cudaMalloc amplitudes");

@@ -146,10 +146,14 @@ def test_refusals_through_the_c_abi(cb):
                  probe_amplitude_relative_width=width)
     with pytest.raises(cb.PtychographyError):
         _gpu(cb, case, "fp32", iterations=1, position_correction=object())
-    bad = case.amplitudes.copy()
-    bad.flat[5] = -1
-    with pytest.raises(cb.PtychographyError):
-        cb.SingleslicePtychography.reconstruct(bad, case.positions, case.object, case.probe, iterations=1)
+    for value in (-1.0, np.nan, np.inf):  # checked on the device after the upload
+        bad = case.amplitudes.copy()
+        bad.flat[5] = value
+        with pytest.raises(cb.PtychographyError):
+            cb.SingleslicePtychography.reconstruct(bad, case.positions, case.object, case.probe, iterations=1)
+    with pytest.raises(cb.PtychographyError):  # no supplied energy to normalise the errors by
+        cb.SingleslicePtychography.reconstruct(np.zeros_like(case.amplitudes), case.positions, case.object, case.probe,
+                                               iterations=1)
     with pytest.raises(cb.PtychographyError):
         cb.SingleslicePtychography.reconstruct(case.amplitudes, case.positions, case.object, case.probe, iterations=1,
                                                step_size=0.0)
