@@ -351,7 +351,9 @@ def main():
         roofline = {"kernel": "position_pass (bf16_position_kernel)", "bound": "tensor",
                     "achieved": tensor_flops / pass_avg_s / 1e12, "peak": bf16_peak, "unit": "TFLOP/s",
                     "frac": tensor_flops / pass_avg_s / 1e12 / bf16_peak, "peak_kind": peak_kind + " (bf16 dense burst)",
-                    "traffic": None, "executed_tflop_per_launch": tensor_flops / 1e12,
+                    # ncu dram__bytes_read.sum + dram__bytes_write.sum of one launch at 4096 positions (748.3 MB,
+                    # profiles/position_pass_bf16_scan64_det128.md), scaled to this launch by positions
+                    "traffic": 748.3e6 / 4096 * P, "executed_tflop_per_launch": tensor_flops / 1e12,
                     "note": "executed split-BF16 DFT-GEMM flops (100.7 MFLOP per position); the FFT-equivalent "
                             "algorithmic rate is fft_equivalent_tflops",
                     "fft_equivalent_tflops": fft_flops / pass_avg_s / 1e12,
