@@ -48,8 +48,7 @@ constexpr uint32_t kLBO = 144, kSBO = 16 * kLBO;
 constexpr int kPlaneBytes = 16 * kSBO;          // 36 KB
 constexpr uint64_t kWaitLimit = 2000000000ull;  // ns of wall time an mbarrier wait may take before giving up
 constexpr uint32_t kCNat = 0, kCSigma = 128, kSlotRe = 256, kSlotIm = 384;  // tensor-memory columns
-constexpr int kReHi = 0, kImHi = 2;
-constexpr int kBatch = 8;                       // exit-wave row halves whose loads are in flight together             // B planes: re hi, re lo, im hi, im lo
+constexpr int kReHi = 0, kImHi = 2;             // B planes: re hi, re lo, im hi, im lo
 constexpr uint32_t kIdescK = idesc_bf16(128, 128, false, false), kIdescMN = idesc_bf16(128, 128, false, true);
 
 __device__ __forceinline__ uint32_t kmajor_offset(int row, int k) {
@@ -222,46 +221,55 @@ __global__ void __launch_bounds__(kThreads, 1) bf16_position_kernel(Bf16Args a) 
     for (int p = a.first + blockIdx.x; p < last; p += gridDim.x) {
         // ---- stage 1: B[n = r][k = c] = X.  Warp w takes rows 8w .. 8w + 7, each in two halves of 64 columns; lane i
         // the columns 2i, 2i + 1 of a half: one contiguous 512-byte segment of the object row and of the probe row per
-        // warp and load, one 4-byte bf16 pair per plane and lane per store.  kBatch halves per batch, loads first.
+        // warp and load, one 4-byte bf16 pair per plane and lane per store.
         {
             const int rr = a.scan.rr[p], cc = a.scan.cc[p], cls = a.scan.cls[p];
-            const float2 *S = a.shifted + (size_t)cls * (kN * kN);
             const int OC = a.object_columns;
-            // the patch row is the object row segment [cc - 64, cc + 64) (its columns 64..127, then 0..63)
-            const bool contiguous = cc >= kN / 2 && cc + kN / 2 <= OC;
-#pragma unroll 1
-            for (int b0 = 0; b0 < 16; b0 += kBatch) {
-                float4 sv[kBatch];
-                float2 o0[kBatch], o1[kBatch];
+            const float2 *S = a.shifted + (size_t)cls * (kN * kN) + 8 * warp * kN + 2 * lane;
+            // patch rows 8w .. 8w + 7 are object rows y0 .. y0 + 7 (wrapped), y0 = rr + 8w, or rr + 8w - 128 past the
+            // centre row
+            const int y0 = rr + (warp < 8 ? 8 * warp : 8 * warp - kN);
+            // the patch row is the object row segment [cc - 64, cc + 64) (its columns 64..127, then 0..63): one
+            // aligned float4 per lane and half when it does not wrap and starts on an even complex
+            if (cc >= kN / 2 && cc + kN / 2 <= OC && ((cc | OC) & 1) == 0) {
 #pragma unroll
-                for (int b = 0; b < kBatch; b++) {
-                    const int r = 8 * warp + ((b0 + b) >> 1), c = 64 * ((b0 + b) & 1) + 2 * lane;
-                    const int y = wrap_once(rr + (r < kN / 2 ? r : r - kN), a.object_rows);
-                    const float2 *orow = a.object + (size_t)y * OC;
-                    const int x = cc + (c < kN / 2 ? c : c - kN);
-                    sv[b] = __ldg(reinterpret_cast<const float4 *>(S + r * kN + c));
-                    if (contiguous && (((size_t)y * OC + cc) & 1) == 0) {
-                        const float4 v = __ldg(reinterpret_cast<const float4 *>(orow + x));
-                        o0[b] = make_float2(v.x, v.y);
-                        o1[b] = make_float2(v.z, v.w);
-                    } else if (contiguous) {
-                        o0[b] = __ldg(orow + x);
-                        o1[b] = __ldg(orow + x + 1);
-                    } else {
-                        o0[b] = __ldg(orow + wrap_once(x, OC));
-                        o1[b] = __ldg(orow + wrap_once(x + 1, OC));
+                for (int b0 = 0; b0 < 8; b0 += 4) {  // rows b0 .. b0 + 3 of the warp, both halves: 16 loads in flight
+                    float4 sv[8], ov[8];
+#pragma unroll
+                    for (int i = 0; i < 4; i++) {
+                        const float2 *orow = a.object + (size_t)wrap_once(y0 + b0 + i, a.object_rows) * OC + cc + 2 * lane;
+                        sv[2 * i] = __ldg(reinterpret_cast<const float4 *>(S + (b0 + i) * kN));
+                        sv[2 * i + 1] = __ldg(reinterpret_cast<const float4 *>(S + (b0 + i) * kN + kN / 2));
+                        ov[2 * i] = __ldg(reinterpret_cast<const float4 *>(orow));
+                        ov[2 * i + 1] = __ldg(reinterpret_cast<const float4 *>(orow - kN / 2));
+                    }
+#pragma unroll
+                    for (int u = 0; u < 8; u++) {
+                        const float4 sp = sv[u], o = ov[u];
+                        uint32_t rh, rl, ih, il;
+                        split_bf16x2(sp.x * o.x - sp.y * o.y, sp.z * o.z - sp.w * o.w, rh, rl);
+                        split_bf16x2(sp.x * o.y + sp.y * o.x, sp.z * o.w + sp.w * o.z, ih, il);
+                        // row 8w + b0 + u/2, columns 64 (u & 1) + 2 lane
+                        const uint32_t off = kmajor_offset(8 * warp + b0 + (u >> 1), 64 * (u & 1) + 2 * lane);
+                        *reinterpret_cast<uint32_t *>(planes + (kReHi + 0) * kPlaneBytes + off) = rh;
+                        *reinterpret_cast<uint32_t *>(planes + (kReHi + 1) * kPlaneBytes + off) = rl;
+                        *reinterpret_cast<uint32_t *>(planes + (kImHi + 0) * kPlaneBytes + off) = ih;
+                        *reinterpret_cast<uint32_t *>(planes + (kImHi + 1) * kPlaneBytes + off) = il;
                     }
                 }
-#pragma unroll
-                for (int b = 0; b < kBatch; b++) {
-                    const int r = 8 * warp + ((b0 + b) >> 1), c = 64 * ((b0 + b) & 1) + 2 * lane;
-                    const float4 sp = sv[b];
-                    const float xr0 = sp.x * o0[b].x - sp.y * o0[b].y, xi0 = sp.x * o0[b].y + sp.y * o0[b].x;
-                    const float xr1 = sp.z * o1[b].x - sp.w * o1[b].y, xi1 = sp.z * o1[b].y + sp.w * o1[b].x;
+            } else {
+                // near the object's edge (or an odd row length): complex by complex, each column wrapped
+#pragma unroll 1
+                for (int u = 0; u < 16; u++) {
+                    const int i = u >> 1, c = 64 * (u & 1) + 2 * lane;
+                    const float2 *orow = a.object + (size_t)wrap_once(y0 + i, a.object_rows) * OC;
+                    const int x = cc + (c < kN / 2 ? c : c - kN);
+                    const float4 sp = __ldg(reinterpret_cast<const float4 *>(S + i * kN + 64 * (u & 1)));
+                    const float2 o0 = __ldg(orow + wrap_once(x, OC)), o1 = __ldg(orow + wrap_once(x + 1, OC));
                     uint32_t rh, rl, ih, il;
-                    split_bf16x2(xr0, xr1, rh, rl);
-                    split_bf16x2(xi0, xi1, ih, il);
-                    const uint32_t off = kmajor_offset(r, c);
+                    split_bf16x2(sp.x * o0.x - sp.y * o0.y, sp.z * o1.x - sp.w * o1.y, rh, rl);
+                    split_bf16x2(sp.x * o0.y + sp.y * o0.x, sp.z * o1.y + sp.w * o1.x, ih, il);
+                    const uint32_t off = kmajor_offset(8 * warp + i, c);
                     *reinterpret_cast<uint32_t *>(planes + (kReHi + 0) * kPlaneBytes + off) = rh;
                     *reinterpret_cast<uint32_t *>(planes + (kReHi + 1) * kPlaneBytes + off) = rl;
                     *reinterpret_cast<uint32_t *>(planes + (kImHi + 0) * kPlaneBytes + off) = ih;

@@ -32,6 +32,23 @@ def test_split_bf16_against_fp64_oracle(fractional):
     assert np.all(np.abs(r.errors - ref[2]) <= 1e-4 * ref[2]), (r.errors, ref[2])
 
 
+@pytest.mark.parametrize("shift,odd_width", [(-40, False), (0, True)])
+def test_split_bf16_patches_across_the_object_edge(shift, odd_width):
+    """Windows that wrap around the periodic object's edge, and an object of odd width, take the kernel's
+    complex-by-complex exit-wave gather instead of its aligned row loads; both must match the FP64 oracle."""
+    import cubokit_b200 as cb
+    s = scenes.raster_scene(scan=4, det=128, step=4, seed=17)
+    positions = s["positions"].copy()
+    positions[:, 1] += shift
+    obj = np.ascontiguousarray(s["object"][:, :-1]) if odd_width else s["object"]
+    ref = c_oracle.reconstruct(s["amplitudes"].astype(np.float32), positions, obj, s["probe"], iterations=3)
+    r = cb.SingleslicePtychography.reconstruct(s["amplitudes"], positions, obj, s["probe"], iterations=3,
+                                               precision="split_bf16")
+    assert rel_l2(r.object, ref[0]) <= 1e-4, rel_l2(r.object, ref[0])
+    assert rel_l2(r.probe, ref[1]) <= 1e-4, rel_l2(r.probe, ref[1])
+    assert np.all(np.abs(r.errors - ref[2]) <= 1e-4 * ref[2]), (r.errors, ref[2])
+
+
 def test_split_bf16_is_deterministic_and_close_to_fp32():
     import cubokit_b200 as cb
     s = scenes.raster_scene(scan=4, det=128, step=4, seed=17)
