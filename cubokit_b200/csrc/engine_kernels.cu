@@ -119,25 +119,54 @@ __global__ void __launch_bounds__(NT, 1) position_pass_kernel(PositionPassArgs<T
 
 constexpr int kChunk = 256;
 
+constexpr int kGatherChunk = 128;   // candidates whose window offsets are staged at a time
+constexpr int kMaxTileSide = 64;    // the longest tile side (tiles are 32 x 8, 16 x 16 or 64 x 4)
+
+// Per object pixel, the sum over the positions covering it (ascending, as listed for its tile) of conj(S) dpsi and
+// |S|^2 (Ptychography.swift:351-358 as a gather).  For each chunk of candidates the tile's window offsets are staged
+// first: per candidate, the residual row offset kr * columns of each tile row and the residual column kc of each tile
+// column (corner-centred, periodic; negative where the window does not reach), so a pixel's residual index is one sum.
 template <typename T>
 __global__ void __launch_bounds__(kGatherThreads) object_gather_kernel(ObjectGatherArgs<T> a) {
-    __shared__ int s_p[kChunk], s_rr[kChunk], s_cc[kChunk], s_cls[kChunk];
+    __shared__ int s_p[kGatherChunk], s_cls[kGatherChunk];
+    __shared__ int s_off[kGatherChunk][kMaxTileSide + kGatherThreads / kMaxTileSide + 4];  // rows, then columns
     __shared__ double scratch[32];
     const int tile = blockIdx.x;
     const int tx = tile % a.tiles_x, ty = tile / a.tiles_x;
+    const int x0 = tx * a.tile_w, y0 = ty * a.tile_h;
     // consecutive threads take consecutive object columns, hence consecutive addresses of each [row][column] residual
-    const int x = tx * a.tile_w + (threadIdx.x % a.tile_w);
-    const int y = ty * a.tile_h + threadIdx.x / a.tile_w;
+    const int lx = threadIdx.x % a.tile_w, ly = threadIdx.x / a.tile_w;
+    const int x = x0 + lx, y = y0 + ly;
     const bool inside = x < a.object_columns && y < a.object_rows;
+    const int entries = a.tile_h + a.tile_w;
+    constexpr int kInvalid = -(1 << 30);
     C2<T> g = mk<T>(0, 0);
     T w = 0;
     const int begin = a.tile_start[tile], end = a.tile_start[tile + 1];
-    for (int base = begin; base < end; base += kChunk) {
-        const int cnt = min(kChunk, end - base);
+    for (int base = begin; base < end; base += kGatherChunk) {
+        const int cnt = min(kGatherChunk, end - base);
         __syncthreads();
         for (int i = threadIdx.x; i < cnt; i += kGatherThreads) {
             const int p = a.tile_list[base + i];
-            s_p[i] = p; s_rr[i] = a.scan.rr[p]; s_cc[i] = a.scan.cc[p]; s_cls[i] = a.scan.cls[p];
+            s_p[i] = p;
+            s_cls[i] = a.scan.cls[p];
+        }
+        for (int e = threadIdx.x; e < cnt * entries; e += kGatherThreads) {
+            const int i = e / entries, f = e - i * entries;
+            const int p = a.tile_list[base + i];
+            int v;
+            if (f < a.tile_h) {  // tile row y0 + f
+                int dy = y0 + f - a.scan.rr[p];
+                dy = dy < 0 ? dy + a.object_rows : (dy >= a.object_rows ? dy - a.object_rows : dy);
+                const int kr = window_index(dy, a.rows, a.object_rows);
+                v = kr >= 0 ? kr * a.columns : kInvalid;
+            } else {  // tile column x0 + f - tile_h
+                int dx = x0 + f - a.tile_h - a.scan.cc[p];
+                dx = dx < 0 ? dx + a.object_columns : (dx >= a.object_columns ? dx - a.object_columns : dx);
+                const int kc = window_index(dx, a.columns, a.object_columns);
+                v = kc >= 0 ? kc : kInvalid;
+            }
+            s_off[i][f] = v;
         }
         __syncthreads();
         if (inside) {
@@ -145,18 +174,7 @@ __global__ void __launch_bounds__(kGatherThreads) object_gather_kernel(ObjectGat
             for (int i = 0; i < cnt; i += 4) {
                 int k[4];
 #pragma unroll
-                for (int u = 0; u < 4; u++) {
-                    k[u] = -1;
-                    if (i + u < cnt) {
-                        int dy = y - s_rr[i + u];
-                        if (dy < 0) dy += a.object_rows;
-                        const int kr = window_index(dy, a.rows, a.object_rows);
-                        int dx = x - s_cc[i + u];
-                        if (dx < 0) dx += a.object_columns;
-                        const int kc = window_index(dx, a.columns, a.object_columns);
-                        if (kr >= 0 && kc >= 0) k[u] = kr * a.columns + kc;
-                    }
-                }
+                for (int u = 0; u < 4; u++) k[u] = i + u < cnt ? s_off[i + u][ly] + s_off[i + u][a.tile_h + lx] : -1;
                 C2<T> d[4], sv[4];
 #pragma unroll
                 for (int u = 0; u < 4; u++) {
