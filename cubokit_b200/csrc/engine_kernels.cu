@@ -206,33 +206,54 @@ __global__ void __launch_bounds__(kGatherThreads) object_gather_kernel(ObjectGat
 
 constexpr int kProbeThreads = 256;
 
+// Per detector pixel k and position group, the sum over the group's positions (in order) of conj(O[window]) dpsi and
+// |O|^2.  Per chunk of positions the window's object base rr * OC + cc is staged, or -1 where the window wraps around
+// the object's edge; an interior window's pixel is then base + (offr * OC + offc), the wrapped ones are computed in full.
 template <typename T>
 __global__ void __launch_bounds__(kProbeThreads) probe_gather_kernel(ProbeGatherArgs<T> a) {
     __shared__ int s_rr[kChunk], s_cc[kChunk];
+    __shared__ long long s_base[kChunk];
     const int k = blockIdx.x * kProbeThreads + threadIdx.x;  // pixel index, [row][column]
     const int group = blockIdx.y;
     const int p0 = (int)((long long)a.count * group / a.groups), p1 = (int)((long long)a.count * (group + 1) / a.groups);
     const bool valid = k < a.n;
     const int kr = valid ? k / a.columns : 0, kc = valid ? k - kr * a.columns : 0;
     const int offr = corner_offset(kr, a.rows), offc = corner_offset(kc, a.columns);
+    const long long shift = (long long)offr * a.object_columns + offc;
+    // the window [rr - low_r, rr + high_r) x [cc - low_c, cc + high_c) stays inside the object
+    const int low_r = a.rows / 2, high_r = (a.rows + 1) / 2, low_c = a.columns / 2, high_c = (a.columns + 1) / 2;
     C2<T> g = mk<T>(0, 0);
     T w = 0;
     for (int base = p0; base < p1; base += kChunk) {
         const int cnt = min(kChunk, p1 - base);
         __syncthreads();
-        for (int i = threadIdx.x; i < cnt; i += kProbeThreads) { s_rr[i] = a.scan.rr[base + i]; s_cc[i] = a.scan.cc[base + i]; }
+        for (int i = threadIdx.x; i < cnt; i += kProbeThreads) {
+            const int rr = a.scan.rr[base + i], cc = a.scan.cc[base + i];
+            s_rr[i] = rr;
+            s_cc[i] = cc;
+            const bool interior = rr >= low_r && rr + high_r <= a.object_rows && cc >= low_c && cc + high_c <= a.object_columns;
+            s_base[i] = interior ? (long long)rr * a.object_columns + cc : -1;
+        }
         __syncthreads();
         if (valid) {
+            const C2<T> *dp = a.dpsi + (size_t)base * a.n + k;
             // four positions at a time: independent loads, sums in position order
             for (int i = 0; i < cnt; i += 4) {
                 C2<T> o[4], d[4];
 #pragma unroll
                 for (int u = 0; u < 4; u++) {
                     if (i + u < cnt) {
-                        const int y = wrap_once(s_rr[i + u] + offr, a.object_rows);
-                        const int x = wrap_once(s_cc[i + u] + offc, a.object_columns);
-                        o[u] = a.object[(size_t)y * a.object_columns + x];
-                        d[u] = a.dpsi[(size_t)(base + i + u) * a.n + k];
+                        const long long b0 = s_base[i + u];
+                        long long idx;
+                        if (b0 >= 0) {
+                            idx = b0 + shift;
+                        } else {
+                            const int y = wrap_once(s_rr[i + u] + offr, a.object_rows);
+                            const int x = wrap_once(s_cc[i + u] + offc, a.object_columns);
+                            idx = (long long)y * a.object_columns + x;
+                        }
+                        o[u] = a.object[idx];
+                        d[u] = dp[(size_t)(i + u) * a.n];
                     }
                 }
 #pragma unroll
