@@ -117,6 +117,11 @@ cudaError_t launch_object_update(C2<T> *object, const C2<T> *grad, const T *weig
 cudaError_t launch_error_reduce(const double *error, long long count, double divisor, double *errors, int *iteration,
                                 double *scratch, cudaStream_t s);
 int error_reduce_scratch();  // doubles of scratch launch_error_reduce needs
+// object-gather candidate lists on the device: without `list`, counts[tile] = the number of positions whose window
+// touches the tile; with it (and starts = exclusive sums of the counts), those positions in ascending order
+cudaError_t launch_tile_lists(const int *rr, const int *cc, int count, int rows, int columns, int object_rows,
+                              int object_columns, int tile_w, int tile_h, int tiles_x, int tiles, int *counts,
+                              const int *starts, int *list, cudaStream_t s);
 // sum A^2 of `count` amplitudes into scratch[amplitude_check_scratch() - 1] (FP64, fixed order); *bad = 1 if any is not
 // finite and non-negative (*bad is not cleared)
 cudaError_t launch_amplitude_check(const float *amplitudes, long long count, double *scratch, int *bad, cudaStream_t s);

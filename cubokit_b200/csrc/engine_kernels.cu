@@ -202,6 +202,40 @@ __global__ void __launch_bounds__(kGatherThreads) object_gather_kernel(ObjectGat
     if (threadIdx.x == 0) a.tile_max[tile] = m;
 }
 
+// ------------------------------------------------------------------------------------------------ candidate lists
+
+// Whether the cyclic window [start, start + length) of a periodic axis of `size` meets [t0, t0 + len).
+__device__ __forceinline__ bool cyclic_overlap(int start, int length, int t0, int len, int size) {
+    int d = (t0 - start) % size;
+    if (d < 0) d += size;
+    return d < length || d + len > size;
+}
+
+// One warp per object-gather tile: the positions whose window touches the tile, in ascending order.  Without `list`
+// it counts them into counts[tile]; with it, it writes them from starts[tile] on.  A window covers the object rows
+// rr - rows/2 .. rr + (rows+1)/2 - 1 and the columns likewise, wrapped.
+__global__ void __launch_bounds__(256) tile_lists_kernel(const int *rr, const int *cc, int count, int rows, int columns,
+                                                         int object_rows, int object_columns, int tile_w, int tile_h,
+                                                         int tiles_x, int tiles, int *counts, const int *starts,
+                                                         int *list) {
+    const int tile = blockIdx.x * 8 + (threadIdx.x >> 5), lane = threadIdx.x & 31;
+    if (tile >= tiles) return;
+    const int ty = tile / tiles_x, tx = tile - ty * tiles_x;
+    const int y0 = ty * tile_h, x0 = tx * tile_w;
+    const int hy = min(tile_h, object_rows - y0), hx = min(tile_w, object_columns - x0);
+    int n = 0;
+    const int base = list ? starts[tile] : 0;
+    for (int i0 = 0; i0 < count; i0 += 32) {
+        const int i = i0 + lane;
+        const bool hit = i < count && cyclic_overlap(rr[i] - rows / 2, rows, y0, hy, object_rows) &&
+                         cyclic_overlap(cc[i] - columns / 2, columns, x0, hx, object_columns);
+        const unsigned ballot = __ballot_sync(0xffffffffu, hit);
+        if (list && hit) list[base + n + __popc(ballot & ((1u << lane) - 1u))] = i;
+        n += __popc(ballot);
+    }
+    if (!list && lane == 0) counts[tile] = n;
+}
+
 // ------------------------------------------------------------------------------------------------ probe gather
 
 constexpr int kProbeThreads = 256;
@@ -452,6 +486,14 @@ cudaError_t launch_object_update(C2<T> *object, const C2<T> *grad, const T *weig
 }
 
 int error_reduce_scratch() { return kErrorBlocks; }
+
+cudaError_t launch_tile_lists(const int *rr, const int *cc, int count, int rows, int columns, int object_rows,
+                              int object_columns, int tile_w, int tile_h, int tiles_x, int tiles, int *counts,
+                              const int *starts, int *list, cudaStream_t s) {
+    tile_lists_kernel<<<(tiles + 7) / 8, 256, 0, s>>>(rr, cc, count, rows, columns, object_rows, object_columns, tile_w,
+                                                      tile_h, tiles_x, tiles, counts, starts, list);
+    return cudaGetLastError();
+}
 
 int amplitude_check_scratch() { return kAmplitudeBlocks + 1; }
 

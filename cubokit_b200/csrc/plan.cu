@@ -278,40 +278,28 @@ void build_plan(cubo_ptycho_plan *p, const cubo_ptycho_problem *pr) {
     p->tiles_x = (p->OC + p->tile_w - 1) / p->tile_w;
     const int tiles_y = (p->OR + p->tile_h - 1) / p->tile_h;
     p->tiles = p->tiles_x * tiles_y;
-    std::vector<int> counts(p->tiles + 1, 0);
-    std::vector<int> mark_y(tiles_y, -1), mark_x(p->tiles_x, -1);
-    std::vector<int> ty_list, tx_list;
-    auto tiles_of = [&](int i) {
-        ty_list.clear();
-        tx_list.clear();
-        for (int k = 0; k < R; k++) {
-            const int y = (int)wrap_ll((long long)rr[i] + corner_offset(k, R), p->OR);
-            const int t = y / p->tile_h;
-            if (mark_y[t] != i) { mark_y[t] = i; ty_list.push_back(t); }
+    {
+        // counted and listed on the device from the wrapped centres (one warp per tile, positions ascending)
+        check(p->tile_start.alloc((size_t)(p->tiles + 1) * sizeof(int)), "cudaMalloc");
+        check(launch_tile_lists(p->rr.as<int>(), p->cc.as<int>(), P, R, C, p->OR, p->OC, p->tile_w, p->tile_h, p->tiles_x,
+                                p->tiles, p->tile_start.as<int>(), nullptr, nullptr, s), "count candidates");
+        std::vector<int> counts(p->tiles + 1, 0);
+        check(cudaMemcpyAsync(counts.data(), p->tile_start.ptr, (size_t)p->tiles * sizeof(int), cudaMemcpyDeviceToHost, s),
+              "download counts");
+        check(cudaStreamSynchronize(s), "count candidates");
+        long long total = 0;
+        for (int t = 0; t < p->tiles; t++) {  // exclusive sums
+            const int c = counts[t];
+            counts[t] = (int)total;
+            total += c;
         }
-        for (int k = 0; k < C; k++) {
-            const int x = (int)wrap_ll((long long)cc[i] + corner_offset(k, C), p->OC);
-            const int t = x / p->tile_w;
-            if (mark_x[t] != i) { mark_x[t] = i; tx_list.push_back(t); }
-        }
-    };
-    for (int i = 0; i < P; i++) {
-        tiles_of(i);
-        for (int ty : ty_list)
-            for (int tx : tx_list) counts[ty * p->tiles_x + tx + 1]++;
+        if (total > INT32_MAX) fail(CUBO_PTYCHO_UNSUPPORTED, "object-gather candidate lists exceed 2^31 entries");
+        counts[p->tiles] = (int)total;
+        upload(p->tile_start, counts, s);
+        check(p->tile_list.alloc((size_t)std::max<long long>(total, 1) * sizeof(int)), "cudaMalloc");
+        check(launch_tile_lists(p->rr.as<int>(), p->cc.as<int>(), P, R, C, p->OR, p->OC, p->tile_w, p->tile_h, p->tiles_x,
+                                p->tiles, nullptr, p->tile_start.as<int>(), p->tile_list.as<int>(), s), "list candidates");
     }
-    for (int t = 0; t < p->tiles; t++) counts[t + 1] += counts[t];
-    std::vector<int> list((size_t)counts[p->tiles]);
-    std::vector<int> fill(counts.begin(), counts.end() - 1);
-    std::fill(mark_y.begin(), mark_y.end(), -1);
-    std::fill(mark_x.begin(), mark_x.end(), -1);
-    for (int i = 0; i < P; i++) {
-        tiles_of(i);
-        for (int ty : ty_list)
-            for (int tx : tx_list) list[fill[ty * p->tiles_x + tx]++] = i;
-    }
-    upload(p->tile_start, counts, s);
-    upload(p->tile_list, list, s);
     // ---- amplitudes (Float32, [position][row][column]; the 128 x 128 kernel's register order when it runs)
     check(p->amplitudes.alloc((size_t)P * n * sizeof(float)), "cudaMalloc amplitudes");
     check(cudaMemcpyAsync(p->amplitudes.ptr, pr->amplitudes, (size_t)P * n * sizeof(float), cudaMemcpyHostToDevice, s),
