@@ -3,8 +3,10 @@
 The engine is ``libcuboptycho.so`` (CUDA kernels behind the C ABI of ``include/cubo_ptycho.h``); this package is its
 Python binding and the host-side mirror of CuboPtycho's API.
 """
-from .ptycho import (Batch, CancellationError, Context, DeviceError, Plan, PtychographyError, PtychographyProbe, Result,
-                     SingleslicePtychography, UnsupportedError, context, electron_wavelength)
+from .ptycho import (Batch, CancellationError, Context, DeviceError, Plan, PtychographyAmplitudes, PtychographyError,
+                     PtychographyPreparation, PtychographyProbe, Result, SingleslicePtychography, UnsupportedError, context,
+                     electron_wavelength)
 
-__all__ = ["Batch", "CancellationError", "Context", "DeviceError", "Plan", "PtychographyError", "PtychographyProbe", "Result",
-           "SingleslicePtychography", "UnsupportedError", "context", "electron_wavelength"]
+__all__ = ["Batch", "CancellationError", "Context", "DeviceError", "Plan", "PtychographyAmplitudes", "PtychographyError",
+           "PtychographyPreparation", "PtychographyProbe", "Result", "SingleslicePtychography", "UnsupportedError", "context",
+           "electron_wavelength"]

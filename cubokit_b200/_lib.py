@@ -19,11 +19,14 @@ VARIANT_AUTO, VARIANT_GENERIC = 0, 1
 PROGRESS_FN = C.CFUNCTYPE(None, C.c_int, C.c_int, C.c_void_p)
 
 
+SHIFT_BILINEAR, SHIFT_CUBIC_SPLINE = 0, 1
+
+
 class Problem(C.Structure):
     _fields_ = [
         ("rows", C.c_int), ("columns", C.c_int), ("object_rows", C.c_int), ("object_columns", C.c_int),
         ("count", C.c_int), ("amplitudes", C.POINTER(C.c_float)), ("position_rows", C.POINTER(C.c_double)),
-        ("position_columns", C.POINTER(C.c_double)),
+        ("position_columns", C.POINTER(C.c_double)), ("amplitudes_on_device", C.c_int),
     ]
 
 
@@ -62,6 +65,12 @@ SIGNATURES = {
                                                 C.POINTER(C.c_longlong), C.POINTER(C.c_int)]),
     "cubo_ptycho_plan_launch_count": (C.c_longlong, [C.c_void_p]),
     "cubo_ptycho_probe_build": (C.c_int, [C.c_void_p, C.c_int, C.c_int] + [C.c_double] * 9 + [C.c_int, _dp, _dp, _dp]),
+    "cubo_ptycho_prepare_amplitudes": (C.c_int, [C.c_void_p, C.c_int, C.c_int, C.c_int, C.c_void_p, _dp, _dp, C.c_int,
+                                                 C.c_void_p, _dp, _dp]),
+    "cubo_ptycho_set_timing": (C.c_int, [C.c_void_p, C.c_int]),
+    "cubo_ptycho_prepare_kernel_stats": (C.c_int, [C.c_void_p, _dp, C.POINTER(C.c_longlong)]),
+    "cubo_ptycho_prepare_amplitudes_device": (C.c_int, [C.c_void_p, C.c_int, C.c_int, C.c_int, C.c_void_p, _dp, _dp,
+                                                        C.c_int, C.c_void_p, _dp, _dp]),
     "cubo_ptycho_plan_forward": (C.c_int, [C.c_void_p, _dp]),
     "cubo_ptycho_plan_backward": (C.c_int, [C.c_void_p, C.c_int, _dp, _dp, _dp, _dp, _dp]),
     "cubo_ptycho_batch_create": (C.c_int, [C.c_void_p, C.c_int, C.POINTER(Problem), C.POINTER(Params),

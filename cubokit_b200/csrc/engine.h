@@ -99,6 +99,26 @@ cudaError_t configure_bf16();
 cudaError_t launch_bf16(const Bf16Args &a, int ctas, cudaStream_t s);
 cudaError_t launch_permute_bf16_amplitudes(const float *in, float *out, long long positions, cudaStream_t s);
 
+// prepare.cu: amplitude preprocessing (pattern shift, square root, mean intensities)
+// dynamic shared memory of one CTA: cubic, the coefficients in FP64 and the prefilter's carries; when `staged`, one
+// (cubic) or two (bilinear) Float32 patterns copied in ahead of use
+size_t prepare_smem(int rows, int columns, bool cubic, bool staged);
+int prepare_max_line();         // the longest line the cubic prefilter takes (either axis)
+int prepare_scratch_doubles();  // scratch of launch_prepare_means; the two means are its last two values
+int prepare_sums_per_pattern();  // values launch_prepare writes per pattern into `sums`
+cudaError_t configure_prepare();
+// patterns [count][rows][columns] (Float32) -> amplitudes (same layout); sums[p * prepare_sums_per_pattern() ..] = the
+// partial sums (of the shifted pattern p, of its positive part) of each of the CTA's warps, in pairs. *bad gains bit 1 if a value is not finite (*bad is not cleared). Patterns
+// are staged in shared memory ahead of use when that fits in smem_limit bytes and the copy's alignment allows it.
+struct PatternShift {  // one pattern's origin: its whole part wrapped into [0, rows) x [0, columns), and its fraction
+    double row_fraction, column_fraction;
+    int row, column;
+};
+cudaError_t launch_prepare(const float *cube, int count, int rows, int columns, const PatternShift *shifts, bool cubic,
+                           float *amplitudes, double *sums, int *bad, int ctas, size_t smem_limit, cudaStream_t s);
+// the mean intensities over `count` patterns' partial sums, in a fixed order
+cudaError_t launch_prepare_means(const double *sums, int count, double *scratch, cudaStream_t s);
+
 constexpr int kTileW = 32, kTileH = 8;   // object-gather tile (one pixel per thread)
 constexpr int kGatherThreads = kTileW * kTileH;
 

@@ -21,6 +21,9 @@ struct cubo_ptycho_context {
     int device = 0;
     cudaStream_t stream = nullptr;
     std::string last_error;
+    bool timing = false;           // CUDA events around each preprocessing kernel launch
+    double prepare_ms = 0.0;       // their device time, summed
+    long long prepare_launches = 0;
 };
 
 namespace {
@@ -302,7 +305,8 @@ void build_plan(cubo_ptycho_plan *p, const cubo_ptycho_problem *pr) {
     }
     // ---- amplitudes (Float32, [position][row][column]; the 128 x 128 kernel's register order when it runs)
     check(p->amplitudes.alloc((size_t)P * n * sizeof(float)), "cudaMalloc amplitudes");
-    check(cudaMemcpyAsync(p->amplitudes.ptr, pr->amplitudes, (size_t)P * n * sizeof(float), cudaMemcpyHostToDevice, s),
+    check(cudaMemcpyAsync(p->amplitudes.ptr, pr->amplitudes, (size_t)P * n * sizeof(float),
+                          pr->amplitudes_on_device ? cudaMemcpyDeviceToDevice : cudaMemcpyHostToDevice, s),
           "upload amplitudes");
     {
         // every amplitude finite and non-negative, and sum A^2 (Ptychography.swift:247-259), in the supplied order
@@ -1101,6 +1105,170 @@ int cubo_ptycho_batch_run(cubo_ptycho_batch *b, int iterations, int synchronize)
             for (auto *p : b->plans) check_fault(p);
         }
     });
+}
+
+namespace {
+// PtychographyPreparation.amplitudes(from:origins:shift:) (PtychographyPreparation.swift:142-183); `on_device`: cube and
+// amplitudes are device pointers.  Host data moves in chunks of at most 256 MB, alternating between two streams so that
+// one chunk's upload overlaps the previous chunk's download; the per-pattern sums are kept for all patterns and summed
+// once at the end in a fixed order, so the result does not depend on the chunking.
+void prepare_amplitudes(cubo_ptycho_context *ctx, int count, int rows, int columns, const float *cube,
+                        const double *origin_rows, const double *origin_columns, int shift, float *amplitudes,
+                        double *mean_intensity, double *clipped_mean_intensity, bool on_device) {
+    // PtychographyPreparation.swift:148-159
+    if (!(count > 0 && rows > 1 && columns > 1)) fail(CUBO_PTYCHO_INVALID_INPUT, "cube shape");
+    const long long n = (long long)rows * columns;
+    if ((long long)count * n > (1LL << 40)) fail(CUBO_PTYCHO_INVALID_INPUT, "too many samples");
+    if (!cube || !origin_rows || !origin_columns || !amplitudes || !mean_intensity || !clipped_mean_intensity)
+        fail(CUBO_PTYCHO_INVALID_INPUT, "null input");
+    if (shift != CUBO_PTYCHO_SHIFT_BILINEAR && shift != CUBO_PTYCHO_SHIFT_CUBIC_SPLINE) fail(CUBO_PTYCHO_INVALID_INPUT, "shift");
+    for (int i = 0; i < count; i++)
+        if (!(std::isfinite(origin_rows[i]) && std::fabs(origin_rows[i]) < 1e9 && std::isfinite(origin_columns[i]) &&
+              std::fabs(origin_columns[i]) < 1e9))
+            fail(CUBO_PTYCHO_INVALID_INPUT, "origin");
+    int optin = 0, sms = 0;
+    check(cudaDeviceGetAttribute(&optin, cudaDevAttrMaxSharedMemoryPerBlockOptin, ctx->device), "attribute");
+    check(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, ctx->device), "attribute");
+    const bool cubic = shift == CUBO_PTYCHO_SHIFT_CUBIC_SPLINE;
+    const size_t smem_limit = (size_t)optin - 1024;
+    if (n > (1LL << 30) || (cubic && (prepare_smem(rows, columns, true, false) > smem_limit ||
+                                      std::max(rows, columns) > prepare_max_line())))
+        fail(CUBO_PTYCHO_UNSUPPORTED, "pattern of " + std::to_string(n) + " pixels exceeds one CTA's shared memory");
+    check(configure_prepare(), "configure preprocessing");
+    const int ctas = sms;  // CTAs of 1024 threads, one per SM
+    cudaStream_t s0 = ctx->stream;
+    DeviceBuffer sums, scratch, bad, dorig;
+    check(sums.alloc((size_t)prepare_sums_per_pattern() * count * sizeof(double)), "cudaMalloc");
+    check(scratch.alloc((size_t)prepare_scratch_doubles() * sizeof(double)), "cudaMalloc");
+    check(bad.alloc(sizeof(int)), "cudaMalloc");
+    check(cudaMemsetAsync(bad.ptr, 0, sizeof(int), s0), "memset");
+    // Swift :301-306, :321-328: the whole part floor(origin) (wrapped into the pattern) and the fraction
+    // origin - floor(origin), which is exact
+    std::vector<PatternShift> shifts((size_t)count);
+    for (int i = 0; i < count; i++) {
+        const double fr = std::floor(origin_rows[i]), fc = std::floor(origin_columns[i]);
+        const long long wr = (long long)fr % rows, wc = (long long)fc % columns;
+        shifts[i] = PatternShift{origin_rows[i] - fr, origin_columns[i] - fc, (int)(wr < 0 ? wr + rows : wr),
+                                 (int)(wc < 0 ? wc + columns : wc)};
+    }
+    upload(dorig, shifts, s0);
+    const PatternShift *dshift = dorig.as<PatternShift>();
+    // with timing on, one event pair around each kernel launch (on its stream), read after the final synchronize
+    struct EventPair {
+        cudaEvent_t start = nullptr, stop = nullptr;
+    };
+    std::vector<EventPair> timed;
+    struct ReleaseEvents {
+        std::vector<EventPair> &v;
+        ~ReleaseEvents() {
+            for (auto &e : v) {
+                if (e.start) cudaEventDestroy(e.start);
+                if (e.stop) cudaEventDestroy(e.stop);
+            }
+        }
+    } release_events{timed};
+    auto timed_launch = [&](cudaStream_t st, const std::function<cudaError_t()> &launch) {
+        if (!ctx->timing) return check(launch(), "preprocess");
+        timed.emplace_back();
+        check(cudaEventCreate(&timed.back().start), "cudaEventCreate");
+        check(cudaEventCreate(&timed.back().stop), "cudaEventCreate");
+        check(cudaEventRecord(timed.back().start, st), "cudaEventRecord");
+        check(launch(), "preprocess");
+        check(cudaEventRecord(timed.back().stop, st), "cudaEventRecord");
+    };
+    if (on_device) {
+        timed_launch(s0, [&] {
+            return launch_prepare(cube, count, rows, columns, dshift, cubic, amplitudes, sums.as<double>(),
+                                  bad.as<int>(), ctas, smem_limit, s0);
+        });
+    } else {
+        const long long chunk = std::max<long long>(1, std::min<long long>(count, (256LL << 20) / (n * 4)));
+        cudaStream_t s1 = nullptr;
+        cudaEvent_t ready = nullptr, done[2] = {nullptr, nullptr};
+        check(cudaStreamCreateWithFlags(&s1, cudaStreamNonBlocking), "cudaStreamCreate");
+        struct Release {
+            cudaStream_t &s; cudaEvent_t &a, &b0, &b1;
+            ~Release() { if (a) cudaEventDestroy(a); if (b0) cudaEventDestroy(b0); if (b1) cudaEventDestroy(b1); if (s) cudaStreamDestroy(s); }
+        } release{s1, ready, done[0], done[1]};
+        check(cudaEventCreateWithFlags(&ready, cudaEventDisableTiming), "cudaEventCreate");
+        check(cudaEventCreateWithFlags(&done[0], cudaEventDisableTiming), "cudaEventCreate");
+        check(cudaEventCreateWithFlags(&done[1], cudaEventDisableTiming), "cudaEventCreate");
+        check(cudaEventRecord(ready, s0), "cudaEventRecord");  // origins uploaded, flag cleared
+        check(cudaStreamWaitEvent(s1, ready, 0), "cudaStreamWaitEvent");
+        DeviceBuffer in[2], out[2];
+        for (int b = 0; b < 2; b++) {
+            check(in[b].alloc((size_t)(chunk * n) * sizeof(float)), "cudaMalloc");
+            check(out[b].alloc((size_t)(chunk * n) * sizeof(float)), "cudaMalloc");
+        }
+        int slot = 0;
+        for (long long first = 0; first < count; first += chunk, slot ^= 1) {
+            const int c = (int)std::min<long long>(chunk, count - first);
+            cudaStream_t st = slot ? s1 : s0;
+            check(cudaMemcpyAsync(in[slot].ptr, cube + first * n, (size_t)(c * n) * sizeof(float), cudaMemcpyHostToDevice,
+                                  st), "upload cube");
+            timed_launch(st, [&] {
+                return launch_prepare(in[slot].as<float>(), c, rows, columns, dshift + first, cubic,
+                                      out[slot].as<float>(), sums.as<double>() + (size_t)prepare_sums_per_pattern() * first,
+                                      bad.as<int>(), ctas, smem_limit, st);
+            });
+            check(cudaMemcpyAsync(amplitudes + first * n, out[slot].ptr, (size_t)(c * n) * sizeof(float),
+                                  cudaMemcpyDeviceToHost, st), "download amplitudes");
+        }
+        check(cudaEventRecord(done[1], s1), "cudaEventRecord");
+        check(cudaStreamWaitEvent(s0, done[1], 0), "cudaStreamWaitEvent");
+        check(cudaStreamSynchronize(s1), "preprocess");
+    }
+    check(launch_prepare_means(sums.as<double>(), count, scratch.as<double>(), s0), "mean intensities");
+    double means[2] = {0, 0};
+    int any_bad = 0;
+    check(cudaMemcpyAsync(means, scratch.as<double>() + prepare_scratch_doubles() - 2, sizeof(means),
+                          cudaMemcpyDeviceToHost, s0), "download");
+    check(cudaMemcpyAsync(&any_bad, bad.ptr, sizeof(int), cudaMemcpyDeviceToHost, s0), "download");
+    check(cudaStreamSynchronize(s0), "preprocess");
+    for (auto &e : timed) {
+        float ms = 0.0f;
+        check(cudaEventElapsedTime(&ms, e.start, e.stop), "cudaEventElapsedTime");
+        ctx->prepare_ms += ms;
+        ctx->prepare_launches += 1;
+    }
+    if (any_bad) fail(CUBO_PTYCHO_INVALID_INPUT, "cube value not finite");
+    *mean_intensity = means[0];
+    *clipped_mean_intensity = means[1];
+}
+}  // namespace
+
+int cubo_ptycho_prepare_amplitudes(cubo_ptycho_context *ctx, int count, int rows, int columns, const float *cube,
+                                   const double *origin_rows, const double *origin_columns, int shift, float *amplitudes,
+                                   double *mean_intensity, double *clipped_mean_intensity) {
+    return run_guarded(ctx, [&] {
+        prepare_amplitudes(ctx, count, rows, columns, cube, origin_rows, origin_columns, shift, amplitudes, mean_intensity,
+                           clipped_mean_intensity, false);
+    });
+}
+
+int cubo_ptycho_prepare_amplitudes_device(cubo_ptycho_context *ctx, int count, int rows, int columns,
+                                          const float *cube_device, const double *origin_rows,
+                                          const double *origin_columns, int shift, float *amplitudes_device,
+                                          double *mean_intensity, double *clipped_mean_intensity) {
+    return run_guarded(ctx, [&] {
+        prepare_amplitudes(ctx, count, rows, columns, cube_device, origin_rows, origin_columns, shift, amplitudes_device,
+                           mean_intensity, clipped_mean_intensity, true);
+    });
+}
+
+int cubo_ptycho_set_timing(cubo_ptycho_context *ctx, int enabled) {
+    if (!ctx) return CUBO_PTYCHO_INVALID_INPUT;
+    ctx->timing = enabled != 0;
+    ctx->prepare_ms = 0.0;
+    ctx->prepare_launches = 0;
+    return CUBO_PTYCHO_OK;
+}
+
+int cubo_ptycho_prepare_kernel_stats(cubo_ptycho_context *ctx, double *ms, long long *launches) {
+    if (!ctx || !ms || !launches) return CUBO_PTYCHO_INVALID_INPUT;
+    *ms = ctx->prepare_ms;
+    *launches = ctx->prepare_launches;
+    return CUBO_PTYCHO_OK;
 }
 
 int cubo_ptycho_probe_build(cubo_ptycho_context *ctx, int rows, int columns, double row_sampling, double column_sampling,

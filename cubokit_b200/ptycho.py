@@ -72,6 +72,16 @@ class Context:
     def synchronize(self):
         self.check(self.lib.cubo_ptycho_synchronize(self.handle))
 
+    def set_timing(self, enabled: bool):
+        """CUDA events around each preprocessing kernel launch (clears the totals)."""
+        self.check(self.lib.cubo_ptycho_set_timing(self.handle, 1 if enabled else 0))
+
+    def prepare_kernel_stats(self) -> tuple[float, int]:
+        """(device milliseconds, launches) of the preprocessing kernel since timing was switched on."""
+        ms, launches = C.c_double(), C.c_longlong()
+        self.check(self.lib.cubo_ptycho_prepare_kernel_stats(self.handle, C.byref(ms), C.byref(launches)))
+        return ms.value, launches.value
+
     def close(self):
         if getattr(self, "handle", None):
             self.lib.cubo_ptycho_destroy(self.handle)
@@ -115,6 +125,16 @@ def _ptr(a, t=C.c_double):
     return a.ctypes.data_as(C.POINTER(t))
 
 
+def _torch():
+    import torch
+    return torch
+
+
+def _is_cuda_tensor(x):
+    mod = type(x).__module__
+    return mod.startswith("torch") and getattr(x, "is_cuda", False)
+
+
 class _Inputs:
     """Keeps the ctypes structures and the arrays they point into alive for one call."""
 
@@ -126,14 +146,24 @@ class _Inputs:
         rows, columns = probe_shape
         positions = np.asarray(positions, np.float64).reshape(-1, 2) if np.size(positions) else np.zeros((0, 2))
         count = len(positions)
-        amps = np.asarray(amplitudes)
-        if amps.size != count * rows * columns:
+        on_device = _is_cuda_tensor(amplitudes)
+        if on_device:  # a CUDA tensor (e.g. PtychographyPreparation.amplitudes(..., keep_on_device=True)): no upload
+            if amplitudes.dtype != _torch().float32 or not amplitudes.is_contiguous():
+                raise PtychographyError("device amplitudes must be a contiguous float32 tensor")
+            size = amplitudes.numel()
+            self.amplitudes = amplitudes
+            amp_ptr = C.cast(C.c_void_p(amplitudes.data_ptr()), C.POINTER(C.c_float))
+        else:
+            amps = np.asarray(amplitudes)
+            size = amps.size
+            self.amplitudes = np.ascontiguousarray(amps, dtype=np.float32).ravel()
+            amp_ptr = _ptr(self.amplitudes, C.c_float)
+        if size != count * rows * columns:
             raise PtychographyError("amplitudes.count != positions * probe pixels")  # Ptychography.swift:248
-        self.amplitudes = np.ascontiguousarray(amps, dtype=np.float32).ravel()
         self.rows_ = np.ascontiguousarray(positions[:, 0])
         self.cols_ = np.ascontiguousarray(positions[:, 1])
-        self.problem = L.Problem(rows, columns, object_shape[0], object_shape[1], count, _ptr(self.amplitudes, C.c_float),
-                                 _ptr(self.rows_), _ptr(self.cols_))
+        self.problem = L.Problem(rows, columns, object_shape[0], object_shape[1], count, amp_ptr, _ptr(self.rows_),
+                                 _ptr(self.cols_), 1 if on_device else 0)
         self.params = L.Params()
         p = self.params
         p.iterations = int(iterations)
@@ -403,6 +433,86 @@ class Batch:
             self.close()
         except Exception:
             pass
+
+
+@dataclass
+class PtychographyAmplitudes:
+    """``PtychographyAmplitudes`` (``PtychographyPreparation.swift:62-75``): square-root amplitudes of a cube,
+    corner-centred, ``[position][row][column]`` (Float32 here: the engine's input), with the mean intensities."""
+    values: object                 # numpy float32 array, or a CUDA tensor when kept on the device
+    position_count: int
+    detector_rows: int
+    detector_columns: int
+    mean_intensity: float          # mean over positions of the summed shifted intensity, negatives included
+    clipped_mean_intensity: float  # the same with negative shifted values set to zero first
+
+    @property
+    def error_normalization(self):
+        """py4DSTEM's error normalisation for the engines: ``.meanIntensity(meanIntensity)``."""
+        return ("meanIntensity", self.mean_intensity)
+
+
+class PtychographyPreparation:
+    """``PtychographyPreparation.amplitudes(from:origins:shift:)`` (``PtychographyPreparation.swift:142-183``) on the
+    device: every pattern shifted so its origin sits on the corner pixel (bilinear or periodic cubic B-spline, wrapped,
+    FP64), then ``sqrt(max(., 0))``; see ``cubo_ptycho_prepare_amplitudes`` in ``include/cubo_ptycho.h``."""
+
+    SHIFTS = {"bilinear": L.SHIFT_BILINEAR, "cubicSpline": L.SHIFT_CUBIC_SPLINE}
+
+    @staticmethod
+    def amplitudes(cube, origins, shift: str = "cubicSpline", keep_on_device: bool = False,
+                   ctx: Optional[Context] = None, device: int = 0, out=None) -> PtychographyAmplitudes:
+        """``cube``: ``[position][row][column]`` (or ``[scan row][scan column][row][column]``), Float32 values, a numpy
+        array or a CUDA tensor.  ``origins``: ``(row, column)`` for every pattern (``PtychographyOrigins.uniform``) or
+        ``(rows, columns)`` arrays with one value per position (``.perPosition``).  ``keep_on_device``: return the
+        amplitudes as a CUDA tensor (for ``reconstruct`` / ``Plan`` without a host round trip).  ``out``: a contiguous
+        Float32 CUDA tensor of ``count * rows * columns`` values on the context's device to write the amplitudes into
+        (implies ``keep_on_device``; repeated calls then allocate no device memory for the result)."""
+        if shift not in PtychographyPreparation.SHIFTS:
+            raise PtychographyError(f"shift {shift!r}")
+        ctx = ctx or context(device)
+        cuda_in = _is_cuda_tensor(cube)
+        shape = tuple(cube.shape)
+        if len(shape) == 4:
+            shape = (shape[0] * shape[1], shape[2], shape[3])
+        if len(shape) != 3:
+            raise PtychographyError("cube must be [position][row][column]")
+        count, rows, columns = shape
+        o_rows, o_cols = origins
+        if np.ndim(o_rows) == 0 and np.ndim(o_cols) == 0:
+            o_rows = np.full(count, float(o_rows))
+            o_cols = np.full(count, float(o_cols))
+        o_rows = np.ascontiguousarray(o_rows, np.float64).ravel()
+        o_cols = np.ascontiguousarray(o_cols, np.float64).ravel()
+        if o_rows.size != count or o_cols.size != count:
+            raise PtychographyError("one origin per position")  # PtychographyPreparation.swift:157
+        mean, clipped = C.c_double(), C.c_double()
+        code = PtychographyPreparation.SHIFTS[shift]
+        if out is not None:
+            keep_on_device = True
+            if not (_is_cuda_tensor(out) and str(out.dtype) == "torch.float32" and out.is_contiguous()
+                    and out.numel() == count * rows * columns and out.device.index == ctx.device):
+                raise PtychographyError("out must be a contiguous Float32 CUDA tensor of count * rows * columns values "
+                                        "on the context's device")
+        if cuda_in or keep_on_device:
+            torch = _torch()
+            dev = torch.device("cuda", ctx.device)
+            src = cube if cuda_in else torch.from_numpy(np.ascontiguousarray(cube, np.float32))
+            src = src.to(dev, torch.float32).contiguous().reshape(count, rows, columns)
+            out = (torch.empty((count, rows, columns), dtype=torch.float32, device=dev) if out is None
+                   else out.view(count, rows, columns))
+            torch.cuda.synchronize(dev)
+            ctx.check(ctx.lib.cubo_ptycho_prepare_amplitudes_device(
+                ctx.handle, count, rows, columns, C.c_void_p(src.data_ptr()), _ptr(o_rows), _ptr(o_cols), code,
+                C.c_void_p(out.data_ptr()), C.byref(mean), C.byref(clipped)))
+            values = out if keep_on_device else out.cpu().numpy()
+        else:
+            src = np.ascontiguousarray(cube, np.float32).reshape(count, rows, columns)
+            values = np.empty((count, rows, columns), np.float32)
+            ctx.check(ctx.lib.cubo_ptycho_prepare_amplitudes(
+                ctx.handle, count, rows, columns, src.ctypes.data_as(C.c_void_p), _ptr(o_rows), _ptr(o_cols), code,
+                values.ctypes.data_as(C.c_void_p), C.byref(mean), C.byref(clipped)))
+        return PtychographyAmplitudes(values, count, rows, columns, mean.value, clipped.value)
 
 
 class PtychographyProbe:

@@ -70,6 +70,9 @@ typedef struct {
     const float *amplitudes;           /* count * rows * columns */
     const double *position_rows;       /* count */
     const double *position_columns;    /* count */
+    int amplitudes_on_device;          /* nonzero: `amplitudes` is device memory on the context's device (for example
+                                        * the output of cubo_ptycho_prepare_amplitudes_device), copied on the device
+                                        * instead of uploaded */
 } cubo_ptycho_problem;
 
 typedef void (*cubo_ptycho_progress_fn)(int completed, int total, void *user);
@@ -201,6 +204,39 @@ CUBO_PTYCHO_API int cubo_ptycho_probe_build(cubo_ptycho_context *context, int ro
                             double column_sampling, double wavelength, double cutoff, double rolloff, double defocus,
                             double astigmatism, double astigmatism_angle, double spherical_aberration, int term_count,
                             const double *terms, double *re, double *im);
+
+/* PtychographyShift (PtychographyPreparation.swift:56-62). */
+enum { CUBO_PTYCHO_SHIFT_BILINEAR = 0, CUBO_PTYCHO_SHIFT_CUBIC_SPLINE = 1 };
+
+/* PtychographyPreparation.amplitudes(from:origins:shift:) (PtychographyPreparation.swift:142-183) on the device: every
+ * pattern of `cube` (count patterns of rows * columns Float32 values, [position][row][column], host memory) is shifted
+ * so that its origin (origin_rows[p], origin_columns[p], detector pixels; a uniform origin is repeated) sits on the
+ * corner pixel, out[i][j] = pattern[i + origin_row][j + origin_column] interpolated (bilinear or periodic cubic
+ * B-spline, with wrap-around) in FP64, and amplitudes (host, same layout, Float32: the engine's input) receives
+ * sqrt(max(out, 0)).  mean_intensity = the mean over patterns of the summed shifted intensity (negatives included,
+ * py4DSTEM's mean_intensity and the .meanIntensity error normalisation); clipped_mean_intensity = the same with the
+ * negative values set to zero first.  Invalid input (empty cube, an axis of one pixel, an origin not finite or beyond
+ * 1e9, a cube value not finite) returns CUBO_PTYCHO_INVALID_INPUT; cubic-spline patterns whose FP64 copy does not fit
+ * the shared memory of one CTA (above about 26,000 pixels, 160 x 160) return CUBO_PTYCHO_UNSUPPORTED. */
+CUBO_PTYCHO_API int cubo_ptycho_prepare_amplitudes(cubo_ptycho_context *context, int count, int rows, int columns,
+                                                   const float *cube, const double *origin_rows,
+                                                   const double *origin_columns, int shift, float *amplitudes,
+                                                   double *mean_intensity, double *clipped_mean_intensity);
+
+/* The same with `cube` and `amplitudes` in device memory on the context's device (the origins stay on the host);
+ * enqueued on the context's stream and completed before it returns.  The amplitudes can be handed to
+ * cubo_ptycho_plan_create with problem.amplitudes_on_device set, so the prepared data never leaves the GPU. */
+CUBO_PTYCHO_API int cubo_ptycho_prepare_amplitudes_device(cubo_ptycho_context *context, int count, int rows,
+                                                          int columns, const float *cube_device,
+                                                          const double *origin_rows, const double *origin_columns,
+                                                          int shift, float *amplitudes_device, double *mean_intensity,
+                                                          double *clipped_mean_intensity);
+
+/* Kernel timing of the preprocessing calls on a context: when enabled (which also clears the totals), each launch of
+ * the preprocessing kernel is bracketed by CUDA events on its stream, and the device time is summed once the call has
+ * synchronised.  No counterpart in the reference (CPU code); for measurement. */
+CUBO_PTYCHO_API int cubo_ptycho_set_timing(cubo_ptycho_context *context, int enabled);
+CUBO_PTYCHO_API int cubo_ptycho_prepare_kernel_stats(cubo_ptycho_context *context, double *ms, long long *launches);
 
 /* ---- Loss without allocating.  No counterpart in the reference: CuboPtycho computes on the CPU and never allocates
  * device memory.  For callers that cannot call cudaMalloc: a host application whose device memory belongs to its own

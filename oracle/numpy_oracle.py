@@ -10,6 +10,8 @@ It restates, in vectorised NumPy (``np.fft`` is pocketfft in double, NumPy's fft
   * ``Sources/CuboPtycho/Ptychography.swift:474``      ``frequency``
   * ``Sources/CuboPtycho/PtychographyConstraints.swift:9-83``  probe constraints
   * ``Sources/CuboPtycho/PtychographyPreparation.swift:244-259``  ``initialProbe`` energy scaling
+  * ``Sources/CuboPtycho/PtychographyPreparation.swift:142-183,296-344``  ``amplitudes(from:origins:shift:)``: the
+    bilinear and periodic cubic-spline pattern shifts, square-root amplitudes and mean intensities
 Position correction (``Ptychography.swift:371-377,411-472``) is not part of the GPU path and is not restated here.
 
 Pinned against the py4DSTEM fixtures of CuboKit's own tests (``tests/golden/*.npz``) by ``tests/test_oracle.py``.
@@ -335,3 +337,93 @@ def loss_and_gradients(amplitudes, positions, obj, probe):
     np.add.at(go, idx.ravel(), (np.conj(s) * d).ravel())
     gp = np.sum(np.conj(op) * d, axis=0)
     return loss, (-2 * n * go).reshape(obj.shape), (-2 * n * gp).reshape(rows, columns)
+
+
+# ---------------------------------------------------------------------------------------------------- preprocessing
+
+@dataclass
+class PreparedAmplitudes:
+    """``PtychographyAmplitudes`` (``PtychographyPreparation.swift:62-75``)."""
+    values: np.ndarray            # [position][row][column], sqrt(max(shifted, 0))
+    mean_intensity: float         # mean over positions of the summed shifted intensity, negatives included
+    clipped_mean_intensity: float  # the same with negative shifted values set to zero first
+
+
+def _bilinear_shift(p, origin_row, origin_column):
+    """``shiftPattern(.bilinear)`` (``PtychographyPreparation.swift:301-315``): out[i, j] = p[i + origin_row,
+    j + origin_column], bilinear, wrapped."""
+    rows, columns = p.shape
+    xr = np.arange(rows) + origin_row
+    fr = np.floor(xr)
+    tr = (xr - fr)[:, None]
+    r0 = np.mod(fr.astype(np.int64), rows)
+    r1 = np.mod(fr.astype(np.int64) + 1, rows)
+    xc = np.arange(columns) + origin_column
+    fc = np.floor(xc)
+    tc = (xc - fc)[None, :]
+    c0 = np.mod(fc.astype(np.int64), columns)
+    c1 = np.mod(fc.astype(np.int64) + 1, columns)
+    return (p[np.ix_(r0, c0)] * (1 - tr) * (1 - tc) + p[np.ix_(r1, c0)] * tr * (1 - tc)
+            + p[np.ix_(r0, c1)] * (1 - tr) * tc + p[np.ix_(r1, c1)] * tr * tc)
+
+
+def _cubic_weights(origin, n):
+    """Per output index i: the four wrapped taps floor(x) - 1 .. floor(x) + 2 of x = i + origin and the cubic B-spline
+    weights of the fraction (``PtychographyPreparation.swift:330-334``)."""
+    x = np.arange(n) + origin
+    f = np.floor(x)
+    t = x - f
+    w = np.stack([(1 - t) ** 3 / 6, (3 * t ** 3 - 6 * t ** 2 + 4) / 6, (-3 * t ** 3 + 3 * t ** 2 + 3 * t + 1) / 6,
+                  t ** 3 / 6], axis=1)
+    idx = np.mod(f.astype(np.int64)[:, None] + np.arange(-1, 3)[None, :], n)
+    return idx, w
+
+
+def _cubic_spline_shift(p, origin_row, origin_column):
+    """``shiftPattern(.cubicSpline)`` (``PtychographyPreparation.swift:317-342``): periodic cubic B-spline coefficients
+    by division in Fourier space (the kernel's DFT is (4 + 2 cos(2 pi k / n)) / 6 per axis), then 4 x 4 taps."""
+    rows, columns = p.shape
+    hr = (4 + 2 * np.cos(2 * np.pi * np.arange(rows) / rows)) / 6
+    hc = (4 + 2 * np.cos(2 * np.pi * np.arange(columns) / columns)) / 6
+    coef = np.fft.ifft2(np.fft.fft2(p) / (hr[:, None] * hc[None, :])).real
+    ri, rw = _cubic_weights(origin_row, rows)
+    ci, cw = _cubic_weights(origin_column, columns)
+    out = np.zeros((rows, columns))
+    for a in range(4):
+        for b in range(4):
+            out += rw[:, a][:, None] * cw[:, b][None, :] * coef[np.ix_(ri[:, a], ci[:, b])]
+    return out
+
+
+def prepare_amplitudes(cube, origin_rows, origin_columns, shift="cubicSpline"):
+    """``PtychographyPreparation.amplitudes(from:origins:shift:)`` (``PtychographyPreparation.swift:142-183``).
+
+    ``cube`` is ``[position][row][column]`` (Float32 values, taken to Double); ``origin_rows/columns`` one origin per
+    position (a uniform origin repeated).  Each pattern is shifted so its origin sits on the corner, and the result is
+    ``sqrt(max(shifted, 0))`` with the mean intensities over positions (unclipped and clipped)."""
+    cube = np.asarray(cube, np.float32).astype(np.float64)
+    if cube.ndim != 3:
+        raise PtychographyError("cube must be [position][row][column]")
+    count, rows, columns = cube.shape
+    origin_rows = np.asarray(origin_rows, np.float64).ravel()
+    origin_columns = np.asarray(origin_columns, np.float64).ravel()
+    if not (count > 0 and rows > 1 and columns > 1):
+        raise PtychographyError("cube shape")
+    if origin_rows.size != count or origin_columns.size != count:
+        raise PtychographyError("one origin per position")
+    for o in (origin_rows, origin_columns):
+        if not (np.all(np.isfinite(o)) and np.all(np.abs(o) < 1e9)):
+            raise PtychographyError("origin")
+    if not np.all(np.isfinite(cube)):
+        raise PtychographyError("cube value not finite")
+    if shift not in ("bilinear", "cubicSpline"):
+        raise PtychographyError("shift")
+    fn = _bilinear_shift if shift == "bilinear" else _cubic_spline_shift
+    out = np.empty_like(cube)
+    total = clipped = 0.0
+    for i in range(count):
+        shifted = fn(cube[i], origin_rows[i], origin_columns[i])
+        total += float(shifted.sum())
+        clipped += float(np.maximum(shifted, 0).sum())
+        out[i] = np.sqrt(np.maximum(shifted, 0))
+    return PreparedAmplitudes(out, total / count, clipped / count)

@@ -12,6 +12,10 @@ Which reference test each group pins (paths inside the CuboKit project):
   odd.npz      Tests/CuboPtychoTests/OddSizeTests.swift:122-146 (15x13 probe on a 31x29 object, single-slice cases)
   engines.npz  Tests/CuboPtychoTests/EngineTests.swift:262-305 (aperture / support extras, single-slice engine only)
   options.npz  Tests/CuboPtychoTests/OptionsTests.swift:48-145 (object amplitude toggle, higher-order probe terms)
+  preprocess.npz  Tests/CuboPtychoTests/PreparationTests.swift:39-81 (pattern shifts, square-root amplitudes, mean
+                  intensities: bilinear and cubic-spline orders, per-position origins)
+  ptycho.npz also keeps the raw cube and uniform origin of PtychographyTests.swift:184-193 (bilinear preprocessing
+                  through to the engine's amplitude pin)
 """
 import json
 import sys
@@ -39,6 +43,8 @@ def ptycho(fx):
     s["positions"] = np.asarray(p["positions"], np.float64)
     s["amplitudes"] = np.asarray(p["amplitudes"], np.float64)
     _scalar(s, "meanIntensity", p["preprocessing"]["meanIntensity"])
+    s["preprocessing_raw"] = np.asarray(p["preprocessing"]["raw"], np.float64)
+    s["preprocessing_origin"] = np.asarray(p["preprocessing"]["origin"], np.float64)
     for k in ("initialProbe", "initialObject", "builtProbe", "object", "probe", "rectangularProbe", "offcentreProbe"):
         _cx(s, k, p[k])
     s["errors"] = np.asarray(p["errors"], np.float64)
@@ -151,10 +157,25 @@ def options(fx):
     return s
 
 
+def preprocess(fx):
+    q = json.loads((fx / "preprocess.json").read_text())
+    s = {}
+    for k in ("scanRows", "scanColumns", "detectorRows", "detectorColumns"):
+        _scalar(s, k, q[k])
+    for k in ("cube", "originRows", "originColumns"):
+        s[k] = np.asarray(q[k], np.float64)
+    for order, c in q["amplitudes"].items():
+        s[f"order{order}_amplitudes"] = np.asarray(c["amplitudes"], np.float64)
+        _scalar(s, f"order{order}_meanIntensity", c["meanIntensity"])
+        _scalar(s, f"order{order}_clippedMeanIntensity", c["clippedMeanIntensity"])
+    return s
+
+
 def main():
     root = Path(sys.argv[1]) if len(sys.argv) > 1 else Path("/root/reference")
     fx = root / "Tests/CuboPtychoTests/Fixtures"
-    for name, fn in (("ptycho", ptycho), ("odd", odd), ("engines", engines), ("options", options)):
+    for name, fn in (("ptycho", ptycho), ("odd", odd), ("engines", engines), ("options", options),
+                     ("preprocess", preprocess)):
         arrays = fn(fx)
         np.savez_compressed(HERE / f"{name}.npz", **arrays)
         print(name, len(arrays), "arrays", (HERE / f"{name}.npz").stat().st_size, "bytes")

@@ -2,6 +2,8 @@
 
 Bound and metric are the reference's: ``max|a - b| / max(1, max|b|) < 2e-6`` (``PtychographyTests.swift:28-31,60``).
 """
+from pathlib import Path
+
 import numpy as np
 import pytest
 
@@ -155,3 +157,68 @@ def test_adjoint_matches_central_differences_in_fp64():
                   numpy_oracle.loss_and_gradients(amps, s["positions"], o2, s["probe"])[0]) / (2 * h)
             an = go[j].real if part == "re" else go[j].imag
             assert abs(fd - an) <= 1e-6 * max(1.0, abs(an)) + 1e-5 * abs(loss) * h, (j, part, fd, an)
+
+
+# ---------------------------------------------------------------------------------------------------- preprocessing
+
+PRE = np.load(Path(__file__).resolve().parent / "golden" / "preprocess.npz")
+PTYCHO = np.load(Path(__file__).resolve().parent / "golden" / "ptycho.npz")
+no = numpy_oracle
+gap = gc.gap
+
+
+def _pre_cube():
+    rows, columns = int(PRE["detectorRows"]), int(PRE["detectorColumns"])
+    count = int(PRE["scanRows"]) * int(PRE["scanColumns"])
+    return PRE["cube"].reshape(count, rows, columns)
+
+
+@pytest.mark.parametrize("order,shift", [("1", "bilinear"), ("3", "cubicSpline")])
+def test_prepared_amplitudes_meet_the_preprocessing_pins(order, shift):
+    """``PreparationTests.swift:39-53``: both interpolation orders, per-position origins, at the reference's bounds
+    (2e-6 of max(1, max|a|); mean intensities 2e-6 relative)."""
+    r = no.prepare_amplitudes(_pre_cube(), PRE["originRows"], PRE["originColumns"], shift)
+    assert gap(r.values.ravel(), PRE[f"order{order}_amplitudes"]) < 2e-6
+    assert abs(r.mean_intensity / float(PRE[f"order{order}_meanIntensity"]) - 1) < 2e-6
+    assert abs(r.clipped_mean_intensity / float(PRE[f"order{order}_clippedMeanIntensity"]) - 1) < 2e-6
+
+
+def test_prepared_amplitudes_meet_the_engine_pin():
+    """``PtychographyTests.swift:184-193``: the raw 64-pattern cube with a uniform origin, bilinear, through to the
+    engine's amplitude pin and py4DSTEM's mean intensity."""
+    rows, columns = int(PTYCHO["rows"]), int(PTYCHO["columns"])
+    raw = PTYCHO["preprocessing_raw"].reshape(-1, rows, columns)
+    o = PTYCHO["preprocessing_origin"]
+    r = no.prepare_amplitudes(raw, np.full(len(raw), o[0]), np.full(len(raw), o[1]), "bilinear")
+    assert gap(r.values.ravel(), PTYCHO["amplitudes"]) < 2e-6
+    assert abs(r.mean_intensity / float(PTYCHO["meanIntensity"]) - 1) < 2e-6
+
+
+def test_zero_origin_and_integer_roll():
+    """``PreparationTests.swift:63-81``: a zero origin reproduces the clipped data (exact for bilinear, FFT roundoff for
+    the spline, compared as intensities), and an integer origin is a roll of the pattern."""
+    cube = _pre_cube()
+    count = len(cube)
+    for shift, bound in (("bilinear", 1e-15), ("cubicSpline", 1e-13)):
+        r = no.prepare_amplitudes(cube, np.zeros(count), np.zeros(count), shift)
+        expected = np.maximum(cube.astype(np.float32).astype(np.float64), 0)
+        assert gap((r.values ** 2).ravel(), expected.ravel()) < bound
+    r = no.prepare_amplitudes(cube, np.full(count, 2.0), np.full(count, -3.0), "bilinear")
+    rolled = np.roll(np.roll(cube.astype(np.float32).astype(np.float64), -2, axis=1), 3, axis=2)
+    assert np.array_equal(r.values, np.sqrt(np.maximum(rolled, 0)))
+
+
+def test_preprocessing_refusals():
+    """``PreparationTests.swift:170-186`` (the amplitude part): empty cubes, a one-pixel axis, non-finite or huge
+    origins, origins of the wrong count and non-finite values are invalid input."""
+    cube = _pre_cube()
+    count = len(cube)
+    z = np.zeros(count)
+    bad = [(cube[:0], z[:0], z[:0]), (cube[:, :1, :], z, z), (cube, np.full(count, np.nan), z),
+           (cube, z, np.full(count, 1e9)), (cube, z[:-1], z)]
+    c2 = cube.copy()
+    c2[0, 0, 0] = np.inf
+    bad.append((c2, z, z))
+    for c, r, k in bad:
+        with pytest.raises(no.PtychographyError):
+            no.prepare_amplitudes(c, r, k, "bilinear")
