@@ -4,9 +4,9 @@ The engine is ``libcuboptycho.so`` (CUDA kernels behind the C ABI of ``include/c
 Python binding and the host-side mirror of CuboPtycho's API.
 """
 from .ptycho import (Batch, CancellationError, Context, DeviceError, Plan, PtychographyAmplitudes, PtychographyError,
-                     PtychographyPreparation, PtychographyProbe, Result, SingleslicePtychography, UnsupportedError, context,
-                     electron_wavelength)
+                     PtychographyPositionCorrection, PtychographyPreparation, PtychographyProbe, Result,
+                     SingleslicePtychography, UnsupportedError, context, electron_wavelength)
 
 __all__ = ["Batch", "CancellationError", "Context", "DeviceError", "Plan", "PtychographyAmplitudes", "PtychographyError",
-           "PtychographyPreparation", "PtychographyProbe", "Result", "SingleslicePtychography", "UnsupportedError", "context",
+           "PtychographyPositionCorrection", "PtychographyPreparation", "PtychographyProbe", "Result", "SingleslicePtychography", "UnsupportedError", "context",
            "electron_wavelength"]

@@ -40,6 +40,11 @@ class Params(C.Structure):
         ("error_normalization", C.c_int), ("mean_intensity", C.c_double), ("has_position_correction", C.c_int),
         ("form", C.c_int), ("cancel", C.POINTER(C.c_int)), ("progress", PROGRESS_FN), ("progress_user", C.c_void_p),
         ("variant", C.c_int), ("gather_tile", C.c_int),
+        ("position_step_size", C.c_double), ("has_max_position_update_distance", C.c_int),
+        ("max_position_update_distance", C.c_double), ("has_max_position_total_distance", C.c_int),
+        ("max_position_total_distance", C.c_double), ("position_row_sampling", C.c_double),
+        ("position_column_sampling", C.c_double), ("constrain_positions_center_of_mass", C.c_int),
+        ("position_rows_out", C.POINTER(C.c_double)), ("position_columns_out", C.POINTER(C.c_double)),
     ]
 
 
@@ -55,6 +60,7 @@ SIGNATURES = {
     "cubo_ptycho_plan_destroy": (C.c_int, [C.c_void_p]),
     "cubo_ptycho_plan_set_state": (C.c_int, [C.c_void_p, _dp, _dp, _dp, _dp]),
     "cubo_ptycho_plan_get_state": (C.c_int, [C.c_void_p, _dp, _dp, _dp, _dp]),
+    "cubo_ptycho_plan_get_positions": (C.c_int, [C.c_void_p, _dp, _dp]),
     "cubo_ptycho_plan_iterate": (C.c_int, [C.c_void_p, C.c_int, _dp]),
     "cubo_ptycho_plan_enqueue": (C.c_int, [C.c_void_p, C.c_int]),
     "cubo_ptycho_plan_errors": (C.c_int, [C.c_void_p, C.c_int, _dp]),

@@ -139,6 +139,23 @@ cudaError_t launch_error_reduce(const double *error, long long count, double div
 int error_reduce_scratch();  // doubles of scratch launch_error_reduce needs
 // object-gather candidate lists on the device: without `list`, counts[tile] = the number of positions whose window
 // touches the tile; with it (and starts = exclusive sums of the counts), those positions in ascending order
+template <typename T>
+cudaError_t launch_object_cap(C2<T> *object, int count, int pure_phase, cudaStream_t s);
+
+// position_kernels.cu: position correction (Ptychography.swift:411-472), FP64.  Positions are [rows | columns].
+// Exit waves of positions first .. first + m - 1: out[(i * 3 + v) * n + k] = shifted probe x object patch, v = 0 the
+// object before the update at the centre, v = 1 / 2 the updated object one row / one column further.
+cudaError_t launch_position_exit_waves(const double2 *shifted, ScanTables scan, const double2 *before,
+                                       const double2 *after, int first, int m, int rows, int columns, int object_rows,
+                                       int object_columns, double2 *out, cudaStream_t s);
+// From their far fields: per position the 2 x 2 normal equations over the detector, the step and its limits, the new
+// position (limit_update / limit_total in pixels, infinite = none); *bad = 1 for a position beyond 2^61.
+cudaError_t launch_position_solve(const double2 *far, const float *amplitudes, int first, int m, int n, double *positions,
+                                  const double *initial, int count, double step, double limit_update,
+                                  double limit_total, int *bad, cudaStream_t s);
+// Ptychography.swift:398-401: every position shifted so that their mean is the initial mean again.
+cudaError_t launch_position_center(double *positions, int count, double initial_mean_row, double initial_mean_column,
+                                   cudaStream_t s);
 cudaError_t launch_tile_lists(const int *rr, const int *cc, int count, int rows, int columns, int object_rows,
                               int object_columns, int tile_w, int tile_h, int tiles_x, int tiles, int *counts,
                               const int *starts, int *list, cudaStream_t s);

@@ -333,6 +333,15 @@ __global__ void __launch_bounds__(1024) max_reduce_kernel(const double *v, int c
 }
 
 // Ptychography.swift:362-370,378-382: O += step / sqrt(1e-16 + ((1 - m) w)^2 + (m max w)^2) * grad, then the cap.
+// Ptychography.swift:378-381: |object| <= 1 (or = 1 for a pure-phase object); a zero sample becomes the target.
+template <typename T>
+__device__ __forceinline__ void object_cap(C2<T> &o, int pure_phase) {
+    const T amp = sqrt(o.x * o.x + o.y * o.y);
+    const T target = pure_phase ? (T)1 : (amp < (T)1 ? amp : (T)1);
+    if (amp > (T)0) { const T r = target / amp; o.x *= r; o.y *= r; }
+    else { o.x = target; o.y = 0; }
+}
+
 template <typename T>
 __global__ void __launch_bounds__(256) object_update_kernel(C2<T> *object, const C2<T> *grad, const T *weight,
                                                             int count, const double *max_weight, double step,
@@ -344,12 +353,17 @@ __global__ void __launch_bounds__(256) object_update_kernel(C2<T> *object, const
     C2<T> o = object[j];
     const C2<T> g = grad[j];
     o.x += s * g.x; o.y += s * g.y;
-    if (cap || pure_phase) {
-        const T amp = sqrt(o.x * o.x + o.y * o.y);
-        const T target = pure_phase ? (T)1 : (amp < (T)1 ? amp : (T)1);
-        if (amp > (T)0) { const T r = target / amp; o.x *= r; o.y *= r; }
-        else { o.x = target; o.y = 0; }
-    }
+    if (cap || pure_phase) object_cap<T>(o, pure_phase);
+    object[j] = o;
+}
+
+// The cap alone, for position correction, which reads the updated object before it is capped (Ptychography.swift:371-381).
+template <typename T>
+__global__ void __launch_bounds__(256) object_cap_kernel(C2<T> *object, int count, int pure_phase) {
+    const int j = blockIdx.x * 256 + threadIdx.x;
+    if (j >= count) return;
+    C2<T> o = object[j];
+    object_cap<T>(o, pure_phase);
     object[j] = o;
 }
 
@@ -485,6 +499,12 @@ cudaError_t launch_object_update(C2<T> *object, const C2<T> *grad, const T *weig
     return cudaGetLastError();
 }
 
+template <typename T>
+cudaError_t launch_object_cap(C2<T> *object, int count, int pure_phase, cudaStream_t s) {
+    object_cap_kernel<T><<<(count + 255) / 256, 256, 0, s>>>(object, count, pure_phase);
+    return cudaGetLastError();
+}
+
 int error_reduce_scratch() { return kErrorBlocks; }
 
 cudaError_t launch_tile_lists(const int *rr, const int *cc, int count, int rows, int columns, int object_rows,
@@ -521,7 +541,8 @@ cudaError_t launch_error_reduce(const double *error, long long count, double div
     template cudaError_t launch_probe_reduce<T>(const C2<T> *, const T *, int, int, double2 *, double *, double *,     \
                                                 cudaStream_t);                                                         \
     template cudaError_t launch_object_update<T>(C2<T> *, const C2<T> *, const T *, int, const double *, double,       \
-                                                 double, int, int, cudaStream_t);
+                                                 double, int, int, cudaStream_t);                                      \
+    template cudaError_t launch_object_cap<T>(C2<T> *, int, int, cudaStream_t);
 INSTANTIATE(float)
 INSTANTIATE(double)
 

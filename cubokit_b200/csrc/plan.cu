@@ -3,6 +3,8 @@
 #include <algorithm>
 #include <cmath>
 #include <functional>
+#include <limits>
+#include <type_traits>
 #include <cstdint>
 #include <cstdio>
 #include <cstring>
@@ -126,6 +128,13 @@ struct cubo_ptycho_plan {
     long long errors_capacity = 0;
     long long launches = 0;
     Radices rad_rows{}, rad_columns{};
+    // position correction (FP64 form): positions on the device ([rows | columns]), their start, limits in pixels
+    bool correct_positions = false;
+    double limit_update = 0, limit_total = 0;
+    double initial_mean_row = 0, initial_mean_column = 0;
+    bool scan_stale = false;             // positions moved since the scan tables were built
+    int correction_chunk = 1;            // positions per exit-wave batch
+    std::vector<double> positions_given; // [rows | columns] as supplied
 
     // timing
     bool timing = false;
@@ -144,6 +153,7 @@ struct cubo_ptycho_plan {
     DeviceBuffer maxes, sums, aperture64, mask_dev, error_scratch, loss_slot;
     DeviceBuffer tw_r, tw_c, tw_r64, tw_c64;
     DeviceBuffer c_planes, fault;
+    DeviceBuffer positions64, initial64, object_before, far64, position_bad;
 
     ~cubo_ptycho_plan() {
         for (auto &t : pending) { event_pool.push_back(t.a); event_pool.push_back(t.b); }
@@ -154,9 +164,10 @@ struct cubo_ptycho_plan {
 namespace {
 
 enum Kind { kPositionPass, kObjectGather, kProbeGather, kProbeReduce, kMaxReduce, kObjectUpdate, kProbeSide,
-            kErrorReduce, kShiftTable, kKinds };
+            kErrorReduce, kShiftTable, kPositionCorrection, kKinds };
 const char *kKindNames[kKinds] = {"position_pass", "object_gather", "probe_gather", "probe_reduce", "max_reduce",
-                                  "object_update", "probe_update_constraints", "error_reduce", "shift_table"};
+                                  "object_update", "probe_update_constraints", "error_reduce", "shift_table",
+                                  "position_correction"};
 
 cudaEvent_t take_event(cubo_ptycho_plan *p) {
     if (!p->event_pool.empty()) {
@@ -201,10 +212,36 @@ void collect_timing(cubo_ptycho_plan *p) {
     p->pending.clear();
 }
 
-// Ptychography.swift:247-259 (+ :236 for position correction, refused as .single refuses it).
+// PtychographyPositionCorrection.pixelDistances (Ptychography.swift:74-84): the two limits in pixels, or a refusal.
+void position_limits(const cubo_ptycho_params *pp, double *update, double *total) {
+    if (!std::isfinite(pp->position_step_size)) fail(CUBO_PTYCHO_INVALID_INPUT, "position step");
+    double scale = 1.0;
+    if (pp->has_max_position_update_distance || pp->has_max_position_total_distance) {
+        const double r = pp->position_row_sampling, c = pp->position_column_sampling;
+        if (!(std::isfinite(r) && r > 0 && std::isfinite(c) && c > 0))
+            fail(CUBO_PTYCHO_INVALID_INPUT, "position correction needs both samplings with a distance");
+        scale = std::sqrt(r * r + c * c);
+    }
+    const double inf = std::numeric_limits<double>::infinity();
+    for (int k = 0; k < 2; k++) {
+        const bool has = k == 0 ? pp->has_max_position_update_distance : pp->has_max_position_total_distance;
+        const double d = k == 0 ? pp->max_position_update_distance : pp->max_position_total_distance;
+        if (has && !(std::isfinite(d) && d > 0)) fail(CUBO_PTYCHO_INVALID_INPUT, "position distance");
+    }
+    *update = (pp->has_max_position_update_distance ? pp->max_position_update_distance : inf) / scale;
+    *total = (pp->has_max_position_total_distance ? pp->max_position_total_distance : inf) / scale;
+}
+
+// Ptychography.swift:236-264: the refusals of the reference (position correction only on the Double path: here the
+// FP64 form).
 void validate(const cubo_ptycho_problem *pr, const cubo_ptycho_params *pp, double *divisor_out) {
     if (!pr || !pp) fail(CUBO_PTYCHO_INVALID_INPUT, "null problem or params");
-    if (pp->has_position_correction) fail(CUBO_PTYCHO_INVALID_INPUT, "position correction is not available on the GPU path");
+    if (pp->has_position_correction) {
+        if (pp->form != CUBO_PTYCHO_FORM_FP64)
+            fail(CUBO_PTYCHO_INVALID_INPUT, "position correction runs in the FP64 form (the reference's Double path)");
+        double u, t;
+        position_limits(pp, &u, &t);
+    }
     if (!(pr->rows > 1 && pr->columns > 1 && pr->object_rows > 1 && pr->object_columns > 1))
         fail(CUBO_PTYCHO_INVALID_INPUT, "array dimensions must exceed 1");
     const long long n = (long long)pr->rows * pr->columns;
@@ -241,16 +278,17 @@ long long wrap_ll(long long v, long long m) {
     return r < 0 ? r + m : r;
 }
 
-template <typename T>
-void build_plan(cubo_ptycho_plan *p, const cubo_ptycho_problem *pr) {
+// Scan tables from positions (host, count each): ties-to-even centres (Ptychography.swift:301), wrapped; shift classes
+// by exact fraction, with their phase ramps; the object-gather candidate lists.  Run at plan creation and, with
+// position correction, whenever the positions have moved.
+void build_scan(cubo_ptycho_plan *p, const double *rows_in, const double *columns_in) {
     cudaStream_t s = p->ctx->stream;
     const int R = p->R, C = p->C, n = p->n, P = p->P;
-    // ---- scan tables: ties-to-even centres (Ptychography.swift:301), wrapped; shift classes by exact fraction
     std::vector<int> rr(P), cc(P), cls(P);
     std::map<std::pair<uint64_t, uint64_t>, int> class_of;
     std::vector<std::pair<double, double>> fractions;  // classes 1..
     for (int i = 0; i < P; i++) {
-        const double r = pr->position_rows[i], c = pr->position_columns[i];
+        const double r = rows_in[i], c = columns_in[i];
         const double rn = std::nearbyint(r), cn = std::nearbyint(c);
         const double dr = r - rn, dc = c - cn;
         rr[i] = (int)wrap_ll((long long)rn, p->OR);
@@ -283,7 +321,8 @@ void build_plan(cubo_ptycho_plan *p, const cubo_ptycho_problem *pr) {
     p->tiles = p->tiles_x * tiles_y;
     {
         // counted and listed on the device from the wrapped centres (one warp per tile, positions ascending)
-        check(p->tile_start.alloc((size_t)(p->tiles + 1) * sizeof(int)), "cudaMalloc");
+        if (p->tile_start.bytes < (size_t)(p->tiles + 1) * sizeof(int))
+            check(p->tile_start.alloc((size_t)(p->tiles + 1) * sizeof(int)), "cudaMalloc");
         check(launch_tile_lists(p->rr.as<int>(), p->cc.as<int>(), P, R, C, p->OR, p->OC, p->tile_w, p->tile_h, p->tiles_x,
                                 p->tiles, p->tile_start.as<int>(), nullptr, nullptr, s), "count candidates");
         std::vector<int> counts(p->tiles + 1, 0);
@@ -299,10 +338,38 @@ void build_plan(cubo_ptycho_plan *p, const cubo_ptycho_problem *pr) {
         if (total > INT32_MAX) fail(CUBO_PTYCHO_UNSUPPORTED, "object-gather candidate lists exceed 2^31 entries");
         counts[p->tiles] = (int)total;
         upload(p->tile_start, counts, s);
-        check(p->tile_list.alloc((size_t)std::max<long long>(total, 1) * sizeof(int)), "cudaMalloc");
+        if (p->tile_list.bytes < (size_t)std::max<long long>(total, 1) * sizeof(int))
+            check(p->tile_list.alloc((size_t)std::max<long long>(total, 1) * sizeof(int)), "cudaMalloc");
         check(launch_tile_lists(p->rr.as<int>(), p->cc.as<int>(), P, R, C, p->OR, p->OC, p->tile_w, p->tile_h, p->tiles_x,
                                 p->tiles, nullptr, p->tile_start.as<int>(), p->tile_list.as<int>(), s), "list candidates");
     }
+    const size_t shifted_bytes = (size_t)p->classes * n * (p->fp64 ? sizeof(double2) : sizeof(float2));
+    if (p->shifted.bytes < shifted_bytes) check(p->shifted.alloc(shifted_bytes), "cudaMalloc");
+    const int frac = p->classes - 1;
+    if (frac > 0) {
+        if (p->shift_tmp64.bytes < (size_t)frac * n * sizeof(double2))
+            check(p->shift_tmp64.alloc((size_t)frac * n * sizeof(double2)), "cudaMalloc shift table");
+        std::vector<double2> rrmp((size_t)frac * R), crmp((size_t)frac * C);
+        for (int f = 0; f < frac; f++) {  // Ptychography.swift:304-311
+            for (int r = 0; r < R; r++) {
+                const double a = -2 * kPi * frequency(r, R) * fractions[f].first;
+                rrmp[(size_t)f * R + r] = make_double2(std::cos(a), std::sin(a));
+            }
+            for (int c = 0; c < C; c++) {
+                const double a = -2 * kPi * frequency(c, C) * fractions[f].second;
+                crmp[(size_t)f * C + c] = make_double2(std::cos(a), std::sin(a));
+            }
+        }
+        upload(p->ramps_r64, rrmp, s);
+        upload(p->ramps_c64, crmp, s);
+    }
+}
+
+template <typename T>
+void build_plan(cubo_ptycho_plan *p, const cubo_ptycho_problem *pr) {
+    cudaStream_t s = p->ctx->stream;
+    const int R = p->R, C = p->C, n = p->n, P = p->P;
+    build_scan(p, pr->position_rows, pr->position_columns);
     // ---- amplitudes (Float32, [position][row][column]; the 128 x 128 kernel's register order when it runs)
     check(p->amplitudes.alloc((size_t)P * n * sizeof(float)), "cudaMalloc amplitudes");
     check(cudaMemcpyAsync(p->amplitudes.ptr, pr->amplitudes, (size_t)P * n * sizeof(float),
@@ -380,24 +447,6 @@ void build_plan(cubo_ptycho_plan *p, const cubo_ptycho_problem *pr) {
     check(p->probe64.alloc((size_t)n * sizeof(double2)), "cudaMalloc");
     check(p->scratch64.alloc((size_t)n * sizeof(double2)), "cudaMalloc");
     check(p->spectrum64.alloc((size_t)n * sizeof(double2)), "cudaMalloc");
-    check(p->shifted.alloc((size_t)p->classes * n * sizeof(C2<T>)), "cudaMalloc");
-    const int frac = p->classes - 1;
-    if (frac > 0) {
-        check(p->shift_tmp64.alloc((size_t)frac * n * sizeof(double2)), "cudaMalloc shift table");
-        std::vector<double2> rrmp((size_t)frac * R), crmp((size_t)frac * C);
-        for (int f = 0; f < frac; f++) {  // Ptychography.swift:304-311
-            for (int r = 0; r < R; r++) {
-                const double a = -2 * kPi * frequency(r, R) * fractions[f].first;
-                rrmp[(size_t)f * R + r] = make_double2(std::cos(a), std::sin(a));
-            }
-            for (int c = 0; c < C; c++) {
-                const double a = -2 * kPi * frequency(c, C) * fractions[f].second;
-                crmp[(size_t)f * C + c] = make_double2(std::cos(a), std::sin(a));
-            }
-        }
-        upload(p->ramps_r64, rrmp, s);
-        upload(p->ramps_c64, crmp, s);
-    }
     // probe-gather groups: about eight CTAs per SM of a 148-SM part; a function of the problem only, so the summation
     // order (and the result) does not depend on the device
     const int kblocks = (n + 255) / 256;
@@ -598,28 +647,89 @@ void enqueue_gathers(cubo_ptycho_plan *p) {
     });
 }
 
+// Position correction after the object update, before the amplitude cap (Ptychography.swift:371-377): the exit waves
+// of a chunk of positions with the object before and after the update, their far fields, the per-position solve.
+void enqueue_position_correction(cubo_ptycho_plan *p) {
+    cudaStream_t s = p->ctx->stream;
+    const ScanTables scan{p->rr.as<int>(), p->cc.as<int>(), p->cls.as<int>()};
+    for (int first = 0; first < p->P; first += p->correction_chunk) {
+        const int m = std::min(p->correction_chunk, p->P - first);
+        timed(p, kPositionCorrection, 3, [&] {
+            cudaError_t e = launch_position_exit_waves(p->shifted.as<double2>(), scan, p->object_before.as<double2>(),
+                                                       p->object.as<double2>(), first, m, p->R, p->C, p->OR, p->OC,
+                                                       p->far64.as<double2>(), s);
+            if (e == cudaSuccess) e = launch_fft2_f64(fft64(p), p->far64.as<double2>(), 3 * m, false, s);
+            if (e == cudaSuccess)
+                e = launch_position_solve(p->far64.as<double2>(), p->amplitudes.as<float>(), first, m, p->n,
+                                          p->positions64.as<double>(), p->initial64.as<double>(), p->P,
+                                          p->params.position_step_size, p->limit_update, p->limit_total,
+                                          p->position_bad.as<int>(), s);
+            return e;
+        });
+    }
+}
+
 template <typename T>
 void enqueue_iteration(cubo_ptycho_plan *p) {
     cudaStream_t s = p->ctx->stream;
     enqueue_position_pass<T>(p);
     enqueue_gathers<T>(p);
     const cubo_ptycho_params &pp = p->params;
+    const bool correct = std::is_same<T, double>::value && p->correct_positions;
+    if (correct)
+        check(cudaMemcpyAsync(p->object_before.ptr, p->object.ptr, (size_t)p->objects * sizeof(double2),
+                              cudaMemcpyDeviceToDevice, s), "copy object");
+    const int cap = !correct && pp.constrain_object_amplitude ? 1 : 0, pure = !correct && pp.pure_phase_object ? 1 : 0;
     timed(p, kObjectUpdate, 1, [&] {
         return launch_object_update<T>(p->object.as<C2<T>>(), p->grad_o.as<C2<T>>(), p->weight_o.as<T>(),
                                        (int)p->objects, p->maxes.as<double>(), pp.step_size, pp.normalization_minimum,
-                                       pp.constrain_object_amplitude ? 1 : 0, pp.pure_phase_object ? 1 : 0, s);
+                                       cap, pure, s);
     });
+    if (correct) {
+        enqueue_position_correction(p);
+        if (pp.constrain_object_amplitude || pp.pure_phase_object)
+            timed(p, kObjectUpdate, 1, [&] {
+                return launch_object_cap<T>(p->object.as<C2<T>>(), (int)p->objects, pp.pure_phase_object ? 1 : 0, s);
+            });
+        p->scan_stale = true;
+    }
     enqueue_probe_side(p);
+    if (correct && pp.constrain_positions_center_of_mass)  // Ptychography.swift:398-401
+        timed(p, kPositionCorrection, 1, [&] {
+            return launch_position_center(p->positions64.as<double>(), p->P, p->initial_mean_row,
+                                          p->initial_mean_column, s);
+        });
     timed(p, kErrorReduce, 2, [&] {
         return launch_error_reduce(p->error.as<double>(), p->error_count, p->divisor, p->errors.as<double>(),
                                    p->iteration.as<int>(), p->error_scratch.as<double>(), s);
     });
 }
 
+// The positions on the device after position correction: [rows | columns].
+std::vector<double> download_positions(cubo_ptycho_plan *p) {
+    std::vector<double> v((size_t)2 * p->P);
+    int bad = 0;
+    check(cudaMemcpyAsync(v.data(), p->positions64.ptr, v.size() * sizeof(double), cudaMemcpyDeviceToHost, p->ctx->stream),
+          "download positions");
+    check(cudaMemcpyAsync(&bad, p->position_bad.ptr, sizeof(int), cudaMemcpyDeviceToHost, p->ctx->stream), "download");
+    check(cudaStreamSynchronize(p->ctx->stream), "position correction");
+    if (bad) fail(CUBO_PTYCHO_INVALID_INPUT, "a corrected position left the representable range");
+    return v;
+}
+
+// Scan tables for the positions position correction moved (the next iteration's forward model uses them).
+void refresh_scan(cubo_ptycho_plan *p) {
+    if (!p->correct_positions || !p->scan_stale) return;
+    const std::vector<double> v = download_positions(p);
+    build_scan(p, v.data(), v.data() + p->P);
+    p->scan_stale = false;
+}
+
 void enqueue_iterations(cubo_ptycho_plan *p, int iterations) {
     ensure_errors(p, p->iterations_done + iterations);
     if (iterations > 0) p->tape_valid = false;
     for (int i = 0; i < iterations; i++) {
+        refresh_scan(p);
         if (p->fp64) enqueue_iteration<double>(p);
         else enqueue_iteration<float>(p);
         p->iterations_done++;
@@ -662,6 +772,9 @@ void cubo_ptycho_params_default(cubo_ptycho_params *p) {
     p->probe_amplitude_relative_width = 0.05;
     p->error_normalization = CUBO_PTYCHO_ERRORS_SUPPLIED_AMPLITUDE_ENERGY;
     p->form = CUBO_PTYCHO_FORM_FP32;
+    p->position_step_size = 0.5;  // PtychographyPositionCorrection defaults (Ptychography.swift:68-69)
+    p->position_row_sampling = std::numeric_limits<double>::quiet_NaN();
+    p->position_column_sampling = std::numeric_limits<double>::quiet_NaN();
 }
 
 int cubo_ptycho_create(int device, cubo_ptycho_context **out) {
@@ -746,6 +859,29 @@ int cubo_ptycho_plan_create(cubo_ptycho_context *ctx, const cubo_ptycho_problem 
         p->kind_launches.assign(kKinds, 0);
         if (p->fp64) build_plan<double>(p, pr);
         else build_plan<float>(p, pr);
+        p->positions_given.resize((size_t)2 * p->P);
+        std::copy(pr->position_rows, pr->position_rows + p->P, p->positions_given.begin());
+        std::copy(pr->position_columns, pr->position_columns + p->P, p->positions_given.begin() + p->P);
+        if (pp->has_position_correction) {
+            p->correct_positions = true;
+            position_limits(pp, &p->limit_update, &p->limit_total);
+            double mr = 0, mc = 0;  // Ptychography.swift:270, summed in order
+            for (int i = 0; i < p->P; i++) {
+                mr += pr->position_rows[i];
+                mc += pr->position_columns[i];
+            }
+            p->initial_mean_row = mr / (double)p->P;
+            p->initial_mean_column = mc / (double)p->P;
+            upload(p->positions64, p->positions_given, ctx->stream);
+            upload(p->initial64, p->positions_given, ctx->stream);
+            check(p->object_before.alloc((size_t)p->objects * sizeof(double2)), "cudaMalloc");
+            check(p->position_bad.alloc(sizeof(int)), "cudaMalloc");
+            check(cudaMemsetAsync(p->position_bad.ptr, 0, sizeof(int), ctx->stream), "memset");
+            // three far fields per position, FP64: chunks of at most 1 GiB
+            const size_t per_position = (size_t)3 * p->n * sizeof(double2);
+            p->correction_chunk = (int)std::max<size_t>(1, std::min<size_t>(p->P, (1ull << 30) / per_position));
+            check(p->far64.alloc((size_t)p->correction_chunk * per_position), "cudaMalloc");
+        }
         check(cudaStreamSynchronize(ctx->stream), "plan upload");
     });
     if (status == CUBO_PTYCHO_OK) *out = plan.release();
@@ -816,6 +952,16 @@ int cubo_ptycho_plan_get_state(cubo_ptycho_plan *p, double *ore, double *oim, do
     });
 }
 
+int cubo_ptycho_plan_get_positions(cubo_ptycho_plan *p, double *rows, double *columns) {
+    if (!p) return CUBO_PTYCHO_INVALID_INPUT;
+    return run_guarded(p->ctx, [&] {
+        if (!rows || !columns) fail(CUBO_PTYCHO_INVALID_INPUT, "null output");
+        const std::vector<double> v = p->correct_positions ? download_positions(p) : p->positions_given;
+        std::copy(v.begin(), v.begin() + p->P, rows);
+        std::copy(v.begin() + p->P, v.end(), columns);
+    });
+}
+
 int cubo_ptycho_plan_enqueue(cubo_ptycho_plan *p, int iterations) {
     if (!p) return CUBO_PTYCHO_INVALID_INPUT;
     return run_guarded(p->ctx, [&] {
@@ -853,6 +999,7 @@ int cubo_ptycho_plan_iterate(cubo_ptycho_plan *p, int iterations, double *errors
         }
         check(cudaStreamSynchronize(p->ctx->stream), "sync");
         check_fault(p);
+        if (p->correct_positions) download_positions(p);  // a position out of range fails the call, as it throws
         if (!cancelled && errors && iterations > 0)
             check(cudaMemcpy(errors, p->errors.as<double>() + start, (size_t)iterations * sizeof(double),
                              cudaMemcpyDeviceToHost), "download errors");
@@ -877,6 +1024,8 @@ int cubo_ptycho_reconstruct(cubo_ptycho_context *ctx, const cubo_ptycho_problem 
     status = cubo_ptycho_plan_set_state(plan, ore, oim, pre, pim);
     if (status == CUBO_PTYCHO_OK) status = cubo_ptycho_plan_iterate(plan, pp->iterations, errors);
     if (status == CUBO_PTYCHO_OK) status = cubo_ptycho_plan_get_state(plan, ore, oim, pre, pim);
+    if (status == CUBO_PTYCHO_OK && pp->position_rows_out && pp->position_columns_out)
+        status = cubo_ptycho_plan_get_positions(plan, pp->position_rows_out, pp->position_columns_out);
     const std::string message = ctx->last_error;
     cubo_ptycho_plan_destroy(plan);
     ctx->last_error = message;
@@ -888,6 +1037,7 @@ int cubo_ptycho_reconstruct(cubo_ptycho_context *ctx, const cubo_ptycho_problem 
 namespace {
 template <typename T>
 void enqueue_forward(cubo_ptycho_plan *p) {
+    refresh_scan(p);
     enqueue_position_pass<T>(p);
     check(cudaMemsetAsync(p->loss_slot.ptr, 0, 2 * sizeof(double), p->ctx->stream), "memset");
     timed(p, kErrorReduce, 2, [&] {
@@ -1042,6 +1192,12 @@ int cubo_ptycho_batch_create(cubo_ptycho_context *ctx, int count, const cubo_pty
     if (!b) return CUBO_PTYCHO_OUT_OF_MEMORY;
     b->ctx = ctx;
     for (int i = 0; i < count; i++) {
+        if (params[i].has_position_correction) {  // the positions it moves are read back between iterations
+            delete b;
+            ctx->last_error = "reconstruction " + std::to_string(i) + ": position correction is not available in a "
+                              "graph-replayed batch";
+            return CUBO_PTYCHO_INVALID_INPUT;
+        }
         cubo_ptycho_plan *p = nullptr;
         const int st = cubo_ptycho_plan_create(ctx, &problems[i], &params[i], &p);
         if (st != CUBO_PTYCHO_OK) {

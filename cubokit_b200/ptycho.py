@@ -104,6 +104,19 @@ def context(device: int = 0) -> Context:
 
 
 @dataclass
+class PtychographyPositionCorrection:
+    """``PtychographyPositionCorrection`` (``Ptychography.swift:53-85``): the step, the two distance limits in Å
+    (``None`` = unlimited; they need both samplings, Å per pixel) and the centre-of-mass constraint.  Runs with
+    ``precision="fp64"`` (the reference's Double path; its Float path refuses it)."""
+    step_size: float = 0.5
+    max_update_distance: Optional[float] = None
+    max_total_distance: Optional[float] = None
+    row_sampling: Optional[float] = None
+    column_sampling: Optional[float] = None
+    constrain_center_of_mass: bool = False
+
+
+@dataclass
 class Result:
     """``SingleslicePtychography.Result`` (``Ptychography.swift:179-188``)."""
     object: np.ndarray
@@ -195,6 +208,21 @@ class _Inputs:
         else:
             raise PtychographyError("error normalisation")
         p.has_position_correction = 0 if position_correction is None else 1
+        p.position_step_size = 0.5
+        p.position_row_sampling = p.position_column_sampling = float("nan")
+        if position_correction is not None:
+            pc = position_correction
+            p.position_step_size = float(pc.step_size)
+            p.has_max_position_update_distance = int(pc.max_update_distance is not None)
+            p.max_position_update_distance = float(pc.max_update_distance or 0.0)
+            p.has_max_position_total_distance = int(pc.max_total_distance is not None)
+            p.max_position_total_distance = float(pc.max_total_distance or 0.0)
+            p.position_row_sampling = float("nan") if pc.row_sampling is None else float(pc.row_sampling)
+            p.position_column_sampling = float("nan") if pc.column_sampling is None else float(pc.column_sampling)
+            p.constrain_positions_center_of_mass = int(bool(pc.constrain_center_of_mass))
+        self.positions_out = (np.zeros(count), np.zeros(count))
+        p.position_rows_out = _ptr(self.positions_out[0])
+        p.position_columns_out = _ptr(self.positions_out[1])
         if precision not in FORMS:
             raise PtychographyError(f"precision {precision!r}")
         p.form = FORMS[precision]
@@ -260,7 +288,7 @@ class SingleslicePtychography:
         st = ctx.lib.cubo_ptycho_reconstruct(ctx.handle, C.byref(inp.problem), C.byref(inp.params), _ptr(ore),
                                              _ptr(oim), _ptr(pre), _ptr(pim), _ptr(errors))
         ctx.check(st)
-        pos = np.column_stack([inp.rows_, inp.cols_]) if inp.count else np.zeros((0, 2))
+        pos = np.column_stack(inp.positions_out) if inp.count else np.zeros((0, 2))
         return Result((ore + 1j * oim).reshape(obj.shape), (pre + 1j * pim).reshape(prb.shape),
                       errors[: int(iterations)].copy(), pos)
 
@@ -296,6 +324,13 @@ class Plan:
         ore, oim, pre, pim = np.zeros(no), np.zeros(no), np.zeros(npb), np.zeros(npb)
         self.ctx.check(self.ctx.lib.cubo_ptycho_plan_get_state(self.handle, _ptr(ore), _ptr(oim), _ptr(pre), _ptr(pim)))
         return (ore + 1j * oim).reshape(self.object_shape), (pre + 1j * pim).reshape(self.probe_shape)
+
+    def positions(self) -> np.ndarray:
+        """The current scan positions (P, 2): the given ones, moved by position correction when it is on."""
+        count = self.inputs.count
+        rows, columns = np.zeros(max(count, 1)), np.zeros(max(count, 1))
+        self.ctx.check(self.ctx.lib.cubo_ptycho_plan_get_positions(self.handle, _ptr(rows), _ptr(columns)))
+        return np.column_stack([rows[:count], columns[:count]])
 
     def iterate(self, iterations: int):
         errors = np.zeros(max(iterations, 1))

@@ -77,9 +77,8 @@ typedef struct {
 
 typedef void (*cubo_ptycho_progress_fn)(int completed, int total, void *user);
 
-/* Every parameter of SingleslicePtychography.reconstruct (Ptychography.swift:218-234) except positionCorrection, which
- * the GPU path refuses as the reference's .single path does (Ptychography.swift:236).  Booleans are ints (0 / nonzero).
- * cubo_ptycho_params_default fills in the reference's defaults. */
+/* Every parameter of SingleslicePtychography.reconstruct (Ptychography.swift:218-234).  Booleans are ints
+ * (0 / nonzero).  cubo_ptycho_params_default fills in the reference's defaults. */
 typedef struct {
     int iterations;                    /* 8 */
     double step_size;                  /* 0.5 */
@@ -95,7 +94,7 @@ typedef struct {
     const unsigned char *probe_support_mask; /* NULL, or rows * columns bytes, nonzero = kept */
     int error_normalization;           /* CUBO_PTYCHO_ERRORS_SUPPLIED_AMPLITUDE_ENERGY */
     double mean_intensity;             /* for CUBO_PTYCHO_ERRORS_MEAN_INTENSITY */
-    int has_position_correction;       /* nonzero: refused with CUBO_PTYCHO_INVALID_INPUT */
+    int has_position_correction;       /* nonzero: positionCorrection is given (its settings at the end of this struct) */
     int form;                          /* CUBO_PTYCHO_FORM_FP32 */
     /* isCancelled: read before every iteration; nonzero stops the call with CUBO_PTYCHO_CANCELLED and leaves the
      * caller's object and probe untouched.  NULL: never cancelled. */
@@ -110,6 +109,22 @@ typedef struct {
      * along the residual's contiguous axis).  A performance choice only: every pixel sums the same positions in the same
      * order whatever the tile, so results are bitwise the same. */
     int gather_tile;
+    /* positionCorrection (PtychographyPositionCorrection, Ptychography.swift:53-85), read when has_position_correction
+     * is nonzero.  The reference runs it on its Double path only (its .single path refuses it, Ptychography.swift:236):
+     * here the FP64 form; the FP32 and split-BF16 forms refuse it with CUBO_PTYCHO_INVALID_INPUT, and so do batches.
+     * Distances in Å with has_* = 0 for nil (unlimited); samplings in Å per pixel, NaN for nil, needed (finite,
+     * positive) when a distance is given; invalid settings are refused as pixelDistances refuses them (:74-84). */
+    double position_step_size;                  /* 0.5 */
+    int has_max_position_update_distance;       /* false */
+    double max_position_update_distance;
+    int has_max_position_total_distance;        /* false */
+    double max_position_total_distance;
+    double position_row_sampling;               /* NaN */
+    double position_column_sampling;            /* NaN */
+    int constrain_positions_center_of_mass;     /* false */
+    /* Result.positions: when both are non-NULL, cubo_ptycho_reconstruct writes the positions after the last iteration
+     * (count values each; the given positions when nothing corrected them). */
+    double *position_rows_out, *position_columns_out;
 } cubo_ptycho_params;
 
 enum { CUBO_PTYCHO_VARIANT_AUTO = 0, CUBO_PTYCHO_VARIANT_GENERIC = 1 };
@@ -124,11 +139,11 @@ CUBO_PTYCHO_API int cubo_ptycho_destroy(cubo_ptycho_context *context);
 /* Human-readable reason of the last non-zero status returned on this context (never NULL). */
 CUBO_PTYCHO_API const char *cubo_ptycho_last_error(const cubo_ptycho_context *context);
 
-/* SingleslicePtychography.reconstruct (Ptychography.swift:218-406) with positions fixed.
+/* SingleslicePtychography.reconstruct (Ptychography.swift:218-406).
  * object_re/object_im (object_rows * object_columns) and probe_re/probe_im (rows * columns) hold the start on entry and
  * the result on return (Result.object, Result.probe, Ptychography.swift:179-188); errors receives params->iterations
- * values (Result.errors).  Result.positions are the positions given.  Validation is the reference's
- * (Ptychography.swift:247-259): CUBO_PTYCHO_INVALID_INPUT and nothing written on a refusal. */
+ * values (Result.errors); params->position_rows_out / _columns_out, when given, Result.positions.  Validation is the
+ * reference's (Ptychography.swift:247-264): CUBO_PTYCHO_INVALID_INPUT and nothing written on a refusal. */
 CUBO_PTYCHO_API int cubo_ptycho_reconstruct(cubo_ptycho_context *context, const cubo_ptycho_problem *problem,
                             const cubo_ptycho_params *params, double *object_re, double *object_im, double *probe_re,
                             double *probe_im, double *errors);
@@ -143,11 +158,15 @@ CUBO_PTYCHO_API int cubo_ptycho_plan_set_state(cubo_ptycho_plan *plan, const dou
                                const double *probe_re, const double *probe_im);
 CUBO_PTYCHO_API int cubo_ptycho_plan_get_state(cubo_ptycho_plan *plan, double *object_re, double *object_im, double *probe_re,
                                double *probe_im);
+/* The plan's current scan positions (count values each): the given ones, moved by position correction when it is on. */
+CUBO_PTYCHO_API int cubo_ptycho_plan_get_positions(cubo_ptycho_plan *plan, double *rows, double *columns);
 /* Runs `iterations` GD iterations on the resident state; errors (may be NULL) receives one value per iteration.
  * Honours params->cancel and params->progress. */
 CUBO_PTYCHO_API int cubo_ptycho_plan_iterate(cubo_ptycho_plan *plan, int iterations, double *errors);
 /* Enqueues `iterations` iterations on the context's stream and returns without waiting (no cancel, no progress; the
- * errors stay on the device, read them with cubo_ptycho_plan_errors after a synchronize).  For timing. */
+ * errors stay on the device, read them with cubo_ptycho_plan_errors after a synchronize).  For timing.  With position
+ * correction each iteration after the first waits for the previous one: the positions it moved are read back to
+ * rebuild the scan tables. */
 CUBO_PTYCHO_API int cubo_ptycho_plan_enqueue(cubo_ptycho_plan *plan, int iterations);
 CUBO_PTYCHO_API int cubo_ptycho_plan_errors(cubo_ptycho_plan *plan, int count, double *errors);
 /* The context's cudaStream_t, as an opaque pointer. */

@@ -12,7 +12,9 @@ It restates, in vectorised NumPy (``np.fft`` is pocketfft in double, NumPy's fft
   * ``Sources/CuboPtycho/PtychographyPreparation.swift:244-259``  ``initialProbe`` energy scaling
   * ``Sources/CuboPtycho/PtychographyPreparation.swift:142-183,296-344``  ``amplitudes(from:origins:shift:)``: the
     bilinear and periodic cubic-spline pattern shifts, square-root amplitudes and mean intensities
-Position correction (``Ptychography.swift:371-377,411-472``) is not part of the GPU path and is not restated here.
+  * ``Sources/CuboPtycho/Ptychography.swift:53-85,260-264,371-377,398-401,411-472``  position correction
+    (``PtychographyPositionCorrection``: the per-position 2 x 2 least-squares step, its limits, the centre-of-mass
+    constraint)
 
 Pinned against the py4DSTEM fixtures of CuboKit's own tests (``tests/golden/*.npz``) by ``tests/test_oracle.py``.
 """
@@ -229,16 +231,94 @@ def validate(amplitudes, positions, object_shape, probe_shape, iterations, step_
         raise PtychographyError("invalid input")
 
 
+@dataclass
+class PositionCorrection:
+    """``PtychographyPositionCorrection`` (``Ptychography.swift:53-72``); distances in Å, ``None`` = unlimited."""
+    step_size: float = 0.5
+    max_update_distance: float | None = None
+    max_total_distance: float | None = None
+    row_sampling: float | None = None
+    column_sampling: float | None = None
+    constrain_center_of_mass: bool = False
+
+    def pixel_distances(self):
+        """``pixelDistances`` (``Ptychography.swift:74-84``): (update, total) in pixels, or a refusal."""
+        if not math.isfinite(self.step_size):
+            raise PtychographyError("position step")
+        scale = 1.0
+        if self.max_update_distance is not None or self.max_total_distance is not None:
+            r, c = self.row_sampling, self.column_sampling
+            if r is None or c is None or not (math.isfinite(r) and r > 0 and math.isfinite(c) and c > 0):
+                raise PtychographyError("samplings")
+            scale = math.sqrt(r * r + c * c)
+        for d in (self.max_update_distance, self.max_total_distance):
+            if d is not None and not (math.isfinite(d) and d > 0):
+                raise PtychographyError("distance")
+        return ((math.inf if self.max_update_distance is None else self.max_update_distance) / scale,
+                (math.inf if self.max_total_distance is None else self.max_total_distance) / scale)
+
+
+def position_update(before, after, spectrum, amp, positions, initial, step, limits):
+    """``positionUpdate`` (``Ptychography.swift:411-472``) for all positions at once.  ``before`` / ``after``: the
+    object (flat) the forward model used and the one with the update added; ``spectrum``: the forward model's probe
+    spectrum (R, C); ``amp`` (P, n).  Returns the new positions (P, 2)."""
+    rows, columns = spectrum.shape
+    n = rows * columns
+    object_rows, object_columns = before.shape if before.ndim == 2 else (None, None)
+    before, after = before.reshape(-1), after.reshape(-1)
+    count = len(positions)
+    rr = round_half_even(positions[:, 0])
+    cc = round_half_even(positions[:, 1])
+    dr, dc = positions[:, 0] - rr, positions[:, 1] - cc
+    fr, fc = fftfreq_grid(rows, columns)
+    phase = -2 * np.pi * (fr[None, :, None] * dr[:, None, None] + fc[None, None, :] * dc[:, None, None])
+    s = np.fft.ifft2(spectrum[None] * (np.cos(phase) + 1j * np.sin(phase))).reshape(count, n)
+    ri, ci = rr.astype(np.int64), cc.astype(np.int64)
+
+    def far(obj, row_step, column_step):  # :424-436
+        idx = patch_indices(rows, columns, object_rows, object_columns, ri + row_step, ci + column_step)
+        return np.fft.fft2((s * obj[idx]).reshape(count, rows, columns)).reshape(count, n)
+
+    f, fdx, fdy = far(before, 0, 0), far(after, 1, 0), far(after, 0, 1)
+    difference = amp * amp - (f.real ** 2 + f.imag ** 2)
+    dx = 2 * ((f.real - fdx.real) * f.real + (f.imag - fdx.imag) * f.imag)
+    dy = 2 * ((f.real - fdy.real) * f.real + (f.imag - fdy.imag) * f.imag)
+    axx, axy, ayy = np.sum(dx * dx, 1), np.sum(dx * dy, 1), np.sum(dy * dy, 1)
+    bx, by = np.sum(dx * difference, 1), np.sum(dy * difference, 1)
+    out = positions.copy()
+    for i in range(count):  # :447-470
+        det = axx[i] * ayy[i] - axy[i] * axy[i]
+        u0 = u1 = 0.0
+        if det != 0 and math.isfinite(det):
+            u0 = (ayy[i] * bx[i] - axy[i] * by[i]) / det * step
+            u1 = (axx[i] * by[i] - axy[i] * bx[i]) / det * step
+        if not (math.isfinite(u0) and math.isfinite(u1)):
+            continue
+        norm = math.hypot(u0, u1)
+        if norm > limits[0]:
+            u0 /= norm / limits[0]
+            u1 /= norm / limits[0]
+        if math.isfinite(limits[1]):
+            if math.hypot(positions[i, 0] - initial[i, 0] - u0, positions[i, 1] - initial[i, 1] - u1) > limits[1]:
+                u0 = u1 = 0.0
+        row, column = positions[i, 0] - u0, positions[i, 1] - u1
+        if not (abs(row) < float((2 ** 63 - 1) // 4) and abs(column) < float((2 ** 63 - 1) // 4)):
+            raise PtychographyError("position")
+        out[i] = (row, column)
+    return out
+
+
 def reconstruct(amplitudes, positions, obj, probe, iterations=8, step_size=0.5, normalization_minimum=1.0,
                 fix_probe=False, pure_phase_object=False, constrain_object_amplitude=True,
                 fix_probe_center_of_mass=False, constrain_probe_amplitude=False,
                 probe_amplitude_relative_radius=0.5, probe_amplitude_relative_width=0.05,
                 fix_probe_aperture=False, probe_support_mask=None, error_normalization="suppliedAmplitudeEnergy",
-                mean_intensity=None, progress=None):
-    """``SingleslicePtychography.reconstruct`` Double path (``Ptychography.swift:218-406``), positions fixed.
+                mean_intensity=None, progress=None, position_correction: PositionCorrection | None = None):
+    """``SingleslicePtychography.reconstruct`` Double path (``Ptychography.swift:218-406``).
 
     ``amplitudes`` (P, R, C) or flat; ``positions`` (P, 2) rows/columns in object pixels; ``obj`` (OR, OC) and
-    ``probe`` (R, C) complex.  Returns ``(object, probe, errors)``.
+    ``probe`` (R, C) complex.  Returns ``(object, probe, errors)``, and the corrected positions (P, 2) as a fourth value
+    when ``position_correction`` is given.
     """
     obj = np.array(obj, np.complex128)
     probe = np.array(probe, np.complex128)
@@ -248,21 +328,25 @@ def reconstruct(amplitudes, positions, obj, probe, iterations=8, step_size=0.5, 
     count = len(positions)
     validate(amplitudes, positions, obj.shape, probe.shape, iterations, step_size, normalization_minimum,
              probe_amplitude_relative_radius, probe_amplitude_relative_width, probe_support_mask)
+    limits = position_correction.pixel_distances() if position_correction is not None else None
     amp = np.asarray(amplitudes, np.float64).reshape(count, n)
     divisor = error_divisor(amp, count, error_normalization, mean_intensity)
     initial_aperture = np.abs(np.fft.fft2(probe)) if fix_probe_aperture else None
     object_rows, object_columns = obj.shape
-    rr = round_half_even(positions[:, 0])
-    cc = round_half_even(positions[:, 1])
-    dr = positions[:, 0] - rr
-    dc = positions[:, 1] - cc
-    idx = patch_indices(rows, columns, object_rows, object_columns, rr.astype(np.int64), cc.astype(np.int64))
+    initial = positions.copy()
+    initial_mean = (np.sum(initial[:, 0]) / count, np.sum(initial[:, 1]) / count)
+    current = positions.copy()
     mask = None if probe_support_mask is None else np.asarray(probe_support_mask, bool).reshape(rows, columns)
     m = normalization_minimum
     errors = []
     o = obj.reshape(-1).copy()
     p = probe.copy()
     for it in range(iterations):
+        rr = round_half_even(current[:, 0])
+        cc = round_half_even(current[:, 1])
+        dr = current[:, 0] - rr
+        dc = current[:, 1] - cc
+        idx = patch_indices(rows, columns, object_rows, object_columns, rr.astype(np.int64), cc.astype(np.int64))
         spectrum = np.fft.fft2(p)
         s = shifted_probes(spectrum, dr, dc).reshape(count, n)
         op = o[idx]
@@ -285,7 +369,11 @@ def reconstruct(amplitudes, positions, obj, probe, iterations=8, step_size=0.5, 
         def inverse(local, maximum):
             return 1 / np.sqrt(1e-16 + ((1 - m) * local) ** 2 + (m * maximum) ** 2)
 
+        before = o
         o = o + step_size * inverse(pn, max_pn) * grad_o
+        if position_correction is not None:  # :371-377, with the updated object, before the amplitude cap
+            current = position_update(before.reshape(object_rows, object_columns), o.reshape(object_rows, object_columns),
+                                      spectrum, amp, current, initial, position_correction.step_size, limits)
         if constrain_object_amplitude or pure_phase_object:
             a = np.abs(o)
             target = np.ones_like(a) if pure_phase_object else np.minimum(a, 1.0)
@@ -301,9 +389,15 @@ def reconstruct(amplitudes, positions, obj, probe, iterations=8, step_size=0.5, 
                 p = amplitude_constraint(p, probe_amplitude_relative_radius, probe_amplitude_relative_width)
         if mask is not None:
             p = np.where(mask, p, 0)
+        if position_correction is not None and position_correction.constrain_center_of_mass:  # :398-401
+            mean = (np.sum(current[:, 0]) / count, np.sum(current[:, 1]) / count)
+            current = np.stack([current[:, 0] - (mean[0] - initial_mean[0]),
+                                current[:, 1] - (mean[1] - initial_mean[1])], axis=1)
         errors.append(error / divisor)
         if progress is not None:
             progress(it + 1, iterations)
+    if position_correction is not None:
+        return o.reshape(object_rows, object_columns), p, np.asarray(errors), current
     return o.reshape(object_rows, object_columns), p, np.asarray(errors)
 
 

@@ -16,6 +16,9 @@ Which reference test each group pins (paths inside the CuboKit project):
                   intensities: bilinear and cubic-spline orders, per-position origins)
   ptycho.npz also keeps the raw cube and uniform origin of PtychographyTests.swift:184-193 (bilinear preprocessing
                   through to the engine's amplitude pin)
+  positions.npz  Tests/CuboPtychoTests/PositionCorrectionTests.swift:43-110 (position correction: five settings on
+                  8 x 8 positions started up to 0.3 px off, four iterations; the exact-data case; tools/ptycho/
+                  position_pins.py, py4DSTEM reconstruct(fix_positions=False))
 """
 import json
 import sys
@@ -171,11 +174,45 @@ def preprocess(fx):
     return s
 
 
+def positions(fx):
+    q = json.loads((fx / "positions.json").read_text())
+    s = {}
+    for k in ("rows", "columns", "objectRows", "objectColumns", "rowSampling", "columnSampling", "meanIntensity"):
+        _scalar(s, k, q[k])
+    for k in ("nominalPositions", "truthPositions", "amplitudes"):
+        s[k] = np.asarray(q[k], np.float64)
+    _cx(s, "startObject", q["startObject"])
+    _cx(s, "startProbe", q["startProbe"])
+    e = q["exact"]
+    s["exact_amplitudes"] = np.asarray(e["amplitudes"], np.float64)
+    _scalar(s, "exact_meanIntensity", e["meanIntensity"])
+    _cx(s, "exact_object", e["object"])
+    _cx(s, "exact_probe", e["probe"])
+    s["exact_positions"] = np.asarray(e["positions"], np.float64)
+    s["exact_errors"] = np.asarray(e["errors"], np.float64)
+    names = []
+    for c in q["cases"]:
+        name = c["name"]
+        names.append(name)
+        st = c["settings"]
+        # settings: stepSize, maxUpdateDistance (NaN = none), maxTotalDistance (NaN = none), constrainCenterOfMass
+        s[f"case_{name}_settings"] = np.asarray([st["stepSize"], st.get("maxUpdateDistance", np.nan),
+                                                 st.get("maxTotalDistance", np.nan),
+                                                 1.0 if st.get("constrainCenterOfMass", False) else 0.0])
+        _scalar(s, f"case_{name}_fixProbe", bool(c["fixProbe"]))
+        _cx(s, f"case_{name}_object", c["object"])
+        _cx(s, f"case_{name}_probe", c["probe"])
+        s[f"case_{name}_errors"] = np.asarray(c["errors"], np.float64)
+        s[f"case_{name}_positions"] = np.asarray(c["positions"], np.float64)
+    s["cases"] = np.asarray(names)
+    return s
+
+
 def main():
     root = Path(sys.argv[1]) if len(sys.argv) > 1 else Path("/root/reference")
     fx = root / "Tests/CuboPtychoTests/Fixtures"
     for name, fn in (("ptycho", ptycho), ("odd", odd), ("engines", engines), ("options", options),
-                     ("preprocess", preprocess)):
+                     ("preprocess", preprocess), ("positions", positions)):
         arrays = fn(fx)
         np.savez_compressed(HERE / f"{name}.npz", **arrays)
         print(name, len(arrays), "arrays", (HERE / f"{name}.npz").stat().st_size, "bytes")

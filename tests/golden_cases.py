@@ -185,3 +185,41 @@ def probe_cases():
                                                      astigmatism_angle=float(0.5 * np.arctan2(c12b, c12a)),
                                                      terms=v("terms")), _cx(o, f"app{i}_probe", (R, C))))
     return out
+
+
+def position_cases():
+    """``PositionCorrectionTests.swift:43-62``: the five settings on the shared start, four iterations, step 0.35,
+    normalisation minimum 0.7, mean-intensity errors.  Each entry: (name, inputs, settings, expected) with settings
+    ``dict(step_size, max_update_distance, max_total_distance, row_sampling, column_sampling,
+    constrain_center_of_mass)`` (distances in Å, None = unlimited) and expected ``(object, probe, errors, positions)``."""
+    z = load("positions")
+    R, C, OR, OC = int(z["rows"]), int(z["columns"]), int(z["objectRows"]), int(z["objectColumns"])
+    base = dict(amplitudes=z["amplitudes"].reshape(-1, R, C), positions=z["nominalPositions"],
+                obj=_cx(z, "startObject", (OR, OC)), probe=_cx(z, "startProbe", (R, C)), iterations=4, step_size=0.35,
+                normalization_minimum=0.7, error_normalization="meanIntensity", mean_intensity=float(z["meanIntensity"]))
+    out = []
+    for name in z["cases"]:
+        st = z[f"case_{name}_settings"]
+        settings = dict(step_size=float(st[0]), max_update_distance=None if np.isnan(st[1]) else float(st[1]),
+                        max_total_distance=None if np.isnan(st[2]) else float(st[2]),
+                        row_sampling=float(z["rowSampling"]), column_sampling=float(z["columnSampling"]),
+                        constrain_center_of_mass=bool(st[3]))
+        inputs = dict(base, fix_probe=bool(z[f"case_{name}_fixProbe"]))
+        expected = (_cx(z, f"case_{name}_object", (OR, OC)), _cx(z, f"case_{name}_probe", (R, C)),
+                    z[f"case_{name}_errors"], z[f"case_{name}_positions"])
+        out.append((str(name), inputs, settings, expected))
+    return out
+
+
+def position_exact_case():
+    """``PositionCorrectionTests.swift:83-101``: exact object and probe, data taken at ``truthPositions``, the object
+    frozen (step 1e-12), one iteration: the correction alone moves the positions."""
+    z = load("positions")
+    R, C, OR, OC = int(z["rows"]), int(z["columns"]), int(z["objectRows"]), int(z["objectColumns"])
+    inputs = dict(amplitudes=z["exact_amplitudes"].reshape(-1, R, C), positions=z["nominalPositions"],
+                  obj=_cx(z, "exact_object", (OR, OC)), probe=_cx(z, "exact_probe", (R, C)), iterations=1,
+                  step_size=1e-12, normalization_minimum=0.7, fix_probe=True, error_normalization="meanIntensity",
+                  mean_intensity=float(z["exact_meanIntensity"]))
+    settings = dict(step_size=0.5, max_update_distance=None, max_total_distance=None, row_sampling=None,
+                    column_sampling=None, constrain_center_of_mass=False)
+    return inputs, settings, z["exact_positions"], z["truthPositions"], (float(z["rowSampling"]), float(z["columnSampling"]))

@@ -144,8 +144,9 @@ def test_refusals_through_the_c_abi(cb):
         with pytest.raises(cb.PtychographyError):
             _gpu(cb, case, "fp32", iterations=1, constrain_probe_amplitude=True, probe_amplitude_relative_radius=radius,
                  probe_amplitude_relative_width=width)
-    with pytest.raises(cb.PtychographyError):
-        _gpu(cb, case, "fp32", iterations=1, position_correction=object())
+    for precision in ("fp32", "split_bf16"):  # the reference's Float path refuses position correction
+        with pytest.raises((cb.PtychographyError, cb.UnsupportedError)):
+            _gpu(cb, case, precision, iterations=1, position_correction=cb.PtychographyPositionCorrection())
     for value in (-1.0, np.nan, np.inf):  # checked on the device after the upload
         bad = case.amplitudes.copy()
         bad.flat[5] = value

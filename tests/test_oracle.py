@@ -222,3 +222,55 @@ def test_preprocessing_refusals():
     for c, r, k in bad:
         with pytest.raises(no.PtychographyError):
             no.prepare_amplitudes(c, r, k, "bilinear")
+
+
+# ---------------------------------------------------------------------------------------------- position correction
+
+@pytest.mark.parametrize("case", gc.position_cases(), ids=lambda c: c[0])
+def test_position_correction_meets_the_pins(case):
+    """``PositionCorrectionTests.swift:43-62``: object, probe and errors within 2e-6 of max(1, max|b|), positions within
+    2e-6 px, and the positions did move (more than 0.05 px)."""
+    name, inputs, settings, (obj, probe, errors, positions) = case
+    o, p, e, pos = no.reconstruct(**inputs, position_correction=no.PositionCorrection(**settings))
+    assert max(gap(pos[:, 0], positions[:, 0]), gap(pos[:, 1], positions[:, 1])) < 2e-6
+    assert max(gc.complex_gap(o, obj), gc.complex_gap(p, probe), gap(e, errors)) < 2e-6
+    assert np.max(np.abs(pos - inputs["positions"])) > 0.05
+
+
+def test_position_correction_moves_toward_the_data_positions():
+    """``PositionCorrectionTests.swift:83-101``: exact object and probe, object frozen; the corrected positions meet
+    py4DSTEM's at 2e-6 and their mean distance to the data's positions drops below 0.7 of the start's."""
+    inputs, settings, expected, truth, _ = gc.position_exact_case()
+    _, _, _, pos = no.reconstruct(**inputs, position_correction=no.PositionCorrection(**settings))
+    assert max(gap(pos[:, 0], expected[:, 0]), gap(pos[:, 1], expected[:, 1])) < 2e-6
+    before = np.mean(np.hypot(*(inputs["positions"] - truth).T))
+    after = np.mean(np.hypot(*(pos - truth).T))
+    assert after < 0.7 * before
+
+
+def test_position_correction_limits_zero_step_and_refusals():
+    """``PositionCorrectionTests.swift:64-81,103-141``: a zero step leaves everything as without the option; the update
+    limit clips moves (some to the limit); a total limit smaller than any move keeps every position; invalid settings
+    are refused."""
+    name, inputs, settings, _ = gc.position_cases()[0]
+    short = dict(inputs, iterations=2)
+    o0, p0, e0 = no.reconstruct(**short)
+    o1, p1, e1, pos = no.reconstruct(**short, position_correction=no.PositionCorrection(step_size=0.0))
+    assert np.array_equal(pos, inputs["positions"]) and np.array_equal(o0, o1) and np.array_equal(e0, e1)
+    one = dict(inputs, iterations=1)
+    rs, cs = settings["row_sampling"], settings["column_sampling"]
+    _, _, _, pos = no.reconstruct(**one, position_correction=no.PositionCorrection(
+        step_size=0.5, max_update_distance=0.2, row_sampling=rs, column_sampling=cs))
+    limit = 0.2 / np.hypot(rs, cs)
+    moves = np.hypot(*(pos - inputs["positions"]).T)
+    assert moves.max() <= limit * (1 + 1e-12) and moves.max() > 0.5 * limit
+    _, _, _, pos = no.reconstruct(**one, position_correction=no.PositionCorrection(
+        step_size=0.5, max_total_distance=1e-6, row_sampling=rs, column_sampling=cs))
+    assert np.array_equal(pos, inputs["positions"])
+    for bad in (no.PositionCorrection(step_size=np.nan), no.PositionCorrection(step_size=np.inf),
+                no.PositionCorrection(max_update_distance=1.0),
+                no.PositionCorrection(max_update_distance=-1.0, row_sampling=rs, column_sampling=cs),
+                no.PositionCorrection(max_total_distance=0.0, row_sampling=rs, column_sampling=cs),
+                no.PositionCorrection(max_update_distance=1.0, row_sampling=0.0, column_sampling=cs)):
+        with pytest.raises(no.PtychographyError):
+            no.reconstruct(**one, position_correction=bad)
