@@ -14,7 +14,7 @@ OK, INVALID_INPUT, CANCELLED = 0, 1, 2
 CUDA_ERROR, OUT_OF_MEMORY, DEVICE_TIMEOUT, NO_DEVICE, UNSUPPORTED = -1, -2, -3, -4, -5
 FORM_FP32, FORM_SPLIT_BF16, FORM_FP64 = 0, 1, 2
 ERRORS_SUPPLIED_AMPLITUDE_ENERGY, ERRORS_MEAN_INTENSITY = 0, 1
-VARIANT_AUTO, VARIANT_GENERIC = 0, 1
+VARIANT_AUTO, VARIANT_GENERIC, VARIANT_GLOBAL = 0, 1, 2
 
 PROGRESS_FN = C.CFUNCTYPE(None, C.c_int, C.c_int, C.c_void_p)
 

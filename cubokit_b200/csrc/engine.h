@@ -173,6 +173,11 @@ struct Fft2Plan64 {
     const double2 *tw_rows, *tw_columns;
 };
 cudaError_t launch_fft2_f64(const Fft2Plan64 &p, double2 *data, int batch, bool inverse, cudaStream_t s);
+// The FP64 position pass through global memory (any detector whose sides are at most 4096): exit waves into dpsi,
+// batched FFT, projection with the per-position error, inverse FFT.  *launches receives the kernels it enqueued.
+cudaError_t launch_position_pass_global(const PositionPassArgs<double> &a, const Fft2Plan64 &fft, int *launches,
+                                       cudaStream_t s);
+bool line_fft_supported(int rows, int columns);
 cudaError_t configure_fft_lines();
 cudaError_t launch_scale_f64(double2 *data, int count, double scale, cudaStream_t s);
 cudaError_t launch_probe_update(double2 *probe, const double2 *grad, const double *weight, int n, const double *max_weight,

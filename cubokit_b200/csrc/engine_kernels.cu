@@ -13,6 +13,8 @@
 //   error reduce    FP64 fixed-order sum of the per-position residuals divided by the normalisation (:400).
 #include <cfloat>
 
+#include <algorithm>
+
 #include "engine.h"
 
 namespace cubo {
@@ -113,6 +115,45 @@ __global__ void __launch_bounds__(NT, 1) position_pass_kernel(PositionPassArgs<T
     fft2_smem<T, NT, MAXN>(D, a.rows, a.columns, a.rad_rows, a.rad_columns, twr, twc, true);
     C2<T> *out = a.dpsi + (size_t)p * a.n;
     for (int k = tid; k < a.n; k += NT) out[k] = D[k];
+}
+
+// FP64 position pass through global memory, for detectors whose FP64 plane does not fit one CTA's shared memory (above
+// 12,288 pixels, e.g. 128 x 128): the exit waves are written into dpsi, transformed by the batched line FFT, projected
+// in place (the same arithmetic and the same per-position error sum as the shared-memory pass) and transformed back.
+__global__ void __launch_bounds__(256) exit_wave_global_kernel(PositionPassArgs<double> a, int m) {
+    const long long t = (long long)blockIdx.x * 256 + threadIdx.x;
+    if (t >= (long long)m * a.n) return;
+    const int i = (int)(t / a.n), k = (int)(t - (long long)i * a.n);
+    const int p = a.first + i;
+    const int rr = a.scan.rr[p], cc = a.scan.cc[p], cls = a.scan.cls[p];
+    const int kr = k / a.columns, kc = k - kr * a.columns;
+    const int y = wrap_once(rr + corner_offset(kr, a.rows), a.object_rows);
+    const int x = wrap_once(cc + corner_offset(kc, a.columns), a.object_columns);
+    a.dpsi[(size_t)p * a.n + k] = cmul(a.shifted[(size_t)cls * a.n + k], a.object[(size_t)y * a.object_columns + x]);
+}
+
+template <int NT>
+__global__ void __launch_bounds__(NT) project_global_kernel(PositionPassArgs<double> a) {
+    __shared__ double scratch[NT / 32];
+    const int p = a.first + blockIdx.x;
+    double2 *D = a.dpsi + (size_t)p * a.n;
+    const float *A = a.amplitudes + (size_t)p * a.n;
+    double err = 0;
+    for (int k = threadIdx.x; k < a.n; k += NT) {
+        const double2 f = D[k];
+        const double mag = sqrt(f.x * f.x + f.y * f.y);
+        const double measured = (double)A[k];
+        const double miss = measured - mag;
+        err += miss * miss;
+        if (mag > 0.0) {
+            const double sc = (measured / mag - 1.0) * a.inv_n;
+            D[k] = make_double2(f.x * sc, f.y * sc);
+        } else {
+            D[k] = make_double2(measured * a.inv_n, 0.0);
+        }
+    }
+    const double total = block_sum<NT>(err, scratch);
+    if (threadIdx.x == 0) a.error[p] = total;
 }
 
 // ------------------------------------------------------------------------------------------------ object gather
@@ -456,6 +497,30 @@ cudaError_t configure_kernels() {
 
 size_t position_pass_smem(int n, int rows, int columns, bool fp64) {
     return fp64 ? pass_smem<double>(n, rows, columns) : pass_smem<float>(n, rows, columns);
+}
+
+cudaError_t launch_position_pass_global(const PositionPassArgs<double> &a, const Fft2Plan64 &fft, int *launches,
+                                       cudaStream_t s) {
+    const int chunk = (int)std::max<long long>(1, (1LL << 28) / a.n);  // at most 4 GiB of exit waves per round
+    int count = 0;
+    for (int first = 0; first < a.count; first += chunk) {
+        PositionPassArgs<double> b = a;
+        b.first = a.first + first;
+        const int m = std::min(chunk, a.count - first);
+        const long long total = (long long)m * a.n;
+        exit_wave_global_kernel<<<(unsigned)((total + 255) / 256), 256, 0, s>>>(b, m);
+        cudaError_t e = cudaGetLastError();
+        if (e == cudaSuccess) e = launch_fft2_f64(fft, b.dpsi + (size_t)b.first * a.n, m, false, s);
+        if (e == cudaSuccess) {
+            project_global_kernel<kPassThreads><<<m, kPassThreads, 0, s>>>(b);
+            e = cudaGetLastError();
+        }
+        if (e == cudaSuccess) e = launch_fft2_f64(fft, b.dpsi + (size_t)b.first * a.n, m, true, s);
+        if (e != cudaSuccess) return e;
+        count += 6;
+    }
+    if (launches) *launches = count;
+    return cudaSuccess;
 }
 
 template <typename T>

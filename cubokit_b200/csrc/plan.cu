@@ -121,6 +121,7 @@ struct cubo_ptycho_plan {
     int probe_blocks = 0;
     bool fast = false;      // 128 x 128 FP32 register-resident position pass
     bool bf16 = false;      // 128 x 128 split-BF16 tensor-core position pass
+    bool global64 = false;  // FP64 position pass through global memory (the plane does not fit shared memory)
     int sms = 148;
     long long error_count = 0;  // residual partials summed by the error kernel
     bool tape_valid = false;    // dpsi holds the residuals of the current state (forward ran, nothing changed since)
@@ -270,6 +271,8 @@ void validate(const cubo_ptycho_problem *pr, const cubo_ptycho_params *pp, doubl
     }
     if (pp->form < CUBO_PTYCHO_FORM_FP32 || pp->form > CUBO_PTYCHO_FORM_FP64) fail(CUBO_PTYCHO_INVALID_INPUT, "form");
     if (pp->gather_tile < 0 || pp->gather_tile > 3) fail(CUBO_PTYCHO_INVALID_INPUT, "gather tile");
+    if (pp->variant < CUBO_PTYCHO_VARIANT_AUTO || pp->variant > CUBO_PTYCHO_VARIANT_GLOBAL)
+        fail(CUBO_PTYCHO_INVALID_INPUT, "variant");
     *divisor_out = d;
 }
 
@@ -611,6 +614,13 @@ void enqueue_position_pass(cubo_ptycho_plan *p) {
         fa.partial_grad = p->partial_grad.as<float2>(); fa.partial_weight = p->partial_weight.as<float>();
         fa.fault = p->fault.as<int>();
         timed(p, kPositionPass, 1, [&] { return launch_fast128(fa, p->sms, s); });
+    } else if (p->global64) {
+        int count = 0;
+        if constexpr (std::is_same<T, double>::value) {
+            timed(p, kPositionPass, 0, [&] { return launch_position_pass_global(pa, fft64(p), &count, s); });
+            p->launches += count;
+            if (p->timing) p->kind_launches[kPositionPass] += count;
+        }
     } else {
         timed(p, kPositionPass, 1, [&] { return launch_position_pass<T>(pa, s); });
     }
@@ -841,13 +851,15 @@ int cubo_ptycho_plan_create(cubo_ptycho_context *ctx, const cubo_ptycho_problem 
         p->fp64 = pp->form == CUBO_PTYCHO_FORM_FP64;
         if (pp->form == CUBO_PTYCHO_FORM_SPLIT_BF16 && !bf16_applicable(p->R, p->C))
             fail(CUBO_PTYCHO_UNSUPPORTED, "the split-BF16 tensor-core form needs a 128 x 128 detector");
-        if (!position_pass_supported(p->n, p->fp64))
-            fail(CUBO_PTYCHO_UNSUPPORTED, "detector of " + std::to_string(p->n) + " pixels exceeds the shared-memory "
-                                              "transform of this form");
         int optin = 0;
         check(cudaDeviceGetAttribute(&optin, cudaDevAttrMaxSharedMemoryPerBlockOptin, ctx->device), "attribute");
-        if (position_pass_smem(p->n, p->R, p->C, p->fp64) > (size_t)optin)
-            fail(CUBO_PTYCHO_UNSUPPORTED, "detector too large for shared memory");
+        const bool smem_pass = position_pass_supported(p->n, p->fp64) &&
+                               position_pass_smem(p->n, p->R, p->C, p->fp64) <= (size_t)optin;
+        // FP64 planes too large for one CTA go through global memory (any size the line transform takes)
+        p->global64 = p->fp64 && (!smem_pass || pp->variant == CUBO_PTYCHO_VARIANT_GLOBAL);
+        if (!smem_pass && !(p->global64 && line_fft_supported(p->R, p->C)))
+            fail(CUBO_PTYCHO_UNSUPPORTED, "detector of " + std::to_string(p->n) + " pixels exceeds the shared-memory "
+                                              "transform of this form");
         check(configure_kernels(), "configure kernels");
         check(configure_fft_lines(), "configure line transforms");
         p->bf16 = pp->form == CUBO_PTYCHO_FORM_SPLIT_BF16;

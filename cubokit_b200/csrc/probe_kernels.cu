@@ -27,22 +27,27 @@ __global__ void __launch_bounds__(kLineThreads) fft_lines_kernel(double2 *data, 
     const int first = blockIdx.x * lines_per_block;
     const int nl = min(lines_per_block, lines_total - first);
     const long long n = (long long)rows * columns;
-    // line l: rows pass -> field l / rows, row l % rows, stride 1; columns pass -> field l / columns, column, stride C
-    for (int i = threadIdx.x; i < nl * L; i += kLineThreads) {
-        const int l = first + i / L, e = i % L;
-        long long off;
-        if (columns_pass) off = (long long)(l / columns) * n + (long long)e * columns + (l % columns);
-        else off = (long long)l * columns + e;
-        D[i] = data[off];
+    // line l: rows pass -> field l / rows, row l % rows, stride 1, one line after the other in shared memory;
+    // columns pass -> field l / columns, column l % columns, stride C, staged as rows of the nl columns (element e of
+    // line j at e * nl + j) so that consecutive threads read consecutive columns of one row
+    if (columns_pass) {
+        for (int i = threadIdx.x; i < nl * L; i += kLineThreads) {
+            const int j = i % nl, e = i / nl, l = first + j;
+            D[i] = data[(long long)(l / columns) * n + (long long)e * columns + (l % columns)];
+        }
+    } else {
+        for (int i = threadIdx.x; i < nl * L; i += kLineThreads) D[i] = data[(long long)(first + i / L) * columns + i % L];
     }
     __syncthreads();
-    line_fft<double, kLineThreads, kLineMaxN>(D, LineGeom{L, nl, 1, L}, rad, tw, inv);
-    for (int i = threadIdx.x; i < nl * L; i += kLineThreads) {
-        const int l = first + i / L, e = i % L;
-        long long off;
-        if (columns_pass) off = (long long)(l / columns) * n + (long long)e * columns + (l % columns);
-        else off = (long long)l * columns + e;
-        data[off] = D[i];
+    line_fft<double, kLineThreads, kLineMaxN>(D, columns_pass ? LineGeom{L, nl, nl, 1} : LineGeom{L, nl, 1, L}, rad, tw,
+                                              inv);
+    if (columns_pass) {
+        for (int i = threadIdx.x; i < nl * L; i += kLineThreads) {
+            const int j = i % nl, e = i / nl, l = first + j;
+            data[(long long)(l / columns) * n + (long long)e * columns + (l % columns)] = D[i];
+        }
+    } else {
+        for (int i = threadIdx.x; i < nl * L; i += kLineThreads) data[(long long)(first + i / L) * columns + i % L] = D[i];
     }
 }
 
@@ -239,6 +244,8 @@ cudaError_t launch_fft2_f64(const Fft2Plan64 &p, double2 *data, int batch, bool 
     }
     return cudaSuccess;
 }
+
+bool line_fft_supported(int rows, int columns) { return rows <= kLineMaxN && columns <= kLineMaxN; }
 
 // The line-FFT kernel's shared-memory limit, once per device (outside any stream capture).
 cudaError_t configure_fft_lines() {

@@ -226,9 +226,10 @@ class _Inputs:
         if precision not in FORMS:
             raise PtychographyError(f"precision {precision!r}")
         p.form = FORMS[precision]
-        if variant not in ("auto", "generic"):
+        variants = {"auto": L.VARIANT_AUTO, "generic": L.VARIANT_GENERIC, "global": L.VARIANT_GLOBAL}
+        if variant not in variants:
             raise PtychographyError(f"variant {variant!r}")
-        p.variant = L.VARIANT_GENERIC if variant == "generic" else L.VARIANT_AUTO
+        p.variant = variants[variant]
         if gather_tile not in (0, 1, 2, 3):
             raise PtychographyError(f"gather_tile {gather_tile!r}")
         p.gather_tile = int(gather_tile)

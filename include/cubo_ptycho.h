@@ -103,7 +103,9 @@ typedef struct {
     cubo_ptycho_progress_fn progress;
     void *progress_user;
     /* Kernel choice: CUBO_PTYCHO_VARIANT_AUTO picks the specialised kernel for the detector size when there is one;
-     * CUBO_PTYCHO_VARIANT_GENERIC forces the any-size shared-memory transform (for cross-checks). */
+     * CUBO_PTYCHO_VARIANT_GENERIC forces the any-size shared-memory transform (for cross-checks);
+     * CUBO_PTYCHO_VARIANT_GLOBAL (FP64 form) forces the position pass through global memory that detectors too large
+     * for one CTA's FP64 plane use (for cross-checks). */
     int variant;
     /* Object-gather tile (pixels per CTA, 256 in all): 0 = default, 1 = 32 x 8, 2 = 16 x 16, 3 = 64 x 4 (width x height
      * along the residual's contiguous axis).  A performance choice only: every pixel sums the same positions in the same
@@ -127,7 +129,7 @@ typedef struct {
     double *position_rows_out, *position_columns_out;
 } cubo_ptycho_params;
 
-enum { CUBO_PTYCHO_VARIANT_AUTO = 0, CUBO_PTYCHO_VARIANT_GENERIC = 1 };
+enum { CUBO_PTYCHO_VARIANT_AUTO = 0, CUBO_PTYCHO_VARIANT_GENERIC = 1, CUBO_PTYCHO_VARIANT_GLOBAL = 2 };
 
 /* Replaces the default arguments of SingleslicePtychography.reconstruct (Ptychography.swift:220-232). */
 CUBO_PTYCHO_API void cubo_ptycho_params_default(cubo_ptycho_params *params);

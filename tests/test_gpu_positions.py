@@ -148,3 +148,36 @@ def test_against_the_oracle_on_a_raster_started_off_its_positions(cb, shape):
     assert _position_gap(r.positions, pos) < 2e-6
     assert max(gc.complex_gap(r.object, o), gc.complex_gap(r.probe, p), gap(r.errors, e)) < 2e-6
     assert np.max(np.abs(r.positions - start)) > 0.01
+
+
+# ------------------------------------------------------------------ FP64 planes larger than one CTA (global memory)
+
+def test_fp64_global_pass_equals_the_shared_memory_pass(cb):
+    """The FP64 position pass through global memory (forced on a 48 x 40 detector) against the shared-memory pass:
+    the same line transforms in the same order, so the same results to FP64 roundoff."""
+    s = scenes.raster_scene(scan=4, det=48, step=6, seed=21, shape=(48, 40))
+    kw = dict(iterations=3, step_size=0.5, precision="fp64")
+    a = cb.SingleslicePtychography.reconstruct(s["amplitudes"], s["positions"] + 0.25, s["object"], s["probe"], **kw)
+    b = cb.SingleslicePtychography.reconstruct(s["amplitudes"], s["positions"] + 0.25, s["object"], s["probe"],
+                                               variant="global", **kw)
+    assert gc.complex_gap(a.object, b.object) < 1e-12 and gc.complex_gap(a.probe, b.probe) < 1e-12
+    assert gap(a.errors, b.errors) < 1e-12
+
+
+def test_fp64_form_at_128x128_against_the_oracle(cb):
+    """128 x 128 detectors in the FP64 form (the reference's default precision): against the FP64 restatement, with
+    fractional positions and with position correction."""
+    s = scenes.raster_scene(scan=3, det=128, step=8, seed=5)
+    start = s["positions"] + np.array([0.3, -0.2])
+    kw = dict(iterations=2, step_size=0.5, normalization_minimum=0.8)
+    o, p, e = no.reconstruct(s["amplitudes"], start, s["object"], s["probe"], **kw)
+    r = cb.SingleslicePtychography.reconstruct(s["amplitudes"], start, s["object"], s["probe"], precision="fp64", **kw)
+    assert max(gc.complex_gap(r.object, o), gc.complex_gap(r.probe, p), gap(r.errors, e)) < 1e-9
+    settings = dict(step_size=0.5, max_update_distance=None, max_total_distance=None, row_sampling=None,
+                    column_sampling=None, constrain_center_of_mass=False)
+    o, p, e, pos = no.reconstruct(s["amplitudes"], start, s["object"], s["probe"], **kw,
+                                  position_correction=no.PositionCorrection(**settings))
+    r = cb.SingleslicePtychography.reconstruct(s["amplitudes"], start, s["object"], s["probe"], precision="fp64",
+                                               position_correction=cb.PtychographyPositionCorrection(**settings), **kw)
+    assert _position_gap(r.positions, pos) < 2e-6
+    assert max(gc.complex_gap(r.object, o), gc.complex_gap(r.probe, p), gap(r.errors, e)) < 2e-6
