@@ -198,6 +198,9 @@ cudaError_t launch_support_mask(double2 *probe, const unsigned char *mask, int n
 cudaError_t launch_magnitude(const double2 *data, double *out, int n, cudaStream_t s);
 cudaError_t launch_shift_ramps(const double2 *spectrum, const double2 *ramps_rows, const double2 *ramps_columns,
                                int rows, int columns, int classes, double2 *out, cudaStream_t s);
+// The phase ramps of `classes` fractional shifts (dr, dc) = fractions[f]: exp(-2 pi i frequency(k) d) per row and column.
+cudaError_t launch_ramp_table(const double2 *fractions, int classes, int rows, int columns, double2 *ramps_rows,
+                              double2 *ramps_columns, cudaStream_t s);
 template <typename T>
 cudaError_t launch_convert(const double2 *in, C2<T> *out, long long count, cudaStream_t s);
 cudaError_t configure_kernels();

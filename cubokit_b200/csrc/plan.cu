@@ -5,6 +5,7 @@
 #include <functional>
 #include <limits>
 #include <type_traits>
+#include <unordered_map>
 #include <cstdint>
 #include <cstdio>
 #include <cstring>
@@ -80,9 +81,11 @@ std::vector<double2> twiddles(int L) {
     return t;
 }
 
+// Copies v into b, reusing b's memory when it is large enough (no cudaFree, which waits for the device, when tables are
+// rebuilt between iterations).
 template <typename X>
 void upload(DeviceBuffer &b, const std::vector<X> &v, cudaStream_t s) {
-    check(b.alloc(v.size() * sizeof(X)), "cudaMalloc");
+    if (b.ptr == nullptr || b.bytes < v.size() * sizeof(X)) check(b.alloc(v.size() * sizeof(X)), "cudaMalloc");
     if (!v.empty()) check(cudaMemcpyAsync(b.ptr, v.data(), v.size() * sizeof(X), cudaMemcpyHostToDevice, s), "upload");
 }
 
@@ -154,7 +157,7 @@ struct cubo_ptycho_plan {
     DeviceBuffer maxes, sums, aperture64, mask_dev, error_scratch, loss_slot;
     DeviceBuffer tw_r, tw_c, tw_r64, tw_c64;
     DeviceBuffer c_planes, fault;
-    DeviceBuffer positions64, initial64, object_before, far64, position_bad;
+    DeviceBuffer positions64, initial64, object_before, far64, position_bad, fractions64;
 
     ~cubo_ptycho_plan() {
         for (auto &t : pending) { event_pool.push_back(t.a); event_pool.push_back(t.b); }
@@ -288,7 +291,13 @@ void build_scan(cubo_ptycho_plan *p, const double *rows_in, const double *column
     cudaStream_t s = p->ctx->stream;
     const int R = p->R, C = p->C, n = p->n, P = p->P;
     std::vector<int> rr(P), cc(P), cls(P);
-    std::map<std::pair<uint64_t, uint64_t>, int> class_of;
+    struct PairHash {
+        size_t operator()(const std::pair<uint64_t, uint64_t> &k) const {
+            return std::hash<uint64_t>()(k.first * 0x9E3779B97F4A7C15ull ^ k.second);
+        }
+    };
+    std::unordered_map<std::pair<uint64_t, uint64_t>, int, PairHash> class_of;
+    class_of.reserve((size_t)P);
     std::vector<std::pair<double, double>> fractions;  // classes 1..
     for (int i = 0; i < P; i++) {
         const double r = rows_in[i], c = columns_in[i];
@@ -352,19 +361,15 @@ void build_scan(cubo_ptycho_plan *p, const double *rows_in, const double *column
     if (frac > 0) {
         if (p->shift_tmp64.bytes < (size_t)frac * n * sizeof(double2))
             check(p->shift_tmp64.alloc((size_t)frac * n * sizeof(double2)), "cudaMalloc shift table");
-        std::vector<double2> rrmp((size_t)frac * R), crmp((size_t)frac * C);
-        for (int f = 0; f < frac; f++) {  // Ptychography.swift:304-311
-            for (int r = 0; r < R; r++) {
-                const double a = -2 * kPi * frequency(r, R) * fractions[f].first;
-                rrmp[(size_t)f * R + r] = make_double2(std::cos(a), std::sin(a));
-            }
-            for (int c = 0; c < C; c++) {
-                const double a = -2 * kPi * frequency(c, C) * fractions[f].second;
-                crmp[(size_t)f * C + c] = make_double2(std::cos(a), std::sin(a));
-            }
-        }
-        upload(p->ramps_r64, rrmp, s);
-        upload(p->ramps_c64, crmp, s);
+        if (p->ramps_r64.bytes < (size_t)frac * R * sizeof(double2))
+            check(p->ramps_r64.alloc((size_t)frac * R * sizeof(double2)), "cudaMalloc");
+        if (p->ramps_c64.bytes < (size_t)frac * C * sizeof(double2))
+            check(p->ramps_c64.alloc((size_t)frac * C * sizeof(double2)), "cudaMalloc");
+        std::vector<double2> fr((size_t)frac);
+        for (int f = 0; f < frac; f++) fr[f] = make_double2(fractions[f].first, fractions[f].second);
+        upload(p->fractions64, fr, s);  // the ramps themselves are computed on the device (Ptychography.swift:304-311)
+        check(launch_ramp_table(p->fractions64.as<double2>(), frac, R, C, p->ramps_r64.as<double2>(),
+                                p->ramps_c64.as<double2>(), s), "shift ramps");
     }
 }
 

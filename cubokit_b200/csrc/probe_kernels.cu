@@ -320,6 +320,33 @@ cudaError_t launch_shift_ramps(const double2 *spectrum, const double2 *ramps_row
     return cudaGetLastError();
 }
 
+// The phase ramps of the shift classes (Ptychography.swift:304-311): rows[f][r] = exp(-2 pi i frequency(r) dr_f),
+// columns[f][c] likewise with dc_f; fractions[f] = (dr_f, dc_f).
+__global__ void ramp_table_kernel(const double2 *fractions, int classes, int rows, int columns, double2 *ramps_rows,
+                                  double2 *ramps_columns) {
+    const long long i = (long long)blockIdx.x * 256 + threadIdx.x;
+    const int per = rows + columns;
+    if (i >= (long long)classes * per) return;
+    const int f = (int)(i / per), j = (int)(i - (long long)f * per);
+    double sn, cs;
+    if (j < rows) {
+        sincospi(-2.0 * frequency(j, rows) * fractions[f].x, &sn, &cs);
+        ramps_rows[(size_t)f * rows + j] = make_double2(cs, sn);
+    } else {
+        const int c = j - rows;
+        sincospi(-2.0 * frequency(c, columns) * fractions[f].y, &sn, &cs);
+        ramps_columns[(size_t)f * columns + c] = make_double2(cs, sn);
+    }
+}
+
+cudaError_t launch_ramp_table(const double2 *fractions, int classes, int rows, int columns, double2 *ramps_rows,
+                              double2 *ramps_columns, cudaStream_t s) {
+    if (classes <= 0) return cudaSuccess;
+    ramp_table_kernel<<<blocks((long long)classes * (rows + columns)), 256, 0, s>>>(fractions, classes, rows, columns,
+                                                                                    ramps_rows, ramps_columns);
+    return cudaGetLastError();
+}
+
 template <typename T>
 cudaError_t launch_convert(const double2 *in, C2<T> *out, long long count, cudaStream_t s) {
     convert_kernel<T><<<blocks(count), 256, 0, s>>>(in, out, count);
