@@ -12,6 +12,8 @@ It restates, in vectorised NumPy (``np.fft`` is pocketfft in double, NumPy's fft
   * ``Sources/CuboPtycho/PtychographyPreparation.swift:244-259``  ``initialProbe`` energy scaling
   * ``Sources/CuboPtycho/PtychographyPreparation.swift:142-183,296-344``  ``amplitudes(from:origins:shift:)``: the
     bilinear and periodic cubic-spline pattern shifts, square-root amplitudes and mean intensities
+  * ``Sources/CuboPtycho/PtychographyEngines.swift:121-267,270-298``  ``MixedstatePtychography`` (reconstruct,
+    orthogonalize, initialProbes: NumPy's own legacy ``RandomState`` draws)
   * ``Sources/CuboPtycho/Ptychography.swift:53-85,260-264,371-377,398-401,411-472``  position correction
     (``PtychographyPositionCorrection``: the per-position 2 x 2 least-squares step, its limits, the centre-of-mass
     constraint)
@@ -398,6 +400,115 @@ def reconstruct(amplitudes, positions, obj, probe, iterations=8, step_size=0.5, 
             progress(it + 1, iterations)
     if position_correction is not None:
         return o.reshape(object_rows, object_columns), p, np.asarray(errors), current
+    return o.reshape(object_rows, object_columns), p, np.asarray(errors)
+
+
+# ---------------------------------------------------------------- mixed state (PtychographyEngines.swift)
+
+def orthogonalize(probes):
+    """``MixedstatePtychography.orthogonalize`` (``PtychographyEngines.swift:265-269,300-323``): the states become the
+    eigenvectors of their Gram matrix ``G[i][j] = sum conj(p_i) p_j``, ``new_i = sum_j V[j][i] p_j``, by decreasing
+    eigenvalue (ties: the later index first, NumPy's ascending argsort reversed).  Eigenvector phases are LAPACK's."""
+    p = np.asarray(probes, np.complex128)
+    states = p.shape[0]
+    flat = p.reshape(states, -1)
+    g = np.conj(flat) @ flat.T
+    values, vectors = np.linalg.eigh(g)
+    mixed = vectors.T @ flat
+    order = sorted(range(states), key=lambda i: (-values[i], -i))
+    return mixed[order].reshape(p.shape)
+
+
+def initial_probes(first, count, seed):
+    """``MixedstatePtychography.initialProbes`` (``PtychographyEngines.swift:270-298``): state 0 is ``first``; each further
+    state is the previous one times exp(-2 pi i ((u - 1/2) f_row + (v - 1/2) f_col)), u then v drawn from
+    ``np.random.RandomState(seed)``."""
+    if not (0 < count < 4096):
+        raise PtychographyError("count")
+    first = np.asarray(first, np.complex128)
+    rows, columns = first.shape
+    rng = np.random.RandomState(seed)
+    fr, fc = fftfreq_grid(rows, columns)
+    out = [first]
+    for _ in range(1, count):
+        u, v = rng.rand(), rng.rand()
+        phase = -2 * np.pi * (u - 0.5) * fr[:, None] - 2 * np.pi * (v - 0.5) * fc[None, :]
+        out.append(out[-1] * (np.cos(phase) + 1j * np.sin(phase)))
+    return np.stack(out)
+
+
+def mixedstate_reconstruct(amplitudes, positions, obj, probes, iterations=8, step_size=0.5, normalization_minimum=1.0,
+                           fix_probe=False, pure_phase_object=False, fix_probe_center_of_mass=False,
+                           constrain_probe_amplitude=False, probe_amplitude_relative_radius=0.5,
+                           probe_amplitude_relative_width=0.05, orthogonalize_probes=True, fix_probe_aperture=False,
+                           probe_support_mask=None, error_normalization="suppliedAmplitudeEnergy", mean_intensity=None,
+                           zero_pixel_error="reference"):
+    """``MixedstatePtychography.reconstruct`` (``PtychographyEngines.swift:146-262``): several incoherent probe states on
+    one object; the far-field intensity is the sum over states.  ``probes`` (S, R, C).  Returns ``(object, probes,
+    errors)``."""
+    obj = np.array(obj, np.complex128)
+    p = np.array(probes, np.complex128)
+    states, rows, columns = p.shape
+    n = rows * columns
+    positions = np.asarray(positions, np.float64).reshape(-1, 2)
+    count = len(positions)
+    validate(amplitudes, positions, obj.shape, (rows, columns), iterations, step_size, normalization_minimum,
+             probe_amplitude_relative_radius, probe_amplitude_relative_width, probe_support_mask)
+    amp = np.asarray(amplitudes, np.float64).reshape(count, n)
+    divisor = error_divisor(amp, count, error_normalization, mean_intensity)
+    initial_aperture = np.abs(np.fft.fft2(p[0])) if fix_probe_aperture else None
+    object_rows, object_columns = obj.shape
+    rr = round_half_even(positions[:, 0])
+    cc = round_half_even(positions[:, 1])
+    dr, dc = positions[:, 0] - rr, positions[:, 1] - cc
+    idx = patch_indices(rows, columns, object_rows, object_columns, rr.astype(np.int64), cc.astype(np.int64))
+    mask = None if probe_support_mask is None else np.asarray(probe_support_mask, bool).reshape(rows, columns)
+    m = normalization_minimum
+    o = obj.reshape(-1).copy()
+    errors = []
+
+    def norm(local, maximum):
+        return 1 / np.sqrt(1e-16 + ((1 - m) * local) ** 2 + (m * maximum) ** 2)
+
+    for it in range(iterations):
+        op = o[idx]                                                   # (P, n)
+        shifted = np.stack([shifted_probes(np.fft.fft2(p[s]), dr, dc).reshape(count, n) for s in range(states)])
+        far = np.fft.fft2((shifted * op[None]).reshape(states, count, rows, columns)).reshape(states, count, n)
+        intensity = np.sum(far.real ** 2 + far.imag ** 2, axis=0)     # (P, n)
+        amplitude = np.sqrt(intensity)
+        zero = amplitude == 0
+        with np.errstate(divide="ignore", invalid="ignore"):
+            factor = np.where(zero, 0.0, amp / np.where(zero, 1.0, amplitude) - 1)
+        terms = np.where(zero, np.inf if zero_pixel_error == "reference" else amp * amp, (amp - amplitude) ** 2)
+        error = float(np.sum(terms))
+        e = np.fft.ifft2((far * factor[None]).reshape(states, count, rows, columns)).reshape(states, count, n)
+        grad_o = np.zeros(o.size, np.complex128)
+        pn = np.zeros(o.size)
+        np.add.at(grad_o, idx.ravel(), np.sum(np.conj(shifted) * e, axis=0).ravel())
+        np.add.at(pn, idx.ravel(), np.sum(shifted.real ** 2 + shifted.imag ** 2, axis=0).ravel())
+        grad_p = np.sum(np.conj(op)[None] * e, axis=1).reshape(states, rows, columns)
+        on = np.sum(op.real ** 2 + op.imag ** 2, axis=0).reshape(rows, columns)
+        o = o + step_size * norm(pn, pn.max()) * grad_o
+        a = np.abs(o)                                                 # the threshold, always (:112-116)
+        target = np.ones_like(a) if pure_phase_object else np.minimum(a, 1.0)
+        ph = np.arctan2(o.imag, o.real)
+        o = target * np.cos(ph) + 1j * target * np.sin(ph)
+        if not fix_probe:
+            p = p + step_size * norm(on, on.max())[None] * grad_p
+            if fix_probe_center_of_mass:
+                com = probe_center_of_mass(p[0])
+                if com is not None:
+                    p = np.stack([fourier_shift(p[s], -com[0], -com[1]) for s in range(states)])
+            if fix_probe_aperture:
+                p[0] = aperture_constraint(p[0], initial_aperture)
+            if constrain_probe_amplitude:
+                p = np.stack([amplitude_constraint(p[s], probe_amplitude_relative_radius,
+                                                   probe_amplitude_relative_width) for s in range(states)])
+        if mask is not None:
+            p = np.where(mask[None], p, 0)
+        if orthogonalize_probes and states > 1:
+            p = orthogonalize(p)
+        errors.append(error / divisor)
     return o.reshape(object_rows, object_columns), p, np.asarray(errors)
 
 

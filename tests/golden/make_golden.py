@@ -16,6 +16,8 @@ Which reference test each group pins (paths inside the CuboKit project):
                   intensities: bilinear and cubic-spline orders, per-position origins)
   ptycho.npz also keeps the raw cube and uniform origin of PtychographyTests.swift:184-193 (bilinear preprocessing
                   through to the engine's amplitude pin)
+  mixed.npz    Tests/CuboPtychoTests/EngineTests.swift:86-188,262-305 (mixed-state engine: five cases, the
+                orthogonalisation, py4DSTEM's initial states, the mixed engine's support / aperture extras)
   positions.npz  Tests/CuboPtychoTests/PositionCorrectionTests.swift:43-110 (position correction: five settings on
                   8 x 8 positions started up to 0.3 px off, four iterations; the exact-data case; tools/ptycho/
                   position_pins.py, py4DSTEM reconstruct(fix_positions=False))
@@ -120,6 +122,56 @@ def engines(fx):
     return s
 
 
+def mixed(fx):
+    """The mixed-state part of engines.json: reconstruction cases, the orthogonalisation pin, the initial states, and the
+    mixed engine's support / aperture extras."""
+    p = json.loads((fx / "engines.json").read_text())
+    m, x = p["mixed"], p["extras"]
+    s = {}
+    for k in ("rows", "columns", "objectRows", "objectColumns"):
+        _scalar(s, k, p[k])
+    s["positions"] = np.asarray(p["positions"], np.float64)
+    _cx(s, "initialObject", p["initialObject"])
+    s["amplitudes"] = np.asarray(m["amplitudes"], np.float64)
+    _scalar(s, "meanIntensity", m["preprocessing"]["meanIntensity"])
+    s["preprocessing_raw"] = np.asarray(m["preprocessing"]["raw"], np.float64)
+    s["preprocessing_origin"] = np.asarray(m["preprocessing"]["origin"], np.float64)
+    _cx(s, "startStates", m["startStates"])
+    _scalar(s, "cases", len(m["cases"]))
+    for i, c in enumerate(m["cases"]):
+        pre = f"case{i}_"
+        for k in ("name", "numProbes", "fixProbeCenterOfMass", "orthogonalize", "constrainProbeAmplitude", "radius",
+                  "width", "fixProbe", "purePhase"):
+            _scalar(s, pre + k, c[k])
+        _cx(s, pre + "object", c["object"])
+        _cx(s, pre + "probes", c["probes"])
+        s[pre + "errors"] = np.asarray(c["errors"], np.float64)
+    o = m["orthogonalization"]
+    _scalar(s, "orth_count", o["count"])
+    _cx(s, "orth_input", o["input"])
+    _cx(s, "orth_output", o["output"])
+    _scalar(s, "inits", len(m["inits"]))
+    for i, c in enumerate(m["inits"]):
+        pre = f"init{i}_"
+        for k in ("seed", "count", "meanIntensity"):
+            _scalar(s, pre + k, c[k])
+        _cx(s, pre + "first", c["first"])
+        _cx(s, pre + "states", c["states"])
+        s[pre + "draws"] = np.asarray(c["draws"], np.float64)
+    s["support"] = np.asarray(x["support"], np.bool_)
+    extras = [c for c in x["cases"] if c["engine"] == "mixed"]
+    _scalar(s, "extras", len(extras))
+    for i, c in enumerate(extras):
+        pre = f"extra{i}_"
+        _scalar(s, pre + "name", c["name"])
+        for k in ("fixProbeCenterOfMass", "fixProbeAperture", "fixProbe", "constrainProbeAmplitude", "radius", "width"):
+            _scalar(s, pre + k, c[k])
+        _cx(s, pre + "object", c["object"])
+        _cx(s, pre + "probe", c["probe"])
+        s[pre + "errors"] = np.asarray(c["errors"], np.float64)
+    return s
+
+
 def options(fx):
     o = json.loads((fx / "options.json").read_text())
     s = {}
@@ -212,7 +264,7 @@ def main():
     root = Path(sys.argv[1]) if len(sys.argv) > 1 else Path("/root/reference")
     fx = root / "Tests/CuboPtychoTests/Fixtures"
     for name, fn in (("ptycho", ptycho), ("odd", odd), ("engines", engines), ("options", options),
-                     ("preprocess", preprocess), ("positions", positions)):
+                     ("preprocess", preprocess), ("positions", positions), ("mixed", mixed)):
         arrays = fn(fx)
         np.savez_compressed(HERE / f"{name}.npz", **arrays)
         print(name, len(arrays), "arrays", (HERE / f"{name}.npz").stat().st_size, "bytes")

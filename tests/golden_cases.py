@@ -223,3 +223,72 @@ def position_exact_case():
     settings = dict(step_size=0.5, max_update_distance=None, max_total_distance=None, row_sampling=None,
                     column_sampling=None, constrain_center_of_mass=False)
     return inputs, settings, z["exact_positions"], z["truthPositions"], (float(z["rowSampling"]), float(z["columnSampling"]))
+
+
+def align_phases(a, b):
+    """Each state of ``a`` rotated by the global phase that best matches ``b`` (the eigenvector phase convention of the
+    orthogonalisation is free; ``EngineTests.swift:46-64``)."""
+    out = np.array(a, np.complex128)
+    for s in range(out.shape[0]):
+        z = np.sum(np.conj(b[s]) * out[s])
+        if abs(z) > 0:
+            out[s] = out[s] * np.conj(z) / abs(z)
+    return out
+
+
+def mixed_cases():
+    """``EngineTests.swift:86-110``: five mixed-state settings on the shared start, three iterations, step 0.35,
+    normalisation minimum 0.7, mean-intensity errors.  Each entry: (name, inputs, expected (object, probes, errors),
+    orthogonalised)."""
+    z = load("mixed")
+    R, C, OR, OC = int(z["rows"]), int(z["columns"]), int(z["objectRows"]), int(z["objectColumns"])
+    start = _cx(z, "startStates", (3, R, C))
+    out = []
+    for i in range(int(z["cases"])):
+        g = lambda k: z[f"case{i}_{k}"]
+        S = int(g("numProbes"))
+        inputs = dict(amplitudes=z["amplitudes"].reshape(-1, R, C), positions=z["positions"],
+                      obj=_cx(z, "initialObject", (OR, OC)), probes=start[:S], iterations=3, step_size=0.35,
+                      normalization_minimum=0.7, fix_probe=bool(g("fixProbe")), pure_phase_object=bool(g("purePhase")),
+                      fix_probe_center_of_mass=bool(g("fixProbeCenterOfMass")),
+                      constrain_probe_amplitude=bool(g("constrainProbeAmplitude")),
+                      probe_amplitude_relative_radius=float(g("radius")),
+                      probe_amplitude_relative_width=float(g("width")), orthogonalize_probes=bool(g("orthogonalize")),
+                      error_normalization="meanIntensity", mean_intensity=float(z["meanIntensity"]))
+        expected = (_cx(z, f"case{i}_object", (OR, OC)), _cx(z, f"case{i}_probes", (S, R, C)), g("errors"))
+        out.append((str(g("name")), inputs, expected, bool(g("orthogonalize"))))
+    for i in range(int(z["extras"])):  # EngineTests.swift:262-305, the mixed engine's aperture / support cases
+        g = lambda k: z[f"extra{i}_{k}"]
+        inputs = dict(amplitudes=z["amplitudes"].reshape(-1, R, C), positions=z["positions"],
+                      obj=_cx(z, "initialObject", (OR, OC)), probes=start[:2], iterations=3, step_size=0.35,
+                      normalization_minimum=0.7, fix_probe=bool(g("fixProbe")),
+                      fix_probe_center_of_mass=bool(g("fixProbeCenterOfMass")),
+                      constrain_probe_amplitude=bool(g("constrainProbeAmplitude")),
+                      probe_amplitude_relative_radius=float(g("radius")),
+                      probe_amplitude_relative_width=float(g("width")), fix_probe_aperture=bool(g("fixProbeAperture")),
+                      probe_support_mask=z["support"].reshape(R, C), error_normalization="meanIntensity",
+                      mean_intensity=float(z["meanIntensity"]))
+        expected = (_cx(z, f"extra{i}_object", (OR, OC)), _cx(z, f"extra{i}_probe", (2, R, C)), g("errors"))
+        out.append(("extras." + str(g("name")), inputs, expected, True))
+    return out
+
+
+def mixed_orthogonalization_case():
+    z = load("mixed")
+    R, C = int(z["rows"]), int(z["columns"])
+    count = int(z["orth_count"])
+    return _cx(z, "orth_input", (count, R, C)), _cx(z, "orth_output", (count, R, C))
+
+
+def mixed_init_cases():
+    """``EngineTests.swift:131-149``: py4DSTEM's initial states (first state scaled to the mean intensity)."""
+    z = load("mixed")
+    R, C = int(z["rows"]), int(z["columns"])
+    out = []
+    for i in range(int(z["inits"])):
+        g = lambda k: z[f"init{i}_{k}"]
+        first = _cx(z, f"init{i}_first", (R, C))
+        first = first * np.sqrt(float(g("meanIntensity")) / (np.sum(np.abs(first) ** 2) * R * C))
+        count = int(g("count"))
+        out.append((first, count, int(g("seed")), _cx(z, f"init{i}_states", (count, R, C)), g("draws")))
+    return out

@@ -274,3 +274,33 @@ def test_position_correction_limits_zero_step_and_refusals():
                 no.PositionCorrection(max_update_distance=1.0, row_sampling=0.0, column_sampling=cs)):
         with pytest.raises(no.PtychographyError):
             no.reconstruct(**one, position_correction=bad)
+
+
+# ---------------------------------------------------------------------------------------------------- mixed state
+
+@pytest.mark.parametrize("case", gc.mixed_cases(), ids=lambda c: c[0])
+def test_mixedstate_meets_the_pins(case):
+    """``EngineTests.swift:86-110,262-305``: object, errors and phase-aligned probes within 2e-6; without the
+    orthogonalisation the probes themselves (no free phase)."""
+    name, inputs, (obj, probes, errors), orthogonalized = case
+    o, p, e = no.mixedstate_reconstruct(**inputs)
+    assert max(gc.complex_gap(o, obj), gap(e, errors), gc.complex_gap(gc.align_phases(p, probes), probes)) < 2e-6
+    if not orthogonalized:
+        assert gc.complex_gap(p, probes) < 2e-6
+
+
+def test_mixedstate_orthogonalization_and_initial_states():
+    """``EngineTests.swift:111-149``: the orthogonalisation pin (phase-aligned), mutually orthogonal states of the same
+    total intensity in decreasing order; py4DSTEM's initial states from NumPy's RandomState draws."""
+    x, expected = gc.mixed_orthogonalization_case()
+    q = no.orthogonalize(x)
+    assert gc.complex_gap(gc.align_phases(q, expected), expected) < 2e-6
+    flat = q.reshape(len(q), -1)
+    g = np.conj(flat) @ flat.T
+    assert np.max(np.abs(g - np.diag(np.diag(g)))) < 1e-13 * np.max(np.abs(np.diag(g)))
+    assert abs(np.sum(np.abs(q) ** 2) - np.sum(np.abs(x) ** 2)) < 1e-12 * np.sum(np.abs(x) ** 2)
+    energy = np.real(np.diag(g))
+    assert np.all(energy[:-1] >= energy[1:])
+    for first, count, seed, states, draws in gc.mixed_init_cases():
+        assert gc.complex_gap(no.initial_probes(first, count, seed), states) < 2e-6
+        assert np.array_equal(np.random.RandomState(seed).rand(len(draws)), draws)
