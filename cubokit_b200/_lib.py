@@ -48,6 +48,13 @@ class Params(C.Structure):
     ]
 
 
+class MixedParams(C.Structure):
+    _fields_ = [("states", C.c_int), ("orthogonalize_probes", C.c_int), ("zero_pixel_error", C.c_int)]
+
+
+ZERO_PIXEL_REFERENCE, ZERO_PIXEL_FINITE = 0, 1
+
+
 # Every symbol the header declares, with its ctypes signature (restype, argtypes).
 _dp = C.POINTER(C.c_double)
 SIGNATURES = {
@@ -61,6 +68,12 @@ SIGNATURES = {
     "cubo_ptycho_plan_set_state": (C.c_int, [C.c_void_p, _dp, _dp, _dp, _dp]),
     "cubo_ptycho_plan_get_state": (C.c_int, [C.c_void_p, _dp, _dp, _dp, _dp]),
     "cubo_ptycho_plan_get_positions": (C.c_int, [C.c_void_p, _dp, _dp]),
+    "cubo_ptycho_mixed_params_default": (None, [C.POINTER(MixedParams)]),
+    "cubo_ptycho_mixed_reconstruct": (C.c_int, [C.c_void_p, C.POINTER(Problem), C.POINTER(Params),
+                                                C.POINTER(MixedParams), _dp, _dp, _dp, _dp, _dp]),
+    "cubo_ptycho_mixed_plan_create": (C.c_int, [C.c_void_p, C.POINTER(Problem), C.POINTER(Params),
+                                                C.POINTER(MixedParams), C.POINTER(C.c_void_p)]),
+    "cubo_ptycho_orthogonalize": (C.c_int, [C.c_void_p, C.c_int, C.c_int, C.c_int, _dp, _dp]),
     "cubo_ptycho_plan_iterate": (C.c_int, [C.c_void_p, C.c_int, _dp]),
     "cubo_ptycho_plan_enqueue": (C.c_int, [C.c_void_p, C.c_int]),
     "cubo_ptycho_plan_errors": (C.c_int, [C.c_void_p, C.c_int, _dp]),

@@ -43,6 +43,8 @@ struct ObjectGatherArgs {
     C2<T> *grad;               // object gradient sum conj(S) dpsi
     T *weight;                 // sum |S|^2
     double *tile_max;          // per-tile max of weight
+    int states = 1;            // mixed state (FP64): dpsi and shifted hold one block per state, these strides apart
+    long long dpsi_state_stride = 0, shifted_state_stride = 0;
 };
 
 template <typename T>
@@ -178,6 +180,27 @@ cudaError_t launch_fft2_f64(const Fft2Plan64 &p, double2 *data, int batch, bool 
 cudaError_t launch_position_pass_global(const PositionPassArgs<double> &a, const Fft2Plan64 &fft, int *launches,
                                        cudaStream_t s);
 bool line_fft_supported(int rows, int columns);
+
+// mixed_kernels.cu: the mixed-state engine (MixedstatePtychography, PtychographyEngines.swift:121-267), FP64.
+constexpr int kMaxStates = 16;
+struct MixedPassArgs {
+    int rows, columns, object_rows, object_columns, count, states;
+    ScanTables scan;
+    const double2 *shifted;          // [state][class][pixel]
+    long long shifted_state_stride;  // classes * n
+    const double2 *object;
+    const float *amplitudes;
+    double2 *dpsi;                   // [state][position][pixel]
+    double *error;                   // per position
+    int zero_pixel_infinite;         // a pixel whose summed intensity is 0 adds an infinite error term (else A^2)
+};
+// Exit waves of every state, their far fields, the summed-intensity projection, the inverse transforms.
+cudaError_t launch_mixed_position_pass(const MixedPassArgs &a, const Fft2Plan64 &fft, int *launches, cudaStream_t s);
+// The states become the eigenvectors of their Gram matrix, by decreasing intensity (gram, mixing: states^2 values;
+// scratch: states * n).
+cudaError_t launch_orthogonalize(double2 *probes, int states, int n, double2 *gram, double2 *mixing, double2 *scratch,
+                                 cudaStream_t s);
+
 cudaError_t configure_fft_lines();
 cudaError_t launch_scale_f64(double2 *data, int count, double scale, cudaStream_t s);
 cudaError_t launch_probe_update(double2 *probe, const double2 *grad, const double *weight, int n, const double *max_weight,

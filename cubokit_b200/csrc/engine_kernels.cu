@@ -14,6 +14,7 @@
 #include <cfloat>
 
 #include <algorithm>
+#include <type_traits>
 
 #include "engine.h"
 
@@ -210,7 +211,19 @@ __global__ void __launch_bounds__(kGatherThreads) object_gather_kernel(ObjectGat
             s_off[i][f] = v;
         }
         __syncthreads();
-        if (inside) {
+        if (inside && std::is_same<T, double>::value && a.states > 1) {
+            // mixed state: for each candidate in order, its states in order (PtychographyEngines.swift:197-205)
+            for (int i = 0; i < cnt; i++) {
+                const int k = s_off[i][ly] + s_off[i][a.tile_h + lx];
+                if (k < 0) continue;
+                for (int st = 0; st < a.states; st++) {
+                    const C2<T> d = a.dpsi[(size_t)st * a.dpsi_state_stride + (size_t)s_p[i] * a.n + k];
+                    const C2<T> sv = a.shifted[(size_t)st * a.shifted_state_stride + (size_t)s_cls[i] * a.n + k];
+                    g = cadd(g, cmulc(sv, d));
+                    w += sv.x * sv.x + sv.y * sv.y;
+                }
+            }
+        } else if (inside) {
             // four candidates at a time: their loads are independent, the sums stay in candidate order
             for (int i = 0; i < cnt; i += 4) {
                 int k[4];

@@ -125,6 +125,9 @@ struct cubo_ptycho_plan {
     bool fast = false;      // 128 x 128 FP32 register-resident position pass
     bool bf16 = false;      // 128 x 128 split-BF16 tensor-core position pass
     bool global64 = false;  // FP64 position pass through global memory (the plane does not fit shared memory)
+    int states = 1;         // probe states (the mixed-state engine; 1 = single slice)
+    bool orthogonalize = false;     // mixed state: orthogonalise the states after every iteration
+    bool zero_pixel_infinite = true; // mixed state: an exactly zero far-field pixel adds an infinite error term
     int sms = 148;
     long long error_count = 0;  // residual partials summed by the error kernel
     bool tape_valid = false;    // dpsi holds the residuals of the current state (forward ran, nothing changed since)
@@ -158,6 +161,7 @@ struct cubo_ptycho_plan {
     DeviceBuffer tw_r, tw_c, tw_r64, tw_c64;
     DeviceBuffer c_planes, fault;
     DeviceBuffer positions64, initial64, object_before, far64, position_bad, fractions64;
+    DeviceBuffer gram64, mixing64, ortho64;
 
     ~cubo_ptycho_plan() {
         for (auto &t : pending) { event_pool.push_back(t.a); event_pool.push_back(t.b); }
@@ -355,7 +359,7 @@ void build_scan(cubo_ptycho_plan *p, const double *rows_in, const double *column
         check(launch_tile_lists(p->rr.as<int>(), p->cc.as<int>(), P, R, C, p->OR, p->OC, p->tile_w, p->tile_h, p->tiles_x,
                                 p->tiles, nullptr, p->tile_start.as<int>(), p->tile_list.as<int>(), s), "list candidates");
     }
-    const size_t shifted_bytes = (size_t)p->classes * n * (p->fp64 ? sizeof(double2) : sizeof(float2));
+    const size_t shifted_bytes = (size_t)p->states * p->classes * n * (p->fp64 ? sizeof(double2) : sizeof(float2));
     if (p->shifted.bytes < shifted_bytes) check(p->shifted.alloc(shifted_bytes), "cudaMalloc");
     const int frac = p->classes - 1;
     if (frac > 0) {
@@ -417,7 +421,7 @@ void build_plan(cubo_ptycho_plan *p, const cubo_ptycho_problem *pr) {
     check(p->grad_o.alloc((size_t)p->objects * sizeof(C2<T>)), "cudaMalloc");
     check(p->weight_o.alloc((size_t)p->objects * sizeof(T)), "cudaMalloc");
     check(p->tile_max.alloc((size_t)p->tiles * sizeof(double)), "cudaMalloc");
-    check(p->dpsi.alloc((size_t)P * n * sizeof(C2<T>)), "cudaMalloc dpsi");
+    check(p->dpsi.alloc((size_t)p->states * P * n * sizeof(C2<T>)), "cudaMalloc dpsi");
     p->error_count = p->fast ? (long long)P * fast128_partials_per_position()
                              : p->bf16 ? (long long)P * bf16_partials_per_position() : P;
     if (p->fast) {
@@ -452,7 +456,12 @@ void build_plan(cubo_ptycho_plan *p, const cubo_ptycho_problem *pr) {
     check(p->error.alloc((size_t)p->error_count * sizeof(double)), "cudaMalloc");
     check(p->iteration.alloc(sizeof(int)), "cudaMalloc");
     check(cudaMemsetAsync(p->iteration.ptr, 0, sizeof(int), s), "memset");
-    check(p->probe64.alloc((size_t)n * sizeof(double2)), "cudaMalloc");
+    check(p->probe64.alloc((size_t)p->states * n * sizeof(double2)), "cudaMalloc");
+    if (p->states > 1) {
+        check(p->gram64.alloc((size_t)p->states * p->states * sizeof(double2)), "cudaMalloc");
+        check(p->mixing64.alloc((size_t)p->states * p->states * sizeof(double2)), "cudaMalloc");
+        check(p->ortho64.alloc((size_t)p->states * n * sizeof(double2)), "cudaMalloc");
+    }
     check(p->scratch64.alloc((size_t)n * sizeof(double2)), "cudaMalloc");
     check(p->spectrum64.alloc((size_t)n * sizeof(double2)), "cudaMalloc");
     // probe-gather groups: about eight CTAs per SM of a 148-SM part; a function of the problem only, so the summation
@@ -462,7 +471,7 @@ void build_plan(cubo_ptycho_plan *p, const cubo_ptycho_problem *pr) {
     if (p->fast) p->groups = std::min(P, fast128_ctas());  // the position pass writes one partial per CTA
     check(p->partial_grad.alloc((size_t)p->groups * n * sizeof(C2<T>)), "cudaMalloc");
     check(p->partial_weight.alloc((size_t)p->groups * n * sizeof(T)), "cudaMalloc");
-    check(p->grad_p64.alloc((size_t)n * sizeof(double2)), "cudaMalloc");
+    check(p->grad_p64.alloc((size_t)p->states * n * sizeof(double2)), "cudaMalloc");
     check(p->weight_p64.alloc((size_t)n * sizeof(double)), "cudaMalloc");
     p->probe_blocks = kblocks;
     check(p->probe_block_max.alloc((size_t)kblocks * sizeof(double)), "cudaMalloc");
@@ -514,15 +523,17 @@ void ensure_errors(cubo_ptycho_plan *p, long long needed) {
     p->errors_capacity = cap;
 }
 
-// The shifted-probe table for the current probe: class 0 is the probe itself, classes 1.. its Fourier shifts.
+// The shift table of probe state `st`.
 template <typename T>
-void enqueue_shift_table(cubo_ptycho_plan *p) {
+void enqueue_shift_table_state(cubo_ptycho_plan *p, int st) {
     cudaStream_t s = p->ctx->stream;
     const int n = p->n, frac = p->classes - 1;
-    timed(p, kShiftTable, 1, [&] { return launch_convert<T>(p->probe64.as<double2>(), p->shifted.as<C2<T>>(), n, s); });
+    const double2 *probe = p->probe64.as<double2>() + (size_t)st * n;
+    C2<T> *table = p->shifted.as<C2<T>>() + (size_t)st * p->classes * n;
+    timed(p, kShiftTable, 1, [&] { return launch_convert<T>(probe, table, n, s); });
     if (frac == 0) return;
     timed(p, kShiftTable, 2 + 1 + 2 + 1 + 1, [&] {
-        cudaError_t e = cudaMemcpyAsync(p->spectrum64.ptr, p->probe64.ptr, (size_t)n * sizeof(double2),
+        cudaError_t e = cudaMemcpyAsync(p->spectrum64.ptr, probe, (size_t)n * sizeof(double2),
                                         cudaMemcpyDeviceToDevice, s);
         if (e == cudaSuccess) e = launch_fft2_f64(fft64(p), p->spectrum64.as<double2>(), 1, false, s);
         if (e == cudaSuccess)
@@ -531,36 +542,52 @@ void enqueue_shift_table(cubo_ptycho_plan *p) {
         if (e == cudaSuccess) e = launch_fft2_f64(fft64(p), p->shift_tmp64.as<double2>(), frac, true, s);
         if (e == cudaSuccess) e = launch_scale_f64(p->shift_tmp64.as<double2>(), frac * n, 1.0 / n, s);
         if (e == cudaSuccess)
-            e = launch_convert<T>(p->shift_tmp64.as<double2>(), p->shifted.as<C2<T>>() + n, (long long)frac * n, s);
+            e = launch_convert<T>(p->shift_tmp64.as<double2>(), table + n, (long long)frac * n, s);
         return e;
     });
 }
 
-// Probe update and constraints, FP64 (Ptychography.swift:383-395).
+// The shifted-probe table for the current probe: class 0 is the probe itself, classes 1.. its Fourier shifts (one
+// table per probe state, [state][class][pixel]).
+template <typename T>
+void enqueue_shift_table(cubo_ptycho_plan *p) {
+    for (int st = 0; st < p->states; st++) enqueue_shift_table_state<T>(p, st);
+}
+
+// Probe update and constraints, FP64 (Ptychography.swift:383-395).  With several probe states
+// (PtychographyEngines.swift:212-244): every state takes its own gradient with the shared normalisation; the centre of
+// mass of state 0 shifts every state; the aperture constrains state 0; the amplitude constraint and the support apply
+// to every state; then the orthogonalisation.
 void enqueue_probe_side(cubo_ptycho_plan *p) {
     cudaStream_t s = p->ctx->stream;
     const cubo_ptycho_params &pp = p->params;
-    const int n = p->n;
-    double2 *probe = p->probe64.as<double2>(), *x = p->scratch64.as<double2>();
+    const int n = p->n, S = p->states;
+    double2 *probes = p->probe64.as<double2>(), *x = p->scratch64.as<double2>();
     double *sums = p->sums.as<double>();
     if (!pp.fix_probe) {
-        timed(p, kProbeSide, 1, [&] {
-            return launch_probe_update(probe, p->grad_p64.as<double2>(), p->weight_p64.as<double>(), n,
-                                       p->maxes.as<double>() + 1, pp.step_size, pp.normalization_minimum, s);
-        });
-        if (pp.fix_probe_center_of_mass) {  // PtychographyConstraints.swift:34-37
-            timed(p, kProbeSide, 7, [&] {
-                cudaError_t e = launch_probe_moments(probe, p->R, p->C, sums, s);
-                if (e == cudaSuccess) e = cudaMemcpyAsync(x, probe, (size_t)n * sizeof(double2), cudaMemcpyDeviceToDevice, s);
-                if (e == cudaSuccess) e = launch_fft2_f64(fft64(p), x, 1, false, s);
-                if (e == cudaSuccess) e = launch_com_ramp(x, p->R, p->C, sums, s);
-                if (e == cudaSuccess) e = launch_fft2_f64(fft64(p), x, 1, true, s);
-                if (e == cudaSuccess) e = launch_scale_f64(x, n, 1.0 / n, s);
-                if (e == cudaSuccess) e = launch_commit_if_valid(probe, x, n, sums, s);
-                return e;
+        for (int st = 0; st < S; st++)
+            timed(p, kProbeSide, 1, [&] {
+                return launch_probe_update(probes + (size_t)st * n, p->grad_p64.as<double2>() + (size_t)st * n,
+                                           p->weight_p64.as<double>(), n, p->maxes.as<double>() + 1, pp.step_size,
+                                           pp.normalization_minimum, s);
             });
+        if (pp.fix_probe_center_of_mass) {  // PtychographyConstraints.swift:34-37: the centre of mass of state 0
+            timed(p, kProbeSide, 1, [&] { return launch_probe_moments(probes, p->R, p->C, sums, s); });
+            for (int st = 0; st < S; st++) {
+                double2 *probe = probes + (size_t)st * n;
+                timed(p, kProbeSide, 6, [&] {
+                    cudaError_t e = cudaMemcpyAsync(x, probe, (size_t)n * sizeof(double2), cudaMemcpyDeviceToDevice, s);
+                    if (e == cudaSuccess) e = launch_fft2_f64(fft64(p), x, 1, false, s);
+                    if (e == cudaSuccess) e = launch_com_ramp(x, p->R, p->C, sums, s);
+                    if (e == cudaSuccess) e = launch_fft2_f64(fft64(p), x, 1, true, s);
+                    if (e == cudaSuccess) e = launch_scale_f64(x, n, 1.0 / n, s);
+                    if (e == cudaSuccess) e = launch_commit_if_valid(probe, x, n, sums, s);
+                    return e;
+                });
+            }
         }
-        if (pp.fix_probe_aperture) {  // PtychographyConstraints.swift:59-71
+        if (pp.fix_probe_aperture) {  // PtychographyConstraints.swift:59-71, state 0
+            double2 *probe = probes;
             timed(p, kProbeSide, 8, [&] {
                 cudaError_t e = launch_energy(probe, n, sums + 3, s);
                 if (e == cudaSuccess) e = cudaMemcpyAsync(x, probe, (size_t)n * sizeof(double2), cudaMemcpyDeviceToDevice, s);
@@ -573,20 +600,31 @@ void enqueue_probe_side(cubo_ptycho_plan *p) {
                 return e;
             });
         }
-        if (pp.constrain_probe_amplitude) {  // PtychographyConstraints.swift:40-55
-            timed(p, kProbeSide, 4, [&] {
-                cudaError_t e = launch_energy(probe, n, sums + 3, s);
-                if (e == cudaSuccess)
-                    e = launch_amplitude_mask(probe, p->R, p->C, pp.probe_amplitude_relative_radius,
-                                              pp.probe_amplitude_relative_width, s);
-                if (e == cudaSuccess) e = launch_energy(probe, n, sums + 4, s);
-                if (e == cudaSuccess) e = launch_renormalise(probe, probe, n, sums + 3, sums + 4, s);
-                return e;
-            });
+        if (pp.constrain_probe_amplitude) {  // PtychographyConstraints.swift:40-55, every state
+            for (int st = 0; st < S; st++) {
+                double2 *probe = probes + (size_t)st * n;
+                timed(p, kProbeSide, 4, [&] {
+                    cudaError_t e = launch_energy(probe, n, sums + 3, s);
+                    if (e == cudaSuccess)
+                        e = launch_amplitude_mask(probe, p->R, p->C, pp.probe_amplitude_relative_radius,
+                                                  pp.probe_amplitude_relative_width, s);
+                    if (e == cudaSuccess) e = launch_energy(probe, n, sums + 4, s);
+                    if (e == cudaSuccess) e = launch_renormalise(probe, probe, n, sums + 3, sums + 4, s);
+                    return e;
+                });
+            }
         }
     }
     if (!p->mask.empty())  // Ptychography.swift:395, not gated on fixProbe
-        timed(p, kProbeSide, 1, [&] { return launch_support_mask(probe, p->mask_dev.as<unsigned char>(), n, s); });
+        for (int st = 0; st < S; st++)
+            timed(p, kProbeSide, 1, [&] {
+                return launch_support_mask(probes + (size_t)st * n, p->mask_dev.as<unsigned char>(), n, s);
+            });
+    if (p->orthogonalize && S > 1)  // PtychographyEngines.swift:250-253, not gated on fixProbe
+        timed(p, kProbeSide, 4, [&] {
+            return launch_orthogonalize(probes, S, n, p->gram64.as<double2>(), p->mixing64.as<double2>(),
+                                        p->ortho64.as<double2>(), s);
+        });
 }
 
 // Shifted probes, then the position pass over every position: residuals (dpsi) and per-position squared errors.
@@ -619,6 +657,19 @@ void enqueue_position_pass(cubo_ptycho_plan *p) {
         fa.partial_grad = p->partial_grad.as<float2>(); fa.partial_weight = p->partial_weight.as<float>();
         fa.fault = p->fault.as<int>();
         timed(p, kPositionPass, 1, [&] { return launch_fast128(fa, p->sms, s); });
+    } else if (p->states > 1) {
+        if constexpr (std::is_same<T, double>::value) {
+            MixedPassArgs ma{};
+            ma.rows = p->R; ma.columns = p->C; ma.object_rows = p->OR; ma.object_columns = p->OC; ma.count = p->P;
+            ma.states = p->states; ma.scan = scan; ma.shifted = p->shifted.as<double2>();
+            ma.shifted_state_stride = (long long)p->classes * n; ma.object = p->object.as<double2>();
+            ma.amplitudes = p->amplitudes.as<float>(); ma.dpsi = p->dpsi.as<double2>(); ma.error = p->error.as<double>();
+            ma.zero_pixel_infinite = p->zero_pixel_infinite ? 1 : 0;
+            int count = 0;
+            timed(p, kPositionPass, 0, [&] { return launch_mixed_position_pass(ma, fft64(p), &count, s); });
+            p->launches += count;
+            if (p->timing) p->kind_launches[kPositionPass] += count;
+        }
     } else if (p->global64) {
         int count = 0;
         if constexpr (std::is_same<T, double>::value) {
@@ -642,19 +693,25 @@ void enqueue_gathers(cubo_ptycho_plan *p) {
     ga.tiles_x = p->tiles_x; ga.tile_w = p->tile_w; ga.tile_h = p->tile_h; ga.tile_start = p->tile_start.as<int>(); ga.tile_list = p->tile_list.as<int>();
     ga.scan = scan; ga.shifted = p->shifted.as<C2<T>>(); ga.dpsi = p->dpsi.as<C2<T>>();
     ga.grad = p->grad_o.as<C2<T>>(); ga.weight = p->weight_o.as<T>(); ga.tile_max = p->tile_max.as<double>();
+    ga.states = p->states;
+    ga.dpsi_state_stride = (long long)p->P * n;
+    ga.shifted_state_stride = (long long)p->classes * n;
     timed(p, kObjectGather, 1, [&] { return launch_object_gather<T>(ga, p->tiles, s); });
 
     ProbeGatherArgs<T> pg{};
     pg.rows = p->R; pg.columns = p->C; pg.object_rows = p->OR; pg.object_columns = p->OC; pg.n = n;
     pg.count = p->P; pg.groups = p->groups; pg.scan = scan; pg.object = p->object.as<C2<T>>();
     pg.dpsi = p->dpsi.as<C2<T>>(); pg.partial_grad = p->partial_grad.as<C2<T>>(); pg.partial_weight = p->partial_weight.as<T>();
-    if (!p->fast)  // the 128 x 128 FP32 position pass already wrote per-CTA probe partials
-        timed(p, kProbeGather, 1, [&] { return launch_probe_gather<T>(pg, s); });
-    timed(p, kProbeReduce, 1, [&] {
-        return launch_probe_reduce<T>(p->partial_grad.as<C2<T>>(), p->partial_weight.as<T>(), p->groups, n,
-                                      p->grad_p64.as<double2>(), p->weight_p64.as<double>(),
-                                      p->probe_block_max.as<double>(), s);
-    });
+    for (int st = 0; st < p->states; st++) {  // each probe state's gradient from its own residuals
+        pg.dpsi = p->dpsi.as<C2<T>>() + (size_t)st * p->P * n;
+        if (!p->fast)  // the 128 x 128 FP32 position pass already wrote per-CTA probe partials
+            timed(p, kProbeGather, 1, [&] { return launch_probe_gather<T>(pg, s); });
+        timed(p, kProbeReduce, 1, [&] {
+            return launch_probe_reduce<T>(p->partial_grad.as<C2<T>>(), p->partial_weight.as<T>(), p->groups, n,
+                                          p->grad_p64.as<double2>() + (size_t)st * n, p->weight_p64.as<double>(),
+                                          p->probe_block_max.as<double>(), s);
+        });
+    }
     timed(p, kMaxReduce, 2, [&] {
         cudaError_t e = launch_max_reduce(p->tile_max.as<double>(), p->tiles, p->maxes.as<double>(), s);
         if (e == cudaSuccess) e = launch_max_reduce(p->probe_block_max.as<double>(), p->probe_blocks, p->maxes.as<double>() + 1, s);
@@ -694,7 +751,9 @@ void enqueue_iteration(cubo_ptycho_plan *p) {
     if (correct)
         check(cudaMemcpyAsync(p->object_before.ptr, p->object.ptr, (size_t)p->objects * sizeof(double2),
                               cudaMemcpyDeviceToDevice, s), "copy object");
-    const int cap = !correct && pp.constrain_object_amplitude ? 1 : 0, pure = !correct && pp.pure_phase_object ? 1 : 0;
+    // the mixed-state engine always applies the threshold (PtychographyEngines.swift:209)
+    const bool threshold = p->states > 1 || pp.constrain_object_amplitude;
+    const int cap = !correct && threshold ? 1 : 0, pure = !correct && pp.pure_phase_object ? 1 : 0;
     timed(p, kObjectUpdate, 1, [&] {
         return launch_object_update<T>(p->object.as<C2<T>>(), p->grad_o.as<C2<T>>(), p->weight_o.as<T>(),
                                        (int)p->objects, p->maxes.as<double>(), pp.step_size, pp.normalization_minimum,
@@ -834,19 +893,40 @@ int cubo_ptycho_synchronize(cubo_ptycho_context *ctx) {
     return run_guarded(ctx, [&] { check(cudaStreamSynchronize(ctx->stream), "cudaStreamSynchronize"); });
 }
 
-int cubo_ptycho_plan_create(cubo_ptycho_context *ctx, const cubo_ptycho_problem *pr, const cubo_ptycho_params *pp,
-                            cubo_ptycho_plan **out) {
+}  // extern "C"
+
+namespace {
+// cubo_ptycho_plan_create, and the mixed-state engine's plan when `mixed` is given.
+int create_plan(cubo_ptycho_context *ctx, const cubo_ptycho_problem *pr, const cubo_ptycho_params *pp,
+                const cubo_ptycho_mixed_params *mixed, cubo_ptycho_plan **out) {
     if (!out) return CUBO_PTYCHO_INVALID_INPUT;
     *out = nullptr;
     std::unique_ptr<cubo_ptycho_plan> plan;
     const int status = run_guarded(ctx, [&] {
         double divisor = 0;
         validate(pr, pp, &divisor);
+        if (mixed) {  // PtychographyEngines.swift:159-166; the engine is the reference's Double one
+            if (!(mixed->states >= 1 && mixed->states <= kMaxStates))
+                fail(CUBO_PTYCHO_INVALID_INPUT, "probe states: 1 to " + std::to_string(kMaxStates));
+            if (pp->form != CUBO_PTYCHO_FORM_FP64)
+                fail(CUBO_PTYCHO_INVALID_INPUT, "the mixed-state engine runs in the FP64 form (the reference's is Double)");
+            if (pp->has_position_correction) fail(CUBO_PTYCHO_INVALID_INPUT, "no position correction in mixed state");
+            if (mixed->zero_pixel_error != CUBO_PTYCHO_ZERO_PIXEL_REFERENCE &&
+                mixed->zero_pixel_error != CUBO_PTYCHO_ZERO_PIXEL_FINITE)
+                fail(CUBO_PTYCHO_INVALID_INPUT, "zero-pixel error mode");
+            if (!line_fft_supported(pr->rows, pr->columns))
+                fail(CUBO_PTYCHO_UNSUPPORTED, "detector sides above the line transform's 4096");
+        }
         plan.reset(new cubo_ptycho_plan());
         cubo_ptycho_plan *p = plan.get();
         p->ctx = ctx;
         p->R = pr->rows; p->C = pr->columns; p->OR = pr->object_rows; p->OC = pr->object_columns; p->P = pr->count;
         p->n = p->R * p->C;
+        if (mixed) {
+            p->states = mixed->states;
+            p->orthogonalize = mixed->orthogonalize_probes != 0;
+            p->zero_pixel_infinite = mixed->zero_pixel_error == CUBO_PTYCHO_ZERO_PIXEL_REFERENCE;
+        }
         p->objects = (long long)p->OR * p->OC;
         p->params = *pp;
         if (pp->probe_support_mask) p->mask.assign(pp->probe_support_mask, pp->probe_support_mask + p->n);
@@ -861,7 +941,7 @@ int cubo_ptycho_plan_create(cubo_ptycho_context *ctx, const cubo_ptycho_problem 
         const bool smem_pass = position_pass_supported(p->n, p->fp64) &&
                                position_pass_smem(p->n, p->R, p->C, p->fp64) <= (size_t)optin;
         // FP64 planes too large for one CTA go through global memory (any size the line transform takes)
-        p->global64 = p->fp64 && (!smem_pass || pp->variant == CUBO_PTYCHO_VARIANT_GLOBAL);
+        p->global64 = p->fp64 && (!smem_pass || pp->variant == CUBO_PTYCHO_VARIANT_GLOBAL || p->states > 1);
         if (!smem_pass && !(p->global64 && line_fft_supported(p->R, p->C)))
             fail(CUBO_PTYCHO_UNSUPPORTED, "detector of " + std::to_string(p->n) + " pixels exceeds the shared-memory "
                                               "transform of this form");
@@ -904,6 +984,77 @@ int cubo_ptycho_plan_create(cubo_ptycho_context *ctx, const cubo_ptycho_problem 
     if (status == CUBO_PTYCHO_OK) *out = plan.release();
     return status;
 }
+}  // namespace
+
+extern "C" {
+
+int cubo_ptycho_plan_create(cubo_ptycho_context *ctx, const cubo_ptycho_problem *pr, const cubo_ptycho_params *pp,
+                            cubo_ptycho_plan **out) {
+    return create_plan(ctx, pr, pp, nullptr, out);
+}
+
+void cubo_ptycho_mixed_params_default(cubo_ptycho_mixed_params *m) {
+    if (!m) return;
+    m->states = 1;
+    m->orthogonalize_probes = 1;
+    m->zero_pixel_error = CUBO_PTYCHO_ZERO_PIXEL_REFERENCE;
+}
+
+int cubo_ptycho_mixed_plan_create(cubo_ptycho_context *ctx, const cubo_ptycho_problem *pr,
+                                  const cubo_ptycho_params *pp, const cubo_ptycho_mixed_params *mixed,
+                                  cubo_ptycho_plan **out) {
+    if (!mixed) return CUBO_PTYCHO_INVALID_INPUT;
+    return create_plan(ctx, pr, pp, mixed, out);
+}
+
+int cubo_ptycho_orthogonalize(cubo_ptycho_context *ctx, int states, int rows, int columns, double *re, double *im) {
+    return run_guarded(ctx, [&] {  // MixedstatePtychography.orthogonalize (PtychographyEngines.swift:265-269)
+        if (!re || !im) fail(CUBO_PTYCHO_INVALID_INPUT, "null probes");
+        if (!(states >= 1 && states <= kMaxStates && rows > 1 && columns > 1 && (long long)rows * columns <= (1 << 26)))
+            fail(CUBO_PTYCHO_INVALID_INPUT, "shape");
+        const size_t n = (size_t)rows * columns, total = (size_t)states * n;
+        std::vector<double2> v(total);
+        for (size_t k = 0; k < total; k++) {
+            if (!std::isfinite(re[k]) || !std::isfinite(im[k])) fail(CUBO_PTYCHO_INVALID_INPUT, "probe not finite");
+            v[k] = make_double2(re[k], im[k]);
+        }
+        if (states == 1) return;
+        cudaStream_t s = ctx->stream;
+        DeviceBuffer probes, gram, mixing, scratch;
+        upload(probes, v, s);
+        check(gram.alloc((size_t)states * states * sizeof(double2)), "cudaMalloc");
+        check(mixing.alloc((size_t)states * states * sizeof(double2)), "cudaMalloc");
+        check(scratch.alloc(total * sizeof(double2)), "cudaMalloc");
+        check(launch_orthogonalize(probes.as<double2>(), states, (int)n, gram.as<double2>(), mixing.as<double2>(),
+                                   scratch.as<double2>(), s), "orthogonalize");
+        check(cudaMemcpyAsync(v.data(), probes.ptr, total * sizeof(double2), cudaMemcpyDeviceToHost, s), "download");
+        check(cudaStreamSynchronize(s), "orthogonalize");
+        for (size_t k = 0; k < total; k++) {
+            re[k] = v[k].x;
+            im[k] = v[k].y;
+        }
+    });
+}
+
+int cubo_ptycho_mixed_reconstruct(cubo_ptycho_context *ctx, const cubo_ptycho_problem *pr,
+                                  const cubo_ptycho_params *pp, const cubo_ptycho_mixed_params *mixed, double *ore,
+                                  double *oim, double *pre, double *pim, double *errors) {
+    if (!ctx) return CUBO_PTYCHO_INVALID_INPUT;
+    if (!mixed || !ore || !oim || !pre || !pim || (pp && pp->iterations > 0 && !errors)) {
+        ctx->last_error = "null input or output";
+        return CUBO_PTYCHO_INVALID_INPUT;
+    }
+    cubo_ptycho_plan *plan = nullptr;
+    int status = create_plan(ctx, pr, pp, mixed, &plan);
+    if (status != CUBO_PTYCHO_OK) return status;
+    status = cubo_ptycho_plan_set_state(plan, ore, oim, pre, pim);
+    if (status == CUBO_PTYCHO_OK) status = cubo_ptycho_plan_iterate(plan, pp->iterations, errors);
+    if (status == CUBO_PTYCHO_OK) status = cubo_ptycho_plan_get_state(plan, ore, oim, pre, pim);
+    const std::string message = ctx->last_error;
+    cubo_ptycho_plan_destroy(plan);
+    ctx->last_error = message;
+    return status;
+}
 
 int cubo_ptycho_plan_destroy(cubo_ptycho_plan *plan) {
     if (!plan) return CUBO_PTYCHO_OK;
@@ -920,13 +1071,15 @@ int cubo_ptycho_plan_set_state(cubo_ptycho_plan *p, const double *ore, const dou
         if (!ore || !oim || !pre || !pim) fail(CUBO_PTYCHO_INVALID_INPUT, "null state");
         for (long long j = 0; j < p->objects; j++)
             if (!std::isfinite(ore[j]) || !std::isfinite(oim[j])) fail(CUBO_PTYCHO_INVALID_INPUT, "object not finite");
-        for (int k = 0; k < p->n; k++)
+        const size_t probe_values = (size_t)p->states * p->n;  // every probe state, [state][row][column]
+        for (size_t k = 0; k < probe_values; k++)
             if (!std::isfinite(pre[k]) || !std::isfinite(pim[k])) fail(CUBO_PTYCHO_INVALID_INPUT, "probe not finite");
         cudaStream_t s = p->ctx->stream;
         p->tape_valid = false;
-        std::vector<double2> probe(p->n);
-        for (int k = 0; k < p->n; k++) probe[k] = make_double2(pre[k], pim[k]);
-        check(cudaMemcpyAsync(p->probe64.ptr, probe.data(), (size_t)p->n * sizeof(double2), cudaMemcpyHostToDevice, s), "upload probe");
+        std::vector<double2> probe(probe_values);
+        for (size_t k = 0; k < probe_values; k++) probe[k] = make_double2(pre[k], pim[k]);
+        check(cudaMemcpyAsync(p->probe64.ptr, probe.data(), probe_values * sizeof(double2), cudaMemcpyHostToDevice, s),
+              "upload probe");
         if (p->fp64) {
             std::vector<double2> o((size_t)p->objects);
             for (long long j = 0; j < p->objects; j++) o[j] = make_double2(ore[j], oim[j]);
@@ -952,8 +1105,10 @@ int cubo_ptycho_plan_get_state(cubo_ptycho_plan *p, double *ore, double *oim, do
     if (!p) return CUBO_PTYCHO_INVALID_INPUT;
     return run_guarded(p->ctx, [&] {
         cudaStream_t s = p->ctx->stream;
-        std::vector<double2> probe(p->n);
-        check(cudaMemcpyAsync(probe.data(), p->probe64.ptr, (size_t)p->n * sizeof(double2), cudaMemcpyDeviceToHost, s), "download probe");
+        const size_t probe_values = (size_t)p->states * p->n;
+        std::vector<double2> probe(probe_values);
+        check(cudaMemcpyAsync(probe.data(), p->probe64.ptr, probe_values * sizeof(double2), cudaMemcpyDeviceToHost, s),
+              "download probe");
         if (p->fp64) {
             std::vector<double2> o((size_t)p->objects);
             check(cudaMemcpyAsync(o.data(), p->object.ptr, o.size() * sizeof(double2), cudaMemcpyDeviceToHost, s), "download object");
@@ -965,7 +1120,7 @@ int cubo_ptycho_plan_get_state(cubo_ptycho_plan *p, double *ore, double *oim, do
             check(cudaStreamSynchronize(s), "sync");
             for (long long j = 0; j < p->objects; j++) { if (ore) ore[j] = o[j].x; if (oim) oim[j] = o[j].y; }
         }
-        for (int k = 0; k < p->n; k++) { if (pre) pre[k] = probe[k].x; if (pim) pim[k] = probe[k].y; }
+        for (size_t k = 0; k < probe_values; k++) { if (pre) pre[k] = probe[k].x; if (pim) pim[k] = probe[k].y; }
     });
 }
 
@@ -1082,6 +1237,7 @@ extern "C" {
 int cubo_ptycho_plan_forward(cubo_ptycho_plan *p, double *loss) {
     if (!p) return CUBO_PTYCHO_INVALID_INPUT;
     return run_guarded(p->ctx, [&] {
+        if (p->states > 1) fail(CUBO_PTYCHO_UNSUPPORTED, "the adjoint pair is single-slice only");
         if (p->fp64) enqueue_forward<double>(p);
         else enqueue_forward<float>(p);
         p->tape_valid = true;
@@ -1097,6 +1253,7 @@ int cubo_ptycho_plan_backward(cubo_ptycho_plan *p, int recompute, double *loss, 
                               double *gpre, double *gpim) {
     if (!p) return CUBO_PTYCHO_INVALID_INPUT;
     return run_guarded(p->ctx, [&] {
+        if (p->states > 1) fail(CUBO_PTYCHO_UNSUPPORTED, "the adjoint pair is single-slice only");
         if (recompute || !p->tape_valid) {
             if (p->fp64) enqueue_forward<double>(p);
             else enqueue_forward<float>(p);

@@ -294,6 +294,89 @@ class SingleslicePtychography:
                       errors[: int(iterations)].copy(), pos)
 
 
+@dataclass
+class MixedstateResult:
+    """``MixedstatePtychography.Result`` (``PtychographyEngines.swift:126-134``)."""
+    object: np.ndarray
+    probes: np.ndarray  # (states, rows, columns)
+    errors: np.ndarray
+
+
+class MixedstatePtychography:
+    """``MixedstatePtychography`` (``PtychographyEngines.swift:121-298``) on the GPU, FP64: several incoherent probe
+    states on one object; see ``cubo_ptycho_mixed_reconstruct`` in ``include/cubo_ptycho.h``."""
+
+    Result = MixedstateResult
+
+    @staticmethod
+    def reconstruct(amplitudes, positions, object, probes, iterations: int = 8, step_size: float = 0.5,
+                    normalization_minimum: float = 1.0, fix_probe: bool = False, pure_phase_object: bool = False,
+                    fix_probe_center_of_mass: bool = False, constrain_probe_amplitude: bool = False,
+                    probe_amplitude_relative_radius: float = 0.5, probe_amplitude_relative_width: float = 0.05,
+                    orthogonalize_probes: bool = True, fix_probe_aperture: bool = False, probe_support_mask=None,
+                    error_normalization="suppliedAmplitudeEnergy", zero_far_field_pixel_error: str = "reference",
+                    device: int = 0) -> MixedstateResult:
+        """``probes`` is ``(states, rows, columns)`` complex (``PtychographyStack``); ``zero_far_field_pixel_error``
+        is ``"reference"`` (an infinite error term, py4DSTEM) or ``"finite"``."""
+        obj = np.asarray(object)
+        prb = np.asarray(probes)
+        if obj.ndim != 2 or prb.ndim != 3:
+            raise PtychographyError("object must be 2-D and probes (states, rows, columns)")
+        if zero_far_field_pixel_error not in ("reference", "finite"):
+            raise PtychographyError(f"zero_far_field_pixel_error {zero_far_field_pixel_error!r}")
+        ctx = context(device)
+        inp = _Inputs(amplitudes, positions, obj.shape, prb.shape[1:], iterations, step_size, normalization_minimum,
+                      fix_probe, pure_phase_object, True, fix_probe_center_of_mass, constrain_probe_amplitude,
+                      probe_amplitude_relative_radius, probe_amplitude_relative_width, fix_probe_aperture,
+                      probe_support_mask, error_normalization, None, "fp64")
+        mixed = L.MixedParams()
+        ctx.lib.cubo_ptycho_mixed_params_default(C.byref(mixed))
+        mixed.states = int(prb.shape[0])
+        mixed.orthogonalize_probes = int(bool(orthogonalize_probes))
+        mixed.zero_pixel_error = L.ZERO_PIXEL_REFERENCE if zero_far_field_pixel_error == "reference" \
+            else L.ZERO_PIXEL_FINITE
+        ore, oim = _split(obj)
+        pre, pim = _split(prb)
+        errors = np.zeros(max(int(iterations), 1))
+        ctx.check(ctx.lib.cubo_ptycho_mixed_reconstruct(ctx.handle, C.byref(inp.problem), C.byref(inp.params),
+                                                        C.byref(mixed), _ptr(ore), _ptr(oim), _ptr(pre), _ptr(pim),
+                                                        _ptr(errors)))
+        return MixedstateResult((ore + 1j * oim).reshape(obj.shape), (pre + 1j * pim).reshape(prb.shape),
+                                errors[: int(iterations)].copy())
+
+    @staticmethod
+    def orthogonalize(probes, device: int = 0) -> np.ndarray:
+        """``MixedstatePtychography.orthogonalize`` on the device: the eigenvectors of the states' Gram matrix, by
+        decreasing intensity (each state's overall phase is free)."""
+        prb = np.asarray(probes)
+        if prb.ndim != 3:
+            raise PtychographyError("probes must be (states, rows, columns)")
+        ctx = context(device)
+        re, im = _split(prb)
+        ctx.check(ctx.lib.cubo_ptycho_orthogonalize(ctx.handle, prb.shape[0], prb.shape[1], prb.shape[2], _ptr(re),
+                                                    _ptr(im)))
+        return (re + 1j * im).reshape(prb.shape)
+
+    @staticmethod
+    def initial_probes(first, count: int, seed: int) -> np.ndarray:
+        """``MixedstatePtychography.initialProbes`` (``PtychographyEngines.swift:270-298``), host-side set-up: state 0 is
+        ``first``; each further state is the previous one times ``exp(-2 pi i ((u - 1/2) f_row + (v - 1/2) f_col))``
+        with u, v drawn from NumPy's legacy ``RandomState(seed)`` (what the reference's generator reproduces)."""
+        if not (0 < count < 4096):
+            raise PtychographyError("count")
+        first = np.asarray(first, np.complex128)
+        rows, columns = first.shape
+        rng = np.random.RandomState(seed)
+        f = lambda n: np.where(np.arange(n) < (n + 1) // 2, np.arange(n), np.arange(n) - n) / n
+        fr, fc = f(rows), f(columns)
+        out = [first]
+        for _ in range(1, count):
+            u, v = rng.rand(), rng.rand()
+            phase = -2 * np.pi * (u - 0.5) * fr[:, None] - 2 * np.pi * (v - 0.5) * fc[None, :]
+            out.append(out[-1] * (np.cos(phase) + 1j * np.sin(phase)))
+        return np.stack(out)
+
+
 class Plan:
     """A device-resident reconstruction (``cubo_ptycho_plan_*``): upload once, iterate, read the state back."""
 

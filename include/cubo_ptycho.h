@@ -150,6 +150,41 @@ CUBO_PTYCHO_API int cubo_ptycho_reconstruct(cubo_ptycho_context *context, const 
                             const cubo_ptycho_params *params, double *object_re, double *object_im, double *probe_re,
                             double *probe_im, double *errors);
 
+/* ---- The mixed-state engine: MixedstatePtychography.reconstruct (PtychographyEngines.swift:121-262).  Several mutually
+ * incoherent probe states share one object; the detector intensity is the sum of the states' far-field intensities.
+ * Runs in the FP64 form (params->form must be CUBO_PTYCHO_FORM_FP64: the reference's engine is Double) with the shared
+ * params: iterations, step_size, normalization_minimum, fix_probe, pure_phase_object, fix_probe_center_of_mass (the
+ * centre of mass of state 0 shifts every state), constrain_probe_amplitude (every state), fix_probe_aperture (state 0),
+ * probe_support_mask (every state), error_normalization; the object threshold |O| <= 1 always applies (no
+ * constrain_object_amplitude switch in this engine); position correction is refused.  Probes are `states` complex
+ * grids, [state][row][column]. */
+enum { CUBO_PTYCHO_ZERO_PIXEL_REFERENCE = 0, CUBO_PTYCHO_ZERO_PIXEL_FINITE = 1 };  /* MixedstateZeroPixelError */
+typedef struct {
+    int states;                /* probe states, 1 to 16 */
+    int orthogonalize_probes;  /* true: after every iteration the states become the eigenvectors of their Gram matrix,
+                                * by decreasing intensity (also with fix_probe, as py4DSTEM) */
+    int zero_pixel_error;      /* a far-field pixel of zero summed intensity adds an infinite error term
+                                * (CUBO_PTYCHO_ZERO_PIXEL_REFERENCE, py4DSTEM) or measured^2 (_FINITE) */
+} cubo_ptycho_mixed_params;
+CUBO_PTYCHO_API void cubo_ptycho_mixed_params_default(cubo_ptycho_mixed_params *mixed);
+/* object_re/_im hold the start and receive Result.object; probes_re/_im (states * rows * columns) hold the starting
+ * states and receive Result.probes; errors receives params->iterations values. */
+CUBO_PTYCHO_API int cubo_ptycho_mixed_reconstruct(cubo_ptycho_context *context, const cubo_ptycho_problem *problem,
+                                                  const cubo_ptycho_params *params,
+                                                  const cubo_ptycho_mixed_params *mixed, double *object_re,
+                                                  double *object_im, double *probes_re, double *probes_im,
+                                                  double *errors);
+/* MixedstatePtychography.orthogonalize (PtychographyEngines.swift:265-269,300-330) on the device, in place: the states
+ * become the eigenvectors of their Gram matrix G[i][j] = sum conj(p_i) p_j, new_i = sum_j V[j][i] p_j, by decreasing
+ * eigenvalue.  Each state's overall phase is an eigenvector convention (free). */
+CUBO_PTYCHO_API int cubo_ptycho_orthogonalize(cubo_ptycho_context *context, int states, int rows, int columns,
+                                              double *re, double *im);
+/* A device-resident mixed-state plan: the cubo_ptycho_plan_* calls then take and return every state (set_state /
+ * get_state probes of states * rows * columns values); forward / backward are single-slice only. */
+CUBO_PTYCHO_API int cubo_ptycho_mixed_plan_create(cubo_ptycho_context *context, const cubo_ptycho_problem *problem,
+                                                  const cubo_ptycho_params *params,
+                                                  const cubo_ptycho_mixed_params *mixed, cubo_ptycho_plan **out);
+
 /* ---- Device-resident plans: the same reconstruction split into its upload, iterations and download, so data stays in
  * HBM across calls (resume = more iterations on the same plan).  No counterpart in the reference, whose arrays are
  * Swift values; reconstruct() is create + set_state + iterate + get_state + destroy. */

@@ -43,8 +43,10 @@ def test_struct_layouts_match_the_header():
 #include <stddef.h>
 #include "cubo_ptycho.h"
 int main(void) {
-  printf("%zu %zu %zu %zu\n", sizeof(cubo_ptycho_problem), sizeof(cubo_ptycho_params),
-         offsetof(cubo_ptycho_params, form), offsetof(cubo_ptycho_params, progress_user));
+  printf("%zu %zu %zu %zu %zu %zu %zu\n", sizeof(cubo_ptycho_problem), sizeof(cubo_ptycho_params),
+         offsetof(cubo_ptycho_params, form), offsetof(cubo_ptycho_params, progress_user),
+         offsetof(cubo_ptycho_params, max_position_total_distance),
+         offsetof(cubo_ptycho_params, position_columns_out), sizeof(cubo_ptycho_mixed_params));
   return 0;
 }
 '''
@@ -57,6 +59,9 @@ int main(void) {
     assert int(out[1]) == C.sizeof(_lib.Params)
     assert int(out[2]) == _lib.Params.form.offset
     assert int(out[3]) == _lib.Params.progress_user.offset
+    assert int(out[4]) == _lib.Params.max_position_total_distance.offset
+    assert int(out[5]) == _lib.Params.position_columns_out.offset
+    assert int(out[6]) == C.sizeof(_lib.MixedParams)
 
 
 def test_context_without_a_device_is_refused_cleanly():

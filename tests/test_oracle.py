@@ -304,3 +304,11 @@ def test_mixedstate_orthogonalization_and_initial_states():
     for first, count, seed, states, draws in gc.mixed_init_cases():
         assert gc.complex_gap(no.initial_probes(first, count, seed), states) < 2e-6
         assert np.array_equal(np.random.RandomState(seed).rand(len(draws)), draws)
+
+
+def test_mixedstate_initial_probes_of_the_package():
+    """``EngineTests.swift:131-149``: the package's host-side ``initial_probes`` (NumPy's RandomState draws) against
+    py4DSTEM's initial states."""
+    import cubokit_b200 as cb
+    for first, count, seed, states, draws in gc.mixed_init_cases():
+        assert gc.complex_gap(cb.MixedstatePtychography.initial_probes(first, count, seed), states) < 2e-6
