@@ -155,12 +155,20 @@ cudaError_t launch_position_exit_waves(const double2 *shifted, ScanTables scan, 
 cudaError_t launch_position_solve(const double2 *far, const float *amplitudes, int first, int m, int n, double *positions,
                                   const double *initial, int count, double step, double limit_update,
                                   double limit_total, int *bad, cudaStream_t s);
+// Scan tables of the positions on the device ([rows | columns]): wrapped ties-to-even centres, class p + 1 for position
+// p (0 for a whole-pixel position) and its fractional shift (for the ramp table).
+cudaError_t launch_scan_tables(const double *positions, int count, int object_rows, int object_columns, int *rr,
+                               int *cc, int *cls, double2 *fractions, cudaStream_t s);
+// starts[t] = sum of counts[0 .. t) for t <= tiles (one CTA, fixed order); *bad gains bit 2 if the total exceeds
+// capacity.
+cudaError_t launch_exclusive_scan(const int *counts, int tiles, int *starts, long long capacity, int *bad,
+                                  cudaStream_t s);
 // Ptychography.swift:398-401: every position shifted so that their mean is the initial mean again.
 cudaError_t launch_position_center(double *positions, int count, double initial_mean_row, double initial_mean_column,
                                    cudaStream_t s);
 cudaError_t launch_tile_lists(const int *rr, const int *cc, int count, int rows, int columns, int object_rows,
                               int object_columns, int tile_w, int tile_h, int tiles_x, int tiles, int *counts,
-                              const int *starts, int *list, cudaStream_t s);
+                              const int *starts, int *list, int capacity, cudaStream_t s);
 // sum A^2 of `count` amplitudes into scratch[amplitude_check_scratch() - 1] (FP64, fixed order); *bad = 1 if any is not
 // finite and non-negative (*bad is not cleared)
 cudaError_t launch_amplitude_check(const float *amplitudes, long long count, double *scratch, int *bad, cudaStream_t s);

@@ -271,7 +271,7 @@ __device__ __forceinline__ bool cyclic_overlap(int start, int length, int t0, in
 __global__ void __launch_bounds__(256) tile_lists_kernel(const int *rr, const int *cc, int count, int rows, int columns,
                                                          int object_rows, int object_columns, int tile_w, int tile_h,
                                                          int tiles_x, int tiles, int *counts, const int *starts,
-                                                         int *list) {
+                                                         int *list, int capacity) {
     const int tile = blockIdx.x * 8 + (threadIdx.x >> 5), lane = threadIdx.x & 31;
     if (tile >= tiles) return;
     const int ty = tile / tiles_x, tx = tile - ty * tiles_x;
@@ -284,7 +284,10 @@ __global__ void __launch_bounds__(256) tile_lists_kernel(const int *rr, const in
         const bool hit = i < count && cyclic_overlap(rr[i] - rows / 2, rows, y0, hy, object_rows) &&
                          cyclic_overlap(cc[i] - columns / 2, columns, x0, hx, object_columns);
         const unsigned ballot = __ballot_sync(0xffffffffu, hit);
-        if (list && hit) list[base + n + __popc(ballot & ((1u << lane) - 1u))] = i;
+        if (list && hit) {
+            const int at = base + n + __popc(ballot & ((1u << lane) - 1u));
+            if (at < capacity) list[at] = i;  // never past the list (a count beyond it is reported by the scan)
+        }
         n += __popc(ballot);
     }
     if (!list && lane == 0) counts[tile] = n;
@@ -587,9 +590,9 @@ int error_reduce_scratch() { return kErrorBlocks; }
 
 cudaError_t launch_tile_lists(const int *rr, const int *cc, int count, int rows, int columns, int object_rows,
                               int object_columns, int tile_w, int tile_h, int tiles_x, int tiles, int *counts,
-                              const int *starts, int *list, cudaStream_t s) {
+                              const int *starts, int *list, int capacity, cudaStream_t s) {
     tile_lists_kernel<<<(tiles + 7) / 8, 256, 0, s>>>(rr, cc, count, rows, columns, object_rows, object_columns, tile_w,
-                                                      tile_h, tiles_x, tiles, counts, starts, list);
+                                                      tile_h, tiles_x, tiles, counts, starts, list, capacity);
     return cudaGetLastError();
 }
 

@@ -106,6 +106,19 @@ __device__ __forceinline__ void small_dft<float, 8>(float2 (&v)[8], const float2
 template <>
 __device__ __forceinline__ void small_dft<double, 8>(double2 (&v)[8], const double2 *, int, bool inv) { dft8<double>(v, inv); }
 
+// Which (line, butterfly) work item b is: consecutive items take consecutive lines when the lines are interleaved
+// (line stride 1: the same element of neighbouring lines is contiguous, so a warp's accesses are too), else
+// consecutive butterflies of one line.  Only the assignment of work to threads changes, not the arithmetic.
+__device__ __forceinline__ void line_item(const LineGeom &g, int per, int b, int &ln, int &j) {
+    if (g.line == 1) {
+        j = b / g.nlines;
+        ln = b - j * g.nlines;
+    } else {
+        ln = b / per;
+        j = b - ln * per;
+    }
+}
+
 // One Stockham stage of radix R over every line of `g`, in place through registers.  All NT threads must call it.
 template <typename T, int R, int NT, int ITER>
 __device__ __forceinline__ void stockham_stage(C2<T> *D, const LineGeom &g, int Ns, const C2<T> *tw, bool inv) {
@@ -117,7 +130,8 @@ __device__ __forceinline__ void stockham_stage(C2<T> *D, const LineGeom &g, int 
     for (int i = 0; i < ITER; i++) {
         const int b = threadIdx.x + i * NT;
         if (b < total) {
-            const int ln = b / per, j = b - ln * per;
+            int ln, j;
+            line_item(g, per, b, ln, j);
             const C2<T> *x = D + ln * g.line;
 #pragma unroll
             for (int r = 0; r < R; r++) v[i][r] = x[(j + r * per) * g.elem];
@@ -138,7 +152,8 @@ __device__ __forceinline__ void stockham_stage(C2<T> *D, const LineGeom &g, int 
     for (int i = 0; i < ITER; i++) {
         const int b = threadIdx.x + i * NT;
         if (b < total) {
-            const int ln = b / per, j = b - ln * per;
+            int ln, j;
+            line_item(g, per, b, ln, j);
             C2<T> *y = D + ln * g.line;
             const int base = (j / Ns) * Ns * R + (j % Ns);
 #pragma unroll
@@ -157,7 +172,8 @@ __device__ __forceinline__ void direct_lines(C2<T> *D, const LineGeom &g, const 
     for (int i = 0; i < ITER; i++) {
         const int b = threadIdx.x + i * NT;
         if (b < total) {
-            const int ln = b / g.L, k = b - ln * g.L;
+            int ln, k;
+            line_item(g, g.L, b, ln, k);
             const C2<T> *x = D + ln * g.line;
             C2<T> acc = mk<T>(0, 0);
             int idx = 0;  // (m k) mod L
@@ -176,7 +192,8 @@ __device__ __forceinline__ void direct_lines(C2<T> *D, const LineGeom &g, const 
     for (int i = 0; i < ITER; i++) {
         const int b = threadIdx.x + i * NT;
         if (b < total) {
-            const int ln = b / g.L, k = b - ln * g.L;
+            int ln, k;
+            line_item(g, g.L, b, ln, k);
             D[ln * g.line + k * g.elem] = v[i];
         }
     }
@@ -203,6 +220,20 @@ __device__ __noinline__ void line_fft(C2<T> *D, const LineGeom &g, const Radices
         }
         Ns *= R;
     }
+}
+
+// The same transform with the radix plan fixed at compile time (R1, R2 = 0: no stage): no run-time dispatch, so the
+// compiler keeps each stage's values in registers.  The stages and their arithmetic are line_fft's for that plan.
+template <typename T, int NT, int MAXN, int R0, int R1, int R2>
+__device__ __forceinline__ void line_fft_fixed(C2<T> *D, const LineGeom &g, const C2<T> *tw, bool inv) {
+    int Ns = 1;
+    stockham_stage<T, R0, NT, (MAXN + R0 * NT - 1) / (R0 * NT)>(D, g, Ns, tw, inv);
+    Ns *= R0;
+    if constexpr (R1 > 0) {
+        stockham_stage<T, R1, NT, (MAXN + R1 * NT - 1) / (R1 * NT)>(D, g, Ns, tw, inv);
+        Ns *= R1;
+    }
+    if constexpr (R2 > 0) stockham_stage<T, R2, NT, (MAXN + R2 * NT - 1) / (R2 * NT)>(D, g, Ns, tw, inv);
 }
 
 // 2-D transform of a rows x columns field held row-major in shared memory: rows, then columns.

@@ -162,6 +162,8 @@ struct cubo_ptycho_plan {
     DeviceBuffer c_planes, fault;
     DeviceBuffer positions64, initial64, object_before, far64, position_bad, fractions64;
     DeviceBuffer gram64, mixing64, ortho64;
+    DeviceBuffer tile_counts;          // position correction: candidate counts per tile, rebuilt on the device
+    long long tile_capacity = 0;       // entries the candidate list holds
 
     ~cubo_ptycho_plan() {
         for (auto &t : pending) { event_pool.push_back(t.a); event_pool.push_back(t.b); }
@@ -309,6 +311,11 @@ void build_scan(cubo_ptycho_plan *p, const double *rows_in, const double *column
         const double dr = r - rn, dc = c - cn;
         rr[i] = (int)wrap_ll((long long)rn, p->OR);
         cc[i] = (int)wrap_ll((long long)cn, p->OC);
+        if (p->correct_positions) {  // positions move every iteration: one class each, as the device rebuilds them
+            fractions.push_back({dr, dc});
+            cls[i] = dr == 0 && dc == 0 ? 0 : i + 1;
+            continue;
+        }
         if (dr == 0 && dc == 0) { cls[i] = 0; continue; }
         uint64_t kr, kc;
         std::memcpy(&kr, &dr, 8);
@@ -340,7 +347,7 @@ void build_scan(cubo_ptycho_plan *p, const double *rows_in, const double *column
         if (p->tile_start.bytes < (size_t)(p->tiles + 1) * sizeof(int))
             check(p->tile_start.alloc((size_t)(p->tiles + 1) * sizeof(int)), "cudaMalloc");
         check(launch_tile_lists(p->rr.as<int>(), p->cc.as<int>(), P, R, C, p->OR, p->OC, p->tile_w, p->tile_h, p->tiles_x,
-                                p->tiles, p->tile_start.as<int>(), nullptr, nullptr, s), "count candidates");
+                                p->tiles, p->tile_start.as<int>(), nullptr, nullptr, 0, s), "count candidates");
         std::vector<int> counts(p->tiles + 1, 0);
         check(cudaMemcpyAsync(counts.data(), p->tile_start.ptr, (size_t)p->tiles * sizeof(int), cudaMemcpyDeviceToHost, s),
               "download counts");
@@ -354,10 +361,16 @@ void build_scan(cubo_ptycho_plan *p, const double *rows_in, const double *column
         if (total > INT32_MAX) fail(CUBO_PTYCHO_UNSUPPORTED, "object-gather candidate lists exceed 2^31 entries");
         counts[p->tiles] = (int)total;
         upload(p->tile_start, counts, s);
-        if (p->tile_list.bytes < (size_t)std::max<long long>(total, 1) * sizeof(int))
-            check(p->tile_list.alloc((size_t)std::max<long long>(total, 1) * sizeof(int)), "cudaMalloc");
+        // with position correction the lists are rebuilt on the device: room for every window's largest tile count
+        const long long capacity =
+            p->correct_positions ? std::max<long long>(total, (long long)P * (R / p->tile_h + 3) * (C / p->tile_w + 3))
+                                 : total;
+        if (p->tile_list.bytes < (size_t)std::max<long long>(capacity, 1) * sizeof(int))
+            check(p->tile_list.alloc((size_t)std::max<long long>(capacity, 1) * sizeof(int)), "cudaMalloc");
+        p->tile_capacity = std::max<long long>(capacity, 1);
         check(launch_tile_lists(p->rr.as<int>(), p->cc.as<int>(), P, R, C, p->OR, p->OC, p->tile_w, p->tile_h, p->tiles_x,
-                                p->tiles, nullptr, p->tile_start.as<int>(), p->tile_list.as<int>(), s), "list candidates");
+                                p->tiles, nullptr, p->tile_start.as<int>(), p->tile_list.as<int>(),
+                                (int)std::min<long long>(p->tile_capacity, INT32_MAX), s), "list candidates");
     }
     const size_t shifted_bytes = (size_t)p->states * p->classes * n * (p->fp64 ? sizeof(double2) : sizeof(float2));
     if (p->shifted.bytes < shifted_bytes) check(p->shifted.alloc(shifted_bytes), "cudaMalloc");
@@ -787,15 +800,38 @@ std::vector<double> download_positions(cubo_ptycho_plan *p) {
           "download positions");
     check(cudaMemcpyAsync(&bad, p->position_bad.ptr, sizeof(int), cudaMemcpyDeviceToHost, p->ctx->stream), "download");
     check(cudaStreamSynchronize(p->ctx->stream), "position correction");
+    if (bad & 2) fail(CUBO_PTYCHO_CUDA_ERROR, "object-gather candidate lists outgrew their capacity");
     if (bad) fail(CUBO_PTYCHO_INVALID_INPUT, "a corrected position left the representable range");
     return v;
 }
 
-// Scan tables for the positions position correction moved (the next iteration's forward model uses them).
+// Scan tables for the positions position correction moved (the next iteration's forward model uses them), built on the
+// device without waiting: centres and one shift class per position, their phase ramps, the candidate lists (counted,
+// scanned and listed in a fixed order, so the lists equal the host's).
 void refresh_scan(cubo_ptycho_plan *p) {
     if (!p->correct_positions || !p->scan_stale) return;
-    const std::vector<double> v = download_positions(p);
-    build_scan(p, v.data(), v.data() + p->P);
+    cudaStream_t s = p->ctx->stream;
+    const int P = p->P;
+    if (p->tile_counts.bytes < (size_t)p->tiles * sizeof(int))
+        check(p->tile_counts.alloc((size_t)p->tiles * sizeof(int)), "cudaMalloc");
+    timed(p, kPositionCorrection, 5, [&] {
+        cudaError_t e = launch_scan_tables(p->positions64.as<double>(), P, p->OR, p->OC, p->rr.as<int>(),
+                                           p->cc.as<int>(), p->cls.as<int>(), p->fractions64.as<double2>(), s);
+        if (e == cudaSuccess)
+            e = launch_ramp_table(p->fractions64.as<double2>(), P, p->R, p->C, p->ramps_r64.as<double2>(),
+                                  p->ramps_c64.as<double2>(), s);
+        if (e == cudaSuccess)
+            e = launch_tile_lists(p->rr.as<int>(), p->cc.as<int>(), P, p->R, p->C, p->OR, p->OC, p->tile_w, p->tile_h,
+                                  p->tiles_x, p->tiles, p->tile_counts.as<int>(), nullptr, nullptr, 0, s);
+        if (e == cudaSuccess)
+            e = launch_exclusive_scan(p->tile_counts.as<int>(), p->tiles, p->tile_start.as<int>(), p->tile_capacity,
+                                      p->position_bad.as<int>(), s);
+        if (e == cudaSuccess)
+            e = launch_tile_lists(p->rr.as<int>(), p->cc.as<int>(), P, p->R, p->C, p->OR, p->OC, p->tile_w, p->tile_h,
+                                  p->tiles_x, p->tiles, nullptr, p->tile_start.as<int>(), p->tile_list.as<int>(),
+                                  (int)std::min<long long>(p->tile_capacity, INT32_MAX), s);
+        return e;
+    });
     p->scan_stale = false;
 }
 
@@ -954,6 +990,7 @@ int create_plan(cubo_ptycho_context *ctx, const cubo_ptycho_problem *pr, const c
         check(cudaDeviceGetAttribute(&p->sms, cudaDevAttrMultiProcessorCount, ctx->device), "attribute");
         p->kind_ms.assign(kKinds, 0.0);
         p->kind_launches.assign(kKinds, 0);
+        p->correct_positions = pp->has_position_correction != 0;  // before the scan tables: one class per position
         if (p->fp64) build_plan<double>(p, pr);
         else build_plan<float>(p, pr);
         p->positions_given.resize((size_t)2 * p->P);

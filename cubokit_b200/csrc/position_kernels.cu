@@ -151,7 +151,65 @@ __global__ void __launch_bounds__(1024) center_kernel(double *positions, int cou
     }
 }
 
+// Scan tables of moved positions: ties-to-even centres wrapped into the object, one shift class per position (class
+// p + 1 with its fraction for the ramp table; class 0, the unshifted probe, for a whole-pixel position), as the host
+// builds them for a plan with position correction.
+__global__ void __launch_bounds__(256) scan_kernel(const double *positions, int count, int object_rows,
+                                                   int object_columns, int *rr, int *cc, int *cls, double2 *fractions) {
+    const int p = blockIdx.x * 256 + threadIdx.x;
+    if (p >= count) return;
+    const double r = positions[p], c = positions[count + p];
+    const double rn = rint(r), cn = rint(c);  // rint rounds half to even
+    long long wr = (long long)rn % object_rows, wc = (long long)cn % object_columns;
+    rr[p] = (int)(wr < 0 ? wr + object_rows : wr);
+    cc[p] = (int)(wc < 0 ? wc + object_columns : wc);
+    const double dr = r - rn, dc = c - cn;
+    cls[p] = dr == 0.0 && dc == 0.0 ? 0 : p + 1;  // class 0: the probe itself, as without position correction
+    fractions[p] = make_double2(dr, dc);
+}
+
+// Exclusive prefix sums of counts[0 .. tiles) into starts (starts[tiles] = the total), one CTA in a fixed order;
+// *bad gains bit 2 when the total exceeds `capacity` (the starts are then clamped to it).
+__global__ void __launch_bounds__(1024) exclusive_scan_kernel(const int *counts, int tiles, int *starts,
+                                                              long long capacity, int *bad) {
+    __shared__ long long part[1024];
+    const int per = (tiles + 1023) / 1024, begin = threadIdx.x * per, end = min(tiles, begin + per);
+    long long s = 0;
+    for (int t = begin; t < end; t++) s += counts[t];
+    part[threadIdx.x] = s;
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        long long run = 0;
+        for (int i = 0; i < 1024; i++) {
+            const long long v = part[i];
+            part[i] = run;
+            run += v;
+        }
+        starts[tiles] = (int)(run > capacity ? capacity : run);
+        if (run > capacity) *bad |= 2;
+    }
+    __syncthreads();
+    long long run = part[threadIdx.x];
+    for (int t = begin; t < end; t++) {
+        starts[t] = (int)(run > capacity ? capacity : run);
+        run += counts[t];
+    }
+}
+
 }  // namespace
+
+cudaError_t launch_scan_tables(const double *positions, int count, int object_rows, int object_columns, int *rr,
+                               int *cc, int *cls, double2 *fractions, cudaStream_t s) {
+    scan_kernel<<<(count + 255) / 256, 256, 0, s>>>(positions, count, object_rows, object_columns, rr, cc, cls,
+                                                    fractions);
+    return cudaGetLastError();
+}
+
+cudaError_t launch_exclusive_scan(const int *counts, int tiles, int *starts, long long capacity, int *bad,
+                                  cudaStream_t s) {
+    exclusive_scan_kernel<<<1, 1024, 0, s>>>(counts, tiles, starts, capacity, bad);
+    return cudaGetLastError();
+}
 
 cudaError_t launch_position_exit_waves(const double2 *shifted, ScanTables scan, const double2 *before,
                                        const double2 *after, int first, int m, int rows, int columns, int object_rows,

@@ -15,6 +15,8 @@ constexpr int kLineThreads = 256;
 constexpr int kLineMaxN = 4096;  // elements of the lines one CTA holds (64 KB of complex128)
 
 // Rows (columns == false) or columns of `batch` rows x columns fields, lines_per_block lines per CTA.
+// R0 = 0: the plan `rad` at run time; else the compile-time plan R0 x R1 x R2 (it must equal `rad`).
+template <int R0, int R1, int R2>
 __global__ void __launch_bounds__(kLineThreads) fft_lines_kernel(double2 *data, int rows, int columns, int batch,
                                                                  bool columns_pass, int lines_per_block, Radices rad,
                                                                  const double2 *tw_global, bool inv) {
@@ -30,24 +32,47 @@ __global__ void __launch_bounds__(kLineThreads) fft_lines_kernel(double2 *data, 
     // line l: rows pass -> field l / rows, row l % rows, stride 1, one line after the other in shared memory;
     // columns pass -> field l / columns, column l % columns, stride C, staged as rows of the nl columns (element e of
     // line j at e * nl + j) so that consecutive threads read consecutive columns of one row
+    // the tile comes in with 16-byte asynchronous copies (all of a thread's copies in flight at once)
+    const uint32_t d0 = (uint32_t)__cvta_generic_to_shared(D);
+    auto copy_in = [&](int i, long long src) {
+        asm volatile("cp.async.cg.shared.global [%0], [%1], 16;" ::"r"(d0 + 16u * (uint32_t)i), "l"(data + src)
+                     : "memory");
+    };
     if (columns_pass) {
-        for (int i = threadIdx.x; i < nl * L; i += kLineThreads) {
-            const int j = i % nl, e = i / nl, l = first + j;
-            D[i] = data[(long long)(l / columns) * n + (long long)e * columns + (l % columns)];
+        if (columns % nl == 0 && kLineThreads % nl == 0) {
+            // the block's nl columns lie in one field: each thread keeps its column and walks down the rows
+            const long long base = (long long)(first / columns) * n + first % columns;
+            const int j = threadIdx.x % nl, rows_step = kLineThreads / nl;
+            for (int e = threadIdx.x / nl; e < L; e += rows_step) copy_in(e * nl + j, base + (long long)e * columns + j);
+        } else {
+            for (int i = threadIdx.x; i < nl * L; i += kLineThreads) {
+                const int j = i % nl, e = i / nl, l = first + j;
+                copy_in(i, (long long)(l / columns) * n + (long long)e * columns + (l % columns));
+            }
         }
     } else {
-        for (int i = threadIdx.x; i < nl * L; i += kLineThreads) D[i] = data[(long long)(first + i / L) * columns + i % L];
+        const long long base = (long long)first * columns;  // consecutive lines are consecutive rows
+        for (int i = threadIdx.x; i < nl * L; i += kLineThreads) copy_in(i, base + i);
     }
+    asm volatile("cp.async.commit_group;\n\tcp.async.wait_group 0;" ::: "memory");
     __syncthreads();
-    line_fft<double, kLineThreads, kLineMaxN>(D, columns_pass ? LineGeom{L, nl, nl, 1} : LineGeom{L, nl, 1, L}, rad, tw,
-                                              inv);
+    const LineGeom geom = columns_pass ? LineGeom{L, nl, nl, 1} : LineGeom{L, nl, 1, L};
+    if constexpr (R0 == 0) line_fft<double, kLineThreads, kLineMaxN>(D, geom, rad, tw, inv);
+    else line_fft_fixed<double, kLineThreads, kLineMaxN, R0, R1, R2>(D, geom, tw, inv);
     if (columns_pass) {
-        for (int i = threadIdx.x; i < nl * L; i += kLineThreads) {
-            const int j = i % nl, e = i / nl, l = first + j;
-            data[(long long)(l / columns) * n + (long long)e * columns + (l % columns)] = D[i];
+        if (columns % nl == 0 && kLineThreads % nl == 0) {
+            const long long base = (long long)(first / columns) * n + first % columns;
+            const int j = threadIdx.x % nl, rows_step = kLineThreads / nl;
+            for (int e = threadIdx.x / nl; e < L; e += rows_step) data[base + (long long)e * columns + j] = D[e * nl + j];
+        } else {
+            for (int i = threadIdx.x; i < nl * L; i += kLineThreads) {
+                const int j = i % nl, e = i / nl, l = first + j;
+                data[(long long)(l / columns) * n + (long long)e * columns + (l % columns)] = D[i];
+            }
         }
     } else {
-        for (int i = threadIdx.x; i < nl * L; i += kLineThreads) data[(long long)(first + i / L) * columns + i % L] = D[i];
+        const long long base = (long long)first * columns;
+        for (int i = threadIdx.x; i < nl * L; i += kLineThreads) data[base + i] = D[i];
     }
 }
 
@@ -236,9 +261,23 @@ cudaError_t launch_fft2_f64(const Fft2Plan64 &p, double2 *data, int batch, bool 
         const int lines = batch * (cols ? p.columns : p.rows);
         const int lpb = kLineMaxN / L;
         const size_t smem = ((size_t)lpb * L + L) * sizeof(double2);
-        fft_lines_kernel<<<(lines + lpb - 1) / lpb, kLineThreads, smem, s>>>(
-            data, p.rows, p.columns, batch, cols, lpb, cols ? p.rad_rows : p.rad_columns,
-            cols ? p.tw_rows : p.tw_columns, inverse);
+        const Radices &rad = cols ? p.rad_rows : p.rad_columns;
+        auto plan_is = [&](int a, int b, int c) {
+            const int want[3] = {a, b, c};
+            const int count = c ? 3 : (b ? 2 : 1);
+            if (rad.count != count) return false;
+            for (int i = 0; i < count; i++)
+                if (rad.r[i] != want[i]) return false;
+            return true;
+        };
+        // compile-time plans of the usual line lengths (128 = 8 x 8 x 2, 64 = 8 x 8, 256 = 8 x 8 x 4, 32 = 8 x 4)
+        auto kernel = plan_is(8, 8, 2) ? fft_lines_kernel<8, 8, 2>
+                      : plan_is(8, 8, 0) ? fft_lines_kernel<8, 8, 0>
+                      : plan_is(8, 8, 4) ? fft_lines_kernel<8, 8, 4>
+                      : plan_is(8, 4, 0) ? fft_lines_kernel<8, 4, 0>
+                                         : fft_lines_kernel<0, 0, 0>;
+        kernel<<<(lines + lpb - 1) / lpb, kLineThreads, smem, s>>>(data, p.rows, p.columns, batch, cols, lpb, rad,
+                                                                   cols ? p.tw_rows : p.tw_columns, inverse);
         const cudaError_t e = cudaGetLastError();
         if (e != cudaSuccess) return e;
     }
@@ -249,8 +288,13 @@ bool line_fft_supported(int rows, int columns) { return rows <= kLineMaxN && col
 
 // The line-FFT kernel's shared-memory limit, once per device (outside any stream capture).
 cudaError_t configure_fft_lines() {
-    return cudaFuncSetAttribute(fft_lines_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                (int)((kLineMaxN + kLineMaxN) * sizeof(double2)));
+    const int bytes = (int)((kLineMaxN + kLineMaxN) * sizeof(double2));
+    for (auto f : {fft_lines_kernel<0, 0, 0>, fft_lines_kernel<8, 8, 2>, fft_lines_kernel<8, 8, 0>,
+                   fft_lines_kernel<8, 8, 4>, fft_lines_kernel<8, 4, 0>}) {
+        const cudaError_t e = cudaFuncSetAttribute(f, cudaFuncAttributeMaxDynamicSharedMemorySize, bytes);
+        if (e != cudaSuccess) return e;
+    }
+    return cudaSuccess;
 }
 
 cudaError_t launch_scale_f64(double2 *data, int count, double scale, cudaStream_t s) {

@@ -381,7 +381,15 @@ class Plan:
     """A device-resident reconstruction (``cubo_ptycho_plan_*``): upload once, iterate, read the state back."""
 
     def __init__(self, amplitudes, positions, object_shape, probe_shape, ctx: Optional[Context] = None, **kwargs):
+        """``mixed_states=S`` makes a mixed-state plan (``cubo_ptycho_mixed_plan_create``, FP64; with
+        ``orthogonalize_probes`` and ``zero_far_field_pixel_error``): its state holds S probes."""
         self.ctx = ctx or context(kwargs.pop("device", 0))
+        states = kwargs.pop("mixed_states", None)
+        orthogonalize_probes = kwargs.pop("orthogonalize_probes", True)
+        zero_error = kwargs.pop("zero_far_field_pixel_error", "reference")
+        if states is not None:
+            kwargs["precision"] = "fp64"
+            kwargs.setdefault("constrain_object_amplitude", True)
         defaults = dict(iterations=0, step_size=0.5, normalization_minimum=1.0, fix_probe=False,
                         pure_phase_object=False, constrain_object_amplitude=True, fix_probe_center_of_mass=False,
                         constrain_probe_amplitude=False, probe_amplitude_relative_radius=0.5,
@@ -391,10 +399,20 @@ class Plan:
         defaults.update(kwargs)
         self.inputs = _Inputs(amplitudes, positions, tuple(object_shape), tuple(probe_shape), **defaults)
         self.object_shape = tuple(object_shape)
-        self.probe_shape = tuple(probe_shape)
+        self.probe_shape = tuple(probe_shape) if states is None else (int(states),) + tuple(probe_shape)
         h = C.c_void_p()
-        self.ctx.check(self.ctx.lib.cubo_ptycho_plan_create(self.ctx.handle, C.byref(self.inputs.problem),
-                                                            C.byref(self.inputs.params), C.byref(h)))
+        if states is None:
+            self.ctx.check(self.ctx.lib.cubo_ptycho_plan_create(self.ctx.handle, C.byref(self.inputs.problem),
+                                                                C.byref(self.inputs.params), C.byref(h)))
+        else:
+            mixed = L.MixedParams()
+            self.ctx.lib.cubo_ptycho_mixed_params_default(C.byref(mixed))
+            mixed.states = int(states)
+            mixed.orthogonalize_probes = int(bool(orthogonalize_probes))
+            mixed.zero_pixel_error = L.ZERO_PIXEL_REFERENCE if zero_error == "reference" else L.ZERO_PIXEL_FINITE
+            self.ctx.check(self.ctx.lib.cubo_ptycho_mixed_plan_create(self.ctx.handle, C.byref(self.inputs.problem),
+                                                                      C.byref(self.inputs.params), C.byref(mixed),
+                                                                      C.byref(h)))
         self.handle = h
 
     def set_state(self, obj, probe):
