@@ -14,6 +14,7 @@ It restates, in vectorised NumPy (``np.fft`` is pocketfft in double, NumPy's fft
     bilinear and periodic cubic-spline pattern shifts, square-root amplitudes and mean intensities
   * ``Sources/CuboPtycho/PtychographyEngines.swift:121-267,270-298``  ``MixedstatePtychography`` (reconstruct,
     orthogonalize, initialProbes: NumPy's own legacy ``RandomState`` draws)
+  * ``Sources/CuboPtycho/PtychographyEngines.swift:427-589``  ``MultislicePtychography`` (propagators, reconstruct)
   * ``Sources/CuboPtycho/Ptychography.swift:53-85,260-264,371-377,398-401,411-472``  position correction
     (``PtychographyPositionCorrection``: the per-position 2 x 2 least-squares step, its limits, the centre-of-mass
     constraint)
@@ -510,6 +511,119 @@ def mixedstate_reconstruct(amplitudes, positions, obj, probes, iterations=8, ste
             p = orthogonalize(p)
         errors.append(error / divisor)
     return o.reshape(object_rows, object_columns), p, np.asarray(errors)
+
+
+# ---------------------------------------------------------------- multislice (PtychographyEngines.swift)
+
+def propagators(rows, columns, row_sampling, column_sampling, wavelength, slice_thicknesses):
+    """``MultislicePtychography.propagators`` (``PtychographyEngines.swift:427-442``): exp(-i pi lambda dz (kr^2 + kc^2))
+    with k = frequency / sampling, one (rows, columns) grid per thickness."""
+    ok = (rows > 1 and columns > 1 and math.isfinite(row_sampling) and row_sampling > 0
+          and math.isfinite(column_sampling) and column_sampling > 0 and math.isfinite(wavelength) and wavelength > 0
+          and len(slice_thicknesses) > 0 and all(math.isfinite(d) for d in slice_thicknesses))
+    if not ok:
+        raise PtychographyError("propagators")
+    fr, fc = fftfreq_grid(rows, columns)
+    k2 = (fr / row_sampling)[:, None] ** 2 + (fc / column_sampling)[None, :] ** 2
+    out = []
+    for dz in slice_thicknesses:
+        phase = -np.pi * wavelength * dz * k2
+        out.append(np.cos(phase) + 1j * np.sin(phase))
+    return np.stack(out)
+
+
+def multislice_reconstruct(amplitudes, positions, obj, probe, slice_thicknesses, wavelength, row_sampling,
+                           column_sampling, iterations=8, step_size=0.5, normalization_minimum=1.0, fix_probe=False,
+                           pure_phase_object=False, identical_slices=False, fix_probe_center_of_mass=False,
+                           constrain_probe_amplitude=False, probe_amplitude_relative_radius=0.5,
+                           probe_amplitude_relative_width=0.05, fix_probe_aperture=False, probe_support_mask=None,
+                           error_normalization="suppliedAmplitudeEnergy", mean_intensity=None):
+    """``MultislicePtychography.reconstruct`` (``PtychographyEngines.swift:458-588``): ``obj`` (L, OR, OC) slices,
+    entrance first; ``slice_thicknesses`` L - 1 values (A).  Returns ``(slices, probe, errors)``."""
+    obj = np.array(obj, np.complex128)
+    probe = np.array(probe, np.complex128)
+    slices, object_rows, object_columns = obj.shape
+    rows, columns = probe.shape
+    n = rows * columns
+    positions = np.asarray(positions, np.float64).reshape(-1, 2)
+    count = len(positions)
+    validate(amplitudes, positions, (object_rows, object_columns), probe.shape, iterations, step_size,
+             normalization_minimum, probe_amplitude_relative_radius, probe_amplitude_relative_width,
+             probe_support_mask)
+    if len(slice_thicknesses) != slices - 1:
+        raise PtychographyError("slice thicknesses")
+    amp = np.asarray(amplitudes, np.float64).reshape(count, n)
+    divisor = error_divisor(amp, count, error_normalization, mean_intensity)
+    props = propagators(rows, columns, row_sampling, column_sampling, wavelength,
+                        list(slice_thicknesses) if len(slice_thicknesses) else [0.0])
+    initial_aperture = np.abs(np.fft.fft2(probe)) if fix_probe_aperture else None
+    rr = round_half_even(positions[:, 0])
+    cc = round_half_even(positions[:, 1])
+    dr, dc = positions[:, 0] - rr, positions[:, 1] - cc
+    idx = patch_indices(rows, columns, object_rows, object_columns, rr.astype(np.int64), cc.astype(np.int64))
+    mask = None if probe_support_mask is None else np.asarray(probe_support_mask, bool).reshape(rows, columns)
+    m = normalization_minimum
+    o = obj.reshape(slices, -1).copy()
+    p = probe.copy()
+    errors = []
+
+    def norm(local, maximum):
+        return 1 / np.sqrt(1e-16 + ((1 - m) * local) ** 2 + (m * maximum) ** 2)
+
+    def propagate(x, s, conjugate):
+        f = np.fft.fft2(x.reshape(count, rows, columns))
+        f = f * (np.conj(props[s]) if conjugate else props[s])[None]
+        return np.fft.ifft2(f).reshape(count, n)
+
+    for it in range(iterations):
+        current = shifted_probes(np.fft.fft2(p), dr, dc).reshape(count, n)
+        waves, patches = [], []
+        for s in range(slices):                                        # :503-515
+            waves.append(current)
+            patch = o[s][idx]
+            patches.append(patch)
+            exit_wave = current * patch
+            if s + 1 < slices:
+                current = propagate(exit_wave, s, False)
+        f = np.fft.fft2(exit_wave.reshape(count, rows, columns)).reshape(count, n)
+        magnitude = np.abs(f)
+        error = float(np.sum((amp - magnitude) ** 2))
+        angle = np.arctan2(f.imag, f.real)
+        chi = np.fft.ifft2((amp * np.cos(angle) - f.real + 1j * (amp * np.sin(angle) - f.imag))
+                           .reshape(count, rows, columns)).reshape(count, n)
+        grads, weights = [None] * slices, [None] * slices
+        for s in range(slices - 1, -1, -1):                            # :526-545
+            g = np.zeros(object_rows * object_columns, np.complex128)
+            w = np.zeros(object_rows * object_columns)
+            np.add.at(g, idx.ravel(), (np.conj(waves[s]) * chi).ravel())
+            np.add.at(w, idx.ravel(), (waves[s].real ** 2 + waves[s].imag ** 2).ravel())
+            grads[s], weights[s] = g, w
+            chi = chi * np.conj(patches[s])
+            if s > 0:
+                chi = propagate(chi, s - 1, True)
+        grad_p = np.sum(chi, axis=0).reshape(rows, columns)
+        on = np.sum(patches[0].real ** 2 + patches[0].imag ** 2, axis=0).reshape(rows, columns)
+        for s in range(slices):
+            o[s] = o[s] + step_size * norm(weights[s], weights[s].max()) * grads[s]
+        if not fix_probe:
+            p = p + step_size * norm(on, on.max()) * grad_p
+        if identical_slices:
+            o[:] = np.sum(o, axis=0) / slices
+        a = np.abs(o)
+        target = np.ones_like(a) if pure_phase_object else np.minimum(a, 1.0)
+        ph = np.arctan2(o.imag, o.real)
+        o = target * np.cos(ph) + 1j * target * np.sin(ph)
+        if not fix_probe:
+            if fix_probe_center_of_mass:
+                p = center_of_mass_constraint(p)
+            if fix_probe_aperture:
+                p = aperture_constraint(p, initial_aperture)
+            if constrain_probe_amplitude:
+                p = amplitude_constraint(p, probe_amplitude_relative_radius, probe_amplitude_relative_width)
+        if mask is not None:
+            p = np.where(mask, p, 0)
+        errors.append(error / divisor)
+    return o.reshape(slices, object_rows, object_columns), p, np.asarray(errors)
 
 
 def loss_and_gradients(amplitudes, positions, obj, probe):

@@ -18,6 +18,8 @@ Which reference test each group pins (paths inside the CuboKit project):
                   through to the engine's amplitude pin)
   mixed.npz    Tests/CuboPtychoTests/EngineTests.swift:86-188,262-305 (mixed-state engine: five cases, the
                 orthogonalisation, py4DSTEM's initial states, the mixed engine's support / aperture extras)
+  multislice.npz  Tests/CuboPtychoTests/EngineTests.swift:190-255,262-305 (multislice engine: propagators, six
+                  cases, the multislice engine's support / aperture extras)
   positions.npz  Tests/CuboPtychoTests/PositionCorrectionTests.swift:43-110 (position correction: five settings on
                   8 x 8 positions started up to 0.3 px off, four iterations; the exact-data case; tools/ptycho/
                   position_pins.py, py4DSTEM reconstruct(fix_positions=False))
@@ -172,6 +174,45 @@ def mixed(fx):
     return s
 
 
+def multislice(fx):
+    """The multislice part of engines.json: propagators, reconstruction cases and the multislice engine's support /
+    aperture extras."""
+    p = json.loads((fx / "engines.json").read_text())
+    m, x = p["multislice"], p["extras"]
+    s = {}
+    for k in ("rows", "columns", "objectRows", "objectColumns", "rowSampling", "columnSampling", "wavelength"):
+        _scalar(s, k, p[k])
+    s["positions"] = np.asarray(p["positions"], np.float64)
+    s["amplitudes"] = np.asarray(m["amplitudes"], np.float64)
+    _scalar(s, "meanIntensity", m["preprocessing"]["meanIntensity"])
+    s["sliceThicknesses"] = np.asarray(m["sliceThicknesses"], np.float64)
+    _cx(s, "propagators", m["propagators"])
+    _cx(s, "startSlices", m["startSlices"])
+    _cx(s, "startProbe", m["startProbe"])
+    _scalar(s, "cases", len(m["cases"]))
+    for i, c in enumerate(m["cases"]):
+        pre = f"case{i}_"
+        for k in ("name", "slices", "fixProbeCenterOfMass", "constrainProbeAmplitude", "radius", "width", "fixProbe",
+                  "purePhase", "identicalSlices"):
+            _scalar(s, pre + k, c[k])
+        s[pre + "thicknesses"] = np.asarray(c["thicknesses"], np.float64)
+        _cx(s, pre + "object", c["object"])
+        _cx(s, pre + "probe", c["probe"])
+        s[pre + "errors"] = np.asarray(c["errors"], np.float64)
+    s["support"] = np.asarray(x["support"], np.bool_)
+    extras = [c for c in x["cases"] if c["engine"] == "multislice"]
+    _scalar(s, "extras", len(extras))
+    for i, c in enumerate(extras):
+        pre = f"extra{i}_"
+        _scalar(s, pre + "name", c["name"])
+        for k in ("fixProbeCenterOfMass", "fixProbeAperture", "fixProbe", "constrainProbeAmplitude", "radius", "width"):
+            _scalar(s, pre + k, c[k])
+        _cx(s, pre + "object", c["object"])
+        _cx(s, pre + "probe", c["probe"])
+        s[pre + "errors"] = np.asarray(c["errors"], np.float64)
+    return s
+
+
 def options(fx):
     o = json.loads((fx / "options.json").read_text())
     s = {}
@@ -264,7 +305,8 @@ def main():
     root = Path(sys.argv[1]) if len(sys.argv) > 1 else Path("/root/reference")
     fx = root / "Tests/CuboPtychoTests/Fixtures"
     for name, fn in (("ptycho", ptycho), ("odd", odd), ("engines", engines), ("options", options),
-                     ("preprocess", preprocess), ("positions", positions), ("mixed", mixed)):
+                     ("preprocess", preprocess), ("positions", positions), ("mixed", mixed),
+                     ("multislice", multislice)):
         arrays = fn(fx)
         np.savez_compressed(HERE / f"{name}.npz", **arrays)
         print(name, len(arrays), "arrays", (HERE / f"{name}.npz").stat().st_size, "bytes")

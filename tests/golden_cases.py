@@ -292,3 +292,48 @@ def mixed_init_cases():
         count = int(g("count"))
         out.append((first, count, int(g("seed")), _cx(z, f"init{i}_states", (count, R, C)), g("draws")))
     return out
+
+
+def multislice_cases():
+    """``EngineTests.swift:205-228`` (six cases) and ``:262-305`` (the multislice engine's aperture / support extras):
+    three iterations, step 0.35, normalisation minimum 0.7, mean-intensity errors.  Each entry: (name, inputs, expected
+    (slices, probe, errors))."""
+    z = load("multislice")
+    R, C, OR, OC = int(z["rows"]), int(z["columns"]), int(z["objectRows"]), int(z["objectColumns"])
+    start = _cx(z, "startSlices", (3, OR, OC))
+    common = dict(amplitudes=z["amplitudes"].reshape(-1, R, C), positions=z["positions"],
+                  probe=_cx(z, "startProbe", (R, C)), wavelength=float(z["wavelength"]),
+                  row_sampling=float(z["rowSampling"]), column_sampling=float(z["columnSampling"]), iterations=3,
+                  step_size=0.35, normalization_minimum=0.7, error_normalization="meanIntensity",
+                  mean_intensity=float(z["meanIntensity"]))
+    out = []
+    for i in range(int(z["cases"])):
+        g = lambda k: z[f"case{i}_{k}"]
+        L = int(g("slices"))
+        inputs = dict(common, obj=start[:L], slice_thicknesses=list(g("thicknesses")), fix_probe=bool(g("fixProbe")),
+                      pure_phase_object=bool(g("purePhase")), identical_slices=bool(g("identicalSlices")),
+                      fix_probe_center_of_mass=bool(g("fixProbeCenterOfMass")),
+                      constrain_probe_amplitude=bool(g("constrainProbeAmplitude")),
+                      probe_amplitude_relative_radius=float(g("radius")),
+                      probe_amplitude_relative_width=float(g("width")))
+        out.append((str(g("name")), inputs, (_cx(z, f"case{i}_object", (L, OR, OC)), _cx(z, f"case{i}_probe", (R, C)),
+                                             g("errors"))))
+    for i in range(int(z["extras"])):
+        g = lambda k: z[f"extra{i}_{k}"]
+        inputs = dict(common, obj=start[:3], slice_thicknesses=[55.0, 80.0], fix_probe=bool(g("fixProbe")),
+                      fix_probe_center_of_mass=bool(g("fixProbeCenterOfMass")),
+                      constrain_probe_amplitude=bool(g("constrainProbeAmplitude")),
+                      probe_amplitude_relative_radius=float(g("radius")),
+                      probe_amplitude_relative_width=float(g("width")), fix_probe_aperture=bool(g("fixProbeAperture")),
+                      probe_support_mask=z["support"].reshape(R, C))
+        out.append(("extras." + str(g("name")), inputs,
+                    (_cx(z, f"extra{i}_object", (3, OR, OC)), _cx(z, f"extra{i}_probe", (R, C)), g("errors"))))
+    return out
+
+
+def multislice_propagator_case():
+    z = load("multislice")
+    R, C = int(z["rows"]), int(z["columns"])
+    args = dict(rows=R, columns=C, row_sampling=float(z["rowSampling"]), column_sampling=float(z["columnSampling"]),
+                wavelength=float(z["wavelength"]), slice_thicknesses=list(z["sliceThicknesses"]))
+    return args, _cx(z, "propagators", (len(z["sliceThicknesses"]), R, C))

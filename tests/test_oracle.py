@@ -312,3 +312,33 @@ def test_mixedstate_initial_probes_of_the_package():
     import cubokit_b200 as cb
     for first, count, seed, states, draws in gc.mixed_init_cases():
         assert gc.complex_gap(cb.MixedstatePtychography.initial_probes(first, count, seed), states) < 2e-6
+
+
+# ---------------------------------------------------------------------------------------------------- multislice
+
+@pytest.mark.parametrize("case", gc.multislice_cases(), ids=lambda c: c[0])
+def test_multislice_meets_the_pins(case):
+    """``EngineTests.swift:205-228,262-305``: slices, probe and errors within 2e-6."""
+    name, inputs, (obj, probe, errors) = case
+    o, p, e = no.multislice_reconstruct(**inputs)
+    assert max(gc.complex_gap(o, obj), gc.complex_gap(p, probe), gap(e, errors)) < 2e-6
+
+
+def test_multislice_propagators_one_slice_and_refusals():
+    """``EngineTests.swift:192-203,230-255``: the propagator pin (unit modulus), one slice equals the single-slice engine
+    (1e-12), a thickness count other than slices - 1 and non-positive samplings are refused."""
+    args, expected = gc.multislice_propagator_case()
+    props = no.propagators(**args)
+    assert gc.complex_gap(props, expected) < 2e-6
+    assert np.max(np.abs(np.abs(props) - 1)) < 1e-14
+    name, inputs, _ = gc.multislice_cases()[0]
+    one = dict(inputs, obj=inputs["obj"][:1], slice_thicknesses=[], error_normalization="suppliedAmplitudeEnergy")
+    one.pop("mean_intensity")
+    o1, p1, e1 = no.multislice_reconstruct(**one)
+    o2, p2, e2 = no.reconstruct(one["amplitudes"], one["positions"], one["obj"][0], one["probe"], iterations=3,
+                                step_size=0.35, normalization_minimum=0.7)
+    assert max(gc.complex_gap(o1[0], o2), gc.complex_gap(p1, p2), gap(e1, e2)) < 1e-12
+    with pytest.raises(no.PtychographyError):
+        no.multislice_reconstruct(**dict(inputs, slice_thicknesses=[10.0]))
+    with pytest.raises(no.PtychographyError):
+        no.propagators(**dict(args, row_sampling=0.0))
