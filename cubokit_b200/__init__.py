@@ -3,11 +3,12 @@
 The engine is ``libcuboptycho.so`` (CUDA kernels behind the C ABI of ``include/cubo_ptycho.h``); this package is its
 Python binding and the host-side mirror of CuboPtycho's API.
 """
-from .ptycho import (Batch, CancellationError, Context, DeviceError, MixedstatePtychography, Plan,
+from .ptycho import (Batch, CancellationError, Context, DeviceError, MixedstatePtychography,
+                     MultislicePtychography, Plan,
                      PtychographyAmplitudes, PtychographyError,
                      PtychographyPositionCorrection, PtychographyPreparation, PtychographyProbe, Result,
                      SingleslicePtychography, UnsupportedError, context, electron_wavelength)
 
-__all__ = ["Batch", "CancellationError", "Context", "DeviceError", "MixedstatePtychography", "Plan", "PtychographyAmplitudes", "PtychographyError",
+__all__ = ["Batch", "CancellationError", "Context", "DeviceError", "MixedstatePtychography", "MultislicePtychography", "Plan", "PtychographyAmplitudes", "PtychographyError",
            "PtychographyPositionCorrection", "PtychographyPreparation", "PtychographyProbe", "Result", "SingleslicePtychography", "UnsupportedError", "context",
            "electron_wavelength"]

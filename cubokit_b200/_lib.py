@@ -55,6 +55,11 @@ class MixedParams(C.Structure):
 ZERO_PIXEL_REFERENCE, ZERO_PIXEL_FINITE = 0, 1
 
 
+class MultisliceParams(C.Structure):
+    _fields_ = [("slices", C.c_int), ("slice_thicknesses", C.POINTER(C.c_double)), ("wavelength", C.c_double),
+                ("row_sampling", C.c_double), ("column_sampling", C.c_double), ("identical_slices", C.c_int)]
+
+
 # Every symbol the header declares, with its ctypes signature (restype, argtypes).
 _dp = C.POINTER(C.c_double)
 SIGNATURES = {
@@ -74,6 +79,12 @@ SIGNATURES = {
     "cubo_ptycho_mixed_plan_create": (C.c_int, [C.c_void_p, C.POINTER(Problem), C.POINTER(Params),
                                                 C.POINTER(MixedParams), C.POINTER(C.c_void_p)]),
     "cubo_ptycho_orthogonalize": (C.c_int, [C.c_void_p, C.c_int, C.c_int, C.c_int, _dp, _dp]),
+    "cubo_ptycho_propagators": (C.c_int, [C.c_int, C.c_int, C.c_double, C.c_double, C.c_double, C.c_int, _dp, _dp,
+                                          _dp]),
+    "cubo_ptycho_multislice_reconstruct": (C.c_int, [C.c_void_p, C.POINTER(Problem), C.POINTER(Params),
+                                                     C.POINTER(MultisliceParams), _dp, _dp, _dp, _dp, _dp]),
+    "cubo_ptycho_multislice_plan_create": (C.c_int, [C.c_void_p, C.POINTER(Problem), C.POINTER(Params),
+                                                     C.POINTER(MultisliceParams), C.POINTER(C.c_void_p)]),
     "cubo_ptycho_plan_iterate": (C.c_int, [C.c_void_p, C.c_int, _dp]),
     "cubo_ptycho_plan_enqueue": (C.c_int, [C.c_void_p, C.c_int]),
     "cubo_ptycho_plan_errors": (C.c_int, [C.c_void_p, C.c_int, _dp]),

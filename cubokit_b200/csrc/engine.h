@@ -188,6 +188,21 @@ cudaError_t launch_fft2_f64(const Fft2Plan64 &p, double2 *data, int batch, bool 
 cudaError_t launch_position_pass_global(const PositionPassArgs<double> &a, const Fft2Plan64 &fft, int *launches,
                                        cudaStream_t s);
 bool line_fft_supported(int rows, int columns);
+// The projection alone, in place on dpsi of positions first .. first + count - 1 (their far fields): the inverse
+// transform's 1/n folded in, the per-position squared error written.
+cudaError_t launch_project_global(const PositionPassArgs<double> &a, cudaStream_t s);
+
+// multislice_kernels.cu: the multislice engine (MultislicePtychography, PtychographyEngines.swift:458-588), FP64.
+// out[p][k] = in[class][k] x O[patch(p)][k] (conj(O) when conj_object; no object factor when object is null), class =
+// scan.cls[p] when by_class, else p; in and out may be the same buffer.
+cudaError_t launch_patch_multiply(const double2 *in, bool by_class, const double2 *object, bool conj_object,
+                                  ScanTables scan, int first, int m, int rows, int columns, int object_rows,
+                                  int object_columns, double2 *out, cudaStream_t s);
+// data[plane][k] *= scale x prop[k] (or its conjugate) for `planes` planes of n values.
+cudaError_t launch_spectrum_multiply(double2 *data, long long planes, int n, const double2 *prop, bool conj_prop,
+                                     double scale, cudaStream_t s);
+// identicalSlices: every slice becomes the mean of the slices.
+cudaError_t launch_average_slices(double2 *object, int slices, long long plane, cudaStream_t s);
 
 // mixed_kernels.cu: the mixed-state engine (MixedstatePtychography, PtychographyEngines.swift:121-267), FP64.
 constexpr int kMaxStates = 16;

@@ -515,6 +515,12 @@ size_t position_pass_smem(int n, int rows, int columns, bool fp64) {
     return fp64 ? pass_smem<double>(n, rows, columns) : pass_smem<float>(n, rows, columns);
 }
 
+cudaError_t launch_project_global(const PositionPassArgs<double> &a, cudaStream_t s) {
+    if (a.count <= 0) return cudaSuccess;
+    project_global_kernel<kPassThreads><<<a.count, kPassThreads, 0, s>>>(a);
+    return cudaGetLastError();
+}
+
 cudaError_t launch_position_pass_global(const PositionPassArgs<double> &a, const Fft2Plan64 &fft, int *launches,
                                        cudaStream_t s) {
     const int chunk = (int)std::max<long long>(1, (1LL << 28) / a.n);  // at most 4 GiB of exit waves per round

@@ -126,6 +126,9 @@ struct cubo_ptycho_plan {
     bool bf16 = false;      // 128 x 128 split-BF16 tensor-core position pass
     bool global64 = false;  // FP64 position pass through global memory (the plane does not fit shared memory)
     int states = 1;         // probe states (the mixed-state engine; 1 = single slice)
+    int slices = 1;         // object slices (the multislice engine)
+    bool multislice = false;        // the multislice engine (its iteration, even with one slice)
+    bool identical_slices = false;  // multislice: every slice replaced by their mean after each update
     bool orthogonalize = false;     // mixed state: orthogonalise the states after every iteration
     bool zero_pixel_infinite = true; // mixed state: an exactly zero far-field pixel adds an infinite error term
     int sms = 148;
@@ -162,6 +165,7 @@ struct cubo_ptycho_plan {
     DeviceBuffer c_planes, fault;
     DeviceBuffer positions64, initial64, object_before, far64, position_bad, fractions64;
     DeviceBuffer gram64, mixing64, ortho64;
+    DeviceBuffer waves64, props64, ident, slice_max;  // multislice: entering waves, propagators, identity classes
     DeviceBuffer tile_counts;          // position correction: candidate counts per tile, rebuilt on the device
     long long tile_capacity = 0;       // entries the candidate list holds
 
@@ -174,10 +178,10 @@ struct cubo_ptycho_plan {
 namespace {
 
 enum Kind { kPositionPass, kObjectGather, kProbeGather, kProbeReduce, kMaxReduce, kObjectUpdate, kProbeSide,
-            kErrorReduce, kShiftTable, kPositionCorrection, kKinds };
+            kErrorReduce, kShiftTable, kPositionCorrection, kBackPropagation, kKinds };
 const char *kKindNames[kKinds] = {"position_pass", "object_gather", "probe_gather", "probe_reduce", "max_reduce",
                                   "object_update", "probe_update_constraints", "error_reduce", "shift_table",
-                                  "position_correction"};
+                                  "position_correction", "back_propagation"};
 
 cudaEvent_t take_event(cubo_ptycho_plan *p) {
     if (!p->event_pool.empty()) {
@@ -430,10 +434,17 @@ void build_plan(cubo_ptycho_plan *p, const cubo_ptycho_problem *pr) {
         std::swap(p->amplitudes.bytes, permuted.bytes);
     }
     // ---- state and work buffers
-    check(p->object.alloc((size_t)p->objects * sizeof(C2<T>)), "cudaMalloc object");
-    check(p->grad_o.alloc((size_t)p->objects * sizeof(C2<T>)), "cudaMalloc");
-    check(p->weight_o.alloc((size_t)p->objects * sizeof(T)), "cudaMalloc");
-    check(p->tile_max.alloc((size_t)p->tiles * sizeof(double)), "cudaMalloc");
+    check(p->object.alloc((size_t)p->slices * p->objects * sizeof(C2<T>)), "cudaMalloc object");
+    check(p->grad_o.alloc((size_t)p->slices * p->objects * sizeof(C2<T>)), "cudaMalloc");
+    check(p->weight_o.alloc((size_t)p->slices * p->objects * sizeof(T)), "cudaMalloc");
+    check(p->tile_max.alloc((size_t)p->slices * p->tiles * sizeof(double)), "cudaMalloc");
+    if (p->multislice) {
+        check(p->waves64.alloc((size_t)(p->slices - 1) * P * n * sizeof(double2)), "cudaMalloc entering waves");
+        check(p->slice_max.alloc((size_t)p->slices * sizeof(double)), "cudaMalloc");
+        std::vector<int> ident(P);
+        for (int i = 0; i < P; i++) ident[i] = i;
+        upload(p->ident, ident, s);
+    }
     check(p->dpsi.alloc((size_t)p->states * P * n * sizeof(C2<T>)), "cudaMalloc dpsi");
     p->error_count = p->fast ? (long long)P * fast128_partials_per_position()
                              : p->bf16 ? (long long)P * bf16_partials_per_position() : P;
@@ -792,6 +803,114 @@ void enqueue_iteration(cubo_ptycho_plan *p) {
     });
 }
 
+// One multislice iteration (MultislicePtychography.reconstruct, PtychographyEngines.swift:495-585), FP64.  The object
+// holds the slices [slice][row][column]; waves64 the waves entering slices 1 .. L-1 ([slice - 1][position][pixel]; the
+// wave entering slice 0 is the shifted probe, read from the shift table); dpsi the exit wave of the last slice, then
+// its residual chi, then chi carried back through the slices.
+void enqueue_multislice_iteration(cubo_ptycho_plan *p) {
+    cudaStream_t s = p->ctx->stream;
+    const cubo_ptycho_params &pp = p->params;
+    const int n = p->n, P = p->P, L = p->slices;
+    const long long plane = p->objects, planes = (long long)P * n;
+    const double inv_n = 1.0 / n;
+    const ScanTables scan{p->rr.as<int>(), p->cc.as<int>(), p->cls.as<int>()};
+    const ScanTables own{p->rr.as<int>(), p->cc.as<int>(), p->ident.as<int>()};  // class p = position p
+    double2 *obj = p->object.as<double2>(), *chi = p->dpsi.as<double2>(), *waves = p->waves64.as<double2>();
+    const double2 *shifted = p->shifted.as<double2>(), *props = p->props64.as<double2>();
+    const Fft2Plan64 f = fft64(p);
+    enqueue_shift_table<double>(p);
+    // forward (:503-515): exit_s = wave_s x O_s; wave_{s+1} = IFFT(FFT(exit_s) x prop_s / n)
+    timed(p, kPositionPass, 6 * (L - 1) + 1, [&] {
+        cudaError_t e = cudaSuccess;
+        for (int sl = 0; sl < L && e == cudaSuccess; sl++) {
+            const bool last = sl == L - 1;
+            double2 *target = last ? chi : waves + (size_t)sl * planes;
+            if (sl == 0)
+                e = launch_patch_multiply(shifted, true, obj, false, scan, 0, P, p->R, p->C, p->OR, p->OC, target, s);
+            else
+                e = launch_patch_multiply(waves + (size_t)(sl - 1) * planes, false, obj + (size_t)sl * plane, false,
+                                          scan, 0, P, p->R, p->C, p->OR, p->OC, target, s);
+            if (last) break;
+            if (e == cudaSuccess) e = launch_fft2_f64(f, target, P, false, s);
+            if (e == cudaSuccess) e = launch_spectrum_multiply(target, P, n, props + (size_t)sl * n, false, inv_n, s);
+            if (e == cudaSuccess) e = launch_fft2_f64(f, target, P, true, s);
+        }
+        return e;
+    });
+    // detector (:516-524): the projection of the last exit wave's far field, chi its inverse transform
+    PositionPassArgs<double> pa{};
+    pa.rows = p->R; pa.columns = p->C; pa.object_rows = p->OR; pa.object_columns = p->OC; pa.n = n;
+    pa.first = 0; pa.count = P; pa.scan = scan; pa.amplitudes = p->amplitudes.as<float>(); pa.dpsi = chi;
+    pa.error = p->error.as<double>(); pa.inv_n = inv_n;
+    timed(p, kPositionPass, 5, [&] {
+        cudaError_t e = launch_fft2_f64(f, chi, P, false, s);
+        if (e == cudaSuccess) e = launch_project_global(pa, s);
+        if (e == cudaSuccess) e = launch_fft2_f64(f, chi, P, true, s);
+        return e;
+    });
+    // backward (:526-545): slice s's gradient from its entering wave and chi, chi x conj(O_s) carried back one slice;
+    // at slice 0 the probe gradient from conj(O_0) chi
+    ObjectGatherArgs<double> ga{};
+    ga.rows = p->R; ga.columns = p->C; ga.object_rows = p->OR; ga.object_columns = p->OC; ga.n = n;
+    ga.tiles_x = p->tiles_x; ga.tile_w = p->tile_w; ga.tile_h = p->tile_h;
+    ga.tile_start = p->tile_start.as<int>(); ga.tile_list = p->tile_list.as<int>(); ga.dpsi = chi;
+    for (int sl = L - 1; sl >= 0; sl--) {
+        ga.scan = sl == 0 ? scan : own;
+        ga.shifted = sl == 0 ? shifted : waves + (size_t)(sl - 1) * planes;
+        ga.grad = p->grad_o.as<double2>() + (size_t)sl * plane;
+        ga.weight = p->weight_o.as<double>() + (size_t)sl * plane;
+        ga.tile_max = p->tile_max.as<double>() + (size_t)sl * p->tiles;
+        timed(p, kObjectGather, 1, [&] { return launch_object_gather<double>(ga, p->tiles, s); });
+        if (sl == 0) break;
+        timed(p, kBackPropagation, 6, [&] {
+            cudaError_t e = launch_patch_multiply(chi, false, obj + (size_t)sl * plane, true, scan, 0, P, p->R, p->C,
+                                                  p->OR, p->OC, chi, s);
+            if (e == cudaSuccess) e = launch_fft2_f64(f, chi, P, false, s);
+            if (e == cudaSuccess) e = launch_spectrum_multiply(chi, P, n, props + (size_t)(sl - 1) * n, true, inv_n, s);
+            if (e == cudaSuccess) e = launch_fft2_f64(f, chi, P, true, s);
+            return e;
+        });
+    }
+    ProbeGatherArgs<double> pg{};
+    pg.rows = p->R; pg.columns = p->C; pg.object_rows = p->OR; pg.object_columns = p->OC; pg.n = n;
+    pg.count = P; pg.groups = p->groups; pg.scan = scan; pg.object = obj; pg.dpsi = chi;
+    pg.partial_grad = p->partial_grad.as<double2>(); pg.partial_weight = p->partial_weight.as<double>();
+    timed(p, kProbeGather, 1, [&] { return launch_probe_gather<double>(pg, s); });
+    timed(p, kProbeReduce, 1, [&] {
+        return launch_probe_reduce<double>(pg.partial_grad, pg.partial_weight, p->groups, n, p->grad_p64.as<double2>(),
+                                           p->weight_p64.as<double>(), p->probe_block_max.as<double>(), s);
+    });
+    timed(p, kMaxReduce, L + 1, [&] {
+        cudaError_t e = cudaSuccess;
+        for (int sl = 0; sl < L && e == cudaSuccess; sl++)
+            e = launch_max_reduce(p->tile_max.as<double>() + (size_t)sl * p->tiles, p->tiles,
+                                  p->slice_max.as<double>() + sl, s);
+        if (e == cudaSuccess)
+            e = launch_max_reduce(p->probe_block_max.as<double>(), p->probe_blocks, p->maxes.as<double>() + 1, s);
+        return e;
+    });
+    // updates (:547-572): each slice with its own maximum weight; identical slices averaged before the threshold,
+    // which always applies
+    const bool identical = p->identical_slices;
+    timed(p, kObjectUpdate, L + (identical ? 2 : 0), [&] {
+        cudaError_t e = cudaSuccess;
+        for (int sl = 0; sl < L && e == cudaSuccess; sl++)
+            e = launch_object_update<double>(obj + (size_t)sl * plane, p->grad_o.as<double2>() + (size_t)sl * plane,
+                                             p->weight_o.as<double>() + (size_t)sl * plane, (int)plane,
+                                             p->slice_max.as<double>() + sl, pp.step_size, pp.normalization_minimum,
+                                             identical ? 0 : 1, !identical && pp.pure_phase_object ? 1 : 0, s);
+        if (identical && e == cudaSuccess) e = launch_average_slices(obj, L, plane, s);
+        if (identical && e == cudaSuccess)
+            e = launch_object_cap<double>(obj, (int)(L * plane), pp.pure_phase_object ? 1 : 0, s);
+        return e;
+    });
+    enqueue_probe_side(p);
+    timed(p, kErrorReduce, 2, [&] {
+        return launch_error_reduce(p->error.as<double>(), p->error_count, p->divisor, p->errors.as<double>(),
+                                   p->iteration.as<int>(), p->error_scratch.as<double>(), s);
+    });
+}
+
 // The positions on the device after position correction: [rows | columns].
 std::vector<double> download_positions(cubo_ptycho_plan *p) {
     std::vector<double> v((size_t)2 * p->P);
@@ -840,7 +959,8 @@ void enqueue_iterations(cubo_ptycho_plan *p, int iterations) {
     if (iterations > 0) p->tape_valid = false;
     for (int i = 0; i < iterations; i++) {
         refresh_scan(p);
-        if (p->fp64) enqueue_iteration<double>(p);
+        if (p->multislice) enqueue_multislice_iteration(p);
+        else if (p->fp64) enqueue_iteration<double>(p);
         else enqueue_iteration<float>(p);
         p->iterations_done++;
     }
@@ -933,8 +1053,34 @@ int cubo_ptycho_synchronize(cubo_ptycho_context *ctx) {
 
 namespace {
 // cubo_ptycho_plan_create, and the mixed-state engine's plan when `mixed` is given.
+// MultislicePtychography.propagators (PtychographyEngines.swift:427-442): per thickness dz the Fresnel kernel
+// exp(-i pi lambda dz (kr^2 + kc^2)), k = fftfreq / sampling, [thickness][row][column].
+std::vector<double2> fresnel_propagators(int rows, int columns, double row_sampling, double column_sampling,
+                                         double wavelength, int count, const double *thicknesses) {
+    const bool ok = rows > 1 && columns > 1 && std::isfinite(row_sampling) && row_sampling > 0 &&
+                    std::isfinite(column_sampling) && column_sampling > 0 && std::isfinite(wavelength) &&
+                    wavelength > 0 && count > 0 && thicknesses != nullptr;
+    if (!ok) fail(CUBO_PTYCHO_INVALID_INPUT, "propagators: sides above 1, positive finite samplings and wavelength, "
+                                             "at least one thickness");
+    for (int i = 0; i < count; i++)
+        if (!std::isfinite(thicknesses[i])) fail(CUBO_PTYCHO_INVALID_INPUT, "propagators: thickness not finite");
+    const size_t n = (size_t)rows * columns;
+    std::vector<double2> out((size_t)count * n);
+    for (int i = 0; i < count; i++)
+        for (int r = 0; r < rows; r++) {
+            const double kr = frequency(r, rows) / row_sampling;
+            for (int c = 0; c < columns; c++) {
+                const double kc = frequency(c, columns) / column_sampling;
+                const double phase = -kPi * wavelength * thicknesses[i] * (kr * kr + kc * kc);
+                out[(size_t)i * n + (size_t)r * columns + c] = make_double2(std::cos(phase), std::sin(phase));
+            }
+        }
+    return out;
+}
+
 int create_plan(cubo_ptycho_context *ctx, const cubo_ptycho_problem *pr, const cubo_ptycho_params *pp,
-                const cubo_ptycho_mixed_params *mixed, cubo_ptycho_plan **out) {
+                const cubo_ptycho_mixed_params *mixed, const cubo_ptycho_multislice_params *multi,
+                cubo_ptycho_plan **out) {
     if (!out) return CUBO_PTYCHO_INVALID_INPUT;
     *out = nullptr;
     std::unique_ptr<cubo_ptycho_plan> plan;
@@ -953,6 +1099,23 @@ int create_plan(cubo_ptycho_context *ctx, const cubo_ptycho_problem *pr, const c
             if (!line_fft_supported(pr->rows, pr->columns))
                 fail(CUBO_PTYCHO_UNSUPPORTED, "detector sides above the line transform's 4096");
         }
+        std::vector<double2> props;
+        if (multi) {  // PtychographyEngines.swift:471-480; the engine is the reference's Double one
+            if (mixed) fail(CUBO_PTYCHO_INVALID_INPUT, "one engine per plan");
+            if (!(multi->slices >= 1 && multi->slices <= 1024))
+                fail(CUBO_PTYCHO_INVALID_INPUT, "object slices: 1 to 1024");
+            if (multi->slices > 1 && !multi->slice_thicknesses)
+                fail(CUBO_PTYCHO_INVALID_INPUT, "slice thicknesses: one per gap between slices");
+            if (pp->form != CUBO_PTYCHO_FORM_FP64)
+                fail(CUBO_PTYCHO_INVALID_INPUT, "the multislice engine runs in the FP64 form (the reference's is Double)");
+            if (pp->has_position_correction) fail(CUBO_PTYCHO_INVALID_INPUT, "no position correction in multislice");
+            const double zero = 0.0;  // one slice: the propagator of a zero thickness, validated but never applied
+            props = fresnel_propagators(pr->rows, pr->columns, multi->row_sampling, multi->column_sampling,
+                                        multi->wavelength, std::max(1, multi->slices - 1),
+                                        multi->slices > 1 ? multi->slice_thicknesses : &zero);
+            if (!line_fft_supported(pr->rows, pr->columns))
+                fail(CUBO_PTYCHO_UNSUPPORTED, "detector sides above the line transform's 4096");
+        }
         plan.reset(new cubo_ptycho_plan());
         cubo_ptycho_plan *p = plan.get();
         p->ctx = ctx;
@@ -962,6 +1125,11 @@ int create_plan(cubo_ptycho_context *ctx, const cubo_ptycho_problem *pr, const c
             p->states = mixed->states;
             p->orthogonalize = mixed->orthogonalize_probes != 0;
             p->zero_pixel_infinite = mixed->zero_pixel_error == CUBO_PTYCHO_ZERO_PIXEL_REFERENCE;
+        }
+        if (multi) {
+            p->slices = multi->slices;
+            p->multislice = true;
+            p->identical_slices = multi->identical_slices != 0;
         }
         p->objects = (long long)p->OR * p->OC;
         p->params = *pp;
@@ -977,7 +1145,8 @@ int create_plan(cubo_ptycho_context *ctx, const cubo_ptycho_problem *pr, const c
         const bool smem_pass = position_pass_supported(p->n, p->fp64) &&
                                position_pass_smem(p->n, p->R, p->C, p->fp64) <= (size_t)optin;
         // FP64 planes too large for one CTA go through global memory (any size the line transform takes)
-        p->global64 = p->fp64 && (!smem_pass || pp->variant == CUBO_PTYCHO_VARIANT_GLOBAL || p->states > 1);
+        p->global64 = p->fp64 && (!smem_pass || pp->variant == CUBO_PTYCHO_VARIANT_GLOBAL || p->states > 1 ||
+                                  p->multislice);
         if (!smem_pass && !(p->global64 && line_fft_supported(p->R, p->C)))
             fail(CUBO_PTYCHO_UNSUPPORTED, "detector of " + std::to_string(p->n) + " pixels exceeds the shared-memory "
                                               "transform of this form");
@@ -993,6 +1162,7 @@ int create_plan(cubo_ptycho_context *ctx, const cubo_ptycho_problem *pr, const c
         p->correct_positions = pp->has_position_correction != 0;  // before the scan tables: one class per position
         if (p->fp64) build_plan<double>(p, pr);
         else build_plan<float>(p, pr);
+        if (p->multislice && p->slices > 1) upload(p->props64, props, ctx->stream);
         p->positions_given.resize((size_t)2 * p->P);
         std::copy(pr->position_rows, pr->position_rows + p->P, p->positions_given.begin());
         std::copy(pr->position_columns, pr->position_columns + p->P, p->positions_given.begin() + p->P);
@@ -1027,7 +1197,7 @@ extern "C" {
 
 int cubo_ptycho_plan_create(cubo_ptycho_context *ctx, const cubo_ptycho_problem *pr, const cubo_ptycho_params *pp,
                             cubo_ptycho_plan **out) {
-    return create_plan(ctx, pr, pp, nullptr, out);
+    return create_plan(ctx, pr, pp, nullptr, nullptr, out);
 }
 
 void cubo_ptycho_mixed_params_default(cubo_ptycho_mixed_params *m) {
@@ -1041,7 +1211,7 @@ int cubo_ptycho_mixed_plan_create(cubo_ptycho_context *ctx, const cubo_ptycho_pr
                                   const cubo_ptycho_params *pp, const cubo_ptycho_mixed_params *mixed,
                                   cubo_ptycho_plan **out) {
     if (!mixed) return CUBO_PTYCHO_INVALID_INPUT;
-    return create_plan(ctx, pr, pp, mixed, out);
+    return create_plan(ctx, pr, pp, mixed, nullptr, out);
 }
 
 int cubo_ptycho_orthogonalize(cubo_ptycho_context *ctx, int states, int rows, int columns, double *re, double *im) {
@@ -1082,7 +1252,55 @@ int cubo_ptycho_mixed_reconstruct(cubo_ptycho_context *ctx, const cubo_ptycho_pr
         return CUBO_PTYCHO_INVALID_INPUT;
     }
     cubo_ptycho_plan *plan = nullptr;
-    int status = create_plan(ctx, pr, pp, mixed, &plan);
+    int status = create_plan(ctx, pr, pp, mixed, nullptr, &plan);
+    if (status != CUBO_PTYCHO_OK) return status;
+    status = cubo_ptycho_plan_set_state(plan, ore, oim, pre, pim);
+    if (status == CUBO_PTYCHO_OK) status = cubo_ptycho_plan_iterate(plan, pp->iterations, errors);
+    if (status == CUBO_PTYCHO_OK) status = cubo_ptycho_plan_get_state(plan, ore, oim, pre, pim);
+    const std::string message = ctx->last_error;
+    cubo_ptycho_plan_destroy(plan);
+    ctx->last_error = message;
+    return status;
+}
+
+int cubo_ptycho_propagators(int rows, int columns, double row_sampling, double column_sampling, double wavelength,
+                            int count, const double *thicknesses, double *re, double *im) {
+    if (!re || !im) return CUBO_PTYCHO_INVALID_INPUT;
+    try {
+        const std::vector<double2> v =
+            fresnel_propagators(rows, columns, row_sampling, column_sampling, wavelength, count, thicknesses);
+        for (size_t k = 0; k < v.size(); k++) {
+            re[k] = v[k].x;
+            im[k] = v[k].y;
+        }
+    } catch (const Failure &f) {
+        return f.status;
+    } catch (const std::bad_alloc &) {
+        return CUBO_PTYCHO_OUT_OF_MEMORY;
+    }
+    return CUBO_PTYCHO_OK;
+}
+
+int cubo_ptycho_multislice_plan_create(cubo_ptycho_context *ctx, const cubo_ptycho_problem *pr,
+                                       const cubo_ptycho_params *pp, const cubo_ptycho_multislice_params *multi,
+                                       cubo_ptycho_plan **out) {
+    if (!multi) {
+        if (out) *out = nullptr;
+        return CUBO_PTYCHO_INVALID_INPUT;
+    }
+    return create_plan(ctx, pr, pp, nullptr, multi, out);
+}
+
+int cubo_ptycho_multislice_reconstruct(cubo_ptycho_context *ctx, const cubo_ptycho_problem *pr,
+                                       const cubo_ptycho_params *pp, const cubo_ptycho_multislice_params *multi,
+                                       double *ore, double *oim, double *pre, double *pim, double *errors) {
+    if (!ctx) return CUBO_PTYCHO_INVALID_INPUT;
+    if (!multi || !ore || !oim || !pre || !pim || (pp && pp->iterations > 0 && !errors)) {
+        ctx->last_error = "null input or output";
+        return CUBO_PTYCHO_INVALID_INPUT;
+    }
+    cubo_ptycho_plan *plan = nullptr;
+    int status = create_plan(ctx, pr, pp, nullptr, multi, &plan);
     if (status != CUBO_PTYCHO_OK) return status;
     status = cubo_ptycho_plan_set_state(plan, ore, oim, pre, pim);
     if (status == CUBO_PTYCHO_OK) status = cubo_ptycho_plan_iterate(plan, pp->iterations, errors);
@@ -1106,7 +1324,8 @@ int cubo_ptycho_plan_set_state(cubo_ptycho_plan *p, const double *ore, const dou
     if (!p) return CUBO_PTYCHO_INVALID_INPUT;
     return run_guarded(p->ctx, [&] {
         if (!ore || !oim || !pre || !pim) fail(CUBO_PTYCHO_INVALID_INPUT, "null state");
-        for (long long j = 0; j < p->objects; j++)
+        const long long object_values = (long long)p->slices * p->objects;  // every slice, [slice][row][column]
+        for (long long j = 0; j < object_values; j++)
             if (!std::isfinite(ore[j]) || !std::isfinite(oim[j])) fail(CUBO_PTYCHO_INVALID_INPUT, "object not finite");
         const size_t probe_values = (size_t)p->states * p->n;  // every probe state, [state][row][column]
         for (size_t k = 0; k < probe_values; k++)
@@ -1118,8 +1337,8 @@ int cubo_ptycho_plan_set_state(cubo_ptycho_plan *p, const double *ore, const dou
         check(cudaMemcpyAsync(p->probe64.ptr, probe.data(), probe_values * sizeof(double2), cudaMemcpyHostToDevice, s),
               "upload probe");
         if (p->fp64) {
-            std::vector<double2> o((size_t)p->objects);
-            for (long long j = 0; j < p->objects; j++) o[j] = make_double2(ore[j], oim[j]);
+            std::vector<double2> o((size_t)object_values);
+            for (long long j = 0; j < object_values; j++) o[j] = make_double2(ore[j], oim[j]);
             check(cudaMemcpyAsync(p->object.ptr, o.data(), o.size() * sizeof(double2), cudaMemcpyHostToDevice, s), "upload object");
             check(cudaStreamSynchronize(s), "sync");
         } else {
@@ -1147,10 +1366,10 @@ int cubo_ptycho_plan_get_state(cubo_ptycho_plan *p, double *ore, double *oim, do
         check(cudaMemcpyAsync(probe.data(), p->probe64.ptr, probe_values * sizeof(double2), cudaMemcpyDeviceToHost, s),
               "download probe");
         if (p->fp64) {
-            std::vector<double2> o((size_t)p->objects);
+            std::vector<double2> o((size_t)p->slices * p->objects);
             check(cudaMemcpyAsync(o.data(), p->object.ptr, o.size() * sizeof(double2), cudaMemcpyDeviceToHost, s), "download object");
             check(cudaStreamSynchronize(s), "sync");
-            for (long long j = 0; j < p->objects; j++) { if (ore) ore[j] = o[j].x; if (oim) oim[j] = o[j].y; }
+            for (size_t j = 0; j < o.size(); j++) { if (ore) ore[j] = o[j].x; if (oim) oim[j] = o[j].y; }
         } else {
             std::vector<float2> o((size_t)p->objects);
             check(cudaMemcpyAsync(o.data(), p->object.ptr, o.size() * sizeof(float2), cudaMemcpyDeviceToHost, s), "download object");
@@ -1274,7 +1493,7 @@ extern "C" {
 int cubo_ptycho_plan_forward(cubo_ptycho_plan *p, double *loss) {
     if (!p) return CUBO_PTYCHO_INVALID_INPUT;
     return run_guarded(p->ctx, [&] {
-        if (p->states > 1) fail(CUBO_PTYCHO_UNSUPPORTED, "the adjoint pair is single-slice only");
+        if (p->states > 1 || p->multislice) fail(CUBO_PTYCHO_UNSUPPORTED, "the adjoint pair is single-slice only");
         if (p->fp64) enqueue_forward<double>(p);
         else enqueue_forward<float>(p);
         p->tape_valid = true;
@@ -1290,7 +1509,7 @@ int cubo_ptycho_plan_backward(cubo_ptycho_plan *p, int recompute, double *loss, 
                               double *gpre, double *gpim) {
     if (!p) return CUBO_PTYCHO_INVALID_INPUT;
     return run_guarded(p->ctx, [&] {
-        if (p->states > 1) fail(CUBO_PTYCHO_UNSUPPORTED, "the adjoint pair is single-slice only");
+        if (p->states > 1 || p->multislice) fail(CUBO_PTYCHO_UNSUPPORTED, "the adjoint pair is single-slice only");
         if (recompute || !p->tape_valid) {
             if (p->fp64) enqueue_forward<double>(p);
             else enqueue_forward<float>(p);

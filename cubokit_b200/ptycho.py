@@ -377,17 +377,101 @@ class MixedstatePtychography:
         return np.stack(out)
 
 
+@dataclass
+class MultisliceResult:
+    """``MultislicePtychography.Result`` (``PtychographyEngines.swift:460-466``)."""
+    object: np.ndarray  # (slices, rows, columns), entrance first
+    probe: np.ndarray
+    errors: np.ndarray
+
+
+def _multislice_params(slices, slice_thicknesses, wavelength, row_sampling, column_sampling, identical_slices):
+    """The ``cubo_ptycho_multislice_params`` of a call and the thickness array it points into (kept alive by the
+    caller)."""
+    thick = np.ascontiguousarray(np.asarray(slice_thicknesses, np.float64).ravel())
+    if len(thick) != int(slices) - 1:
+        raise PtychographyError("sliceThicknesses.count != slices - 1")  # PtychographyEngines.swift:477
+    m = L.MultisliceParams()
+    m.slices = int(slices)
+    m.slice_thicknesses = _ptr(thick) if len(thick) else None
+    m.wavelength = float(wavelength)
+    m.row_sampling = float(row_sampling)
+    m.column_sampling = float(column_sampling)
+    m.identical_slices = int(bool(identical_slices))
+    return m, thick
+
+
+class MultislicePtychography:
+    """``MultislicePtychography`` (``PtychographyEngines.swift:420-588``) on the GPU, FP64: a stack of object slices
+    with Fresnel propagation between them; see ``cubo_ptycho_multislice_reconstruct`` in ``include/cubo_ptycho.h``."""
+
+    Result = MultisliceResult
+
+    @staticmethod
+    def propagators(rows: int, columns: int, row_sampling: float, column_sampling: float, wavelength: float,
+                    slice_thicknesses) -> np.ndarray:
+        """``MultislicePtychography.propagators``: one ``(rows, columns)`` Fresnel kernel
+        ``exp(-i pi lambda dz (kr^2 + kc^2))`` per thickness (host arithmetic; no device needed)."""
+        thick = np.ascontiguousarray(np.asarray(slice_thicknesses, np.float64).ravel())
+        count = len(thick)
+        size = max(count, 1) * max(int(rows), 1) * max(int(columns), 1)
+        re, im = np.zeros(size), np.zeros(size)
+        st = L.load().cubo_ptycho_propagators(int(rows), int(columns), float(row_sampling), float(column_sampling),
+                                         float(wavelength), count, _ptr(thick) if count else None, _ptr(re), _ptr(im))
+        if st != 0:
+            raise PtychographyError("propagators")
+        return (re + 1j * im).reshape(count, int(rows), int(columns))
+
+    @staticmethod
+    def reconstruct(amplitudes, positions, object, probe, slice_thicknesses, wavelength: float, row_sampling: float,
+                    column_sampling: float, iterations: int = 8, step_size: float = 0.5,
+                    normalization_minimum: float = 1.0, fix_probe: bool = False, pure_phase_object: bool = False,
+                    identical_slices: bool = False, fix_probe_center_of_mass: bool = False,
+                    constrain_probe_amplitude: bool = False, probe_amplitude_relative_radius: float = 0.5,
+                    probe_amplitude_relative_width: float = 0.05, fix_probe_aperture: bool = False,
+                    probe_support_mask=None, error_normalization="suppliedAmplitudeEnergy",
+                    device: int = 0) -> MultisliceResult:
+        """``object`` is ``(slices, rows, columns)`` complex (entrance first), ``slice_thicknesses`` the
+        ``slices - 1`` gaps, in the units of ``wavelength`` and the samplings."""
+        obj = np.asarray(object)
+        prb = np.asarray(probe)
+        if obj.ndim != 3 or prb.ndim != 2:
+            raise PtychographyError("object must be (slices, rows, columns) and probe 2-D")
+        ctx = context(device)
+        inp = _Inputs(amplitudes, positions, obj.shape[1:], prb.shape, iterations, step_size, normalization_minimum,
+                      fix_probe, pure_phase_object, True, fix_probe_center_of_mass, constrain_probe_amplitude,
+                      probe_amplitude_relative_radius, probe_amplitude_relative_width, fix_probe_aperture,
+                      probe_support_mask, error_normalization, None, "fp64")
+        multi, thick = _multislice_params(obj.shape[0], slice_thicknesses, wavelength, row_sampling,
+                                          column_sampling, identical_slices)
+        ore, oim = _split(obj)
+        pre, pim = _split(prb)
+        errors = np.zeros(max(int(iterations), 1))
+        ctx.check(ctx.lib.cubo_ptycho_multislice_reconstruct(ctx.handle, C.byref(inp.problem), C.byref(inp.params),
+                                                             C.byref(multi), _ptr(ore), _ptr(oim), _ptr(pre),
+                                                             _ptr(pim), _ptr(errors)))
+        del thick
+        return MultisliceResult((ore + 1j * oim).reshape(obj.shape), (pre + 1j * pim).reshape(prb.shape),
+                                errors[: int(iterations)].copy())
+
+
 class Plan:
     """A device-resident reconstruction (``cubo_ptycho_plan_*``): upload once, iterate, read the state back."""
 
     def __init__(self, amplitudes, positions, object_shape, probe_shape, ctx: Optional[Context] = None, **kwargs):
         """``mixed_states=S`` makes a mixed-state plan (``cubo_ptycho_mixed_plan_create``, FP64; with
-        ``orthogonalize_probes`` and ``zero_far_field_pixel_error``): its state holds S probes."""
+        ``orthogonalize_probes`` and ``zero_far_field_pixel_error``): its state holds S probes.
+        ``multislice=dict(slices=L, slice_thicknesses=..., wavelength=..., row_sampling=..., column_sampling=...[,
+        identical_slices=...])`` makes a multislice plan (``cubo_ptycho_multislice_plan_create``, FP64): its object
+        holds L slices of ``object_shape``."""
         self.ctx = ctx or context(kwargs.pop("device", 0))
         states = kwargs.pop("mixed_states", None)
+        multislice = kwargs.pop("multislice", None)
         orthogonalize_probes = kwargs.pop("orthogonalize_probes", True)
         zero_error = kwargs.pop("zero_far_field_pixel_error", "reference")
-        if states is not None:
+        if states is not None and multislice is not None:
+            raise PtychographyError("one engine per plan")
+        if states is not None or multislice is not None:
             kwargs["precision"] = "fp64"
             kwargs.setdefault("constrain_object_amplitude", True)
         defaults = dict(iterations=0, step_size=0.5, normalization_minimum=1.0, fix_probe=False,
@@ -399,9 +483,19 @@ class Plan:
         defaults.update(kwargs)
         self.inputs = _Inputs(amplitudes, positions, tuple(object_shape), tuple(probe_shape), **defaults)
         self.object_shape = tuple(object_shape)
+        if multislice is not None:
+            self.object_shape = (int(multislice["slices"]),) + self.object_shape
         self.probe_shape = tuple(probe_shape) if states is None else (int(states),) + tuple(probe_shape)
         h = C.c_void_p()
-        if states is None:
+        if multislice is not None:
+            ms = dict(multislice)
+            multi, self._thicknesses = _multislice_params(ms["slices"], ms["slice_thicknesses"], ms["wavelength"],
+                                                          ms["row_sampling"], ms["column_sampling"],
+                                                          ms.get("identical_slices", False))
+            self.ctx.check(self.ctx.lib.cubo_ptycho_multislice_plan_create(
+                self.ctx.handle, C.byref(self.inputs.problem), C.byref(self.inputs.params), C.byref(multi),
+                C.byref(h)))
+        elif states is None:
             self.ctx.check(self.ctx.lib.cubo_ptycho_plan_create(self.ctx.handle, C.byref(self.inputs.problem),
                                                                 C.byref(self.inputs.params), C.byref(h)))
         else:

@@ -185,6 +185,38 @@ CUBO_PTYCHO_API int cubo_ptycho_mixed_plan_create(cubo_ptycho_context *context, 
                                                   const cubo_ptycho_params *params,
                                                   const cubo_ptycho_mixed_params *mixed, cubo_ptycho_plan **out);
 
+/* ---- The multislice engine: MultislicePtychography.reconstruct (PtychographyEngines.swift:458-588).  The object is a
+ * stack of `slices` transmission functions (entrance first) with a Fresnel propagation between neighbours; the
+ * problem's object_rows x object_columns is one slice.  Runs in the FP64 form (the reference's engine is Double) with
+ * the shared params: iterations, step_size, normalization_minimum, fix_probe, pure_phase_object, fix_probe_center_of_mass,
+ * constrain_probe_amplitude, fix_probe_aperture, probe_support_mask, error_normalization; the object threshold
+ * |O| <= 1 always applies; position correction is refused.  Objects are [slice][row][column]. */
+typedef struct {
+    int slices;                       /* object slices, 1 to 1024 */
+    const double *slice_thicknesses;  /* slices - 1 gaps (length units of the samplings); may be NULL for one slice */
+    double wavelength;                /* same units */
+    double row_sampling, column_sampling;  /* object pixel sizes, same units */
+    int identical_slices;             /* true: after each update every slice becomes the slices' mean */
+} cubo_ptycho_multislice_params;
+/* MultislicePtychography.propagators (PtychographyEngines.swift:427-442), on the host: count grids of rows x columns,
+ * exp(-i pi wavelength dz (kr^2 + kc^2)) with k = fftfreq / sampling, into re / im ([thickness][row][column]). */
+CUBO_PTYCHO_API int cubo_ptycho_propagators(int rows, int columns, double row_sampling, double column_sampling,
+                                            double wavelength, int count, const double *thicknesses, double *re,
+                                            double *im);
+/* object_re/_im (slices * object_rows * object_columns) hold the start and receive Result.object; probe_re/_im the
+ * probe; errors receives params->iterations values. */
+CUBO_PTYCHO_API int cubo_ptycho_multislice_reconstruct(cubo_ptycho_context *context, const cubo_ptycho_problem *problem,
+                                                       const cubo_ptycho_params *params,
+                                                       const cubo_ptycho_multislice_params *multislice,
+                                                       double *object_re, double *object_im, double *probe_re,
+                                                       double *probe_im, double *errors);
+/* A device-resident multislice plan: set_state / get_state take and return every slice; forward / backward are
+ * single-slice only. */
+CUBO_PTYCHO_API int cubo_ptycho_multislice_plan_create(cubo_ptycho_context *context, const cubo_ptycho_problem *problem,
+                                                       const cubo_ptycho_params *params,
+                                                       const cubo_ptycho_multislice_params *multislice,
+                                                       cubo_ptycho_plan **out);
+
 /* ---- Device-resident plans: the same reconstruction split into its upload, iterations and download, so data stays in
  * HBM across calls (resume = more iterations on the same plan).  No counterpart in the reference, whose arrays are
  * Swift values; reconstruct() is create + set_state + iterate + get_state + destroy. */

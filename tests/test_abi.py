@@ -7,6 +7,7 @@ import ctypes as C
 import re
 from pathlib import Path
 
+import numpy as np
 import pytest
 
 ROOT = Path(__file__).resolve().parents[1]
@@ -43,10 +44,11 @@ def test_struct_layouts_match_the_header():
 #include <stddef.h>
 #include "cubo_ptycho.h"
 int main(void) {
-  printf("%zu %zu %zu %zu %zu %zu %zu\n", sizeof(cubo_ptycho_problem), sizeof(cubo_ptycho_params),
+  printf("%zu %zu %zu %zu %zu %zu %zu %zu %zu\n", sizeof(cubo_ptycho_problem), sizeof(cubo_ptycho_params),
          offsetof(cubo_ptycho_params, form), offsetof(cubo_ptycho_params, progress_user),
          offsetof(cubo_ptycho_params, max_position_total_distance),
-         offsetof(cubo_ptycho_params, position_columns_out), sizeof(cubo_ptycho_mixed_params));
+         offsetof(cubo_ptycho_params, position_columns_out), sizeof(cubo_ptycho_mixed_params),
+         sizeof(cubo_ptycho_multislice_params), offsetof(cubo_ptycho_multislice_params, identical_slices));
   return 0;
 }
 '''
@@ -62,6 +64,26 @@ int main(void) {
     assert int(out[4]) == _lib.Params.max_position_total_distance.offset
     assert int(out[5]) == _lib.Params.position_columns_out.offset
     assert int(out[6]) == C.sizeof(_lib.MixedParams)
+    assert int(out[7]) == C.sizeof(_lib.MultisliceParams)
+    assert int(out[8]) == _lib.MultisliceParams.identical_slices.offset
+
+
+def test_propagators_on_the_host():
+    """``MultislicePtychography.propagators`` (host arithmetic, no device): the Fresnel kernels equal the oracle's
+    restatement, and invalid samplings, wavelengths and thicknesses are refused (``PtychographyEngines.swift:427-433``)."""
+    import cubokit_b200
+    from oracle import numpy_oracle as no
+    args = (12, 10, 0.45, 0.5, 0.0197, [40.0, 55.0, 0.0])
+    got = cubokit_b200.MultislicePtychography.propagators(*args)
+    want = no.propagators(*args)
+    assert got.shape == (3, 12, 10)
+    assert np.max(np.abs(got - want)) < 1e-12
+    bad = [(1, 10, 0.45, 0.5, 0.0197, [1.0]), (12, 10, 0.0, 0.5, 0.0197, [1.0]),
+           (12, 10, 0.45, np.inf, 0.0197, [1.0]), (12, 10, 0.45, 0.5, -1.0, [1.0]),
+           (12, 10, 0.45, 0.5, 0.0197, []), (12, 10, 0.45, 0.5, 0.0197, [np.nan])]
+    for b in bad:
+        with pytest.raises(cubokit_b200.PtychographyError):
+            cubokit_b200.MultislicePtychography.propagators(*b)
 
 
 def test_context_without_a_device_is_refused_cleanly():
