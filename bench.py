@@ -483,6 +483,82 @@ def run_mixed(args, world, rank, local):
             "cpu_baseline": cpu, "e2e": None, "gpu_launches": launches, "clocks": clocks.summary()}), flush=True)
 
 
+def run_multislice(args, world, rank, local):
+    """The multislice engine (MultislicePtychography, FP64) on the precision workload's data: 4 slices of the start
+    object 20 A apart at 300 kV and the data's object sampling; one step = one full-batch iteration (forward through
+    every slice, projection, back-propagation with every slice's gradient, the updates)."""
+    import torch
+    import cubokit_b200 as cb
+    from cubokit_b200 import synthetic
+    slices, thickness = 4, 20.0
+    ds = synthetic.dataset(args.scan, DET, dose=DOSE, step=STEP, pinned=True, device=local)
+    P, n = len(ds.positions), DET * DET
+    sampling = float(ds.config["sampling_A"])
+    wavelength = cb.electron_wavelength(300e3)
+    obj = np.stack([ds.object_start] * slices)
+    multislice = dict(slices=slices, slice_thicknesses=[thickness] * (slices - 1), wavelength=wavelength,
+                      row_sampling=sampling, column_sampling=sampling)
+    ctx = cb.Context(local)
+    stream = torch.cuda.ExternalStream(ctx.stream, device=torch.device("cuda", local))
+    plan = cb.Plan(ds.amplitudes, ds.positions, ds.object_start.shape, ds.probe.shape, ctx=ctx, step_size=0.5,
+                   fix_probe_center_of_mass=True, multislice=multislice)
+    plan.set_state(obj, ds.probe)
+    plan.enqueue(args.warmup)
+    ctx.synchronize()
+    barrier(world)
+    start_ev, stop_ev = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    launches0 = plan.launch_count
+    with ClockSampler(local) as clocks:
+        start_ev.record(stream)
+        plan.enqueue(args.steps)
+        stop_ev.record(stream)
+        stop_ev.synchronize()
+    ms = max_over_ranks(start_ev.elapsed_time(stop_ev), world)
+    launches = plan.launch_count - launches0
+    errors = plan.errors(args.warmup + args.steps)
+    plan.set_timing(True)
+    timed_iterations = max(2, min(args.steps, 4))
+    plan.enqueue(timed_iterations)
+    stats = plan.kernel_stats()
+    plan.set_timing(False)
+    plan.close()
+    value = P * args.steps / (ms * 1e-3) * world
+    hbm_peak, _, peak_kind = measured_peaks()
+    pass_ms = stats["position_pass"][0] / timed_iterations
+    # algorithmic bytes of the forward pass: amplitudes read once (4n), the waves entering slices 1 .. L-1 and the
+    # last exit wave's residual written once each (16n per slice)
+    pass_bytes = P * (4 + 16 * slices) * n
+    cpu = None
+    if rank == 0 and not args.no_cpu:
+        from oracle import numpy_oracle as no
+        sample = 32
+        amps = ds.amplitudes.reshape(P, DET, DET)[:sample].astype(np.float64)
+        t0 = time.perf_counter()
+        no.multislice_reconstruct(amps, ds.positions[:sample], obj, ds.probe, multislice["slice_thicknesses"],
+                                  wavelength, sampling, sampling, iterations=1, step_size=0.5,
+                                  fix_probe_center_of_mass=True)
+        cpu = {"value": sample / (time.perf_counter() - t0), "unit": UNIT, "cores": 1, "kind": "port",
+               "sample": f"one iteration over {sample} of {P} positions, {slices} slices, NumPy FP64 restatement"}
+    if rank == 0:
+        per_kind = {k: round(v[0] / timed_iterations, 3) for k, v in stats.items() if v[1]}
+        print(json.dumps({
+            "metric": f"positions*iter/s, multislice GD ({slices} slices, FP64, 128^2 detector)", "value": value,
+            "unit": UNIT, "n_gpus": world, "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms / args.steps,
+            "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+            "config": {"workload": f"multislice: {P} positions ({args.scan}^2 raster), {DET}x{DET} detector, "
+                                   f"{slices} slices {thickness:g} A apart, 300 kV, centre of mass",
+                       "l2": f"amplitudes {P * n * 4 / 1e9:.1f} GB, entering waves and residuals "
+                             f"{P * n * 16 * slices / 1e9:.0f} GB: far larger than L2"},
+            "roofline": {"kernel": "multislice forward pass (patch products, FP64 line FFTs, propagators, projection)",
+                         "bound": "hbm", "achieved": pass_bytes / (pass_ms * 1e-3) / 1e9, "peak": hbm_peak,
+                         "unit": "GB/s", "frac": pass_bytes / (pass_ms * 1e-3) / 1e9 / hbm_peak,
+                         "peak_kind": peak_kind, "launch_ms": pass_ms,
+                         "note": "each slice's waves go through HBM for every FFT pass (FP64 planes of 128^2 do "
+                                 "not fit one CTA)", "traffic": None},
+            "kernel_ms_per_iteration": per_kind, "errors_first_last": [errors[0], errors[-1]],
+            "cpu_baseline": cpu, "e2e": None, "gpu_launches": launches, "clocks": clocks.summary()}), flush=True)
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -495,11 +571,11 @@ def main():
     ap.add_argument("--no-cpu", action="store_true")
     ap.add_argument("--scan", type=int, default=SCAN, help="scan side (the benchmark workload is 256)")
     ap.add_argument("--workload", default="precision",
-                    choices=["precision", "batched", "preprocess", "positions", "mixed"],
+                    choices=["precision", "batched", "preprocess", "positions", "mixed", "multislice"],
                     help="precision: the 256^2-scan 128^2-detector GD (default); batched: 64 independent "
                          "reconstructions of uneven sizes in one graph; preprocess: amplitude preprocessing of the "
                          "precision workload's cube; positions: GD with position correction (FP64 form); mixed: the mixed-state "
-                         "engine with 4 probe states (FP64)")
+                         "engine with 4 probe states (FP64); multislice: the multislice engine with 4 slices (FP64)")
     args = ap.parse_args()
     world, rank, local = dist_setup(args)
     if args.impl == "reference":
@@ -523,6 +599,9 @@ def main():
         return
     if args.workload == "mixed":
         run_mixed(args, world, rank, local)
+        return
+    if args.workload == "multislice":
+        run_multislice(args, world, rank, local)
         return
 
     ds = synthetic.dataset(args.scan, DET, dose=DOSE, step=STEP, pinned=True, device=local)

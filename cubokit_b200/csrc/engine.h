@@ -204,6 +204,31 @@ cudaError_t launch_spectrum_multiply(double2 *data, long long planes, int n, con
 // identicalSlices: every slice becomes the mean of the slices.
 cudaError_t launch_average_slices(double2 *object, int slices, long long plane, cudaStream_t s);
 
+// plane128.cu: the 128 x 128 FP64 plane transform of positions first .. first + count - 1 in one launch: the input plane
+// (times the object patch) -> FFT -> the pointwise step -> inverse FFT (unscaled) -> out.  A cluster of
+// plane128_cluster() CTAs holds one plane.
+struct Plane128Args {
+    int first, count;
+    const double2 *in;              // plane of position p: in + (in_by_class ? scan.cls[p] : p) * 16384
+    int in_by_class;
+    const double2 *object;          // the object patch factor, conjugated when conj_object; null: none
+    int conj_object;
+    ScanTables scan;
+    int object_rows, object_columns;
+    int project;                    // 1: modulus projection with amplitudes (x inv_n) and error[p]; 0: x prop x scale
+    const double2 *prop;            // [128 x 128], conjugated when conj_prop
+    int conj_prop;
+    double scale;
+    const float *amplitudes;        // [positions][128 x 128]
+    double *error;                  // [positions] squared amplitude residual
+    double inv_n;
+    const double2 *tw;              // W_128^k, k = 0..127 (forward sign)
+    double2 *out;                   // plane of position p: out + p * 16384 (may be `in`)
+};
+int plane128_cluster();
+cudaError_t configure_plane128();
+cudaError_t launch_plane128(const Plane128Args &a, int cluster, cudaStream_t s);
+
 // mixed_kernels.cu: the mixed-state engine (MixedstatePtychography, PtychographyEngines.swift:121-267), FP64.
 constexpr int kMaxStates = 16;
 struct MixedPassArgs {

@@ -125,6 +125,8 @@ struct cubo_ptycho_plan {
     bool fast = false;      // 128 x 128 FP32 register-resident position pass
     bool bf16 = false;      // 128 x 128 split-BF16 tensor-core position pass
     bool global64 = false;  // FP64 position pass through global memory (the plane does not fit shared memory)
+    bool plane128 = false;  // FP64 128 x 128 planes: FFT, pointwise step and inverse FFT in one clustered launch
+    int plane_cluster = 2;  // CTAs per plane of that launch
     int states = 1;         // probe states (the mixed-state engine; 1 = single slice)
     int slices = 1;         // object slices (the multislice engine)
     bool multislice = false;        // the multislice engine (its iteration, even with one slice)
@@ -651,6 +653,20 @@ void enqueue_probe_side(cubo_ptycho_plan *p) {
         });
 }
 
+// The clustered 128 x 128 plane launch of every position: `in` (by class or by position) times the object patch
+// (conjugated), FFT, the propagator `prop` x scale (project == false) or the modulus projection with the error
+// (project == true), inverse FFT, into `out`.
+void enqueue_plane128(cubo_ptycho_plan *p, Kind kind, const double2 *in, bool by_class, const double2 *object,
+                      bool conj_object, bool project, const double2 *prop, bool conj_prop, double2 *out) {
+    Plane128Args a{};
+    a.first = 0; a.count = p->P; a.in = in; a.in_by_class = by_class ? 1 : 0; a.object = object;
+    a.conj_object = conj_object ? 1 : 0; a.scan = ScanTables{p->rr.as<int>(), p->cc.as<int>(), p->cls.as<int>()};
+    a.object_rows = p->OR; a.object_columns = p->OC; a.project = project ? 1 : 0; a.prop = prop;
+    a.conj_prop = conj_prop ? 1 : 0; a.scale = 1.0 / p->n; a.amplitudes = p->amplitudes.as<float>();
+    a.error = p->error.as<double>(); a.inv_n = 1.0 / p->n; a.tw = p->tw_r64.as<double2>(); a.out = out;
+    timed(p, kind, 1, [&] { return launch_plane128(a, p->plane_cluster, p->ctx->stream); });
+}
+
 // Shifted probes, then the position pass over every position: residuals (dpsi) and per-position squared errors.
 template <typename T>
 void enqueue_position_pass(cubo_ptycho_plan *p) {
@@ -694,6 +710,10 @@ void enqueue_position_pass(cubo_ptycho_plan *p) {
             p->launches += count;
             if (p->timing) p->kind_launches[kPositionPass] += count;
         }
+    } else if (p->plane128) {
+        if constexpr (std::is_same<T, double>::value)
+            enqueue_plane128(p, kPositionPass, p->shifted.as<double2>(), true, p->object.as<double2>(), false, true,
+                             nullptr, false, p->dpsi.as<double2>());
     } else if (p->global64) {
         int count = 0;
         if constexpr (std::is_same<T, double>::value) {
@@ -819,6 +839,14 @@ void enqueue_multislice_iteration(cubo_ptycho_plan *p) {
     const double2 *shifted = p->shifted.as<double2>(), *props = p->props64.as<double2>();
     const Fft2Plan64 f = fft64(p);
     enqueue_shift_table<double>(p);
+    if (p->plane128) {  // forward and detector, one plane launch per slice
+        for (int sl = 0; sl < L; sl++) {
+            const double2 *in = sl == 0 ? shifted : waves + (size_t)(sl - 1) * planes;
+            const bool last = sl == L - 1;
+            enqueue_plane128(p, kPositionPass, in, sl == 0, obj + (size_t)sl * plane, false, last,
+                             last ? nullptr : props + (size_t)sl * n, false, last ? chi : waves + (size_t)sl * planes);
+        }
+    } else {
     // forward (:503-515): exit_s = wave_s x O_s; wave_{s+1} = IFFT(FFT(exit_s) x prop_s / n)
     timed(p, kPositionPass, 6 * (L - 1) + 1, [&] {
         cudaError_t e = cudaSuccess;
@@ -848,6 +876,7 @@ void enqueue_multislice_iteration(cubo_ptycho_plan *p) {
         if (e == cudaSuccess) e = launch_fft2_f64(f, chi, P, true, s);
         return e;
     });
+    }
     // backward (:526-545): slice s's gradient from its entering wave and chi, chi x conj(O_s) carried back one slice;
     // at slice 0 the probe gradient from conj(O_0) chi
     ObjectGatherArgs<double> ga{};
@@ -862,6 +891,11 @@ void enqueue_multislice_iteration(cubo_ptycho_plan *p) {
         ga.tile_max = p->tile_max.as<double>() + (size_t)sl * p->tiles;
         timed(p, kObjectGather, 1, [&] { return launch_object_gather<double>(ga, p->tiles, s); });
         if (sl == 0) break;
+        if (p->plane128) {
+            enqueue_plane128(p, kBackPropagation, chi, false, obj + (size_t)sl * plane, true, false,
+                             props + (size_t)(sl - 1) * n, true, chi);
+            continue;
+        }
         timed(p, kBackPropagation, 6, [&] {
             cudaError_t e = launch_patch_multiply(chi, false, obj + (size_t)sl * plane, true, scan, 0, P, p->R, p->C,
                                                   p->OR, p->OC, chi, s);
@@ -1147,6 +1181,13 @@ int create_plan(cubo_ptycho_context *ctx, const cubo_ptycho_problem *pr, const c
         // FP64 planes too large for one CTA go through global memory (any size the line transform takes)
         p->global64 = p->fp64 && (!smem_pass || pp->variant == CUBO_PTYCHO_VARIANT_GLOBAL || p->states > 1 ||
                                   p->multislice);
+        // 128 x 128 FP64 planes of one probe state: the clustered plane launch (not with the generic variant)
+        p->plane128 = p->global64 && p->states == 1 && p->R == 128 && p->C == 128 &&
+                      pp->variant != CUBO_PTYCHO_VARIANT_GENERIC;
+        if (p->plane128) {
+            check(configure_plane128(), "configure plane transform");
+            p->plane_cluster = plane128_cluster();
+        }
         if (!smem_pass && !(p->global64 && line_fft_supported(p->R, p->C)))
             fail(CUBO_PTYCHO_UNSUPPORTED, "detector of " + std::to_string(p->n) + " pixels exceeds the shared-memory "
                                               "transform of this form");

@@ -1,0 +1,321 @@
+// The 128 x 128 FP64 plane transform: one position's plane through FFT -> a pointwise step -> inverse FFT in ONE
+// launch, read once from HBM and written once.  An FP64 plane of 128 x 128 (256 KB) is larger than one SM's shared
+// memory, so a cluster of Q CTAs holds it: each CTA keeps 128 / Q rows in registers (16 complex values per thread,
+// eight threads per line), and the row / column redistributions go through distributed shared memory.
+//
+// Per line of 128 = 16 x 8 (n = j + 8 m, k = k1 + 16 k2), the eight threads j of a line each hold x[j + 8 m]:
+//   1. a 16-point DFT over m in registers, then the twiddle W_128^(j k1);
+//   2. an 8 x 8 transpose of pairs across the line's eight lanes (three xor-shuffle rounds);
+//   3. 8-point DFTs over j: thread j' then holds X[2 j' + c + 16 k2], c = 0, 1, k2 = 0 .. 7.
+// The inverse runs the same steps in the opposite order (from that distribution back to x[j + 8 m]), so the spectrum
+// never needs reordering: rows -> columns -> pointwise -> inverse columns -> inverse rows.
+//
+// The pointwise step is either the Fresnel propagator times a scale (multislice propagation, MultislicePtychography,
+// PtychographyEngines.swift:503-545) or the modulus projection with the per-position squared error
+// (Ptychography.swift:327-349 and PtychographyEngines.swift:516-524).  The input can be multiplied by the object patch
+// of the position (or its conjugate) as it is read: the exit wave of the forward model, or chi x conj(O) of the
+// backward one.
+#include <cooperative_groups.h>
+
+#include <cstdlib>
+
+#include "engine.h"
+
+namespace cg = cooperative_groups;
+
+namespace cubo {
+
+namespace {
+
+constexpr int kSide = 128, kPlane = kSide * kSide;
+
+template <int Q>
+struct PlaneGeometry {
+    static constexpr int kLines = kSide / Q;            // rows (row passes) or columns (column passes) per CTA
+    static constexpr int kThreads = 8 * kLines;         // eight threads per line
+    static constexpr int kStrideA = kLines + 1;          // [128 rows][kLines columns] + 1 (conflict-free columns)
+    static constexpr int kStrideB = kSide + 1;           // [kLines rows][128 columns] + 1
+    static constexpr int kBuffer = (kSide * kStrideA > kLines * kStrideB) ? kSide * kStrideA : kLines * kStrideB;
+    static constexpr size_t kSmem = (size_t)(kBuffer + kSide) * sizeof(double2) + (32 + 8) * sizeof(double);
+};
+
+__device__ __forceinline__ int wrap_once(int v, int n) { return v < 0 ? v + n : (v >= n ? v - n : v); }
+
+// 4-point DFT in place (sign -1 forward, +1 when INV, unscaled).
+template <bool INV>
+__device__ __forceinline__ void dft4(double2 &x0, double2 &x1, double2 &x2, double2 &x3) {
+    const double2 a0 = cadd(x0, x2), a1 = csub(x0, x2), b0 = cadd(x1, x3), b1 = cmul_mi(csub(x1, x3), INV);
+    x0 = cadd(a0, b0);
+    x2 = csub(a0, b0);
+    x1 = cadd(a1, b1);
+    x3 = csub(a1, b1);
+}
+
+// 8-point DFT of x[0..7] in place (radix 2 over two 4-point DFTs).
+template <bool INV>
+__device__ __forceinline__ void dft8(double2 (&x)[8]) {
+    constexpr double h = 0.70710678118654752440;  // 1 / sqrt(2)
+    double2 e0 = x[0], e1 = x[2], e2 = x[4], e3 = x[6], o0 = x[1], o1 = x[3], o2 = x[5], o3 = x[7];
+    dft4<INV>(e0, e1, e2, e3);
+    dft4<INV>(o0, o1, o2, o3);
+    // W_8^k o_k: k = 1 -> (1 -/+ i) h, k = 2 -> -/+ i, k = 3 -> (-1 -/+ i) h
+    const double s = INV ? 1.0 : -1.0;
+    const double2 t1 = make_double2((o1.x - s * o1.y) * h, (o1.y + s * o1.x) * h);
+    const double2 t2 = cmul_mi(o2, INV);
+    const double2 t3 = make_double2((-o3.x - s * o3.y) * h, (-o3.y + s * o3.x) * h);
+    x[0] = cadd(e0, o0);
+    x[4] = csub(e0, o0);
+    x[1] = cadd(e1, t1);
+    x[5] = csub(e1, t1);
+    x[2] = cadd(e2, t2);
+    x[6] = csub(e2, t2);
+    x[3] = cadd(e3, t3);
+    x[7] = csub(e3, t3);
+}
+
+// 16-point DFT of v[0..15] in place (radix 4 x 4).
+template <bool INV>
+__device__ __forceinline__ void dft16(double2 (&v)[16]) {
+    constexpr double c1 = 0.92387953251128675613, s1 = 0.38268343236508977173, h = 0.70710678118654752440;
+    const double s = INV ? 1.0 : -1.0;  // sign of the exponent
+#pragma unroll
+    for (int m1 = 0; m1 < 4; m1++) dft4<INV>(v[m1], v[m1 + 4], v[m1 + 8], v[m1 + 12]);
+    // v[m1 + 4 a] *= W_16^(m1 a)
+    const double2 w1 = make_double2(c1, s * s1), w2 = make_double2(h, s * h), w3 = make_double2(s1, s * c1);
+    const double2 w6 = make_double2(-h, s * h), w9 = make_double2(-c1, -s * s1);
+    v[5] = cmul(v[5], w1);
+    v[9] = cmul(v[9], w2);
+    v[13] = cmul(v[13], w3);
+    v[6] = cmul(v[6], w2);
+    v[10] = cmul_mi(v[10], INV);
+    v[14] = cmul(v[14], w6);
+    v[7] = cmul(v[7], w3);
+    v[11] = cmul(v[11], w6);
+    v[15] = cmul(v[15], w9);
+#pragma unroll
+    for (int a = 0; a < 4; a++) dft4<INV>(v[4 * a], v[4 * a + 1], v[4 * a + 2], v[4 * a + 3]);
+    // X[a + 4 b] sits at v[4 a + b]: transpose the 4 x 4 index
+    double2 t[16];
+#pragma unroll
+    for (int a = 0; a < 4; a++)
+#pragma unroll
+        for (int b = 0; b < 4; b++) t[a + 4 * b] = v[4 * a + b];
+#pragma unroll
+    for (int k = 0; k < 16; k++) v[k] = t[k];
+}
+
+// Thread j of a line holds blocks b = 0..7 (pairs v[2b], v[2b+1]); afterwards thread b holds what thread j had in
+// block b, in block j.  Three xor rounds over the line's eight consecutive lanes.
+__device__ __forceinline__ void pair_transpose(double2 (&v)[16], int j) {
+#pragma unroll
+    for (int mask = 1; mask < 8; mask <<= 1) {
+        const bool upper = (j & mask) != 0;
+#pragma unroll
+        for (int b = 0; b < 8; b++) {
+            if (b & mask) continue;
+            const int bp = b | mask;
+#pragma unroll
+            for (int c = 0; c < 2; c++) {
+                const double2 send = upper ? v[2 * b + c] : v[2 * bp + c];
+                double2 got;
+                got.x = __shfl_xor_sync(0xffffffffu, send.x, mask);
+                got.y = __shfl_xor_sync(0xffffffffu, send.y, mask);
+                if (upper) v[2 * b + c] = got;
+                else v[2 * bp + c] = got;
+            }
+        }
+    }
+}
+
+// Forward line transform: thread j holds x[j + 8 m] in v[m]; afterwards thread j holds X[2 j + c + 16 k2] in
+// v[2 k2 + c].  tw = W_128^k (forward sign), k = 0..127.
+__device__ __forceinline__ void line_forward(double2 (&v)[16], int j, const double2 *tw) {
+    dft16<false>(v);
+#pragma unroll
+    for (int k1 = 1; k1 < 16; k1++) v[k1] = cmul(v[k1], tw[(j * k1) & (kSide - 1)]);
+    pair_transpose(v, j);
+#pragma unroll
+    for (int c = 0; c < 2; c++) {
+        double2 x[8];
+#pragma unroll
+        for (int i = 0; i < 8; i++) x[i] = v[2 * i + c];
+        dft8<false>(x);
+#pragma unroll
+        for (int k2 = 0; k2 < 8; k2++) v[2 * k2 + c] = x[k2];
+    }
+}
+
+// Inverse line transform (unscaled) from the forward's output distribution back to x[j + 8 m] in v[m].
+__device__ __forceinline__ void line_inverse(double2 (&v)[16], int j, const double2 *tw) {
+#pragma unroll
+    for (int c = 0; c < 2; c++) {
+        double2 x[8];
+#pragma unroll
+        for (int k2 = 0; k2 < 8; k2++) x[k2] = v[2 * k2 + c];
+        dft8<true>(x);
+        const int k1 = 2 * j + c;
+        v[c] = x[0];
+#pragma unroll
+        for (int i = 1; i < 8; i++) v[2 * i + c] = cmul(x[i], cconj(tw[(i * k1) & (kSide - 1)]));
+    }
+    pair_transpose(v, j);
+    dft16<true>(v);
+}
+
+template <int Q>
+__global__ void __cluster_dims__(Q, 1, 1) __launch_bounds__(PlaneGeometry<Q>::kThreads, Q == 4 ? 2 : 1)
+    plane128_kernel(Plane128Args a) {
+    using G = PlaneGeometry<Q>;
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    double2 *buf = reinterpret_cast<double2 *>(smem_raw);
+    double2 *tw = buf + G::kBuffer;
+    double *warp_err = reinterpret_cast<double *>(tw + kSide);  // [32]
+    double *cluster_err = warp_err + 32;                        // [8], rank 0's copy is read
+    cg::cluster_group cluster = cg::this_cluster();
+    const int rank = (int)cluster.block_rank();
+    const int p = a.first + (int)(blockIdx.x / Q);
+    const int t = threadIdx.x, line = t >> 3, j = t & 7;
+    for (int i = t; i < kSide; i += G::kThreads) tw[i] = a.tw[i];
+    cluster.sync();  // the peers run (distributed shared memory is valid) and tw is in place
+
+    // ---- rows in: the input plane times the object patch
+    const int row = rank * G::kLines + line;
+    const double2 *src = a.in + (size_t)(a.in_by_class ? a.scan.cls[p] : p) * kPlane + (size_t)row * kSide;
+    double2 v[16];
+#pragma unroll
+    for (int m = 0; m < 16; m++) v[m] = src[j + 8 * m];
+    if (a.object) {
+        const int oy = wrap_once(a.scan.rr[p] + corner_offset(row, kSide), a.object_rows);
+        const double2 *orow = a.object + (size_t)oy * a.object_columns;
+        const int cc = a.scan.cc[p];
+#pragma unroll
+        for (int m = 0; m < 16; m++) {
+            double2 o = orow[wrap_once(cc + corner_offset(j + 8 * m, kSide), a.object_columns)];
+            if (a.conj_object) o.y = -o.y;
+            v[m] = cmul(v[m], o);
+        }
+    }
+    __syncthreads();  // tw visible to every thread
+    line_forward(v, j, tw);
+
+    // ---- rows -> columns: X[row][k] to the CTA holding column k, buffer [row][k mod kLines]
+    constexpr int kPerRank = G::kLines / 16;  // k2 values per destination CTA
+    double2 *dest[Q];
+#pragma unroll
+    for (int q = 0; q < Q; q++) dest[q] = cluster.map_shared_rank(buf, q);
+#pragma unroll
+    for (int k2 = 0; k2 < 8; k2++)
+#pragma unroll
+        for (int c = 0; c < 2; c++)
+            dest[k2 / kPerRank][row * G::kStrideA + 2 * j + c + 16 * (k2 % kPerRank)] = v[2 * k2 + c];
+    cluster.sync();
+    const int column = rank * G::kLines + line;
+#pragma unroll
+    for (int m = 0; m < 16; m++) v[m] = buf[(j + 8 * m) * G::kStrideA + line];
+    line_forward(v, j, tw);
+
+    // ---- the pointwise step on F[2 j + c + 16 k2][column]
+    double err = 0.0;
+    if (a.project) {
+        const float *amp = a.amplitudes + (size_t)p * kPlane + column;
+#pragma unroll
+        for (int k2 = 0; k2 < 8; k2++)
+#pragma unroll
+            for (int c = 0; c < 2; c++) {
+                const int kr = 2 * j + c + 16 * k2;
+                const double2 f = v[2 * k2 + c];
+                const double mag = sqrt(f.x * f.x + f.y * f.y);
+                const double measured = (double)amp[(size_t)kr * kSide];
+                const double miss = measured - mag;
+                err += miss * miss;
+                if (mag > 0.0) {
+                    const double sc = (measured / mag - 1.0) * a.inv_n;
+                    v[2 * k2 + c] = make_double2(f.x * sc, f.y * sc);
+                } else {
+                    v[2 * k2 + c] = make_double2(measured * a.inv_n, 0.0);
+                }
+            }
+    } else {
+#pragma unroll
+        for (int k2 = 0; k2 < 8; k2++)
+#pragma unroll
+            for (int c = 0; c < 2; c++) {
+                const int kr = 2 * j + c + 16 * k2;
+                double2 w = a.prop[(size_t)kr * kSide + column];
+                if (a.conj_prop) w.y = -w.y;
+                const double2 u = cmul(v[2 * k2 + c], w);
+                v[2 * k2 + c] = make_double2(u.x * a.scale, u.y * a.scale);
+            }
+    }
+    line_inverse(v, j, tw);  // v[m] = column's value at row j + 8 m
+
+    if (a.project) {  // the position's squared error: warps, then the CTA in warp order, then ranks in order
+#pragma unroll
+        for (int o = 16; o > 0; o >>= 1) err += __shfl_down_sync(0xffffffffu, err, o);
+        if ((t & 31) == 0) warp_err[t >> 5] = err;
+        __syncthreads();
+        if (t == 0) {
+            double total = 0.0;
+            for (int w = 0; w < G::kThreads / 32; w++) total += warp_err[w];
+            *cluster.map_shared_rank(cluster_err + rank, 0) = total;
+        }
+    }
+    cluster.sync();  // every CTA has read its columns: the buffers take the second exchange
+
+    // ---- columns -> rows: G[r][column] to the CTA holding row r, buffer [r mod kLines][column]
+    constexpr int kRowsPerRank = G::kLines / 8;  // m values per destination CTA
+#pragma unroll
+    for (int m = 0; m < 16; m++)
+        dest[m / kRowsPerRank][(j + 8 * (m % kRowsPerRank)) * G::kStrideB + column] = v[m];
+    cluster.sync();
+#pragma unroll
+    for (int k2 = 0; k2 < 8; k2++)
+#pragma unroll
+        for (int c = 0; c < 2; c++) v[2 * k2 + c] = buf[line * G::kStrideB + 2 * j + c + 16 * k2];
+    line_inverse(v, j, tw);
+    double2 *dst = a.out + (size_t)p * kPlane + (size_t)row * kSide;
+#pragma unroll
+    for (int m = 0; m < 16; m++) dst[j + 8 * m] = v[m];
+    if (a.project && rank == 0 && t == 0) {
+        double total = 0.0;
+        for (int q = 0; q < Q; q++) total += cluster_err[q];
+        a.error[p] = total;
+    }
+}
+
+template <int Q>
+cudaError_t launch_q(const Plane128Args &a, cudaStream_t s) {
+    using G = PlaneGeometry<Q>;
+    plane128_kernel<Q><<<(unsigned)a.count * Q, G::kThreads, G::kSmem, s>>>(a);
+    return cudaGetLastError();
+}
+
+}  // namespace
+
+// CTAs per plane: 2 (512 threads each, one CTA per SM) by default; CUBO_PTYCHO_PLANE_CLUSTER=4 selects four CTAs of
+// 256 threads (two per SM).  Either gives the same results bit for bit.
+int plane128_cluster() {
+    static const int q = [] {
+        const char *v = std::getenv("CUBO_PTYCHO_PLANE_CLUSTER");
+        return v && std::atoi(v) == 4 ? 4 : 2;
+    }();
+    return q;
+}
+
+cudaError_t configure_plane128() {
+    cudaError_t e = cudaFuncSetAttribute(plane128_kernel<2>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                         (int)PlaneGeometry<2>::kSmem);
+    if (e == cudaSuccess)
+        e = cudaFuncSetAttribute(plane128_kernel<4>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                 (int)PlaneGeometry<4>::kSmem);
+    return e;
+}
+
+cudaError_t launch_plane128(const Plane128Args &a, int cluster, cudaStream_t s) {
+    if (a.count <= 0) return cudaSuccess;
+    if (cluster == 4) return launch_q<4>(a, s);
+    if (cluster == 2) return launch_q<2>(a, s);
+    return cudaErrorInvalidValue;
+}
+
+}  // namespace cubo

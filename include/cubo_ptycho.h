@@ -103,7 +103,9 @@ typedef struct {
     cubo_ptycho_progress_fn progress;
     void *progress_user;
     /* Kernel choice: CUBO_PTYCHO_VARIANT_AUTO picks the specialised kernel for the detector size when there is one;
-     * CUBO_PTYCHO_VARIANT_GENERIC forces the any-size shared-memory transform (for cross-checks);
+     * CUBO_PTYCHO_VARIANT_GENERIC forces the any-size transforms (for cross-checks): the shared-memory one, and for
+     * FP64 planes larger than one CTA the batched line transform through global memory instead of the clustered
+     * 128 x 128 plane launch;
      * CUBO_PTYCHO_VARIANT_GLOBAL (FP64 form) forces the position pass through global memory that detectors too large
      * for one CTA's FP64 plane use (for cross-checks). */
     int variant;
