@@ -525,9 +525,10 @@ def run_multislice(args, world, rank, local):
     value = P * args.steps / (ms * 1e-3) * world
     hbm_peak, _, peak_kind = measured_peaks()
     pass_ms = stats["position_pass"][0] / timed_iterations
-    # algorithmic bytes of the forward pass: amplitudes read once (4n), the waves entering slices 1 .. L-1 and the
-    # last exit wave's residual written once each (16n per slice)
-    pass_bytes = P * (4 + 16 * slices) * n
+    # algorithmic bytes of the forward pass per pixel: slice 0 writes the wave entering slice 1 (16; the shifted probe
+    # and the object come from L2), slices 1 .. L-2 read their entering wave and write the next (32), the last slice
+    # reads its entering wave and the amplitude and writes the residual (36): 32 L - 12
+    pass_bytes = P * (32 * slices - 12) * n
     cpu = None
     if rank == 0 and not args.no_cpu:
         from oracle import numpy_oracle as no
@@ -549,12 +550,13 @@ def run_multislice(args, world, rank, local):
                                    f"{slices} slices {thickness:g} A apart, 300 kV, centre of mass",
                        "l2": f"amplitudes {P * n * 4 / 1e9:.1f} GB, entering waves and residuals "
                              f"{P * n * 16 * slices / 1e9:.0f} GB: far larger than L2"},
-            "roofline": {"kernel": "multislice forward pass (patch products, FP64 line FFTs, propagators, projection)",
+            "roofline": {"kernel": "multislice forward pass (one clustered plane launch per slice: patch product, "
+                                   "FP64 FFT, propagator or projection, inverse FFT)",
                          "bound": "hbm", "achieved": pass_bytes / (pass_ms * 1e-3) / 1e9, "peak": hbm_peak,
                          "unit": "GB/s", "frac": pass_bytes / (pass_ms * 1e-3) / 1e9 / hbm_peak,
                          "peak_kind": peak_kind, "launch_ms": pass_ms,
-                         "note": "each slice's waves go through HBM for every FFT pass (FP64 planes of 128^2 do "
-                                 "not fit one CTA)", "traffic": None},
+                         "note": "latency-bound: one 512-thread CTA per SM holds half a plane in registers; its "
+                                 "load, transform and store phases do not overlap", "traffic": None},
             "kernel_ms_per_iteration": per_kind, "errors_first_last": [errors[0], errors[-1]],
             "cpu_baseline": cpu, "e2e": None, "gpu_launches": launches, "clocks": clocks.summary()}), flush=True)
 

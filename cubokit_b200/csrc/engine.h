@@ -224,6 +224,7 @@ struct Plane128Args {
     double inv_n;
     const double2 *tw;              // W_128^k, k = 0..127 (forward sign)
     double2 *out;                   // plane of position p: out + p * 16384 (may be `in`)
+    int *fault;                     // set when the input copies' wait ran out
 };
 int plane128_cluster();
 cudaError_t configure_plane128();

@@ -450,7 +450,7 @@ void build_plan(cubo_ptycho_plan *p, const cubo_ptycho_problem *pr) {
     check(p->dpsi.alloc((size_t)p->states * P * n * sizeof(C2<T>)), "cudaMalloc dpsi");
     p->error_count = p->fast ? (long long)P * fast128_partials_per_position()
                              : p->bf16 ? (long long)P * bf16_partials_per_position() : P;
-    if (p->fast) {
+    if (p->fast || p->plane128) {
         check(p->fault.alloc(sizeof(int)), "cudaMalloc");
         check(cudaMemsetAsync(p->fault.ptr, 0, sizeof(int), s), "memset");
     }
@@ -526,7 +526,7 @@ Fft2Plan64 fft64(const cubo_ptycho_plan *p) {
 
 // After a synchronize: a device wait that ran out (split-BF16 kernel) turns into CUBO_PTYCHO_DEVICE_TIMEOUT.
 void check_fault(cubo_ptycho_plan *p) {
-    if (!p->bf16 && !p->fast) return;
+    if (!p->bf16 && !p->fast && !p->plane128) return;
     int f = 0;
     check(cudaMemcpy(&f, p->fault.ptr, sizeof(int), cudaMemcpyDeviceToHost), "read fault flag");
     if (f) {
@@ -664,6 +664,7 @@ void enqueue_plane128(cubo_ptycho_plan *p, Kind kind, const double2 *in, bool by
     a.object_rows = p->OR; a.object_columns = p->OC; a.project = project ? 1 : 0; a.prop = prop;
     a.conj_prop = conj_prop ? 1 : 0; a.scale = 1.0 / p->n; a.amplitudes = p->amplitudes.as<float>();
     a.error = p->error.as<double>(); a.inv_n = 1.0 / p->n; a.tw = p->tw_r64.as<double2>(); a.out = out;
+    a.fault = p->fault.as<int>();
     timed(p, kind, 1, [&] { return launch_plane128(a, p->plane_cluster, p->ctx->stream); });
 }
 

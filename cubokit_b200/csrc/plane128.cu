@@ -5,12 +5,13 @@
 //
 // Per line of 128 = 16 x 8 (n = j + 8 m, k = k1 + 16 k2), the eight threads j of a line each hold x[j + 8 m]:
 //   1. a 16-point DFT over m in registers, then the twiddle W_128^(j k1);
-//   2. an 8 x 8 transpose of pairs across the line's eight lanes (three xor-shuffle rounds);
+//   2. an 8 x 8 transpose of pairs across the line's eight lanes, through a swizzled per-warp shared-memory scratch;
 //   3. 8-point DFTs over j: thread j' then holds X[2 j' + c + 16 k2], c = 0, 1, k2 = 0 .. 7.
 // The inverse runs the same steps in the opposite order (from that distribution back to x[j + 8 m]), so the spectrum
 // never needs reordering: rows -> columns -> pointwise -> inverse columns -> inverse rows.
 //
-// The pointwise step is either the Fresnel propagator times a scale (multislice propagation, MultislicePtychography,
+// The CTA's input rows (contiguous in HBM) arrive by bulk asynchronous copies on an mbarrier; its output rows leave
+// the same way.  The pointwise step is either the Fresnel propagator times a scale (multislice propagation, MultislicePtychography,
 // PtychographyEngines.swift:503-545) or the modulus projection with the per-position squared error
 // (Ptychography.swift:327-349 and PtychographyEngines.swift:516-524).  The input can be multiplied by the object patch
 // of the position (or its conjugate) as it is read: the exit wave of the forward model, or chi x conj(O) of the
@@ -36,7 +37,8 @@ struct PlaneGeometry {
     static constexpr int kStrideA = kLines + 1;          // [128 rows][kLines columns] + 1 (conflict-free columns)
     static constexpr int kStrideB = kSide + 1;           // [kLines rows][128 columns] + 1
     static constexpr int kBuffer = (kSide * kStrideA > kLines * kStrideB) ? kSide * kStrideA : kLines * kStrideB;
-    static constexpr size_t kSmem = (size_t)(kBuffer + kSide) * sizeof(double2) + (32 + 8) * sizeof(double);
+    static constexpr int kTwiddles = 256;                // forward table [k1][j], inverse table [i][c][j]
+    static constexpr size_t kSmem = (size_t)(kBuffer + kTwiddles) * sizeof(double2) + (32 + 8 + 1) * sizeof(double);
 };
 
 __device__ __forceinline__ int wrap_once(int v, int n) { return v < 0 ? v + n : (v >= n ? v - n : v); }
@@ -104,36 +106,32 @@ __device__ __forceinline__ void dft16(double2 (&v)[16]) {
     for (int k = 0; k < 16; k++) v[k] = t[k];
 }
 
-// Thread j of a line holds blocks b = 0..7 (pairs v[2b], v[2b+1]); afterwards thread b holds what thread j had in
-// block b, in block j.  Three xor rounds over the line's eight consecutive lanes.
-__device__ __forceinline__ void pair_transpose(double2 (&v)[16], int j) {
+// Thread j of line lw (of the warp's four) holds blocks b = 0..7 (pairs v[2b], v[2b+1]); afterwards thread b holds
+// what thread j had in block b, in block j.  Through the warp's 512-entry scratch: row lw * 8 + j, column k stored at
+// k ^ (j ^ lw) (both the writes and the pair reads take the minimum four wavefronts).
+__device__ __forceinline__ void pair_transpose(double2 (&v)[16], int j, int lw, double2 *scratch) {
+    double2 *mine = scratch + (lw * 8 + j) * 16;
+    const int sw = j ^ lw;
 #pragma unroll
-    for (int mask = 1; mask < 8; mask <<= 1) {
-        const bool upper = (j & mask) != 0;
+    for (int k = 0; k < 16; k++) mine[k ^ sw] = v[k];
+    __syncwarp();
 #pragma unroll
-        for (int b = 0; b < 8; b++) {
-            if (b & mask) continue;
-            const int bp = b | mask;
+    for (int i = 0; i < 8; i++) {
+        const double2 *row = scratch + (lw * 8 + i) * 16;
+        const int si = i ^ lw;
 #pragma unroll
-            for (int c = 0; c < 2; c++) {
-                const double2 send = upper ? v[2 * b + c] : v[2 * bp + c];
-                double2 got;
-                got.x = __shfl_xor_sync(0xffffffffu, send.x, mask);
-                got.y = __shfl_xor_sync(0xffffffffu, send.y, mask);
-                if (upper) v[2 * b + c] = got;
-                else v[2 * bp + c] = got;
-            }
-        }
+        for (int c = 0; c < 2; c++) v[2 * i + c] = row[(2 * j + c) ^ si];
     }
+    __syncwarp();
 }
 
 // Forward line transform: thread j holds x[j + 8 m] in v[m]; afterwards thread j holds X[2 j + c + 16 k2] in
-// v[2 k2 + c].  tw = W_128^k (forward sign), k = 0..127.
-__device__ __forceinline__ void line_forward(double2 (&v)[16], int j, const double2 *tw) {
+// v[2 k2 + c].  tf[k1 * 8 + j] = W_128^(j k1).
+__device__ __forceinline__ void line_forward(double2 (&v)[16], int j, int lw, const double2 *tf, double2 *scratch) {
     dft16<false>(v);
 #pragma unroll
-    for (int k1 = 1; k1 < 16; k1++) v[k1] = cmul(v[k1], tw[(j * k1) & (kSide - 1)]);
-    pair_transpose(v, j);
+    for (int k1 = 1; k1 < 16; k1++) v[k1] = cmul(v[k1], tf[k1 * 8 + j]);
+    pair_transpose(v, j, lw, scratch);
 #pragma unroll
     for (int c = 0; c < 2; c++) {
         double2 x[8];
@@ -146,20 +144,36 @@ __device__ __forceinline__ void line_forward(double2 (&v)[16], int j, const doub
 }
 
 // Inverse line transform (unscaled) from the forward's output distribution back to x[j + 8 m] in v[m].
-__device__ __forceinline__ void line_inverse(double2 (&v)[16], int j, const double2 *tw) {
+// ti[(i * 2 + c) * 8 + j] = W_128^(-i (2 j + c)).
+__device__ __forceinline__ void line_inverse(double2 (&v)[16], int j, int lw, const double2 *ti, double2 *scratch) {
 #pragma unroll
     for (int c = 0; c < 2; c++) {
         double2 x[8];
 #pragma unroll
         for (int k2 = 0; k2 < 8; k2++) x[k2] = v[2 * k2 + c];
         dft8<true>(x);
-        const int k1 = 2 * j + c;
         v[c] = x[0];
 #pragma unroll
-        for (int i = 1; i < 8; i++) v[2 * i + c] = cmul(x[i], cconj(tw[(i * k1) & (kSide - 1)]));
+        for (int i = 1; i < 8; i++) v[2 * i + c] = cmul(x[i], ti[(i * 2 + c) * 8 + j]);
     }
-    pair_transpose(v, j);
+    pair_transpose(v, j, lw, scratch);
     dft16<true>(v);
+}
+
+__device__ __forceinline__ uint32_t smem_address(const void *p) { return (uint32_t)__cvta_generic_to_shared(p); }
+
+__device__ __forceinline__ bool mbarrier_try_wait(uint64_t *bar, uint32_t phase) {
+    uint32_t ok;
+    asm volatile("{\n\t.reg .pred p;\n\tmbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n\tselp.u32 %0, 1, 0, p;\n\t}"
+                 : "=r"(ok) : "r"(smem_address(bar)), "r"(phase) : "memory");
+    return ok != 0;
+}
+
+// Waits for phase 0 of `bar` a bounded number of times; false if it did not complete.
+__device__ __forceinline__ bool mbarrier_wait_bounded(uint64_t *bar) {
+    for (int i = 0; i < (1 << 22); i++)
+        if (mbarrier_try_wait(bar, 0)) return true;
+    return false;
 }
 
 template <int Q>
@@ -168,23 +182,49 @@ __global__ void __cluster_dims__(Q, 1, 1) __launch_bounds__(PlaneGeometry<Q>::kT
     using G = PlaneGeometry<Q>;
     extern __shared__ __align__(16) unsigned char smem_raw[];
     double2 *buf = reinterpret_cast<double2 *>(smem_raw);
-    double2 *tw = buf + G::kBuffer;
-    double *warp_err = reinterpret_cast<double *>(tw + kSide);  // [32]
-    double *cluster_err = warp_err + 32;                        // [8], rank 0's copy is read
+    double2 *tf = buf + G::kBuffer;       // [k1][j] W_128^(j k1)
+    double2 *ti = tf + 128;               // [i][c][j] W_128^(-i (2 j + c))
+    double *warp_err = reinterpret_cast<double *>(ti + 128);  // [32]
+    double *cluster_err = warp_err + 32;                       // [8], rank 0's copy is read
+    uint64_t *input_ready = reinterpret_cast<uint64_t *>(cluster_err + 8);
     cg::cluster_group cluster = cg::this_cluster();
     const int rank = (int)cluster.block_rank();
     const int p = a.first + (int)(blockIdx.x / Q);
-    const int t = threadIdx.x, line = t >> 3, j = t & 7;
-    for (int i = t; i < kSide; i += G::kThreads) tw[i] = a.tw[i];
-    cluster.sync();  // the peers run (distributed shared memory is valid) and tw is in place
-
-    // ---- rows in: the input plane times the object patch
+    const int t = threadIdx.x, line = t >> 3, j = t & 7, lw = (t >> 3) & 3;
+    double2 *scratch = buf + (t >> 5) * 512;  // the warp's four lines of 128 = its transpose scratch
     const int row = rank * G::kLines + line;
-    const double2 *src = a.in + (size_t)(a.in_by_class ? a.scan.cls[p] : p) * kPlane + (size_t)row * kSide;
+    const size_t plane_in = (size_t)(a.in_by_class ? a.scan.cls[p] : p) * kPlane;
+
+    // ---- the CTA's kLines input rows (contiguous) into buf[line][128] by bulk copies
+    constexpr uint32_t kInputBytes = G::kLines * kSide * sizeof(double2), kChunk = 16384;
+    if (t == 0) {
+        asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" ::"r"(smem_address(input_ready)) : "memory");
+        asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+        asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;"
+                     ::"r"(smem_address(input_ready)), "r"(kInputBytes) : "memory");
+        const double2 *src = a.in + plane_in + (size_t)rank * G::kLines * kSide;
+        for (uint32_t off = 0; off < kInputBytes; off += kChunk)
+            asm volatile("cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];"
+                         ::"r"(smem_address(buf) + off), "l"(reinterpret_cast<const char *>(src) + off), "r"(kChunk),
+                         "r"(smem_address(input_ready))
+                         : "memory");
+    }
+    for (int i = t; i < 128; i += G::kThreads) {
+        const int k1 = i >> 3, jj = i & 7;
+        tf[i] = a.tw[(jj * k1) & (kSide - 1)];
+        const int ii = i >> 4, c = (i >> 3) & 1;
+        ti[i] = cconj(a.tw[(ii * (2 * jj + c)) & (kSide - 1)]);
+    }
+    __syncthreads();  // the mbarrier is initialised and the tables are in place
+    bool arrived = mbarrier_wait_bounded(input_ready);
+    if (!arrived) {
+        atomicOr(a.fault, 1);
+        arrived = mbarrier_wait_bounded(input_ready);  // the copies land before the buffer is reused, or give up
+    }
     double2 v[16];
 #pragma unroll
-    for (int m = 0; m < 16; m++) v[m] = src[j + 8 * m];
-    if (a.object) {
+    for (int m = 0; m < 16; m++) v[m] = buf[line * kSide + j + 8 * m];
+    if (a.object) {  // times the object patch (conjugated), read from L2
         const int oy = wrap_once(a.scan.rr[p] + corner_offset(row, kSide), a.object_rows);
         const double2 *orow = a.object + (size_t)oy * a.object_columns;
         const int cc = a.scan.cc[p];
@@ -195,24 +235,26 @@ __global__ void __cluster_dims__(Q, 1, 1) __launch_bounds__(PlaneGeometry<Q>::kT
             v[m] = cmul(v[m], o);
         }
     }
-    __syncthreads();  // tw visible to every thread
-    line_forward(v, j, tw);
+    __syncwarp();  // the warp's input rows are read: the same region is its scratch
+    line_forward(v, j, lw, tf, scratch);
 
     // ---- rows -> columns: X[row][k] to the CTA holding column k, buffer [row][k mod kLines]
+    cluster.sync();  // every CTA has finished with its input and scratch (and runs): the buffers take the exchange
     constexpr int kPerRank = G::kLines / 16;  // k2 values per destination CTA
-    double2 *dest[Q];
 #pragma unroll
-    for (int q = 0; q < Q; q++) dest[q] = cluster.map_shared_rank(buf, q);
+    for (int q = 0; q < Q; q++) {
+        double2 *dest = cluster.map_shared_rank(buf, q) + row * G::kStrideA + 2 * j;
 #pragma unroll
-    for (int k2 = 0; k2 < 8; k2++)
+        for (int k2 = q * kPerRank; k2 < (q + 1) * kPerRank; k2++)
 #pragma unroll
-        for (int c = 0; c < 2; c++)
-            dest[k2 / kPerRank][row * G::kStrideA + 2 * j + c + 16 * (k2 % kPerRank)] = v[2 * k2 + c];
+            for (int c = 0; c < 2; c++) dest[c + 16 * (k2 % kPerRank)] = v[2 * k2 + c];
+    }
     cluster.sync();
     const int column = rank * G::kLines + line;
 #pragma unroll
     for (int m = 0; m < 16; m++) v[m] = buf[(j + 8 * m) * G::kStrideA + line];
-    line_forward(v, j, tw);
+    __syncthreads();  // the columns are read: buf is scratch until the next exchange
+    line_forward(v, j, lw, tf, scratch);
 
     // ---- the pointwise step on F[2 j + c + 16 k2][column]
     double err = 0.0;
@@ -247,7 +289,7 @@ __global__ void __cluster_dims__(Q, 1, 1) __launch_bounds__(PlaneGeometry<Q>::kT
                 v[2 * k2 + c] = make_double2(u.x * a.scale, u.y * a.scale);
             }
     }
-    line_inverse(v, j, tw);  // v[m] = column's value at row j + 8 m
+    line_inverse(v, j, lw, ti, scratch);  // v[m] = column's value at row j + 8 m
 
     if (a.project) {  // the position's squared error: warps, then the CTA in warp order, then ranks in order
 #pragma unroll
@@ -260,26 +302,42 @@ __global__ void __cluster_dims__(Q, 1, 1) __launch_bounds__(PlaneGeometry<Q>::kT
             *cluster.map_shared_rank(cluster_err + rank, 0) = total;
         }
     }
-    cluster.sync();  // every CTA has read its columns: the buffers take the second exchange
+    cluster.sync();  // every CTA is done with its scratch: the buffers take the second exchange
 
     // ---- columns -> rows: G[r][column] to the CTA holding row r, buffer [r mod kLines][column]
     constexpr int kRowsPerRank = G::kLines / 8;  // m values per destination CTA
 #pragma unroll
-    for (int m = 0; m < 16; m++)
-        dest[m / kRowsPerRank][(j + 8 * (m % kRowsPerRank)) * G::kStrideB + column] = v[m];
+    for (int q = 0; q < Q; q++) {
+        double2 *dest = cluster.map_shared_rank(buf, q) + j * G::kStrideB + column;
+#pragma unroll
+        for (int m = q * kRowsPerRank; m < (q + 1) * kRowsPerRank; m++)
+            dest[8 * (m % kRowsPerRank) * G::kStrideB] = v[m];
+    }
     cluster.sync();
 #pragma unroll
     for (int k2 = 0; k2 < 8; k2++)
 #pragma unroll
         for (int c = 0; c < 2; c++) v[2 * k2 + c] = buf[line * G::kStrideB + 2 * j + c + 16 * k2];
-    line_inverse(v, j, tw);
-    double2 *dst = a.out + (size_t)p * kPlane + (size_t)row * kSide;
+    __syncthreads();  // the rows are read: buf is scratch, then the output rows
+    line_inverse(v, j, lw, ti, scratch);
+
+    // ---- the output rows: buf[line][128] (the warp's own region), then bulk copies to HBM
 #pragma unroll
-    for (int m = 0; m < 16; m++) dst[j + 8 * m] = v[m];
-    if (a.project && rank == 0 && t == 0) {
-        double total = 0.0;
-        for (int q = 0; q < Q; q++) total += cluster_err[q];
-        a.error[p] = total;
+    for (int m = 0; m < 16; m++) buf[line * kSide + j + 8 * m] = v[m];
+    asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+    __syncthreads();
+    if (t == 0) {
+        char *dst = reinterpret_cast<char *>(a.out + (size_t)p * kPlane + (size_t)rank * G::kLines * kSide);
+        for (uint32_t off = 0; off < kInputBytes; off += kChunk)
+            asm volatile("cp.async.bulk.global.shared::cta.bulk_group [%0], [%1], %2;"
+                         ::"l"(dst + off), "r"(smem_address(buf) + off), "r"(kChunk) : "memory");
+        asm volatile("cp.async.bulk.commit_group;" ::: "memory");
+        if (a.project && rank == 0) {
+            double total = 0.0;
+            for (int q = 0; q < Q; q++) total += cluster_err[q];
+            a.error[p] = total;
+        }
+        asm volatile("cp.async.bulk.wait_group.read 0;" ::: "memory");
     }
 }
 
