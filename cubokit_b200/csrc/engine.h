@@ -216,7 +216,8 @@ struct Plane128Args {
     ScanTables scan;
     int object_rows, object_columns;
     int project;                    // 1: modulus projection with amplitudes (x inv_n) and error[p]; 0: x prop x scale
-    const double2 *prop;            // [128 x 128], conjugated when conj_prop
+    const double2 *prop_rows;       // the propagator as prop_rows[row frequency] x prop_columns[column frequency],
+    const double2 *prop_columns;    // 128 values each (a Fresnel kernel factors so), both conjugated when conj_prop
     int conj_prop;
     double scale;
     const float *amplitudes;        // [positions][128 x 128]
@@ -225,6 +226,7 @@ struct Plane128Args {
     const double2 *tw;              // W_128^k, k = 0..127 (forward sign)
     double2 *out;                   // plane of position p: out + p * 16384 (may be `in`)
     int *fault;                     // set when the input copies' wait ran out
+    int ahead;                      // L2 prefetch distance in planes (0: the clusters resident at once)
 };
 int plane128_cluster();
 cudaError_t configure_plane128();

@@ -168,6 +168,7 @@ struct cubo_ptycho_plan {
     DeviceBuffer positions64, initial64, object_before, far64, position_bad, fractions64;
     DeviceBuffer gram64, mixing64, ortho64;
     DeviceBuffer waves64, props64, ident, slice_max;  // multislice: entering waves, propagators, identity classes
+    DeviceBuffer prop_factors64;  // multislice, 128 x 128 planes: per gap the row and the column factor (128 + 128)
     DeviceBuffer tile_counts;          // position correction: candidate counts per tile, rebuilt on the device
     long long tile_capacity = 0;       // entries the candidate list holds
 
@@ -657,11 +658,12 @@ void enqueue_probe_side(cubo_ptycho_plan *p) {
 // (conjugated), FFT, the propagator `prop` x scale (project == false) or the modulus projection with the error
 // (project == true), inverse FFT, into `out`.
 void enqueue_plane128(cubo_ptycho_plan *p, Kind kind, const double2 *in, bool by_class, const double2 *object,
-                      bool conj_object, bool project, const double2 *prop, bool conj_prop, double2 *out) {
+                      bool conj_object, bool project, const double2 *prop_factors, bool conj_prop, double2 *out) {
     Plane128Args a{};
     a.first = 0; a.count = p->P; a.in = in; a.in_by_class = by_class ? 1 : 0; a.object = object;
     a.conj_object = conj_object ? 1 : 0; a.scan = ScanTables{p->rr.as<int>(), p->cc.as<int>(), p->cls.as<int>()};
-    a.object_rows = p->OR; a.object_columns = p->OC; a.project = project ? 1 : 0; a.prop = prop;
+    a.object_rows = p->OR; a.object_columns = p->OC; a.project = project ? 1 : 0;
+    a.prop_rows = prop_factors; a.prop_columns = prop_factors ? prop_factors + 128 : nullptr;
     a.conj_prop = conj_prop ? 1 : 0; a.scale = 1.0 / p->n; a.amplitudes = p->amplitudes.as<float>();
     a.error = p->error.as<double>(); a.inv_n = 1.0 / p->n; a.tw = p->tw_r64.as<double2>(); a.out = out;
     a.fault = p->fault.as<int>();
@@ -838,6 +840,7 @@ void enqueue_multislice_iteration(cubo_ptycho_plan *p) {
     const ScanTables own{p->rr.as<int>(), p->cc.as<int>(), p->ident.as<int>()};  // class p = position p
     double2 *obj = p->object.as<double2>(), *chi = p->dpsi.as<double2>(), *waves = p->waves64.as<double2>();
     const double2 *shifted = p->shifted.as<double2>(), *props = p->props64.as<double2>();
+    const double2 *factors = p->prop_factors64.as<double2>();
     const Fft2Plan64 f = fft64(p);
     enqueue_shift_table<double>(p);
     if (p->plane128) {  // forward and detector, one plane launch per slice
@@ -845,7 +848,7 @@ void enqueue_multislice_iteration(cubo_ptycho_plan *p) {
             const double2 *in = sl == 0 ? shifted : waves + (size_t)(sl - 1) * planes;
             const bool last = sl == L - 1;
             enqueue_plane128(p, kPositionPass, in, sl == 0, obj + (size_t)sl * plane, false, last,
-                             last ? nullptr : props + (size_t)sl * n, false, last ? chi : waves + (size_t)sl * planes);
+                             last ? nullptr : factors + (size_t)sl * 256, false, last ? chi : waves + (size_t)sl * planes);
         }
     } else {
     // forward (:503-515): exit_s = wave_s x O_s; wave_{s+1} = IFFT(FFT(exit_s) x prop_s / n)
@@ -894,7 +897,7 @@ void enqueue_multislice_iteration(cubo_ptycho_plan *p) {
         if (sl == 0) break;
         if (p->plane128) {
             enqueue_plane128(p, kBackPropagation, chi, false, obj + (size_t)sl * plane, true, false,
-                             props + (size_t)(sl - 1) * n, true, chi);
+                             factors + (size_t)(sl - 1) * 256, true, chi);
             continue;
         }
         timed(p, kBackPropagation, 6, [&] {
@@ -1113,6 +1116,27 @@ std::vector<double2> fresnel_propagators(int rows, int columns, double row_sampl
     return out;
 }
 
+// The same kernels as separable factors: exp(-i pi lambda dz kr^2) per row frequency and exp(-i pi lambda dz kc^2)
+// per column frequency, [thickness][rows + columns]; their product is the propagator.
+std::vector<double2> fresnel_factors(int rows, int columns, double row_sampling, double column_sampling,
+                                     double wavelength, int count, const double *thicknesses) {
+    std::vector<double2> out((size_t)count * (rows + columns));
+    for (int i = 0; i < count; i++) {
+        double2 *f = out.data() + (size_t)i * (rows + columns);
+        for (int r = 0; r < rows; r++) {
+            const double kr = frequency(r, rows) / row_sampling;
+            const double phase = -kPi * wavelength * thicknesses[i] * (kr * kr);
+            f[r] = make_double2(std::cos(phase), std::sin(phase));
+        }
+        for (int c = 0; c < columns; c++) {
+            const double kc = frequency(c, columns) / column_sampling;
+            const double phase = -kPi * wavelength * thicknesses[i] * (kc * kc);
+            f[rows + c] = make_double2(std::cos(phase), std::sin(phase));
+        }
+    }
+    return out;
+}
+
 int create_plan(cubo_ptycho_context *ctx, const cubo_ptycho_problem *pr, const cubo_ptycho_params *pp,
                 const cubo_ptycho_mixed_params *mixed, const cubo_ptycho_multislice_params *multi,
                 cubo_ptycho_plan **out) {
@@ -1204,7 +1228,14 @@ int create_plan(cubo_ptycho_context *ctx, const cubo_ptycho_problem *pr, const c
         p->correct_positions = pp->has_position_correction != 0;  // before the scan tables: one class per position
         if (p->fp64) build_plan<double>(p, pr);
         else build_plan<float>(p, pr);
-        if (p->multislice && p->slices > 1) upload(p->props64, props, ctx->stream);
+        if (p->multislice && p->slices > 1) {
+            upload(p->props64, props, ctx->stream);
+            if (p->plane128)
+                upload(p->prop_factors64,
+                       fresnel_factors(p->R, p->C, multi->row_sampling, multi->column_sampling, multi->wavelength,
+                                       p->slices - 1, multi->slice_thicknesses),
+                       ctx->stream);
+        }
         p->positions_given.resize((size_t)2 * p->P);
         std::copy(pr->position_rows, pr->position_rows + p->P, p->positions_given.begin());
         std::copy(pr->position_columns, pr->position_columns + p->P, p->positions_given.begin() + p->P);

@@ -37,8 +37,10 @@ struct PlaneGeometry {
     static constexpr int kStrideA = kLines + 1;          // [128 rows][kLines columns] + 1 (conflict-free columns)
     static constexpr int kStrideB = kSide + 1;           // [kLines rows][128 columns] + 1
     static constexpr int kBuffer = (kSide * kStrideA > kLines * kStrideB) ? kSide * kStrideA : kLines * kStrideB;
-    static constexpr int kTwiddles = 256;                // forward table [k1][j], inverse table [i][c][j]
-    static constexpr size_t kSmem = (size_t)(kBuffer + kTwiddles) * sizeof(double2) + (32 + 8 + 1) * sizeof(double);
+    static constexpr int kTables = 512;                  // twiddles [k1][j] and [i][c][j], propagator factors
+    static constexpr int kAmpStride = kLines + 4;        // amplitude rows of the CTA's columns (16-byte rows)
+    static constexpr size_t kSmem = (size_t)(kBuffer + kTables) * sizeof(double2) +
+                                    (size_t)kSide * kAmpStride * sizeof(float) + (32 + 8 + 2) * sizeof(double);
 };
 
 __device__ __forceinline__ int wrap_once(int v, int n) { return v < 0 ? v + n : (v >= n ? v - n : v); }
@@ -169,6 +171,17 @@ __device__ __forceinline__ bool mbarrier_try_wait(uint64_t *bar, uint32_t phase)
     return ok != 0;
 }
 
+// The shared::cluster address of `local` (this CTA's shared memory) in CTA `rank` of the cluster.
+__device__ __forceinline__ uint32_t cluster_address(uint32_t local, int rank) {
+    uint32_t out;
+    asm volatile("mapa.shared::cluster.u32 %0, %1, %2;" : "=r"(out) : "r"(local), "r"(rank));
+    return out;
+}
+
+__device__ __forceinline__ void store_cluster(uint32_t address, double2 v) {
+    asm volatile("st.shared::cluster.v2.f64 [%0], {%1, %2};" ::"r"(address), "d"(v.x), "d"(v.y) : "memory");
+}
+
 // Waits for phase 0 of `bar` a bounded number of times; false if it did not complete.
 __device__ __forceinline__ bool mbarrier_wait_bounded(uint64_t *bar) {
     for (int i = 0; i < (1 << 22); i++)
@@ -184,38 +197,94 @@ __global__ void __cluster_dims__(Q, 1, 1) __launch_bounds__(PlaneGeometry<Q>::kT
     double2 *buf = reinterpret_cast<double2 *>(smem_raw);
     double2 *tf = buf + G::kBuffer;       // [k1][j] W_128^(j k1)
     double2 *ti = tf + 128;               // [i][c][j] W_128^(-i (2 j + c))
-    double *warp_err = reinterpret_cast<double *>(ti + 128);  // [32]
-    double *cluster_err = warp_err + 32;                       // [8], rank 0's copy is read
+    double2 *pr = ti + 128;               // propagator factor of the row frequency (conjugated when asked)
+    double2 *pc = pr + 128;               // of the column frequency
+    float *amp = reinterpret_cast<float *>(pc + 128);  // [frequency row][kAmpStride]: the CTA's columns
+    double *warp_err = reinterpret_cast<double *>(amp + kSide * G::kAmpStride);  // [32]
+    double *cluster_err = warp_err + 32;                                          // [8], rank 0's copy is read
     uint64_t *input_ready = reinterpret_cast<uint64_t *>(cluster_err + 8);
+    uint64_t *amp_ready = input_ready + 1;
     cg::cluster_group cluster = cg::this_cluster();
     const int rank = (int)cluster.block_rank();
     const int p = a.first + (int)(blockIdx.x / Q);
     const int t = threadIdx.x, line = t >> 3, j = t & 7, lw = (t >> 3) & 3;
     double2 *scratch = buf + (t >> 5) * 512;  // the warp's four lines of 128 = its transpose scratch
-    const int row = rank * G::kLines + line;
-    const size_t plane_in = (size_t)(a.in_by_class ? a.scan.cls[p] : p) * kPlane;
-
-    // ---- the CTA's kLines input rows (contiguous) into buf[line][128] by bulk copies
+    const int row = rank * G::kLines + line, column = rank * G::kLines + line;
     constexpr uint32_t kInputBytes = G::kLines * kSide * sizeof(double2), kChunk = 16384;
+    constexpr uint32_t kAmpRowBytes = G::kLines * sizeof(float);
+
     if (t == 0) {
         asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" ::"r"(smem_address(input_ready)) : "memory");
+        asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" ::"r"(smem_address(amp_ready)) : "memory");
         asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
-        asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;"
-                     ::"r"(smem_address(input_ready)), "r"(kInputBytes) : "memory");
-        const double2 *src = a.in + plane_in + (size_t)rank * G::kLines * kSide;
-        for (uint32_t off = 0; off < kInputBytes; off += kChunk)
-            asm volatile("cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];"
-                         ::"r"(smem_address(buf) + off), "l"(reinterpret_cast<const char *>(src) + off), "r"(kChunk),
-                         "r"(smem_address(input_ready))
-                         : "memory");
     }
     for (int i = t; i < 128; i += G::kThreads) {
         const int k1 = i >> 3, jj = i & 7;
         tf[i] = a.tw[(jj * k1) & (kSide - 1)];
         const int ii = i >> 4, c = (i >> 3) & 1;
         ti[i] = cconj(a.tw[(ii * (2 * jj + c)) & (kSide - 1)]);
+        if (!a.project) {
+            double2 r = a.prop_rows[i], q = a.prop_columns[i];
+            if (a.conj_prop) { r.y = -r.y; q.y = -q.y; }
+            pr[i] = r;
+            pc[i] = q;
+        }
     }
-    __syncthreads();  // the mbarrier is initialised and the tables are in place
+    __syncthreads();  // the mbarriers are initialised
+
+    // ---- bulk copies: the CTA's kLines input rows (contiguous) into buf[line][128]; for the projection, the
+    // amplitudes of its columns into amp; an L2 prefetch of what the cluster `ahead` planes further will read
+    if (t < 32) {
+        if (t == 0) {
+            asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;"
+                         ::"r"(smem_address(input_ready)), "r"(kInputBytes) : "memory");
+            if (a.project)
+                asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;"
+                             ::"r"(smem_address(amp_ready)), "r"(kSide * kAmpRowBytes) : "memory");
+        }
+        __syncwarp();
+        if (t == 0) {
+            const double2 *src =
+                a.in + (size_t)(a.in_by_class ? a.scan.cls[p] : p) * kPlane + (size_t)rank * G::kLines * kSide;
+            for (uint32_t off = 0; off < kInputBytes; off += kChunk)
+                asm volatile("cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];"
+                             ::"r"(smem_address(buf) + off), "l"(reinterpret_cast<const char *>(src) + off),
+                             "r"(kChunk), "r"(smem_address(input_ready))
+                             : "memory");
+            const int next = p + a.ahead;
+            if (a.ahead > 0 && next < a.first + a.count) {
+                if (!a.in_by_class)
+                    asm volatile("cp.async.bulk.prefetch.L2.global [%0], %1;"
+                                 ::"l"(a.in + (size_t)next * kPlane + (size_t)rank * G::kLines * kSide),
+                                 "r"(kInputBytes) : "memory");
+                if (a.project && rank == 0)
+                    asm volatile("cp.async.bulk.prefetch.L2.global [%0], %1;"
+                                 ::"l"(a.amplitudes + (size_t)next * kPlane), "r"((uint32_t)(kPlane * sizeof(float)))
+                                 : "memory");
+            }
+        }
+        if (a.project) {
+            for (int r = t; r < kSide; r += 32)
+                asm volatile("cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];"
+                             ::"r"(smem_address(amp + r * G::kAmpStride)),
+                             "l"(a.amplitudes + (size_t)p * kPlane + (size_t)r * kSide + rank * G::kLines),
+                             "r"(kAmpRowBytes), "r"(smem_address(amp_ready))
+                             : "memory");
+        }
+    }
+
+    // ---- the object patch (from L2) while the rows arrive, then the input times the patch
+    double2 o[16];
+    if (a.object) {
+        const int oy = wrap_once(a.scan.rr[p] + corner_offset(row, kSide), a.object_rows);
+        const double2 *orow = a.object + (size_t)oy * a.object_columns;
+        const int cc = a.scan.cc[p];
+#pragma unroll
+        for (int m = 0; m < 16; m++) {
+            o[m] = orow[wrap_once(cc + corner_offset(j + 8 * m, kSide), a.object_columns)];
+            if (a.conj_object) o[m].y = -o[m].y;
+        }
+    }
     bool arrived = mbarrier_wait_bounded(input_ready);
     if (!arrived) {
         atomicOr(a.fault, 1);
@@ -224,16 +293,9 @@ __global__ void __cluster_dims__(Q, 1, 1) __launch_bounds__(PlaneGeometry<Q>::kT
     double2 v[16];
 #pragma unroll
     for (int m = 0; m < 16; m++) v[m] = buf[line * kSide + j + 8 * m];
-    if (a.object) {  // times the object patch (conjugated), read from L2
-        const int oy = wrap_once(a.scan.rr[p] + corner_offset(row, kSide), a.object_rows);
-        const double2 *orow = a.object + (size_t)oy * a.object_columns;
-        const int cc = a.scan.cc[p];
+    if (a.object) {
 #pragma unroll
-        for (int m = 0; m < 16; m++) {
-            double2 o = orow[wrap_once(cc + corner_offset(j + 8 * m, kSide), a.object_columns)];
-            if (a.conj_object) o.y = -o.y;
-            v[m] = cmul(v[m], o);
-        }
+        for (int m = 0; m < 16; m++) v[m] = cmul(v[m], o[m]);
     }
     __syncwarp();  // the warp's input rows are read: the same region is its scratch
     line_forward(v, j, lw, tf, scratch);
@@ -241,16 +303,16 @@ __global__ void __cluster_dims__(Q, 1, 1) __launch_bounds__(PlaneGeometry<Q>::kT
     // ---- rows -> columns: X[row][k] to the CTA holding column k, buffer [row][k mod kLines]
     cluster.sync();  // every CTA has finished with its input and scratch (and runs): the buffers take the exchange
     constexpr int kPerRank = G::kLines / 16;  // k2 values per destination CTA
+    const uint32_t buf_local = smem_address(buf);
 #pragma unroll
     for (int q = 0; q < Q; q++) {
-        double2 *dest = cluster.map_shared_rank(buf, q) + row * G::kStrideA + 2 * j;
+        const uint32_t dest = cluster_address(buf_local, q) + (uint32_t)(row * G::kStrideA + 2 * j) * 16u;
 #pragma unroll
         for (int k2 = q * kPerRank; k2 < (q + 1) * kPerRank; k2++)
 #pragma unroll
-            for (int c = 0; c < 2; c++) dest[c + 16 * (k2 % kPerRank)] = v[2 * k2 + c];
+            for (int c = 0; c < 2; c++) store_cluster(dest + (uint32_t)(c + 16 * (k2 % kPerRank)) * 16u, v[2 * k2 + c]);
     }
     cluster.sync();
-    const int column = rank * G::kLines + line;
 #pragma unroll
     for (int m = 0; m < 16; m++) v[m] = buf[(j + 8 * m) * G::kStrideA + line];
     __syncthreads();  // the columns are read: buf is scratch until the next exchange
@@ -259,7 +321,11 @@ __global__ void __cluster_dims__(Q, 1, 1) __launch_bounds__(PlaneGeometry<Q>::kT
     // ---- the pointwise step on F[2 j + c + 16 k2][column]
     double err = 0.0;
     if (a.project) {
-        const float *amp = a.amplitudes + (size_t)p * kPlane + column;
+        bool landed = mbarrier_wait_bounded(amp_ready);
+        if (!landed) {
+            atomicOr(a.fault, 1);
+            landed = mbarrier_wait_bounded(amp_ready);
+        }
 #pragma unroll
         for (int k2 = 0; k2 < 8; k2++)
 #pragma unroll
@@ -267,7 +333,7 @@ __global__ void __cluster_dims__(Q, 1, 1) __launch_bounds__(PlaneGeometry<Q>::kT
                 const int kr = 2 * j + c + 16 * k2;
                 const double2 f = v[2 * k2 + c];
                 const double mag = sqrt(f.x * f.x + f.y * f.y);
-                const double measured = (double)amp[(size_t)kr * kSide];
+                const double measured = (double)amp[kr * G::kAmpStride + line];
                 const double miss = measured - mag;
                 err += miss * miss;
                 if (mag > 0.0) {
@@ -278,14 +344,12 @@ __global__ void __cluster_dims__(Q, 1, 1) __launch_bounds__(PlaneGeometry<Q>::kT
                 }
             }
     } else {
+        const double2 wc = pc[column];
 #pragma unroll
         for (int k2 = 0; k2 < 8; k2++)
 #pragma unroll
             for (int c = 0; c < 2; c++) {
-                const int kr = 2 * j + c + 16 * k2;
-                double2 w = a.prop[(size_t)kr * kSide + column];
-                if (a.conj_prop) w.y = -w.y;
-                const double2 u = cmul(v[2 * k2 + c], w);
+                const double2 u = cmul(v[2 * k2 + c], cmul(pr[2 * j + c + 16 * k2], wc));
                 v[2 * k2 + c] = make_double2(u.x * a.scale, u.y * a.scale);
             }
     }
@@ -293,7 +357,7 @@ __global__ void __cluster_dims__(Q, 1, 1) __launch_bounds__(PlaneGeometry<Q>::kT
 
     if (a.project) {  // the position's squared error: warps, then the CTA in warp order, then ranks in order
 #pragma unroll
-        for (int o = 16; o > 0; o >>= 1) err += __shfl_down_sync(0xffffffffu, err, o);
+        for (int o2 = 16; o2 > 0; o2 >>= 1) err += __shfl_down_sync(0xffffffffu, err, o2);
         if ((t & 31) == 0) warp_err[t >> 5] = err;
         __syncthreads();
         if (t == 0) {
@@ -308,10 +372,10 @@ __global__ void __cluster_dims__(Q, 1, 1) __launch_bounds__(PlaneGeometry<Q>::kT
     constexpr int kRowsPerRank = G::kLines / 8;  // m values per destination CTA
 #pragma unroll
     for (int q = 0; q < Q; q++) {
-        double2 *dest = cluster.map_shared_rank(buf, q) + j * G::kStrideB + column;
+        const uint32_t dest = cluster_address(buf_local, q) + (uint32_t)(j * G::kStrideB + column) * 16u;
 #pragma unroll
         for (int m = q * kRowsPerRank; m < (q + 1) * kRowsPerRank; m++)
-            dest[8 * (m % kRowsPerRank) * G::kStrideB] = v[m];
+            store_cluster(dest + (uint32_t)(8 * (m % kRowsPerRank) * G::kStrideB) * 16u, v[m]);
     }
     cluster.sync();
 #pragma unroll
@@ -342,8 +406,14 @@ __global__ void __cluster_dims__(Q, 1, 1) __launch_bounds__(PlaneGeometry<Q>::kT
 }
 
 template <int Q>
-cudaError_t launch_q(const Plane128Args &a, cudaStream_t s) {
+cudaError_t launch_q(Plane128Args a, cudaStream_t s) {
     using G = PlaneGeometry<Q>;
+    if (a.ahead == 0) {  // the clusters resident at once: the L2 prefetch distance
+        int device = 0, sms = 0;
+        cudaGetDevice(&device);
+        cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, device);
+        a.ahead = sms * (Q == 4 ? 2 : 1) / Q;
+    }
     plane128_kernel<Q><<<(unsigned)a.count * Q, G::kThreads, G::kSmem, s>>>(a);
     return cudaGetLastError();
 }
