@@ -204,28 +204,37 @@ cudaError_t launch_spectrum_multiply(double2 *data, long long planes, int n, con
 // identicalSlices: every slice becomes the mean of the slices.
 cudaError_t launch_average_slices(double2 *object, int slices, long long plane, cudaStream_t s);
 
-// plane128.cu: the 128 x 128 FP64 plane transform of positions first .. first + count - 1 in one launch: the input plane
-// (times the object patch) -> FFT -> the pointwise step -> inverse FFT (unscaled) -> out.  A cluster of
-// plane128_cluster() CTAs holds one plane.
+// plane128.cu: the 128 x 128 FP64 plane transform of positions first .. first + count - 1 in one launch, one cluster
+// of plane128_cluster() CTAs per plane.  kPlaneFull: the input plane (times the object patch) -> FFT -> the pointwise
+// step -> inverse FFT (unscaled) -> out; kPlaneForward: the input (times the patch) -> FFT -> out, unscaled;
+// kPlaneInverse: a spectrum -> the pointwise step -> inverse FFT (unscaled) -> out.
+enum { kPlaneFull = 0, kPlaneForward = 1, kPlaneInverse = 2 };
+enum { kInputByPosition = 0, kInputByClass = 1, kInputSingle = 2 };
+enum { kPointwiseNone = 0, kPointwiseFactors = 1, kPointwiseProjection = 2 };
 struct Plane128Args {
+    int mode;
     int first, count;
-    const double2 *in;              // plane of position p: in + (in_by_class ? scan.cls[p] : p) * 16384
-    int in_by_class;
-    const double2 *object;          // the object patch factor, conjugated when conj_object; null: none
+    const double2 *in;              // input plane of position p: in + (p, scan.cls[p] or 0 by in_kind) * 16384
+    int in_kind;
+    const double2 *object;          // full / forward: the object patch factor, conjugated when conj_object; null: none
     int conj_object;
+    int object_row_offset, object_column_offset;  // the patch one row / column further (position correction)
     ScanTables scan;
     int object_rows, object_columns;
-    int project;                    // 1: modulus projection with amplitudes (x inv_n) and error[p]; 0: x prop x scale
-    const double2 *prop_rows;       // the propagator as prop_rows[row frequency] x prop_columns[column frequency],
-    const double2 *prop_columns;    // 128 values each (a Fresnel kernel factors so), both conjugated when conj_prop
+    int pointwise;                  // kPointwiseFactors: x prop_rows[kr] prop_columns[kc] x scale; kPointwiseProjection
+                                    // (full mode): modulus projection with amplitudes (x inv_n) and error[p]
+    const double2 *prop_rows;       // 128 factors of the row frequency, then prop_stride further per position
+    const double2 *prop_columns;    // 128 of the column frequency; both conjugated when conj_prop
+    long long prop_stride;          // (a Fresnel kernel and the Fourier-shift ramps both factor so)
     int conj_prop;
     double scale;
     const float *amplitudes;        // [positions][128 x 128]
     double *error;                  // [positions] squared amplitude residual
     double inv_n;
     const double2 *tw;              // W_128^k, k = 0..127 (forward sign)
-    double2 *out;                   // plane of position p: out + p * 16384 (may be `in`)
-    int *fault;                     // set when the input copies' wait ran out
+    double2 *out;                   // output plane of position p: out + (p * out_stride + out_offset) * 16384
+    long long out_stride, out_offset;
+    int *fault;                     // set when a bulk copy's wait ran out
     int ahead;                      // L2 prefetch distance in planes (0: the clusters resident at once)
 };
 int plane128_cluster();
@@ -247,6 +256,10 @@ struct MixedPassArgs {
 };
 // Exit waves of every state, their far fields, the summed-intensity projection, the inverse transforms.
 cudaError_t launch_mixed_position_pass(const MixedPassArgs &a, const Fft2Plan64 &fft, int *launches, cudaStream_t s);
+// The summed-intensity projection alone, in place on the states' far fields dpsi[state][position][pixel] of `count`
+// positions (the inverse transform's 1/n folded in), the per-position error written.
+cudaError_t launch_mixed_project(double2 *dpsi, const float *amplitudes, int count, int states, int n,
+                                 bool zero_pixel_infinite, double *error, cudaStream_t s);
 // The states become the eigenvectors of their Gram matrix, by decreasing intensity (gram, mixing: states^2 values;
 // scratch: states * n).
 cudaError_t launch_orthogonalize(double2 *probes, int states, int n, double2 *gram, double2 *mixing, double2 *scratch,

@@ -32,6 +32,7 @@ struct cubo_ptycho_context {
 namespace {
 
 constexpr double kPi = 3.14159265358979323846;
+constexpr int kSide128 = 128;
 
 // --------------------------------------------------------------------------------------------- device buffers
 
@@ -550,6 +551,34 @@ void ensure_errors(cubo_ptycho_plan *p, long long needed) {
     p->errors_capacity = cap;
 }
 
+// A clustered 128 x 128 plane launch (FP64) over every position: the fields every use shares.
+Plane128Args plane_args(const cubo_ptycho_plan *p, int mode) {
+    Plane128Args a{};
+    a.mode = mode; a.first = 0; a.count = p->P; a.in_kind = kInputByPosition;
+    a.scan = ScanTables{p->rr.as<int>(), p->cc.as<int>(), p->cls.as<int>()};
+    a.object_rows = p->OR; a.object_columns = p->OC; a.pointwise = kPointwiseNone; a.scale = 1.0 / p->n;
+    a.amplitudes = p->amplitudes.as<float>(); a.error = p->error.as<double>(); a.inv_n = 1.0 / p->n;
+    a.tw = p->tw_r64.as<double2>(); a.out_stride = 1; a.out_offset = 0; a.fault = p->fault.as<int>();
+    return a;
+}
+
+void enqueue_plane(cubo_ptycho_plan *p, Kind kind, const Plane128Args &a) {
+    timed(p, kind, 1, [&] { return launch_plane128(a, p->plane_cluster, p->ctx->stream); });
+}
+
+// The full plane launch of every position: `in` (by class or by position) times the object patch (conjugated), FFT,
+// the propagator factors x 1/n (project == false) or the modulus projection with the error (project == true),
+// inverse FFT, into `out`.
+void enqueue_plane128(cubo_ptycho_plan *p, Kind kind, const double2 *in, bool by_class, const double2 *object,
+                      bool conj_object, bool project, const double2 *prop_factors, bool conj_prop, double2 *out) {
+    Plane128Args a = plane_args(p, kPlaneFull);
+    a.in = in; a.in_kind = by_class ? kInputByClass : kInputByPosition; a.object = object;
+    a.conj_object = conj_object ? 1 : 0; a.pointwise = project ? kPointwiseProjection : kPointwiseFactors;
+    a.prop_rows = prop_factors; a.prop_columns = prop_factors ? prop_factors + 128 : nullptr; a.prop_stride = 0;
+    a.conj_prop = conj_prop ? 1 : 0; a.out = out;
+    enqueue_plane(p, kind, a);
+}
+
 // The shift table of probe state `st`.
 template <typename T>
 void enqueue_shift_table_state(cubo_ptycho_plan *p, int st) {
@@ -559,6 +588,22 @@ void enqueue_shift_table_state(cubo_ptycho_plan *p, int st) {
     C2<T> *table = p->shifted.as<C2<T>>() + (size_t)st * p->classes * n;
     timed(p, kShiftTable, 1, [&] { return launch_convert<T>(probe, table, n, s); });
     if (frac == 0) return;
+    if constexpr (std::is_same<T, double>::value) {
+        if (p->plane128) {  // classes 1 .. frac: the probe's spectrum x the class's ramps, inverse FFT, one launch
+            timed(p, kShiftTable, 2, [&] {
+                cudaError_t e = cudaMemcpyAsync(p->spectrum64.ptr, probe, (size_t)n * sizeof(double2),
+                                                cudaMemcpyDeviceToDevice, s);
+                if (e == cudaSuccess) e = launch_fft2_f64(fft64(p), p->spectrum64.as<double2>(), 1, false, s);
+                return e;
+            });
+            Plane128Args a = plane_args(p, kPlaneInverse);
+            a.first = 1; a.count = frac; a.in = p->spectrum64.as<double2>(); a.in_kind = kInputSingle;
+            a.pointwise = kPointwiseFactors; a.prop_rows = p->ramps_r64.as<double2>();
+            a.prop_columns = p->ramps_c64.as<double2>(); a.prop_stride = kSide128; a.out = table;
+            enqueue_plane(p, kShiftTable, a);
+            return;
+        }
+    }
     timed(p, kShiftTable, 2 + 1 + 2 + 1 + 1, [&] {
         cudaError_t e = cudaMemcpyAsync(p->spectrum64.ptr, probe, (size_t)n * sizeof(double2),
                                         cudaMemcpyDeviceToDevice, s);
@@ -654,22 +699,6 @@ void enqueue_probe_side(cubo_ptycho_plan *p) {
         });
 }
 
-// The clustered 128 x 128 plane launch of every position: `in` (by class or by position) times the object patch
-// (conjugated), FFT, the propagator `prop` x scale (project == false) or the modulus projection with the error
-// (project == true), inverse FFT, into `out`.
-void enqueue_plane128(cubo_ptycho_plan *p, Kind kind, const double2 *in, bool by_class, const double2 *object,
-                      bool conj_object, bool project, const double2 *prop_factors, bool conj_prop, double2 *out) {
-    Plane128Args a{};
-    a.first = 0; a.count = p->P; a.in = in; a.in_by_class = by_class ? 1 : 0; a.object = object;
-    a.conj_object = conj_object ? 1 : 0; a.scan = ScanTables{p->rr.as<int>(), p->cc.as<int>(), p->cls.as<int>()};
-    a.object_rows = p->OR; a.object_columns = p->OC; a.project = project ? 1 : 0;
-    a.prop_rows = prop_factors; a.prop_columns = prop_factors ? prop_factors + 128 : nullptr;
-    a.conj_prop = conj_prop ? 1 : 0; a.scale = 1.0 / p->n; a.amplitudes = p->amplitudes.as<float>();
-    a.error = p->error.as<double>(); a.inv_n = 1.0 / p->n; a.tw = p->tw_r64.as<double2>(); a.out = out;
-    a.fault = p->fault.as<int>();
-    timed(p, kind, 1, [&] { return launch_plane128(a, p->plane_cluster, p->ctx->stream); });
-}
-
 // Shifted probes, then the position pass over every position: residuals (dpsi) and per-position squared errors.
 template <typename T>
 void enqueue_position_pass(cubo_ptycho_plan *p) {
@@ -700,6 +729,24 @@ void enqueue_position_pass(cubo_ptycho_plan *p) {
         fa.partial_grad = p->partial_grad.as<float2>(); fa.partial_weight = p->partial_weight.as<float>();
         fa.fault = p->fault.as<int>();
         timed(p, kPositionPass, 1, [&] { return launch_fast128(fa, p->sms, s); });
+    } else if (p->states > 1 && p->plane128) {
+        if constexpr (std::is_same<T, double>::value) {  // every state's far field, the summed projection, inverses
+            for (int st = 0; st < p->states; st++) {
+                Plane128Args a = plane_args(p, kPlaneForward);
+                a.in = p->shifted.as<double2>() + (size_t)st * p->classes * n; a.in_kind = kInputByClass;
+                a.object = p->object.as<double2>(); a.out = p->dpsi.as<double2>() + (size_t)st * p->P * n;
+                enqueue_plane(p, kPositionPass, a);
+            }
+            timed(p, kPositionPass, 1, [&] {
+                return launch_mixed_project(p->dpsi.as<double2>(), p->amplitudes.as<float>(), p->P, p->states, n,
+                                            p->zero_pixel_infinite, p->error.as<double>(), s);
+            });
+            for (int st = 0; st < p->states; st++) {
+                Plane128Args a = plane_args(p, kPlaneInverse);
+                a.in = p->dpsi.as<double2>() + (size_t)st * p->P * n; a.out = const_cast<double2 *>(a.in);
+                enqueue_plane(p, kPositionPass, a);
+            }
+        }
     } else if (p->states > 1) {
         if constexpr (std::is_same<T, double>::value) {
             MixedPassArgs ma{};
@@ -773,6 +820,23 @@ void enqueue_position_correction(cubo_ptycho_plan *p) {
     const ScanTables scan{p->rr.as<int>(), p->cc.as<int>(), p->cls.as<int>()};
     for (int first = 0; first < p->P; first += p->correction_chunk) {
         const int m = std::min(p->correction_chunk, p->P - first);
+        if (p->plane128) {  // the three far fields of each position, one forward plane launch each
+            for (int v = 0; v < 3; v++) {
+                Plane128Args a = plane_args(p, kPlaneForward);
+                a.first = first; a.count = m; a.in = p->shifted.as<double2>(); a.in_kind = kInputByClass;
+                a.object = v == 0 ? p->object_before.as<double2>() : p->object.as<double2>();
+                a.object_row_offset = v == 1 ? 1 : 0; a.object_column_offset = v == 2 ? 1 : 0;
+                a.out = p->far64.as<double2>(); a.out_stride = 3; a.out_offset = v - 3LL * first;
+                enqueue_plane(p, kPositionCorrection, a);
+            }
+            timed(p, kPositionCorrection, 1, [&] {
+                return launch_position_solve(p->far64.as<double2>(), p->amplitudes.as<float>(), first, m, p->n,
+                                             p->positions64.as<double>(), p->initial64.as<double>(), p->P,
+                                             p->params.position_step_size, p->limit_update, p->limit_total,
+                                             p->position_bad.as<int>(), s);
+            });
+            continue;
+        }
         timed(p, kPositionCorrection, 3, [&] {
             cudaError_t e = launch_position_exit_waves(p->shifted.as<double2>(), scan, p->object_before.as<double2>(),
                                                        p->object.as<double2>(), first, m, p->R, p->C, p->OR, p->OC,
@@ -1206,9 +1270,8 @@ int create_plan(cubo_ptycho_context *ctx, const cubo_ptycho_problem *pr, const c
         // FP64 planes too large for one CTA go through global memory (any size the line transform takes)
         p->global64 = p->fp64 && (!smem_pass || pp->variant == CUBO_PTYCHO_VARIANT_GLOBAL || p->states > 1 ||
                                   p->multislice);
-        // 128 x 128 FP64 planes of one probe state: the clustered plane launch (not with the generic variant)
-        p->plane128 = p->global64 && p->states == 1 && p->R == 128 && p->C == 128 &&
-                      pp->variant != CUBO_PTYCHO_VARIANT_GENERIC;
+        // 128 x 128 FP64 planes: the clustered plane launches (not with the generic variant)
+        p->plane128 = p->global64 && p->R == 128 && p->C == 128 && pp->variant != CUBO_PTYCHO_VARIANT_GENERIC;
         if (p->plane128) {
             check(configure_plane128(), "configure plane transform");
             p->plane_cluster = plane128_cluster();

@@ -1,5 +1,5 @@
 // The 128 x 128 FP64 plane transform: one position's plane through FFT -> a pointwise step -> inverse FFT in ONE
-// launch, read once from HBM and written once.  An FP64 plane of 128 x 128 (256 KB) is larger than one SM's shared
+// launch, read once from HBM and written once (or the forward FFT alone, or a pointwise step and the inverse alone).  An FP64 plane of 128 x 128 (256 KB) is larger than one SM's shared
 // memory, so a cluster of Q CTAs holds it: each CTA keeps 128 / Q rows in registers (16 complex values per thread,
 // eight threads per line), and the row / column redistributions go through distributed shared memory.
 //
@@ -189,7 +189,7 @@ __device__ __forceinline__ bool mbarrier_wait_bounded(uint64_t *bar) {
     return false;
 }
 
-template <int Q>
+template <int Q, int MODE>
 __global__ void __cluster_dims__(Q, 1, 1) __launch_bounds__(PlaneGeometry<Q>::kThreads, Q == 4 ? 2 : 1)
     plane128_kernel(Plane128Args a) {
     using G = PlaneGeometry<Q>;
@@ -197,7 +197,7 @@ __global__ void __cluster_dims__(Q, 1, 1) __launch_bounds__(PlaneGeometry<Q>::kT
     double2 *buf = reinterpret_cast<double2 *>(smem_raw);
     double2 *tf = buf + G::kBuffer;       // [k1][j] W_128^(j k1)
     double2 *ti = tf + 128;               // [i][c][j] W_128^(-i (2 j + c))
-    double2 *pr = ti + 128;               // propagator factor of the row frequency (conjugated when asked)
+    double2 *pr = ti + 128;               // factor of the row frequency (conjugated when asked)
     double2 *pc = pr + 128;               // of the column frequency
     float *amp = reinterpret_cast<float *>(pc + 128);  // [frequency row][kAmpStride]: the CTA's columns
     double *warp_err = reinterpret_cast<double *>(amp + kSide * G::kAmpStride);  // [32]
@@ -210,8 +210,13 @@ __global__ void __cluster_dims__(Q, 1, 1) __launch_bounds__(PlaneGeometry<Q>::kT
     const int t = threadIdx.x, line = t >> 3, j = t & 7, lw = (t >> 3) & 3;
     double2 *scratch = buf + (t >> 5) * 512;  // the warp's four lines of 128 = its transpose scratch
     const int row = rank * G::kLines + line, column = rank * G::kLines + line;
-    constexpr uint32_t kInputBytes = G::kLines * kSide * sizeof(double2), kChunk = 16384;
-    constexpr uint32_t kAmpRowBytes = G::kLines * sizeof(float);
+    const bool project = MODE == kPlaneFull && a.pointwise == kPointwiseProjection;
+    const bool factors = MODE != kPlaneForward && a.pointwise == kPointwiseFactors;
+    constexpr uint32_t kHalfBytes = G::kLines * kSide * sizeof(double2), kChunk = 16384;
+    constexpr uint32_t kAmpRowBytes = G::kLines * sizeof(float), kSpanBytes = G::kLines * sizeof(double2);
+    const size_t in_plane = (size_t)(a.in_kind == kInputByClass ? a.scan.cls[p] : a.in_kind == kInputSingle ? 0 : p) *
+                            kPlane;
+    double2 *const out_plane = a.out + (size_t)((long long)p * a.out_stride + a.out_offset) * kPlane;
 
     if (t == 0) {
         asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" ::"r"(smem_address(input_ready)) : "memory");
@@ -223,8 +228,9 @@ __global__ void __cluster_dims__(Q, 1, 1) __launch_bounds__(PlaneGeometry<Q>::kT
         tf[i] = a.tw[(jj * k1) & (kSide - 1)];
         const int ii = i >> 4, c = (i >> 3) & 1;
         ti[i] = cconj(a.tw[(ii * (2 * jj + c)) & (kSide - 1)]);
-        if (!a.project) {
-            double2 r = a.prop_rows[i], q = a.prop_columns[i];
+        if (factors) {
+            const size_t off = (size_t)((long long)(p - a.first) * a.prop_stride);
+            double2 r = a.prop_rows[off + i], q = a.prop_columns[off + i];
             if (a.conj_prop) { r.y = -r.y; q.y = -q.y; }
             pr[i] = r;
             pc[i] = q;
@@ -232,38 +238,49 @@ __global__ void __cluster_dims__(Q, 1, 1) __launch_bounds__(PlaneGeometry<Q>::kT
     }
     __syncthreads();  // the mbarriers are initialised
 
-    // ---- bulk copies: the CTA's kLines input rows (contiguous) into buf[line][128]; for the projection, the
-    // amplitudes of its columns into amp; an L2 prefetch of what the cluster `ahead` planes further will read
+    // ---- bulk copies.  Full / forward: the CTA's kLines input rows (contiguous) into buf[line][128]; inverse: the
+    // spectrum's rows restricted to the CTA's columns into buf[row][kStrideA].  For the projection, the amplitudes of
+    // the CTA's columns into amp.  An L2 prefetch of what the cluster `ahead` planes further will read.
     if (t < 32) {
         if (t == 0) {
             asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;"
-                         ::"r"(smem_address(input_ready)), "r"(kInputBytes) : "memory");
-            if (a.project)
+                         ::"r"(smem_address(input_ready)), "r"(kHalfBytes) : "memory");
+            if (project)
                 asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;"
                              ::"r"(smem_address(amp_ready)), "r"(kSide * kAmpRowBytes) : "memory");
         }
         __syncwarp();
-        if (t == 0) {
-            const double2 *src =
-                a.in + (size_t)(a.in_by_class ? a.scan.cls[p] : p) * kPlane + (size_t)rank * G::kLines * kSide;
-            for (uint32_t off = 0; off < kInputBytes; off += kChunk)
+        if (MODE != kPlaneInverse) {
+            if (t == 0) {
+                const char *src = reinterpret_cast<const char *>(a.in + in_plane + (size_t)rank * G::kLines * kSide);
+                for (uint32_t off = 0; off < kHalfBytes; off += kChunk)
+                    asm volatile(
+                        "cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];"
+                        ::"r"(smem_address(buf) + off), "l"(src + off), "r"(kChunk), "r"(smem_address(input_ready))
+                        : "memory");
+            }
+        } else {
+            for (int r = t; r < kSide; r += 32)
                 asm volatile("cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];"
-                             ::"r"(smem_address(buf) + off), "l"(reinterpret_cast<const char *>(src) + off),
-                             "r"(kChunk), "r"(smem_address(input_ready))
+                             ::"r"(smem_address(buf + r * G::kStrideA)),
+                             "l"(a.in + in_plane + (size_t)r * kSide + rank * G::kLines), "r"(kSpanBytes),
+                             "r"(smem_address(input_ready))
                              : "memory");
+        }
+        if (t == 0) {
             const int next = p + a.ahead;
             if (a.ahead > 0 && next < a.first + a.count) {
-                if (!a.in_by_class)
+                if (a.in_kind == kInputByPosition)
                     asm volatile("cp.async.bulk.prefetch.L2.global [%0], %1;"
                                  ::"l"(a.in + (size_t)next * kPlane + (size_t)rank * G::kLines * kSide),
-                                 "r"(kInputBytes) : "memory");
-                if (a.project && rank == 0)
+                                 "r"(kHalfBytes) : "memory");
+                if (project && rank == 0)
                     asm volatile("cp.async.bulk.prefetch.L2.global [%0], %1;"
                                  ::"l"(a.amplitudes + (size_t)next * kPlane), "r"((uint32_t)(kPlane * sizeof(float)))
                                  : "memory");
             }
         }
-        if (a.project) {
+        if (project) {
             for (int r = t; r < kSide; r += 32)
                 asm volatile("cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];"
                              ::"r"(smem_address(amp + r * G::kAmpStride)),
@@ -273,54 +290,90 @@ __global__ void __cluster_dims__(Q, 1, 1) __launch_bounds__(PlaneGeometry<Q>::kT
         }
     }
 
-    // ---- the object patch (from L2) while the rows arrive, then the input times the patch
-    double2 o[16];
-    if (a.object) {
-        const int oy = wrap_once(a.scan.rr[p] + corner_offset(row, kSide), a.object_rows);
-        const double2 *orow = a.object + (size_t)oy * a.object_columns;
-        const int cc = a.scan.cc[p];
-#pragma unroll
-        for (int m = 0; m < 16; m++) {
-            o[m] = orow[wrap_once(cc + corner_offset(j + 8 * m, kSide), a.object_columns)];
-            if (a.conj_object) o[m].y = -o[m].y;
-        }
-    }
-    bool arrived = mbarrier_wait_bounded(input_ready);
-    if (!arrived) {
-        atomicOr(a.fault, 1);
-        arrived = mbarrier_wait_bounded(input_ready);  // the copies land before the buffer is reused, or give up
-    }
     double2 v[16];
-#pragma unroll
-    for (int m = 0; m < 16; m++) v[m] = buf[line * kSide + j + 8 * m];
-    if (a.object) {
-#pragma unroll
-        for (int m = 0; m < 16; m++) v[m] = cmul(v[m], o[m]);
-    }
-    __syncwarp();  // the warp's input rows are read: the same region is its scratch
-    line_forward(v, j, lw, tf, scratch);
-
-    // ---- rows -> columns: X[row][k] to the CTA holding column k, buffer [row][k mod kLines]
-    cluster.sync();  // every CTA has finished with its input and scratch (and runs): the buffers take the exchange
-    constexpr int kPerRank = G::kLines / 16;  // k2 values per destination CTA
     const uint32_t buf_local = smem_address(buf);
+    if constexpr (MODE != kPlaneInverse) {
+        // ---- the object patch (from L2) while the rows arrive, then the input times the patch
+        double2 o[16];
+        if (a.object) {
+            const int oy = wrap_once(a.scan.rr[p] + a.object_row_offset + corner_offset(row, kSide), a.object_rows);
+            const double2 *orow = a.object + (size_t)oy * a.object_columns;
+            const int cc = a.scan.cc[p] + a.object_column_offset;
 #pragma unroll
-    for (int q = 0; q < Q; q++) {
-        const uint32_t dest = cluster_address(buf_local, q) + (uint32_t)(row * G::kStrideA + 2 * j) * 16u;
+            for (int m = 0; m < 16; m++) {
+                o[m] = orow[wrap_once(cc + corner_offset(j + 8 * m, kSide), a.object_columns)];
+                if (a.conj_object) o[m].y = -o[m].y;
+            }
+        }
+        bool arrived = mbarrier_wait_bounded(input_ready);
+        if (!arrived) {
+            atomicOr(a.fault, 1);
+            arrived = mbarrier_wait_bounded(input_ready);  // the copies land before the buffer is reused, or give up
+        }
 #pragma unroll
-        for (int k2 = q * kPerRank; k2 < (q + 1) * kPerRank; k2++)
+        for (int m = 0; m < 16; m++) v[m] = buf[line * kSide + j + 8 * m];
+        if (a.object) {
 #pragma unroll
-            for (int c = 0; c < 2; c++) store_cluster(dest + (uint32_t)(c + 16 * (k2 % kPerRank)) * 16u, v[2 * k2 + c]);
+            for (int m = 0; m < 16; m++) v[m] = cmul(v[m], o[m]);
+        }
+        __syncwarp();  // the warp's input rows are read: the same region is its scratch
+        line_forward(v, j, lw, tf, scratch);
+
+        // ---- rows -> columns: X[row][k] to the CTA holding column k, buffer [row][k mod kLines]
+        cluster.sync();  // every CTA has finished with its input and scratch (and runs): the buffers take the exchange
+        constexpr int kPerRank = G::kLines / 16;  // k2 values per destination CTA
+#pragma unroll
+        for (int q = 0; q < Q; q++) {
+            const uint32_t dest = cluster_address(buf_local, q) + (uint32_t)(row * G::kStrideA + 2 * j) * 16u;
+#pragma unroll
+            for (int k2 = q * kPerRank; k2 < (q + 1) * kPerRank; k2++)
+#pragma unroll
+                for (int c = 0; c < 2; c++)
+                    store_cluster(dest + (uint32_t)(c + 16 * (k2 % kPerRank)) * 16u, v[2 * k2 + c]);
+        }
+        cluster.sync();
+#pragma unroll
+        for (int m = 0; m < 16; m++) v[m] = buf[(j + 8 * m) * G::kStrideA + line];
+        __syncthreads();  // the columns are read: buf is scratch until the next exchange
+        line_forward(v, j, lw, tf, scratch);  // v[2 k2 + c] = F[2 j + c + 16 k2][column]
+    } else {
+        // ---- the spectrum's values of the CTA's columns: F[2 j + c + 16 k2][column]
+        bool arrived = mbarrier_wait_bounded(input_ready);
+        if (!arrived) {
+            atomicOr(a.fault, 1);
+            arrived = mbarrier_wait_bounded(input_ready);
+        }
+#pragma unroll
+        for (int k2 = 0; k2 < 8; k2++)
+#pragma unroll
+            for (int c = 0; c < 2; c++) v[2 * k2 + c] = buf[(2 * j + c + 16 * k2) * G::kStrideA + line];
+        __syncthreads();  // the spectrum is read: buf is scratch until the exchange
     }
-    cluster.sync();
+
+    if constexpr (MODE == kPlaneForward) {
+        // ---- the spectrum out: buf[row][kStrideA] as the columns' exchange buffer, then one bulk copy per row
+        __syncthreads();  // every warp is done with its scratch
 #pragma unroll
-    for (int m = 0; m < 16; m++) v[m] = buf[(j + 8 * m) * G::kStrideA + line];
-    __syncthreads();  // the columns are read: buf is scratch until the next exchange
-    line_forward(v, j, lw, tf, scratch);
+        for (int k2 = 0; k2 < 8; k2++)
+#pragma unroll
+            for (int c = 0; c < 2; c++) buf[(2 * j + c + 16 * k2) * G::kStrideA + line] = v[2 * k2 + c];
+        asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+        __syncthreads();
+        if (t < 32) {
+            for (int r = t; r < kSide; r += 32)
+                asm volatile("cp.async.bulk.global.shared::cta.bulk_group [%0], [%1], %2;"
+                             ::"l"(out_plane + (size_t)r * kSide + rank * G::kLines),
+                             "r"(smem_address(buf + r * G::kStrideA)), "r"(kSpanBytes)
+                             : "memory");
+            asm volatile("cp.async.bulk.commit_group;" ::: "memory");
+            asm volatile("cp.async.bulk.wait_group.read 0;" ::: "memory");
+        }
+        return;
+    }
 
     // ---- the pointwise step on F[2 j + c + 16 k2][column]
     double err = 0.0;
-    if (a.project) {
+    if (project) {
         bool landed = mbarrier_wait_bounded(amp_ready);
         if (!landed) {
             atomicOr(a.fault, 1);
@@ -343,7 +396,7 @@ __global__ void __cluster_dims__(Q, 1, 1) __launch_bounds__(PlaneGeometry<Q>::kT
                     v[2 * k2 + c] = make_double2(measured * a.inv_n, 0.0);
                 }
             }
-    } else {
+    } else if (factors) {
         const double2 wc = pc[column];
 #pragma unroll
         for (int k2 = 0; k2 < 8; k2++)
@@ -355,7 +408,7 @@ __global__ void __cluster_dims__(Q, 1, 1) __launch_bounds__(PlaneGeometry<Q>::kT
     }
     line_inverse(v, j, lw, ti, scratch);  // v[m] = column's value at row j + 8 m
 
-    if (a.project) {  // the position's squared error: warps, then the CTA in warp order, then ranks in order
+    if (project) {  // the position's squared error: warps, then the CTA in warp order, then ranks in order
 #pragma unroll
         for (int o2 = 16; o2 > 0; o2 >>= 1) err += __shfl_down_sync(0xffffffffu, err, o2);
         if ((t & 31) == 0) warp_err[t >> 5] = err;
@@ -366,7 +419,7 @@ __global__ void __cluster_dims__(Q, 1, 1) __launch_bounds__(PlaneGeometry<Q>::kT
             *cluster.map_shared_rank(cluster_err + rank, 0) = total;
         }
     }
-    cluster.sync();  // every CTA is done with its scratch: the buffers take the second exchange
+    cluster.sync();  // every CTA is done with its buffer (and runs): the buffers take the second exchange
 
     // ---- columns -> rows: G[r][column] to the CTA holding row r, buffer [r mod kLines][column]
     constexpr int kRowsPerRank = G::kLines / 8;  // m values per destination CTA
@@ -391,12 +444,12 @@ __global__ void __cluster_dims__(Q, 1, 1) __launch_bounds__(PlaneGeometry<Q>::kT
     asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
     __syncthreads();
     if (t == 0) {
-        char *dst = reinterpret_cast<char *>(a.out + (size_t)p * kPlane + (size_t)rank * G::kLines * kSide);
-        for (uint32_t off = 0; off < kInputBytes; off += kChunk)
+        char *dst = reinterpret_cast<char *>(out_plane + (size_t)rank * G::kLines * kSide);
+        for (uint32_t off = 0; off < kHalfBytes; off += kChunk)
             asm volatile("cp.async.bulk.global.shared::cta.bulk_group [%0], [%1], %2;"
                          ::"l"(dst + off), "r"(smem_address(buf) + off), "r"(kChunk) : "memory");
         asm volatile("cp.async.bulk.commit_group;" ::: "memory");
-        if (a.project && rank == 0) {
+        if (project && rank == 0) {
             double total = 0.0;
             for (int q = 0; q < Q; q++) total += cluster_err[q];
             a.error[p] = total;
@@ -405,7 +458,7 @@ __global__ void __cluster_dims__(Q, 1, 1) __launch_bounds__(PlaneGeometry<Q>::kT
     }
 }
 
-template <int Q>
+template <int Q, int MODE>
 cudaError_t launch_q(Plane128Args a, cudaStream_t s) {
     using G = PlaneGeometry<Q>;
     if (a.ahead == 0) {  // the clusters resident at once: the L2 prefetch distance
@@ -414,8 +467,28 @@ cudaError_t launch_q(Plane128Args a, cudaStream_t s) {
         cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, device);
         a.ahead = sms * (Q == 4 ? 2 : 1) / Q;
     }
-    plane128_kernel<Q><<<(unsigned)a.count * Q, G::kThreads, G::kSmem, s>>>(a);
+    plane128_kernel<Q, MODE><<<(unsigned)a.count * Q, G::kThreads, G::kSmem, s>>>(a);
     return cudaGetLastError();
+}
+
+template <int Q>
+cudaError_t set_smem() {
+    const int bytes = (int)PlaneGeometry<Q>::kSmem;
+    cudaError_t e = cudaFuncSetAttribute(plane128_kernel<Q, kPlaneFull>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                         bytes);
+    if (e == cudaSuccess)
+        e = cudaFuncSetAttribute(plane128_kernel<Q, kPlaneForward>, cudaFuncAttributeMaxDynamicSharedMemorySize, bytes);
+    if (e == cudaSuccess)
+        e = cudaFuncSetAttribute(plane128_kernel<Q, kPlaneInverse>, cudaFuncAttributeMaxDynamicSharedMemorySize, bytes);
+    return e;
+}
+
+template <int Q>
+cudaError_t launch_mode(const Plane128Args &a, cudaStream_t s) {
+    if (a.mode == kPlaneFull) return launch_q<Q, kPlaneFull>(a, s);
+    if (a.mode == kPlaneForward) return launch_q<Q, kPlaneForward>(a, s);
+    if (a.mode == kPlaneInverse) return launch_q<Q, kPlaneInverse>(a, s);
+    return cudaErrorInvalidValue;
 }
 
 }  // namespace
@@ -431,18 +504,15 @@ int plane128_cluster() {
 }
 
 cudaError_t configure_plane128() {
-    cudaError_t e = cudaFuncSetAttribute(plane128_kernel<2>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                         (int)PlaneGeometry<2>::kSmem);
-    if (e == cudaSuccess)
-        e = cudaFuncSetAttribute(plane128_kernel<4>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                 (int)PlaneGeometry<4>::kSmem);
+    cudaError_t e = set_smem<2>();
+    if (e == cudaSuccess) e = set_smem<4>();
     return e;
 }
 
 cudaError_t launch_plane128(const Plane128Args &a, int cluster, cudaStream_t s) {
     if (a.count <= 0) return cudaSuccess;
-    if (cluster == 4) return launch_q<4>(a, s);
-    if (cluster == 2) return launch_q<2>(a, s);
+    if (cluster == 4) return launch_mode<4>(a, s);
+    if (cluster == 2) return launch_mode<2>(a, s);
     return cudaErrorInvalidValue;
 }
 

@@ -100,43 +100,3 @@ def test_plan_resume_and_refusals(cb):
     with pytest.raises(cb.PtychographyError):
         _gpu(cb, dict(inputs, row_sampling=0.0))
 
-
-@pytest.mark.parametrize("cluster", [2, 4])
-def test_plane_launch_equals_the_line_transforms(cb, cluster):
-    """At 128 x 128 the clustered plane launch (forward, detector and back-propagation in one launch per slice)
-    against the batched line transforms of the generic variant, on the same multislice problem: the same arithmetic
-    in another order, so the same results to FP64 roundoff.  The cluster size is read once per process, so the check
-    of the other size runs in a child process."""
-    if cluster != 2:
-        import os
-        import subprocess
-        import sys
-        code = ("import sys; sys.path.insert(0, '.'); import pytest; "
-                "sys.exit(pytest.main(['-q', '-x', "
-                "'tests/test_gpu_multislice.py::test_plane_launch_equals_the_line_transforms[2]', "
-                "'-p', 'no:cacheprovider']))")
-        env = dict(os.environ, CUBO_PTYCHO_PLANE_CLUSTER=str(cluster))
-        r = subprocess.run([sys.executable, "-c", code], env=env, cwd=str(__import__("pathlib").Path(__file__).parents[1]),
-                           capture_output=True, text=True, timeout=600)
-        assert r.returncode == 0, r.stdout[-2000:] + r.stderr[-2000:]
-        return
-    s = scenes.raster_scene(scan=3, det=128, step=8, seed=9)
-    obj = np.stack([s["object"] * np.exp(0.03j * i) for i in range(3)])
-    ms = dict(slices=3, slice_thicknesses=[30.0, 50.0], wavelength=0.0197, row_sampling=0.45, column_sampling=0.5)
-    start = s["positions"] + np.array([0.25, -0.4])
-    out = []
-    for variant in ("auto", "generic"):
-        plan = cb.Plan(s["amplitudes"], start, s["object"].shape, s["probe"].shape, multislice=ms, variant=variant,
-                       step_size=0.5, fix_probe_center_of_mass=True)
-        plan.set_state(obj, s["probe"])
-        e = plan.iterate(3)
-        o, p = plan.get_state()
-        plan.close()
-        out.append((o, p, e))
-    (o1, p1, e1), (o2, p2, e2) = out
-    assert max(gc.complex_gap(o1, o2), gc.complex_gap(p1, p2), gap(e1, e2)) < 1e-12
-    single = [cb.SingleslicePtychography.reconstruct(s["amplitudes"], start, s["object"], s["probe"], iterations=3,
-                                                     step_size=0.5, precision="fp64", variant=v)
-              for v in ("auto", "generic")]
-    assert max(gc.complex_gap(single[0].object, single[1].object), gc.complex_gap(single[0].probe, single[1].probe),
-               gap(single[0].errors, single[1].errors)) < 1e-12
