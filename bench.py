@@ -407,8 +407,9 @@ def run_positions(args, world, rank, local):
             "roofline": {"kernel": "position update (exit waves, FP64 far fields, 2x2 solves)", "bound": "hbm",
                          "achieved": corr_bytes / (corr_ms * 1e-3) / 1e9, "peak": hbm_peak, "unit": "GB/s",
                          "frac": corr_bytes / (corr_ms * 1e-3) / 1e9 / hbm_peak, "peak_kind": peak_kind,
-                         "launch_ms": corr_ms, "note": "the three far fields per position go through HBM "
-                                                       "(batched line FFT), 20 bytes per pixel is the algorithmic floor",
+                         "launch_ms": corr_ms, "note": "three forward plane launches write each position's far "
+                                                       "fields, the 2x2 solves read them back; 20 bytes per pixel is "
+                                                       "the algorithmic floor",
                          "traffic": None},
             "kernel_ms_per_iteration": per_kind, "moved_px_max": moved,
             "cpu_baseline": cpu, "e2e": None, "gpu_launches": launches, "clocks": clocks.summary()}), flush=True)
@@ -473,12 +474,14 @@ def run_mixed(args, world, rank, local):
             "config": {"workload": f"mixed: {P} positions ({args.scan}^2 raster), {DET}x{DET} detector, "
                                    f"{states} states, centre of mass + orthogonalisation",
                        "l2": "amplitudes 4.3 GB, residuals 69 GB: far larger than L2"},
-            "roofline": {"kernel": "mixed position pass (exit waves, FP64 line FFTs, summed-intensity projection)",
+            "roofline": {"kernel": "mixed position pass (per state a forward plane launch, the summed-intensity "
+                                   "projection, per state an inverse plane launch; FP64)",
                          "bound": "hbm", "achieved": pass_bytes / (pass_ms * 1e-3) / 1e9, "peak": hbm_peak,
                          "unit": "GB/s", "frac": pass_bytes / (pass_ms * 1e-3) / 1e9 / hbm_peak,
                          "peak_kind": peak_kind, "launch_ms": pass_ms,
-                         "note": "every state's plane goes through HBM for each FFT pass (FP64 planes of 128^2 do "
-                                 "not fit one CTA)", "traffic": None},
+                         "note": "every state's far field is written, projected in place and read back (the "
+                                 "projection needs all states); the plane launches are latency-bound",
+                         "traffic": None},
             "kernel_ms_per_iteration": per_kind, "errors_first_last": [errors[0], errors[-1]],
             "cpu_baseline": cpu, "e2e": None, "gpu_launches": launches, "clocks": clocks.summary()}), flush=True)
 
