@@ -190,7 +190,7 @@ __device__ __forceinline__ bool mbarrier_wait_bounded(uint64_t *bar) {
 }
 
 template <int Q, int MODE>
-__global__ void __cluster_dims__(Q, 1, 1) __launch_bounds__(PlaneGeometry<Q>::kThreads, Q == 4 ? 2 : 1)
+__global__ void __cluster_dims__(Q, 1, 1) __launch_bounds__(PlaneGeometry<Q>::kThreads, Q / 2)
     plane128_kernel(Plane128Args a) {
     using G = PlaneGeometry<Q>;
     extern __shared__ __align__(16) unsigned char smem_raw[];
@@ -465,7 +465,7 @@ cudaError_t launch_q(Plane128Args a, cudaStream_t s) {
         int device = 0, sms = 0;
         cudaGetDevice(&device);
         cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, device);
-        a.ahead = sms * (Q == 4 ? 2 : 1) / Q;
+        a.ahead = sms / 2;  // Q / 2 CTAs per SM, Q per cluster
     }
     plane128_kernel<Q, MODE><<<(unsigned)a.count * Q, G::kThreads, G::kSmem, s>>>(a);
     return cudaGetLastError();
@@ -493,12 +493,13 @@ cudaError_t launch_mode(const Plane128Args &a, cudaStream_t s) {
 
 }  // namespace
 
-// CTAs per plane: 2 (512 threads each, one CTA per SM) by default; CUBO_PTYCHO_PLANE_CLUSTER=4 selects four CTAs of
-// 256 threads (two per SM).  Either gives the same results bit for bit.
+// CTAs per plane: 2 (512 threads each, one CTA per SM) by default; CUBO_PTYCHO_PLANE_CLUSTER=4 or 8 selects four CTAs
+// of 256 threads (two per SM) or eight of 128 (four per SM).  Every size gives the same results bit for bit.
 int plane128_cluster() {
     static const int q = [] {
         const char *v = std::getenv("CUBO_PTYCHO_PLANE_CLUSTER");
-        return v && std::atoi(v) == 4 ? 4 : 2;
+        const int want = v ? std::atoi(v) : 2;
+        return want == 4 || want == 8 ? want : 2;
     }();
     return q;
 }
@@ -506,11 +507,13 @@ int plane128_cluster() {
 cudaError_t configure_plane128() {
     cudaError_t e = set_smem<2>();
     if (e == cudaSuccess) e = set_smem<4>();
+    if (e == cudaSuccess) e = set_smem<8>();
     return e;
 }
 
 cudaError_t launch_plane128(const Plane128Args &a, int cluster, cudaStream_t s) {
     if (a.count <= 0) return cudaSuccess;
+    if (cluster == 8) return launch_mode<8>(a, s);
     if (cluster == 4) return launch_mode<4>(a, s);
     if (cluster == 2) return launch_mode<2>(a, s);
     return cudaErrorInvalidValue;

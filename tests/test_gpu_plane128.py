@@ -1,7 +1,7 @@
 """The clustered 128 x 128 FP64 plane launches (``plane128.cu``: full, forward-only and inverse-only) against the
 batched line transforms of the generic variant, engine by engine: the same arithmetic in another order, so the same
-results to FP64 roundoff (1e-12 of max(1, max|b|)).  Both cluster sizes; the size is read once per process, so the
-four-CTA form runs in a child process."""
+results to FP64 roundoff (1e-12 of max(1, max|b|)).  Every cluster size (2, 4 and 8 CTAs per plane); the size is
+read once per process, so the other sizes run in child processes."""
 import os
 import subprocess
 import sys
@@ -92,12 +92,13 @@ def test_multislice(cb, scene):
     assert max(gc.complex_gap(o1, o2), gc.complex_gap(p1, p2), gap(e1, e2)) < TOL
 
 
-def test_four_ctas_per_plane():
-    """The same four checks with four CTAs per plane (CUBO_PTYCHO_PLANE_CLUSTER=4), in a child process."""
-    if os.environ.get("CUBO_PTYCHO_PLANE_CLUSTER") == "4":
-        pytest.skip("this process already runs the four-CTA form")
-    env = dict(os.environ, CUBO_PTYCHO_PLANE_CLUSTER="4")
+@pytest.mark.parametrize("cluster", ["4", "8"])
+def test_other_cluster_sizes(cluster):
+    """The same four checks with four or eight CTAs per plane (CUBO_PTYCHO_PLANE_CLUSTER), in a child process."""
+    if os.environ.get("CUBO_PTYCHO_PLANE_CLUSTER"):
+        pytest.skip("this process already runs another cluster size")
+    env = dict(os.environ, CUBO_PTYCHO_PLANE_CLUSTER=cluster)
     r = subprocess.run([sys.executable, "-m", "pytest", "-q", "-x", "-p", "no:cacheprovider",
-                        "tests/test_gpu_plane128.py", "-k", "not four_ctas"],
+                        "tests/test_gpu_plane128.py", "-k", "not other_cluster_sizes"],
                        env=env, cwd=str(ROOT), capture_output=True, text=True, timeout=900)
     assert r.returncode == 0, r.stdout[-3000:] + r.stderr[-2000:]
