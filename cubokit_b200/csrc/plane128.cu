@@ -239,53 +239,49 @@ __global__ void __cluster_dims__(Q, 1, 1) __launch_bounds__(PlaneGeometry<Q>::kT
     __syncthreads();  // the mbarriers are initialised
 
     // ---- bulk copies.  Full / forward: the CTA's kLines input rows (contiguous) into buf[line][128]; inverse: the
-    // spectrum's rows restricted to the CTA's columns into buf[row][kStrideA].  For the projection, the amplitudes of
-    // the CTA's columns into amp.  An L2 prefetch of what the cluster `ahead` planes further will read.
-    if (t < 32) {
-        if (t == 0) {
+    // spectrum's rows restricted to the CTA's columns into buf[row][kStrideA], one row per thread of the first 128.
+    // For the projection, the amplitudes of the CTA's columns into amp, likewise.  An L2 prefetch of what the cluster
+    // `ahead` planes further will read.  The expected bytes are set before any copy is issued.
+    if (t == 0) {
+        asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;"
+                     ::"r"(smem_address(input_ready)), "r"(kHalfBytes) : "memory");
+        if (project)
             asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;"
-                         ::"r"(smem_address(input_ready)), "r"(kHalfBytes) : "memory");
-            if (project)
-                asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;"
-                             ::"r"(smem_address(amp_ready)), "r"(kSide * kAmpRowBytes) : "memory");
-        }
-        __syncwarp();
-        if (MODE != kPlaneInverse) {
-            if (t == 0) {
-                const char *src = reinterpret_cast<const char *>(a.in + in_plane + (size_t)rank * G::kLines * kSide);
-                for (uint32_t off = 0; off < kHalfBytes; off += kChunk)
-                    asm volatile(
-                        "cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];"
-                        ::"r"(smem_address(buf) + off), "l"(src + off), "r"(kChunk), "r"(smem_address(input_ready))
-                        : "memory");
-            }
-        } else {
-            for (int r = t; r < kSide; r += 32)
+                         ::"r"(smem_address(amp_ready)), "r"(kSide * kAmpRowBytes) : "memory");
+    }
+    __syncthreads();
+    static_assert(PlaneGeometry<Q>::kThreads >= kSide, "one row copy per thread");
+    if (MODE != kPlaneInverse) {
+        if (t == 0) {
+            const char *src = reinterpret_cast<const char *>(a.in + in_plane + (size_t)rank * G::kLines * kSide);
+            for (uint32_t off = 0; off < kHalfBytes; off += kChunk)
                 asm volatile("cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];"
-                             ::"r"(smem_address(buf + r * G::kStrideA)),
-                             "l"(a.in + in_plane + (size_t)r * kSide + rank * G::kLines), "r"(kSpanBytes),
-                             "r"(smem_address(input_ready))
+                             ::"r"(smem_address(buf) + off), "l"(src + off), "r"(kChunk), "r"(smem_address(input_ready))
                              : "memory");
         }
-        if (t == 0) {
-            const int next = p + a.ahead;
-            if (a.ahead > 0 && next < a.first + a.count) {
-                if (a.in_kind == kInputByPosition)
-                    asm volatile("cp.async.bulk.prefetch.L2.global [%0], %1;"
-                                 ::"l"(a.in + (size_t)next * kPlane + (size_t)rank * G::kLines * kSide),
-                                 "r"(kHalfBytes) : "memory");
-                if (project && rank == 0)
-                    asm volatile("cp.async.bulk.prefetch.L2.global [%0], %1;"
-                                 ::"l"(a.amplitudes + (size_t)next * kPlane), "r"((uint32_t)(kPlane * sizeof(float)))
-                                 : "memory");
-            }
-        }
-        if (project) {
-            for (int r = t; r < kSide; r += 32)
-                asm volatile("cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];"
-                             ::"r"(smem_address(amp + r * G::kAmpStride)),
-                             "l"(a.amplitudes + (size_t)p * kPlane + (size_t)r * kSide + rank * G::kLines),
-                             "r"(kAmpRowBytes), "r"(smem_address(amp_ready))
+    } else if (t < kSide) {
+        asm volatile("cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];"
+                     ::"r"(smem_address(buf + t * G::kStrideA)),
+                     "l"(a.in + in_plane + (size_t)t * kSide + rank * G::kLines), "r"(kSpanBytes),
+                     "r"(smem_address(input_ready))
+                     : "memory");
+    }
+    if (project && t < kSide)
+        asm volatile("cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];"
+                     ::"r"(smem_address(amp + t * G::kAmpStride)),
+                     "l"(a.amplitudes + (size_t)p * kPlane + (size_t)t * kSide + rank * G::kLines),
+                     "r"(kAmpRowBytes), "r"(smem_address(amp_ready))
+                     : "memory");
+    if (t == 32) {  // another warp than the input copies
+        const int next = p + a.ahead;
+        if (a.ahead > 0 && next < a.first + a.count) {
+            if (a.in_kind == kInputByPosition)
+                asm volatile("cp.async.bulk.prefetch.L2.global [%0], %1;"
+                             ::"l"(a.in + (size_t)next * kPlane + (size_t)rank * G::kLines * kSide), "r"(kHalfBytes)
+                             : "memory");
+            if (project && rank == 0)
+                asm volatile("cp.async.bulk.prefetch.L2.global [%0], %1;"
+                             ::"l"(a.amplitudes + (size_t)next * kPlane), "r"((uint32_t)(kPlane * sizeof(float)))
                              : "memory");
         }
     }
