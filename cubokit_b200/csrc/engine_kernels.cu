@@ -180,7 +180,6 @@ __global__ void __launch_bounds__(kGatherThreads) object_gather_kernel(ObjectGat
     const int lx = threadIdx.x % a.tile_w, ly = threadIdx.x / a.tile_w;
     const int x = x0 + lx, y = y0 + ly;
     const bool inside = x < a.object_columns && y < a.object_rows;
-    const int entries = a.tile_h + a.tile_w;
     constexpr int kInvalid = -(1 << 30);
     C2<T> g = mk<T>(0, 0);
     T w = 0;
@@ -188,27 +187,24 @@ __global__ void __launch_bounds__(kGatherThreads) object_gather_kernel(ObjectGat
     for (int base = begin; base < end; base += kGatherChunk) {
         const int cnt = min(kGatherChunk, end - base);
         __syncthreads();
+        // one candidate per thread: its centre once, then the tile's row and column offsets from it
         for (int i = threadIdx.x; i < cnt; i += kGatherThreads) {
             const int p = a.tile_list[base + i];
+            const int rr = a.scan.rr[p], cc = a.scan.cc[p];
             s_p[i] = p;
             s_cls[i] = a.scan.cls[p];
-        }
-        for (int e = threadIdx.x; e < cnt * entries; e += kGatherThreads) {
-            const int i = e / entries, f = e - i * entries;
-            const int p = a.tile_list[base + i];
-            int v;
-            if (f < a.tile_h) {  // tile row y0 + f
-                int dy = y0 + f - a.scan.rr[p];
+            for (int f = 0; f < a.tile_h; f++) {  // tile row y0 + f
+                int dy = y0 + f - rr;
                 dy = dy < 0 ? dy + a.object_rows : (dy >= a.object_rows ? dy - a.object_rows : dy);
                 const int kr = window_index(dy, a.rows, a.object_rows);
-                v = kr >= 0 ? kr * a.columns : kInvalid;
-            } else {  // tile column x0 + f - tile_h
-                int dx = x0 + f - a.tile_h - a.scan.cc[p];
+                s_off[i][f] = kr >= 0 ? kr * a.columns : kInvalid;
+            }
+            for (int f = 0; f < a.tile_w; f++) {  // tile column x0 + f
+                int dx = x0 + f - cc;
                 dx = dx < 0 ? dx + a.object_columns : (dx >= a.object_columns ? dx - a.object_columns : dx);
                 const int kc = window_index(dx, a.columns, a.object_columns);
-                v = kc >= 0 ? kc : kInvalid;
+                s_off[i][a.tile_h + f] = kc >= 0 ? kc : kInvalid;
             }
-            s_off[i][f] = v;
         }
         __syncthreads();
         if (inside && std::is_same<T, double>::value && a.states > 1) {
