@@ -570,8 +570,9 @@ def main():
     ap.add_argument("--steps", type=int, default=20)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
-    ap.add_argument("--form", default="both", choices=["both", "fp32", "split_bf16"],
-                    help="both: split-BF16 (the headline) and FP32 measured on the same data")
+    ap.add_argument("--form", default="both", choices=["both", "all", "fp32", "split_bf16"],
+                    help="both: split-BF16 (the headline) and FP32 measured on the same data; all: also the any-size "
+                         "FP32 transform (fp32_generic) and the FP64 form")
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--no-cpu", action="store_true")
     ap.add_argument("--scan", type=int, default=SCAN, help="scan side (the benchmark workload is 256)")
@@ -614,11 +615,14 @@ def main():
     objects = ds.object_start.size
     ctx = cb.Context(local)
     stream = torch.cuda.ExternalStream(ctx.stream, device=torch.device("cuda", local))
-    forms = ["split_bf16", "fp32"] if args.form == "both" else [args.form]
+    forms = {"both": ["split_bf16", "fp32"], "all": ["split_bf16", "fp32", "fp32_generic", "fp64"]}.get(
+        args.form, [args.form])
     results = {}
     for form in forms:
+        # fp32_generic: the FP32 form through the any-size shared-memory transform instead of the 128 x 128 kernel
         plan = cb.Plan(ds.amplitudes, ds.positions, ds.object_start.shape, ds.probe.shape, ctx=ctx, step_size=0.5,
-                       precision=form)
+                       precision="fp32" if form == "fp32_generic" else form,
+                       variant="generic" if form == "fp32_generic" else "auto")
         plan.set_state(ds.object_start, ds.probe)
         plan.enqueue(args.warmup)
         ctx.synchronize()
@@ -684,11 +688,17 @@ def main():
                            "position_pass_ms": fr["stats"]["position_pass"][0] / max(fr["stats"]["position_pass"][1], 1),
                            "error_last": float(fr["errors"][-1])}
     comparison = None
-    if len(results) == 2:
+    if "split_bf16" in results and "fp32" in results:
         a, b = results["split_bf16"]["object"], results["fp32"]["object"]
         comparison = {"ratio_split_bf16_over_fp32": forms_out["split_bf16"]["value"] / forms_out["fp32"]["value"],
                       "object_rel_l2_split_bf16_vs_fp32": float(np.linalg.norm(a - b) / np.linalg.norm(b)),
                       "iterations_compared": args.warmup + args.steps}
+        for other in ("fp32_generic", "fp64"):
+            if other in results:
+                c = results[other]["object"]
+                comparison[f"ratio_split_bf16_over_{other}"] = (forms_out["split_bf16"]["value"] /
+                                                                forms_out[other]["value"])
+                comparison[f"object_rel_l2_split_bf16_vs_{other}"] = float(np.linalg.norm(a - c) / np.linalg.norm(c))
 
     e2e = None
     if not args.no_e2e:
