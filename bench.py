@@ -110,6 +110,12 @@ def measured_peaks():
     return 6650.0, 1590.0, "fallback"
 
 
+def fma_peaks(ctx):
+    """This device's FP32 and FP64 CUDA-core FMA rates, TFLOP/s (measured by the library's FMA-chain kernel)."""
+    f32, f64 = ctx.measure_peaks()
+    return {"fp32_tflops": f32, "fp64_tflops": f64, "kind": "measured (FMA chains)"}
+
+
 def dist_setup(args):
     world = int(os.environ.get("WORLD_SIZE", "1"))
     rank = int(os.environ.get("RANK", "0"))
@@ -455,6 +461,8 @@ def run_mixed(args, world, rank, local):
     pass_ms = stats["position_pass"][0] / timed_iterations
     # algorithmic bytes of the position pass: amplitudes read once (4n), every state's residual written once (16n)
     pass_bytes = P * (4 + 16 * states) * n
+    peaks = fma_peaks(ctx)
+    pass_flops = states * P * 10 * n * math.log2(n)  # every state's FFT and inverse (FFT-equivalent)
     cpu = None
     if rank == 0 and not args.no_cpu:
         from oracle import numpy_oracle as no
@@ -481,7 +489,9 @@ def run_mixed(args, world, rank, local):
                          "peak_kind": peak_kind, "launch_ms": pass_ms,
                          "note": "every state's far field is written, projected in place and read back (the "
                                  "projection needs all states); the plane launches are latency-bound",
-                         "traffic": None},
+                         "traffic": None, "fft_equivalent_tflops": pass_flops / (pass_ms * 1e-3) / 1e12,
+                         "frac_of_fp64_fma_peak": pass_flops / (pass_ms * 1e-3) / 1e12 / peaks["fp64_tflops"],
+                         "cuda_core_peaks": peaks},
             "kernel_ms_per_iteration": per_kind, "errors_first_last": [errors[0], errors[-1]],
             "cpu_baseline": cpu, "e2e": None, "gpu_launches": launches, "clocks": clocks.summary()}), flush=True)
 
@@ -532,6 +542,8 @@ def run_multislice(args, world, rank, local):
     # and the object come from L2), slices 1 .. L-2 read their entering wave and write the next (32), the last slice
     # reads its entering wave and the amplitude and writes the residual (36): 32 L - 12
     pass_bytes = P * (32 * slices - 12) * n
+    peaks = fma_peaks(ctx)
+    pass_flops = slices * P * 10 * n * math.log2(n)  # one FFT and one inverse per slice (FFT-equivalent)
     cpu = None
     if rank == 0 and not args.no_cpu:
         from oracle import numpy_oracle as no
@@ -559,7 +571,10 @@ def run_multislice(args, world, rank, local):
                          "unit": "GB/s", "frac": pass_bytes / (pass_ms * 1e-3) / 1e9 / hbm_peak,
                          "peak_kind": peak_kind, "launch_ms": pass_ms,
                          "note": "latency-bound: one 512-thread CTA per SM holds half a plane in registers; its "
-                                 "load, transform and store phases do not overlap", "traffic": None},
+                                 "load, transform and store phases do not overlap", "traffic": None,
+                         "fft_equivalent_tflops": pass_flops / (pass_ms * 1e-3) / 1e12,
+                         "frac_of_fp64_fma_peak": pass_flops / (pass_ms * 1e-3) / 1e12 / peaks["fp64_tflops"],
+                         "cuda_core_peaks": peaks},
             "kernel_ms_per_iteration": per_kind, "errors_first_last": [errors[0], errors[-1]],
             "cpu_baseline": cpu, "e2e": None, "gpu_launches": launches, "clocks": clocks.summary()}), flush=True)
 
@@ -682,11 +697,18 @@ def main():
     roofline["iteration_hbm_gbs"] = bytes_iter / (ms / args.steps * 1e-3) / 1e9
     total_stat_ms = sum(v[0] for v in stats.values())
 
+    peaks = fma_peaks(ctx)
     forms_out = {}
     for form, fr in results.items():
+        pass_form_ms = fr["stats"]["position_pass"][0] / max(fr["stats"]["position_pass"][1], 1)
         forms_out[form] = {"value": P * args.steps / (fr["ms"] * 1e-3) * world, "ms_per_step": fr["ms"] / args.steps,
-                           "position_pass_ms": fr["stats"]["position_pass"][0] / max(fr["stats"]["position_pass"][1], 1),
-                           "error_last": float(fr["errors"][-1])}
+                           "position_pass_ms": pass_form_ms, "error_last": float(fr["errors"][-1]),
+                           "fft_equivalent_tflops": fft_flops / (pass_form_ms * 1e-3) / 1e12}
+        if form in ("fp32", "fp32_generic"):
+            forms_out[form]["frac_of_fp32_fma_peak"] = forms_out[form]["fft_equivalent_tflops"] / peaks["fp32_tflops"]
+        if form == "fp64":
+            forms_out[form]["frac_of_fp64_fma_peak"] = forms_out[form]["fft_equivalent_tflops"] / peaks["fp64_tflops"]
+    roofline["cuda_core_peaks"] = peaks
     comparison = None
     if "split_bf16" in results and "fp32" in results:
         a, b = results["split_bf16"]["object"], results["fp32"]["object"]

@@ -112,6 +112,7 @@ SIGNATURES = {
     "cubo_ptycho_batch_errors": (C.c_int, [C.c_void_p, C.c_int, C.c_int, _dp]),
     "cubo_ptycho_batch_launches_per_iteration": (C.c_longlong, [C.c_void_p]),
     "cubo_ptycho_loss_fp32_noalloc": (C.c_int, [C.c_int] * 5 + [C.c_void_p] * 7),
+    "cubo_ptycho_measure_peaks": (C.c_int, [C.c_void_p, _dp, _dp]),
 }
 
 _lib = None

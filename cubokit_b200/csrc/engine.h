@@ -241,6 +241,9 @@ int plane128_cluster();
 cudaError_t configure_plane128();
 cudaError_t launch_plane128(const Plane128Args &a, int cluster, cudaStream_t s);
 
+// peaks.cu: the FP32 and FP64 FMA rates of the device (TFLOP/s, best of three timed launches on stream s).
+cudaError_t measure_fma_peaks(cudaStream_t s, int sms, double *fp32_tflops, double *fp64_tflops);
+
 // mixed_kernels.cu: the mixed-state engine (MixedstatePtychography, PtychographyEngines.swift:121-267), FP64.
 constexpr int kMaxStates = 16;
 struct MixedPassArgs {

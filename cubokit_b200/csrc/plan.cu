@@ -1978,6 +1978,15 @@ int cubo_ptycho_prepare_amplitudes_device(cubo_ptycho_context *ctx, int count, i
     });
 }
 
+int cubo_ptycho_measure_peaks(cubo_ptycho_context *ctx, double *fp32_tflops, double *fp64_tflops) {
+    return run_guarded(ctx, [&] {
+        if (!fp32_tflops || !fp64_tflops) fail(CUBO_PTYCHO_INVALID_INPUT, "null output");
+        int sms = 0;
+        check(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, ctx->device), "attribute");
+        check(measure_fma_peaks(ctx->stream, sms, fp32_tflops, fp64_tflops), "FMA peaks");
+    });
+}
+
 int cubo_ptycho_set_timing(cubo_ptycho_context *ctx, int enabled) {
     if (!ctx) return CUBO_PTYCHO_INVALID_INPUT;
     ctx->timing = enabled != 0;

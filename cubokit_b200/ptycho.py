@@ -82,6 +82,12 @@ class Context:
         self.check(self.lib.cubo_ptycho_prepare_kernel_stats(self.handle, C.byref(ms), C.byref(launches)))
         return ms.value, launches.value
 
+    def measure_peaks(self):
+        """``(fp32_tflops, fp64_tflops)``: this device's CUDA-core FMA rates (``cubo_ptycho_measure_peaks``)."""
+        f32, f64 = C.c_double(0), C.c_double(0)
+        self.check(self.lib.cubo_ptycho_measure_peaks(self.handle, C.byref(f32), C.byref(f64)))
+        return f32.value, f64.value
+
     def close(self):
         if getattr(self, "handle", None):
             self.lib.cubo_ptycho_destroy(self.handle)

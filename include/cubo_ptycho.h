@@ -328,6 +328,11 @@ CUBO_PTYCHO_API int cubo_ptycho_prepare_amplitudes_device(cubo_ptycho_context *c
 CUBO_PTYCHO_API int cubo_ptycho_set_timing(cubo_ptycho_context *context, int enabled);
 CUBO_PTYCHO_API int cubo_ptycho_prepare_kernel_stats(cubo_ptycho_context *context, double *ms, long long *launches);
 
+/* The device's FP32 and FP64 CUDA-core FMA rates in TFLOP/s (eight independent multiply-add chains per thread, best of
+ * three timed launches): the denominators of the compute fractions reported for the FP32 and FP64 forms.  No
+ * counterpart in the reference; for measurement. */
+CUBO_PTYCHO_API int cubo_ptycho_measure_peaks(cubo_ptycho_context *context, double *fp32_tflops, double *fp64_tflops);
+
 /* ---- Loss without allocating.  No counterpart in the reference: CuboPtycho computes on the CPU and never allocates
  * device memory.  For callers that cannot call cudaMalloc: a host application whose device memory belongs to its own
  * pool allocator, or a latency-critical loop that must not allocate (cudaMalloc can synchronise the device).

@@ -212,3 +212,12 @@ def test_fast128_against_generic_and_oracle(cb, fractional):
         assert np.max(np.abs(r.probe - ref[1])) <= 1e-5 * max(1.0, np.max(np.abs(ref[1])))
         assert np.all(np.abs(r.errors - ref[2]) <= 1e-5 * ref[2])
     assert np.max(np.abs(fast.object - gen.object)) <= 2e-5
+
+
+def test_measured_fma_peaks_are_plausible():
+    """``cubo_ptycho_measure_peaks``: the FP32 and FP64 FMA rates the compute fractions divide by, within what a B200
+    can do (FP32 at most ~90 TFLOP/s, FP64 at most ~45) and well above a broken measurement."""
+    import cubokit_b200 as cb
+    f32, f64 = cb.context(0).measure_peaks()
+    assert 20.0 < f32 < 120.0
+    assert 5.0 < f64 < 60.0
