@@ -1,10 +1,11 @@
-// CuboPtycho.hpp — C++ mirror of CuboPtycho's single-slice API over the B200 engine (include/cubo_ptycho.h).
+// CuboPtycho.hpp — C++ mirror of CuboPtycho's ptychography API over the B200 engine (include/cubo_ptycho.h).
 //
 // Names, argument meanings, defaults and error behaviour follow the Swift API (Sources/CuboPtycho/Ptychography.swift:
 // PtychographyArray :5-21, PtychographyError :24-27, PtychographyErrorNormalization :30-48, PtychographyPosition :88-93,
 // PtychographyAberrationTerm :101-133, PtychographyProbe.build :142-172, SingleslicePtychography.reconstruct
-// :218-406 and its Result :179-188).  Swift's labelled default arguments become the fields of
-// SingleslicePtychography::Options, with the same defaults.  Refusals throw PtychographyError (invalidInput),
+// :218-406 and its Result :179-188; PtychographyEngines.swift: PtychographyStack :13-27, MixedstatePtychography
+// :121-330, MultislicePtychography :413-588).  Swift's labelled default arguments become the fields of each engine's
+// Options, with the same defaults.  Refusals throw PtychographyError (invalidInput),
 // cancellation throws CancellationError; device failures the CPU path cannot have throw DeviceError.
 // Header-only; link with libcuboptycho.so.
 #pragma once
@@ -45,6 +46,21 @@ struct PtychographyArray {
         if (!ok) throw PtychographyError("array shape");
         for (size_t i = 0; i < real.size(); i++)
             if (!std::isfinite(real[i]) || !std::isfinite(imaginary[i])) throw PtychographyError("array not finite");
+    }
+};
+
+// `count` finite complex grids of rows x columns, [index][row][column] (PtychographyEngines.swift:13-27): probe states
+// or object slices.
+struct PtychographyStack {
+    int count = 0, rows = 0, columns = 0;
+    std::vector<double> real, imaginary;
+    PtychographyStack(int count_, int rows_, int columns_, std::vector<double> real_, std::vector<double> imaginary_)
+        : count(count_), rows(rows_), columns(columns_), real(std::move(real_)), imaginary(std::move(imaginary_)) {
+        const bool ok = count > 0 && rows > 1 && columns > 1 &&
+                        (long long)count * rows * columns == (long long)real.size() && imaginary.size() == real.size();
+        if (!ok) throw PtychographyError("stack shape");
+        for (size_t i = 0; i < real.size(); i++)
+            if (!std::isfinite(real[i]) || !std::isfinite(imaginary[i])) throw PtychographyError("stack not finite");
     }
 };
 
@@ -237,6 +253,178 @@ struct SingleslicePtychography {
             f[i] = (float)amplitudes[i];
         }
         return reconstruct(f, positions, object, probe, o, ctx);
+    }
+};
+
+namespace detail {
+
+// The arguments every engine shares, as the C ABI takes them (the FP64 form: the engines are the reference's Double
+// ones).  `mask` keeps the support mask's bytes alive for the call.
+template <typename Options>
+cubo_ptycho_params engine_params(const Options &o, size_t n, std::vector<unsigned char> &mask) {
+    cubo_ptycho_params p;
+    cubo_ptycho_params_default(&p);
+    p.iterations = o.iterations;
+    p.step_size = o.stepSize;
+    p.normalization_minimum = o.normalizationMinimum;
+    p.fix_probe = o.fixProbe;
+    p.pure_phase_object = o.purePhaseObject;
+    p.constrain_object_amplitude = 1;  // the engines always apply the threshold
+    p.fix_probe_center_of_mass = o.fixProbeCenterOfMass;
+    p.constrain_probe_amplitude = o.constrainProbeAmplitude;
+    p.probe_amplitude_relative_radius = o.probeAmplitudeRelativeRadius;
+    p.probe_amplitude_relative_width = o.probeAmplitudeRelativeWidth;
+    p.fix_probe_aperture = o.fixProbeAperture;
+    if (o.probeSupportMask) {
+        if (o.probeSupportMask->size() != n) throw PtychographyError("probe support mask");
+        for (bool b : *o.probeSupportMask) mask.push_back(b ? 1 : 0);
+        p.probe_support_mask = mask.data();
+    }
+    p.error_normalization = o.errorNormalization.mean ? CUBO_PTYCHO_ERRORS_MEAN_INTENSITY
+                                                      : CUBO_PTYCHO_ERRORS_SUPPLIED_AMPLITUDE_ENERGY;
+    p.mean_intensity = o.errorNormalization.meanIntensityValue;
+    p.form = CUBO_PTYCHO_FORM_FP64;
+    return p;
+}
+
+inline cubo_ptycho_problem engine_problem(const std::vector<float> &amplitudes,
+                                          const std::vector<PtychographyPosition> &positions, int rows, int columns,
+                                          int object_rows, int object_columns, std::vector<double> &pr,
+                                          std::vector<double> &pc) {
+    const size_t n = (size_t)rows * columns;
+    if (positions.empty() || amplitudes.size() != positions.size() * n) throw PtychographyError("amplitudes");
+    pr.resize(positions.size());
+    pc.resize(positions.size());
+    for (size_t i = 0; i < positions.size(); i++) { pr[i] = positions[i].row; pc[i] = positions[i].column; }
+    return cubo_ptycho_problem{rows, columns, object_rows, object_columns, (int)positions.size(), amplitudes.data(),
+                               pr.data(), pc.data(), 0};
+}
+
+}  // namespace detail
+
+// MixedstateZeroPixelError (PtychographyEngines.swift:4-10)
+enum class MixedstateZeroPixelError { reference, finite };
+
+// The labelled arguments of MixedstatePtychography.reconstruct(...) with their defaults (PtychographyEngines.swift:
+// 148-157).
+struct MixedstatePtychographyOptions {
+    int iterations = 8;
+    double stepSize = 0.5;
+    double normalizationMinimum = 1;
+    bool fixProbe = false;
+    bool purePhaseObject = false;
+    bool fixProbeCenterOfMass = false;
+    bool constrainProbeAmplitude = false;
+    double probeAmplitudeRelativeRadius = 0.5;
+    double probeAmplitudeRelativeWidth = 0.05;
+    bool orthogonalizeProbes = true;
+    bool fixProbeAperture = false;
+    const std::vector<bool> *probeSupportMask = nullptr;
+    PtychographyErrorNormalization errorNormalization = PtychographyErrorNormalization::suppliedAmplitudeEnergy();
+    MixedstateZeroPixelError zeroFarFieldPixelError = MixedstateZeroPixelError::reference;
+};
+
+// MixedstatePtychography (PtychographyEngines.swift:121-330): several incoherent probe states on one object, FP64.
+struct MixedstatePtychography {
+    struct Result {  // :126-134
+        PtychographyArray object;
+        PtychographyStack probes;
+        std::vector<double> errors;
+    };
+    using Options = MixedstatePtychographyOptions;
+
+    static Result reconstruct(const std::vector<float> &amplitudes, const std::vector<PtychographyPosition> &positions,
+                              const PtychographyArray &object, const PtychographyStack &probes,
+                              const Options &o = Options(), Context &ctx = Context::shared()) {
+        std::vector<double> pr, pc;
+        std::vector<unsigned char> mask;
+        cubo_ptycho_problem problem = detail::engine_problem(amplitudes, positions, probes.rows, probes.columns,
+                                                             object.rows, object.columns, pr, pc);
+        cubo_ptycho_params p = detail::engine_params(o, (size_t)probes.rows * probes.columns, mask);
+        cubo_ptycho_mixed_params m;
+        cubo_ptycho_mixed_params_default(&m);
+        m.states = probes.count;
+        m.orthogonalize_probes = o.orthogonalizeProbes;
+        m.zero_pixel_error = o.zeroFarFieldPixelError == MixedstateZeroPixelError::reference
+                                 ? CUBO_PTYCHO_ZERO_PIXEL_REFERENCE : CUBO_PTYCHO_ZERO_PIXEL_FINITE;
+        std::vector<double> ore = object.real, oim = object.imaginary, pre = probes.real, pim = probes.imaginary;
+        std::vector<double> errors(o.iterations > 0 ? o.iterations : 1);
+        ctx.check(cubo_ptycho_mixed_reconstruct(ctx.get(), &problem, &p, &m, ore.data(), oim.data(), pre.data(),
+                                                pim.data(), errors.data()));
+        errors.resize(o.iterations > 0 ? o.iterations : 0);
+        return Result{PtychographyArray(object.rows, object.columns, std::move(ore), std::move(oim)),
+                      PtychographyStack(probes.count, probes.rows, probes.columns, std::move(pre), std::move(pim)),
+                      std::move(errors)};
+    }
+
+    // MixedstatePtychography.orthogonalize (:265-269): the eigenvectors of the states' Gram matrix, by decreasing
+    // intensity (each state's overall phase is free).
+    static PtychographyStack orthogonalize(const PtychographyStack &probes, Context &ctx = Context::shared()) {
+        std::vector<double> re = probes.real, im = probes.imaginary;
+        ctx.check(cubo_ptycho_orthogonalize(ctx.get(), probes.count, probes.rows, probes.columns, re.data(), im.data()));
+        return PtychographyStack(probes.count, probes.rows, probes.columns, std::move(re), std::move(im));
+    }
+};
+
+// The labelled arguments of MultislicePtychography.reconstruct(...) after the geometry, with their defaults
+// (PtychographyEngines.swift:454-462).
+struct MultislicePtychographyOptions {
+    int iterations = 8;
+    double stepSize = 0.5;
+    double normalizationMinimum = 1;
+    bool fixProbe = false;
+    bool purePhaseObject = false;
+    bool identicalSlices = false;
+    bool fixProbeCenterOfMass = false;
+    bool constrainProbeAmplitude = false;
+    double probeAmplitudeRelativeRadius = 0.5;
+    double probeAmplitudeRelativeWidth = 0.05;
+    bool fixProbeAperture = false;
+    const std::vector<bool> *probeSupportMask = nullptr;
+    PtychographyErrorNormalization errorNormalization = PtychographyErrorNormalization::suppliedAmplitudeEnergy();
+};
+
+// MultislicePtychography (PtychographyEngines.swift:413-588): object slices with Fresnel propagation between them, FP64.
+struct MultislicePtychography {
+    struct Result {  // :417-424
+        PtychographyStack object;
+        PtychographyArray probe;
+        std::vector<double> errors;
+    };
+    using Options = MultislicePtychographyOptions;
+
+    // MultislicePtychography.propagators (:427-442), host arithmetic.
+    static PtychographyStack propagators(int rows, int columns, double rowSampling, double columnSampling,
+                                         double wavelength, const std::vector<double> &sliceThicknesses) {
+        const size_t size = sliceThicknesses.size() * (size_t)(rows > 0 ? rows : 0) * (size_t)(columns > 0 ? columns : 0);
+        std::vector<double> re(size), im(size);
+        const int st = cubo_ptycho_propagators(rows, columns, rowSampling, columnSampling, wavelength,
+                                               (int)sliceThicknesses.size(),
+                                               sliceThicknesses.empty() ? nullptr : sliceThicknesses.data(), re.data(),
+                                               im.data());
+        if (st != CUBO_PTYCHO_OK) throw PtychographyError("propagators");
+        return PtychographyStack((int)sliceThicknesses.size(), rows, columns, std::move(re), std::move(im));
+    }
+
+    static Result reconstruct(const std::vector<float> &amplitudes, const std::vector<PtychographyPosition> &positions,
+                              const PtychographyStack &object, const PtychographyArray &probe,
+                              const std::vector<double> &sliceThicknesses, double wavelength, double rowSampling,
+                              double columnSampling, const Options &o = Options(), Context &ctx = Context::shared()) {
+        if ((int)sliceThicknesses.size() != object.count - 1) throw PtychographyError("slice thicknesses");
+        std::vector<double> pr, pc;
+        std::vector<unsigned char> mask;
+        cubo_ptycho_problem problem = detail::engine_problem(amplitudes, positions, probe.rows, probe.columns,
+                                                             object.rows, object.columns, pr, pc);
+        cubo_ptycho_params p = detail::engine_params(o, (size_t)probe.rows * probe.columns, mask);
+        cubo_ptycho_multislice_params m{object.count, sliceThicknesses.empty() ? nullptr : sliceThicknesses.data(),
+                                        wavelength, rowSampling, columnSampling, o.identicalSlices ? 1 : 0};
+        std::vector<double> ore = object.real, oim = object.imaginary, pre = probe.real, pim = probe.imaginary;
+        std::vector<double> errors(o.iterations > 0 ? o.iterations : 1);
+        ctx.check(cubo_ptycho_multislice_reconstruct(ctx.get(), &problem, &p, &m, ore.data(), oim.data(), pre.data(),
+                                                     pim.data(), errors.data()));
+        errors.resize(o.iterations > 0 ? o.iterations : 0);
+        return Result{PtychographyStack(object.count, object.rows, object.columns, std::move(ore), std::move(oim)),
+                      PtychographyArray(probe.rows, probe.columns, std::move(pre), std::move(pim)), std::move(errors)};
     }
 };
 
