@@ -210,7 +210,7 @@ cudaError_t launch_average_slices(double2 *object, int slices, long long plane, 
 // kPlaneInverse: a spectrum -> the pointwise step -> inverse FFT (unscaled) -> out.
 enum { kPlaneFull = 0, kPlaneForward = 1, kPlaneInverse = 2 };
 enum { kInputByPosition = 0, kInputByClass = 1, kInputSingle = 2 };
-enum { kPointwiseNone = 0, kPointwiseFactors = 1, kPointwiseProjection = 2 };
+enum { kPointwiseNone = 0, kPointwiseFactors = 1, kPointwiseProjection = 2, kPointwiseSolve = 3 };
 struct Plane128Args {
     int mode;
     int first, count;
@@ -236,6 +236,16 @@ struct Plane128Args {
     long long out_stride, out_offset;
     int *fault;                     // set when a bulk copy's wait ran out
     int ahead;                      // L2 prefetch distance in planes (0: the clusters resident at once)
+    // forward mode with kPointwiseSolve (position correction): the spectrum is the far field of the updated object one
+    // column further; with the forward model's far field and the one of the updated object one row further
+    // (far + ((p - first) * 2 + 0 or 1) * 16384) and the amplitudes, position p's 2 x 2 normal equations are summed and
+    // the position moved (positions / initial [rows | columns] of position_count); nothing is written to out
+    const double2 *far;
+    double *positions;
+    const double *initial;
+    int position_count;
+    double position_step_size, limit_update, limit_total;
+    int *position_bad;
 };
 int plane128_cluster();
 cudaError_t configure_plane128();

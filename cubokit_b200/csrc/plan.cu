@@ -820,21 +820,24 @@ void enqueue_position_correction(cubo_ptycho_plan *p) {
     const ScanTables scan{p->rr.as<int>(), p->cc.as<int>(), p->cls.as<int>()};
     for (int first = 0; first < p->P; first += p->correction_chunk) {
         const int m = std::min(p->correction_chunk, p->P - first);
-        if (p->plane128) {  // the three far fields of each position, one forward plane launch each
+        if (p->plane128) {
+            // the forward model's far field and the updated object's one row further (two forward plane launches),
+            // then the one column further with the solve of every position in the same launch
             for (int v = 0; v < 3; v++) {
                 Plane128Args a = plane_args(p, kPlaneForward);
                 a.first = first; a.count = m; a.in = p->shifted.as<double2>(); a.in_kind = kInputByClass;
                 a.object = v == 0 ? p->object_before.as<double2>() : p->object.as<double2>();
                 a.object_row_offset = v == 1 ? 1 : 0; a.object_column_offset = v == 2 ? 1 : 0;
-                a.out = p->far64.as<double2>(); a.out_stride = 3; a.out_offset = v - 3LL * first;
+                a.out = p->far64.as<double2>(); a.out_stride = 2; a.out_offset = v - 2LL * first;
+                if (v == 2) {
+                    a.pointwise = kPointwiseSolve; a.out_offset = 0; a.far = p->far64.as<double2>();
+                    a.positions = p->positions64.as<double>(); a.initial = p->initial64.as<double>();
+                    a.position_count = p->P; a.position_step_size = p->params.position_step_size;
+                    a.limit_update = p->limit_update; a.limit_total = p->limit_total;
+                    a.position_bad = p->position_bad.as<int>();
+                }
                 enqueue_plane(p, kPositionCorrection, a);
             }
-            timed(p, kPositionCorrection, 1, [&] {
-                return launch_position_solve(p->far64.as<double2>(), p->amplitudes.as<float>(), first, m, p->n,
-                                             p->positions64.as<double>(), p->initial64.as<double>(), p->P,
-                                             p->params.position_step_size, p->limit_update, p->limit_total,
-                                             p->position_bad.as<int>(), s);
-            });
             continue;
         }
         timed(p, kPositionCorrection, 3, [&] {
@@ -1317,9 +1320,11 @@ int create_plan(cubo_ptycho_context *ctx, const cubo_ptycho_problem *pr, const c
             check(p->object_before.alloc((size_t)p->objects * sizeof(double2)), "cudaMalloc");
             check(p->position_bad.alloc(sizeof(int)), "cudaMalloc");
             check(cudaMemsetAsync(p->position_bad.ptr, 0, sizeof(int), ctx->stream), "memset");
-            // three far fields per position, FP64: chunks of at most 1 GiB
-            const size_t per_position = (size_t)3 * p->n * sizeof(double2);
-            p->correction_chunk = (int)std::max<size_t>(1, std::min<size_t>(p->P, (1ull << 30) / per_position));
+            // far fields per position, FP64 (three; two with the clustered plane launches, which solve with the
+            // third on chip): chunks of at most 1 GiB (2 GiB)
+            const size_t per_position = (size_t)(p->plane128 ? 2 : 3) * p->n * sizeof(double2);
+            const size_t budget = p->plane128 ? (2ull << 30) : (1ull << 30);
+            p->correction_chunk = (int)std::max<size_t>(1, std::min<size_t>(p->P, budget / per_position));
             check(p->far64.alloc((size_t)p->correction_chunk * per_position), "cudaMalloc");
         }
         check(cudaStreamSynchronize(ctx->stream), "plan upload");

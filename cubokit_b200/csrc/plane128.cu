@@ -21,6 +21,7 @@
 #include <cstdlib>
 
 #include "engine.h"
+#include "position_step.cuh"
 
 namespace cg = cooperative_groups;
 
@@ -211,6 +212,8 @@ __global__ void __cluster_dims__(Q, 1, 1) __launch_bounds__(PlaneGeometry<Q>::kT
     double2 *scratch = buf + (t >> 5) * 512;  // the warp's four lines of 128 = its transpose scratch
     const int row = rank * G::kLines + line, column = rank * G::kLines + line;
     const bool project = MODE == kPlaneFull && a.pointwise == kPointwiseProjection;
+    const bool solve = MODE == kPlaneForward && a.pointwise == kPointwiseSolve;
+    const bool stage_amp = project || solve;  // the amplitudes of the CTA's columns are bulk-copied into amp
     const bool factors = MODE != kPlaneForward && a.pointwise == kPointwiseFactors;
     constexpr uint32_t kHalfBytes = G::kLines * kSide * sizeof(double2), kChunk = 16384;
     constexpr uint32_t kAmpRowBytes = G::kLines * sizeof(float), kSpanBytes = G::kLines * sizeof(double2);
@@ -245,7 +248,7 @@ __global__ void __cluster_dims__(Q, 1, 1) __launch_bounds__(PlaneGeometry<Q>::kT
     if (t == 0) {
         asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;"
                      ::"r"(smem_address(input_ready)), "r"(kHalfBytes) : "memory");
-        if (project)
+        if (stage_amp)
             asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;"
                          ::"r"(smem_address(amp_ready)), "r"(kSide * kAmpRowBytes) : "memory");
     }
@@ -266,7 +269,7 @@ __global__ void __cluster_dims__(Q, 1, 1) __launch_bounds__(PlaneGeometry<Q>::kT
                      "r"(smem_address(input_ready))
                      : "memory");
     }
-    if (project && t < kSide)
+    if (stage_amp && t < kSide)
         asm volatile("cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];"
                      ::"r"(smem_address(amp + t * G::kAmpStride)),
                      "l"(a.amplitudes + (size_t)p * kPlane + (size_t)t * kSide + rank * G::kLines),
@@ -279,7 +282,7 @@ __global__ void __cluster_dims__(Q, 1, 1) __launch_bounds__(PlaneGeometry<Q>::kT
                 asm volatile("cp.async.bulk.prefetch.L2.global [%0], %1;"
                              ::"l"(a.in + (size_t)next * kPlane + (size_t)rank * G::kLines * kSide), "r"(kHalfBytes)
                              : "memory");
-            if (project && rank == 0)
+            if (stage_amp && rank == 0)
                 asm volatile("cp.async.bulk.prefetch.L2.global [%0], %1;"
                              ::"l"(a.amplitudes + (size_t)next * kPlane), "r"((uint32_t)(kPlane * sizeof(float)))
                              : "memory");
@@ -353,6 +356,51 @@ __global__ void __cluster_dims__(Q, 1, 1) __launch_bounds__(PlaneGeometry<Q>::kT
         for (int k2 = 0; k2 < 8; k2++)
 #pragma unroll
             for (int c = 0; c < 2; c++) buf[(2 * j + c + 16 * k2) * G::kStrideA + line] = v[2 * k2 + c];
+        if (solve) {
+            // ---- position correction: this CTA's columns of the normal equations, summed thread -> warp -> CTA ->
+            // cluster in a fixed order, then rank 0 moves the position (Ptychography.swift:411-472)
+            __syncthreads();
+            bool landed = mbarrier_wait_bounded(amp_ready);
+            if (!landed) {
+                atomicOr(a.fault, 1);
+                landed = mbarrier_wait_bounded(amp_ready);
+            }
+            const double2 *f0 = a.far + (size_t)(p - a.first) * 2 * kPlane, *fx = f0 + kPlane;
+            double terms[5] = {0.0, 0.0, 0.0, 0.0, 0.0};
+            for (int e = 0; e < 16; e++) {
+                const int kr = 2 * j + (e & 1) + 16 * (e >> 1);
+                const size_t k = (size_t)kr * kSide + column;
+                position_terms(f0[k], fx[k], buf[kr * G::kStrideA + line], (double)amp[kr * G::kAmpStride + line],
+                               terms);
+            }
+            double *warp_terms = reinterpret_cast<double *>(ti);            // [5][warps], ti is unused here
+            double *cluster_terms = reinterpret_cast<double *>(ti) + 128;   // [Q][5], rank 0's copy is read
+#pragma unroll
+            for (int q = 0; q < 5; q++)
+#pragma unroll
+                for (int o2 = 16; o2 > 0; o2 >>= 1) terms[q] += __shfl_down_sync(0xffffffffu, terms[q], o2);
+            if ((t & 31) == 0)
+#pragma unroll
+                for (int q = 0; q < 5; q++) warp_terms[q * (G::kThreads / 32) + (t >> 5)] = terms[q];
+            __syncthreads();
+            if (t == 0) {
+                double *dest = cluster.map_shared_rank(cluster_terms + 5 * rank, 0);
+                for (int q = 0; q < 5; q++) {
+                    double total = 0.0;
+                    for (int w = 0; w < G::kThreads / 32; w++) total += warp_terms[q * (G::kThreads / 32) + w];
+                    dest[q] = total;
+                }
+            }
+            cluster.sync();  // every rank's sums are in rank 0
+            if (rank == 0 && t == 0) {
+                double sums[5] = {0.0, 0.0, 0.0, 0.0, 0.0};
+                for (int r = 0; r < Q; r++)
+                    for (int q = 0; q < 5; q++) sums[q] += cluster_terms[5 * r + q];
+                position_step(sums, p, a.positions, a.initial, a.position_count, a.position_step_size, a.limit_update,
+                              a.limit_total, a.position_bad);
+            }
+            return;
+        }
         asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
         __syncthreads();
         if (t < 32) {

@@ -12,6 +12,7 @@
 // The three exit waves of a chunk of positions are formed by one kernel, transformed by the engine's batched FP64 FFT,
 // and reduced by one CTA per position (fixed-order FP64 sums: the same inputs give the same bits).
 #include "engine.h"
+#include "position_step.cuh"
 
 namespace cubo {
 
@@ -74,46 +75,10 @@ __global__ void __launch_bounds__(kSolveThreads) solve_kernel(const double2 *far
     const double2 *f0 = far + (size_t)i * 3 * n, *fx = f0 + n, *fy = f0 + 2 * n;
     const float *a = amplitudes + (size_t)p * n;
     double v[5] = {0.0, 0.0, 0.0, 0.0, 0.0};  // axx, axy, ayy, bx, by
-    for (int k = threadIdx.x; k < n; k += kSolveThreads) {
-        const double2 f = f0[k], gx = fx[k], gy = fy[k];
-        const double measured = (double)a[k];
-        const double difference = measured * measured - (f.x * f.x + f.y * f.y);
-        const double dx = 2 * ((f.x - gx.x) * f.x + (f.y - gx.y) * f.y);
-        const double dy = 2 * ((f.x - gy.x) * f.x + (f.y - gy.y) * f.y);
-        v[0] += dx * dx;
-        v[1] += dx * dy;
-        v[2] += dy * dy;
-        v[3] += dx * difference;
-        v[4] += dy * difference;
-    }
+    for (int k = threadIdx.x; k < n; k += kSolveThreads) position_terms(f0[k], fx[k], fy[k], (double)a[k], v);
     block_sum5(v, scratch);
     if (threadIdx.x != 0) return;
-    const double axx = v[0], axy = v[1], ayy = v[2], bx = v[3], by = v[4];
-    const double determinant = axx * ayy - axy * axy;
-    double u0 = 0.0, u1 = 0.0;
-    if (determinant != 0 && isfinite(determinant)) {
-        u0 = (ayy * bx - axy * by) / determinant * step;
-        u1 = (axx * by - axy * bx) / determinant * step;
-    }
-    if (!isfinite(u0) || !isfinite(u1)) return;  // the position stays
-    const double norm = hypot(u0, u1);
-    if (norm > limit_update) {
-        u0 /= norm / limit_update;
-        u1 /= norm / limit_update;
-    }
-    const double row = positions[p], column = positions[count + p];
-    if (isfinite(limit_total) && hypot(row - initial[p] - u0, column - initial[count + p] - u1) > limit_total) {
-        u0 = 0.0;
-        u1 = 0.0;
-    }
-    const double moved_row = row - u0, moved_column = column - u1;
-    const double bound = 2305843009213693951.0;  // Int.max / 4 (Ptychography.swift:469)
-    if (!(fabs(moved_row) < bound && fabs(moved_column) < bound)) {
-        *bad = 1;
-        return;
-    }
-    positions[p] = moved_row;
-    positions[count + p] = moved_column;
+    position_step(v, p, positions, initial, count, step, limit_update, limit_total, bad);
 }
 
 __global__ void __launch_bounds__(1024) center_kernel(double *positions, int count, double initial_mean_row,
