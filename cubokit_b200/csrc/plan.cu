@@ -559,6 +559,7 @@ Plane128Args plane_args(const cubo_ptycho_plan *p, int mode) {
     a.object_rows = p->OR; a.object_columns = p->OC; a.pointwise = kPointwiseNone; a.scale = 1.0 / p->n;
     a.amplitudes = p->amplitudes.as<float>(); a.error = p->error.as<double>(); a.inv_n = 1.0 / p->n;
     a.tw = p->tw_r64.as<double2>(); a.out_stride = 1; a.out_offset = 0; a.fault = p->fault.as<int>();
+    a.ahead = p->sms / 2;  // the clusters resident at once (Q / 2 CTAs per SM, Q per cluster)
     return a;
 }
 
