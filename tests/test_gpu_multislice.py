@@ -100,3 +100,26 @@ def test_plan_resume_and_refusals(cb):
     with pytest.raises(cb.PtychographyError):
         _gpu(cb, dict(inputs, row_sampling=0.0))
 
+
+
+def test_edge_cases(cb):
+    """Zero iterations return the inputs bit for bit with no errors; one position, and six slices on a non-square
+    detector, agree with the restatement."""
+    name, inputs, _ = gc.multislice_cases()[0]
+    r0 = _gpu(cb, dict(inputs, iterations=0))
+    assert np.array_equal(r0.object, inputs["obj"]) and np.array_equal(r0.probe, inputs["probe"])
+    assert len(r0.errors) == 0
+    one = dict(inputs, amplitudes=inputs["amplitudes"][:1], positions=inputs["positions"][:1],
+               error_normalization="suppliedAmplitudeEnergy")
+    one.pop("mean_intensity")
+    r1 = _gpu(cb, one)
+    kw = {k: v for k, v in one.items() if k not in ("amplitudes", "positions", "obj", "probe")}
+    o, p, e = no.multislice_reconstruct(one["amplitudes"], one["positions"], one["obj"], one["probe"], **kw)
+    assert max(gc.complex_gap(r1.object, o), gc.complex_gap(r1.probe, p), gap(r1.errors, e)) < 1e-9
+    s = scenes.raster_scene(scan=2, det=24, step=5, seed=3, shape=(24, 20))
+    obj = np.stack([s["object"]] * 6)
+    kw6 = dict(slice_thicknesses=[12.0] * 5, wavelength=0.0197, row_sampling=0.5, column_sampling=0.45, iterations=2,
+               step_size=0.5)
+    o, p, e = no.multislice_reconstruct(s["amplitudes"], s["positions"] + 0.3, obj, s["probe"], **kw6)
+    r6 = cb.MultislicePtychography.reconstruct(s["amplitudes"], s["positions"] + 0.3, obj, s["probe"], **kw6)
+    assert max(gc.complex_gap(r6.object, o), gc.complex_gap(r6.probe, p), gap(r6.errors, e)) < 1e-9
