@@ -210,7 +210,8 @@ cudaError_t launch_average_slices(double2 *object, int slices, long long plane, 
 // kPlaneInverse: a spectrum -> the pointwise step -> inverse FFT (unscaled) -> out.
 enum { kPlaneFull = 0, kPlaneForward = 1, kPlaneInverse = 2 };
 enum { kInputByPosition = 0, kInputByClass = 1, kInputSingle = 2 };
-enum { kPointwiseNone = 0, kPointwiseFactors = 1, kPointwiseProjection = 2, kPointwiseSolve = 3 };
+enum { kPointwiseNone = 0, kPointwiseFactors = 1, kPointwiseProjection = 2, kPointwiseSolve = 3,
+       kPointwiseFactorPlane = 4 };
 struct Plane128Args {
     int mode;
     int first, count;
@@ -246,6 +247,7 @@ struct Plane128Args {
     int position_count;
     double position_step_size, limit_update, limit_total;
     int *position_bad;
+    const double *factors;          // inverse mode with kPointwiseFactorPlane: [positions][128 x 128] real scales
 };
 int plane128_cluster();
 cudaError_t configure_plane128();
@@ -273,6 +275,10 @@ cudaError_t launch_mixed_position_pass(const MixedPassArgs &a, const Fft2Plan64 
 // positions (the inverse transform's 1/n folded in), the per-position error written.
 cudaError_t launch_mixed_project(double2 *dpsi, const float *amplitudes, int count, int states, int n,
                                  bool zero_pixel_infinite, double *error, cudaStream_t s);
+// The same projection's common factor of every pixel into factors[position][pixel] (the inverse transform's 1/n folded
+// in), the states left as they are, the per-position error written.
+cudaError_t launch_mixed_factors(const double2 *dpsi, const float *amplitudes, int count, int states, int n,
+                                 bool zero_pixel_infinite, double *error, double *factors, cudaStream_t s);
 // The states become the eigenvectors of their Gram matrix, by decreasing intensity (gram, mixing: states^2 values;
 // scratch: states * n).
 cudaError_t launch_orthogonalize(double2 *probes, int states, int n, double2 *gram, double2 *mixing, double2 *scratch,

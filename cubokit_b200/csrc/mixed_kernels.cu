@@ -54,9 +54,12 @@ __device__ double block_sum_project(double v, double *scratch) {
     return s;
 }
 
+// With `factors` the common factor of each pixel is written there and the states are left as they are (the inverse
+// plane launches apply it); without, the states are scaled in place.
 __global__ void __launch_bounds__(kProjectThreads) mixed_project_kernel(double2 *dpsi, const float *amplitudes, int first,
                                                                         int count, int states, int n, double inv_n,
-                                                                        int zero_infinite, double *error) {
+                                                                        int zero_infinite, double *error,
+                                                                        double *factors) {
     __shared__ double scratch[kProjectThreads / 32];
     const int p = first + blockIdx.x;
     const float *A = amplitudes + (size_t)p * n;
@@ -75,6 +78,10 @@ __global__ void __launch_bounds__(kProjectThreads) mixed_project_kernel(double2 
         } else {
             err += (measured - amplitude) * (measured - amplitude);
             factor = (measured / amplitude - 1.0) * inv_n;
+        }
+        if (factors) {
+            factors[(size_t)p * n + k] = factor;
+            continue;
         }
         for (int s = 0; s < states; s++) {
             double2 *f = dpsi + ((size_t)s * count + p) * n + k;
@@ -222,7 +229,7 @@ cudaError_t launch_mixed_position_pass(const MixedPassArgs &a, const Fft2Plan64 
             e = launch_fft2_f64(fft, a.dpsi + ((size_t)st * a.count + first) * n, m, false, s);
         if (e == cudaSuccess) {
             mixed_project_kernel<<<m, kProjectThreads, 0, s>>>(a.dpsi, a.amplitudes, first, a.count, a.states, n,
-                                                               1.0 / n, a.zero_pixel_infinite, a.error);
+                                                               1.0 / n, a.zero_pixel_infinite, a.error, nullptr);
             e = cudaGetLastError();
             count++;
         }
@@ -238,7 +245,15 @@ cudaError_t launch_mixed_project(double2 *dpsi, const float *amplitudes, int cou
                                  bool zero_pixel_infinite, double *error, cudaStream_t s) {
     if (count <= 0) return cudaSuccess;
     mixed_project_kernel<<<count, kProjectThreads, 0, s>>>(dpsi, amplitudes, 0, count, states, n, 1.0 / n,
-                                                           zero_pixel_infinite ? 1 : 0, error);
+                                                           zero_pixel_infinite ? 1 : 0, error, nullptr);
+    return cudaGetLastError();
+}
+
+cudaError_t launch_mixed_factors(const double2 *dpsi, const float *amplitudes, int count, int states, int n,
+                                 bool zero_pixel_infinite, double *error, double *factors, cudaStream_t s) {
+    if (count <= 0) return cudaSuccess;
+    mixed_project_kernel<<<count, kProjectThreads, 0, s>>>(const_cast<double2 *>(dpsi), amplitudes, 0, count, states, n,
+                                                           1.0 / n, zero_pixel_infinite ? 1 : 0, error, factors);
     return cudaGetLastError();
 }
 

@@ -170,6 +170,7 @@ struct cubo_ptycho_plan {
     DeviceBuffer gram64, mixing64, ortho64;
     DeviceBuffer waves64, props64, ident, slice_max;  // multislice: entering waves, propagators, identity classes
     DeviceBuffer prop_factors64;  // multislice, 128 x 128 planes: per gap the row and the column factor (128 + 128)
+    DeviceBuffer mixed_factors64;  // mixed state, 128 x 128 planes: the projection's factor per position and pixel
     DeviceBuffer tile_counts;          // position correction: candidate counts per tile, rebuilt on the device
     long long tile_capacity = 0;       // entries the candidate list holds
 
@@ -739,12 +740,14 @@ void enqueue_position_pass(cubo_ptycho_plan *p) {
                 enqueue_plane(p, kPositionPass, a);
             }
             timed(p, kPositionPass, 1, [&] {
-                return launch_mixed_project(p->dpsi.as<double2>(), p->amplitudes.as<float>(), p->P, p->states, n,
-                                            p->zero_pixel_infinite, p->error.as<double>(), s);
+                return launch_mixed_factors(p->dpsi.as<double2>(), p->amplitudes.as<float>(), p->P, p->states, n,
+                                            p->zero_pixel_infinite, p->error.as<double>(),
+                                            p->mixed_factors64.as<double>(), s);
             });
-            for (int st = 0; st < p->states; st++) {
+            for (int st = 0; st < p->states; st++) {  // each state's residual: its far field x the common factor
                 Plane128Args a = plane_args(p, kPlaneInverse);
                 a.in = p->dpsi.as<double2>() + (size_t)st * p->P * n; a.out = const_cast<double2 *>(a.in);
+                a.pointwise = kPointwiseFactorPlane; a.factors = p->mixed_factors64.as<double>();
                 enqueue_plane(p, kPositionPass, a);
             }
         }
@@ -1295,6 +1298,8 @@ int create_plan(cubo_ptycho_context *ctx, const cubo_ptycho_problem *pr, const c
         p->correct_positions = pp->has_position_correction != 0;  // before the scan tables: one class per position
         if (p->fp64) build_plan<double>(p, pr);
         else build_plan<float>(p, pr);
+        if (p->plane128 && p->states > 1)
+            check(p->mixed_factors64.alloc((size_t)p->P * p->n * sizeof(double)), "cudaMalloc mixed-state factors");
         if (p->multislice && p->slices > 1) {
             upload(p->props64, props, ctx->stream);
             if (p->plane128)

@@ -39,9 +39,17 @@ struct PlaneGeometry {
     static constexpr int kStrideB = kSide + 1;           // [kLines rows][128 columns] + 1
     static constexpr int kBuffer = (kSide * kStrideA > kLines * kStrideB) ? kSide * kStrideA : kLines * kStrideB;
     static constexpr int kTables = 512;                  // twiddles [k1][j] and [i][c][j], propagator factors
-    static constexpr int kAmpStride = kLines + 4;        // amplitude rows of the CTA's columns (16-byte rows)
-    static constexpr size_t kSmem = (size_t)(kBuffer + kTables) * sizeof(double2) +
-                                    (size_t)kSide * kAmpStride * sizeof(float) + (32 + 8 + 2) * sizeof(double);
+    // staged rows of the CTA's columns, 16-byte rows: amplitudes (floats; full and forward modes) or per-pixel factors
+    // (doubles; inverse mode), one region sized for the mode
+    static constexpr int kAmpStride = kLines + 4;        // in floats
+    static constexpr int kFactorStride = kLines + 2;     // in doubles
+    __host__ __device__ static constexpr size_t stage_bytes(int mode) {
+        return mode == kPlaneInverse ? (size_t)kSide * kFactorStride * sizeof(double)
+                                     : (size_t)kSide * kAmpStride * sizeof(float);
+    }
+    __host__ __device__ static constexpr size_t smem(int mode) {
+        return (size_t)(kBuffer + kTables) * sizeof(double2) + stage_bytes(mode) + (32 + 8 + 2) * sizeof(double);
+    }
 };
 
 __device__ __forceinline__ int wrap_once(int v, int n) { return v < 0 ? v + n : (v >= n ? v - n : v); }
@@ -201,7 +209,8 @@ __global__ void __cluster_dims__(Q, 1, 1) __launch_bounds__(PlaneGeometry<Q>::kT
     double2 *pr = ti + 128;               // factor of the row frequency (conjugated when asked)
     double2 *pc = pr + 128;               // of the column frequency
     float *amp = reinterpret_cast<float *>(pc + 128);  // [frequency row][kAmpStride]: the CTA's columns
-    double *warp_err = reinterpret_cast<double *>(amp + kSide * G::kAmpStride);  // [32]
+    double *factor = reinterpret_cast<double *>(amp);  // [frequency row][kFactorStride], the same region
+    double *warp_err = reinterpret_cast<double *>(reinterpret_cast<char *>(amp) + G::stage_bytes(MODE));  // [32]
     double *cluster_err = warp_err + 32;                                          // [8], rank 0's copy is read
     uint64_t *input_ready = reinterpret_cast<uint64_t *>(cluster_err + 8);
     uint64_t *amp_ready = input_ready + 1;
@@ -214,6 +223,7 @@ __global__ void __cluster_dims__(Q, 1, 1) __launch_bounds__(PlaneGeometry<Q>::kT
     const bool project = MODE == kPlaneFull && a.pointwise == kPointwiseProjection;
     const bool solve = MODE == kPlaneForward && a.pointwise == kPointwiseSolve;
     const bool stage_amp = project || solve;  // the amplitudes of the CTA's columns are bulk-copied into amp
+    const bool stage_factor = MODE == kPlaneInverse && a.pointwise == kPointwiseFactorPlane;  // or the factors
     const bool factors = MODE != kPlaneForward && a.pointwise == kPointwiseFactors;
     constexpr uint32_t kHalfBytes = G::kLines * kSide * sizeof(double2), kChunk = 16384;
     constexpr uint32_t kAmpRowBytes = G::kLines * sizeof(float), kSpanBytes = G::kLines * sizeof(double2);
@@ -248,9 +258,10 @@ __global__ void __cluster_dims__(Q, 1, 1) __launch_bounds__(PlaneGeometry<Q>::kT
     if (t == 0) {
         asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;"
                      ::"r"(smem_address(input_ready)), "r"(kHalfBytes) : "memory");
-        if (stage_amp)
+        if (stage_amp || stage_factor)
             asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;"
-                         ::"r"(smem_address(amp_ready)), "r"(kSide * kAmpRowBytes) : "memory");
+                         ::"r"(smem_address(amp_ready)), "r"(kSide * (stage_amp ? kAmpRowBytes : kSpanBytes / 2))
+                         : "memory");
     }
     __syncthreads();
     static_assert(PlaneGeometry<Q>::kThreads >= kSide, "one row copy per thread");
@@ -269,6 +280,12 @@ __global__ void __cluster_dims__(Q, 1, 1) __launch_bounds__(PlaneGeometry<Q>::kT
                      "r"(smem_address(input_ready))
                      : "memory");
     }
+    if (stage_factor && t < kSide)
+        asm volatile("cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];"
+                     ::"r"(smem_address(factor + t * G::kFactorStride)),
+                     "l"(a.factors + (size_t)p * kPlane + (size_t)t * kSide + rank * G::kLines), "r"(kSpanBytes / 2),
+                     "r"(smem_address(amp_ready))
+                     : "memory");
     if (stage_amp && t < kSide)
         asm volatile("cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];"
                      ::"r"(smem_address(amp + t * G::kAmpStride)),
@@ -285,6 +302,10 @@ __global__ void __cluster_dims__(Q, 1, 1) __launch_bounds__(PlaneGeometry<Q>::kT
             if (stage_amp && rank == 0)
                 asm volatile("cp.async.bulk.prefetch.L2.global [%0], %1;"
                              ::"l"(a.amplitudes + (size_t)next * kPlane), "r"((uint32_t)(kPlane * sizeof(float)))
+                             : "memory");
+            if (stage_factor && rank == 0)
+                asm volatile("cp.async.bulk.prefetch.L2.global [%0], %1;"
+                             ::"l"(a.factors + (size_t)next * kPlane), "r"((uint32_t)(kPlane * sizeof(double)))
                              : "memory");
         }
     }
@@ -440,6 +461,19 @@ __global__ void __cluster_dims__(Q, 1, 1) __launch_bounds__(PlaneGeometry<Q>::kT
                     v[2 * k2 + c] = make_double2(measured * a.inv_n, 0.0);
                 }
             }
+    } else if (stage_factor) {  // the mixed states' common factor of each pixel (a real scale)
+        bool landed = mbarrier_wait_bounded(amp_ready);
+        if (!landed) {
+            atomicOr(a.fault, 1);
+            landed = mbarrier_wait_bounded(amp_ready);
+        }
+#pragma unroll
+        for (int k2 = 0; k2 < 8; k2++)
+#pragma unroll
+            for (int c = 0; c < 2; c++) {
+                const double sc = factor[(2 * j + c + 16 * k2) * G::kFactorStride + line];
+                v[2 * k2 + c] = make_double2(v[2 * k2 + c].x * sc, v[2 * k2 + c].y * sc);
+            }
     } else if (factors) {
         const double2 wc = pc[column];
 #pragma unroll
@@ -511,19 +545,21 @@ cudaError_t launch_q(Plane128Args a, cudaStream_t s) {
         cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, device);
         a.ahead = sms / 2;  // Q / 2 CTAs per SM, Q per cluster
     }
-    plane128_kernel<Q, MODE><<<(unsigned)a.count * Q, G::kThreads, G::kSmem, s>>>(a);
+    plane128_kernel<Q, MODE><<<(unsigned)a.count * Q, G::kThreads, G::smem(MODE), s>>>(a);
     return cudaGetLastError();
 }
 
 template <int Q>
 cudaError_t set_smem() {
-    const int bytes = (int)PlaneGeometry<Q>::kSmem;
+    using G = PlaneGeometry<Q>;
     cudaError_t e = cudaFuncSetAttribute(plane128_kernel<Q, kPlaneFull>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                         bytes);
+                                         (int)G::smem(kPlaneFull));
     if (e == cudaSuccess)
-        e = cudaFuncSetAttribute(plane128_kernel<Q, kPlaneForward>, cudaFuncAttributeMaxDynamicSharedMemorySize, bytes);
+        e = cudaFuncSetAttribute(plane128_kernel<Q, kPlaneForward>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                 (int)G::smem(kPlaneForward));
     if (e == cudaSuccess)
-        e = cudaFuncSetAttribute(plane128_kernel<Q, kPlaneInverse>, cudaFuncAttributeMaxDynamicSharedMemorySize, bytes);
+        e = cudaFuncSetAttribute(plane128_kernel<Q, kPlaneInverse>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                 (int)G::smem(kPlaneInverse));
     return e;
 }
 
