@@ -271,12 +271,9 @@ struct MixedPassArgs {
 };
 // Exit waves of every state, their far fields, the summed-intensity projection, the inverse transforms.
 cudaError_t launch_mixed_position_pass(const MixedPassArgs &a, const Fft2Plan64 &fft, int *launches, cudaStream_t s);
-// The summed-intensity projection alone, in place on the states' far fields dpsi[state][position][pixel] of `count`
-// positions (the inverse transform's 1/n folded in), the per-position error written.
-cudaError_t launch_mixed_project(double2 *dpsi, const float *amplitudes, int count, int states, int n,
-                                 bool zero_pixel_infinite, double *error, cudaStream_t s);
-// The same projection's common factor of every pixel into factors[position][pixel] (the inverse transform's 1/n folded
-// in), the states left as they are, the per-position error written.
+// The summed-intensity projection's common factor of every pixel of the states' far fields dpsi[state][position][pixel]
+// into factors[position][pixel] (the inverse transform's 1/n folded in), the states left as they are, the per-position
+// error written.
 cudaError_t launch_mixed_factors(const double2 *dpsi, const float *amplitudes, int count, int states, int n,
                                  bool zero_pixel_infinite, double *error, double *factors, cudaStream_t s);
 // The states become the eigenvectors of their Gram matrix, by decreasing intensity (gram, mixing: states^2 values;

@@ -241,14 +241,6 @@ cudaError_t launch_mixed_position_pass(const MixedPassArgs &a, const Fft2Plan64 
     return cudaSuccess;
 }
 
-cudaError_t launch_mixed_project(double2 *dpsi, const float *amplitudes, int count, int states, int n,
-                                 bool zero_pixel_infinite, double *error, cudaStream_t s) {
-    if (count <= 0) return cudaSuccess;
-    mixed_project_kernel<<<count, kProjectThreads, 0, s>>>(dpsi, amplitudes, 0, count, states, n, 1.0 / n,
-                                                           zero_pixel_infinite ? 1 : 0, error, nullptr);
-    return cudaGetLastError();
-}
-
 cudaError_t launch_mixed_factors(const double2 *dpsi, const float *amplitudes, int count, int states, int n,
                                  bool zero_pixel_infinite, double *error, double *factors, cudaStream_t s) {
     if (count <= 0) return cudaSuccess;
