@@ -168,7 +168,9 @@ constexpr int kMaxTileSide = 64;    // the longest tile side (tiles are 32 x 8, 
 // |S|^2 (Ptychography.swift:351-358 as a gather).  For each chunk of candidates the tile's window offsets are staged
 // first: per candidate, the residual row offset kr * columns of each tile row and the residual column kc of each tile
 // column (corner-centred, periodic; negative where the window does not reach), so a pixel's residual index is one sum.
-template <typename T>
+// MIXED: the mixed-state form (FP64, several states per candidate), its own instance so that its registers do not
+// bound the single-state forms' occupancy.
+template <typename T, bool MIXED>
 __global__ void __launch_bounds__(kGatherThreads) object_gather_kernel(ObjectGatherArgs<T> a) {
     __shared__ int s_p[kGatherChunk], s_cls[kGatherChunk];
     __shared__ int s_off[kGatherChunk][kMaxTileSide + kGatherThreads / kMaxTileSide + 4];  // rows, then columns
@@ -207,16 +209,38 @@ __global__ void __launch_bounds__(kGatherThreads) object_gather_kernel(ObjectGat
             }
         }
         __syncthreads();
-        if (inside && std::is_same<T, double>::value && a.states > 1) {
-            // mixed state: for each candidate in order, its states in order (PtychographyEngines.swift:197-205)
-            for (int i = 0; i < cnt; i++) {
-                const int k = s_off[i][ly] + s_off[i][a.tile_h + lx];
-                if (k < 0) continue;
-                for (int st = 0; st < a.states; st++) {
-                    const C2<T> d = a.dpsi[(size_t)st * a.dpsi_state_stride + (size_t)s_p[i] * a.n + k];
-                    const C2<T> sv = a.shifted[(size_t)st * a.shifted_state_stride + (size_t)s_cls[i] * a.n + k];
-                    g = cadd(g, cmulc(sv, d));
-                    w += sv.x * sv.x + sv.y * sv.y;
+        if constexpr (MIXED) {
+            if (!inside) continue;
+            // mixed state: for each candidate in order, its states in order (PtychographyEngines.swift:197-205), four
+            // (candidate, state) pairs at a time so that their loads are independent
+            const int total = cnt * a.states;
+            int i0 = 0, st0 = 0;  // the pair q0 = i0 * states + st0
+            for (int q0 = 0; q0 < total; q0 += 4) {
+                int k[4], off_d[4], off_s[4];
+                int i = i0, st = st0;
+#pragma unroll
+                for (int u = 0; u < 4; u++) {
+                    k[u] = q0 + u < total ? s_off[i][ly] + s_off[i][a.tile_h + lx] : -1;
+                    off_d[u] = st;
+                    off_s[u] = i;
+                    if (++st == a.states) { st = 0; i++; }
+                }
+                i0 = i;
+                st0 = st;
+                C2<T> d[4], sv[4];
+#pragma unroll
+                for (int u = 0; u < 4; u++) {
+                    if (k[u] >= 0) {
+                        d[u] = a.dpsi[(size_t)off_d[u] * a.dpsi_state_stride + (size_t)s_p[off_s[u]] * a.n + k[u]];
+                        sv[u] = a.shifted[(size_t)off_d[u] * a.shifted_state_stride + (size_t)s_cls[off_s[u]] * a.n + k[u]];
+                    }
+                }
+#pragma unroll
+                for (int u = 0; u < 4; u++) {
+                    if (k[u] >= 0) {
+                        g = cadd(g, cmulc(sv[u], d[u]));
+                        w += sv[u].x * sv[u].x + sv[u].y * sv[u].y;
+                    }
                 }
             }
         } else if (inside) {
@@ -551,7 +575,13 @@ cudaError_t launch_position_pass(const PositionPassArgs<T> &a, cudaStream_t s) {
 
 template <typename T>
 cudaError_t launch_object_gather(const ObjectGatherArgs<T> &a, int tiles, cudaStream_t s) {
-    object_gather_kernel<T><<<tiles, kGatherThreads, 0, s>>>(a);
+    if constexpr (std::is_same<T, double>::value) {
+        if (a.states > 1) {  // the mixed-state form exists in FP64 only
+            object_gather_kernel<T, true><<<tiles, kGatherThreads, 0, s>>>(a);
+            return cudaGetLastError();
+        }
+    }
+    object_gather_kernel<T, false><<<tiles, kGatherThreads, 0, s>>>(a);
     return cudaGetLastError();
 }
 
