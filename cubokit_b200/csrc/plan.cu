@@ -11,6 +11,7 @@
 #include <cstring>
 #include <map>
 #include <memory>
+#include <mutex>
 #include <new>
 #include <string>
 #include <vector>
@@ -36,25 +37,107 @@ constexpr int kSide128 = 128;
 
 // --------------------------------------------------------------------------------------------- device buffers
 
+// Freed device blocks kept per device for reuse while a context of the library is alive on that device: a plan's
+// multi-GB buffers cost milliseconds to map and unmap (cudaMalloc / cudaFree), which a call that creates and destroys a
+// plan pays each time.  A block is kept only after the device has synchronised (what cudaFree does anyway), so no
+// queued work still uses it; a request takes the smallest kept block of at least its size and at most 25 % larger;
+// a failed cudaMalloc empties the cache and tries again; the last context destroyed on a device empties its cache.
+class BlockCache {
+  public:
+    static BlockCache &get() {
+        static BlockCache c;
+        return c;
+    }
+    cudaError_t allocate(void **ptr, size_t *bytes, size_t want, int device) {
+        {
+            std::lock_guard<std::mutex> lock(m_);
+            auto &blocks = free_[slot(device)];
+            auto it = blocks.lower_bound(want);
+            if (it != blocks.end() && it->first <= want + want / 4) {
+                *ptr = it->second;
+                *bytes = it->first;
+                held_[slot(device)] -= it->first;
+                blocks.erase(it);
+                return cudaSuccess;
+            }
+        }
+        cudaError_t e = cudaMalloc(ptr, want);
+        if (e == cudaErrorMemoryAllocation) {
+            cudaGetLastError();
+            flush(device);
+            e = cudaMalloc(ptr, want);
+        }
+        if (e == cudaSuccess) *bytes = want;
+        else *ptr = nullptr;
+        return e;
+    }
+    void release(void *ptr, size_t bytes, int device) {
+        int current = device;
+        cudaGetDevice(&current);
+        if (current != device) cudaSetDevice(device);
+        cudaDeviceSynchronize();
+        bool keep = false;
+        {
+            std::lock_guard<std::mutex> lock(m_);
+            if (contexts_[slot(device)] > 0 && held_[slot(device)] + bytes <= kCap) {
+                free_[slot(device)].emplace(bytes, ptr);
+                held_[slot(device)] += bytes;
+                keep = true;
+            }
+        }
+        if (!keep) cudaFree(ptr);
+        if (current != device) cudaSetDevice(current);
+    }
+    void context_created(int device) {
+        std::lock_guard<std::mutex> lock(m_);
+        contexts_[slot(device)]++;
+    }
+    void context_destroyed(int device) {
+        bool last = false;
+        {
+            std::lock_guard<std::mutex> lock(m_);
+            last = --contexts_[slot(device)] <= 0;
+        }
+        if (last) flush(device);
+    }
+    void flush(int device) {
+        std::multimap<size_t, void *> blocks;
+        {
+            std::lock_guard<std::mutex> lock(m_);
+            blocks.swap(free_[slot(device)]);
+            held_[slot(device)] = 0;
+        }
+        for (auto &b : blocks) cudaFree(b.second);
+    }
+
+  private:
+    static constexpr int kDevices = 64;
+    static constexpr size_t kCap = 64ull << 30;  // bytes kept at most per device
+    static int slot(int device) { return device >= 0 && device < kDevices ? device : 0; }
+    std::mutex m_;
+    std::multimap<size_t, void *> free_[kDevices];
+    size_t held_[kDevices] = {};
+    int contexts_[kDevices] = {};
+};
+
 struct DeviceBuffer {
     void *ptr = nullptr;
     size_t bytes = 0;
+    int device = 0;
     DeviceBuffer() = default;
     DeviceBuffer(const DeviceBuffer &) = delete;
     DeviceBuffer &operator=(const DeviceBuffer &) = delete;
     ~DeviceBuffer() { release(); }
     void release() {
-        if (ptr) cudaFree(ptr);
+        if (ptr) BlockCache::get().release(ptr, bytes, device);
         ptr = nullptr;
         bytes = 0;
     }
     cudaError_t alloc(size_t b) {
         release();
         if (b == 0) b = 16;
-        cudaError_t e = cudaMalloc(&ptr, b);
-        if (e == cudaSuccess) bytes = b;
-        else ptr = nullptr;
-        return e;
+        cudaGetDevice(&device);
+        return BlockCache::get().allocate(&ptr, &bytes, b, device);
     }
     template <typename X> X *as() const { return static_cast<X *>(ptr); }
 };
@@ -437,6 +520,7 @@ void build_plan(cubo_ptycho_plan *p, const cubo_ptycho_problem *pr) {
         check(cudaStreamSynchronize(s), "permute amplitudes");
         std::swap(p->amplitudes.ptr, permuted.ptr);
         std::swap(p->amplitudes.bytes, permuted.bytes);
+        std::swap(p->amplitudes.device, permuted.device);
     }
     // ---- state and work buffers
     check(p->object.alloc((size_t)p->slices * p->objects * sizeof(C2<T>)), "cudaMalloc object");
@@ -549,6 +633,7 @@ void ensure_errors(cubo_ptycho_plan *p, long long needed) {
     check(cudaStreamSynchronize(p->ctx->stream), "cudaStreamSynchronize");
     std::swap(p->errors.ptr, fresh.ptr);
     std::swap(p->errors.bytes, fresh.bytes);
+    std::swap(p->errors.device, fresh.device);
     p->errors_capacity = cap;
 }
 
@@ -1133,6 +1218,7 @@ int cubo_ptycho_create(int device, cubo_ptycho_context **out) {
         delete ctx;
         return CUBO_PTYCHO_CUDA_ERROR;
     }
+    BlockCache::get().context_created(device);
     *out = ctx;
     return CUBO_PTYCHO_OK;
 }
@@ -1144,6 +1230,7 @@ int cubo_ptycho_destroy(cubo_ptycho_context *ctx) {
         cudaStreamSynchronize(ctx->stream);
         cudaStreamDestroy(ctx->stream);
     }
+    BlockCache::get().context_destroyed(ctx->device);
     delete ctx;
     return CUBO_PTYCHO_OK;
 }
