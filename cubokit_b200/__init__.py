@@ -12,3 +12,4 @@ from .ptycho import (Batch, CancellationError, Context, DeviceError, MixedstateP
 __all__ = ["Batch", "CancellationError", "Context", "DeviceError", "MixedstatePtychography", "MultislicePtychography", "Plan", "PtychographyAmplitudes", "PtychographyError",
            "PtychographyPositionCorrection", "PtychographyPreparation", "PtychographyProbe", "Result", "SingleslicePtychography", "UnsupportedError", "context",
            "electron_wavelength"]
+from . import sharded  # noqa: E402  one reconstruction over several GPUs

@@ -113,6 +113,9 @@ SIGNATURES = {
     "cubo_ptycho_batch_launches_per_iteration": (C.c_longlong, [C.c_void_p]),
     "cubo_ptycho_loss_fp32_noalloc": (C.c_int, [C.c_int] * 5 + [C.c_void_p] * 7),
     "cubo_ptycho_measure_peaks": (C.c_int, [C.c_void_p, _dp, _dp]),
+    "cubo_ptycho_plan_enqueue_gradients": (C.c_int, [C.c_void_p]),
+    "cubo_ptycho_plan_gradient_buffers": (C.c_int, [C.c_void_p] + [C.POINTER(C.c_void_p)] * 5 + [C.POINTER(C.c_int)]),
+    "cubo_ptycho_plan_apply_gradients": (C.c_int, [C.c_void_p]),
 }
 
 _lib = None

@@ -132,6 +132,8 @@ template <typename T>
 cudaError_t launch_probe_reduce(const C2<T> *partial_grad, const T *partial_weight, int groups, int n,
                                 double2 *grad, double *weight, double *block_max, cudaStream_t s);
 cudaError_t launch_max_reduce(const double *values, int count, double *out, cudaStream_t s);
+// The maximum of count values (float or double) into *out, one CTA in a fixed order.
+template <typename V> cudaError_t launch_max_values(const V *values, long long count, double *out, cudaStream_t s);
 template <typename T>
 cudaError_t launch_object_update(C2<T> *object, const C2<T> *grad, const T *weight, int count, const double *max_weight,
                                  double step, double minimum, int cap, int pure_phase, cudaStream_t s);

@@ -401,10 +401,11 @@ __global__ void __launch_bounds__(256) probe_reduce_kernel(const C2<T> *pg, cons
     if (threadIdx.x == 0) block_max_out[blockIdx.x] = m;
 }
 
-__global__ void __launch_bounds__(1024) max_reduce_kernel(const double *v, int count, double *out) {
+template <typename V>
+__global__ void __launch_bounds__(1024) max_reduce_kernel(const V *v, long long count, double *out) {
     __shared__ double scratch[32];
     double m = -DBL_MAX;
-    for (int i = threadIdx.x; i < count; i += 1024) m = fmax(m, v[i]);
+    for (long long i = threadIdx.x; i < count; i += 1024) m = fmax(m, (double)v[i]);
     m = block_max<1024>(m, scratch);
     if (threadIdx.x == 0) *out = m;
 }
@@ -600,9 +601,17 @@ cudaError_t launch_probe_reduce(const C2<T> *pg, const T *pw, int groups, int n,
 }
 
 cudaError_t launch_max_reduce(const double *values, int count, double *out, cudaStream_t s) {
-    max_reduce_kernel<<<1, 1024, 0, s>>>(values, count, out);
+    max_reduce_kernel<double><<<1, 1024, 0, s>>>(values, count, out);
     return cudaGetLastError();
 }
+
+template <typename V>
+cudaError_t launch_max_values(const V *values, long long count, double *out, cudaStream_t s) {
+    max_reduce_kernel<V><<<1, 1024, 0, s>>>(values, count, out);
+    return cudaGetLastError();
+}
+template cudaError_t launch_max_values<float>(const float *, long long, double *, cudaStream_t);
+template cudaError_t launch_max_values<double>(const double *, long long, double *, cudaStream_t);
 
 template <typename T>
 cudaError_t launch_object_update(C2<T> *object, const C2<T> *grad, const T *weight, int count, const double *max_weight,

@@ -255,6 +255,7 @@ struct cubo_ptycho_plan {
     DeviceBuffer prop_factors64;  // multislice, 128 x 128 planes: per gap the row and the column factor (128 + 128)
     DeviceBuffer mixed_factors64;  // mixed state, 128 x 128 planes: the projection's factor per position and pixel
     DeviceBuffer tile_counts;          // position correction: candidate counts per tile, rebuilt on the device
+    DeviceBuffer shard_loss, shard_counter;  // sharded iterations: this plan's summed squared error, its reduce counter
     long long tile_capacity = 0;       // entries the candidate list holds
 
     ~cubo_ptycho_plan() {
@@ -1105,6 +1106,41 @@ void enqueue_multislice_iteration(cubo_ptycho_plan *p) {
     });
 }
 
+// A sharded iteration's first half (the plan holds one band of the positions): shifted probes, the position pass and the
+// gathers leave this band's object and probe gradient sums and weights, and its summed squared error in shard_loss, for
+// the caller to sum over the bands (Ptychography.swift:298-359, split at the accumulations).
+template <typename T>
+void enqueue_shard_gradients(cubo_ptycho_plan *p) {
+    cudaStream_t s = p->ctx->stream;
+    enqueue_position_pass<T>(p);
+    enqueue_gathers<T>(p);
+    check(cudaMemsetAsync(p->shard_counter.ptr, 0, sizeof(int), s), "memset");
+    timed(p, kErrorReduce, 2, [&] {
+        return launch_error_reduce(p->error.as<double>(), p->error_count, 1.0, p->shard_loss.as<double>(),
+                                   p->shard_counter.as<int>(), p->error_scratch.as<double>(), s);
+    });
+}
+
+// Its second half, once the gradient sums and weights hold every band's: the maxima of the summed weights, then the
+// object and probe updates with their constraints, as one iteration does (Ptychography.swift:360-399).
+template <typename T>
+void enqueue_shard_update(cubo_ptycho_plan *p) {
+    cudaStream_t s = p->ctx->stream;
+    const cubo_ptycho_params &pp = p->params;
+    timed(p, kMaxReduce, 2, [&] {
+        cudaError_t e = launch_max_values<T>(p->weight_o.as<T>(), p->objects, p->maxes.as<double>(), s);
+        if (e == cudaSuccess) e = launch_max_values<double>(p->weight_p64.as<double>(), p->n, p->maxes.as<double>() + 1, s);
+        return e;
+    });
+    const bool threshold = p->states > 1 || pp.constrain_object_amplitude;
+    timed(p, kObjectUpdate, 1, [&] {
+        return launch_object_update<T>(p->object.as<C2<T>>(), p->grad_o.as<C2<T>>(), p->weight_o.as<T>(),
+                                       (int)p->objects, p->maxes.as<double>(), pp.step_size, pp.normalization_minimum,
+                                       threshold ? 1 : 0, pp.pure_phase_object ? 1 : 0, s);
+    });
+    enqueue_probe_side(p);
+}
+
 // The positions on the device after position correction: [rows | columns].
 std::vector<double> download_positions(cubo_ptycho_plan *p) {
     std::vector<double> v((size_t)2 * p->P);
@@ -1641,6 +1677,44 @@ int cubo_ptycho_plan_errors(cubo_ptycho_plan *p, int count, double *errors) {
         if (count > 0)
             check(cudaMemcpy(errors, p->errors.as<double>() + (p->iterations_done - count), (size_t)count * sizeof(double),
                              cudaMemcpyDeviceToHost), "download errors");
+    });
+}
+
+int cubo_ptycho_plan_enqueue_gradients(cubo_ptycho_plan *p) {
+    if (!p) return CUBO_PTYCHO_INVALID_INPUT;
+    return run_guarded(p->ctx, [&] {
+        if (p->multislice || p->correct_positions)
+            fail(CUBO_PTYCHO_UNSUPPORTED, "sharded iterations: single-slice and mixed-state plans without position correction");
+        if (!p->shard_loss.ptr) {
+            check(p->shard_loss.alloc(sizeof(double)), "cudaMalloc");
+            check(p->shard_counter.alloc(sizeof(int)), "cudaMalloc");
+        }
+        p->tape_valid = false;
+        if (p->fp64) enqueue_shard_gradients<double>(p);
+        else enqueue_shard_gradients<float>(p);
+    });
+}
+
+int cubo_ptycho_plan_gradient_buffers(cubo_ptycho_plan *p, void **grad_object, void **weight_object, void **grad_probe,
+                                      void **weight_probe, void **loss, int *real_bytes) {
+    if (!p) return CUBO_PTYCHO_INVALID_INPUT;
+    return run_guarded(p->ctx, [&] {
+        if (!p->shard_loss.ptr) fail(CUBO_PTYCHO_INVALID_INPUT, "no gradients enqueued on this plan yet");
+        if (grad_object) *grad_object = p->grad_o.ptr;
+        if (weight_object) *weight_object = p->weight_o.ptr;
+        if (grad_probe) *grad_probe = p->grad_p64.ptr;
+        if (weight_probe) *weight_probe = p->weight_p64.ptr;
+        if (loss) *loss = p->shard_loss.ptr;
+        if (real_bytes) *real_bytes = p->fp64 ? 8 : 4;
+    });
+}
+
+int cubo_ptycho_plan_apply_gradients(cubo_ptycho_plan *p) {
+    if (!p) return CUBO_PTYCHO_INVALID_INPUT;
+    return run_guarded(p->ctx, [&] {
+        if (!p->shard_loss.ptr) fail(CUBO_PTYCHO_INVALID_INPUT, "no gradients enqueued on this plan yet");
+        if (p->fp64) enqueue_shard_update<double>(p);
+        else enqueue_shard_update<float>(p);
     });
 }
 

@@ -547,6 +547,40 @@ class Plan:
         self.ctx.check(self.ctx.lib.cubo_ptycho_plan_errors(self.handle, count, _ptr(out)))
         return out[:count]
 
+    # ---- sharded iterations (cubo_ptycho_plan_enqueue_gradients / _gradient_buffers / _apply_gradients)
+    def enqueue_gradients(self):
+        """This plan's band of the positions: position pass and gathers, the sums left for the other bands' to be added."""
+        self.ctx.check(self.ctx.lib.cubo_ptycho_plan_enqueue_gradients(self.handle))
+
+    def apply_gradients(self):
+        """The updates from the gradient sums of every band (after they have been summed into this plan's buffers)."""
+        self.ctx.check(self.ctx.lib.cubo_ptycho_plan_apply_gradients(self.handle))
+
+    def gradient_tensors(self):
+        """Zero-copy torch views of the buffers one sharded iteration sums over the bands: ``grad_object``,
+        ``weight_object``, ``grad_probe``, ``weight_probe`` and ``loss`` (valid after the first enqueue_gradients)."""
+        import torch
+        ptrs = [C.c_void_p() for _ in range(5)]
+        real = C.c_int(0)
+        self.ctx.check(self.ctx.lib.cubo_ptycho_plan_gradient_buffers(self.handle, *[C.byref(x) for x in ptrs],
+                                                                      C.byref(real)))
+        objects = int(np.prod(self.object_shape))
+        n = int(self.probe_shape[-1] * self.probe_shape[-2])
+        states = int(self.probe_shape[0]) if len(self.probe_shape) == 3 else 1
+        t = "<f4" if real.value == 4 else "<f8"
+
+        class _View:  # the CUDA array interface over one of the plan's device buffers
+            def __init__(self, ptr, shape, typestr):
+                self.__cuda_array_interface__ = {"shape": shape, "typestr": typestr, "data": (ptr, False),
+                                                 "version": 3, "strides": None}
+
+        dev = torch.device("cuda", self.ctx.device)
+        return {"grad_object": torch.as_tensor(_View(ptrs[0].value, (objects, 2), t), device=dev),
+                "weight_object": torch.as_tensor(_View(ptrs[1].value, (objects,), t), device=dev),
+                "grad_probe": torch.as_tensor(_View(ptrs[2].value, (states * n, 2), "<f8"), device=dev),
+                "weight_probe": torch.as_tensor(_View(ptrs[3].value, (n,), "<f8"), device=dev),
+                "loss": torch.as_tensor(_View(ptrs[4].value, (1,), "<f8"), device=dev)}
+
     def forward(self) -> float:
         """The unnormalised loss sum (|F| - A)^2 of the current state (``cubo_ptycho_plan_forward``)."""
         loss = C.c_double(0)

@@ -231,6 +231,21 @@ CUBO_PTYCHO_API int cubo_ptycho_plan_get_state(cubo_ptycho_plan *plan, double *o
                                double *probe_im);
 /* The plan's current scan positions (count values each): the given ones, moved by position correction when it is on. */
 CUBO_PTYCHO_API int cubo_ptycho_plan_get_positions(cubo_ptycho_plan *plan, double *rows, double *columns);
+/* ---- Sharded iterations: one reconstruction's positions split into bands, one plan per band (per GPU), each holding
+ * the whole object and probe.  An iteration is enqueue_gradients on every band; the sum over the bands of the buffers
+ * gradient_buffers names (on the device; an NCCL all-reduce, say); apply_gradients on every band, which updates the
+ * object and probe from the sums exactly as one plan over all positions does (the maxima are taken of the summed
+ * weights).  No counterpart in the reference (its engine runs on one CPU thread).  The buffers: the object gradient
+ * sum (complex, real_bytes per part: 4 in the FP32 and split-BF16 forms, 8 in FP64) and weights (one real per object
+ * pixel), the probe gradient sums (complex double, states x rows x columns) and weights (double, rows x columns), and
+ * the band's summed squared amplitude error (one double; the iteration's error is its sum over the bands divided by
+ * the error normalisation of all positions).  Single-slice and mixed-state plans without position correction. */
+CUBO_PTYCHO_API int cubo_ptycho_plan_enqueue_gradients(cubo_ptycho_plan *plan);
+CUBO_PTYCHO_API int cubo_ptycho_plan_gradient_buffers(cubo_ptycho_plan *plan, void **grad_object, void **weight_object,
+                                                      void **grad_probe, void **weight_probe, void **loss,
+                                                      int *real_bytes);
+CUBO_PTYCHO_API int cubo_ptycho_plan_apply_gradients(cubo_ptycho_plan *plan);
+
 /* Runs `iterations` GD iterations on the resident state; errors (may be NULL) receives one value per iteration.
  * Honours params->cancel and params->progress. */
 CUBO_PTYCHO_API int cubo_ptycho_plan_iterate(cubo_ptycho_plan *plan, int iterations, double *errors);
