@@ -227,9 +227,11 @@ __global__ void __cluster_dims__(Q, 1, 1) __launch_bounds__(PlaneGeometry<Q>::kT
     const bool factors = MODE != kPlaneForward && a.pointwise == kPointwiseFactors;
     constexpr uint32_t kHalfBytes = G::kLines * kSide * sizeof(double2), kChunk = 16384;
     constexpr uint32_t kAmpRowBytes = G::kLines * sizeof(float), kSpanBytes = G::kLines * sizeof(double2);
-    const size_t in_plane = (size_t)(a.in_kind == kInputByClass ? a.scan.cls[p] : a.in_kind == kInputSingle ? 0 : p) *
-                            kPlane;
-    double2 *const out_plane = a.out + (size_t)((long long)p * a.out_stride + a.out_offset) * kPlane;
+    // the input and output planes of position p (computed where used: they would hold registers across the kernel)
+    auto in_plane = [&]() -> size_t {
+        return (size_t)(a.in_kind == kInputByClass ? a.scan.cls[p] : a.in_kind == kInputSingle ? 0 : p) * kPlane;
+    };
+    auto out_plane = [&]() -> double2 * { return a.out + (size_t)((long long)p * a.out_stride + a.out_offset) * kPlane; };
 
     if (t == 0) {
         asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" ::"r"(smem_address(input_ready)) : "memory");
@@ -267,7 +269,7 @@ __global__ void __cluster_dims__(Q, 1, 1) __launch_bounds__(PlaneGeometry<Q>::kT
     static_assert(PlaneGeometry<Q>::kThreads >= kSide, "one row copy per thread");
     if (MODE != kPlaneInverse) {
         if (t == 0) {
-            const char *src = reinterpret_cast<const char *>(a.in + in_plane + (size_t)rank * G::kLines * kSide);
+            const char *src = reinterpret_cast<const char *>(a.in + in_plane() + (size_t)rank * G::kLines * kSide);
             for (uint32_t off = 0; off < kHalfBytes; off += kChunk)
                 asm volatile("cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];"
                              ::"r"(smem_address(buf) + off), "l"(src + off), "r"(kChunk), "r"(smem_address(input_ready))
@@ -276,7 +278,7 @@ __global__ void __cluster_dims__(Q, 1, 1) __launch_bounds__(PlaneGeometry<Q>::kT
     } else if (t < kSide) {
         asm volatile("cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];"
                      ::"r"(smem_address(buf + t * G::kStrideA)),
-                     "l"(a.in + in_plane + (size_t)t * kSide + rank * G::kLines), "r"(kSpanBytes),
+                     "l"(a.in + in_plane() + (size_t)t * kSide + rank * G::kLines), "r"(kSpanBytes),
                      "r"(smem_address(input_ready))
                      : "memory");
     }
@@ -427,7 +429,7 @@ __global__ void __cluster_dims__(Q, 1, 1) __launch_bounds__(PlaneGeometry<Q>::kT
         if (t < 32) {
             for (int r = t; r < kSide; r += 32)
                 asm volatile("cp.async.bulk.global.shared::cta.bulk_group [%0], [%1], %2;"
-                             ::"l"(out_plane + (size_t)r * kSide + rank * G::kLines),
+                             ::"l"(out_plane() + (size_t)r * kSide + rank * G::kLines),
                              "r"(smem_address(buf + r * G::kStrideA)), "r"(kSpanBytes)
                              : "memory");
             asm volatile("cp.async.bulk.commit_group;" ::: "memory");
@@ -522,7 +524,7 @@ __global__ void __cluster_dims__(Q, 1, 1) __launch_bounds__(PlaneGeometry<Q>::kT
     asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
     __syncthreads();
     if (t == 0) {
-        char *dst = reinterpret_cast<char *>(out_plane + (size_t)rank * G::kLines * kSide);
+        char *dst = reinterpret_cast<char *>(out_plane() + (size_t)rank * G::kLines * kSide);
         for (uint32_t off = 0; off < kHalfBytes; off += kChunk)
             asm volatile("cp.async.bulk.global.shared::cta.bulk_group [%0], [%1], %2;"
                          ::"l"(dst + off), "r"(smem_address(buf) + off), "r"(kChunk) : "memory");
