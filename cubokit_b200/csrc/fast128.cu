@@ -17,8 +17,8 @@
 //    are free of bank conflicts); the group exchanges use a rotated slot order for the same reason.
 //  * The squared residual is summed per warp and written as 16 FP64 partials per position (reduced in a fixed order
 //    by the error kernels): no atomics, bitwise reproducible.
-//  * The next position's amplitudes are prefetched into shared memory by a bulk copy (no multicast) while the current
-//    one is transformed.
+//  * The next position's amplitudes are prefetched into shared memory by a bulk copy into this CTA alone while the
+//    current one is transformed.
 //  * The probe gradient (conj(O[patch]) dpsi and |O|^2, Ptychography.swift:356-357) is accumulated here, in tensor
 //    memory: every thread owns 32 fixed detector pixels, so each CTA sums its positions in order and writes one
 //    partial; a fixed-order FP64 reduction over the 148 partials follows.  This replaces a second pass over dpsi.

@@ -132,7 +132,7 @@ __device__ __forceinline__ void tmem_st8(uint32_t taddr, const float (&v)[8]) {
                  : "memory");
 }
 
-// Bulk copy global -> shared (no multicast), completing `bytes` of transaction on *mbar; one thread issues it after
+// Bulk copy global -> this CTA's shared memory, completing `bytes` of transaction on *mbar; one thread issues it after
 // arming the barrier.  Both addresses 16-byte aligned, bytes a multiple of 16.
 __device__ __forceinline__ void bulk_load(void *smem_dst, const void *gmem_src, uint32_t bytes, uint64_t *mbar) {
     asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(smem_u32(mbar)), "r"(bytes) : "memory");
