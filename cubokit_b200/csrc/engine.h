@@ -121,7 +121,7 @@ cudaError_t launch_prepare(const float *cube, int count, int rows, int columns, 
 // the mean intensities over `count` patterns' partial sums, in a fixed order
 cudaError_t launch_prepare_means(const double *sums, int count, double *scratch, cudaStream_t s);
 
-constexpr int kTileW = 32, kTileH = 8;   // object-gather tile (one pixel per thread)
+constexpr int kTileW = 16, kTileH = 16;  // default object-gather tile (one pixel per thread)
 constexpr int kGatherThreads = kTileW * kTileH;
 
 // engine_kernels.cu

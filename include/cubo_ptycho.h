@@ -109,9 +109,9 @@ typedef struct {
      * CUBO_PTYCHO_VARIANT_GLOBAL (FP64 form) forces the position pass through global memory that detectors too large
      * for one CTA's FP64 plane use (for cross-checks). */
     int variant;
-    /* Object-gather tile (pixels per CTA, 256 in all): 0 = default, 1 = 32 x 8, 2 = 16 x 16, 3 = 64 x 4 (width x height
-     * along the residual's contiguous axis).  A performance choice only: every pixel sums the same positions in the same
-     * order whatever the tile, so results are bitwise the same. */
+    /* Object-gather tile (pixels per CTA, 256 in all): 0 = default (16 x 16), 1 = 32 x 8, 2 = 16 x 16, 3 = 64 x 4
+     * (width x height along the residual's contiguous axis).  A performance choice only: every pixel sums the same
+     * positions in the same order whatever the tile, so results are bitwise the same. */
     int gather_tile;
     /* positionCorrection (PtychographyPositionCorrection, Ptychography.swift:53-85), read when has_position_correction
      * is nonzero.  The reference runs it on its Double path only (its .single path refuses it, Ptychography.swift:236):
