@@ -128,6 +128,7 @@ constexpr int kGatherThreads = kTileW * kTileH;
 template <typename T> cudaError_t launch_position_pass(const PositionPassArgs<T> &a, cudaStream_t s);
 template <typename T> cudaError_t launch_object_gather(const ObjectGatherArgs<T> &a, int tiles, cudaStream_t s);
 template <typename T> cudaError_t launch_probe_gather(const ProbeGatherArgs<T> &a, cudaStream_t s);
+template <typename T> int probe_gather_resident_ctas();  // CTAs of the probe gather resident on one SM (at least 1)
 template <typename T>
 cudaError_t launch_probe_reduce(const C2<T> *partial_grad, const T *partial_weight, int groups, int n,
                                 double2 *grad, double *weight, double *block_max, cudaStream_t s);

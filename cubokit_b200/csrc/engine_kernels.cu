@@ -594,6 +594,16 @@ cudaError_t launch_probe_gather(const ProbeGatherArgs<T> &a, cudaStream_t s) {
 }
 
 template <typename T>
+int probe_gather_resident_ctas() {
+    int ctas = 0;
+    if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&ctas, probe_gather_kernel<T>, kProbeThreads, 0) != cudaSuccess) {
+        (void)cudaGetLastError();
+        ctas = 0;
+    }
+    return ctas > 0 ? ctas : 1;
+}
+
+template <typename T>
 cudaError_t launch_probe_reduce(const C2<T> *pg, const T *pw, int groups, int n, double2 *grad, double *weight,
                                 double *block_max_out, cudaStream_t s) {
     probe_reduce_kernel<T><<<(n + 255) / 256, 256, 0, s>>>(pg, pw, groups, n, grad, weight, block_max_out);
@@ -660,6 +670,7 @@ cudaError_t launch_error_reduce(const double *error, long long count, double div
     template cudaError_t launch_position_pass<T>(const PositionPassArgs<T> &, cudaStream_t);                           \
     template cudaError_t launch_object_gather<T>(const ObjectGatherArgs<T> &, int, cudaStream_t);                      \
     template cudaError_t launch_probe_gather<T>(const ProbeGatherArgs<T> &, cudaStream_t);                             \
+    template int probe_gather_resident_ctas<T>();                                                                      \
     template cudaError_t launch_probe_reduce<T>(const C2<T> *, const T *, int, int, double2 *, double *, double *,     \
                                                 cudaStream_t);                                                         \
     template cudaError_t launch_object_update<T>(C2<T> *, const C2<T> *, const T *, int, const double *, double,       \

@@ -580,10 +580,11 @@ void build_plan(cubo_ptycho_plan *p, const cubo_ptycho_problem *pr) {
     }
     check(p->scratch64.alloc((size_t)n * sizeof(double2)), "cudaMalloc");
     check(p->spectrum64.alloc((size_t)n * sizeof(double2)), "cudaMalloc");
-    // probe-gather groups: about eight CTAs per SM of a 148-SM part; a function of the problem only, so the summation
-    // order (and the result) does not depend on the device
+    // probe-gather groups: one wave of CTAs on a 148-SM part (the kernel's resident CTAs per SM times 148, over the
+    // pixel blocks: a second, partly filled wave left most SMs waiting on a few); a function of the problem and the
+    // kernel's build only, so the summation order (and the result) does not depend on the device
     const int kblocks = (n + 255) / 256;
-    p->groups = std::max(1, std::min(P, (148 * 8 + kblocks - 1) / kblocks));
+    p->groups = std::max(1, std::min(P, 148 * probe_gather_resident_ctas<T>() / kblocks));
     if (p->fast) p->groups = std::min(P, fast128_ctas());  // the position pass writes one partial per CTA
     check(p->partial_grad.alloc((size_t)p->groups * n * sizeof(C2<T>)), "cudaMalloc");
     check(p->partial_weight.alloc((size_t)p->groups * n * sizeof(T)), "cudaMalloc");
