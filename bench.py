@@ -750,7 +750,8 @@ def main():
             "config": {"workload": f"{args.scan}x{args.scan} scan, step {STEP} px, {DET}x{DET} detector, object "
                                    f"{ds.object_start.shape[0]}x{ds.object_start.shape[1]}, dose 1e5, GD step 0.5",
                        "form": head, "positions": P, "parallelism": f"replicas x{world}" if world > 1 else "1 GPU",
-                       "l2": "inputs larger than L2 (4.3 GB amplitudes, 8.6 GB residuals)"},
+                       "l2": f"inputs larger than L2 ({P * n * 4 / 1e9:.2f} GB amplitudes, "
+                             f"{P * n * 8 / 1e9:.2f} GB residuals; L2 126 MB)"},
             "forms": forms_out, "comparison": comparison, "roofline": roofline,
             "kernels": {k: {"ms_per_launch": v[0] / max(v[1], 1), "launches": v[1],
                             "share": v[0] / total_stat_ms if total_stat_ms else None} for k, v in stats.items() if v[1]},
