@@ -7,15 +7,20 @@ iteration over all 65,536 positions.  Metric: positions * iterations / s.
   python bench.py [--gpus N] [--steps K] [--warmup W] [--form both|fp32|split_bf16] [--impl ours|reference]
 
 The headline form is split-BF16 (the DFT-matrix products on the tensor cores); the FP32 form runs on the same data in
-the same invocation and the line reports both, their ratio and the relative L2 difference of their objects.
+the same invocation and the line reports both and their ratio.  `parity` holds each form's relative L2 object error
+against the FP64 device form after every one of 100 iterations on the same data (bounds: split-BF16 1e-4, FP32 1e-5);
+`extras` adds the FP32 form at the 128^2-scan workload (50 iterations against the FP64 form, and the FP64 form against
+the FP64 C restatement of the Double path after 2 iterations), the CPU-path workload run exactly (32^2 scan, 64^2
+detector, 20 iterations, one core and all cores) and the 64-reconstruction batch.
 
 `value` is device-timed (CUDA events on the engine's stream) with amplitudes resident in HBM; the 4.3 GB amplitude
 stack and the 8.6 GB residual buffer are far larger than L2, so no flush is needed.  `e2e` is one
 SingleslicePtychography.reconstruct call (the public API) of K iterations from pinned host buffers, host<->device
 copies, validation and plan set-up included, timed by the wall clock around the blocking call.  With --gpus N > 1
-(torchrun), every rank runs an independent replica on its own GPU (the path has no cross-GPU exchange: "replicas
-only"); value = sum over ranks, time = max over ranks.  --impl reference times the FP64 C restatement of CuboPtycho's
-Double CPU path (oracle/, OpenMP over all host cores) on a bounded sample of the same workload.
+(torchrun), every rank runs an independent replica on its own GPU; value = sum over ranks, time = max over ranks.
+`cpu_baseline` and `--impl reference` time the same code: the FP64 C restatement of CuboPtycho's Double CPU path
+(oracle/) over the first 4,096 positions of the workload, one iteration per step, OpenMP over all host cores
+(`cpu_baseline` also gives the single-core rate).
 """
 from __future__ import annotations
 
@@ -39,14 +44,6 @@ sys.path.insert(0, str(ROOT))
 METRIC = "positions*iter/s, 128^2 det GD: split-BF16 vs FP32 at <=1e-4 object err"
 UNIT = "positions*iter/s"
 SCAN, DET, STEP, DOSE = 256, 128, 4, 1e5
-
-
-def algorithmic(P, n, objects):
-    """Per-iteration algorithmic bytes and flops of the path (amplitudes read once; object and probe complex64 read
-    and written once; two n-point 2-D FFTs and 40 flops per pixel per position)."""
-    bytes_iter = P * 4 * n + 16 * objects + 16 * n
-    flops_iter = P * (10 * n * math.log2(n) + 40 * n)
-    return bytes_iter, flops_iter
 
 
 class ClockSampler:
@@ -103,11 +100,182 @@ class ClockSampler:
 
 
 def measured_peaks():
+    """HBM copy GB/s and dense BF16 TFLOP/s (burst and sustained) measured on this pool's B200s, else the fallback."""
     p = ROOT / "MEASURED_PEAKS.json"
     if p.exists():
         d = json.loads(p.read_text())
-        return d["hbm_gbs"], d.get("bf16_tflops"), "measured"
-    return 6650.0, 1590.0, "fallback"
+        return {"hbm_gbs": d["hbm_gbs"], "bf16_tflops": d.get("bf16_tflops"),
+                "bf16_tflops_sustained": d.get("bf16_tflops_sustained"), "kind": "measured"}
+    return {"hbm_gbs": 6650.0, "bf16_tflops": 1590.0, "bf16_tflops_sustained": 1400.0, "kind": "fallback"}
+
+
+# DRAM bytes (dram__bytes_read.sum + dram__bytes_write.sum) per position of one position-pass launch, from ncu on a
+# 4,096-position launch (64^2 scan, 128^2 detector) of each kernel, divided by its positions: amplitudes read (64 KB)
+# plus residuals written (128 KB) less what stays in L2.  The bench scales them to its launch by positions.
+PASS_DRAM_BYTES_PER_POSITION = {"split_bf16": 748.3e6 / 4096, "fp32": None}
+
+
+def position_pass_roofline(head, stats, P, n, objects, ms_iter, peaks, fma):
+    """The dominant kernel (the position pass) against the roofline that binds its algorithmic work.
+
+    Algorithmic work per position: the amplitudes read once (4n bytes) and two n-point 2-D FFTs plus 40 flops per
+    pixel (10 n log2 n + 40 n flops).  At the measured peaks the bytes take longer than the flops on any pipe the pass
+    could use, so HBM binds: achieved = 4 n P / launch time, frac = achieved / measured HBM copy rate.  The executed
+    split-BF16 tensor work (100.7 MFLOP per position of real 128 x 128 x 128 products) is reported beside it as a
+    utilisation figure, not as the roofline."""
+    pass_ms, pass_launches = stats["position_pass"]
+    pass_s = pass_ms / max(pass_launches, 1) * 1e-3
+    pass_bytes = P * 4 * n
+    achieved = pass_bytes / pass_s / 1e9
+    per_position = PASS_DRAM_BYTES_PER_POSITION.get(head)
+    traffic = per_position * P if per_position else None
+    bytes_iter = P * 4 * n + 16 * objects + 16 * n
+    fft_flops = P * (10 * n * math.log2(n) + 40 * n)
+    out = {"kernel": "position_pass (bf16_position_kernel)" if head == "split_bf16" else "position_pass (fast128_kernel)",
+           "bound": "hbm", "achieved": achieved, "peak": peaks["hbm_gbs"], "unit": "GB/s",
+           "frac": achieved / peaks["hbm_gbs"], "peak_kind": f"{peaks['kind']} HBM copy",
+           "algorithmic_bytes_per_launch": pass_bytes, "launch_ms": pass_s * 1e3,
+           "traffic": traffic, "traffic_over_algorithmic": traffic / pass_bytes if traffic else None,
+           "traffic_source": "ncu DRAM bytes per position of a 4,096-position launch, scaled to this launch"
+           if traffic else None,
+           "fft_equivalent_tflops": fft_flops / pass_s / 1e12,
+           "iteration": {"algorithmic_bytes": bytes_iter, "ms": ms_iter,
+                         "gbs": bytes_iter / (ms_iter * 1e-3) / 1e9,
+                         "frac": bytes_iter / (ms_iter * 1e-3) / 1e9 / peaks["hbm_gbs"]},
+           "cuda_core_peaks": fma}
+    if head == "split_bf16":
+        tensor_flops = P * 4 * 2 * 3 * 2 * 128 ** 3  # 4 stages x 2 planes x 3 split products x 2 * 128^3
+        t = tensor_flops / pass_s / 1e12
+        out.update({"tensor_exec_tflops": t, "tensor_exec_frac": t / peaks["bf16_tflops"],
+                    "tensor_exec_frac_sustained": t / peaks["bf16_tflops_sustained"]
+                    if peaks.get("bf16_tflops_sustained") else None,
+                    "tensor_exec_note": "executed split-BF16 DFT products (100.7 MFLOP per position) against the "
+                                        "dense BF16 peak: tensor-pipe utilisation, not the roofline fraction"})
+    else:
+        out["frac_of_fp32_fma_peak"] = out["fft_equivalent_tflops"] / fma["fp32_tflops"]
+    return out
+
+
+def error_curves(ds, ctx, iterations, forms):
+    """Relative L2 error of the object and of the probe of each form against the FP64 device form after every
+    iteration, all started from the same state on the same data, plus each form's normalised errors."""
+    import cubokit_b200 as cb
+    plans = {}
+    try:
+        for f in ("fp64",) + tuple(forms):
+            plans[f] = cb.Plan(ds.amplitudes, ds.positions, ds.object_start.shape, ds.probe.shape, ctx=ctx,
+                               step_size=0.5, precision=f)
+            plans[f].set_state(ds.object_start, ds.probe)
+        obj = {f: [] for f in forms}
+        prb = {f: [] for f in forms}
+        for _ in range(iterations):
+            for p in plans.values():
+                p.enqueue(1)
+            ro, rp = plans["fp64"].get_state()
+            no, npb = np.linalg.norm(ro), np.linalg.norm(rp)
+            for f in forms:
+                o, pr = plans[f].get_state()
+                obj[f].append(float(np.linalg.norm(o - ro) / no))
+                prb[f].append(float(np.linalg.norm(pr - rp) / npb))
+        errors = {f: [float(e) for e in plans[f].errors(iterations)] for f in plans}
+    finally:
+        for p in plans.values():
+            p.close()
+    return {"object": obj, "probe": prb, "errors": errors}
+
+
+def curve_summary(curves, bounds, what):
+    out = {"what": what, "iterations": len(next(iter(curves["object"].values())))}
+    for f, c in curves["object"].items():
+        out[f] = {"object_rel_l2_max": max(c), "object_rel_l2_last": c[-1], "bound": bounds[f],
+                  "within_bound_every_iteration": bool(max(c) <= bounds[f]),
+                  "probe_rel_l2_max": max(curves["probe"][f]),
+                  "object_rel_l2_per_iteration": [float(f"{v:.3g}") for v in c],
+                  "error_last": curves["errors"][f][-1], "error_last_fp64": curves["errors"]["fp64"][-1]}
+    return out
+
+
+FP32_SCAN, FP32_ITERATIONS = 128, 50
+CPU_SCAN, CPU_DET, CPU_DOSE, CPU_ITERATIONS = 32, 64, 1e4, 20
+BATCH_STEPS = 5
+
+
+def fp32_workload_parity(ctx, local):
+    """The plain FP32 form at 128^2 scan, 128^2 detector, object 640^2: its object error against the FP64 device form
+    after each of 50 iterations, and the FP64 device form against the FP64 C restatement of the Double path after 2
+    iterations on the same data (all host cores)."""
+    from cubokit_b200 import synthetic
+    from oracle import c_oracle
+    ds = synthetic.dataset(FP32_SCAN, DET, dose=DOSE, step=STEP, pinned=True, device=local)
+    P = len(ds.positions)
+    out = curve_summary(error_curves(ds, ctx, FP32_ITERATIONS, ("fp32",)), {"fp32": 1e-5},
+                        f"{FP32_SCAN}^2 scan, 128^2 detector, object {ds.object_start.shape[0]}^2, "
+                        f"{FP32_ITERATIONS} iterations, FP32 against the FP64 form")
+    import cubokit_b200 as cb
+    plan = cb.Plan(ds.amplitudes, ds.positions, ds.object_start.shape, ds.probe.shape, ctx=ctx, step_size=0.5,
+                   precision="fp64")
+    plan.set_state(ds.object_start, ds.probe)
+    dev_err = plan.iterate(2)
+    do, dp = plan.get_state()
+    plan.close()
+    threads = c_oracle.host_cores()
+    t0 = time.perf_counter()
+    oo, op, oe = c_oracle.reconstruct(ds.amplitudes.reshape(P, -1).astype(np.float64), ds.positions, ds.object_start,
+                                      ds.probe, iterations=2, step_size=0.5, threads=threads,
+                                      shift_every_position=False)
+    t = time.perf_counter() - t0
+    out["fp64_vs_c_oracle"] = {
+        "iterations": 2, "object_rel_l2": float(np.linalg.norm(do - oo) / np.linalg.norm(oo)),
+        "object_max_abs": float(np.max(np.abs(do - oo))),
+        "probe_rel_l2": float(np.linalg.norm(dp - op) / np.linalg.norm(op)),
+        "errors_rel": float(np.max(np.abs(np.asarray(dev_err) - oe) / np.abs(oe))),
+        "c_oracle_seconds": t, "c_oracle_threads": threads}
+    return out
+
+
+def cpu_workload(ctx, local, with_cpu=True):
+    """The CPU-path workload exactly (32^2 raster, step 4, 64^2 detector, object 192^2, 1e4 e/pattern, 20 iterations):
+    the FP64 C restatement of the Double path on one core and on all host cores, and the FP32 GPU form on the same
+    data with its object error against that restatement."""
+    import torch
+    import cubokit_b200 as cb
+    from cubokit_b200 import synthetic
+    from oracle import c_oracle
+    ds = synthetic.dataset(CPU_SCAN, CPU_DET, dose=CPU_DOSE, step=STEP, pinned=True, device=local)
+    P = len(ds.positions)
+    amps = ds.amplitudes.reshape(P, -1).astype(np.float64)
+    out = {"workload": f"{CPU_SCAN}^2 scan, step {STEP}, {CPU_DET}^2 detector, object "
+                       f"{ds.object_start.shape[0]}^2, dose {CPU_DOSE:g}, {CPU_ITERATIONS} iterations",
+           "positions": P}
+    threads = c_oracle.host_cores()
+    ref = None
+    if with_cpu:
+        for label, th in (("one_core", 1), ("all_cores", threads)):
+            t0 = time.perf_counter()
+            ref = c_oracle.reconstruct(amps, ds.positions, ds.object_start, ds.probe, iterations=CPU_ITERATIONS,
+                                       step_size=0.5, threads=th)
+            t = time.perf_counter() - t0
+            out[label] = {"seconds": t, "value": P * CPU_ITERATIONS / t, "unit": UNIT, "cores": th,
+                          "cpu_model": cpu_model()}
+    plan = cb.Plan(ds.amplitudes, ds.positions, ds.object_start.shape, ds.probe.shape, ctx=ctx, step_size=0.5,
+                   precision="fp32")
+    plan.set_state(ds.object_start, ds.probe)
+    plan.enqueue(3)
+    ctx.synchronize()
+    stream = torch.cuda.ExternalStream(ctx.stream, device=torch.device("cuda", local))
+    plan.set_state(ds.object_start, ds.probe)
+    start, stop = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    start.record(stream)
+    plan.enqueue(CPU_ITERATIONS)
+    stop.record(stream)
+    stop.synchronize()
+    ms = start.elapsed_time(stop)
+    o, _ = plan.get_state()
+    plan.close()
+    out["gpu_fp32"] = {"value": P * CPU_ITERATIONS / (ms * 1e-3), "unit": UNIT, "ms": ms}
+    if ref is not None:
+        out["gpu_fp32"]["object_rel_l2_vs_c_oracle"] = float(np.linalg.norm(o - ref[0]) / np.linalg.norm(ref[0]))
+    return out
 
 
 def fma_peaks(ctx):
@@ -144,43 +312,61 @@ def barrier(world):
         dist.barrier()
 
 
-def cpu_oracle_sample(ds, threads, target_s=12.0):
-    """The FP64 C restatement of the Double path on a contiguous subset of the positions (whole detector, whole
-    object), one iteration, sized to about `target_s` seconds; returns positions*iter/s and the sample."""
+CPU_SAMPLE_ALL = 4096  # positions per all-core step of the CPU restatement (its per-call set-up stays below 5 %)
+CPU_SAMPLE_ONE = 512   # positions per single-core step
+
+
+def cpu_model():
+    try:
+        for line in open("/proc/cpuinfo"):
+            if line.startswith("model name"):
+                return line.split(":", 1)[1].strip()
+    except OSError:
+        pass
+    return "unknown"
+
+
+def cpu_iteration(amps, positions, obj, probe, count, threads):
+    """One GD iteration of the FP64 C restatement of the Double CPU path over positions [0, count) (whole detector,
+    whole object); returns its wall time in seconds."""
     from oracle import c_oracle
-    P = len(ds.positions)
-    amps = ds.amplitudes.reshape(P, -1)
+    a = np.ascontiguousarray(amps[:count], np.float64)
+    t0 = time.perf_counter()
+    c_oracle.reconstruct(a, positions[:count], obj, probe, iterations=1, step_size=0.5, threads=threads)
+    return time.perf_counter() - t0
 
-    def run(count):
-        t0 = time.perf_counter()
-        c_oracle.reconstruct(amps[:count].astype(np.float64), ds.positions[:count], ds.object_start, ds.probe,
-                             iterations=1, step_size=0.5, threads=threads)
-        return time.perf_counter() - t0
 
-    count = max(threads, 16)
-    t = run(count)
-    count = int(min(P, max(count, count * target_s / max(t, 1e-3))))
-    t = run(count)
-    return count / t, f"{count} of {P} positions, 1 iteration, full 128x128 detector and 1152x1152 object"
+def cpu_rates(amps, positions, obj, probe, repeats=3):
+    """The CPU baseline both arms report: positions*iter/s of the C restatement on all host cores (median of
+    `repeats` one-iteration calls over CPU_SAMPLE_ALL positions) and on one core (CPU_SAMPLE_ONE positions)."""
+    from oracle import c_oracle
+    threads = c_oracle.host_cores()
+    P = len(positions)
+    count_all, count_one = min(P, CPU_SAMPLE_ALL), min(P, CPU_SAMPLE_ONE)
+    all_t = [cpu_iteration(amps, positions, obj, probe, count_all, threads) for _ in range(repeats)]
+    one_t = [cpu_iteration(amps, positions, obj, probe, count_one, 1) for _ in range(max(1, repeats - 1))]
+    return {"value": count_all / statistics.median(all_t), "unit": UNIT, "cores": threads, "kind": "port",
+            "cpu_model": cpu_model(),
+            "sample": f"one GD iteration over the first {count_all} of {P} positions (whole 128x128 detector and "
+                      f"object), median of {repeats}, FP64 C restatement of the Double path, OpenMP over positions",
+            "single_core": {"value": count_one / statistics.median(one_t), "unit": UNIT, "cores": 1,
+                            "sample": f"one GD iteration over the first {count_one} positions, median of "
+                                      f"{max(1, repeats - 1)}"}}
 
 
 def run_reference(args, world, rank):
     if rank != 0:
         return
-    from cubokit_b200 import synthetic
     from oracle import c_oracle
     threads = c_oracle.host_cores()
     ds = synthetic_dataset_cpu()
     P = len(ds.positions)
     amps = ds.amplitudes.reshape(P, -1)
-    # one step = a bounded sample of the iteration: a fixed subset of positions, scaled to positions*iter/s
-    sample = min(2048, max(threads * 8, 256))
+    # one step = a bounded sample of the iteration: the first CPU_SAMPLE_ALL positions, scaled to positions*iter/s
+    sample = min(P, CPU_SAMPLE_ALL)
     times = []
     for i in range(args.warmup + args.steps):
-        t0 = time.perf_counter()
-        c_oracle.reconstruct(amps[:sample].astype(np.float64), ds.positions[:sample], ds.object_start, ds.probe,
-                             iterations=1, step_size=0.5, threads=threads)
-        dt = time.perf_counter() - t0
+        dt = cpu_iteration(amps, ds.positions, ds.object_start, ds.probe, sample, threads)
         if i >= args.warmup:
             times.append(dt)
     mean = sum(times) / len(times)
@@ -192,6 +378,7 @@ def run_reference(args, world, rank):
                        "form": "CuboPtycho Double CPU path (FP64 C restatement, OpenMP)",
                        "sample_positions_per_step": sample, "l2": "n/a (CPU)"},
             "cpu_baseline": {"value": value, "unit": UNIT, "cores": threads, "kind": "port",
+                             "cpu_model": cpu_model(),
                              "sample": f"{sample} of {P} positions per step, 1 iteration each"},
             "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
     print(json.dumps(line), flush=True)
@@ -212,7 +399,7 @@ def synthetic_dataset_cpu():
     truth = np.exp(1j * synthetic.phase_field(size, size, 1))
     positions = synthetic.raster(SCAN, n, STEP)
     # a sample of rows of the raster is enough for the CPU arm; synthesise only what it reads
-    count = 2048
+    count = CPU_SAMPLE_ALL
     idx = numpy_oracle.patch_indices(n, n, size, size, positions[:count, 0].astype(np.int64),
                                      positions[:count, 1].astype(np.int64))
     f = np.fft.fft2((p.reshape(1, -1) * truth.reshape(-1)[idx]).reshape(count, n, n))
@@ -224,16 +411,17 @@ def synthetic_dataset_cpu():
     return synthetic.Dataset(full, positions, start, p, truth, {})
 
 
-def run_batched(args, world, rank, local):
-    """64 independent reconstructions: scan sides uniform in 24..96 (step 4 px), detectors from {64, 96, 128}^2, each
-    with its own seeded phase field (seed 1000 + i) and probe defocus uniform in 50..200 A; FP32 form; gather tiles
-    picked by the autotuner per detector size; one graph replay per iteration, `steps` iterations timed."""
-    import torch
-    import cubokit_b200 as cb
+BATCH_ITEMS = 64
+
+
+def batched_items(local):
+    """The batched workload's inputs: 64 independent reconstructions, scan sides uniform in 24..96 (step 4 px),
+    detectors from {64, 96, 128}^2, each with its own seeded phase field (seed 1000 + i) and probe defocus uniform in
+    50..200 A; FP32 form; gather tiles picked by the autotuner per detector size."""
     from cubokit_b200 import autotune, synthetic
     rng = np.random.default_rng(7)
     items, sizes = [], []
-    for i in range(64):
+    for i in range(BATCH_ITEMS):
         scan = int(rng.integers(24, 97))
         det = int(rng.choice([64, 96, 128]))
         defocus = float(rng.uniform(50, 200))
@@ -247,32 +435,53 @@ def run_batched(args, world, rank, local):
         if det not in tiles:
             tiles[det] = autotune.tune(it["amplitudes"], it["positions"], it["object"], it["probe"], device=local)[0]
         it["gather_tile"] = tiles[det]
+    return items, sizes, tiles
+
+
+def measure_batched(steps, warmup, world, local):
+    """One graph replay per iteration of the 64-reconstruction batch; `steps` iterations timed on the device."""
+    import torch
+    import cubokit_b200 as cb
+    from cubokit_b200 import autotune
+    items, sizes, tiles = batched_items(local)
     ctx = cb.context(local)
     batch = cb.Batch(items, ctx=ctx)
     stream = torch.cuda.ExternalStream(ctx.stream, device=torch.device("cuda", local))
-    batch.run(args.warmup)
+    batch.run(warmup)
     barrier(world)
     start, stop = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
     with ClockSampler(local) as clocks:
         start.record(stream)
-        batch.run(args.steps, synchronize=False)
+        batch.run(steps, synchronize=False)
         stop.record(stream)
         stop.synchronize()
     ms = max_over_ranks(start.elapsed_time(stop), world)
     total_positions = sum(len(it["positions"]) for it in items)
-    value = total_positions * args.steps / (ms * 1e-3) * world
+    out = {"value": total_positions * steps / (ms * 1e-3) * world, "unit": UNIT, "ms_per_step": ms / steps,
+           "steps": steps, "warmup": warmup, "positions_total": total_positions,
+           "positions_by_detector": {str(d): sum(len(it["positions"]) for it, s in zip(items, sizes) if s[1] == d)
+                                     for d in (64, 96, 128)},
+           "detectors": {str(d): sum(1 for s in sizes if s[1] == d) for d in (64, 96, 128)},
+           "gather_tiles": {str(d): autotune.NAMES[t] for d, t in tiles.items()},
+           "gpu_launches": batch.launches_per_iteration * steps, "graph_launches": steps, "clocks": clocks.summary()}
+    batch.close()
+    return out
+
+
+def run_batched(args, world, rank, local):
+    """The batched workload alone (`--workload batched`)."""
+    r = measure_batched(args.steps, args.warmup, world, local)
     if rank == 0:
         print(json.dumps({
-            "metric": "positions*iter/s, 64 independent reconstructions in one captured graph", "value": value,
-            "unit": UNIT, "n_gpus": world, "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms / args.steps,
-            "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic",
+            "metric": "positions*iter/s, 64 independent reconstructions in one captured graph", "value": r["value"],
+            "unit": UNIT, "n_gpus": world, "steps": args.steps, "warmup": args.warmup,
+            "ms_per_step": r["ms_per_step"], "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+            "dtype": "f32", "data": "synthetic",
             "config": {"workload": "batched: 64 reconstructions, scans 24..96 (step 4), detectors {64,96,128}^2, "
-                                   "defocus 50..200 A, seeds 1000+i", "positions_total": total_positions,
-                       "detectors": {str(d): sum(1 for s in sizes if s[1] == d) for d in (64, 96, 128)},
-                       "gather_tiles": {str(d): autotune.NAMES[t] for d, t in tiles.items()}},
-            "gpu_launches": batch.launches_per_iteration * args.steps, "graph_launches": args.steps,
-            "clocks": clocks.summary()}), flush=True)
-    batch.close()
+                                   "defocus 50..200 A, seeds 1000+i", "positions_total": r["positions_total"],
+                       "detectors": r["detectors"], "gather_tiles": r["gather_tiles"]},
+            "gpu_launches": r["gpu_launches"], "graph_launches": r["graph_launches"], "clocks": r["clocks"]}),
+            flush=True)
 
 
 def run_preprocess(args, world, rank, local):
@@ -308,7 +517,8 @@ def run_preprocess(args, world, rank, local):
     ctx.set_timing(False)
     ms = max_over_ranks(start.elapsed_time(stop), world)
     value = count * args.steps / (ms * 1e-3) * world
-    hbm_peak, _, peak_kind = measured_peaks()
+    _pk = measured_peaks()
+    hbm_peak, peak_kind = _pk["hbm_gbs"], _pk["kind"]
     bytes_step = count * n * 8  # Float32 intensities in, Float32 amplitudes out
     launch_ms = kernel_ms / max(1, kernel_launches)
     e2e = None
@@ -384,7 +594,8 @@ def run_positions(args, world, rank, local):
     plan.set_timing(False)
     plan.close()
     value = P * args.steps / (ms * 1e-3) * world
-    hbm_peak, _, peak_kind = measured_peaks()
+    _pk = measured_peaks()
+    hbm_peak, peak_kind = _pk["hbm_gbs"], _pk["kind"]
     corr_ms, corr_launches = stats["position_correction"]
     corr_ms /= timed_iterations
     # algorithmic bytes of the position update: amplitudes (4n) and the position's shifted probe (16n) read once; the
@@ -457,7 +668,8 @@ def run_mixed(args, world, rank, local):
     plan.set_timing(False)
     plan.close()
     value = P * args.steps / (ms * 1e-3) * world
-    hbm_peak, _, peak_kind = measured_peaks()
+    _pk = measured_peaks()
+    hbm_peak, peak_kind = _pk["hbm_gbs"], _pk["kind"]
     pass_ms = stats["position_pass"][0] / timed_iterations
     # algorithmic bytes of the position pass: amplitudes read once (4n), every state's residual written once (16n)
     pass_bytes = P * (4 + 16 * states) * n
@@ -536,7 +748,8 @@ def run_multislice(args, world, rank, local):
     plan.set_timing(False)
     plan.close()
     value = P * args.steps / (ms * 1e-3) * world
-    hbm_peak, _, peak_kind = measured_peaks()
+    _pk = measured_peaks()
+    hbm_peak, peak_kind = _pk["hbm_gbs"], _pk["kind"]
     pass_ms = stats["position_pass"][0] / timed_iterations
     # algorithmic bytes of the forward pass per pixel: slice 0 writes the wave entering slice 1 (16; the shifted probe
     # and the object come from L2), slices 1 .. L-2 read their entering wave and write the next (32), the last slice
@@ -590,6 +803,10 @@ def main():
                          "FP32 transform (fp32_generic) and the FP64 form")
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--no-cpu", action="store_true")
+    ap.add_argument("--no-parity", action="store_true",
+                    help="skip the per-iteration error curves against the FP64 form and the smaller workloads")
+    ap.add_argument("--parity-iterations", type=int, default=100)
+    ap.add_argument("--no-batched", action="store_true", help="skip the 64-reconstruction batch in the extras")
     ap.add_argument("--scan", type=int, default=SCAN, help="scan side (the benchmark workload is 256)")
     ap.add_argument("--workload", default="precision",
                     choices=["precision", "batched", "preprocess", "positions", "mixed", "multislice"],
@@ -653,51 +870,25 @@ def main():
         ms = max_over_ranks(start.elapsed_time(stop), world)
         launches = plan.launch_count - launches0
         errors = plan.errors(args.warmup + args.steps)
-        obj, _ = plan.get_state()
         # per-kernel device time over separate iterations (events around every launch)
         plan.set_timing(True)
         plan.enqueue(max(3, min(args.steps, 10)))
         stats = plan.kernel_stats()
         plan.set_timing(False)
         plan.close()
-        results[form] = dict(ms=ms, launches=launches, errors=errors, object=obj, stats=stats,
-                             clocks=clocks.summary())
+        results[form] = dict(ms=ms, launches=launches, errors=errors, stats=stats, clocks=clocks.summary())
 
     head = forms[0]
     r = results[head]
     ms = r["ms"]
     stats = r["stats"]
-    bytes_iter, flops_iter = algorithmic(P, n, objects)
-    hbm_peak, bf16_peak, peak_kind = measured_peaks()
     value = P * args.steps / (ms * 1e-3) * world
-    pass_ms, pass_launches = stats["position_pass"]
-    pass_avg_s = pass_ms / max(pass_launches, 1) * 1e-3
-    fft_flops = P * (10 * n * math.log2(n) + 40 * n)  # algorithmic: two 2-D FFTs + 40 flops per pixel per position
-    if head == "split_bf16":
-        # executed tensor work: 4 stages per position, each the real 128 x 128 x 128 product C B of the re and of the im
-        # plane, 3 bf16 split products each: 48 x 2 x 128^3 = 100.7 MFLOP per position
-        tensor_flops = P * 4 * 2 * 3 * 2 * 128 ** 3
-        roofline = {"kernel": "position_pass (bf16_position_kernel)", "bound": "tensor",
-                    "achieved": tensor_flops / pass_avg_s / 1e12, "peak": bf16_peak, "unit": "TFLOP/s",
-                    "frac": tensor_flops / pass_avg_s / 1e12 / bf16_peak, "peak_kind": peak_kind + " (bf16 dense burst)",
-                    # ncu dram__bytes_read.sum + dram__bytes_write.sum of one launch at 4096 positions (748.3 MB,
-                    # profiles/position_pass_bf16_scan64_det128.md), scaled to this launch by positions
-                    "traffic": 748.3e6 / 4096 * P, "executed_tflop_per_launch": tensor_flops / 1e12,
-                    "note": "executed split-BF16 DFT-GEMM flops (100.7 MFLOP per position); the FFT-equivalent "
-                            "algorithmic rate is fft_equivalent_tflops",
-                    "fft_equivalent_tflops": fft_flops / pass_avg_s / 1e12,
-                    "amplitude_hbm_gbs": P * 4 * n / pass_avg_s / 1e9}
-    else:
-        roofline = {"kernel": "position_pass (fast128_kernel)", "bound": "hbm",
-                    "achieved": P * 4 * n / pass_avg_s / 1e9, "peak": hbm_peak, "unit": "GB/s",
-                    "frac": P * 4 * n / pass_avg_s / 1e9 / hbm_peak, "peak_kind": peak_kind, "traffic": None,
-                    "note": "algorithmic bytes = amplitudes read (4n per position); the FP32 form is bound by FP32 "
-                            "issue, reported as fft_equivalent_tflops",
-                    "fft_equivalent_tflops": fft_flops / pass_avg_s / 1e12}
-    roofline["iteration_hbm_gbs"] = bytes_iter / (ms / args.steps * 1e-3) / 1e9
+    peaks = measured_peaks()
+    fma = fma_peaks(ctx)
+    roofline = position_pass_roofline(head, stats, P, n, objects, ms / args.steps, peaks, fma)
     total_stat_ms = sum(v[0] for v in stats.values())
 
-    peaks = fma_peaks(ctx)
+    fft_flops = P * (10 * n * math.log2(n) + 40 * n)
     forms_out = {}
     for form, fr in results.items():
         pass_form_ms = fr["stats"]["position_pass"][0] / max(fr["stats"]["position_pass"][1], 1)
@@ -705,22 +896,25 @@ def main():
                            "position_pass_ms": pass_form_ms, "error_last": float(fr["errors"][-1]),
                            "fft_equivalent_tflops": fft_flops / (pass_form_ms * 1e-3) / 1e12}
         if form in ("fp32", "fp32_generic"):
-            forms_out[form]["frac_of_fp32_fma_peak"] = forms_out[form]["fft_equivalent_tflops"] / peaks["fp32_tflops"]
+            forms_out[form]["frac_of_fp32_fma_peak"] = forms_out[form]["fft_equivalent_tflops"] / fma["fp32_tflops"]
         if form == "fp64":
-            forms_out[form]["frac_of_fp64_fma_peak"] = forms_out[form]["fft_equivalent_tflops"] / peaks["fp64_tflops"]
-    roofline["cuda_core_peaks"] = peaks
+            forms_out[form]["frac_of_fp64_fma_peak"] = forms_out[form]["fft_equivalent_tflops"] / fma["fp64_tflops"]
     comparison = None
     if "split_bf16" in results and "fp32" in results:
-        a, b = results["split_bf16"]["object"], results["fp32"]["object"]
-        comparison = {"ratio_split_bf16_over_fp32": forms_out["split_bf16"]["value"] / forms_out["fp32"]["value"],
-                      "object_rel_l2_split_bf16_vs_fp32": float(np.linalg.norm(a - b) / np.linalg.norm(b)),
-                      "iterations_compared": args.warmup + args.steps}
+        ratio = forms_out["split_bf16"]["value"] / forms_out["fp32"]["value"]
+        comparison = {"ratio_split_bf16_over_fp32": ratio, "target_ratio": 3.0, "target_met": ratio >= 3.0}
         for other in ("fp32_generic", "fp64"):
             if other in results:
-                c = results[other]["object"]
                 comparison[f"ratio_split_bf16_over_{other}"] = (forms_out["split_bf16"]["value"] /
                                                                 forms_out[other]["value"])
-                comparison[f"object_rel_l2_split_bf16_vs_{other}"] = float(np.linalg.norm(a - c) / np.linalg.norm(c))
+
+    # accuracy of the measured forms against the FP64 device form, after every iteration, on this data
+    parity = None
+    if rank == 0 and not args.no_parity and {"split_bf16", "fp32"} <= set(results):
+        parity = {"precision_workload": curve_summary(
+            error_curves(ds, ctx, args.parity_iterations, ("split_bf16", "fp32")),
+            {"split_bf16": 1e-4, "fp32": 1e-5}, f"{args.scan}^2 scan, 128^2 detector, {args.parity_iterations} "
+                                                f"iterations from the same start, each form against the FP64 form")}
 
     e2e = None
     if not args.no_e2e:
@@ -737,10 +931,15 @@ def main():
 
     cpu = None
     if rank == 0 and not args.no_cpu:
-        from oracle import c_oracle
-        threads = c_oracle.host_cores()
-        v, sample = cpu_oracle_sample(ds, threads)
-        cpu = {"value": v, "unit": UNIT, "cores": threads, "kind": "port", "sample": sample}
+        cpu = cpu_rates(ds.amplitudes.reshape(P, -1), ds.positions, ds.object_start, ds.probe)
+    del ds
+
+    extras = {}
+    if rank == 0 and not args.no_parity:
+        extras["fp32_workload"] = fp32_workload_parity(ctx, local)
+        extras["cpu_workload"] = cpu_workload(ctx, local, with_cpu=not args.no_cpu)
+    if rank == 0 and not args.no_batched:
+        extras["batched"] = measure_batched(BATCH_STEPS, 3, 1, local)
 
     if rank == 0:
         line = {
@@ -748,22 +947,21 @@ def main():
             "warmup": args.warmup, "ms_per_step": ms / args.steps, "higher_is_better": True, "scaling": "weak",
             "vs_baseline": None, "dtype": "bf16x3/f32" if head == "split_bf16" else "f32", "data": "synthetic",
             "config": {"workload": f"{args.scan}x{args.scan} scan, step {STEP} px, {DET}x{DET} detector, object "
-                                   f"{ds.object_start.shape[0]}x{ds.object_start.shape[1]}, dose 1e5, GD step 0.5",
+                                   f"{int(math.isqrt(objects))}x{int(math.isqrt(objects))}, dose 1e5, GD step 0.5",
                        "form": head, "positions": P, "parallelism": f"replicas x{world}" if world > 1 else "1 GPU",
                        "l2": f"inputs larger than L2 ({P * n * 4 / 1e9:.2f} GB amplitudes, "
                              f"{P * n * 8 / 1e9:.2f} GB residuals; L2 126 MB)"},
-            "forms": forms_out, "comparison": comparison, "roofline": roofline,
+            "forms": forms_out, "comparison": comparison, "parity": parity, "roofline": roofline,
             "kernels": {k: {"ms_per_launch": v[0] / max(v[1], 1), "launches": v[1],
                             "share": v[0] / total_stat_ms if total_stat_ms else None} for k, v in stats.items() if v[1]},
             "cpu_baseline": cpu, "e2e": e2e, "gpu_launches": r["launches"], "clocks": r["clocks"],
-            "errors_first_last": [float(r["errors"][0]), float(r["errors"][-1])],
+            "errors_first_last": [float(r["errors"][0]), float(r["errors"][-1])], "extras": extras,
         }
         print(json.dumps(line), flush=True)
     barrier(world)
     if world > 1:
         import torch.distributed as dist
         dist.destroy_process_group()
-
 
 if __name__ == "__main__":
     main()

@@ -13,6 +13,7 @@
 // slot that a call reads is written by that same call first, so nothing has to be cleared; the array keeps the last
 // call's values.  All calls on a device share the one array: calls whose kernels overlap on the GPU (different streams,
 // different host threads) race on it, so a caller must order them (one stream, or events).
+#include <cstdint>
 #include <mutex>
 
 #include "../../include/cubo_ptycho.h"
@@ -29,7 +30,8 @@ constexpr int kMaxDevices = 64;
 static __device__ __align__(256) double g_loss_partials[kNoallocMaxPositions];
 
 // Host-side set-up state, per device: the device address of g_loss_partials (the symbol itself is only a host-side
-// stand-in and must never be passed to a kernel).
+// stand-in and must never be passed to a kernel).  It is resolved once per device and kept for the process's life; a
+// cudaDeviceReset of that device would invalidate it, which the header rules out.
 std::mutex g_setup_mutex;
 double *g_partials_address[kMaxDevices] = {};
 
@@ -143,6 +145,11 @@ extern "C" CUBO_PTYCHO_API int cubo_ptycho_loss_fp32_noalloc(int rows, int colum
     if (!(rows > 1 && columns > 1 && object_rows >= rows && object_columns >= columns)) return CUBO_PTYCHO_INVALID_INPUT;
     if (count < 1 || count > kNoallocMaxPositions) return CUBO_PTYCHO_INVALID_INPUT;  // beyond the scratch array
     if (!amplitudes || !centre_rows || !centre_columns || !object || !probe || !loss) return CUBO_PTYCHO_INVALID_INPUT;
+    // the kernels read complex samples as float2 and write the loss as one double: a pointer off that alignment would
+    // fault on the device instead of returning a status
+    if ((((uintptr_t)object | (uintptr_t)probe | (uintptr_t)loss) & 7) != 0 ||
+        (((uintptr_t)amplitudes | (uintptr_t)centre_rows | (uintptr_t)centre_columns) & 3) != 0)
+        return CUBO_PTYCHO_INVALID_INPUT;
     if ((long long)rows * columns > kNoallocMaxN) return CUBO_PTYCHO_UNSUPPORTED;
     int device = 0;
     if (cudaGetDevice(&device) != cudaSuccess) {

@@ -4,7 +4,7 @@
  * This is the drop-in boundary for CuboKit's CuboPtycho hot path.  A SwiftPM system-library target (the way CuboKit
  * already declares CStrainLAPACK and CEmbeddingLAPACK, Package.swift:48,50, with their headers in include/) exposes these
  * functions to Swift; the Swift shim converts [Double]/[Float] to pointers and maps the int status to the reference's
- * throws (INTEGRATION.md shows it).  Conventions follow the reference's C shims
+ * throws (status 1 -> PtychographyError.invalidInput, 2 -> CancellationError).  Conventions follow the reference's C shims
  * (Sources/CStrainLAPACK/include/CStrainLAPACK.h:1-2, Sources/CStrainLAPACK/LeastSquares.c:4-14): functions named
  * cubo_<module>_<verb>, an int status (0 = ok), caller-owned buffers, plain pointers and sizes.
  *
@@ -353,15 +353,18 @@ CUBO_PTYCHO_API int cubo_ptycho_measure_peaks(cubo_ptycho_context *context, doub
  * pool allocator, or a latency-critical loop that must not allocate (cudaMalloc can synchronise the device).
  * Computes loss[0] = sum over positions and detector pixels of (A - |fft2(P * O[patch])|)^2 in FP32 with FP64 sums
  * (the squared amplitude residual of Ptychography.swift:338-342, before any normalisation) for integer scan centres.
- * All pointers are the caller's device memory: amplitudes (count * rows * columns floats, [position][row][column]),
- * centre_rows / centre_columns (count ints, the rounded scan centres; wrapped periodically), object and probe as
- * interleaved complex64 (2 floats per sample, row-major), loss (one double).  Enqueued on `stream` (a cudaStream_t,
+ * All pointers are the caller's device memory: amplitudes (count * rows * columns floats, [position][row][column],
+ * 4-byte aligned), centre_rows / centre_columns (count ints, the rounded scan centres; any value, wrapped periodically),
+ * object and probe as interleaved complex64 (2 floats per sample, row-major, 8-byte aligned), loss (one double, 8-byte
+ * aligned); a misaligned pointer is refused with CUBO_PTYCHO_INVALID_INPUT.  Enqueued on `stream` (a cudaStream_t,
  * NULL = the default stream); returns without waiting.  Allocates nothing: the per-position scratch is a fixed device
  * array of CUBO_PTYCHO_NOALLOC_MAX_POSITIONS doubles inside the library, held on every GPU that loads it until the
- * process exits; count above that maximum is refused with CUBO_PTYCHO_INVALID_INPUT, detectors above 128 x 128 pixels
- * with CUBO_PTYCHO_UNSUPPORTED.  The first call on a device resolves that array's device address (set-up done once per
- * device, with the device current); make that first call before any stream capture.  Every call shares the array, so
- * calls that overlap on the GPU race: order them on one stream. */
+ * process exits; count above that maximum is refused with CUBO_PTYCHO_INVALID_INPUT, detectors of more than 16384
+ * pixels (rows * columns; 128 x 128 is the largest square) with CUBO_PTYCHO_UNSUPPORTED.  The first call on a device
+ * resolves that array's device address (set-up done once per device, with the device current) and keeps it for the
+ * life of the process: make that first call before any stream capture, and do not call this entry point on a device
+ * after cudaDeviceReset of that device.  Every call shares the array, so calls that overlap on the GPU race: order
+ * them on one stream. */
 #define CUBO_PTYCHO_NOALLOC_MAX_POSITIONS (1 << 20)
 CUBO_PTYCHO_API int cubo_ptycho_loss_fp32_noalloc(int rows, int columns, int object_rows, int object_columns, int count,
                                                   const float *amplitudes, const int *centre_rows,

@@ -325,10 +325,11 @@ typedef struct {
     double *pnr, *pni, *on;   /* probe-sized accumulators */
     double *sr, *si, *fr, *fi, *work;
     int *indices;
+    unsigned char *rows_touched; /* object rows any window of this thread's positions covers */
     double error;
 } thread_state;
 
-static void thread_state_init(thread_state *t, size_t objects, size_t n, size_t work) {
+static void thread_state_init(thread_state *t, size_t objects, size_t n, size_t work, int object_rows) {
     t->onr = (double *)calloc(objects, sizeof(double)); t->oni = (double *)calloc(objects, sizeof(double));
     t->pn = (double *)calloc(objects, sizeof(double));
     t->pnr = (double *)calloc(n, sizeof(double)); t->pni = (double *)calloc(n, sizeof(double));
@@ -337,11 +338,24 @@ static void thread_state_init(thread_state *t, size_t objects, size_t n, size_t 
     t->fr = (double *)malloc(n * sizeof(double)); t->fi = (double *)malloc(n * sizeof(double));
     t->work = (double *)malloc(work * sizeof(double));
     t->indices = (int *)malloc(n * sizeof(int));
+    t->rows_touched = (unsigned char *)calloc((size_t)object_rows, 1);
 }
 
 static void thread_state_free(thread_state *t) {
     free(t->onr); free(t->oni); free(t->pn); free(t->pnr); free(t->pni); free(t->on);
-    free(t->sr); free(t->si); free(t->fr); free(t->fi); free(t->work); free(t->indices);
+    free(t->sr); free(t->si); free(t->fr); free(t->fi); free(t->work); free(t->indices); free(t->rows_touched);
+}
+
+/* The object rows the windows of positions [begin, end) cover (the row indices of Ptychography.swift:321-336).  A thread
+ * of the multi-threaded pass zeroes and hands over only these rows of its object-sized accumulators: every other row
+ * holds no contribution, so the fixed-order sum over threads is unchanged while its cost no longer grows with the whole
+ * object per thread. */
+static void mark_rows(unsigned char *touched, int rows, int object_rows, const double *prow, int begin, int end) {
+    memset(touched, 0, (size_t)object_rows);
+    for (int pattern = begin; pattern < end; pattern++) {
+        const long rr = (long)nearbyint(prow[pattern]);
+        for (int r = 0; r < rows; r++) touched[wrapped(rr + (r < (rows + 1) / 2 ? r : r - rows), object_rows)] = 1;
+    }
 }
 
 /* The per-position body of Ptychography.swift:300-358 for positions [begin, end). */
@@ -427,15 +441,28 @@ int oracle_reconstruct(const oracle_params *pp, int rows, int columns, int objec
     int threads = pp->threads > 1 ? pp->threads : 1;
     if (threads > count) threads = count;
     thread_state *ts = (thread_state *)calloc(threads, sizeof(thread_state));
-    for (int t = 0; t < threads; t++) thread_state_init(&ts[t], objects, n, work);
+    for (int t = 0; t < threads; t++) {
+        thread_state_init(&ts[t], objects, n, work, object_rows);
+        mark_rows(ts[t].rows_touched, rows, object_rows, position_rows, (int)((long)count * t / threads),
+                  (int)((long)count * (t + 1) / threads));
+    }
     const double m = pp->normalization_minimum;
+    const size_t row_bytes = sizeof(double) * (size_t)object_columns;
     for (int it = 0; it < pp->iterations; it++) {
         memcpy(psr, probe_re, sizeof(double) * n); memcpy(psi, probe_im, sizeof(double) * n);
         fft2_run_d(&f, psr, psi, 0, w);
         for (int t = 0; t < threads; t++) {
             thread_state *s = &ts[t];
-            memset(s->onr, 0, sizeof(double) * objects); memset(s->oni, 0, sizeof(double) * objects);
-            memset(s->pn, 0, sizeof(double) * objects);
+            if (t == 0) {  /* thread 0's accumulators end up holding the sum: all of them start at zero */
+                memset(s->onr, 0, sizeof(double) * objects); memset(s->oni, 0, sizeof(double) * objects);
+                memset(s->pn, 0, sizeof(double) * objects);
+            } else {
+                for (int y = 0; y < object_rows; y++)
+                    if (s->rows_touched[y]) {
+                        const size_t o = (size_t)y * object_columns;
+                        memset(s->onr + o, 0, row_bytes); memset(s->oni + o, 0, row_bytes); memset(s->pn + o, 0, row_bytes);
+                    }
+            }
             memset(s->pnr, 0, sizeof(double) * n); memset(s->pni, 0, sizeof(double) * n); memset(s->on, 0, sizeof(double) * n);
             s->error = 0;
         }
@@ -454,7 +481,12 @@ int oracle_reconstruct(const oracle_params *pp, int rows, int columns, int objec
             /* fixed-order sum of the per-thread accumulators (thread 0 first) */
             for (int t = 1; t < threads; t++) {
                 thread_state *a = &ts[0], *b = &ts[t];
-                for (size_t j = 0; j < objects; j++) { a->onr[j] += b->onr[j]; a->oni[j] += b->oni[j]; a->pn[j] += b->pn[j]; }
+                for (int y = 0; y < object_rows; y++) {
+                    if (!b->rows_touched[y]) continue;  /* an untouched row of thread t adds nothing */
+                    for (size_t j = (size_t)y * object_columns, e = j + object_columns; j < e; j++) {
+                        a->onr[j] += b->onr[j]; a->oni[j] += b->oni[j]; a->pn[j] += b->pn[j];
+                    }
+                }
                 for (int k = 0; k < n; k++) { a->pnr[k] += b->pnr[k]; a->pni[k] += b->pni[k]; a->on[k] += b->on[k]; }
                 a->error += b->error;
             }

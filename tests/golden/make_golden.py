@@ -5,7 +5,7 @@ The pins are the JSON fixtures of CuboKit's own test suite (``Tests/CuboPtychoTe
 the fields the single-slice gradient-descent engine and the probe builder need and stores them as compressed ``.npz``
 files beside itself, so the tests (which also run where the CuboKit checkout is absent) read plain arrays.
 
-Run once, in a container that has the CuboKit checkout:  python tests/golden/make_golden.py [CUBOKIT_ROOT]
+Run once, in a container that has the CuboKit checkout:  python tests/golden/make_golden.py CUBOKIT_ROOT
 
 Which reference test each group pins (paths inside the CuboKit project):
   ptycho.npz   Tests/CuboPtychoTests/PtychographyTests.swift:33-72,104-118 (engine, variants, constraints, probe build)
@@ -302,7 +302,9 @@ def positions(fx):
 
 
 def main():
-    root = Path(sys.argv[1]) if len(sys.argv) > 1 else Path("/root/reference")
+    if len(sys.argv) != 2:
+        sys.exit("usage: python tests/golden/make_golden.py <CuboKit source tree>")
+    root = Path(sys.argv[1])
     fx = root / "Tests/CuboPtychoTests/Fixtures"
     for name, fn in (("ptycho", ptycho), ("odd", odd), ("engines", engines), ("options", options),
                      ("preprocess", preprocess), ("positions", positions), ("mixed", mixed),
