@@ -17,7 +17,10 @@ detector, 20 iterations, one core and all cores) and the 64-reconstruction batch
 stack and the 8.6 GB residual buffer are far larger than L2, so no flush is needed.  `e2e` is one
 SingleslicePtychography.reconstruct call (the public API) of K iterations from pinned host buffers, host<->device
 copies, validation and plan set-up included, timed by the wall clock around the blocking call.  With --gpus N > 1
-(torchrun), every rank runs an independent replica on its own GPU; value = sum over ranks, time = max over ranks.
+(torchrun), the ranks share ONE reconstruction of the workload (cubokit_b200.sharded: contiguous position bands, the
+bands' gradient sums added in rank order after an all-gather of each rank's touched object rows): value = all
+positions * iterations / the slowest rank's device time, scaling "strong".  The other --workload choices run
+independent replicas per rank.
 `cpu_baseline` and `--impl reference` time the same code: the FP64 C restatement of CuboPtycho's Double CPU path
 (oracle/) over the first 4,096 positions of the workload, one iteration per step, OpenMP over all host cores
 (`cpu_baseline` also gives the single-core rate).
@@ -484,6 +487,73 @@ def run_batched(args, world, rank, local):
             flush=True)
 
 
+def sum_over_ranks(v, world):
+    if world == 1:
+        return v
+    import torch
+    import torch.distributed as dist
+    t = torch.tensor([v], dtype=torch.float64, device="cuda" if dist.get_backend() == "nccl" else "cpu")
+    dist.all_reduce(t)
+    return float(t.item())
+
+
+def run_sharded(args, world, rank, local):
+    """--gpus N > 1: ONE reconstruction of the workload sharded over the ranks (cubokit_b200.sharded: rank r takes
+    the r-th contiguous band of the positions; every iteration each rank runs its band's position pass and gathers,
+    the bands' gradient sums are added in rank order after an all-gather of each rank's touched object rows, and
+    every rank applies the same update).  value = all positions * iterations / the slowest rank's device time
+    (strong scaling: the total work is the workload's whatever N is)."""
+    import torch
+    from cubokit_b200 import sharded, synthetic
+    ds = synthetic.dataset(args.scan, DET, dose=DOSE, step=STEP, pinned=True, device=local)
+    P, n = len(ds.positions), DET * DET
+    form = "fp32" if args.form == "fp32" else "split_bf16"
+    run = sharded.ShardedRun(ds.amplitudes, ds.positions, ds.object_start, ds.probe, precision=form, device=local,
+                             step_size=0.5)
+    try:
+        run.enqueue(args.warmup)
+        run.ctx.synchronize()
+        barrier(world)
+        start, stop = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        launches0 = run.plan.launch_count
+        with ClockSampler(local) as clocks:
+            start.record(run.stream)
+            run.enqueue(args.steps)
+            stop.record(run.stream)
+            stop.synchronize()
+        ms = max_over_ranks(start.elapsed_time(stop), world)
+        launches = sum_over_ranks(run.plan.launch_count - launches0, world)
+        errors = run.result().errors
+    finally:
+        run.close()
+    value = P * args.steps / (ms * 1e-3)
+    e2e = None
+    if not args.no_e2e:
+        barrier(world)
+        t0 = time.perf_counter()
+        r = sharded.reconstruct(ds.amplitudes, ds.positions, ds.object_start, ds.probe, iterations=args.steps,
+                                precision=form, device=local, step_size=0.5)
+        e2e_s = max_over_ranks(time.perf_counter() - t0, world)
+        lo, hi = sharded.band_bounds(P, world, rank)
+        h2d = sum_over_ranks((hi - lo) * n * 4 + (hi - lo) * 16 + ds.object_start.size * 16 + n * 16, world)
+        d2h = sum_over_ranks(ds.object_start.size * 16 + n * 16 + args.steps * 8, world)
+        e2e = {"value": P * args.steps / e2e_s, "unit": UNIT, "seconds": e2e_s, "form": form,
+               "h2d_bytes_per_step": h2d / args.steps, "d2h_bytes_per_step": d2h / args.steps,
+               "final_error": float(r.errors[-1])}
+    if rank == 0:
+        print(json.dumps({
+            "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
+            "warmup": args.warmup, "ms_per_step": ms / args.steps, "higher_is_better": True, "scaling": "strong",
+            "vs_baseline": None, "dtype": "bf16x3/f32" if form == "split_bf16" else "f32", "data": "synthetic",
+            "config": {"workload": f"{args.scan}x{args.scan} scan, step {STEP} px, {DET}x{DET} detector, object "
+                                   f"{ds.object_start.shape[0]}x{ds.object_start.shape[1]}, dose 1e5, GD step 0.5",
+                       "form": form, "positions": P,
+                       "parallelism": f"one reconstruction in {world} position bands (ordered halo exchange)",
+                       "l2": f"inputs larger than L2 ({P * n * 4 / 1e9:.2f} GB amplitudes in all)"},
+            "roofline": None, "cpu_baseline": None, "e2e": e2e, "gpu_launches": launches, "clocks": clocks.summary(),
+            "errors_first_last": [float(errors[0]), float(errors[-1])]}), flush=True)
+
+
 def run_preprocess(args, world, rank, local):
     """Amplitude preprocessing (PtychographyPreparation.amplitudes) over the precision workload's cube: 65,536 patterns
     of 128 x 128 Float32 intensities (the synthetic dataset's squared amplitudes) shifted by a uniform fractional origin
@@ -840,6 +910,13 @@ def main():
         return
     if args.workload == "multislice":
         run_multislice(args, world, rank, local)
+        return
+
+    if world > 1:
+        run_sharded(args, world, rank, local)
+        barrier(world)
+        import torch.distributed as dist
+        dist.destroy_process_group()
         return
 
     ds = synthetic.dataset(args.scan, DET, dose=DOSE, step=STEP, pinned=True, device=local)

@@ -379,7 +379,7 @@ __global__ void __launch_bounds__(kThreads, 1) bf16_position_kernel(Bf16Args a) 
         wait_plane(0);
         wait_plane(1);
         {
-            float2 *out = a.dpsi + (size_t)p * (kN * kN);
+            float2 *out = a.dpsi + (size_t)(p - a.dpsi_first) * (kN * kN);
 #pragma unroll 1
             for (int u = 0; u < 2; u++) {
                 float dr[2][8], di[2][8];

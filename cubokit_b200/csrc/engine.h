@@ -45,6 +45,13 @@ struct ObjectGatherArgs {
     double *tile_max;          // per-tile max of weight
     int states = 1;            // mixed state (FP64): dpsi and shifted hold one block per state, these strides apart
     long long dpsi_state_stride = 0, shifted_state_stride = 0;
+    // One band of the positions ([band_first, band_end), single state): block b takes tile band_tiles[b] and only its
+    // candidates inside the band, whose residuals dpsi holds from position band_first on.  A tile's sums start from
+    // the values grad / weight hold unless the band holds its first candidate, and its tile_max is written by the
+    // band that holds its last one (or by the band that lists it with no candidates at all).  nullptr: every tile,
+    // every candidate, dpsi from position 0.
+    const int *band_tiles = nullptr;
+    int band_first = 0, band_end = 0;
 };
 
 template <typename T>
@@ -56,6 +63,10 @@ struct ProbeGatherArgs {
     const C2<T> *dpsi;
     C2<T> *partial_grad;       // [groups][n]
     T *partial_weight;         // [groups][n]
+    // One band: the positions [first, first + count), their residuals in dpsi from position `first` on, split into the
+    // same `groups`; with `accumulate` each group's sums continue from the partials the earlier bands left.
+    int first = 0;
+    int accumulate = 0;
 };
 
 // The 128 x 128 FP32 position pass (fast128.cu); amplitudes in its register order, 32 residual partials per position.
@@ -66,11 +77,13 @@ struct Fast128Args {
     const float2 *shifted;
     const float2 *object;
     const float *amplitudes;   // [positions][column][h][t][e] (fast128.cu)
-    float2 *dpsi;              // [positions][row][column]
+    float2 *dpsi;              // [positions - dpsi_first][row][column]
+    int dpsi_first;            // the position whose residual dpsi[0] holds (a band's first, or 0)
     double *error;             // [positions][fast128_partials_per_position()]
     const float2 *tw128;       // W_128^t
     float2 *partial_grad;      // [fast128_ctas()][n] probe-gradient partials, one per CTA
     float *partial_weight;     // [fast128_ctas()][n]
+    int accumulate;            // 1: each CTA's partial continues from the one it left (an earlier band), 0: from zero
     int *fault;                // set when the amplitude prefetch wait ran out
 };
 int fast128_ctas();
@@ -89,7 +102,8 @@ struct Bf16Args {
     const float2 *shifted;
     const float2 *object;
     const float *amplitudes;   // permuted into the order the kernel's threads consume them (permute_bf16_amplitudes)
-    float2 *dpsi;              // [positions][row][column]
+    float2 *dpsi;              // [positions - dpsi_first][row][column]
+    int dpsi_first;            // the position whose residual dpsi[0] holds (a band's first, or 0)
     double *error;             // [positions][bf16_partials_per_position()]
     const uint16_t *c_planes;  // [4][128][128] bf16 bits: C hi, C lo, C_sigma hi, C_sigma lo (rows m, columns k)
     int *fault;                // set when a device wait ran out

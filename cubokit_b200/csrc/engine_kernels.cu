@@ -170,12 +170,21 @@ constexpr int kMaxTileSide = 64;    // the longest tile side (tiles are 32 x 8, 
 // column (corner-centred, periodic; negative where the window does not reach), so a pixel's residual index is one sum.
 // MIXED: the mixed-state form (FP64, several states per candidate), its own instance so that its registers do not
 // bound the single-state forms' occupancy.
+// The first index in list[lo, hi) (ascending) whose value is at least v (hi if none).
+__device__ __forceinline__ int lower_bound_index(const int *list, int lo, int hi, int v) {
+    while (lo < hi) {
+        const int mid = (lo + hi) >> 1;
+        if (list[mid] < v) lo = mid + 1; else hi = mid;
+    }
+    return lo;
+}
+
 template <typename T, bool MIXED>
 __global__ void __launch_bounds__(kGatherThreads) object_gather_kernel(ObjectGatherArgs<T> a) {
     __shared__ int s_p[kGatherChunk], s_cls[kGatherChunk];
     __shared__ int s_off[kGatherChunk][kMaxTileSide + kGatherThreads / kMaxTileSide + 4];  // rows, then columns
     __shared__ double scratch[32];
-    const int tile = blockIdx.x;
+    const int tile = a.band_tiles ? a.band_tiles[blockIdx.x] : (int)blockIdx.x;
     const int tx = tile % a.tiles_x, ty = tile / a.tiles_x;
     const int x0 = tx * a.tile_w, y0 = ty * a.tile_h;
     // consecutive threads take consecutive object columns, hence consecutive addresses of each [row][column] residual
@@ -185,7 +194,17 @@ __global__ void __launch_bounds__(kGatherThreads) object_gather_kernel(ObjectGat
     constexpr int kInvalid = -(1 << 30);
     C2<T> g = mk<T>(0, 0);
     T w = 0;
-    const int begin = a.tile_start[tile], end = a.tile_start[tile + 1];
+    const int list_begin = a.tile_start[tile], list_end = a.tile_start[tile + 1];
+    int begin = list_begin, end = list_end;
+    if (a.band_tiles) {  // this band's candidates only; the running sums continue from memory after the first band
+        begin = lower_bound_index(a.tile_list, list_begin, list_end, a.band_first);
+        end = lower_bound_index(a.tile_list, begin, list_end, a.band_end);
+        if (begin != list_begin && inside) {
+            const size_t j = (size_t)y * a.object_columns + x;
+            g = a.grad[j];
+            w = a.weight[j];
+        }
+    }
     for (int base = begin; base < end; base += kGatherChunk) {
         const int cnt = min(kGatherChunk, end - base);
         __syncthreads();
@@ -253,7 +272,7 @@ __global__ void __launch_bounds__(kGatherThreads) object_gather_kernel(ObjectGat
 #pragma unroll
                 for (int u = 0; u < 4; u++) {
                     if (k[u] >= 0) {
-                        d[u] = a.dpsi[(size_t)s_p[i + u] * a.n + k[u]];
+                        d[u] = a.dpsi[(size_t)(s_p[i + u] - a.band_first) * a.n + k[u]];
                         sv[u] = a.shifted[(size_t)s_cls[i + u] * a.n + k[u]];
                     }
                 }
@@ -272,6 +291,7 @@ __global__ void __launch_bounds__(kGatherThreads) object_gather_kernel(ObjectGat
         a.grad[j] = g;
         a.weight[j] = w;
     }
+    if (end != list_end) return;  // a later band still adds to this tile (uniform over the block)
     const double m = block_max<kGatherThreads>(inside ? (double)w : -DBL_MAX, scratch);
     if (threadIdx.x == 0) a.tile_max[tile] = m;
 }
@@ -326,7 +346,8 @@ __global__ void __launch_bounds__(kProbeThreads) probe_gather_kernel(ProbeGather
     __shared__ long long s_base[kChunk];
     const int k = blockIdx.x * kProbeThreads + threadIdx.x;  // pixel index, [row][column]
     const int group = blockIdx.y;
-    const int p0 = (int)((long long)a.count * group / a.groups), p1 = (int)((long long)a.count * (group + 1) / a.groups);
+    const int p0 = a.first + (int)((long long)a.count * group / a.groups);
+    const int p1 = a.first + (int)((long long)a.count * (group + 1) / a.groups);
     const bool valid = k < a.n;
     const int kr = valid ? k / a.columns : 0, kc = valid ? k - kr * a.columns : 0;
     const int offr = corner_offset(kr, a.rows), offc = corner_offset(kc, a.columns);
@@ -335,6 +356,10 @@ __global__ void __launch_bounds__(kProbeThreads) probe_gather_kernel(ProbeGather
     const int low_r = a.rows / 2, high_r = (a.rows + 1) / 2, low_c = a.columns / 2, high_c = (a.columns + 1) / 2;
     C2<T> g = mk<T>(0, 0);
     T w = 0;
+    if (a.accumulate && valid) {  // continue the group's sums over the earlier bands
+        g = a.partial_grad[(size_t)group * a.n + k];
+        w = a.partial_weight[(size_t)group * a.n + k];
+    }
     for (int base = p0; base < p1; base += kChunk) {
         const int cnt = min(kChunk, p1 - base);
         __syncthreads();
@@ -347,7 +372,7 @@ __global__ void __launch_bounds__(kProbeThreads) probe_gather_kernel(ProbeGather
         }
         __syncthreads();
         if (valid) {
-            const C2<T> *dp = a.dpsi + (size_t)base * a.n + k;
+            const C2<T> *dp = a.dpsi + (size_t)(base - a.first) * a.n + k;
             // four positions at a time: independent loads, sums in position order
             for (int i = 0; i < cnt; i += 4) {
                 C2<T> o[4], d[4];

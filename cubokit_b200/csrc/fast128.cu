@@ -217,7 +217,27 @@ __global__ void __launch_bounds__(kThreads, 1) fast128_kernel(Fast128Args a) {
     __syncthreads();
     umma::fence_after_sync();
     const uint32_t acc = acc_base(tmem_base, warp);
-    {
+    if (a.accumulate) {  // an earlier band's partial of this CTA: its sums continue in the same position order
+#pragma unroll
+        for (int l = 0; l < 2; l++)
+#pragma unroll
+            for (int m0 = 0; m0 < 16; m0 += 8) {
+                float gr[8], gi[8], gw[8];
+#pragma unroll
+                for (int i = 0; i < 8; i++) {
+                    const int k = (g + l * kLines) * kN + t + 8 * (m0 + i);
+                    const float2 v = a.partial_grad[(size_t)blockIdx.x * (kN * kN) + k];
+                    gr[i] = v.x;
+                    gi[i] = v.y;
+                    gw[i] = a.partial_weight[(size_t)blockIdx.x * (kN * kN) + k];
+                }
+                const uint32_t col = acc + l * 16 + m0;
+                umma::tmem_st8(col, gr);
+                umma::tmem_st8(col + 32, gi);
+                umma::tmem_st8(col + 64, gw);
+            }
+        umma::tmem_wait_st();
+    } else {
         const float zero[8] = {0, 0, 0, 0, 0, 0, 0, 0};
 #pragma unroll
         for (int c = 0; c < 96; c += 8) umma::tmem_st8(acc + c, zero);
@@ -321,7 +341,7 @@ __global__ void __launch_bounds__(kThreads, 1) fast128_kernel(Fast128Args a) {
         lines_inverse(u0, u1, t, tw, line, x);
 #pragma unroll
         for (int l = 0; l < 2; l++) {
-            float2 *out = a.dpsi + (size_t)p * (kN * kN) + (g + l * kLines) * kN;
+            float2 *out = a.dpsi + (size_t)(p - a.dpsi_first) * (kN * kN) + (g + l * kLines) * kN;
 #pragma unroll
             for (int m = 0; m < 16; m++) out[t + 8 * m] = x[l][m];
         }

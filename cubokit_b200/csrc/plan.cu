@@ -8,6 +8,7 @@
 #include <unordered_map>
 #include <cstdint>
 #include <cstdio>
+#include <cstdlib>
 #include <cstring>
 #include <map>
 #include <memory>
@@ -209,6 +210,11 @@ struct cubo_ptycho_plan {
     bool fast = false;      // 128 x 128 FP32 register-resident position pass
     bool bf16 = false;      // 128 x 128 split-BF16 tensor-core position pass
     bool global64 = false;  // FP64 position pass through global memory (the plane does not fit shared memory)
+    // split-BF16: an iteration runs band by band (position pass, object gather, probe gather of one band of
+    // band_size positions at a time) so that a band's residuals stay in L2 between the pass and the gathers
+    bool banded = false;
+    int band_size = 0, bands = 0;
+    std::vector<int> band_tile_offsets;  // [bands + 1]: band b's object-gather tiles are band_tiles[offsets[b] ..]
     bool plane128 = false;  // FP64 128 x 128 planes: FFT, pointwise step and inverse FFT in one clustered launch
     int plane_cluster = 2;  // CTAs per plane of that launch
     int states = 1;         // probe states (the mixed-state engine; 1 = single slice)
@@ -255,6 +261,7 @@ struct cubo_ptycho_plan {
     DeviceBuffer prop_factors64;  // multislice, 128 x 128 planes: per gap the row and the column factor (128 + 128)
     DeviceBuffer mixed_factors64;  // mixed state, 128 x 128 planes: the projection's factor per position and pixel
     DeviceBuffer tile_counts;          // position correction: candidate counts per tile, rebuilt on the device
+    DeviceBuffer band_tiles, dpsi_band;  // banded iterations: tiles per band, the residuals of one band
     DeviceBuffer shard_loss, shard_counter;  // sharded iterations: this plan's summed squared error, its reduce counter
     long long tile_capacity = 0;       // entries the candidate list holds
 
@@ -485,6 +492,47 @@ void build_scan(cubo_ptycho_plan *p, const double *rows_in, const double *column
     }
 }
 
+// Bands of an iteration run band by band (split-BF16): band b holds positions [b band_size, (b + 1) band_size).  Lists
+// per band the object-gather tiles with a candidate inside it (ascending), and every tile without candidates in band 0,
+// which writes their zero sums and maxima.
+void build_band_tiles(cubo_ptycho_plan *p) {
+    cudaStream_t s = p->ctx->stream;
+    std::vector<int> starts(p->tiles + 1), list;
+    check(cudaMemcpyAsync(starts.data(), p->tile_start.ptr, starts.size() * sizeof(int), cudaMemcpyDeviceToHost, s),
+          "download candidate lists");
+    check(cudaStreamSynchronize(s), "download candidate lists");
+    list.resize(std::max(1, starts[p->tiles]));
+    check(cudaMemcpyAsync(list.data(), p->tile_list.ptr, (size_t)starts[p->tiles] * sizeof(int), cudaMemcpyDeviceToHost,
+                          s), "download candidate lists");
+    check(cudaStreamSynchronize(s), "download candidate lists");
+    std::vector<std::vector<int>> per_band(p->bands);
+    for (int t = 0; t < p->tiles; t++) {
+        if (starts[t] == starts[t + 1]) { per_band[0].push_back(t); continue; }
+        int last = -1;
+        for (int i = starts[t]; i < starts[t + 1]; i++) {  // candidates ascending: their bands too
+            const int b = list[i] / p->band_size;
+            if (b != last) { per_band[b].push_back(t); last = b; }
+        }
+    }
+    p->band_tile_offsets.assign(p->bands + 1, 0);
+    std::vector<int> flat;
+    for (int b = 0; b < p->bands; b++) {
+        std::sort(per_band[b].begin(), per_band[b].end());
+        flat.insert(flat.end(), per_band[b].begin(), per_band[b].end());
+        p->band_tile_offsets[b + 1] = (int)flat.size();
+    }
+    if (flat.empty()) flat.push_back(0);
+    upload(p->band_tiles, flat, s);
+}
+
+// The residuals of every position, for the paths that keep them (the adjoint pair, sharded iterations): allocated at
+// plan creation, or on first use by a banded plan.
+template <typename T>
+void ensure_dpsi(cubo_ptycho_plan *p) {
+    const size_t bytes = (size_t)p->states * p->P * p->n * sizeof(C2<T>);
+    if (p->dpsi.bytes < bytes) check(p->dpsi.alloc(bytes), "cudaMalloc dpsi");
+}
+
 template <typename T>
 void build_plan(cubo_ptycho_plan *p, const cubo_ptycho_problem *pr) {
     cudaStream_t s = p->ctx->stream;
@@ -537,7 +585,14 @@ void build_plan(cubo_ptycho_plan *p, const cubo_ptycho_problem *pr) {
         for (int i = 0; i < P; i++) ident[i] = i;
         upload(p->ident, ident, s);
     }
-    check(p->dpsi.alloc((size_t)p->states * P * n * sizeof(C2<T>)), "cudaMalloc dpsi");
+    if (p->banded) {
+        // one band's residuals; the residuals of every position (the adjoint pair's tape, sharded iterations) are
+        // allocated when first needed
+        check(p->dpsi_band.alloc((size_t)p->band_size * n * sizeof(C2<T>)), "cudaMalloc band residuals");
+        build_band_tiles(p);
+    } else {
+        check(p->dpsi.alloc((size_t)p->states * P * n * sizeof(C2<T>)), "cudaMalloc dpsi");
+    }
     p->error_count = p->fast ? (long long)P * fast128_partials_per_position()
                              : p->bf16 ? (long long)P * bf16_partials_per_position() : P;
     if (p->fast || p->plane128) {
@@ -794,6 +849,7 @@ void enqueue_probe_side(cubo_ptycho_plan *p) {
 template <typename T>
 void enqueue_position_pass(cubo_ptycho_plan *p) {
     cudaStream_t s = p->ctx->stream;
+    ensure_dpsi<T>(p);
     const int n = p->n;
     const ScanTables scan{p->rr.as<int>(), p->cc.as<int>(), p->cls.as<int>()};
     enqueue_shift_table<T>(p);
@@ -808,14 +864,16 @@ void enqueue_position_pass(cubo_ptycho_plan *p) {
         Bf16Args ba{};
         ba.object_rows = p->OR; ba.object_columns = p->OC; ba.first = 0; ba.count = p->P; ba.scan = scan;
         ba.shifted = p->shifted.as<float2>(); ba.object = p->object.as<float2>();
-        ba.amplitudes = p->amplitudes.as<float>(); ba.dpsi = p->dpsi.as<float2>(); ba.error = p->error.as<double>();
+        ba.amplitudes = p->amplitudes.as<float>(); ba.dpsi = p->dpsi.as<float2>(); ba.dpsi_first = 0;
+        ba.error = p->error.as<double>();
         ba.c_planes = p->c_planes.as<uint16_t>(); ba.fault = p->fault.as<int>();
         timed(p, kPositionPass, 1, [&] { return launch_bf16(ba, p->sms, s); });
     } else if (p->fast) {
         Fast128Args fa{};
         fa.object_rows = p->OR; fa.object_columns = p->OC; fa.first = 0; fa.count = p->P; fa.scan = scan;
         fa.shifted = p->shifted.as<float2>(); fa.object = p->object.as<float2>();
-        fa.amplitudes = p->amplitudes.as<float>(); fa.dpsi = p->dpsi.as<float2>(); fa.error = p->error.as<double>();
+        fa.amplitudes = p->amplitudes.as<float>(); fa.dpsi = p->dpsi.as<float2>(); fa.dpsi_first = 0;
+        fa.accumulate = 0; fa.error = p->error.as<double>();
         fa.tw128 = p->tw_r.as<float2>();
         fa.partial_grad = p->partial_grad.as<float2>(); fa.partial_weight = p->partial_weight.as<float>();
         fa.fault = p->fault.as<int>();
@@ -873,6 +931,7 @@ void enqueue_position_pass(cubo_ptycho_plan *p) {
 template <typename T>
 void enqueue_gathers(cubo_ptycho_plan *p) {
     cudaStream_t s = p->ctx->stream;
+    ensure_dpsi<T>(p);
     const int n = p->n;
     const ScanTables scan{p->rr.as<int>(), p->cc.as<int>(), p->cls.as<int>()};
     ObjectGatherArgs<T> ga{};
@@ -899,6 +958,68 @@ void enqueue_gathers(cubo_ptycho_plan *p) {
                                           p->probe_block_max.as<double>(), s);
         });
     }
+    timed(p, kMaxReduce, 2, [&] {
+        cudaError_t e = launch_max_reduce(p->tile_max.as<double>(), p->tiles, p->maxes.as<double>(), s);
+        if (e == cudaSuccess) e = launch_max_reduce(p->probe_block_max.as<double>(), p->probe_blocks, p->maxes.as<double>() + 1, s);
+        return e;
+    });
+}
+
+// The position pass and both gathers band by band (the split-BF16 and the FP32 128 x 128 passes): each band's
+// residuals are written into one band-sized buffer and read back by its object and probe gathers while they are still
+// in L2; the gathers continue every sum from where the previous band left it, in the same candidate order, so the
+// object gradient equals the unbanded gather's bit for bit.  The FP32 pass keeps its per-CTA probe partials across the
+// bands (with bands of whole multiples of its 148 CTAs each CTA still sums its positions in the same order: the probe
+// gradient is the unbanded one too); the split-BF16 form's probe gather groups each band's positions.  Then the probe
+// partials' FP64 reduction and the maxima, as enqueue_gathers.
+void enqueue_banded_pass_and_gathers(cubo_ptycho_plan *p) {
+    cudaStream_t s = p->ctx->stream;
+    const int n = p->n;
+    const ScanTables scan{p->rr.as<int>(), p->cc.as<int>(), p->cls.as<int>()};
+    enqueue_shift_table<float>(p);
+    Fast128Args fa{};  // the FP32 128 x 128 pass: the probe-gradient partials accumulate in the pass, per CTA
+    fa.object_rows = p->OR; fa.object_columns = p->OC; fa.scan = scan;
+    fa.shifted = p->shifted.as<float2>(); fa.object = p->object.as<float2>();
+    fa.amplitudes = p->amplitudes.as<float>(); fa.dpsi = p->dpsi_band.as<float2>(); fa.error = p->error.as<double>();
+    fa.tw128 = p->tw_r.as<float2>();
+    fa.partial_grad = p->partial_grad.as<float2>(); fa.partial_weight = p->partial_weight.as<float>();
+    fa.fault = p->fault.as<int>();
+    Bf16Args ba{};
+    ba.object_rows = p->OR; ba.object_columns = p->OC; ba.scan = scan;
+    ba.shifted = p->shifted.as<float2>(); ba.object = p->object.as<float2>();
+    ba.amplitudes = p->amplitudes.as<float>(); ba.dpsi = p->dpsi_band.as<float2>(); ba.error = p->error.as<double>();
+    ba.c_planes = p->c_planes.as<uint16_t>(); ba.fault = p->fault.as<int>();
+    ObjectGatherArgs<float> ga{};
+    ga.rows = p->R; ga.columns = p->C; ga.object_rows = p->OR; ga.object_columns = p->OC; ga.n = n;
+    ga.tiles_x = p->tiles_x; ga.tile_w = p->tile_w; ga.tile_h = p->tile_h;
+    ga.tile_start = p->tile_start.as<int>(); ga.tile_list = p->tile_list.as<int>();
+    ga.scan = scan; ga.shifted = p->shifted.as<float2>(); ga.dpsi = p->dpsi_band.as<float2>();
+    ga.grad = p->grad_o.as<float2>(); ga.weight = p->weight_o.as<float>(); ga.tile_max = p->tile_max.as<double>();
+    ProbeGatherArgs<float> pg{};
+    pg.rows = p->R; pg.columns = p->C; pg.object_rows = p->OR; pg.object_columns = p->OC; pg.n = n;
+    pg.groups = p->groups; pg.scan = scan; pg.object = p->object.as<float2>(); pg.dpsi = p->dpsi_band.as<float2>();
+    pg.partial_grad = p->partial_grad.as<float2>(); pg.partial_weight = p->partial_weight.as<float>();
+    for (int b = 0; b < p->bands; b++) {
+        const int first = b * p->band_size, count = std::min(p->band_size, p->P - first);
+        if (p->bf16) {
+            ba.first = first; ba.count = count; ba.dpsi_first = first;
+            timed(p, kPositionPass, 1, [&] { return launch_bf16(ba, p->sms, s); });
+        } else {
+            fa.first = first; fa.count = count; fa.dpsi_first = first; fa.accumulate = b > 0 ? 1 : 0;
+            timed(p, kPositionPass, 1, [&] { return launch_fast128(fa, p->sms, s); });
+        }
+        const int tiles = p->band_tile_offsets[b + 1] - p->band_tile_offsets[b];
+        ga.band_tiles = p->band_tiles.as<int>() + p->band_tile_offsets[b];
+        ga.band_first = first; ga.band_end = first + count;
+        if (tiles > 0) timed(p, kObjectGather, 1, [&] { return launch_object_gather<float>(ga, tiles, s); });
+        pg.first = first; pg.count = count; pg.accumulate = b > 0 ? 1 : 0;
+        if (p->bf16) timed(p, kProbeGather, 1, [&] { return launch_probe_gather<float>(pg, s); });
+    }
+    timed(p, kProbeReduce, 1, [&] {
+        return launch_probe_reduce<float>(p->partial_grad.as<float2>(), p->partial_weight.as<float>(), p->groups, n,
+                                          p->grad_p64.as<double2>(), p->weight_p64.as<double>(),
+                                          p->probe_block_max.as<double>(), s);
+    });
     timed(p, kMaxReduce, 2, [&] {
         cudaError_t e = launch_max_reduce(p->tile_max.as<double>(), p->tiles, p->maxes.as<double>(), s);
         if (e == cudaSuccess) e = launch_max_reduce(p->probe_block_max.as<double>(), p->probe_blocks, p->maxes.as<double>() + 1, s);
@@ -951,8 +1072,12 @@ void enqueue_position_correction(cubo_ptycho_plan *p) {
 template <typename T>
 void enqueue_iteration(cubo_ptycho_plan *p) {
     cudaStream_t s = p->ctx->stream;
-    enqueue_position_pass<T>(p);
-    enqueue_gathers<T>(p);
+    if (p->banded) {
+        enqueue_banded_pass_and_gathers(p);
+    } else {
+        enqueue_position_pass<T>(p);
+        enqueue_gathers<T>(p);
+    }
     const cubo_ptycho_params &pp = p->params;
     const bool correct = std::is_same<T, double>::value && p->correct_positions;
     if (correct)
@@ -1419,6 +1544,21 @@ int create_plan(cubo_ptycho_context *ctx, const cubo_ptycho_problem *pr, const c
         p->fast = !p->fp64 && !p->bf16 && pp->variant != CUBO_PTYCHO_VARIANT_GENERIC && fast128_applicable(p->R, p->C);
         if (p->fast) check(configure_fast128(), "configure 128 x 128 kernel");
         check(cudaDeviceGetAttribute(&p->sms, cudaDevAttrMultiProcessorCount, ctx->device), "attribute");
+        if (p->bf16 || p->fast) {
+            // bands of whole waves of the pass (one position per CTA each: the SMs, or the FP32 pass's fixed 148
+            // CTAs) whose residuals take at most ~64 MB of the 126 MB L2; CUBO_PTYCHO_BAND_POSITIONS overrides the
+            // size (0: one band of every position, i.e. the residuals of the whole scan in HBM)
+            const size_t per_position = (size_t)p->n * sizeof(float2);
+            const int wave = p->fast ? fast128_ctas() : p->sms;
+            long long size = (long long)std::max<size_t>(1, (64ull << 20) / per_position / wave) * wave;
+            if (const char *env = std::getenv("CUBO_PTYCHO_BAND_POSITIONS")) {
+                const long long v = std::atoll(env);
+                size = v > 0 ? v : p->P;
+            }
+            p->band_size = (int)std::max<long long>(1, std::min<long long>(size, p->P));
+            p->bands = (p->P + p->band_size - 1) / p->band_size;
+            p->banded = true;
+        }
         p->kind_ms.assign(kKinds, 0.0);
         p->kind_launches.assign(kKinds, 0);
         p->correct_positions = pp->has_position_correction != 0;  // before the scan tables: one class per position
