@@ -460,7 +460,31 @@ def measure_batched(steps, warmup, world, local):
         stop.synchronize()
     ms = max_over_ranks(start.elapsed_time(stop), world)
     total_positions = sum(len(it["positions"]) for it in items)
+    # one reconstruction of each detector size alone (a 60 x 60 scan, the batch's mean side), to set the batch's rate
+    # against the single-reconstruction rate at equal detector sizes
+    from cubokit_b200 import synthetic
+    single = {}
+    for det in (64, 96, 128):
+        ds = synthetic.dataset(60, det, dose=DOSE, step=STEP, seed_object=77, seed_noise=78, seed_start=79,
+                               device=local)
+        plan = cb.Plan(ds.amplitudes, ds.positions, ds.object_start.shape, ds.probe.shape, ctx=ctx, step_size=0.5,
+                       precision="fp32", gather_tile=tiles.get(det, 0))
+        plan.set_state(ds.object_start, ds.probe)
+        plan.enqueue(warmup)
+        ctx.synchronize()
+        a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        a.record(stream)
+        plan.enqueue(steps)
+        b.record(stream)
+        b.synchronize()
+        single[str(det)] = len(ds.positions) * steps / (a.elapsed_time(b) * 1e-3)
+        plan.close()
+    by_det = {d: sum(len(it["positions"]) for it, s in zip(items, sizes) if s[1] == d) for d in (64, 96, 128)}
+    single_equivalent = total_positions / sum(by_det[d] / single[str(d)] for d in (64, 96, 128) if by_det[d])
     out = {"value": total_positions * steps / (ms * 1e-3) * world, "unit": UNIT, "ms_per_step": ms / steps,
+           "single_reconstruction_by_detector": {"value": single, "unit": UNIT, "scan": "60x60, FP32 form"},
+           "single_equivalent_value": single_equivalent,
+           "batch_over_single_equivalent": total_positions * steps / (ms * 1e-3) * world / single_equivalent,
            "steps": steps, "warmup": warmup, "positions_total": total_positions,
            "positions_by_detector": {str(d): sum(len(it["positions"]) for it, s in zip(items, sizes) if s[1] == d)
                                      for d in (64, 96, 128)},

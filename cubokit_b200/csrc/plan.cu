@@ -1545,19 +1545,20 @@ int create_plan(cubo_ptycho_context *ctx, const cubo_ptycho_problem *pr, const c
         if (p->fast) check(configure_fast128(), "configure 128 x 128 kernel");
         check(cudaDeviceGetAttribute(&p->sms, cudaDevAttrMultiProcessorCount, ctx->device), "attribute");
         if (p->bf16 || p->fast) {
-            // bands of whole waves of the pass (one position per CTA each: the SMs, or the FP32 pass's fixed 148
-            // CTAs) whose residuals take at most ~64 MB of the 126 MB L2; CUBO_PTYCHO_BAND_POSITIONS overrides the
-            // size (0: one band of every position, i.e. the residuals of the whole scan in HBM)
-            const size_t per_position = (size_t)p->n * sizeof(float2);
-            const int wave = p->fast ? fast128_ctas() : p->sms;
-            long long size = (long long)std::max<size_t>(1, (64ull << 20) / per_position / wave) * wave;
+            // CUBO_PTYCHO_BAND_POSITIONS = k > 0 runs the iteration in bands of k positions (their residuals in one
+            // band-sized buffer, read back by the band's gathers while still in L2); unset or 0: one pass over every
+            // position.  Bands of 444 positions (three waves of the pass, 57 MB of residuals) measured 19.4 ms per
+            // iteration at the 256^2-scan, 128^2-detector workload against 12.3 ms in one pass: each band's launches
+            // cost more than the L2 reads save (the pass ~30 us more per launch than its share of one pass, the
+            // gathers twice as long per position on band-sized grids), so one pass is the default.
+            long long size = p->P;
             if (const char *env = std::getenv("CUBO_PTYCHO_BAND_POSITIONS")) {
                 const long long v = std::atoll(env);
-                size = v > 0 ? v : p->P;
+                if (v > 0) size = v;
             }
             p->band_size = (int)std::max<long long>(1, std::min<long long>(size, p->P));
             p->bands = (p->P + p->band_size - 1) / p->band_size;
-            p->banded = true;
+            p->banded = p->bands > 1;
         }
         p->kind_ms.assign(kKinds, 0.0);
         p->kind_launches.assign(kKinds, 0);

@@ -84,11 +84,11 @@ def test_split_bf16_adjoint_against_fp64():
     assert np.max(np.abs(gp1 - gp2)) <= 1e-3 * np.max(np.abs(gp2))
 
 
-def _bf16_run(s, iterations, band_positions, monkeypatch):
+def _bf16_run(s, iterations, band_positions, monkeypatch, precision="split_bf16"):
     import cubokit_b200 as cb
     monkeypatch.setenv("CUBO_PTYCHO_BAND_POSITIONS", str(band_positions))
     plan = cb.Plan(s["amplitudes"], s["positions"], s["object"].shape, s["probe"].shape, step_size=0.5,
-                   precision="split_bf16")
+                   precision=precision)
     try:
         plan.set_state(s["object"], s["probe"])
         errors = plan.iterate(iterations)
@@ -99,8 +99,8 @@ def _bf16_run(s, iterations, band_positions, monkeypatch):
 
 
 def test_banded_iteration_equals_one_band(monkeypatch):
-    """The iteration runs in bands of positions whose residuals stay in L2 (each band's pass, then its object and probe
-    gathers).  The object gather continues every pixel's sum from memory in the same candidate order, so after one
+    """With CUBO_PTYCHO_BAND_POSITIONS the iteration runs in bands of positions whose residuals stay in L2 (each band's
+    pass, then its object and probe gathers).  The object gather continues every pixel's sum from memory in the same candidate order, so after one
     iteration the object equals the one-band run bit for bit; the probe partials are grouped per band, so the probe
     (and every later iteration) agrees to FP32 round-off.  Band sizes that do not divide the scan, and one position per
     band, included."""
@@ -114,3 +114,13 @@ def test_banded_iteration_equals_one_band(monkeypatch):
     o4, _, _ = _bf16_run(s, 4, 0, monkeypatch)
     ob4, _, _ = _bf16_run(s, 4, 16, monkeypatch)
     assert rel_l2(ob4, o4) <= 1e-6, rel_l2(ob4, o4)
+
+
+def test_banded_fp32_iteration_equals_one_pass(monkeypatch):
+    """The FP32 128 x 128 pass keeps one probe-gradient partial per CTA (148 of them) across the bands: with bands of
+    whole multiples of 148 positions every CTA still sums its positions in the same order, so object, probe and errors
+    equal one pass bit for bit, iteration after iteration (169 positions: a full band and a partial one)."""
+    s = scenes.raster_scene(scan=13, det=128, step=4, seed=31)
+    o1, p1, e1 = _bf16_run(s, 3, 0, monkeypatch, precision="fp32")
+    ob, pb, eb = _bf16_run(s, 3, 148, monkeypatch, precision="fp32")
+    assert np.array_equal(ob, o1) and np.array_equal(pb, p1) and np.array_equal(eb, e1)
