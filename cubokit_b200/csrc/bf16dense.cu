@@ -24,12 +24,15 @@
 // (M = N = 128, K = 16) per plane and stage.  The two planes run as a pipeline: the re plane's result is read out and
 // its next stage issued while the tensor core still works on the im plane.
 //
-// One persistent CTA of 512 threads per SM with 208 KB of shared memory: the four B planes and the next position's
-// amplitudes, bulk-copied in behind stages 3 to 2.  Tensor memory: C hi / lo (columns 0-127), C_sigma hi / lo (128-255), the
-// re-plane result (256-383), the im-plane result (384-511).  Thread (warp w, lane i) owns TMEM lane 32 (w mod 4) + i and
-// the 32-column group w / 4 of each result.  Amplitudes are pre-permuted into the order each thread consumes them
-// (a warp reads 512 contiguous bytes per load); dpsi is written [position][row][column].  Waits are bounded: a wait
-// that runs out sets *fault and the CTA stops after freeing its tensor memory.
+// One persistent CTA of kThreads = 512 threads per SM with 208 KB of shared memory: the four B planes and the next
+// position's amplitudes, bulk-copied in behind stages 3 to 2.  Tensor memory: C hi / lo (columns 0-127), C_sigma hi / lo
+// (128-255), the re-plane result (256-383), the im-plane result (384-511).  Thread (warp w, lane i) owns TMEM lane
+// 32 (w mod 4) + i and the kCols-column group w / 4 of each result (kCols = 32).  The layout constants follow from
+// kThreads; 1024 threads (kCols = 16, 64 registers) measured 8.91 against 8.37 ms per pass of 65,536 positions: the
+// phases between the products are bound by instruction issue more than by latency, and twice the warps only add barrier
+// cost and spills.  Amplitudes are pre-permuted into the order each thread consumes them (a warp reads 512 contiguous
+// bytes per load); dpsi is written [position][row][column].  Waits are bounded: a wait that runs out sets *fault and
+// the CTA stops after freeing its tensor memory.
 #include "engine.h"
 #include "umma.cuh"
 
@@ -41,6 +44,13 @@ using namespace umma;
 
 constexpr int kN = 128;
 constexpr int kThreads = 512;
+constexpr int kWarps = kThreads / 32;
+constexpr int kGroups = kWarps / 4;        // warps per TMEM lane quadrant: column groups of a result
+constexpr int kCols = kN / kGroups;        // result columns per thread (32)
+constexpr int kSub = kCols / 16;           // sub-blocks of 4 column pairs per parity set (2)
+constexpr int kRowsPerWarp = kN / kWarps;  // exit-wave rows per warp (8)
+constexpr int kBatch = 2048 / kThreads;    // exit-wave rows whose loads are in flight at once (4)
+static_assert(kCols % 16 == 0 && kRowsPerWarp % kBatch == 0, "thread layout");
 // Canonical no-swizzle layout of a 128 x 128 bf16 plane with its core matrices (8 rows x 16 bytes) 144 bytes apart
 // along K: the 16 bytes of padding put the K chunks of one row in different banks, so 4-byte stores of consecutive K
 // by consecutive lanes (the exit wave) and 16-byte stores of consecutive rows (the other stages) are conflict-free.
@@ -84,19 +94,18 @@ __device__ __forceinline__ void issue_plane(uint32_t tmem, uint32_t a_col, uint3
     }
 }
 
-// Lane `row`'s 32 columns of one result (from taddr) -> 32 consecutive K of row `row` of a K-major B plane pair.
+// Lane `row`'s kCols columns of one result (from taddr) -> kCols consecutive K of row `row` of a K-major B plane pair.
 __device__ __forceinline__ void readout_kmajor(uint32_t taddr, uint8_t *planes, int hi_plane, int row, int k0) {
-    float a[16], b[16];
-    tmem_ld16(taddr, a);
-    tmem_ld16(taddr + 16, b);
+    float a[kCols];
+#pragma unroll
+    for (int c = 0; c < kCols / 16; c++) tmem_ld16(taddr + 16 * c, *reinterpret_cast<float(*)[16]>(a + 16 * c));
     tmem_wait_ld();
 #pragma unroll
-    for (int c = 0; c < 2; c++) {
-        float v0[8], v1[8];
+    for (int c = 0; c < kCols / 8; c++) {
+        float v[8];
 #pragma unroll
-        for (int i = 0; i < 8; i++) { v0[i] = a[8 * c + i]; v1[i] = b[8 * c + i]; }
-        store_split8(planes, hi_plane, kmajor_offset(row, k0 + 8 * c), v0);
-        store_split8(planes, hi_plane, kmajor_offset(row, k0 + 16 + 8 * c), v1);
+        for (int i = 0; i < 8; i++) v[i] = a[8 * c + i];
+        store_split8(planes, hi_plane, kmajor_offset(row, k0 + 8 * c), v);
     }
 }
 
@@ -114,17 +123,24 @@ __device__ __forceinline__ void combine(float zr, float zi, float sr, float si, 
     }
 }
 
+// The column index J of a thread's value i (0..3) of sub-block u: its column group g and parity h (= L & 1) own the
+// raw result columns kCols g .. kCols g + kCols - 1, i.e. the column pairs (2J, 2J + 1) of J = (kCols / 2) g + 0 ..
+// kCols / 2 - 1, of which it keeps, after the exchange with lane L ^ 1, the half of parity h.
+__host__ __device__ __forceinline__ int column_of(int g, int h, int u, int i) {
+    return (kCols / 2) * g + (kCols / 4) * h + 4 * u + i;
+}
+
 // One thread's 16 values of a combined stage result for sub-block u: T on the columns (in the thread), then the
-// exchange with lane L ^ 1, then T on the row pair (2j, 2j + 1).  out[side][s][i] is the value at row
-// (side ? mirror(j) : j) and column (s ? mirror(J) : J), J = 16 g + 8 h + 4 u + i, h = L & 1.
+// exchange with lane L ^ 1, then T on the row pair (2j, 2j + 1).  out[side][4 s + i] is the value at row
+// (side ? mirror(j) : j) and column (s ? mirror(J) : J), J = column_of(g, h, u, i), h = L & 1.
 template <bool kInverse>
 __device__ __forceinline__ void combined_block(uint32_t lane_addr, int g, int u, int j, int h, float (&out_re)[2][8],
                                                float (&out_im)[2][8]) {
-    float r0[8], r1[8], i0[8], i1[8];  // raw columns of parity sets 0 and 1: 32 g + 16 h' + 8 u .. + 8
-    tmem_ld8(lane_addr + kSlotRe + 32 * g + 8 * u, r0);
-    tmem_ld8(lane_addr + kSlotRe + 32 * g + 16 + 8 * u, r1);
-    tmem_ld8(lane_addr + kSlotIm + 32 * g + 8 * u, i0);
-    tmem_ld8(lane_addr + kSlotIm + 32 * g + 16 + 8 * u, i1);
+    float r0[8], r1[8], i0[8], i1[8];  // raw columns of parity sets 0 and 1: kCols g + (kCols / 2) h' + 8 u .. + 8
+    tmem_ld8(lane_addr + kSlotRe + kCols * g + 8 * u, r0);
+    tmem_ld8(lane_addr + kSlotRe + kCols * g + kCols / 2 + 8 * u, r1);
+    tmem_ld8(lane_addr + kSlotIm + kCols * g + 8 * u, i0);
+    tmem_ld8(lane_addr + kSlotIm + kCols * g + kCols / 2 + 8 * u, i1);
     tmem_wait_ld();
     // T on the columns for both parity sets: ya / yb [s][i] (complex as re, im)
     float ar[2][4], ai[2][4], br[2][4], bi[2][4];
@@ -189,11 +205,15 @@ __global__ void __launch_bounds__(kThreads, 1) bf16_position_kernel(Bf16Args a) 
     // (k = 2c, 2c + 1) of row m
 #pragma unroll 1
     for (int v = 0; v < 4; v++) {
-        uint32_t r[16];
-        const uint32_t *src = reinterpret_cast<const uint32_t *>(a.c_planes + ((size_t)v * kN + L) * kN) + 16 * g;
+        constexpr int kw = 64 / kGroups;  // bf16 pairs of the plane's row per thread
+        const uint32_t *src = reinterpret_cast<const uint32_t *>(a.c_planes + ((size_t)v * kN + L) * kN) + kw * g;
 #pragma unroll
-        for (int i = 0; i < 16; i++) r[i] = src[i];
-        tmem_st16(lane_addr + 64 * v + 16 * g, r);
+        for (int c0 = 0; c0 < kw; c0 += 8) {
+            float r[8];
+#pragma unroll
+            for (int i = 0; i < 8; i++) r[i] = __uint_as_float(src[c0 + i]);
+            tmem_st8(lane_addr + 64 * v + kw * g + c0, r);
+        }
     }
     tmem_wait_st();
     uint32_t phase = 0u, pending = 0u;  // bit x: parity to wait for / commit outstanding, of plane x's barrier
@@ -219,24 +239,25 @@ __global__ void __launch_bounds__(kThreads, 1) bf16_position_kernel(Bf16Args a) 
     };
     const float inv_n = 1.0f / (float)(kN * kN);
     for (int p = a.first + blockIdx.x; p < last; p += gridDim.x) {
-        // ---- stage 1: B[n = r][k = c] = X.  Warp w takes rows 8w .. 8w + 7, each in two halves of 64 columns; lane i
-        // the columns 2i, 2i + 1 of a half: one contiguous 512-byte segment of the object row and of the probe row per
-        // warp and load, one 4-byte bf16 pair per plane and lane per store.
+        // ---- stage 1: B[n = r][k = c] = X.  Warp w takes rows kRowsPerWarp w .. + kRowsPerWarp - 1, each in two halves
+        // of 64 columns; lane i the columns 2i, 2i + 1 of a half: one contiguous 512-byte segment of the object row and
+        // of the probe row per warp and load, one 4-byte bf16 pair per plane and lane per store.
         {
             const int rr = a.scan.rr[p], cc = a.scan.cc[p], cls = a.scan.cls[p];
             const int OC = a.object_columns;
-            const float2 *S = a.shifted + (size_t)cls * (kN * kN) + 8 * warp * kN + 2 * lane;
-            // patch rows 8w .. 8w + 7 are object rows y0 .. y0 + 7 (wrapped), y0 = rr + 8w, or rr + 8w - 128 past the
-            // centre row
-            const int y0 = rr + (warp < 8 ? 8 * warp : 8 * warp - kN);
+            const int row0 = kRowsPerWarp * warp;  // the warp's first patch row
+            const float2 *S = a.shifted + (size_t)cls * (kN * kN) + row0 * kN + 2 * lane;
+            // patch rows row0 .. row0 + kRowsPerWarp - 1 are object rows y0 .. (wrapped), y0 = rr + row0, or
+            // rr + row0 - 128 past the centre row (a warp's rows never straddle it)
+            const int y0 = rr + (row0 < kN / 2 ? row0 : row0 - kN);
             // the patch row is the object row segment [cc - 64, cc + 64) (its columns 64..127, then 0..63): one
             // aligned float4 per lane and half when it does not wrap and starts on an even complex
             if (cc >= kN / 2 && cc + kN / 2 <= OC && ((cc | OC) & 1) == 0) {
 #pragma unroll
-                for (int b0 = 0; b0 < 8; b0 += 4) {  // rows b0 .. b0 + 3 of the warp, both halves: 16 loads in flight
-                    float4 sv[8], ov[8];
+                for (int b0 = 0; b0 < kRowsPerWarp; b0 += kBatch) {  // kBatch rows, both halves: 4 kBatch loads in flight
+                    float4 sv[2 * kBatch], ov[2 * kBatch];
 #pragma unroll
-                    for (int i = 0; i < 4; i++) {
+                    for (int i = 0; i < kBatch; i++) {
                         const float2 *orow = a.object + (size_t)wrap_once(y0 + b0 + i, a.object_rows) * OC + cc + 2 * lane;
                         sv[2 * i] = __ldg(reinterpret_cast<const float4 *>(S + (b0 + i) * kN));
                         sv[2 * i + 1] = __ldg(reinterpret_cast<const float4 *>(S + (b0 + i) * kN + kN / 2));
@@ -244,13 +265,13 @@ __global__ void __launch_bounds__(kThreads, 1) bf16_position_kernel(Bf16Args a) 
                         ov[2 * i + 1] = __ldg(reinterpret_cast<const float4 *>(orow - kN / 2));
                     }
 #pragma unroll
-                    for (int u = 0; u < 8; u++) {
+                    for (int u = 0; u < 2 * kBatch; u++) {
                         const float4 sp = sv[u], o = ov[u];
                         uint32_t rh, rl, ih, il;
                         split_bf16x2(sp.x * o.x - sp.y * o.y, sp.z * o.z - sp.w * o.w, rh, rl);
                         split_bf16x2(sp.x * o.y + sp.y * o.x, sp.z * o.w + sp.w * o.z, ih, il);
-                        // row 8w + b0 + u/2, columns 64 (u & 1) + 2 lane
-                        const uint32_t off = kmajor_offset(8 * warp + b0 + (u >> 1), 64 * (u & 1) + 2 * lane);
+                        // row row0 + b0 + u/2, columns 64 (u & 1) + 2 lane
+                        const uint32_t off = kmajor_offset(row0 + b0 + (u >> 1), 64 * (u & 1) + 2 * lane);
                         *reinterpret_cast<uint32_t *>(planes + (kReHi + 0) * kPlaneBytes + off) = rh;
                         *reinterpret_cast<uint32_t *>(planes + (kReHi + 1) * kPlaneBytes + off) = rl;
                         *reinterpret_cast<uint32_t *>(planes + (kImHi + 0) * kPlaneBytes + off) = ih;
@@ -260,7 +281,7 @@ __global__ void __launch_bounds__(kThreads, 1) bf16_position_kernel(Bf16Args a) 
             } else {
                 // near the object's edge (or an odd row length): complex by complex, each column wrapped
 #pragma unroll 1
-                for (int u = 0; u < 16; u++) {
+                for (int u = 0; u < 2 * kRowsPerWarp; u++) {
                     const int i = u >> 1, c = 64 * (u & 1) + 2 * lane;
                     const float2 *orow = a.object + (size_t)wrap_once(y0 + i, a.object_rows) * OC;
                     const int x = cc + (c < kN / 2 ? c : c - kN);
@@ -269,7 +290,7 @@ __global__ void __launch_bounds__(kThreads, 1) bf16_position_kernel(Bf16Args a) 
                     uint32_t rh, rl, ih, il;
                     split_bf16x2(sp.x * o0.x - sp.y * o0.y, sp.z * o1.x - sp.w * o1.y, rh, rl);
                     split_bf16x2(sp.x * o0.y + sp.y * o0.x, sp.z * o1.y + sp.w * o1.x, ih, il);
-                    const uint32_t off = kmajor_offset(8 * warp + i, c);
+                    const uint32_t off = kmajor_offset(row0 + i, c);
                     *reinterpret_cast<uint32_t *>(planes + (kReHi + 0) * kPlaneBytes + off) = rh;
                     *reinterpret_cast<uint32_t *>(planes + (kReHi + 1) * kPlaneBytes + off) = rl;
                     *reinterpret_cast<uint32_t *>(planes + (kImHi + 0) * kPlaneBytes + off) = ih;
@@ -287,7 +308,7 @@ __global__ void __launch_bounds__(kThreads, 1) bf16_position_kernel(Bf16Args a) 
         pending = 3u;
         // ---- stage 2: B[n = raw c][k = r] = D1, each plane as soon as its stage-1 product is done
         wait_plane(0);
-        readout_kmajor(lane_addr + kSlotRe + 32 * g, planes, kReHi, L, 32 * g);
+        readout_kmajor(lane_addr + kSlotRe + kCols * g, planes, kReHi, L, kCols * g);
         if (!publish()) break;
         if (tid == 0) {
             issue_plane(tmem, kCNat, kSlotRe, smem + kReHi * kPlaneBytes, kIdescK);
@@ -295,7 +316,7 @@ __global__ void __launch_bounds__(kThreads, 1) bf16_position_kernel(Bf16Args a) 
         }
         pending |= 1u;
         wait_plane(1);
-        readout_kmajor(lane_addr + kSlotIm + 32 * g, planes, kImHi, L, 32 * g);
+        readout_kmajor(lane_addr + kSlotIm + kCols * g, planes, kImHi, L, kCols * g);
         if (!publish()) break;
         if (tid == 0) {
             issue_plane(tmem, kCNat, kSlotIm, smem + kImHi * kPlaneBytes, kIdescK);
@@ -315,7 +336,7 @@ __global__ void __launch_bounds__(kThreads, 1) bf16_position_kernel(Bf16Args a) 
         {
             double err = 0;
 #pragma unroll 1
-            for (int u = 0; u < 2; u++) {
+            for (int u = 0; u < kSub; u++) {
                 float4 am4[4];
 #pragma unroll
                 for (int e = 0; e < 4; e++) am4[e] = amp_smem[(4 * u + e) * kThreads + tid];
@@ -337,7 +358,7 @@ __global__ void __launch_bounds__(kThreads, 1) bf16_position_kernel(Bf16Args a) 
                         fr[side][e] = nonzero ? fr[side][e] * sc : am * inv_n;
                         fi[side][e] = nonzero ? fi[side][e] * sc : 0.f;
                     }
-                    const uint32_t off = mnmajor_offset(side ? mirror(j) : j, 32 * g + 16 * h + 8 * u);
+                    const uint32_t off = mnmajor_offset(side ? mirror(j) : j, kCols * g + (kCols / 2) * h + 8 * u);
                     store_split8(planes, kReHi, off, fr[side]);
                     store_split8(planes, kImHi, off, fi[side]);
                 }
@@ -360,7 +381,7 @@ __global__ void __launch_bounds__(kThreads, 1) bf16_position_kernel(Bf16Args a) 
         pending = 3u;
         // ---- stage 4: B[n = raw r][k = pos] = D3, contracted with C_sigma
         wait_plane(0);
-        readout_kmajor(lane_addr + kSlotRe + 32 * g, planes, kReHi, L, 32 * g);
+        readout_kmajor(lane_addr + kSlotRe + kCols * g, planes, kReHi, L, kCols * g);
         if (!publish()) break;
         if (tid == 0) {
             issue_plane(tmem, kCSigma, kSlotRe, smem + kReHi * kPlaneBytes, kIdescK);
@@ -368,7 +389,7 @@ __global__ void __launch_bounds__(kThreads, 1) bf16_position_kernel(Bf16Args a) 
         }
         pending |= 1u;
         wait_plane(1);
-        readout_kmajor(lane_addr + kSlotIm + 32 * g, planes, kImHi, L, 32 * g);
+        readout_kmajor(lane_addr + kSlotIm + kCols * g, planes, kImHi, L, kCols * g);
         if (!publish()) break;
         if (tid == 0) {
             issue_plane(tmem, kCSigma, kSlotIm, smem + kImHi * kPlaneBytes, kIdescK);
@@ -381,7 +402,7 @@ __global__ void __launch_bounds__(kThreads, 1) bf16_position_kernel(Bf16Args a) 
         {
             float2 *out = a.dpsi + (size_t)(p - a.dpsi_first) * (kN * kN);
 #pragma unroll 1
-            for (int u = 0; u < 2; u++) {
+            for (int u = 0; u < kSub; u++) {
                 float dr[2][8], di[2][8];
                 combined_block<true>(lane_addr, g, u, j, h, dr, di);
 #pragma unroll
@@ -389,7 +410,7 @@ __global__ void __launch_bounds__(kThreads, 1) bf16_position_kernel(Bf16Args a) 
                     const int c = side ? mirror(j) : j;
 #pragma unroll
                     for (int e = 0; e < 8; e++) {
-                        const int J = 16 * g + 8 * h + 4 * u + (e & 3);
+                        const int J = column_of(g, h, u, e & 3);
                         const int r = (e >> 2) ? mirror(J) : J;
                         out[r * kN + c] = make_float2(dr[side][e], di[side][e]);
                     }
@@ -410,18 +431,18 @@ __global__ void __launch_bounds__(kThreads, 1) bf16_position_kernel(Bf16Args a) 
 }
 
 // [position][row][column] -> [position][e4][thread][4]: thread T's float4 e4 = 4 u + 2 side + s holds the amplitudes of
-// row (side ? mirror(j) : j), columns (s ? mirror(J) : J), J = 16 g + 8 h + 4 u + i, i = 0..3, for T's lane pair j,
+// row (side ? mirror(j) : j), columns (s ? mirror(J) : J), J = column_of(g, h, u, i), i = 0..3, for T's lane pair j,
 // parity h and column group g.
 __global__ void permute_bf16_amplitudes_kernel(const float *in, float *out, long long positions) {
     const long long idx = (long long)blockIdx.x * 256 + threadIdx.x;
     if (idx >= positions * kN * kN) return;
     const long long p = idx / (kN * kN);
     const int rem = (int)(idx - p * kN * kN);
-    const int i = rem & 3, T = (rem >> 2) & (kThreads - 1), e4 = rem >> 11;
+    const int i = rem & 3, T = (rem >> 2) & (kThreads - 1), e4 = (rem >> 2) / kThreads;
     const int u = e4 >> 2, side = (e4 >> 1) & 1, s = e4 & 1;
     const int w = T >> 5, L = 32 * (w & 3) + (T & 31), g = w >> 2;
     const int jj = L >> 1, h = L & 1;
-    const int J = 16 * g + 8 * h + 4 * u + i;
+    const int J = column_of(g, h, u, i);
     const int kc = s ? mirror(J) : J, kr = side ? mirror(jj) : jj;
     out[idx] = in[p * kN * kN + kr * kN + kc];
 }
@@ -433,9 +454,12 @@ size_t bf16_smem() { return 4 * (size_t)kPlaneBytes + (size_t)kN * kN * sizeof(f
 bool bf16_applicable(int rows, int columns) { return rows == kN && columns == kN; }
 int bf16_partials_per_position() { return kThreads / 32; }
 
+// Stage 3's contraction position pos = kCols g + (kCols / 2) h + 8 u + 4 s + i holds the frequency
+// s ? mirror(J) : J, J = column_of(g, h, u, i): the order in which a thread stores its projected values.
 int bf16_sigma(int pos) {
-    const int g = pos >> 5, h = (pos >> 4) & 1, u = (pos >> 3) & 1, s = (pos >> 2) & 1, i = pos & 3;
-    const int J = 16 * g + 8 * h + 4 * u + i;
+    const int g = pos / kCols, h = (pos % kCols) / (kCols / 2), r = pos % (kCols / 2);
+    const int u = r >> 3, s = (r >> 2) & 1, i = r & 3;
+    const int J = column_of(g, h, u, i);
     return s ? mirror(J) : J;
 }
 
