@@ -72,8 +72,11 @@ __device__ __forceinline__ int wrap_once(int v, int size) { return v < 0 ? v + s
 
 // ------------------------------------------------------------------------------------------------ position pass
 
-template <typename T, int NT, int MAXN>
-__global__ void __launch_bounds__(NT, 1) position_pass_kernel(PositionPassArgs<T> a) {
+// N > 0: an N x N detector with the radix plan (R0, R1, R2) fixed at compile time (the plan factor_length gives N, so the
+// stages and their arithmetic are the run-time plan's), sized for N x N: no run-time dispatch, no stack frame, and
+// MINB CTAs of NT threads per SM.  N = 0: any size up to MAXN, the plan read at run time.
+template <typename T, int NT, int MAXN, int MINB = 1, int N = 0, int R0 = 0, int R1 = 0, int R2 = 0>
+__global__ void __launch_bounds__(NT, MINB) position_pass_kernel(PositionPassArgs<T> a) {
     extern __shared__ __align__(16) unsigned char smem_raw[];
     C2<T> *D = reinterpret_cast<C2<T> *>(smem_raw);
     C2<T> *twr = D + a.n;
@@ -93,7 +96,12 @@ __global__ void __launch_bounds__(NT, 1) position_pass_kernel(PositionPassArgs<T
         D[k] = cmul(S[k], a.object[(size_t)y * a.object_columns + x]);
     }
     __syncthreads();
-    fft2_smem<T, NT, MAXN>(D, a.rows, a.columns, a.rad_rows, a.rad_columns, twr, twc, false);
+    if constexpr (N > 0) {
+        line_fft_fixed<T, NT, MAXN, R0, R1, R2>(D, LineGeom{N, N, 1, N}, twc, false);
+        line_fft_fixed<T, NT, MAXN, R0, R1, R2>(D, LineGeom{N, N, N, 1}, twr, false);
+    } else {
+        fft2_smem<T, NT, MAXN>(D, a.rows, a.columns, a.rad_rows, a.rad_columns, twr, twc, false);
+    }
     // Fourier-modulus projection (Ptychography.swift:338-349), the inverse's 1/n folded in
     const float *A = a.amplitudes + (size_t)p * a.n;
     double err = 0;
@@ -113,7 +121,12 @@ __global__ void __launch_bounds__(NT, 1) position_pass_kernel(PositionPassArgs<T
     const double total = block_sum<NT>(err, scratch);
     if (tid == 0) a.error[p] = total;
     __syncthreads();
-    fft2_smem<T, NT, MAXN>(D, a.rows, a.columns, a.rad_rows, a.rad_columns, twr, twc, true);
+    if constexpr (N > 0) {
+        line_fft_fixed<T, NT, MAXN, R0, R1, R2>(D, LineGeom{N, N, 1, N}, twc, true);
+        line_fft_fixed<T, NT, MAXN, R0, R1, R2>(D, LineGeom{N, N, N, 1}, twr, true);
+    } else {
+        fft2_smem<T, NT, MAXN>(D, a.rows, a.columns, a.rad_rows, a.rad_columns, twr, twc, true);
+    }
     C2<T> *out = a.dpsi + (size_t)p * a.n;
     for (int k = tid; k < a.n; k += NT) out[k] = D[k];
 }
@@ -536,6 +549,19 @@ size_t pass_smem(int n, int rows, int columns) {
     return (size_t)(n + rows + columns) * sizeof(C2<T>) + 32 * sizeof(double);
 }
 
+// The fixed-plan instances of the shared-memory position pass: 64 x 64 (8 * 8) and 96 x 96 (8 * 4 * 3), the square
+// detectors below 128 x 128 that the run-time plan serves with one 512-thread CTA per SM and a local-memory stack frame
+// (its per-stage register arrays are sized for 128 x 128).  256 threads, several CTAs per SM.
+template <typename T, int N> struct FixedPass;
+template <typename T> struct FixedPass<T, 64> {
+    static constexpr int kThreads = 256;
+    static auto kernel() { return position_pass_kernel<T, 256, 64 * 64, 3, 64, 8, 8, 0>; }
+};
+template <typename T> struct FixedPass<T, 96> {  // FP64: one 147 KB plane per SM, 512 threads keep it in registers
+    static constexpr int kThreads = sizeof(T) == 8 ? 512 : 256;
+    static auto kernel() { return position_pass_kernel<T, kThreads, 96 * 96, sizeof(T) == 8 ? 1 : 2, 96, 8, 4, 3>; }
+};
+
 }  // namespace
 
 bool position_pass_supported(int n, bool fp64) {
@@ -553,8 +579,18 @@ cudaError_t configure_kernels() {
     e = cudaFuncSetAttribute(position_pass_kernel<float, kPassThreads, kMaxNFloat>,
                              cudaFuncAttributeMaxDynamicSharedMemorySize, optin);
     if (e != cudaSuccess) return e;
-    return cudaFuncSetAttribute(position_pass_kernel<double, kPassThreads, kMaxNDouble>,
-                                cudaFuncAttributeMaxDynamicSharedMemorySize, optin);
+    e = cudaFuncSetAttribute(position_pass_kernel<double, kPassThreads, kMaxNDouble>,
+                             cudaFuncAttributeMaxDynamicSharedMemorySize, optin);
+    if (e != cudaSuccess) return e;
+    for (auto f : {FixedPass<float, 64>::kernel(), FixedPass<float, 96>::kernel()}) {
+        e = cudaFuncSetAttribute(f, cudaFuncAttributeMaxDynamicSharedMemorySize, optin);
+        if (e != cudaSuccess) return e;
+    }
+    for (auto f : {FixedPass<double, 64>::kernel(), FixedPass<double, 96>::kernel()}) {
+        e = cudaFuncSetAttribute(f, cudaFuncAttributeMaxDynamicSharedMemorySize, optin);
+        if (e != cudaSuccess) return e;
+    }
+    return cudaSuccess;
 }
 
 size_t position_pass_smem(int n, int rows, int columns, bool fp64) {
@@ -595,7 +631,13 @@ template <typename T>
 cudaError_t launch_position_pass(const PositionPassArgs<T> &a, cudaStream_t s) {
     constexpr int maxn = PassConfig<T>::maxn;
     if (a.count <= 0) return cudaSuccess;
-    position_pass_kernel<T, kPassThreads, maxn><<<a.count, kPassThreads, pass_smem<T>(a.n, a.rows, a.columns), s>>>(a);
+    const size_t smem = pass_smem<T>(a.n, a.rows, a.columns);
+    if (a.rows == 64 && a.columns == 64)
+        FixedPass<T, 64>::kernel()<<<a.count, FixedPass<T, 64>::kThreads, smem, s>>>(a);
+    else if (a.rows == 96 && a.columns == 96)
+        FixedPass<T, 96>::kernel()<<<a.count, FixedPass<T, 96>::kThreads, smem, s>>>(a);
+    else
+        position_pass_kernel<T, kPassThreads, maxn><<<a.count, kPassThreads, smem, s>>>(a);
     return cudaGetLastError();
 }
 

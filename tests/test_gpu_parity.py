@@ -105,8 +105,10 @@ def test_options_in_fp32(cb):
     assert np.all(np.abs(np.abs(b.object) - 1) < 1e-5)
 
 
-def test_raster_scene_64_fp32_and_fp64(cb):
-    s = scenes.raster_scene(scan=6, det=64, step=4, seed=7)
+@pytest.mark.parametrize("det", [64, 96])
+def test_raster_scene_64_and_96_fp32_and_fp64(cb, det):
+    """64 x 64 and 96 x 96 detectors take the shared-memory pass with a compile-time radix plan (8 * 8, 8 * 4 * 3)."""
+    s = scenes.raster_scene(scan=6, det=det, step=4, seed=7)
     ref = c_oracle.reconstruct(s["amplitudes"], s["positions"], s["object"], s["probe"], iterations=4)
     for precision, obj_tol in (("fp32", 1e-4), ("fp64", 1e-10)):
         r = cb.SingleslicePtychography.reconstruct(s["amplitudes"], s["positions"], s["object"], s["probe"],
