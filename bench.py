@@ -115,7 +115,7 @@ def measured_peaks():
 # DRAM bytes (dram__bytes_read.sum + dram__bytes_write.sum) per position of one position-pass launch, from ncu on a
 # 4,096-position launch (64^2 scan, 128^2 detector) of each kernel, divided by its positions: amplitudes read (64 KB)
 # plus residuals written (128 KB) less what stays in L2.  The bench scales them to its launch by positions.
-PASS_DRAM_BYTES_PER_POSITION = {"split_bf16": 748.3e6 / 4096, "fp32": None}
+PASS_DRAM_BYTES_PER_POSITION = {"split_bf16": 748.1e6 / 4096, "fp32": None}
 
 
 def position_pass_roofline(head, stats, P, n, objects, ms_iter, peaks, fma):
