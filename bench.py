@@ -433,12 +433,15 @@ def batched_items(local):
         items.append(dict(amplitudes=ds.amplitudes, positions=ds.positions, object=ds.object_start, probe=ds.probe,
                           step_size=0.5, precision="fp32"))
         sizes.append((scan, det))
-    tiles = {}
+    tiles, shapes = {}, {}
     for it, (scan, det) in zip(items, sizes):
         if det not in tiles:
             tiles[det] = autotune.tune(it["amplitudes"], it["positions"], it["object"], it["probe"], device=local)[0]
+            shapes[det] = autotune.tune_pass(it["amplitudes"], it["positions"], it["object"], it["probe"],
+                                             device=local)[0]
         it["gather_tile"] = tiles[det]
-    return items, sizes, tiles
+        it["pass_shape"] = shapes[det]
+    return items, sizes, (tiles, shapes)
 
 
 def measure_batched(steps, warmup, world, local):
@@ -446,7 +449,7 @@ def measure_batched(steps, warmup, world, local):
     import torch
     import cubokit_b200 as cb
     from cubokit_b200 import autotune
-    items, sizes, tiles = batched_items(local)
+    items, sizes, (tiles, shapes) = batched_items(local)
     ctx = cb.context(local)
     batch = cb.Batch(items, ctx=ctx)
     stream = torch.cuda.ExternalStream(ctx.stream, device=torch.device("cuda", local))
@@ -468,7 +471,7 @@ def measure_batched(steps, warmup, world, local):
         ds = synthetic.dataset(60, det, dose=DOSE, step=STEP, seed_object=77, seed_noise=78, seed_start=79,
                                device=local)
         plan = cb.Plan(ds.amplitudes, ds.positions, ds.object_start.shape, ds.probe.shape, ctx=ctx, step_size=0.5,
-                       precision="fp32", gather_tile=tiles.get(det, 0))
+                       precision="fp32", gather_tile=tiles.get(det, 0), pass_shape=shapes.get(det, 0))
         plan.set_state(ds.object_start, ds.probe)
         plan.enqueue(warmup)
         ctx.synchronize()
@@ -490,6 +493,7 @@ def measure_batched(steps, warmup, world, local):
                                      for d in (64, 96, 128)},
            "detectors": {str(d): sum(1 for s in sizes if s[1] == d) for d in (64, 96, 128)},
            "gather_tiles": {str(d): autotune.NAMES[t] for d, t in tiles.items()},
+           "pass_shapes": {str(d): autotune.PASS_NAMES[t] for d, t in shapes.items()},
            "gpu_launches": batch.launches_per_iteration * steps, "graph_launches": steps, "clocks": clocks.summary()}
     batch.close()
     return out

@@ -45,6 +45,7 @@ class Params(C.Structure):
         ("max_position_total_distance", C.c_double), ("position_row_sampling", C.c_double),
         ("position_column_sampling", C.c_double), ("constrain_positions_center_of_mass", C.c_int),
         ("position_rows_out", C.POINTER(C.c_double)), ("position_columns_out", C.POINTER(C.c_double)),
+        ("pass_shape", C.c_int),
     ]
 
 

@@ -1,11 +1,13 @@
-"""Autotuner for the object-gather tile shape.
+"""Autotuner for the object-gather tile and the position-pass CTA shape.
 
-For a problem (detector, object and scan sizes, form) every candidate tile (32 x 8, 16 x 16, 64 x 4 pixels, along the
-residual's contiguous axis) is timed on the problem itself: one plan per candidate, a warm-up iteration, then the
-object-gather kernel's device time over a few iterations from the plan's CUDA-event kernel statistics.  The fastest
-candidate is cached in a JSON file keyed by (detector, object, positions, form, GPU name), so the timing runs once per
-shape per machine.  The tile choice never changes results: every object pixel sums the same positions in the same
-order.
+For a problem (detector, object and scan sizes, form) every candidate is timed on the problem itself: one plan per
+candidate, a warm-up iteration, then the kernel's device time over a few iterations from the plan's CUDA-event kernel
+statistics.  `tune` picks the object-gather tile (32 x 8, 16 x 16, 64 x 4 pixels, along the residual's contiguous
+axis); `tune_pass` the CTA shape of the shared-memory position pass at the detectors it runs with a compile-time radix
+plan (64 x 64: 128, 256 or 512 threads; 96 x 96: 256 or 512).  The fastest candidate is cached in a JSON file keyed by
+(what, detector, object, positions, form, GPU name), so the timing runs once per shape per machine.  Neither choice
+changes the object or the probe: every object pixel sums the same positions in the same order whatever the tile, and
+every butterfly computes the same values whatever the CTA shape.
 """
 from __future__ import annotations
 
@@ -56,28 +58,53 @@ def device_name(device=0):
         return "cuda"
 
 
-def tune(amplitudes, positions, obj, probe, precision="fp32", iterations=3, device=0, use_cache=True):
-    """The fastest gather tile for this problem (and the timings, ms per object-gather launch, by candidate)."""
-    obj = np.asarray(obj)
-    probe = np.asarray(probe)
-    k = key(probe.shape, obj.shape, len(positions), precision, device_name(device))
-    table = _load() if use_cache else {}
-    if k in table:
-        return table[k]["tile"], table[k]["ms"]
+def _time(amplitudes, positions, obj, probe, precision, iterations, device, kernel, option, candidates, names):
     ctx = context(device)
     timings = {}
-    for cand in CANDIDATES:
-        plan = Plan(amplitudes, positions, obj.shape, probe.shape, ctx=ctx, precision=precision, gather_tile=cand)
+    for cand in candidates:
+        plan = Plan(amplitudes, positions, obj.shape, probe.shape, ctx=ctx, precision=precision, **{option: cand})
         plan.set_state(obj, probe)
         plan.iterate(1)
         plan.set_timing(True)
         plan.enqueue(iterations)
-        ms, launches = plan.kernel_stats()["object_gather"]
+        ms, launches = plan.kernel_stats()[kernel]
         plan.close()
-        timings[NAMES[cand]] = ms / max(launches, 1)
-    best = min(CANDIDATES, key=lambda c: timings[NAMES[c]])
+        timings[names[cand]] = ms / max(launches, 1)
+    return min(candidates, key=lambda c: timings[names[c]]), timings
+
+
+def _tuned(what, amplitudes, positions, obj, probe, precision, iterations, device, use_cache, kernel, option,
+           candidates, names):
+    obj = np.asarray(obj)
+    probe = np.asarray(probe)
+    k = what + "|" + key(probe.shape, obj.shape, len(positions), precision, device_name(device))
+    table = _load() if use_cache else {}
+    if k in table:
+        return table[k]["choice"], table[k]["ms"]
+    best, timings = _time(amplitudes, positions, obj, probe, precision, iterations, device, kernel, option, candidates,
+                          names)
     if use_cache:
         table = _load()
-        table[k] = {"tile": best, "ms": timings}
+        table[k] = {"choice": best, "ms": timings}
         _store(table)
     return best, timings
+
+
+def tune(amplitudes, positions, obj, probe, precision="fp32", iterations=3, device=0, use_cache=True):
+    """The fastest gather tile for this problem (and the timings, ms per object-gather launch, by candidate)."""
+    return _tuned("gather", amplitudes, positions, obj, probe, precision, iterations, device, use_cache,
+                  "object_gather", "gather_tile", CANDIDATES, NAMES)
+
+
+PASS_CANDIDATES = {64: (1, 2, 3), 96: (2, 3)}
+PASS_NAMES = {0: "default", 1: "128 threads", 2: "256 threads", 3: "512 threads"}
+
+
+def tune_pass(amplitudes, positions, obj, probe, precision="fp32", iterations=3, device=0, use_cache=True):
+    """The fastest position-pass CTA shape for this problem (and the timings, ms per position-pass launch, by
+    candidate); (0, {}) for detectors without a choice (every size but 64 x 64 and 96 x 96)."""
+    rows, columns = np.asarray(probe).shape
+    if rows != columns or rows not in PASS_CANDIDATES or precision not in ("fp32", "fp64"):
+        return 0, {}
+    return _tuned("pass", amplitudes, positions, obj, probe, precision, iterations, device, use_cache,
+                  "position_pass", "pass_shape", PASS_CANDIDATES[rows], PASS_NAMES)

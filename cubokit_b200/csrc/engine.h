@@ -139,7 +139,7 @@ constexpr int kTileW = 16, kTileH = 16;  // default object-gather tile (one pixe
 constexpr int kGatherThreads = kTileW * kTileH;
 
 // engine_kernels.cu
-template <typename T> cudaError_t launch_position_pass(const PositionPassArgs<T> &a, cudaStream_t s);
+template <typename T> cudaError_t launch_position_pass(const PositionPassArgs<T> &a, int shape, cudaStream_t s);
 template <typename T> cudaError_t launch_object_gather(const ObjectGatherArgs<T> &a, int tiles, cudaStream_t s);
 template <typename T> cudaError_t launch_probe_gather(const ProbeGatherArgs<T> &a, cudaStream_t s);
 template <typename T> int probe_gather_resident_ctas();  // CTAs of the probe gather resident on one SM (at least 1)

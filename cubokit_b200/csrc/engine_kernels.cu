@@ -551,16 +551,41 @@ size_t pass_smem(int n, int rows, int columns) {
 
 // The fixed-plan instances of the shared-memory position pass: 64 x 64 (8 * 8) and 96 x 96 (8 * 4 * 3), the square
 // detectors below 128 x 128 that the run-time plan serves with one 512-thread CTA per SM and a local-memory stack frame
-// (its per-stage register arrays are sized for 128 x 128).  256 threads, several CTAs per SM.
-template <typename T, int N> struct FixedPass;
-template <typename T> struct FixedPass<T, 64> {
-    static constexpr int kThreads = 256;
+// (its per-stage register arrays are sized for 128 x 128).  Each comes in CTA shapes (cubo_ptycho_params.pass_shape:
+// 1 = 128, 2 = 256, 3 = 512 threads; 0 = the default) with as many CTAs per SM as registers and shared memory allow.
+// 96 x 96 at 128 threads would spill its stage arrays and takes 256; the FP64 96 x 96 plane (147 KB) fits one CTA per
+// SM and takes 512 threads whatever the shape.
+template <typename T, int N, int NT> struct FixedShape;
+template <typename T> struct FixedShape<T, 64, 128> {
+    static auto kernel() { return position_pass_kernel<T, 128, 64 * 64, sizeof(T) == 8 ? 3 : 6, 64, 8, 8, 0>; }
+};
+template <typename T> struct FixedShape<T, 64, 256> {
     static auto kernel() { return position_pass_kernel<T, 256, 64 * 64, 3, 64, 8, 8, 0>; }
 };
-template <typename T> struct FixedPass<T, 96> {  // FP64: one 147 KB plane per SM, 512 threads keep it in registers
-    static constexpr int kThreads = sizeof(T) == 8 ? 512 : 256;
-    static auto kernel() { return position_pass_kernel<T, kThreads, 96 * 96, sizeof(T) == 8 ? 1 : 2, 96, 8, 4, 3>; }
+template <typename T> struct FixedShape<T, 64, 512> {
+    static auto kernel() { return position_pass_kernel<T, 512, 64 * 64, 1, 64, 8, 8, 0>; }
 };
+template <typename T> struct FixedShape<T, 96, 256> {
+    static auto kernel() { return position_pass_kernel<T, 256, 96 * 96, 2, 96, 8, 4, 3>; }
+};
+template <typename T> struct FixedShape<T, 96, 512> {
+    static auto kernel() { return position_pass_kernel<T, 512, 96 * 96, 1, 96, 8, 4, 3>; }
+};
+
+// The threads per CTA of the fixed-plan pass for detector side N and shape (0: default), or 0 when N has none.
+template <typename T>
+int fixed_threads(int N, int shape) {
+    if (N == 64) return shape == 1 ? 128 : shape == 3 ? 512 : 256;
+    if (N == 96) return sizeof(T) == 8 || shape == 3 ? 512 : 256;
+    return 0;
+}
+
+template <typename T>
+void (*fixed_kernel(int N, int threads))(PositionPassArgs<T>) {
+    if (N == 64) return threads == 128 ? FixedShape<T, 64, 128>::kernel()
+                      : threads == 512 ? FixedShape<T, 64, 512>::kernel() : FixedShape<T, 64, 256>::kernel();
+    return threads == 512 ? FixedShape<T, 96, 512>::kernel() : FixedShape<T, 96, 256>::kernel();
+}
 
 }  // namespace
 
@@ -582,14 +607,14 @@ cudaError_t configure_kernels() {
     e = cudaFuncSetAttribute(position_pass_kernel<double, kPassThreads, kMaxNDouble>,
                              cudaFuncAttributeMaxDynamicSharedMemorySize, optin);
     if (e != cudaSuccess) return e;
-    for (auto f : {FixedPass<float, 64>::kernel(), FixedPass<float, 96>::kernel()}) {
-        e = cudaFuncSetAttribute(f, cudaFuncAttributeMaxDynamicSharedMemorySize, optin);
-        if (e != cudaSuccess) return e;
-    }
-    for (auto f : {FixedPass<double, 64>::kernel(), FixedPass<double, 96>::kernel()}) {
-        e = cudaFuncSetAttribute(f, cudaFuncAttributeMaxDynamicSharedMemorySize, optin);
-        if (e != cudaSuccess) return e;
-    }
+    for (int N : {64, 96})
+        for (int threads : {128, 256, 512}) {
+            e = cudaFuncSetAttribute(fixed_kernel<float>(N, threads), cudaFuncAttributeMaxDynamicSharedMemorySize, optin);
+            if (e == cudaSuccess)
+                e = cudaFuncSetAttribute(fixed_kernel<double>(N, threads), cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                         optin);
+            if (e != cudaSuccess) return e;
+        }
     return cudaSuccess;
 }
 
@@ -628,14 +653,13 @@ cudaError_t launch_position_pass_global(const PositionPassArgs<double> &a, const
 }
 
 template <typename T>
-cudaError_t launch_position_pass(const PositionPassArgs<T> &a, cudaStream_t s) {
+cudaError_t launch_position_pass(const PositionPassArgs<T> &a, int shape, cudaStream_t s) {
     constexpr int maxn = PassConfig<T>::maxn;
     if (a.count <= 0) return cudaSuccess;
     const size_t smem = pass_smem<T>(a.n, a.rows, a.columns);
-    if (a.rows == 64 && a.columns == 64)
-        FixedPass<T, 64>::kernel()<<<a.count, FixedPass<T, 64>::kThreads, smem, s>>>(a);
-    else if (a.rows == 96 && a.columns == 96)
-        FixedPass<T, 96>::kernel()<<<a.count, FixedPass<T, 96>::kThreads, smem, s>>>(a);
+    const int threads = a.rows == a.columns ? fixed_threads<T>(a.rows, shape) : 0;
+    if (threads > 0)
+        fixed_kernel<T>(a.rows, threads)<<<a.count, threads, smem, s>>>(a);
     else
         position_pass_kernel<T, kPassThreads, maxn><<<a.count, kPassThreads, smem, s>>>(a);
     return cudaGetLastError();
@@ -734,7 +758,7 @@ cudaError_t launch_error_reduce(const double *error, long long count, double div
 }
 
 #define INSTANTIATE(T)                                                                                                 \
-    template cudaError_t launch_position_pass<T>(const PositionPassArgs<T> &, cudaStream_t);                           \
+    template cudaError_t launch_position_pass<T>(const PositionPassArgs<T> &, int, cudaStream_t);                      \
     template cudaError_t launch_object_gather<T>(const ObjectGatherArgs<T> &, int, cudaStream_t);                      \
     template cudaError_t launch_probe_gather<T>(const ProbeGatherArgs<T> &, cudaStream_t);                             \
     template int probe_gather_resident_ctas<T>();                                                                      \

@@ -380,6 +380,7 @@ void validate(const cubo_ptycho_problem *pr, const cubo_ptycho_params *pp, doubl
     }
     if (pp->form < CUBO_PTYCHO_FORM_FP32 || pp->form > CUBO_PTYCHO_FORM_FP64) fail(CUBO_PTYCHO_INVALID_INPUT, "form");
     if (pp->gather_tile < 0 || pp->gather_tile > 3) fail(CUBO_PTYCHO_INVALID_INPUT, "gather tile");
+    if (pp->pass_shape < 0 || pp->pass_shape > 3) fail(CUBO_PTYCHO_INVALID_INPUT, "position-pass shape");
     if (pp->variant < CUBO_PTYCHO_VARIANT_AUTO || pp->variant > CUBO_PTYCHO_VARIANT_GLOBAL)
         fail(CUBO_PTYCHO_INVALID_INPUT, "variant");
     *divisor_out = d;
@@ -923,7 +924,7 @@ void enqueue_position_pass(cubo_ptycho_plan *p) {
             if (p->timing) p->kind_launches[kPositionPass] += count;
         }
     } else {
-        timed(p, kPositionPass, 1, [&] { return launch_position_pass<T>(pa, s); });
+        timed(p, kPositionPass, 1, [&] { return launch_position_pass<T>(pa, p->params.pass_shape, s); });
     }
 }
 

@@ -164,6 +164,7 @@ struct SingleslicePtychographyOptions {
     bool positionCorrection = false;  // refused on the GPU path, as .single refuses it (Ptychography.swift:236)
     PtychographyPrecision precision = PtychographyPrecision::fp32;
     int gatherTile = 0;  // object-gather tile choice (performance only), see cubo_ptycho_params.gather_tile
+    int passShape = 0;   // position-pass CTA shape (performance only), see cubo_ptycho_params.pass_shape
     std::function<bool()> isCancelled;
     std::function<void(int, int)> progress;
 };
@@ -214,6 +215,7 @@ struct SingleslicePtychography {
         p.mean_intensity = o.errorNormalization.meanIntensityValue;
         p.has_position_correction = o.positionCorrection;
         p.gather_tile = o.gatherTile;
+        p.pass_shape = o.passShape;
         p.form = o.precision == PtychographyPrecision::fp64        ? CUBO_PTYCHO_FORM_FP64
                  : o.precision == PtychographyPrecision::splitBF16 ? CUBO_PTYCHO_FORM_SPLIT_BF16
                                                                    : CUBO_PTYCHO_FORM_FP32;

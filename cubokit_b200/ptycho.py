@@ -161,7 +161,7 @@ class _Inputs:
                  fix_probe, pure_phase_object, constrain_object_amplitude, fix_probe_center_of_mass,
                  constrain_probe_amplitude, probe_amplitude_relative_radius, probe_amplitude_relative_width,
                  fix_probe_aperture, probe_support_mask, error_normalization, position_correction, precision,
-                 variant="auto", gather_tile=0):
+                 variant="auto", gather_tile=0, pass_shape=0):
         rows, columns = probe_shape
         positions = np.asarray(positions, np.float64).reshape(-1, 2) if np.size(positions) else np.zeros((0, 2))
         count = len(positions)
@@ -239,6 +239,9 @@ class _Inputs:
         if gather_tile not in (0, 1, 2, 3):
             raise PtychographyError(f"gather_tile {gather_tile!r}")
         p.gather_tile = int(gather_tile)
+        if pass_shape not in (0, 1, 2, 3):
+            raise PtychographyError(f"pass_shape {pass_shape!r}")
+        p.pass_shape = int(pass_shape)
         self.cancel_flag = C.c_int(0)
         self.count = count
 
@@ -485,7 +488,7 @@ class Plan:
                         constrain_probe_amplitude=False, probe_amplitude_relative_radius=0.5,
                         probe_amplitude_relative_width=0.05, fix_probe_aperture=False, probe_support_mask=None,
                         error_normalization="suppliedAmplitudeEnergy", position_correction=None, precision="fp32",
-                        variant="auto", gather_tile=0)
+                        variant="auto", gather_tile=0, pass_shape=0)
         defaults.update(kwargs)
         self.inputs = _Inputs(amplitudes, positions, tuple(object_shape), tuple(probe_shape), **defaults)
         self.object_shape = tuple(object_shape)
@@ -641,13 +644,13 @@ class Batch:
                 "constrain_object_amplitude", "fix_probe_center_of_mass", "constrain_probe_amplitude",
                 "probe_amplitude_relative_radius", "probe_amplitude_relative_width", "fix_probe_aperture",
                 "probe_support_mask", "error_normalization", "position_correction", "precision", "variant",
-                "gather_tile")
+                "gather_tile", "pass_shape")
         defaults = dict(iterations=0, step_size=0.5, normalization_minimum=1.0, fix_probe=False,
                         pure_phase_object=False, constrain_object_amplitude=True, fix_probe_center_of_mass=False,
                         constrain_probe_amplitude=False, probe_amplitude_relative_radius=0.5,
                         probe_amplitude_relative_width=0.05, fix_probe_aperture=False, probe_support_mask=None,
                         error_normalization="suppliedAmplitudeEnergy", position_correction=None, precision="fp32",
-                        variant="auto", gather_tile=0)
+                        variant="auto", gather_tile=0, pass_shape=0)
         self.inputs, self.shapes = [], []
         for it in items:
             kw = dict(defaults)

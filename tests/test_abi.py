@@ -44,11 +44,12 @@ def test_struct_layouts_match_the_header():
 #include <stddef.h>
 #include "cubo_ptycho.h"
 int main(void) {
-  printf("%zu %zu %zu %zu %zu %zu %zu %zu %zu\n", sizeof(cubo_ptycho_problem), sizeof(cubo_ptycho_params),
+  printf("%zu %zu %zu %zu %zu %zu %zu %zu %zu %zu\n", sizeof(cubo_ptycho_problem), sizeof(cubo_ptycho_params),
          offsetof(cubo_ptycho_params, form), offsetof(cubo_ptycho_params, progress_user),
          offsetof(cubo_ptycho_params, max_position_total_distance),
          offsetof(cubo_ptycho_params, position_columns_out), sizeof(cubo_ptycho_mixed_params),
-         sizeof(cubo_ptycho_multislice_params), offsetof(cubo_ptycho_multislice_params, identical_slices));
+         sizeof(cubo_ptycho_multislice_params), offsetof(cubo_ptycho_multislice_params, identical_slices),
+         offsetof(cubo_ptycho_params, pass_shape));
   return 0;
 }
 '''
@@ -63,6 +64,7 @@ int main(void) {
     assert int(out[3]) == _lib.Params.progress_user.offset
     assert int(out[4]) == _lib.Params.max_position_total_distance.offset
     assert int(out[5]) == _lib.Params.position_columns_out.offset
+    assert int(out[9]) == _lib.Params.pass_shape.offset
     assert int(out[6]) == C.sizeof(_lib.MixedParams)
     assert int(out[7]) == C.sizeof(_lib.MultisliceParams)
     assert int(out[8]) == _lib.MultisliceParams.identical_slices.offset

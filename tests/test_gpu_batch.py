@@ -54,3 +54,31 @@ def test_gather_tiles_agree_bitwise_and_autotune_picks_one(tmp_path, monkeypatch
         best, ms = autotune.tune(s["amplitudes"], s["positions"], s["object"], s["probe"], precision=precision)
         assert best in autotune.CANDIDATES and set(ms) == {"32x8", "16x16", "64x4"}
         assert autotune.tune(s["amplitudes"], s["positions"], s["object"], s["probe"], precision=precision)[0] == best
+
+
+def test_pass_shapes_agree_bitwise_and_autotune_picks_one(tmp_path, monkeypatch):
+    """The shared-memory position pass at 64 x 64 and 96 x 96 runs in several CTA shapes (128, 256, 512 threads): every
+    shape gives the same object and probe bit for bit (the reported error is summed over the CTA's threads, so it
+    agrees to round-off), and the autotuner times the shapes and caches its choice."""
+    import cubokit_b200 as cb
+    from cubokit_b200 import autotune
+    monkeypatch.setenv("CUBOKIT_B200_CACHE", str(tmp_path))
+    for precision in ("fp32", "fp64"):
+        for det in (64, 96):
+            s = scenes.raster_scene(scan=4, det=det, step=4, seed=9)
+            ref = None
+            for shape in (0, 1, 2, 3):
+                plan = cb.Plan(s["amplitudes"], s["positions"], s["object"].shape, s["probe"].shape, step_size=0.5,
+                               precision=precision, pass_shape=shape)
+                plan.set_state(s["object"], s["probe"])
+                errors = plan.iterate(2)
+                o, p = plan.get_state()
+                plan.close()
+                if ref is None:
+                    ref = (o, p, errors)
+                assert np.array_equal(o, ref[0]) and np.array_equal(p, ref[1]), (precision, det, shape)
+                assert np.allclose(errors, ref[2], rtol=1e-12 if precision == "fp64" else 1e-6, atol=0), (precision, det)
+            best, ms = autotune.tune_pass(s["amplitudes"], s["positions"], s["object"], s["probe"], precision=precision)
+            assert best in autotune.PASS_CANDIDATES[det] and len(ms) == len(autotune.PASS_CANDIDATES[det])
+            assert autotune.tune_pass(s["amplitudes"], s["positions"], s["object"], s["probe"],
+                                      precision=precision)[0] == best
