@@ -140,6 +140,17 @@ constexpr int kGatherThreads = kTileW * kTileH;
 
 // engine_kernels.cu
 template <typename T> cudaError_t launch_position_pass(const PositionPassArgs<T> &a, int shape, cudaStream_t s);
+// Grouped launches (batches of independent reconstructions): every item's units in one persistent launch.  prefix holds
+// items + 1 offsets (item i owns units prefix[i] .. prefix[i + 1] - 1); args one structure per item, in device memory.
+// The position pass groups items of one square detector with a compile-time plan (position_pass_groupable), units =
+// positions; the object gather's units are tiles; the probe gather's are (pixel block, position group) pairs.
+bool position_pass_groupable(int rows, int columns, bool fp64);
+template <typename T> cudaError_t launch_position_pass_grouped(const PositionPassArgs<T> *args, const int *prefix,
+                                                               int items, int total, int N, int shape, cudaStream_t s);
+template <typename T> cudaError_t launch_object_gather_grouped(const ObjectGatherArgs<T> *args, const int *prefix,
+                                                               int items, int total, cudaStream_t s);
+template <typename T> cudaError_t launch_probe_gather_grouped(const ProbeGatherArgs<T> *args, const int *prefix,
+                                                              int items, int total, cudaStream_t s);
 template <typename T> cudaError_t launch_object_gather(const ObjectGatherArgs<T> &a, int tiles, cudaStream_t s);
 template <typename T> cudaError_t launch_probe_gather(const ProbeGatherArgs<T> &a, cudaStream_t s);
 template <typename T> int probe_gather_resident_ctas();  // CTAs of the probe gather resident on one SM (at least 1)

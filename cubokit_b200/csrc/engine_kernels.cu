@@ -75,15 +75,14 @@ __device__ __forceinline__ int wrap_once(int v, int size) { return v < 0 ? v + s
 // N > 0: an N x N detector with the radix plan (R0, R1, R2) fixed at compile time (the plan factor_length gives N, so the
 // stages and their arithmetic are the run-time plan's), sized for N x N: no run-time dispatch, no stack frame, and
 // MINB CTAs of NT threads per SM.  N = 0: any size up to MAXN, the plan read at run time.
-template <typename T, int NT, int MAXN, int MINB = 1, int N = 0, int R0 = 0, int R1 = 0, int R2 = 0>
-__global__ void __launch_bounds__(NT, MINB) position_pass_kernel(PositionPassArgs<T> a) {
+template <typename T, int NT, int MAXN, int N, int R0, int R1, int R2>
+__device__ __forceinline__ void position_pass_body(const PositionPassArgs<T> &a, int p) {
     extern __shared__ __align__(16) unsigned char smem_raw[];
     C2<T> *D = reinterpret_cast<C2<T> *>(smem_raw);
     C2<T> *twr = D + a.n;
     C2<T> *twc = twr + a.rows;
     double *scratch = reinterpret_cast<double *>(twc + a.columns);
     const int tid = threadIdx.x;
-    const int p = a.first + blockIdx.x;
     for (int i = tid; i < a.rows; i += NT) twr[i] = a.tw_rows[i];
     for (int i = tid; i < a.columns; i += NT) twc[i] = a.tw_columns[i];
     const int rr = a.scan.rr[p], cc = a.scan.cc[p], cls = a.scan.cls[p];
@@ -129,6 +128,35 @@ __global__ void __launch_bounds__(NT, MINB) position_pass_kernel(PositionPassArg
     }
     C2<T> *out = a.dpsi + (size_t)p * a.n;
     for (int k = tid; k < a.n; k += NT) out[k] = D[k];
+}
+
+template <typename T, int NT, int MAXN, int MINB = 1, int N = 0, int R0 = 0, int R1 = 0, int R2 = 0>
+__global__ void __launch_bounds__(NT, MINB) position_pass_kernel(PositionPassArgs<T> a) {
+    position_pass_body<T, NT, MAXN, N, R0, R1, R2>(a, a.first + blockIdx.x);
+}
+
+// The item of a grouped launch that work unit u belongs to: prefix[i] .. prefix[i + 1] - 1 are item i's units.
+__device__ __forceinline__ int group_item(const int *prefix, int items, int u) {
+    int lo = 0, hi = items - 1;
+    while (lo < hi) {
+        const int mid = (lo + hi + 1) >> 1;
+        if (prefix[mid] <= u) lo = mid; else hi = mid - 1;
+    }
+    return lo;
+}
+
+// Grouped position pass: the positions of every item (independent reconstructions with the same detector) in one
+// persistent launch; each CTA walks the work list (item, position) in a fixed stride.  Every position's arithmetic is
+// the one-launch kernel's.
+template <typename T, int NT, int MAXN, int MINB, int N, int R0, int R1, int R2>
+__global__ void __launch_bounds__(NT, MINB) position_pass_grouped_kernel(const PositionPassArgs<T> *args,
+                                                                         const int *prefix, int items, int total) {
+    for (int u = blockIdx.x; u < total; u += gridDim.x) {
+        const int it = group_item(prefix, items, u);
+        const PositionPassArgs<T> &a = args[it];
+        position_pass_body<T, NT, MAXN, N, R0, R1, R2>(a, a.first + (u - prefix[it]));
+        __syncthreads();  // the next unit overwrites the plane and twiddles in shared memory
+    }
 }
 
 // FP64 position pass through global memory, for detectors whose FP64 plane does not fit one CTA's shared memory (above
@@ -193,11 +221,11 @@ __device__ __forceinline__ int lower_bound_index(const int *list, int lo, int hi
 }
 
 template <typename T, bool MIXED>
-__global__ void __launch_bounds__(kGatherThreads) object_gather_kernel(ObjectGatherArgs<T> a) {
+__device__ __forceinline__ void object_gather_body(const ObjectGatherArgs<T> &a, int unit) {
     __shared__ int s_p[kGatherChunk], s_cls[kGatherChunk];
     __shared__ int s_off[kGatherChunk][kMaxTileSide + kGatherThreads / kMaxTileSide + 4];  // rows, then columns
     __shared__ double scratch[32];
-    const int tile = a.band_tiles ? a.band_tiles[blockIdx.x] : (int)blockIdx.x;
+    const int tile = a.band_tiles ? a.band_tiles[unit] : unit;
     const int tx = tile % a.tiles_x, ty = tile / a.tiles_x;
     const int x0 = tx * a.tile_w, y0 = ty * a.tile_h;
     // consecutive threads take consecutive object columns, hence consecutive addresses of each [row][column] residual
@@ -309,6 +337,22 @@ __global__ void __launch_bounds__(kGatherThreads) object_gather_kernel(ObjectGat
     if (threadIdx.x == 0) a.tile_max[tile] = m;
 }
 
+template <typename T, bool MIXED>
+__global__ void __launch_bounds__(kGatherThreads) object_gather_kernel(ObjectGatherArgs<T> a) {
+    object_gather_body<T, MIXED>(a, blockIdx.x);
+}
+
+// Grouped object gather: the tiles of every item in one persistent launch (work list (item, tile), fixed stride).
+template <typename T>
+__global__ void __launch_bounds__(kGatherThreads) object_gather_grouped_kernel(const ObjectGatherArgs<T> *args,
+                                                                               const int *prefix, int items, int total) {
+    for (int u = blockIdx.x; u < total; u += gridDim.x) {
+        const int it = group_item(prefix, items, u);
+        object_gather_body<T, false>(args[it], u - prefix[it]);
+        __syncthreads();  // the next unit restages the candidate offsets
+    }
+}
+
 // ------------------------------------------------------------------------------------------------ candidate lists
 
 // Whether the cyclic window [start, start + length) of a periodic axis of `size` meets [t0, t0 + len).
@@ -354,11 +398,10 @@ constexpr int kProbeThreads = 256;
 // |O|^2.  Per chunk of positions the window's object base rr * OC + cc is staged, or -1 where the window wraps around
 // the object's edge; an interior window's pixel is then base + (offr * OC + offc), the wrapped ones are computed in full.
 template <typename T>
-__global__ void __launch_bounds__(kProbeThreads) probe_gather_kernel(ProbeGatherArgs<T> a) {
+__device__ __forceinline__ void probe_gather_body(const ProbeGatherArgs<T> &a, int block, int group) {
     __shared__ int s_rr[kChunk], s_cc[kChunk];
     __shared__ long long s_base[kChunk];
-    const int k = blockIdx.x * kProbeThreads + threadIdx.x;  // pixel index, [row][column]
-    const int group = blockIdx.y;
+    const int k = block * kProbeThreads + threadIdx.x;  // pixel index, [row][column]
     const int p0 = a.first + (int)((long long)a.count * group / a.groups);
     const int p1 = a.first + (int)((long long)a.count * (group + 1) / a.groups);
     const bool valid = k < a.n;
@@ -418,6 +461,24 @@ __global__ void __launch_bounds__(kProbeThreads) probe_gather_kernel(ProbeGather
     if (valid) {
         a.partial_grad[(size_t)group * a.n + k] = g;
         a.partial_weight[(size_t)group * a.n + k] = w;
+    }
+}
+
+template <typename T>
+__global__ void __launch_bounds__(kProbeThreads) probe_gather_kernel(ProbeGatherArgs<T> a) {
+    probe_gather_body<T>(a, blockIdx.x, blockIdx.y);
+}
+
+// Grouped probe gather: every item's (pixel block, position group) units in one persistent launch.
+template <typename T>
+__global__ void __launch_bounds__(kProbeThreads) probe_gather_grouped_kernel(const ProbeGatherArgs<T> *args,
+                                                                             const int *prefix, int items, int total) {
+    for (int u = blockIdx.x; u < total; u += gridDim.x) {
+        const int it = group_item(prefix, items, u);
+        const ProbeGatherArgs<T> &a = args[it];
+        const int blocks = (a.n + kProbeThreads - 1) / kProbeThreads, v = u - prefix[it];
+        probe_gather_body<T>(a, v % blocks, v / blocks);
+        __syncthreads();  // the next unit restages the window bases
     }
 }
 
@@ -558,18 +619,23 @@ size_t pass_smem(int n, int rows, int columns) {
 template <typename T, int N, int NT> struct FixedShape;
 template <typename T> struct FixedShape<T, 64, 128> {
     static auto kernel() { return position_pass_kernel<T, 128, 64 * 64, sizeof(T) == 8 ? 3 : 6, 64, 8, 8, 0>; }
+    static auto grouped() { return position_pass_grouped_kernel<T, 128, 64 * 64, sizeof(T) == 8 ? 3 : 6, 64, 8, 8, 0>; }
 };
 template <typename T> struct FixedShape<T, 64, 256> {
     static auto kernel() { return position_pass_kernel<T, 256, 64 * 64, 3, 64, 8, 8, 0>; }
+    static auto grouped() { return position_pass_grouped_kernel<T, 256, 64 * 64, 3, 64, 8, 8, 0>; }
 };
 template <typename T> struct FixedShape<T, 64, 512> {
     static auto kernel() { return position_pass_kernel<T, 512, 64 * 64, 1, 64, 8, 8, 0>; }
+    static auto grouped() { return position_pass_grouped_kernel<T, 512, 64 * 64, 1, 64, 8, 8, 0>; }
 };
 template <typename T> struct FixedShape<T, 96, 256> {
     static auto kernel() { return position_pass_kernel<T, 256, 96 * 96, 2, 96, 8, 4, 3>; }
+    static auto grouped() { return position_pass_grouped_kernel<T, 256, 96 * 96, 2, 96, 8, 4, 3>; }
 };
 template <typename T> struct FixedShape<T, 96, 512> {
     static auto kernel() { return position_pass_kernel<T, 512, 96 * 96, 1, 96, 8, 4, 3>; }
+    static auto grouped() { return position_pass_grouped_kernel<T, 512, 96 * 96, 1, 96, 8, 4, 3>; }
 };
 
 // The threads per CTA of the fixed-plan pass for detector side N and shape (0: default), or 0 when N has none.
@@ -585,6 +651,24 @@ void (*fixed_kernel(int N, int threads))(PositionPassArgs<T>) {
     if (N == 64) return threads == 128 ? FixedShape<T, 64, 128>::kernel()
                       : threads == 512 ? FixedShape<T, 64, 512>::kernel() : FixedShape<T, 64, 256>::kernel();
     return threads == 512 ? FixedShape<T, 96, 512>::kernel() : FixedShape<T, 96, 256>::kernel();
+}
+
+template <typename T>
+void (*fixed_grouped_kernel(int N, int threads))(const PositionPassArgs<T> *, const int *, int, int) {
+    if (N == 64) return threads == 128 ? FixedShape<T, 64, 128>::grouped()
+                      : threads == 512 ? FixedShape<T, 64, 512>::grouped() : FixedShape<T, 64, 256>::grouped();
+    return threads == 512 ? FixedShape<T, 96, 512>::grouped() : FixedShape<T, 96, 256>::grouped();
+}
+
+// Persistent grid of a grouped launch: the kernel's resident CTAs on every SM, at most one per unit.
+template <typename K>
+int persistent_grid(K kernel, int threads, size_t smem, int total) {
+    int device = 0, sms = 148, per_sm = 1;
+    if (cudaGetDevice(&device) == cudaSuccess) cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, device);
+    if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kernel, threads, smem) != cudaSuccess || per_sm < 1)
+        per_sm = 1;
+    cudaGetLastError();
+    return (int)std::max<long long>(1, std::min<long long>(total, (long long)per_sm * sms));
 }
 
 }  // namespace
@@ -613,6 +697,12 @@ cudaError_t configure_kernels() {
             if (e == cudaSuccess)
                 e = cudaFuncSetAttribute(fixed_kernel<double>(N, threads), cudaFuncAttributeMaxDynamicSharedMemorySize,
                                          optin);
+            if (e == cudaSuccess)
+                e = cudaFuncSetAttribute(fixed_grouped_kernel<float>(N, threads),
+                                         cudaFuncAttributeMaxDynamicSharedMemorySize, optin);
+            if (e == cudaSuccess)
+                e = cudaFuncSetAttribute(fixed_grouped_kernel<double>(N, threads),
+                                         cudaFuncAttributeMaxDynamicSharedMemorySize, optin);
             if (e != cudaSuccess) return e;
         }
     return cudaSuccess;
@@ -662,6 +752,40 @@ cudaError_t launch_position_pass(const PositionPassArgs<T> &a, int shape, cudaSt
         fixed_kernel<T>(a.rows, threads)<<<a.count, threads, smem, s>>>(a);
     else
         position_pass_kernel<T, kPassThreads, maxn><<<a.count, kPassThreads, smem, s>>>(a);
+    return cudaGetLastError();
+}
+
+bool position_pass_groupable(int rows, int columns, bool fp64) {
+    return rows == columns && (fp64 ? fixed_threads<double>(rows, 0) : fixed_threads<float>(rows, 0)) > 0;
+}
+
+template <typename T>
+cudaError_t launch_position_pass_grouped(const PositionPassArgs<T> *args, const int *prefix, int items, int total,
+                                         int N, int shape, cudaStream_t s) {
+    const int threads = fixed_threads<T>(N, shape);
+    if (threads == 0) return cudaErrorInvalidValue;
+    if (total <= 0) return cudaSuccess;
+    const size_t smem = pass_smem<T>(N * N, N, N);
+    auto kernel = fixed_grouped_kernel<T>(N, threads);
+    kernel<<<persistent_grid(kernel, threads, smem, total), threads, smem, s>>>(args, prefix, items, total);
+    return cudaGetLastError();
+}
+
+template <typename T>
+cudaError_t launch_object_gather_grouped(const ObjectGatherArgs<T> *args, const int *prefix, int items, int total,
+                                         cudaStream_t s) {
+    if (total <= 0) return cudaSuccess;
+    auto kernel = object_gather_grouped_kernel<T>;
+    kernel<<<persistent_grid(kernel, kGatherThreads, 0, total), kGatherThreads, 0, s>>>(args, prefix, items, total);
+    return cudaGetLastError();
+}
+
+template <typename T>
+cudaError_t launch_probe_gather_grouped(const ProbeGatherArgs<T> *args, const int *prefix, int items, int total,
+                                        cudaStream_t s) {
+    if (total <= 0) return cudaSuccess;
+    auto kernel = probe_gather_grouped_kernel<T>;
+    kernel<<<persistent_grid(kernel, kProbeThreads, 0, total), kProbeThreads, 0, s>>>(args, prefix, items, total);
     return cudaGetLastError();
 }
 
@@ -759,6 +883,12 @@ cudaError_t launch_error_reduce(const double *error, long long count, double div
 
 #define INSTANTIATE(T)                                                                                                 \
     template cudaError_t launch_position_pass<T>(const PositionPassArgs<T> &, int, cudaStream_t);                      \
+    template cudaError_t launch_position_pass_grouped<T>(const PositionPassArgs<T> *, const int *, int, int, int, int,   \
+                                                         cudaStream_t);                                              \
+    template cudaError_t launch_object_gather_grouped<T>(const ObjectGatherArgs<T> *, const int *, int, int,          \
+                                                         cudaStream_t);                                              \
+    template cudaError_t launch_probe_gather_grouped<T>(const ProbeGatherArgs<T> *, const int *, int, int,            \
+                                                        cudaStream_t);                                               \
     template cudaError_t launch_object_gather<T>(const ObjectGatherArgs<T> &, int, cudaStream_t);                      \
     template cudaError_t launch_probe_gather<T>(const ProbeGatherArgs<T> &, cudaStream_t);                             \
     template int probe_gather_resident_ctas<T>();                                                                      \

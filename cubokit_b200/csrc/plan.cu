@@ -11,6 +11,7 @@
 #include <cstdlib>
 #include <cstring>
 #include <map>
+#include <tuple>
 #include <memory>
 #include <mutex>
 #include <new>
@@ -214,6 +215,9 @@ struct cubo_ptycho_plan {
     // band_size positions at a time) so that a band's residuals stay in L2 between the pass and the gathers
     bool banded = false;
     int band_size = 0, bands = 0;
+    // in a batch: this plan's generic position pass / its object and probe gathers run in the batch's grouped
+    // (persistent, every item at once) launches instead of its own
+    bool grouped_pass = false, grouped_gathers = false;
     std::vector<int> band_tile_offsets;  // [bands + 1]: band b's object-gather tiles are band_tiles[offsets[b] ..]
     bool plane128 = false;  // FP64 128 x 128 planes: FFT, pointwise step and inverse FFT in one clustered launch
     int plane_cluster = 2;  // CTAs per plane of that launch
@@ -847,6 +851,20 @@ void enqueue_probe_side(cubo_ptycho_plan *p) {
 }
 
 // Shifted probes, then the position pass over every position: residuals (dpsi) and per-position squared errors.
+// The generic position pass's arguments over every position of the plan.
+template <typename T>
+PositionPassArgs<T> position_pass_args(cubo_ptycho_plan *p) {
+    const int n = p->n;
+    PositionPassArgs<T> pa{};
+    pa.rows = p->R; pa.columns = p->C; pa.object_rows = p->OR; pa.object_columns = p->OC; pa.n = n;
+    pa.first = 0; pa.count = p->P; pa.scan = ScanTables{p->rr.as<int>(), p->cc.as<int>(), p->cls.as<int>()};
+    pa.shifted = p->shifted.as<C2<T>>(); pa.object = p->object.as<C2<T>>();
+    pa.amplitudes = p->amplitudes.as<float>(); pa.dpsi = p->dpsi.as<C2<T>>(); pa.error = p->error.as<double>();
+    pa.tw_rows = p->tw_r.as<C2<T>>(); pa.tw_columns = p->tw_c.as<C2<T>>();
+    pa.rad_rows = p->rad_rows; pa.rad_columns = p->rad_columns; pa.inv_n = (T)(1.0 / n);
+    return pa;
+}
+
 template <typename T>
 void enqueue_position_pass(cubo_ptycho_plan *p) {
     cudaStream_t s = p->ctx->stream;
@@ -854,13 +872,7 @@ void enqueue_position_pass(cubo_ptycho_plan *p) {
     const int n = p->n;
     const ScanTables scan{p->rr.as<int>(), p->cc.as<int>(), p->cls.as<int>()};
     enqueue_shift_table<T>(p);
-    PositionPassArgs<T> pa{};
-    pa.rows = p->R; pa.columns = p->C; pa.object_rows = p->OR; pa.object_columns = p->OC; pa.n = n;
-    pa.first = 0; pa.count = p->P; pa.scan = scan;
-    pa.shifted = p->shifted.as<C2<T>>(); pa.object = p->object.as<C2<T>>();
-    pa.amplitudes = p->amplitudes.as<float>(); pa.dpsi = p->dpsi.as<C2<T>>(); pa.error = p->error.as<double>();
-    pa.tw_rows = p->tw_r.as<C2<T>>(); pa.tw_columns = p->tw_c.as<C2<T>>();
-    pa.rad_rows = p->rad_rows; pa.rad_columns = p->rad_columns; pa.inv_n = (T)(1.0 / n);
+    const PositionPassArgs<T> pa = position_pass_args<T>(p);
     if (p->bf16) {
         Bf16Args ba{};
         ba.object_rows = p->OR; ba.object_columns = p->OC; ba.first = 0; ba.count = p->P; ba.scan = scan;
@@ -923,35 +935,51 @@ void enqueue_position_pass(cubo_ptycho_plan *p) {
             p->launches += count;
             if (p->timing) p->kind_launches[kPositionPass] += count;
         }
-    } else {
+    } else if (!p->grouped_pass) {
         timed(p, kPositionPass, 1, [&] { return launch_position_pass<T>(pa, p->params.pass_shape, s); });
     }
 }
 
 // Object and probe gradient sums from dpsi: grad_o / weight_o (object), grad_p64 / weight_p64 (probe), maxima.
+// The object gather's arguments over every tile and candidate of the plan.
+template <typename T>
+ObjectGatherArgs<T> object_gather_args(cubo_ptycho_plan *p) {
+    const int n = p->n;
+    ObjectGatherArgs<T> ga{};
+    ga.rows = p->R; ga.columns = p->C; ga.object_rows = p->OR; ga.object_columns = p->OC; ga.n = n;
+    ga.tiles_x = p->tiles_x; ga.tile_w = p->tile_w; ga.tile_h = p->tile_h; ga.tile_start = p->tile_start.as<int>(); ga.tile_list = p->tile_list.as<int>();
+    ga.scan = ScanTables{p->rr.as<int>(), p->cc.as<int>(), p->cls.as<int>()};
+    ga.shifted = p->shifted.as<C2<T>>(); ga.dpsi = p->dpsi.as<C2<T>>();
+    ga.grad = p->grad_o.as<C2<T>>(); ga.weight = p->weight_o.as<T>(); ga.tile_max = p->tile_max.as<double>();
+    ga.states = p->states;
+    ga.dpsi_state_stride = (long long)p->P * n;
+    ga.shifted_state_stride = (long long)p->classes * n;
+    return ga;
+}
+
+// The probe gather's arguments over every position of the plan (probe state 0).
+template <typename T>
+ProbeGatherArgs<T> probe_gather_args(cubo_ptycho_plan *p) {
+    ProbeGatherArgs<T> pg{};
+    pg.rows = p->R; pg.columns = p->C; pg.object_rows = p->OR; pg.object_columns = p->OC; pg.n = p->n;
+    pg.count = p->P; pg.groups = p->groups; pg.scan = ScanTables{p->rr.as<int>(), p->cc.as<int>(), p->cls.as<int>()};
+    pg.object = p->object.as<C2<T>>(); pg.dpsi = p->dpsi.as<C2<T>>();
+    pg.partial_grad = p->partial_grad.as<C2<T>>(); pg.partial_weight = p->partial_weight.as<T>();
+    return pg;
+}
+
 template <typename T>
 void enqueue_gathers(cubo_ptycho_plan *p) {
     cudaStream_t s = p->ctx->stream;
     ensure_dpsi<T>(p);
     const int n = p->n;
-    const ScanTables scan{p->rr.as<int>(), p->cc.as<int>(), p->cls.as<int>()};
-    ObjectGatherArgs<T> ga{};
-    ga.rows = p->R; ga.columns = p->C; ga.object_rows = p->OR; ga.object_columns = p->OC; ga.n = n;
-    ga.tiles_x = p->tiles_x; ga.tile_w = p->tile_w; ga.tile_h = p->tile_h; ga.tile_start = p->tile_start.as<int>(); ga.tile_list = p->tile_list.as<int>();
-    ga.scan = scan; ga.shifted = p->shifted.as<C2<T>>(); ga.dpsi = p->dpsi.as<C2<T>>();
-    ga.grad = p->grad_o.as<C2<T>>(); ga.weight = p->weight_o.as<T>(); ga.tile_max = p->tile_max.as<double>();
-    ga.states = p->states;
-    ga.dpsi_state_stride = (long long)p->P * n;
-    ga.shifted_state_stride = (long long)p->classes * n;
-    timed(p, kObjectGather, 1, [&] { return launch_object_gather<T>(ga, p->tiles, s); });
+    const ObjectGatherArgs<T> ga = object_gather_args<T>(p);
+    if (!p->grouped_gathers) timed(p, kObjectGather, 1, [&] { return launch_object_gather<T>(ga, p->tiles, s); });
 
-    ProbeGatherArgs<T> pg{};
-    pg.rows = p->R; pg.columns = p->C; pg.object_rows = p->OR; pg.object_columns = p->OC; pg.n = n;
-    pg.count = p->P; pg.groups = p->groups; pg.scan = scan; pg.object = p->object.as<C2<T>>();
-    pg.dpsi = p->dpsi.as<C2<T>>(); pg.partial_grad = p->partial_grad.as<C2<T>>(); pg.partial_weight = p->partial_weight.as<T>();
+    ProbeGatherArgs<T> pg = probe_gather_args<T>(p);
     for (int st = 0; st < p->states; st++) {  // each probe state's gradient from its own residuals
         pg.dpsi = p->dpsi.as<C2<T>>() + (size_t)st * p->P * n;
-        if (!p->fast)  // the 128 x 128 FP32 position pass already wrote per-CTA probe partials
+        if (!p->fast && !p->grouped_gathers)  // the 128 x 128 FP32 position pass already wrote per-CTA probe partials
             timed(p, kProbeGather, 1, [&] { return launch_probe_gather<T>(pg, s); });
         timed(p, kProbeReduce, 1, [&] {
             return launch_probe_reduce<T>(p->partial_grad.as<C2<T>>(), p->partial_weight.as<T>(), p->groups, n,
@@ -1070,15 +1098,10 @@ void enqueue_position_correction(cubo_ptycho_plan *p) {
     }
 }
 
+// The rest of an iteration once the gradient sums are in: updates, constraints, position correction, error.
 template <typename T>
-void enqueue_iteration(cubo_ptycho_plan *p) {
+void enqueue_iteration_tail(cubo_ptycho_plan *p) {
     cudaStream_t s = p->ctx->stream;
-    if (p->banded) {
-        enqueue_banded_pass_and_gathers(p);
-    } else {
-        enqueue_position_pass<T>(p);
-        enqueue_gathers<T>(p);
-    }
     const cubo_ptycho_params &pp = p->params;
     const bool correct = std::is_same<T, double>::value && p->correct_positions;
     if (correct)
@@ -1110,6 +1133,17 @@ void enqueue_iteration(cubo_ptycho_plan *p) {
         return launch_error_reduce(p->error.as<double>(), p->error_count, p->divisor, p->errors.as<double>(),
                                    p->iteration.as<int>(), p->error_scratch.as<double>(), s);
     });
+}
+
+template <typename T>
+void enqueue_iteration(cubo_ptycho_plan *p) {
+    if (p->banded) {
+        enqueue_banded_pass_and_gathers(p);
+    } else {
+        enqueue_position_pass<T>(p);
+        enqueue_gathers<T>(p);
+    }
+    enqueue_iteration_tail<T>(p);
 }
 
 // One multislice iteration (MultislicePtychography.reconstruct, PtychographyEngines.swift:495-585), FP64.  The object
@@ -2026,6 +2060,20 @@ struct cubo_ptycho_batch {
     cudaGraphExec_t exec = nullptr;
     std::vector<void *> captured_errors;  // the error buffers the graph was captured with
     long long launches_per_iteration = 0;
+    // Grouped launches: the generic position passes of every item with the same square compile-time-plan detector,
+    // form and CTA shape in one persistent launch; the object gathers (and, but for the FP32 128 x 128 items, which sum
+    // their probe gradient in the pass, the probe gathers) of every item of a form in one each.  Each group holds one
+    // argument structure per item and the items' unit offsets in device memory.
+    struct Group {
+        int kind = 0;  // 0 position pass, 1 object gather, 2 probe gather
+        bool fp64 = false;
+        int N = 0, shape = 0;
+        std::vector<cubo_ptycho_plan *> plans;
+        std::vector<int> prefix;
+        DeviceBuffer args, offsets;
+    };
+    std::vector<std::unique_ptr<Group>> groups;  // DeviceBuffer does not move: held by pointer
+    bool grouping = true;  // CUBO_PTYCHO_BATCH_GROUPED=0: every item launches its own kernels (for comparison)
     ~cubo_ptycho_batch() {
         if (exec) cudaGraphExecDestroy(exec);
         if (graph) cudaGraphDestroy(graph);
@@ -2035,18 +2083,108 @@ struct cubo_ptycho_batch {
 
 namespace {
 
-// Captures one iteration of every plan of the batch into a graph (again when an error buffer moved).
+template <typename T>
+void upload_group_args(cubo_ptycho_batch::Group &g, cudaStream_t s) {
+    if (g.kind == 0) {
+        std::vector<PositionPassArgs<T>> v;
+        for (auto *p : g.plans) v.push_back(position_pass_args<T>(p));
+        upload(g.args, v, s);
+    } else if (g.kind == 1) {
+        std::vector<ObjectGatherArgs<T>> v;
+        for (auto *p : g.plans) v.push_back(object_gather_args<T>(p));
+        upload(g.args, v, s);
+    } else {
+        std::vector<ProbeGatherArgs<T>> v;
+        for (auto *p : g.plans) v.push_back(probe_gather_args<T>(p));
+        upload(g.args, v, s);
+    }
+    upload(g.offsets, g.prefix, s);
+}
+
+// Sorts the batch's plans into groups (before a capture: the argument tables hold the plans' current buffers).
+void build_groups(cubo_ptycho_batch *b) {
+    cudaStream_t s = b->ctx->stream;
+    b->groups.clear();
+    for (auto *p : b->plans) p->grouped_pass = p->grouped_gathers = false;
+    if (!b->grouping) return;
+    std::map<std::tuple<int, int, bool, int, int>, size_t> index;  // (kind, fp64, N, shape) -> group
+    auto add = [&](int kind, cubo_ptycho_plan *p, int N, int shape, int units) {
+        const auto key = std::make_tuple(kind, p->fp64 ? 1 : 0, false, N, shape);
+        auto it = index.find(key);
+        if (it == index.end()) {
+            it = index.emplace(key, b->groups.size()).first;
+            b->groups.emplace_back(new cubo_ptycho_batch::Group());
+            auto &ng = *b->groups.back();
+            ng.kind = kind;
+            ng.fp64 = p->fp64;
+            ng.N = N;
+            ng.shape = shape;
+            ng.prefix.push_back(0);
+        }
+        auto &g = *b->groups[it->second];
+        g.plans.push_back(p);
+        g.prefix.push_back(g.prefix.back() + units);
+    };
+    for (auto *p : b->plans) {
+        if (p->states != 1 || p->multislice || p->banded || p->correct_positions) continue;
+        if (p->fp64) ensure_dpsi<double>(p);
+        else ensure_dpsi<float>(p);
+        const bool generic_pass = p->fp64 ? !p->global64 && !p->plane128 : !p->fast && !p->bf16;
+        if (generic_pass && position_pass_groupable(p->R, p->C, p->fp64)) {
+            add(0, p, p->R, p->params.pass_shape, p->P);
+            p->grouped_pass = true;
+        }
+        add(1, p, 0, 0, p->tiles);
+        if (!p->fast) add(2, p, 0, 0, ((p->n + 255) / 256) * p->groups);
+        p->grouped_gathers = true;
+    }
+    for (auto &g : b->groups) {
+        if (g->fp64) upload_group_args<double>(*g, s);
+        else upload_group_args<float>(*g, s);
+    }
+}
+
+template <typename T>
+cudaError_t launch_group(const cubo_ptycho_batch::Group &g, cudaStream_t s) {
+    const int items = (int)g.plans.size(), total = g.prefix.back();
+    if (g.kind == 0)
+        return launch_position_pass_grouped<T>(g.args.as<PositionPassArgs<T>>(), g.offsets.as<int>(), items, total,
+                                               g.N, g.shape, s);
+    if (g.kind == 1)
+        return launch_object_gather_grouped<T>(g.args.as<ObjectGatherArgs<T>>(), g.offsets.as<int>(), items, total, s);
+    return launch_probe_gather_grouped<T>(g.args.as<ProbeGatherArgs<T>>(), g.offsets.as<int>(), items, total, s);
+}
+
+// Captures one iteration of every plan of the batch into a graph (again when an error buffer moved): every item's
+// shifted probes and own position passes, the grouped passes, the grouped gathers, then every item's own gathers,
+// reductions, updates, constraints and error.
 void capture_batch(cubo_ptycho_batch *b) {
     if (b->exec) { cudaGraphExecDestroy(b->exec); b->exec = nullptr; }
     if (b->graph) { cudaGraphDestroy(b->graph); b->graph = nullptr; }
     cudaStream_t s = b->ctx->stream;
+    build_groups(b);
+    check(cudaStreamSynchronize(s), "batch groups");
     long long before = 0;
     for (auto *p : b->plans) before += p->launches;
     check(cudaStreamBeginCapture(s, cudaStreamCaptureModeThreadLocal), "cudaStreamBeginCapture");
     try {
         for (auto *p : b->plans) {
-            if (p->fp64) enqueue_iteration<double>(p);
-            else enqueue_iteration<float>(p);
+            if (p->banded) enqueue_banded_pass_and_gathers(p);
+            else if (p->fp64) enqueue_position_pass<double>(p);
+            else enqueue_position_pass<float>(p);
+        }
+        for (int kind = 0; kind < 3; kind++)  // the passes before any gather
+            for (const auto &g : b->groups)
+                if (g->kind == kind)
+                    check(g->fp64 ? launch_group<double>(*g, s) : launch_group<float>(*g, s), "grouped launch");
+        for (auto *p : b->plans) {
+            if (p->fp64) {
+                if (!p->banded) enqueue_gathers<double>(p);
+                enqueue_iteration_tail<double>(p);
+            } else {
+                if (!p->banded) enqueue_gathers<float>(p);
+                enqueue_iteration_tail<float>(p);
+            }
         }
     } catch (...) {
         cudaGraph_t g = nullptr;
@@ -2058,7 +2196,7 @@ void capture_batch(cubo_ptycho_batch *b) {
     check(cudaGraphInstantiate(&b->exec, b->graph, 0), "cudaGraphInstantiate");
     long long after = 0;
     for (auto *p : b->plans) after += p->launches;
-    b->launches_per_iteration = after - before;
+    b->launches_per_iteration = after - before + (long long)b->groups.size();
     b->captured_errors.clear();
     for (auto *p : b->plans) b->captured_errors.push_back(p->errors.ptr);
 }
@@ -2074,6 +2212,7 @@ int cubo_ptycho_batch_create(cubo_ptycho_context *ctx, int count, const cubo_pty
     auto *b = new (std::nothrow) cubo_ptycho_batch();
     if (!b) return CUBO_PTYCHO_OUT_OF_MEMORY;
     b->ctx = ctx;
+    if (const char *env = std::getenv("CUBO_PTYCHO_BATCH_GROUPED")) b->grouping = std::atoi(env) != 0;
     for (int i = 0; i < count; i++) {
         if (params[i].has_position_correction) {  // the positions it moves are read back between iterations
             delete b;

@@ -1,5 +1,6 @@
 """Batches: independent reconstructions of different scan, detector and object sizes, replayed from one captured CUDA
-graph, give bitwise the results of running each reconstruction alone."""
+graph (the passes of items with a compile-time-plan detector and every item's gathers in grouped persistent launches),
+give bitwise the results of running each reconstruction alone."""
 import numpy as np
 import pytest
 
@@ -10,8 +11,9 @@ pytestmark = pytest.mark.gpu
 
 def _items():
     items = []
+    # several items per grouped launch: two 64 x 64 FP32 passes, every item's gathers of a form
     for scan, det, seed, prec in [(4, 32, 1, "fp32"), (6, 64, 2, "fp32"), (3, 128, 3, "fp32"), (3, 128, 4, "split_bf16"),
-                                  (5, 48, 5, "fp32"), (4, 64, 6, "fp64")]:
+                                  (5, 48, 5, "fp32"), (4, 64, 6, "fp64"), (5, 64, 8, "fp32"), (3, 96, 7, "fp32")]:
         s = scenes.raster_scene(scan=scan, det=det, step=4, seed=seed)
         items.append(dict(amplitudes=s["amplitudes"], positions=s["positions"], object=s["object"], probe=s["probe"],
                           step_size=0.5, precision=prec))
