@@ -146,17 +146,16 @@ __device__ __forceinline__ int group_item(const int *prefix, int items, int u) {
 }
 
 // Grouped position pass: the positions of every item (independent reconstructions with the same detector) in one
-// persistent launch; each CTA walks the work list (item, position) in a fixed stride.  Every position's arithmetic is
-// the one-launch kernel's.
+// launch, one CTA per (item, position) unit.  Every position's arithmetic is the one-launch kernel's.  (A persistent
+// form, CTAs walking the work list in a fixed stride, kept the FFT stages' register arrays in local memory: 0.7-1.9 KB
+// of stack per thread; one unit per CTA compiles like the one-launch kernel.)
 template <typename T, int NT, int MAXN, int MINB, int N, int R0, int R1, int R2>
 __global__ void __launch_bounds__(NT, MINB) position_pass_grouped_kernel(const PositionPassArgs<T> *args,
                                                                          const int *prefix, int items, int total) {
-    for (int u = blockIdx.x; u < total; u += gridDim.x) {
-        const int it = group_item(prefix, items, u);
-        const PositionPassArgs<T> &a = args[it];
-        position_pass_body<T, NT, MAXN, N, R0, R1, R2>(a, a.first + (u - prefix[it]));
-        __syncthreads();  // the next unit overwrites the plane and twiddles in shared memory
-    }
+    const int u = blockIdx.x;
+    const int it = group_item(prefix, items, u);
+    const PositionPassArgs<T> a = args[it];
+    position_pass_body<T, NT, MAXN, N, R0, R1, R2>(a, a.first + (u - prefix[it]));
 }
 
 // FP64 position pass through global memory, for detectors whose FP64 plane does not fit one CTA's shared memory (above
@@ -342,15 +341,14 @@ __global__ void __launch_bounds__(kGatherThreads) object_gather_kernel(ObjectGat
     object_gather_body<T, MIXED>(a, blockIdx.x);
 }
 
-// Grouped object gather: the tiles of every item in one persistent launch (work list (item, tile), fixed stride).
+// Grouped object gather: the tiles of every item in one launch, one CTA per (item, tile) unit.
 template <typename T>
 __global__ void __launch_bounds__(kGatherThreads) object_gather_grouped_kernel(const ObjectGatherArgs<T> *args,
                                                                                const int *prefix, int items, int total) {
-    for (int u = blockIdx.x; u < total; u += gridDim.x) {
-        const int it = group_item(prefix, items, u);
-        object_gather_body<T, false>(args[it], u - prefix[it]);
-        __syncthreads();  // the next unit restages the candidate offsets
-    }
+    const int u = blockIdx.x;
+    const int it = group_item(prefix, items, u);
+    const ObjectGatherArgs<T> a = args[it];
+    object_gather_body<T, false>(a, u - prefix[it]);
 }
 
 // ------------------------------------------------------------------------------------------------ candidate lists
@@ -469,17 +467,15 @@ __global__ void __launch_bounds__(kProbeThreads) probe_gather_kernel(ProbeGather
     probe_gather_body<T>(a, blockIdx.x, blockIdx.y);
 }
 
-// Grouped probe gather: every item's (pixel block, position group) units in one persistent launch.
+// Grouped probe gather: every item's (pixel block, position group) units in one launch, one CTA per unit.
 template <typename T>
 __global__ void __launch_bounds__(kProbeThreads) probe_gather_grouped_kernel(const ProbeGatherArgs<T> *args,
                                                                              const int *prefix, int items, int total) {
-    for (int u = blockIdx.x; u < total; u += gridDim.x) {
-        const int it = group_item(prefix, items, u);
-        const ProbeGatherArgs<T> &a = args[it];
-        const int blocks = (a.n + kProbeThreads - 1) / kProbeThreads, v = u - prefix[it];
-        probe_gather_body<T>(a, v % blocks, v / blocks);
-        __syncthreads();  // the next unit restages the window bases
-    }
+    const int u = blockIdx.x;
+    const int it = group_item(prefix, items, u);
+    const ProbeGatherArgs<T> a = args[it];
+    const int blocks = (a.n + kProbeThreads - 1) / kProbeThreads, v = u - prefix[it];
+    probe_gather_body<T>(a, v % blocks, v / blocks);
 }
 
 template <typename T>
@@ -660,17 +656,6 @@ void (*fixed_grouped_kernel(int N, int threads))(const PositionPassArgs<T> *, co
     return threads == 512 ? FixedShape<T, 96, 512>::grouped() : FixedShape<T, 96, 256>::grouped();
 }
 
-// Persistent grid of a grouped launch: the kernel's resident CTAs on every SM, at most one per unit.
-template <typename K>
-int persistent_grid(K kernel, int threads, size_t smem, int total) {
-    int device = 0, sms = 148, per_sm = 1;
-    if (cudaGetDevice(&device) == cudaSuccess) cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, device);
-    if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kernel, threads, smem) != cudaSuccess || per_sm < 1)
-        per_sm = 1;
-    cudaGetLastError();
-    return (int)std::max<long long>(1, std::min<long long>(total, (long long)per_sm * sms));
-}
-
 }  // namespace
 
 bool position_pass_supported(int n, bool fp64) {
@@ -766,8 +751,7 @@ cudaError_t launch_position_pass_grouped(const PositionPassArgs<T> *args, const 
     if (threads == 0) return cudaErrorInvalidValue;
     if (total <= 0) return cudaSuccess;
     const size_t smem = pass_smem<T>(N * N, N, N);
-    auto kernel = fixed_grouped_kernel<T>(N, threads);
-    kernel<<<persistent_grid(kernel, threads, smem, total), threads, smem, s>>>(args, prefix, items, total);
+    fixed_grouped_kernel<T>(N, threads)<<<total, threads, smem, s>>>(args, prefix, items, total);
     return cudaGetLastError();
 }
 
@@ -775,8 +759,7 @@ template <typename T>
 cudaError_t launch_object_gather_grouped(const ObjectGatherArgs<T> *args, const int *prefix, int items, int total,
                                          cudaStream_t s) {
     if (total <= 0) return cudaSuccess;
-    auto kernel = object_gather_grouped_kernel<T>;
-    kernel<<<persistent_grid(kernel, kGatherThreads, 0, total), kGatherThreads, 0, s>>>(args, prefix, items, total);
+    object_gather_grouped_kernel<T><<<total, kGatherThreads, 0, s>>>(args, prefix, items, total);
     return cudaGetLastError();
 }
 
@@ -784,8 +767,7 @@ template <typename T>
 cudaError_t launch_probe_gather_grouped(const ProbeGatherArgs<T> *args, const int *prefix, int items, int total,
                                         cudaStream_t s) {
     if (total <= 0) return cudaSuccess;
-    auto kernel = probe_gather_grouped_kernel<T>;
-    kernel<<<persistent_grid(kernel, kProbeThreads, 0, total), kProbeThreads, 0, s>>>(args, prefix, items, total);
+    probe_gather_grouped_kernel<T><<<total, kProbeThreads, 0, s>>>(args, prefix, items, total);
     return cudaGetLastError();
 }
 
