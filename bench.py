@@ -510,7 +510,8 @@ def run_batched(args, world, rank, local):
             "dtype": "f32", "data": "synthetic",
             "config": {"workload": "batched: 64 reconstructions, scans 24..96 (step 4), detectors {64,96,128}^2, "
                                    "defocus 50..200 A, seeds 1000+i", "positions_total": r["positions_total"],
-                       "detectors": r["detectors"], "gather_tiles": r["gather_tiles"]},
+                       "detectors": r["detectors"], "gather_tiles": r["gather_tiles"],
+                       "pass_shapes": r["pass_shapes"]},
             "gpu_launches": r["gpu_launches"], "graph_launches": r["graph_launches"], "clocks": r["clocks"]}),
             flush=True)
 
