@@ -294,7 +294,9 @@ def dist_setup(args):
     if world > 1:
         import torch.distributed as dist
         from datetime import timedelta
-        backend = "gloo" if args.impl == "reference" else "nccl"
+        # CUBO_BENCH_BACKEND=gloo: the GPU arm's collectives through host memory, so that several ranks can share one
+        # GPU in a test (their kernels never wait on one another); the benchmark itself uses NCCL
+        backend = "gloo" if args.impl == "reference" else os.environ.get("CUBO_BENCH_BACKEND", "nccl")
         dist.init_process_group(backend, timeout=timedelta(seconds=600))
     return world, rank, local
 
@@ -921,6 +923,8 @@ def main():
         return
 
     import torch
+    if world > 1 and os.environ.get("CUBO_BENCH_BACKEND") == "gloo":
+        local %= max(1, torch.cuda.device_count())  # ranks sharing the GPUs there are
     torch.cuda.set_device(local)
     import cubokit_b200 as cb
     from cubokit_b200 import synthetic

@@ -83,3 +83,34 @@ def test_two_bands_of_a_mixed_state_plan(tmp_path):
     one = cb.MixedstatePtychography.reconstruct(s["amplitudes"], start, s["object"], probes, **KW)
     assert max(gc.complex_gap(a["object"], one.object), gc.gap(a["errors"], one.errors),
                gc.complex_gap(gc.align_phases(a["probe"], one.probes), one.probes)) < 1e-11
+
+
+def test_two_runs_at_two_ranks_agree_bit_for_bit(tmp_path):
+    """The sum over the bands has a fixed order (every rank adds the all-gathered band sums in rank order), so two runs
+    with the same number of ranks give the same bits."""
+    (tmp_path / "a").mkdir()
+    (tmp_path / "b").mkdir()
+    first = _run_two_ranks(tmp_path / "a", "fp32", 1)
+    second = _run_two_ranks(tmp_path / "b", "fp32", 1)
+    for key in ("object", "probe", "errors"):
+        assert np.array_equal(first[0][key], second[0][key]), key
+
+
+def test_bench_sharded_line_with_two_ranks():
+    """bench.py --gpus 2 under torchrun: one reconstruction of a 16 x 16 scan in two position bands (the ranks share this
+    GPU over gloo here; on a multi-GPU node each rank has its own GPU and NCCL), one JSON line from rank 0 with the
+    whole job's rate, strong scaling."""
+    import json
+    import subprocess
+    import sys
+    env = dict(os.environ, CUBO_BENCH_BACKEND="gloo")
+    cmd = [sys.executable, "-m", "torch.distributed.run", "--nnodes=1", "--nproc-per-node", "2", "--master-addr",
+           "127.0.0.1", "--master-port", str(_free_port()), "bench.py", "--gpus", "2", "--scan", "16", "--steps", "2",
+           "--warmup", "1", "--no-e2e"]
+    r = subprocess.run(cmd, cwd=str(ROOT), capture_output=True, text=True, timeout=900, env=env)
+    assert r.returncode == 0, r.stdout[-2000:] + r.stderr[-3000:]
+    lines = [json.loads(l) for l in r.stdout.splitlines() if l.startswith("{")]
+    assert len(lines) == 1, r.stdout
+    line = lines[0]
+    assert line["n_gpus"] == 2 and line["scaling"] == "strong" and line["value"] > 0 and line["gpu_launches"] > 0
+    assert "position bands" in line["config"]["parallelism"]
