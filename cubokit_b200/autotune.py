@@ -4,10 +4,11 @@ For a problem (detector, object and scan sizes, form) every candidate is timed o
 candidate, a warm-up iteration, then the kernel's device time over a few iterations from the plan's CUDA-event kernel
 statistics.  `tune` picks the object-gather tile (32 x 8, 16 x 16, 64 x 4 pixels, along the residual's contiguous
 axis); `tune_pass` the CTA shape of the shared-memory position pass at the detectors it runs with a compile-time radix
-plan (64 x 64: 128, 256 or 512 threads; 96 x 96: 256 or 512).  The fastest candidate is cached in a JSON file keyed by
+plan or the FP32 register-line kernel (64 x 64 and 96 x 96).  The fastest candidate is cached in a JSON file keyed by
 (what, detector, object, positions, form, GPU name), so the timing runs once per shape per machine.  Neither choice
-changes the object or the probe: every object pixel sums the same positions in the same order whatever the tile, and
-every butterfly computes the same values whatever the CTA shape.
+changes the object: every object pixel sums the same positions in the same order whatever the tile, and every
+butterfly computes the same values whatever the shared-memory CTA shape; the FP32 register-line kernel agrees with
+those to FP32 round-off.
 """
 from __future__ import annotations
 
@@ -96,15 +97,16 @@ def tune(amplitudes, positions, obj, probe, precision="fp32", iterations=3, devi
                   "object_gather", "gather_tile", CANDIDATES, NAMES)
 
 
-PASS_CANDIDATES = {64: (1, 2, 3), 96: (2, 3)}
-PASS_NAMES = {0: "default", 1: "128 threads", 2: "256 threads", 3: "512 threads"}
+PASS_CANDIDATES = {("fp32", 64): (0, 1, 2, 3), ("fp32", 96): (0, 2, 3), ("fp64", 64): (1, 2, 3), ("fp64", 96): (3,)}
+PASS_NAMES = {0: "default", 1: "shared memory, 128 threads", 2: "shared memory, 256 threads",
+              3: "shared memory, 512 threads"}
 
 
 def tune_pass(amplitudes, positions, obj, probe, precision="fp32", iterations=3, device=0, use_cache=True):
     """The fastest position-pass CTA shape for this problem (and the timings, ms per position-pass launch, by
     candidate); (0, {}) for detectors without a choice (every size but 64 x 64 and 96 x 96)."""
     rows, columns = np.asarray(probe).shape
-    if rows != columns or rows not in PASS_CANDIDATES or precision not in ("fp32", "fp64"):
+    if rows != columns or (precision, rows) not in PASS_CANDIDATES:
         return 0, {}
     return _tuned("pass", amplitudes, positions, obj, probe, precision, iterations, device, use_cache,
-                  "position_pass", "pass_shape", PASS_CANDIDATES[rows], PASS_NAMES)
+                  "position_pass", "pass_shape", PASS_CANDIDATES[(precision, rows)], PASS_NAMES)

@@ -140,6 +140,15 @@ constexpr int kGatherThreads = kTileW * kTileH;
 
 // engine_kernels.cu
 template <typename T> cudaError_t launch_position_pass(const PositionPassArgs<T> &a, int shape, cudaStream_t s);
+// linepass.cu: the FP32 position pass for 64 x 64 and 96 x 96 detectors with register-resident line transforms (four
+// steps: R-point DFTs in registers, one in-group exchange, G-point DFTs), one CTA per position; the default FP32 pass
+// at those sizes (cubo_ptycho_params.pass_shape 0).
+bool line_pass_applicable(int rows, int columns);
+cudaError_t configure_line_pass();
+cudaError_t launch_line_pass(const PositionPassArgs<float> &a, cudaStream_t s);
+cudaError_t launch_line_pass_grouped(const PositionPassArgs<float> *args, const int *prefix, int items, int total, int N,
+                                     cudaStream_t s);
+
 // Grouped launches (batches of independent reconstructions): every item's units in one persistent launch.  prefix holds
 // items + 1 offsets (item i owns units prefix[i] .. prefix[i + 1] - 1); args one structure per item, in device memory.
 // The position pass groups items of one square detector with a compile-time plan (position_pass_groupable), units =

@@ -690,7 +690,7 @@ cudaError_t configure_kernels() {
                                          cudaFuncAttributeMaxDynamicSharedMemorySize, optin);
             if (e != cudaSuccess) return e;
         }
-    return cudaSuccess;
+    return configure_line_pass();
 }
 
 size_t position_pass_smem(int n, int rows, int columns, bool fp64) {
@@ -731,6 +731,8 @@ template <typename T>
 cudaError_t launch_position_pass(const PositionPassArgs<T> &a, int shape, cudaStream_t s) {
     constexpr int maxn = PassConfig<T>::maxn;
     if (a.count <= 0) return cudaSuccess;
+    if constexpr (std::is_same<T, float>::value)
+        if (shape == 0 && line_pass_applicable(a.rows, a.columns)) return launch_line_pass(a, s);
     const size_t smem = pass_smem<T>(a.n, a.rows, a.columns);
     const int threads = a.rows == a.columns ? fixed_threads<T>(a.rows, shape) : 0;
     if (threads > 0)
@@ -747,9 +749,11 @@ bool position_pass_groupable(int rows, int columns, bool fp64) {
 template <typename T>
 cudaError_t launch_position_pass_grouped(const PositionPassArgs<T> *args, const int *prefix, int items, int total,
                                          int N, int shape, cudaStream_t s) {
+    if (total <= 0) return cudaSuccess;
+    if constexpr (std::is_same<T, float>::value)
+        if (shape == 0 && line_pass_applicable(N, N)) return launch_line_pass_grouped(args, prefix, items, total, N, s);
     const int threads = fixed_threads<T>(N, shape);
     if (threads == 0) return cudaErrorInvalidValue;
-    if (total <= 0) return cudaSuccess;
     const size_t smem = pass_smem<T>(N * N, N, N);
     fixed_grouped_kernel<T>(N, threads)<<<total, threads, smem, s>>>(args, prefix, items, total);
     return cudaGetLastError();

@@ -129,13 +129,14 @@ typedef struct {
     /* Result.positions: when both are non-NULL, cubo_ptycho_reconstruct writes the positions after the last iteration
      * (count values each; the given positions when nothing corrected them). */
     double *position_rows_out, *position_columns_out;
-    /* CTA shape of the shared-memory position pass at the detectors it runs with a compile-time radix plan (64 x 64 and
-     * 96 x 96): 0 = default, 1 = 128 threads, 2 = 256 threads, 3 = 512 threads per CTA (as many CTAs per SM as
-     * registers and shared memory allow; a shape that would spill registers falls back to the nearest one that does
-     * not); other detector sizes ignore it.  A performance choice only: the object and probe are bitwise the same
-     * whatever the shape (every butterfly computes the same values); the per-position error is summed over the CTA's
-     * threads, so the reported errors agree to round-off.  Appended last so that the fields before it keep their
-     * offsets. */
+    /* Position-pass kernel at 64 x 64 and 96 x 96 detectors: 0 = default (FP32: register-resident line transforms,
+     * four steps per line; FP64: the shared-memory pass with the compile-time radix plan at 256 threads for 64 x 64 and
+     * 512 for 96 x 96); 1, 2, 3 = the shared-memory pass with the compile-time plan at 128, 256, 512 threads per CTA
+     * (as many CTAs per SM as registers and shared memory allow; a shape that would spill falls back to the nearest one
+     * that does not).  Other detector sizes ignore it.  A performance choice: the shared-memory shapes give the same
+     * object and probe bit for bit (every butterfly computes the same values; the per-position error is summed over the
+     * CTA's threads and agrees to round-off); the register-line kernel factors the transform differently and agrees
+     * with them to FP32 round-off.  Appended last so that the fields before it keep their offsets. */
     int pass_shape;
 } cubo_ptycho_params;
 

@@ -59,16 +59,18 @@ def test_gather_tiles_agree_bitwise_and_autotune_picks_one(tmp_path, monkeypatch
 
 
 def test_pass_shapes_agree_bitwise_and_autotune_picks_one(tmp_path, monkeypatch):
-    """The shared-memory position pass at 64 x 64 and 96 x 96 runs in several CTA shapes (128, 256, 512 threads): every
-    shape gives the same object and probe bit for bit (the reported error is summed over the CTA's threads, so it
-    agrees to round-off), and the autotuner times the shapes and caches its choice."""
+    """The position pass at 64 x 64 and 96 x 96 runs as the shared-memory pass in several CTA shapes (128, 256, 512
+    threads) or, in FP32 by default, as the register-line kernel.  The shared-memory shapes give the same object and
+    probe bit for bit (the reported error is summed over the CTA's threads, so it agrees to round-off); the register-line
+    kernel factors the transforms differently and agrees with them to FP32 round-off.  The autotuner times the
+    candidates and caches its choice."""
     import cubokit_b200 as cb
     from cubokit_b200 import autotune
     monkeypatch.setenv("CUBOKIT_B200_CACHE", str(tmp_path))
     for precision in ("fp32", "fp64"):
         for det in (64, 96):
             s = scenes.raster_scene(scan=4, det=det, step=4, seed=9)
-            ref = None
+            results = {}
             for shape in (0, 1, 2, 3):
                 plan = cb.Plan(s["amplitudes"], s["positions"], s["object"].shape, s["probe"].shape, step_size=0.5,
                                precision=precision, pass_shape=shape)
@@ -76,11 +78,19 @@ def test_pass_shapes_agree_bitwise_and_autotune_picks_one(tmp_path, monkeypatch)
                 errors = plan.iterate(2)
                 o, p = plan.get_state()
                 plan.close()
-                if ref is None:
-                    ref = (o, p, errors)
+                results[shape] = (o, p, errors)
+            ref = results[3]
+            shared = (1, 2, 3) if precision == "fp32" else (0, 1, 2, 3)
+            for shape in shared:
+                o, p, errors = results[shape]
                 assert np.array_equal(o, ref[0]) and np.array_equal(p, ref[1]), (precision, det, shape)
                 assert np.allclose(errors, ref[2], rtol=1e-12 if precision == "fp64" else 1e-6, atol=0), (precision, det)
+            if precision == "fp32":
+                o, p, errors = results[0]
+                assert np.max(np.abs(o - ref[0])) <= 1e-5 and np.max(np.abs(p - ref[1])) <= 1e-5 * np.max(np.abs(ref[1]))
+                assert np.allclose(errors, ref[2], rtol=1e-5, atol=0)
             best, ms = autotune.tune_pass(s["amplitudes"], s["positions"], s["object"], s["probe"], precision=precision)
-            assert best in autotune.PASS_CANDIDATES[det] and len(ms) == len(autotune.PASS_CANDIDATES[det])
+            cands = autotune.PASS_CANDIDATES[(precision, det)]
+            assert best in cands and len(ms) == len(cands)
             assert autotune.tune_pass(s["amplitudes"], s["positions"], s["object"], s["probe"],
                                       precision=precision)[0] == best
