@@ -70,6 +70,30 @@ __device__ __forceinline__ uint32_t mnmajor_offset(int k, int col) {
 
 __device__ __forceinline__ int wrap_once(int v, int size) { return v < 0 ? v + size : (v >= size ? v - size : v); }
 
+// Packed FP32x2 arithmetic (sm_100 mul / fma / sub .f32x2): one instruction for two values, each rounded as the scalar
+// operation rounds it.
+__device__ __forceinline__ float2 pmul(float2 a, float2 b) {
+    float2 d;
+    asm("{\n\t.reg .b64 ra, rb, rd;\n\tmov.b64 ra, {%2, %3};\n\tmov.b64 rb, {%4, %5};\n\t"
+        "mul.rn.f32x2 rd, ra, rb;\n\tmov.b64 {%0, %1}, rd;\n\t}"
+        : "=f"(d.x), "=f"(d.y) : "f"(a.x), "f"(a.y), "f"(b.x), "f"(b.y));
+    return d;
+}
+__device__ __forceinline__ float2 pfma(float2 a, float2 b, float2 c) {
+    float2 d;
+    asm("{\n\t.reg .b64 ra, rb, rc, rd;\n\tmov.b64 ra, {%2, %3};\n\tmov.b64 rb, {%4, %5};\n\tmov.b64 rc, {%6, %7};\n\t"
+        "fma.rn.f32x2 rd, ra, rb, rc;\n\tmov.b64 {%0, %1}, rd;\n\t}"
+        : "=f"(d.x), "=f"(d.y) : "f"(a.x), "f"(a.y), "f"(b.x), "f"(b.y), "f"(c.x), "f"(c.y));
+    return d;
+}
+__device__ __forceinline__ float2 psub(float2 a, float2 b) {
+    float2 d;
+    asm("{\n\t.reg .b64 ra, rb, rd;\n\tmov.b64 ra, {%2, %3};\n\tmov.b64 rb, {%4, %5};\n\t"
+        "sub.rn.f32x2 rd, ra, rb;\n\tmov.b64 {%0, %1}, rd;\n\t}"
+        : "=f"(d.x), "=f"(d.y) : "f"(a.x), "f"(a.y), "f"(b.x), "f"(b.y));
+    return d;
+}
+
 // The frequency paired with j by T: 128 - j, and 64 for j = 0.
 __host__ __device__ __forceinline__ int mirror(int j) { return j == 0 ? 64 : kN - j; }
 
@@ -334,7 +358,11 @@ __global__ void __launch_bounds__(kThreads, 1) bf16_position_kernel(Bf16Args a) 
             *a.fault = 1;
         }
         {
-            double err = 0;
+            // the squared residual of this thread's 32 frequencies in FP32 (two packed lanes), then in FP64 over the
+            // threads, warps and positions, as the reference's Float path sums a pattern in Float and the patterns in
+            // Double (PtychographySingle.swift:157-172)
+            float2 errv = make_float2(0.f, 0.f);
+            const float2 inv_n2 = make_float2(inv_n, inv_n), minus_one = make_float2(-1.f, -1.f);
 #pragma unroll 1
             for (int u = 0; u < kSub; u++) {
                 float4 am4[4];
@@ -345,24 +373,31 @@ __global__ void __launch_bounds__(kThreads, 1) bf16_position_kernel(Bf16Args a) 
 #pragma unroll
                 for (int side = 0; side < 2; side++) {
 #pragma unroll
-                    for (int e = 0; e < 8; e++) {
+                    for (int e = 0; e < 8; e += 2) {  // two frequencies per packed instruction
                         const float4 av = am4[2 * side + (e >> 2)];
-                        const float am = (e & 3) == 0 ? av.x : (e & 3) == 1 ? av.y : (e & 3) == 2 ? av.z : av.w;
+                        const float2 am = (e & 2) ? make_float2(av.z, av.w) : make_float2(av.x, av.y);
+                        const float2 re = make_float2(fr[side][e], fr[side][e + 1]);
+                        const float2 im = make_float2(fi[side][e], fi[side][e + 1]);
                         // |F| and A / |F| through one reciprocal square root; F = 0 takes the amplitude itself
-                        const float m2 = fr[side][e] * fr[side][e] + fi[side][e] * fi[side][e];
-                        const bool nonzero = m2 > 0.f;
-                        const float inv = rsqrtf(m2);
-                        const float miss = am - (nonzero ? m2 * inv : 0.f);
-                        err += (double)(miss * miss);
-                        const float sc = (am * inv - 1.0f) * inv_n;
-                        fr[side][e] = nonzero ? fr[side][e] * sc : am * inv_n;
-                        fi[side][e] = nonzero ? fi[side][e] * sc : 0.f;
+                        const float2 m2 = pfma(re, re, pmul(im, im));
+                        const bool nz0 = m2.x > 0.f, nz1 = m2.y > 0.f;
+                        const float2 inv = make_float2(rsqrtf(m2.x), rsqrtf(m2.y));
+                        const float2 mag = pmul(m2, inv);
+                        const float2 miss = psub(am, make_float2(nz0 ? mag.x : 0.f, nz1 ? mag.y : 0.f));
+                        errv = pfma(miss, miss, errv);
+                        const float2 sc = pmul(pfma(am, inv, minus_one), inv_n2);
+                        const float2 nr = pmul(re, sc), ni = pmul(im, sc), zr = pmul(am, inv_n2);
+                        fr[side][e] = nz0 ? nr.x : zr.x;
+                        fr[side][e + 1] = nz1 ? nr.y : zr.y;
+                        fi[side][e] = nz0 ? ni.x : 0.f;
+                        fi[side][e + 1] = nz1 ? ni.y : 0.f;
                     }
                     const uint32_t off = mnmajor_offset(side ? mirror(j) : j, kCols * g + (kCols / 2) * h + 8 * u);
                     store_split8(planes, kReHi, off, fr[side]);
                     store_split8(planes, kImHi, off, fi[side]);
                 }
             }
+            double err = (double)errv.x + (double)errv.y;
 #pragma unroll
             for (int o = 16; o > 0; o >>= 1) err += __shfl_down_sync(0xffffffffu, err, o);
             if (lane == 0) a.error[(size_t)p * (kThreads / 32) + warp] = err;
