@@ -30,6 +30,10 @@ struct cubo_ptycho_context {
     bool timing = false;           // CUDA events around each preprocessing kernel launch
     double prepare_ms = 0.0;       // their device time, summed
     long long prepare_launches = 0;
+    // page-locked host staging for the object and probe transfers (grown on demand, freed with the context): copies
+    // from it run at full link speed and its pages are already mapped
+    void *pinned = nullptr;
+    size_t pinned_bytes = 0;
 };
 
 namespace {
@@ -192,6 +196,18 @@ double bf16_to_double(uint16_t b) {
 }
 
 }  // namespace
+
+// The context's page-locked staging buffer of at least `bytes` (its contents are not kept when it grows).
+void *pinned_staging(cubo_ptycho_context *ctx, size_t bytes) {
+    if (ctx->pinned_bytes < bytes) {
+        if (ctx->pinned) cudaFreeHost(ctx->pinned);
+        ctx->pinned = nullptr;
+        ctx->pinned_bytes = 0;
+        check(cudaHostAlloc(&ctx->pinned, bytes, cudaHostAllocDefault), "cudaHostAlloc staging");
+        ctx->pinned_bytes = bytes;
+    }
+    return ctx->pinned;
+}
 
 // ------------------------------------------------------------------------------------------------ the plan
 
@@ -1430,6 +1446,7 @@ int cubo_ptycho_destroy(cubo_ptycho_context *ctx) {
         cudaStreamDestroy(ctx->stream);
     }
     BlockCache::get().context_destroyed(ctx->device);
+    if (ctx->pinned) cudaFreeHost(ctx->pinned);
     delete ctx;
     return CUBO_PTYCHO_OK;
 }
@@ -1781,21 +1798,23 @@ int cubo_ptycho_plan_set_state(cubo_ptycho_plan *p, const double *ore, const dou
             if (!std::isfinite(pre[k]) || !std::isfinite(pim[k])) fail(CUBO_PTYCHO_INVALID_INPUT, "probe not finite");
         cudaStream_t s = p->ctx->stream;
         p->tape_valid = false;
-        std::vector<double2> probe(probe_values);
+        // through the context's pinned staging buffer: the probe (complex128), then the object in the plan's type
+        const size_t object_bytes = (size_t)object_values * (p->fp64 ? sizeof(double2) : sizeof(float2));
+        uint8_t *stage = static_cast<uint8_t *>(pinned_staging(p->ctx, probe_values * sizeof(double2) + object_bytes));
+        double2 *probe = reinterpret_cast<double2 *>(stage);
         for (size_t k = 0; k < probe_values; k++) probe[k] = make_double2(pre[k], pim[k]);
-        check(cudaMemcpyAsync(p->probe64.ptr, probe.data(), probe_values * sizeof(double2), cudaMemcpyHostToDevice, s),
-              "upload probe");
         if (p->fp64) {
-            std::vector<double2> o((size_t)object_values);
+            double2 *o = reinterpret_cast<double2 *>(stage + probe_values * sizeof(double2));
             for (long long j = 0; j < object_values; j++) o[j] = make_double2(ore[j], oim[j]);
-            check(cudaMemcpyAsync(p->object.ptr, o.data(), o.size() * sizeof(double2), cudaMemcpyHostToDevice, s), "upload object");
-            check(cudaStreamSynchronize(s), "sync");
         } else {
-            std::vector<float2> o((size_t)p->objects);
+            float2 *o = reinterpret_cast<float2 *>(stage + probe_values * sizeof(double2));
             for (long long j = 0; j < p->objects; j++) o[j] = make_float2((float)ore[j], (float)oim[j]);
-            check(cudaMemcpyAsync(p->object.ptr, o.data(), o.size() * sizeof(float2), cudaMemcpyHostToDevice, s), "upload object");
-            check(cudaStreamSynchronize(s), "sync");
         }
+        check(cudaMemcpyAsync(p->probe64.ptr, probe, probe_values * sizeof(double2), cudaMemcpyHostToDevice, s),
+              "upload probe");
+        check(cudaMemcpyAsync(p->object.ptr, stage + probe_values * sizeof(double2), object_bytes,
+                              cudaMemcpyHostToDevice, s), "upload object");
+        check(cudaStreamSynchronize(s), "sync");
         // the initial Fourier amplitude for fixProbeAperture (PtychographyConstraints.swift:79-83)
         if (p->params.fix_probe_aperture) {
             check(cudaMemcpyAsync(p->scratch64.ptr, p->probe64.ptr, (size_t)p->n * sizeof(double2), cudaMemcpyDeviceToDevice, s), "copy");
@@ -1811,19 +1830,21 @@ int cubo_ptycho_plan_get_state(cubo_ptycho_plan *p, double *ore, double *oim, do
     return run_guarded(p->ctx, [&] {
         cudaStream_t s = p->ctx->stream;
         const size_t probe_values = (size_t)p->states * p->n;
-        std::vector<double2> probe(probe_values);
-        check(cudaMemcpyAsync(probe.data(), p->probe64.ptr, probe_values * sizeof(double2), cudaMemcpyDeviceToHost, s),
+        const size_t object_values = p->fp64 ? (size_t)p->slices * p->objects : (size_t)p->objects;
+        const size_t object_bytes = object_values * (p->fp64 ? sizeof(double2) : sizeof(float2));
+        uint8_t *stage = static_cast<uint8_t *>(pinned_staging(p->ctx, probe_values * sizeof(double2) + object_bytes));
+        const double2 *probe = reinterpret_cast<const double2 *>(stage);
+        check(cudaMemcpyAsync(stage, p->probe64.ptr, probe_values * sizeof(double2), cudaMemcpyDeviceToHost, s),
               "download probe");
+        check(cudaMemcpyAsync(stage + probe_values * sizeof(double2), p->object.ptr, object_bytes,
+                              cudaMemcpyDeviceToHost, s), "download object");
+        check(cudaStreamSynchronize(s), "sync");
         if (p->fp64) {
-            std::vector<double2> o((size_t)p->slices * p->objects);
-            check(cudaMemcpyAsync(o.data(), p->object.ptr, o.size() * sizeof(double2), cudaMemcpyDeviceToHost, s), "download object");
-            check(cudaStreamSynchronize(s), "sync");
-            for (size_t j = 0; j < o.size(); j++) { if (ore) ore[j] = o[j].x; if (oim) oim[j] = o[j].y; }
+            const double2 *o = reinterpret_cast<const double2 *>(stage + probe_values * sizeof(double2));
+            for (size_t j = 0; j < object_values; j++) { if (ore) ore[j] = o[j].x; if (oim) oim[j] = o[j].y; }
         } else {
-            std::vector<float2> o((size_t)p->objects);
-            check(cudaMemcpyAsync(o.data(), p->object.ptr, o.size() * sizeof(float2), cudaMemcpyDeviceToHost, s), "download object");
-            check(cudaStreamSynchronize(s), "sync");
-            for (long long j = 0; j < p->objects; j++) { if (ore) ore[j] = o[j].x; if (oim) oim[j] = o[j].y; }
+            const float2 *o = reinterpret_cast<const float2 *>(stage + probe_values * sizeof(double2));
+            for (size_t j = 0; j < object_values; j++) { if (ore) ore[j] = o[j].x; if (oim) oim[j] = o[j].y; }
         }
         for (size_t k = 0; k < probe_values; k++) { if (pre) pre[k] = probe[k].x; if (pim) pim[k] = probe[k].y; }
     });
