@@ -23,8 +23,11 @@ def _items():
     return items
 
 
-def test_batch_matches_individual_reconstructions_bitwise():
+@pytest.mark.parametrize("grouped", ["1", "0"])
+def test_batch_matches_individual_reconstructions_bitwise(monkeypatch, grouped):
+    """Grouped launches (the default) and every item's own launches (CUBO_PTYCHO_BATCH_GROUPED=0) alike."""
     import cubokit_b200 as cb
+    monkeypatch.setenv("CUBO_PTYCHO_BATCH_GROUPED", grouped)
     items = _items()
     batch = cb.Batch(items)
     batch.run(2)
