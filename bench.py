@@ -536,7 +536,9 @@ def run_sharded(args, world, rank, local):
     (strong scaling: the total work is the workload's whatever N is)."""
     import torch
     from cubokit_b200 import sharded, synthetic
-    ds = synthetic.dataset(args.scan, DET, dose=DOSE, step=STEP, pinned=True, device=local)
+    # every rank builds the same inputs (the same seeds) and uploads its own band; pageable host memory, as N ranks
+    # pinning the whole stack each would lock N x 4.3 GB of host memory
+    ds = synthetic.dataset(args.scan, DET, dose=DOSE, step=STEP, pinned=False, device=local)
     P, n = len(ds.positions), DET * DET
     form = "fp32" if args.form == "fp32" else "split_bf16"
     run = sharded.ShardedRun(ds.amplitudes, ds.positions, ds.object_start, ds.probe, precision=form, device=local,
