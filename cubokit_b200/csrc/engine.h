@@ -220,6 +220,13 @@ struct Fft2Plan64 {
     const double2 *tw_rows, *tw_columns;
 };
 cudaError_t launch_fft2_f64(const Fft2Plan64 &p, double2 *data, int batch, bool inverse, cudaStream_t s);
+// global32.cu: the FP32 position pass through global memory (detectors above one CTA's shared memory, sides at most
+// 4096): exit wave + row transforms, column transforms around the projection, inverse row transforms; its squared
+// residual as global32_partials_per_position partials per position.  *launches receives the kernels it enqueued.
+bool global32_applicable(int rows, int columns);
+int global32_partials_per_position(int rows, int columns);
+cudaError_t configure_global32();
+cudaError_t launch_position_pass_global32(const PositionPassArgs<float> &a, int *launches, cudaStream_t s);
 // The FP64 position pass through global memory (any detector whose sides are at most 4096): exit waves into dpsi,
 // batched FFT, projection with the per-position error, inverse FFT.  *launches receives the kernels it enqueued.
 cudaError_t launch_position_pass_global(const PositionPassArgs<double> &a, const Fft2Plan64 &fft, int *launches,

@@ -227,6 +227,7 @@ struct cubo_ptycho_plan {
     bool fast = false;      // 128 x 128 FP32 register-resident position pass
     bool bf16 = false;      // 128 x 128 split-BF16 tensor-core position pass
     bool global64 = false;  // FP64 position pass through global memory (the plane does not fit shared memory)
+    bool global32 = false;  // FP32 position pass through global memory (global32.cu)
     // split-BF16: an iteration runs band by band (position pass, object gather, probe gather of one band of
     // band_size positions at a time) so that a band's residuals stay in L2 between the pass and the gathers
     bool banded = false;
@@ -614,8 +615,10 @@ void build_plan(cubo_ptycho_plan *p, const cubo_ptycho_problem *pr) {
     } else {
         check(p->dpsi.alloc((size_t)p->states * P * n * sizeof(C2<T>)), "cudaMalloc dpsi");
     }
-    p->error_count = p->fast ? (long long)P * fast128_partials_per_position()
-                             : p->bf16 ? (long long)P * bf16_partials_per_position() : P;
+    p->error_count = p->fast     ? (long long)P * fast128_partials_per_position()
+                     : p->bf16     ? (long long)P * bf16_partials_per_position()
+                     : p->global32 ? (long long)P * global32_partials_per_position(p->R, p->C)
+                                   : P;
     if (p->fast || p->plane128) {
         check(p->fault.alloc(sizeof(int)), "cudaMalloc");
         check(cudaMemsetAsync(p->fault.ptr, 0, sizeof(int), s), "memset");
@@ -948,6 +951,13 @@ void enqueue_position_pass(cubo_ptycho_plan *p) {
         int count = 0;
         if constexpr (std::is_same<T, double>::value) {
             timed(p, kPositionPass, 0, [&] { return launch_position_pass_global(pa, fft64(p), &count, s); });
+            p->launches += count;
+            if (p->timing) p->kind_launches[kPositionPass] += count;
+        }
+    } else if (p->global32) {
+        int count = 0;
+        if constexpr (std::is_same<T, float>::value) {
+            timed(p, kPositionPass, 0, [&] { return launch_position_pass_global32(pa, &count, s); });
             p->launches += count;
             if (p->timing) p->kind_launches[kPositionPass] += count;
         }
@@ -1586,14 +1596,19 @@ int create_plan(cubo_ptycho_context *ctx, const cubo_ptycho_problem *pr, const c
             check(configure_plane128(), "configure plane transform");
             p->plane_cluster = plane128_cluster();
         }
-        if (!smem_pass && !(p->global64 && line_fft_supported(p->R, p->C)))
+        // FP32 planes too large for one CTA (or any size with the global variant): rows and columns through global memory
+        p->global32 = !p->fp64 && pp->form != CUBO_PTYCHO_FORM_SPLIT_BF16 &&
+                      (!smem_pass || pp->variant == CUBO_PTYCHO_VARIANT_GLOBAL) && global32_applicable(p->R, p->C);
+        if (p->global32) check(configure_global32(), "configure global-memory FP32 pass");
+        if (!smem_pass && !(p->global64 && line_fft_supported(p->R, p->C)) && !p->global32)
             fail(CUBO_PTYCHO_UNSUPPORTED, "detector of " + std::to_string(p->n) + " pixels exceeds the shared-memory "
                                               "transform of this form");
         check(configure_kernels(), "configure kernels");
         check(configure_fft_lines(), "configure line transforms");
         p->bf16 = pp->form == CUBO_PTYCHO_FORM_SPLIT_BF16;
         if (p->bf16) check(configure_bf16(), "configure split-BF16 kernel");
-        p->fast = !p->fp64 && !p->bf16 && pp->variant != CUBO_PTYCHO_VARIANT_GENERIC && fast128_applicable(p->R, p->C);
+        p->fast = !p->fp64 && !p->bf16 && !p->global32 && pp->variant != CUBO_PTYCHO_VARIANT_GENERIC &&
+                  fast128_applicable(p->R, p->C);
         if (p->fast) check(configure_fast128(), "configure 128 x 128 kernel");
         check(cudaDeviceGetAttribute(&p->sms, cudaDevAttrMultiProcessorCount, ctx->device), "attribute");
         if (p->bf16 || p->fast) {
@@ -2173,7 +2188,7 @@ void build_groups(cubo_ptycho_batch *b) {
         if (p->states != 1 || p->multislice || p->banded || p->correct_positions) continue;
         if (p->fp64) ensure_dpsi<double>(p);
         else ensure_dpsi<float>(p);
-        const bool generic_pass = p->fp64 ? !p->global64 && !p->plane128 : !p->fast && !p->bf16;
+        const bool generic_pass = p->fp64 ? !p->global64 && !p->plane128 : !p->fast && !p->bf16 && !p->global32;
         if (generic_pass && position_pass_groupable(p->R, p->C, p->fp64)) {
             add(0, p, p->R, p->params.pass_shape, p->P);
             p->grouped_pass = true;
