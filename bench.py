@@ -811,6 +811,79 @@ def run_mixed(args, world, rank, local):
             "cpu_baseline": cpu, "e2e": None, "gpu_launches": launches, "clocks": clocks.summary()}), flush=True)
 
 
+LARGE_DET, LARGE_SCAN = 256, 64
+
+
+def run_large_detector(args, world, rank, local):
+    """The FP32 form on a 256 x 256 detector (more pixels than one CTA's plane holds: the global-memory pass of
+    global32.cu), a 64^2 raster scan (--scan other than 256 sets it), step 4; one step = one full-batch iteration."""
+    import torch
+    import cubokit_b200 as cb
+    from cubokit_b200 import synthetic
+    from oracle import c_oracle
+    scan = LARGE_SCAN if args.scan == SCAN else args.scan
+    ds = synthetic.dataset(scan, LARGE_DET, dose=DOSE, step=STEP, pinned=True, device=local)
+    P, n = len(ds.positions), LARGE_DET * LARGE_DET
+    ctx = cb.Context(local)
+    stream = torch.cuda.ExternalStream(ctx.stream, device=torch.device("cuda", local))
+    plan = cb.Plan(ds.amplitudes, ds.positions, ds.object_start.shape, ds.probe.shape, ctx=ctx, step_size=0.5,
+                   precision="fp32")
+    plan.set_state(ds.object_start, ds.probe)
+    plan.enqueue(args.warmup)
+    ctx.synchronize()
+    barrier(world)
+    start_ev, stop_ev = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    launches0 = plan.launch_count
+    with ClockSampler(local) as clocks:
+        start_ev.record(stream)
+        plan.enqueue(args.steps)
+        stop_ev.record(stream)
+        stop_ev.synchronize()
+    ms = max_over_ranks(start_ev.elapsed_time(stop_ev), world)
+    launches = plan.launch_count - launches0
+    errors = plan.errors(args.warmup + args.steps)
+    plan.set_timing(True)
+    timed_iterations = max(2, min(args.steps, 4))
+    plan.enqueue(timed_iterations)
+    stats = plan.kernel_stats()
+    plan.set_timing(False)
+    plan.close()
+    value = P * args.steps / (ms * 1e-3) * world
+    _pk = measured_peaks()
+    hbm_peak, peak_kind = _pk["hbm_gbs"], _pk["kind"]
+    pass_ms = stats["position_pass"][0] / timed_iterations
+    pass_bytes = P * 4 * n  # algorithmic: the amplitudes, once
+    moved = P * 44 * n  # the three launches: 8n written, 8n + 4n read and 8n written, 8n read and 8n written
+    cpu = None
+    if rank == 0 and not args.no_cpu:
+        threads = c_oracle.host_cores()
+        sample = min(P, 256)
+        t = cpu_iteration(ds.amplitudes.reshape(P, -1), ds.positions, ds.object_start, ds.probe, sample, threads)
+        cpu = {"value": sample / t, "unit": UNIT, "cores": threads, "kind": "port",
+               "sample": f"one GD iteration over the first {sample} of {P} positions (whole detector and object), "
+                         f"FP64 C restatement of the Double path, OpenMP over positions"}
+    if rank == 0:
+        per_kind = {k: round(v[0] / timed_iterations, 3) for k, v in stats.items() if v[1]}
+        print(json.dumps({
+            "metric": f"positions*iter/s, FP32 GD on a {LARGE_DET}^2 detector", "value": value, "unit": UNIT,
+            "n_gpus": world, "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms / args.steps,
+            "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic",
+            "config": {"workload": f"large detector: {P} positions ({scan}^2 raster, step {STEP} px), "
+                                   f"{LARGE_DET}x{LARGE_DET} detector, object {ds.object_start.shape[0]}^2",
+                       "l2": f"amplitudes {P * n * 4 / 1e9:.2f} GB, residuals {P * n * 8 / 1e9:.2f} GB: larger "
+                             f"than L2"},
+            "roofline": {"kernel": "global-memory FP32 position pass (rows with the exit wave, columns around the "
+                                   "projection, inverse rows)",
+                         "bound": "hbm", "achieved": pass_bytes / (pass_ms * 1e-3) / 1e9, "peak": hbm_peak,
+                         "unit": "GB/s", "frac": pass_bytes / (pass_ms * 1e-3) / 1e9 / hbm_peak,
+                         "peak_kind": peak_kind, "launch_ms": pass_ms,
+                         "moved_gbs": moved / (pass_ms * 1e-3) / 1e9,
+                         "note": "algorithmic bytes 4n per position; the three launches move 44n",
+                         "traffic": None},
+            "kernel_ms_per_iteration": per_kind, "errors_first_last": [errors[0], errors[-1]],
+            "cpu_baseline": cpu, "e2e": None, "gpu_launches": launches, "clocks": clocks.summary()}), flush=True)
+
+
 def run_multislice(args, world, rank, local):
     """The multislice engine (MultislicePtychography, FP64) on the precision workload's data: 4 slices of the start
     object 20 A apart at 300 kV and the data's object sampling; one step = one full-batch iteration (forward through
@@ -912,11 +985,14 @@ def main():
     ap.add_argument("--no-batched", action="store_true", help="skip the 64-reconstruction batch in the extras")
     ap.add_argument("--scan", type=int, default=SCAN, help="scan side (the benchmark workload is 256)")
     ap.add_argument("--workload", default="precision",
-                    choices=["precision", "batched", "preprocess", "positions", "mixed", "multislice"],
+                    choices=["precision", "batched", "preprocess", "positions", "mixed", "multislice",
+                             "large_detector"],
                     help="precision: the 256^2-scan 128^2-detector GD (default); batched: 64 independent "
                          "reconstructions of uneven sizes in one graph; preprocess: amplitude preprocessing of the "
-                         "precision workload's cube; positions: GD with position correction (FP64 form); mixed: the mixed-state "
-                         "engine with 4 probe states (FP64); multislice: the multislice engine with 4 slices (FP64)")
+                         "precision workload's cube; positions: GD with position correction (FP64 form); mixed: "
+                         "the mixed-state engine with 4 probe states (FP64); multislice: the multislice engine with 4 "
+                         "slices (FP64); "
+                         "large_detector: the FP32 form on a 256^2 detector (64^2 scan unless --scan is given)")
     args = ap.parse_args()
     world, rank, local = dist_setup(args)
     if args.impl == "reference":
@@ -945,6 +1021,9 @@ def main():
         return
     if args.workload == "multislice":
         run_multislice(args, world, rank, local)
+        return
+    if args.workload == "large_detector":
+        run_large_detector(args, world, rank, local)
         return
 
     if world > 1:

@@ -23,6 +23,8 @@ namespace {
 
 constexpr int kG32Threads = 256;
 constexpr int kG32MaxN = 4096;  // complex64 elements of the lines one CTA holds (32 KB)
+// CTAs per SM: 4 for the compile-time plans (64 registers, no spills), 2 for the run-time plan (its per-stage arrays
+// spill at either count)
 
 __device__ __forceinline__ int g32_wrap(int v, int size) { return v < 0 ? v + size : (v >= size ? v - size : v); }
 
@@ -52,8 +54,8 @@ __device__ __forceinline__ void g32_lines_fft(float2 *D, const LineGeom &g, cons
 // window corner-centred and periodic in the object), else the rows dpsi holds; transformed along the row (forward, or
 // inverse with inv) and written to dpsi.
 template <int R0, int R1, int R2>
-__global__ void __launch_bounds__(kG32Threads, 2) g32_rows_kernel(PositionPassArgs<float> a, int nl, int exit_wave,
-                                                                  int inv) {
+__global__ void __launch_bounds__(kG32Threads, R0 ? 4 : 2)
+    g32_rows_kernel(PositionPassArgs<float> a, int nl, int exit_wave, int inv) {
     extern __shared__ __align__(16) unsigned char smem_raw[];
     float2 *D = reinterpret_cast<float2 *>(smem_raw);
     const int L = a.columns;
@@ -84,7 +86,7 @@ __global__ void __launch_bounds__(kG32Threads, 2) g32_rows_kernel(PositionPassAr
 // projection (Ptychography.swift:338-349) with the inverse's 1/n folded in and its squared residual, inverse column
 // transforms.  The residual of the CTA's pixels goes to error[p (columns / nl) + c0 / nl].
 template <int R0, int R1, int R2>
-__global__ void __launch_bounds__(kG32Threads, 2) g32_columns_kernel(PositionPassArgs<float> a, int nl) {
+__global__ void __launch_bounds__(kG32Threads, R0 ? 4 : 2) g32_columns_kernel(PositionPassArgs<float> a, int nl) {
     extern __shared__ __align__(16) unsigned char smem_raw[];
     __shared__ double scratch[kG32Threads / 32];
     float2 *D = reinterpret_cast<float2 *>(smem_raw);

@@ -106,8 +106,9 @@ typedef struct {
      * CUBO_PTYCHO_VARIANT_GENERIC forces the any-size transforms (for cross-checks): the shared-memory one, and for
      * FP64 planes larger than one CTA the batched line transform through global memory instead of the clustered
      * 128 x 128 plane launch;
-     * CUBO_PTYCHO_VARIANT_GLOBAL (FP64 form) forces the position pass through global memory that detectors too large
-     * for one CTA's FP64 plane use (for cross-checks). */
+     * CUBO_PTYCHO_VARIANT_GLOBAL (FP64 and FP32 forms) forces the position pass through global memory that detectors
+     * too large for one CTA's plane use (FP64: above 12,288 pixels; FP32: above 16,384, sides up to 4096) (for
+     * cross-checks). */
     int variant;
     /* Object-gather tile (pixels per CTA, 256 in all): 0 = default (16 x 16), 1 = 32 x 8, 2 = 16 x 16, 3 = 64 x 4
      * (width x height along the residual's contiguous axis).  A performance choice only: every pixel sums the same
