@@ -53,12 +53,15 @@ __device__ __forceinline__ void g32_lines_fft(float2 *D, const LineGeom &g, cons
 // Rows r0 .. r0 + nl - 1 of position p = first + block / (rows / nl): with exit_wave the rows of X = S O[patch] (the
 // window corner-centred and periodic in the object), else the rows dpsi holds; transformed along the row (forward, or
 // inverse with inv) and written to dpsi.
-template <int R0, int R1, int R2>
+// NL > 0 (compile-time plans only): nl == NL and the line length is R0 R1 R2, so the line geometry is a compile-time
+// constant and the transform's index arithmetic folds.
+template <int R0, int R1, int R2, int NL>
 __global__ void __launch_bounds__(kG32Threads, R0 ? 4 : 2)
-    g32_rows_kernel(PositionPassArgs<float> a, int nl, int exit_wave, int inv) {
+    g32_rows_kernel(PositionPassArgs<float> a, int nl_arg, int exit_wave, int inv) {
     extern __shared__ __align__(16) unsigned char smem_raw[];
     float2 *D = reinterpret_cast<float2 *>(smem_raw);
-    const int L = a.columns;
+    const int L = NL ? R0 * (R1 ? R1 : 1) * (R2 ? R2 : 1) : a.columns;
+    const int nl = NL ? NL : nl_arg;
     float2 *tw = D + (size_t)nl * L;
     for (int i = threadIdx.x; i < L; i += kG32Threads) tw[i] = a.tw_columns[i];
     const int per = a.rows / nl;
@@ -85,12 +88,13 @@ __global__ void __launch_bounds__(kG32Threads, R0 ? 4 : 2)
 // D[e nl + j] (consecutive threads read consecutive columns of one row): forward column transforms, the Fourier-modulus
 // projection (Ptychography.swift:338-349) with the inverse's 1/n folded in and its squared residual, inverse column
 // transforms.  The residual of the CTA's pixels goes to error[p (columns / nl) + c0 / nl].
-template <int R0, int R1, int R2>
-__global__ void __launch_bounds__(kG32Threads, R0 ? 4 : 2) g32_columns_kernel(PositionPassArgs<float> a, int nl) {
+template <int R0, int R1, int R2, int NL>
+__global__ void __launch_bounds__(kG32Threads, R0 ? 4 : 2) g32_columns_kernel(PositionPassArgs<float> a, int nl_arg) {
     extern __shared__ __align__(16) unsigned char smem_raw[];
     __shared__ double scratch[kG32Threads / 32];
     float2 *D = reinterpret_cast<float2 *>(smem_raw);
-    const int L = a.rows;
+    const int L = NL ? R0 * (R1 ? R1 : 1) * (R2 ? R2 : 1) : a.rows;
+    const int nl = NL ? NL : nl_arg;
     float2 *tw = D + (size_t)nl * L;
     for (int i = threadIdx.x; i < L; i += kG32Threads) tw[i] = a.tw_rows[i];
     const int per = a.columns / nl;
@@ -141,29 +145,36 @@ size_t g32_smem(int nl, int line_length) { return ((size_t)nl * line_length + li
 using RowsKernel = void (*)(PositionPassArgs<float>, int, int, int);
 using ColumnsKernel = void (*)(PositionPassArgs<float>, int);
 
-// The instance whose compile-time plan is `rad` (line lengths 128, 192, 256, 512), else the run-time plan's.
-template <typename K, K (*Pick)(int)>
-K g32_pick(const Radices &rad) {
+// Which compile-time plan `rad` is: 1..4 for lines of 128 (8 8 2), 192 (8 8 3), 256 (8 8 4), 512 (8 8 8), else 0 (the
+// run-time plan).
+int g32_plan_index(const Radices &rad) {
     auto is = [&](int a, int b, int c) {
         const int want[3] = {a, b, c};
-        const int count = c ? 3 : (b ? 2 : 1);
-        if (rad.count != count) return false;
-        for (int i = 0; i < count; i++)
+        if (rad.count != 3) return false;
+        for (int i = 0; i < 3; i++)
             if (rad.r[i] != want[i]) return false;
         return true;
     };
-    return is(8, 8, 2) ? Pick(1) : is(8, 8, 3) ? Pick(2) : is(8, 8, 4) ? Pick(3) : is(8, 8, 8) ? Pick(4) : Pick(0);
+    return is(8, 8, 2) ? 1 : is(8, 8, 3) ? 2 : is(8, 8, 4) ? 3 : is(8, 8, 8) ? 4 : 0;
 }
-RowsKernel rows_instance(int i) {
-    constexpr RowsKernel k[5] = {g32_rows_kernel<0, 0, 0>, g32_rows_kernel<8, 8, 2>, g32_rows_kernel<8, 8, 3>,
-                                 g32_rows_kernel<8, 8, 4>, g32_rows_kernel<8, 8, 8>};
-    return k[i];
+// The lines per CTA of each plan's folded instance (the largest power of two within kG32MaxN elements).
+constexpr int kFoldLines[5] = {0, 32, 16, 16, 8};
+RowsKernel rows_instance(int i, bool folded) {
+    constexpr RowsKernel k[5] = {g32_rows_kernel<0, 0, 0, 0>, g32_rows_kernel<8, 8, 2, 0>, g32_rows_kernel<8, 8, 3, 0>,
+                                 g32_rows_kernel<8, 8, 4, 0>, g32_rows_kernel<8, 8, 8, 0>};
+    constexpr RowsKernel f[5] = {g32_rows_kernel<0, 0, 0, 0>, g32_rows_kernel<8, 8, 2, 32>,
+                                 g32_rows_kernel<8, 8, 3, 16>, g32_rows_kernel<8, 8, 4, 16>,
+                                 g32_rows_kernel<8, 8, 8, 8>};
+    return folded ? f[i] : k[i];
 }
-ColumnsKernel columns_instance(int i) {
-    constexpr ColumnsKernel k[5] = {g32_columns_kernel<0, 0, 0>, g32_columns_kernel<8, 8, 2>,
-                                    g32_columns_kernel<8, 8, 3>, g32_columns_kernel<8, 8, 4>,
-                                    g32_columns_kernel<8, 8, 8>};
-    return k[i];
+ColumnsKernel columns_instance(int i, bool folded) {
+    constexpr ColumnsKernel k[5] = {g32_columns_kernel<0, 0, 0, 0>, g32_columns_kernel<8, 8, 2, 0>,
+                                    g32_columns_kernel<8, 8, 3, 0>, g32_columns_kernel<8, 8, 4, 0>,
+                                    g32_columns_kernel<8, 8, 8, 0>};
+    constexpr ColumnsKernel f[5] = {g32_columns_kernel<0, 0, 0, 0>, g32_columns_kernel<8, 8, 2, 32>,
+                                    g32_columns_kernel<8, 8, 3, 16>, g32_columns_kernel<8, 8, 4, 16>,
+                                    g32_columns_kernel<8, 8, 8, 8>};
+    return folded ? f[i] : k[i];
 }
 
 }  // namespace
@@ -176,12 +187,15 @@ int global32_partials_per_position(int rows, int columns) { return columns / g32
 
 cudaError_t configure_global32() {
     const int bytes = (int)((kG32MaxN + kG32MaxN) * sizeof(float2));  // nl lines of at most kG32MaxN, one twiddle table
-    for (int i = 0; i < 5; i++) {
-        cudaError_t e = cudaFuncSetAttribute(rows_instance(i), cudaFuncAttributeMaxDynamicSharedMemorySize, bytes);
-        if (e == cudaSuccess)
-            e = cudaFuncSetAttribute(columns_instance(i), cudaFuncAttributeMaxDynamicSharedMemorySize, bytes);
-        if (e != cudaSuccess) return e;
-    }
+    for (int i = 0; i < 5; i++)
+        for (bool folded : {false, true}) {
+            cudaError_t e = cudaFuncSetAttribute(rows_instance(i, folded), cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                                 bytes);
+            if (e == cudaSuccess)
+                e = cudaFuncSetAttribute(columns_instance(i, folded), cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                         bytes);
+            if (e != cudaSuccess) return e;
+        }
     return cudaSuccess;
 }
 
@@ -192,8 +206,9 @@ cudaError_t launch_position_pass_global32(const PositionPassArgs<float> &a, int 
     const int nr = g32_lines(a.columns, a.rows), nc = g32_lines(a.rows, a.columns);
     const int per_r = a.rows / nr, per_c = a.columns / nc;
     const size_t smem_r = g32_smem(nr, a.columns), smem_c = g32_smem(nc, a.rows);
-    const RowsKernel rows_k = g32_pick<RowsKernel, rows_instance>(a.rad_columns);  // row lines: length columns
-    const ColumnsKernel columns_k = g32_pick<ColumnsKernel, columns_instance>(a.rad_rows);
+    const int ir = g32_plan_index(a.rad_columns), ic = g32_plan_index(a.rad_rows);  // row lines: length columns
+    const RowsKernel rows_k = rows_instance(ir, ir > 0 && nr == kFoldLines[ir]);
+    const ColumnsKernel columns_k = columns_instance(ic, ic > 0 && nc == kFoldLines[ic]);
     // batches of positions whose CTAs fit one grid dimension
     const int chunk = (int)std::max<long long>(1, (1LL << 30) / std::max(per_r, per_c));
     int count = 0;
