@@ -266,7 +266,10 @@ class SingleslicePtychography:
 
         ``object`` and ``probe`` are complex 2-D arrays (``PtychographyArray``); ``positions`` is ``(P, 2)`` rows and
         columns in object pixels.  ``error_normalization`` is ``"suppliedAmplitudeEnergy"`` or
-        ``("meanIntensity", m)``.  ``precision`` is ``"fp32"``, ``"split_bf16"`` or ``"fp64"``.
+        ``("meanIntensity", m)``.  ``precision`` is ``"fp32"``, ``"split_bf16"`` (128 x 128 detectors) or ``"fp64"``;
+        FP32 and FP64 take detectors with sides up to 4096.  ``variant`` picks the position-pass kernel:
+        ``"auto"`` (the specialised one for the detector size), ``"generic"`` (the any-size shared-memory transform)
+        or ``"global"`` (the pass through global memory that detectors too large for one CTA use).
         ``is_cancelled`` is polled before every iteration and raises ``CancellationError``; ``progress(completed,
         total)`` runs after each iteration.
         """
