@@ -28,6 +28,15 @@ constexpr int kG32MaxN = 4096;  // complex64 elements of the lines one CTA holds
 
 __device__ __forceinline__ int g32_wrap(int v, int size) { return v < 0 ? v + size : (v >= size ? v - size : v); }
 
+// 16-byte asynchronous copy global -> shared (both addresses 16-byte aligned); completes at g32_copies_wait.
+__device__ __forceinline__ void g32_copy16(uint32_t smem_dst, const void *src) {
+    asm volatile("cp.async.cg.shared.global [%0], [%1], 16;" ::"r"(smem_dst), "l"(src) : "memory");
+}
+__device__ __forceinline__ void g32_copies_commit() { asm volatile("cp.async.commit_group;" ::: "memory"); }
+// Waits until at most `pending` of this thread's committed groups are still in flight.
+template <int pending>
+__device__ __forceinline__ void g32_copies_wait() { asm volatile("cp.async.wait_group %0;" ::"n"(pending) : "memory"); }
+
 // Fixed-order sum over the CTA: warps by shuffles, then thread 0 adds the warp sums in warp order.
 __device__ double g32_block_sum(double v, double *scratch) {
 #pragma unroll
@@ -76,6 +85,11 @@ __global__ void __launch_bounds__(kG32Threads, R0 ? 4 : 2)
             const int x = g32_wrap(cc + corner_offset(e, a.columns), a.object_columns);
             D[i] = cmul(S[i], a.object[(size_t)y * a.object_columns + x]);
         }
+    } else if ((L & 1) == 0) {  // the rows are contiguous and start on a 16-byte boundary: every copy in flight at once
+        const uint32_t d0 = (uint32_t)__cvta_generic_to_shared(D);
+        for (int i = threadIdx.x; i < nl * L / 2; i += kG32Threads) g32_copy16(d0 + 16u * (uint32_t)i, rows + 2 * i);
+        g32_copies_commit();
+        g32_copies_wait<0>();
     } else {
         for (int i = threadIdx.x; i < nl * L; i += kG32Threads) D[i] = rows[i];
     }
@@ -96,24 +110,49 @@ __global__ void __launch_bounds__(kG32Threads, R0 ? 4 : 2) g32_columns_kernel(Po
     const int L = NL ? R0 * (R1 ? R1 : 1) * (R2 ? R2 : 1) : a.rows;
     const int nl = NL ? NL : nl_arg;
     float2 *tw = D + (size_t)nl * L;
+    float *As = reinterpret_cast<float *>(tw + L);  // the CTA's amplitudes, staged like D
     for (int i = threadIdx.x; i < L; i += kG32Threads) tw[i] = a.tw_rows[i];
     const int per = a.columns / nl;
     const int p = a.first + (int)(blockIdx.x / per), c0 = (int)(blockIdx.x % per) * nl;
     float2 *base = a.dpsi + (size_t)p * a.n + c0;
     const float *A = a.amplitudes + (size_t)p * a.n + c0;
-    for (int i = threadIdx.x; i < nl * L; i += kG32Threads) {
-        const int e = i / nl, j = i - e * nl;
-        D[i] = base[(size_t)e * a.columns + j];
+    // nl and the row length multiples of 4 and the column length even (so every copy's source and destination, the
+    // amplitude area As included, start on 16-byte boundaries): the residual columns in pairs and the amplitudes in
+    // fours by asynchronous copies, every copy in flight at once; the amplitudes land while the forward transforms run
+    const bool staged = (nl & 3) == 0 && (a.columns & 3) == 0 && (L & 1) == 0;
+    if (staged) {
+        const uint32_t d0 = (uint32_t)__cvta_generic_to_shared(D), a0 = (uint32_t)__cvta_generic_to_shared(As);
+        const int pairs = nl / 2, quads = nl / 4;
+        for (int i = threadIdx.x; i < pairs * L; i += kG32Threads) {
+            const int e = i / pairs, j = 2 * (i - e * pairs);
+            g32_copy16(d0 + 8u * (uint32_t)(e * nl + j), base + (size_t)e * a.columns + j);
+        }
+        g32_copies_commit();
+        for (int i = threadIdx.x; i < quads * L; i += kG32Threads) {
+            const int e = i / quads, j = 4 * (i - e * quads);
+            g32_copy16(a0 + 4u * (uint32_t)(e * nl + j), A + (size_t)e * a.columns + j);
+        }
+        g32_copies_commit();
+        g32_copies_wait<1>();  // the residual columns; the amplitudes may still be in flight
+    } else {
+        for (int i = threadIdx.x; i < nl * L; i += kG32Threads) {
+            const int e = i / nl, j = i - e * nl;
+            D[i] = base[(size_t)e * a.columns + j];
+            As[i] = A[(size_t)e * a.columns + j];
+        }
     }
     __syncthreads();
     const LineGeom geom{L, nl, nl, 1};
     g32_lines_fft<R0, R1, R2>(D, geom, a.rad_rows, tw, false);
+    if (staged) {
+        g32_copies_wait<0>();
+        __syncthreads();
+    }
     double err = 0;
     for (int i = threadIdx.x; i < nl * L; i += kG32Threads) {
-        const int e = i / nl, j = i - e * nl;
         const float2 f = D[i];
         const float mag = sqrtf(f.x * f.x + f.y * f.y);
-        const float measured = A[(size_t)e * a.columns + j];
+        const float measured = As[i];
         const float miss = measured - mag;
         err += (double)(miss * miss);
         if (mag > 0.f) {
@@ -140,7 +179,11 @@ int g32_lines(int line_length, int lines) {
     return best;
 }
 
-size_t g32_smem(int nl, int line_length) { return ((size_t)nl * line_length + line_length) * sizeof(float2); }
+// Dynamic shared memory: nl lines and the twiddle table (complex64), and for the columns launch the amplitudes (Float32).
+size_t g32_smem(int nl, int line_length, bool amplitudes) {
+    return ((size_t)nl * line_length + line_length) * sizeof(float2) +
+           (amplitudes ? (size_t)nl * line_length * sizeof(float) : 0);
+}
 
 using RowsKernel = void (*)(PositionPassArgs<float>, int, int, int);
 using ColumnsKernel = void (*)(PositionPassArgs<float>, int);
@@ -186,7 +229,8 @@ bool global32_applicable(int rows, int columns) {
 int global32_partials_per_position(int rows, int columns) { return columns / g32_lines(rows, columns); }
 
 cudaError_t configure_global32() {
-    const int bytes = (int)((kG32MaxN + kG32MaxN) * sizeof(float2));  // nl lines of at most kG32MaxN, one twiddle table
+    // at most kG32MaxN elements and their amplitudes, a twiddle table of at most kG32MaxN
+    const int bytes = (int)((kG32MaxN + kG32MaxN) * sizeof(float2) + kG32MaxN * sizeof(float));
     for (int i = 0; i < 5; i++)
         for (bool folded : {false, true}) {
             cudaError_t e = cudaFuncSetAttribute(rows_instance(i, folded), cudaFuncAttributeMaxDynamicSharedMemorySize,
@@ -205,7 +249,7 @@ cudaError_t launch_position_pass_global32(const PositionPassArgs<float> &a, int 
     if (!global32_applicable(a.rows, a.columns)) return cudaErrorInvalidValue;
     const int nr = g32_lines(a.columns, a.rows), nc = g32_lines(a.rows, a.columns);
     const int per_r = a.rows / nr, per_c = a.columns / nc;
-    const size_t smem_r = g32_smem(nr, a.columns), smem_c = g32_smem(nc, a.rows);
+    const size_t smem_r = g32_smem(nr, a.columns, false), smem_c = g32_smem(nc, a.rows, true);
     const int ir = g32_plan_index(a.rad_columns), ic = g32_plan_index(a.rad_rows);  // row lines: length columns
     const RowsKernel rows_k = rows_instance(ir, ir > 0 && nr == kFoldLines[ir]);
     const ColumnsKernel columns_k = columns_instance(ic, ic > 0 && nc == kFoldLines[ic]);
