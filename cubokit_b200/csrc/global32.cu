@@ -13,8 +13,10 @@
 //
 // The line transforms are the shared-memory Stockham stages of the any-size pass (radices 8/4/2/3/5/7, direct DFT for
 // other primes), nl lines of a CTA at a time; nl is the largest divisor of the line count that keeps nl lines within
-// kG32MaxN elements, so a CTA never straddles two positions and every partial belongs to one position.  The FP64 form
-// has its own global-memory pass (launch_position_pass_global).
+// kG32MaxN elements, so a CTA never straddles two positions and every partial belongs to one position.  Where the
+// lengths keep every address on a 16-byte boundary, the column launch brings its residual columns and amplitudes and
+// the inverse row launch its rows into shared memory by asynchronous 16-byte copies, all in flight at once.  The FP64
+// form has its own global-memory pass (launch_position_pass_global).
 #include "engine.h"
 
 namespace cubo {
