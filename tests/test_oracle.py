@@ -342,3 +342,15 @@ def test_multislice_propagators_one_slice_and_refusals():
         no.multislice_reconstruct(**dict(inputs, slice_thicknesses=[10.0]))
     with pytest.raises(no.PtychographyError):
         no.propagators(**dict(args, row_sampling=0.0))
+
+
+@pytest.mark.parametrize("shape,step", [((256, 256), 8), ((160, 200), 8), ((512, 64), 8)])
+def test_c_and_numpy_oracles_agree_on_large_detectors(shape, step):
+    """The C oracle the large-detector GPU tests check against, against the NumPy restatement on the same scenes:
+    detectors above one CTA's plane, square and not, power-of-two and mixed-radix lengths."""
+    s = scenes.raster_scene(scan=3, det=shape[0], step=step, seed=31, shape=shape)
+    amps = s["amplitudes"].astype(np.float32).astype(np.float64)
+    a = c_oracle.reconstruct(amps, s["positions"], s["object"], s["probe"], iterations=2)
+    b = numpy_oracle.reconstruct(amps, s["positions"], s["object"], s["probe"], iterations=2)
+    for x, y in zip(a, b):
+        assert gc.complex_gap(np.asarray(x), np.asarray(y)) < 1e-11, shape
